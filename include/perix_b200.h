@@ -1,0 +1,177 @@
+/* perix_b200 — B200-native (sm_100a) PDDO hot-path backend for PeriX: the C-ABI.
+ *
+ * Plain C types only (no CUDA or torch types), so a C++ PeriX build, ctypes, or any FFI can bind it.
+ * All functions return a pxb_status (0 = success).  On failure pxb_last_error() returns a human-readable
+ * message (thread-local).  There is no CPU fallback: a device failure is returned as an error.
+ *
+ * Conventions (identical to the reference boundary, include/PDSystem/CudaAssemble.h:59-80):
+ *   - node coordinates are xyz-interleaved doubles (3*N), z = 0 in 2D;
+ *   - families are a CSR: neigh_off[N+1] (0-based offsets), neigh_id[nbtot] with 1-BASED node ids;
+ *   - nodal fields are interleaved, entry (i, a) at i*ndof + a;
+ *   - CSR matrices are 0-based with columns sorted per row.
+ *
+ * Functions suffixed _d take DEVICE pointers and enqueue on the context stream without synchronising;
+ * every other function takes HOST pointers and returns after its results are in the caller's buffers.
+ * A context is not re-entrant: one host thread drives it at a time.
+ */
+#ifndef PERIX_B200_H
+#define PERIX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PXB_VERSION 1
+
+typedef enum {
+    PXB_OK = 0,
+    PXB_ERR_INVALID = 1,        /* bad argument or size */
+    PXB_ERR_CUDA = 2,           /* CUDA runtime error (message in pxb_last_error) */
+    PXB_ERR_DEGENERATE = 3,     /* a non-ghost family cannot support the PDDO order */
+    PXB_ERR_OOM = 4,            /* device allocation failed */
+    PXB_ERR_BLOWUP = 5,         /* explicit loop: non-finite or runaway displacement */
+    PXB_ERR_STATE = 6,          /* call order (e.g. step before geometry) */
+    PXB_ERR_UNSUPPORTED = 7     /* configuration outside what this backend implements */
+} pxb_status;
+
+typedef enum { PXB_FP64 = 0, PXB_MIXED = 1 } pxb_precision;
+
+typedef struct pxb_ctx pxb_ctx;
+
+/* ---- library / context --------------------------------------------------------------------------------- */
+int pxb_version(void);
+const char *pxb_last_error(void);
+/* Create a context on CUDA device `device` with its own non-blocking stream. */
+int pxb_ctx_create(int device, pxb_ctx **out);
+int pxb_ctx_destroy(pxb_ctx *ctx);
+/* Use an external stream (cudaStream_t passed as void*), e.g. torch's current stream.  NULL restores the
+ * context's own stream. */
+int pxb_ctx_set_stream(pxb_ctx *ctx, void *stream);
+int pxb_ctx_synchronize(pxb_ctx *ctx);
+/* Device bytes currently held by the context. */
+int pxb_ctx_device_bytes(pxb_ctx *ctx, size_t *bytes);
+/* Kernel launches issued by this context since creation (graph replays count each captured launch). */
+int pxb_ctx_launch_count(pxb_ctx *ctx, long long *count);
+
+/* ---- host-side mesh utilities (C++20, no device work) ------------------------------------------------------
+ * Structured PD lattice with mirrored ghosts, as PDMesh::createPDMesh builds it for an axis-aligned quad4 or
+ * hex8 background mesh (reference src/PDMesh/CreatePDMesh.cpp:451-800): bulk cell centres (x fastest), then
+ * one ghost per boundary face in the reference group order (2D left,right,bottom,top; 3D
+ * left,right,bottom,top,back,front).  Two-phase: call with coords3==NULL to get *n_nodes. */
+int pxb_lattice(int dim, int nx, int ny, int nz, const double *box /* xmin,xmax,ymin,ymax[,zmin,zmax] */,
+                int *n_nodes, double *coords3, double *vols, int *mirror /* 1-based bulk id, 0 for bulk */,
+                int *ghost_group /* -1 bulk, else group index in the order above */, double *dxyz /* 3 */);
+
+/* Family lists in the reference's visit order (reference src/PDMesh/CreatePDMesh.cpp:910-1082), uniform
+ * horizon `radius` (already including the 1e-6 inclusion margin).  cracks: xy segments (4 doubles) and
+ * bounded quads (12 doubles); with force_only=0 a crossing bond is dropped, with force_only=1 it is kept.
+ * Two-phase: neigh_id==NULL fills neigh_off only.  *nbtot receives the directed bond count. */
+int pxb_families(int n, const double *coords3, double radius, int is3d, int ncracks, const double *cracks,
+                 int nplanes, const double *planes, const int *mirror, int force_only, int *neigh_off,
+                 int *neigh_id, long long *nbtot);
+
+/* Crack-crossing test for every bond of the family (reference src/PDMesh/PDMesh.cpp:104-159); out[t]=1
+ * where bond t is cut.  Used to seed force-only notch health. */
+int pxb_crack_cut_mask(int n, const double *coords3, const int *mirror, const int *neigh_off, const int *neigh_id,
+                       int ncracks, const double *cracks, int nplanes, const double *planes, uint8_t *out);
+
+/* CSR sparsity pattern (reference src/MathUtils/SparseMatrix.cpp:73-185).  Two-phase: cols==NULL. */
+int pxb_csr_pattern(int n, int ndof, const int *neigh_off, const int *neigh_id, const int *mirror, int *rowptr,
+                    int *cols, long long *nnz);
+
+/* ---- geometry ------------------------------------------------------------------------------------------------
+ * Upload the reference geometry (replaces the AssembleMesh upload of reference
+ * src/PDSystem/CudaAssembleKernels.cu:1121-1146).  delta = horizon radius (with margin); dx_char =
+ * max(DX,DY,DZ) or 0 to disable the rim volume correction.  mirror (1-based, 0 = none) and layer_index
+ * (ghost layer, 0 bulk) may be NULL. */
+int pxb_set_geometry(pxb_ctx *ctx, int n, int dim, const double *coords3, const double *vols, const int *neigh_off,
+                     const int *neigh_id, double delta, double dx_char, const int *mirror, const int *layer_index);
+
+/* ---- g-functions (reference PDOperators::buildGeometryCache, src/PDOperators/CalcPDOperators.cpp:356-463) ----
+ * Builds the per-bond operator vectors ops[bond*nop+k] for multi-index order `order` on the device.
+ * precision PXB_MIXED accumulates the moment sums in FP32 on delta-scaled bond vectors with compensated
+ * (two-sum) accumulation, keeps the solve and one refinement step in FP64, and stores g in FP32.
+ * Returns PXB_ERR_DEGENERATE when a non-ghost family is degenerate; *n_degenerate / *first_degenerate
+ * (1-based) describe them (either may be NULL).  Deep ghosts (layer > 1) get zero operators. */
+int pxb_gbuild(pxb_ctx *ctx, int order, int precision, int *n_degenerate, int *first_degenerate);
+/* nop of the current operator cache and its multi-index table (pqr: 3*nop ints, may be NULL). */
+int pxb_gbuild_info(pxb_ctx *ctx, int *nop, int *pqr);
+/* Copy the operator cache to host (always returned as double). */
+int pxb_get_ops(pxb_ctx *ctx, double *ops);
+
+/* ---- family-sum derivative apply ---------------------------------------------------------------------------
+ * out[i*nk + s] = sum_t g^{k_s}_it (u_j - u_i) for the nk operator slots in `slots` (0-based into the
+ * multi-index table), for a scalar field u (N).  The adjoint maps ybar (N*nk) to ubar (N) (transpose). */
+int pxb_apply(pxb_ctx *ctx, const double *u, int nk, const int *slots, double *out);
+int pxb_apply_d(pxb_ctx *ctx, const double *u_d, int nk, const int *slots, double *out_d);
+int pxb_apply_adjoint(pxb_ctx *ctx, const double *ybar, int nk, const int *slots, double *ubar);
+int pxb_apply_adjoint_d(pxb_ctx *ctx, const double *ybar_d, int nk, const int *slots, double *ubar_d);
+
+/* ---- explicit_pddo_frac (reference src/ElmtSystem/ExplicitPDDOFracElement.cpp:85-300) --------------------
+ * Material: C11/C12/C66 Navier constants, rho, body force b[dim], uniform critical stretch sc (0 = no
+ * damage), tension_only.  pxb_epf_setup builds the per-bond Navier operator cache (2D Gxx,Gyy,Gxy;
+ * 3D Gxx,Gyy,Gzz,Gxy,Gxz,Gyz) with the g-build kernel and seeds health from `health0` (nbtot, 1/0; NULL =
+ * all intact). */
+int pxb_epf_setup(pxb_ctx *ctx, int precision, double C11, double C12, double C66, double rho, const double *b,
+                  double sc, int tension_only, const uint8_t *health0);
+
+/* One rate evaluation at u (N*dim): damage then force, a = (L+b)/rho (the reference CUDA entry
+ * assembleExplicitPDDOFracAccel).  *n_broken = bonds that broke in this call. */
+int pxb_epf_rate(pxb_ctx *ctx, const double *u, double *accel, long long *n_broken);
+
+/* Boundary-condition program applied after every central-difference update, in list order (reference
+ * BCSystem::presetSolution, src/BCSystem/BCSystem.cpp:114-129).  Entry e: kind 0 Dirichlet (reflect across
+ * the mirror bulk, or direct when direct[e] or no mirror), kind 1 Neumann copy; comp_mask bit a selects
+ * component a; value/velocity dim doubles each (g(t)=value+velocity*t); has_box/box (6 doubles,
+ * inclusive, on node coordinates); nodes 1-based in node_off[e]..node_off[e+1]. */
+int pxb_epf_set_bcs(pxb_ctx *ctx, int nbc, const int *kind, const int *comp_mask, const int *direct,
+                    const double *value, const double *velocity, const int *has_box, const double *box,
+                    const int *node_off, const int *nodes);
+
+/* Central-difference state: u0, v0 (N*dim, v0 may be NULL).  Evaluates a0 (this also applies damage at u0,
+ * exactly like the reference's pre-loop rate call) and forms u^{-1} = u0 - dt v0 + dt^2/2 a0. */
+int pxb_epf_start(pxb_ctx *ctx, const double *u0, const double *v0, double dt);
+/* Advance nsteps uniform steps on the device (captured into CUDA graphs of `chunk` steps; chunk<=0 picks a
+ * default).  Returns PXB_ERR_BLOWUP with *bad_step (1-based) if the reference blow-up guard trips. */
+int pxb_epf_advance(pxb_ctx *ctx, int nsteps, int chunk, int *bad_step);
+/* Read back state: u (N*dim), u_prev (N*dim), health (nbtot, as 1/0 bytes), t.  Any pointer may be NULL. */
+int pxb_epf_get_state(pxb_ctx *ctx, double *u, double *u_prev, uint8_t *health, double *t);
+/* Overwrite state (u, u_prev, health may be NULL to keep). */
+int pxb_epf_set_state(pxb_ctx *ctx, const double *u, const double *u_prev, const uint8_t *health, double t);
+/* Number of broken bonds (health == 0). */
+int pxb_epf_broken_count(pxb_ctx *ctx, long long *n_broken);
+
+/* Bond-force adjoint with a frozen damage mask: given abar = dJ/da (N*dim) at the current u, returns
+ * ubar = (da/du)^T abar (N*dim) and the derivatives of J with respect to C11, C12, C66 (dC[3]).  The
+ * health mask is held fixed (no damage update). Device-pointer variant for torch. */
+int pxb_epf_force_adjoint(pxb_ctx *ctx, const double *u, const double *abar, double *ubar, double *dC);
+int pxb_epf_force_adjoint_d(pxb_ctx *ctx, const double *u_d, const double *abar_d, double *ubar_d, double *dC_d);
+/* Force (rate) with a frozen mask, device pointers, no damage update: a = (L(u)+b)/rho. */
+int pxb_epf_force_frozen_d(pxb_ctx *ctx, const double *u_d, double *a_d);
+
+/* ---- CSR Jacobian value assembly ---------------------------------------------------------------------------
+ * Sets the matrix pattern (from pxb_csr_pattern or the caller) and precomputes the bond -> CSR-slot map
+ * on the device (no binary search per assembly). */
+int pxb_csr_set_pattern(pxb_ctx *ctx, int ndof, const int *rowptr, const int *cols, long long nnz);
+/* Poisson (type 0) / transient diffusion (type 1) residual + Jacobian with K = -dF/dU, RHS = +F (reference
+ * PoissonElement.cpp:26-58, DiffusionElement, FormResidualAndJacobianParallel.cpp:114-171).  f_node: per-node
+ * source (N) or NULL to use the constant f. uold may be NULL when dt == 0. */
+int pxb_assemble_scalar(pxb_ctx *ctx, int type, double coef, double f, const double *f_node, double dt,
+                        const double *u, const double *uold, double *kvals, double *rhs);
+int pxb_assemble_scalar_d(pxb_ctx *ctx, int type, double coef, double f, const double *f_node_d, double dt,
+                          const double *u_d, const double *uold_d, double *kvals_d, double *rhs_d);
+
+/* Conservative Cahn-Hilliard (2 dof) assembly from a host-built lambda-corrected Laplacian lapbond[nbtot],
+ * reverse-bond map rev[nbtot], ghost flags and Picard-frozen mobility (reference
+ * src/PDSystem/CudaAssembleKernels.cu:1277-1323 boundary; physics CahnHilliardElement.cpp:178-292). */
+int pxb_ch_set_geometry(pxb_ctx *ctx, const int *rev, const double *lapbond, const char *isghost);
+int pxb_assemble_ch(pxb_ctx *ctx, double kappa, double chi, double dt, const double *mnode, const double *u,
+                    const double *uold, double *kvals, double *rhs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,13 @@
+"""Test infrastructure only: the oracle.
+
+Two CPU implementations of PeriX's PDDO hot path, used exclusively as checkers by ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline / reference legs of ``bench.py``:
+
+* ``port``  - ``oracle/_ref/libpddo_oracle.so``, a plain-C restatement (``oracle/pddo_oracle.c``);
+* ``ref``   - ``oracle/_ref/libperix_ref.so``, the reference's own hot-path sources compiled by
+  ``oracle/Makefile`` together with ``oracle/ref_harness.cpp``.
+
+The product (``perix_b200``) never imports this package.
+"""
+from .lib import (PortOracle, RefMesh, RefEpf, port_available, ref_available, bc_program_arrays,  # noqa: F401
+                  ORACLE_DIR)

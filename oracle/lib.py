@@ -1,0 +1,405 @@
+"""ctypes bindings for the two oracle libraries (test infrastructure only, see ``oracle/__init__.py``)."""
+import ctypes as C
+import os
+
+import numpy as np
+
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
+_PORT_SO = os.path.join(ORACLE_DIR, "_ref", "libpddo_oracle.so")
+_REF_SO = os.path.join(ORACLE_DIR, "_ref", "libperix_ref.so")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+def _ptr(a, ctype):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ctype))
+
+
+def port_available():
+    return os.path.exists(_PORT_SO)
+
+
+def ref_available():
+    return os.path.exists(_REF_SO)
+
+
+def bc_program_arrays(bcs, dim):
+    """Encode a BC list (dicts with kind/comps/direct/value/velocity/box/nodes) in the harness' C layout.
+
+    kind: "dirichlet" | "neumann"; comps: list of 0-based components; nodes: 1-based ids.
+    """
+    nbc = len(bcs)
+    kind = np.zeros(nbc, np.int32)
+    mask = np.zeros(nbc, np.int32)
+    direct = np.zeros(nbc, np.int32)
+    val = np.zeros(max(1, nbc) * dim, np.float64)
+    vel = np.zeros(max(1, nbc) * dim, np.float64)
+    has_box = np.zeros(nbc, np.int32)
+    box = np.zeros(max(1, nbc) * 6, np.float64)
+    off = np.zeros(nbc + 1, np.int32)
+    nodes = []
+    for e, bc in enumerate(bcs):
+        kind[e] = 0 if bc["kind"] == "dirichlet" else 1
+        for c in bc["comps"]:
+            mask[e] |= 1 << c
+        direct[e] = int(bc.get("direct", False))
+        v = bc.get("value", [0.0] * dim)
+        w = bc.get("velocity", [0.0] * dim)
+        for a in range(dim):
+            val[e * dim + a] = v[a]
+            vel[e * dim + a] = w[a]
+        if bc.get("box") is not None:
+            has_box[e] = 1
+            box[6 * e:6 * e + 6] = np.asarray(bc["box"], np.float64)
+        nodes.extend(int(x) for x in bc["nodes"])
+        off[e + 1] = len(nodes)
+    return dict(nbc=nbc, kind=kind, mask=mask, direct=direct, val=val, vel=vel, has_box=has_box, box=box,
+                off=off, nodes=np.asarray(nodes if nodes else [0], np.int32))
+
+
+class PortOracle:
+    """The plain-C restatement (oracle/pddo_oracle.c)."""
+
+    def __init__(self):
+        if not port_available():
+            raise RuntimeError("oracle not built: run `make -C oracle port`")
+        L = C.CDLL(_PORT_SO)
+        L.orc_qindices.restype = C.c_int
+        L.orc_families.restype = C.c_longlong
+        L.orc_crack_cuts.restype = C.c_int
+        L.orc_gbuild.restype = C.c_int
+        L.orc_csr_pattern.restype = C.c_longlong
+        L.orc_critical_stretch.restype = C.c_double
+        self.L = L
+
+    def qindices(self, dim, order):
+        pqr = np.zeros(3 * 64, np.int32)
+        fact = np.zeros(64, np.int32)
+        nop = self.L.orc_qindices(dim, order, _ptr(pqr, C.c_int), _ptr(fact, C.c_int))
+        return pqr[:3 * nop].reshape(nop, 3).copy(), fact[:nop].copy()
+
+    def families(self, coords3, radius, is3d, cracks=None, planes=None, mirror=None, force_only=False):
+        coords3 = np.ascontiguousarray(coords3, np.float64).reshape(-1)
+        n = coords3.size // 3
+        cr = None if cracks is None or len(cracks) == 0 else np.ascontiguousarray(cracks, np.float64).reshape(-1)
+        pl = None if planes is None or len(planes) == 0 else np.ascontiguousarray(planes, np.float64).reshape(-1)
+        mir = None if mirror is None else np.ascontiguousarray(mirror, np.int32)
+        off = np.zeros(n + 1, np.int32)
+        args = (n, _ptr(coords3, C.c_double), C.c_double(radius), int(is3d), 0 if cr is None else cr.size // 4,
+                _ptr(cr, C.c_double), 0 if pl is None else pl.size // 12, _ptr(pl, C.c_double),
+                _ptr(mir, C.c_int), int(force_only))
+        nb = self.L.orc_families(*args, _ptr(off, C.c_int), None)
+        ids = np.zeros(max(1, nb), np.int32)
+        self.L.orc_families(*args, _ptr(off, C.c_int), _ptr(ids, C.c_int))
+        return off, ids[:nb]
+
+    def crack_cuts(self, coords3, mirror, cracks, planes, i1, j1):
+        coords3 = np.ascontiguousarray(coords3, np.float64).reshape(-1)
+        cr = None if cracks is None or len(cracks) == 0 else np.ascontiguousarray(cracks, np.float64).reshape(-1)
+        pl = None if planes is None or len(planes) == 0 else np.ascontiguousarray(planes, np.float64).reshape(-1)
+        mir = None if mirror is None else np.ascontiguousarray(mirror, np.int32)
+        return bool(self.L.orc_crack_cuts(coords3.size // 3, _ptr(coords3, C.c_double), _ptr(mir, C.c_int),
+                                          0 if cr is None else cr.size // 4, _ptr(cr, C.c_double),
+                                          0 if pl is None else pl.size // 12, _ptr(pl, C.c_double), i1, j1))
+
+    def gbuild(self, dim, order, coords3, vols, off, ids, delta, dx_char, volume_correction=True):
+        coords3 = np.ascontiguousarray(coords3, np.float64).reshape(-1)
+        n = coords3.size // 3
+        nop = self.qindices(dim, order)[0].shape[0]
+        ops = np.zeros(int(off[-1]) * nop, np.float64)
+        deg = np.zeros(n, np.uint8)
+        self.L.orc_gbuild(n, dim, order, _ptr(coords3, C.c_double), _ptr(np.ascontiguousarray(vols, np.float64),
+                          C.c_double), _ptr(off, C.c_int), _ptr(ids, C.c_int), C.c_double(delta),
+                          C.c_double(dx_char), int(volume_correction), _ptr(ops, C.c_double), _ptr(deg, C.c_ubyte))
+        return ops.reshape(-1, nop), deg
+
+    def apply(self, off, ids, ops, u):
+        n = off.size - 1
+        nop = ops.shape[1]
+        out = np.zeros(n * nop, np.float64)
+        self.L.orc_apply(n, nop, _ptr(off, C.c_int), _ptr(ids, C.c_int),
+                         _ptr(np.ascontiguousarray(ops, np.float64), C.c_double),
+                         _ptr(np.ascontiguousarray(u, np.float64), C.c_double), _ptr(out, C.c_double))
+        return out.reshape(n, nop)
+
+    def csr_pattern(self, off, ids, mirror, ndof=1):
+        n = off.size - 1
+        rowptr = np.zeros(n * ndof + 1, np.int32)
+        mir = None if mirror is None else np.ascontiguousarray(mirror, np.int32)
+        nnz = self.L.orc_csr_pattern(n, ndof, _ptr(off, C.c_int), _ptr(ids, C.c_int), _ptr(mir, C.c_int),
+                                     _ptr(rowptr, C.c_int), None)
+        cols = np.zeros(max(1, nnz), np.int32)
+        self.L.orc_csr_pattern(n, ndof, _ptr(off, C.c_int), _ptr(ids, C.c_int), _ptr(mir, C.c_int),
+                               _ptr(rowptr, C.c_int), _ptr(cols, C.c_int))
+        return rowptr, cols[:nnz]
+
+    def poisson_assemble(self, dim, off, ids, ops, lapslots, sigma, f, u, rowptr, cols):
+        n = off.size - 1
+        kv = np.zeros(int(rowptr[-1]), np.float64)
+        rhs = np.zeros(n, np.float64)
+        ls = np.ascontiguousarray(lapslots, np.int32)
+        self.L.orc_poisson_assemble(n, dim, ops.shape[1], _ptr(ls, C.c_int), _ptr(off, C.c_int), _ptr(ids, C.c_int),
+                                    _ptr(np.ascontiguousarray(ops, np.float64), C.c_double), C.c_double(sigma),
+                                    _ptr(None if f is None else np.ascontiguousarray(f, np.float64), C.c_double),
+                                    _ptr(np.ascontiguousarray(u, np.float64), C.c_double), _ptr(rowptr, C.c_int),
+                                    _ptr(cols, C.c_int), _ptr(kv, C.c_double), _ptr(rhs, C.c_double))
+        return kv, rhs
+
+    def elastic_constants(self, dim, plane_stress, E, nu):
+        Cv = np.zeros(3, np.float64)
+        self.L.orc_elastic_constants(dim, int(plane_stress), C.c_double(E), C.c_double(nu), _ptr(Cv, C.c_double))
+        return Cv
+
+    def critical_stretch(self, dim, plane_stress, G0, E, delta):
+        return self.L.orc_critical_stretch(dim, int(plane_stress), C.c_double(G0), C.c_double(E), C.c_double(delta))
+
+    def epf_rate(self, dim, coords3, off, ids, navier, Cv, rho, b, sc, u, health, tension_only=True,
+                 damage_on=True):
+        coords3 = np.ascontiguousarray(coords3, np.float64).reshape(-1)
+        n = coords3.size // 3
+        h = np.ascontiguousarray(health, np.float64).copy()
+        acc = np.zeros(n * dim, np.float64)
+        self.L.orc_epf_rate(n, dim, _ptr(coords3, C.c_double), _ptr(off, C.c_int), _ptr(ids, C.c_int),
+                            _ptr(np.ascontiguousarray(navier, np.float64), C.c_double), C.c_double(Cv[0]),
+                            C.c_double(Cv[1]), C.c_double(Cv[2]), C.c_double(rho),
+                            _ptr(np.ascontiguousarray(b, np.float64), C.c_double), C.c_double(sc), int(tension_only),
+                            int(damage_on), _ptr(np.ascontiguousarray(u, np.float64), C.c_double),
+                            _ptr(h, C.c_double), _ptr(acc, C.c_double))
+        return acc, h
+
+    def bc_preset(self, dim, coords3, mirror, bcs, t, u):
+        coords3 = np.ascontiguousarray(coords3, np.float64).reshape(-1)
+        p = bc_program_arrays(bcs, dim)
+        uu = np.ascontiguousarray(u, np.float64).copy()
+        mir = None if mirror is None else np.ascontiguousarray(mirror, np.int32)
+        self.L.orc_bc_preset(coords3.size // 3, dim, _ptr(coords3, C.c_double), _ptr(mir, C.c_int), p["nbc"],
+                             _ptr(p["kind"], C.c_int), _ptr(p["mask"], C.c_int), _ptr(p["direct"], C.c_int),
+                             _ptr(p["val"], C.c_double), _ptr(p["vel"], C.c_double), _ptr(p["has_box"], C.c_int),
+                             _ptr(p["box"], C.c_double), _ptr(p["off"], C.c_int), _ptr(p["nodes"], C.c_int),
+                             C.c_double(t), _ptr(uu, C.c_double))
+        return uu
+
+    def epf_run(self, dim, coords3, mirror, off, ids, navier, Cv, rho, b, sc, u0, v0, dt, nsteps, bcs, health,
+                tension_only=True, damage_on=True):
+        coords3 = np.ascontiguousarray(coords3, np.float64).reshape(-1)
+        n = coords3.size // 3
+        p = bc_program_arrays(bcs, dim)
+        u = np.zeros(n * dim, np.float64)
+        uo = np.zeros(n * dim, np.float64)
+        h = np.ascontiguousarray(health, np.float64).copy()
+        mir = None if mirror is None else np.ascontiguousarray(mirror, np.int32)
+        self.L.orc_epf_run(n, dim, _ptr(coords3, C.c_double), _ptr(mir, C.c_int), _ptr(off, C.c_int),
+                           _ptr(ids, C.c_int), _ptr(np.ascontiguousarray(navier, np.float64), C.c_double),
+                           C.c_double(Cv[0]), C.c_double(Cv[1]), C.c_double(Cv[2]), C.c_double(rho),
+                           _ptr(np.ascontiguousarray(b, np.float64), C.c_double), C.c_double(sc), int(tension_only),
+                           int(damage_on), _ptr(np.ascontiguousarray(u0, np.float64), C.c_double),
+                           _ptr(None if v0 is None else np.ascontiguousarray(v0, np.float64), C.c_double),
+                           C.c_double(dt), int(nsteps), p["nbc"], _ptr(p["kind"], C.c_int), _ptr(p["mask"], C.c_int),
+                           _ptr(p["direct"], C.c_int), _ptr(p["val"], C.c_double), _ptr(p["vel"], C.c_double),
+                           _ptr(p["has_box"], C.c_int), _ptr(p["box"], C.c_double), _ptr(p["off"], C.c_int),
+                           _ptr(p["nodes"], C.c_int), _ptr(u, C.c_double), _ptr(uo, C.c_double), _ptr(h, C.c_double))
+        return u, uo, h
+
+
+_REF = None
+
+
+def _ref_lib():
+    global _REF
+    if _REF is None:
+        if not ref_available():
+            raise RuntimeError("reference harness not built: run `make -C oracle ref` where the reference is present")
+        L = C.CDLL(_REF_SO)
+        vp = C.c_void_p
+        L.ref_mesh_structured.restype = vp
+        L.ref_mesh_cloud.restype = vp
+        L.ref_mesh_nodes.restype = C.c_int
+        L.ref_mesh_bonds.restype = C.c_longlong
+        L.ref_group_size.restype = C.c_int
+        L.ref_crack_cuts.restype = C.c_int
+        L.ref_gbuild_time.restype = C.c_double
+        L.ref_csr_nnz.restype = C.c_int
+        L.ref_poisson_assemble.restype = C.c_double
+        L.ref_epf_create.restype = vp
+        L.ref_epf_rate.restype = C.c_double
+        L.ref_epf_run.restype = C.c_double
+        L.ref_max_threads.restype = C.c_int
+        for name in ("ref_mesh_free", "ref_mesh_nodes", "ref_mesh_bonds", "ref_mesh_scalars", "ref_mesh_get",
+                     "ref_group_size", "ref_group_get", "ref_crack_cuts", "ref_qindices", "ref_gbuild",
+                     "ref_gbuild_time", "ref_apply", "ref_csr_nnz", "ref_csr_pattern", "ref_poisson_assemble",
+                     "ref_epf_free", "ref_epf_rate", "ref_epf_set_health", "ref_epf_constants", "ref_epf_opcache",
+                     "ref_bc_preset", "ref_epf_run"):
+            getattr(L, name).argtypes = None
+        _REF = L
+    return _REF
+
+
+class RefMesh:
+    """A PD mesh built by the reference's own generators/createPDMesh/createNeighborNodes."""
+
+    def __init__(self, handle, dim, order):
+        self.L = _ref_lib()
+        self.h = C.c_void_p(handle)
+        self.dim = dim
+        self.order = order
+        self.n = self.L.ref_mesh_nodes(self.h)
+        self.nb = self.L.ref_mesh_bonds(self.h)
+        sc = np.zeros(6, np.float64)
+        self.L.ref_mesh_scalars(self.h, _ptr(sc, C.c_double))
+        self.delta, self.dx, self.dy, self.dz, self.dx_char, nop = sc
+        self.nop = int(nop)
+        self.coords = np.zeros(3 * self.n, np.float64)
+        self.vols = np.zeros(self.n, np.float64)
+        self.off = np.zeros(self.n + 1, np.int32)
+        self.ids = np.zeros(max(1, self.nb), np.int32)
+        self.mirror = np.zeros(self.n, np.int32)
+        self.L.ref_mesh_get(self.h, _ptr(self.coords, C.c_double), _ptr(self.vols, C.c_double),
+                            _ptr(self.off, C.c_int), _ptr(self.ids, C.c_int), _ptr(self.mirror, C.c_int))
+        self.ids = self.ids[:self.nb]
+
+    @classmethod
+    def structured(cls, dim, nx, ny, nz, box, factor, order=2, cracks=None, planes=None, force_only=False):
+        L = _ref_lib()
+        b = np.ascontiguousarray(list(box) + [0.0] * (6 - len(box)), np.float64)
+        cr = None if not cracks else np.ascontiguousarray(cracks, np.float64).reshape(-1)
+        pl = None if not planes else np.ascontiguousarray(planes, np.float64).reshape(-1)
+        h = L.ref_mesh_structured(int(dim), int(nx), int(ny), int(nz), _ptr(b, C.c_double), C.c_double(factor),
+                                  int(order), int(force_only), 0 if cr is None else cr.size // 4,
+                                  _ptr(cr, C.c_double), 0 if pl is None else pl.size // 12, _ptr(pl, C.c_double))
+        m = cls(h, dim, order)
+        m.cracks = cr
+        m.planes = pl
+        m.force_only = force_only
+        return m
+
+    @classmethod
+    def cloud(cls, dim, coords3, vols, dx, dy, dz, horizon, order=2, volume_correction=True):
+        L = _ref_lib()
+        c = np.ascontiguousarray(coords3, np.float64).reshape(-1)
+        v = np.ascontiguousarray(vols, np.float64)
+        h = L.ref_mesh_cloud(int(dim), c.size // 3, _ptr(c, C.c_double), _ptr(v, C.c_double), C.c_double(dx),
+                             C.c_double(dy), C.c_double(dz), C.c_double(horizon), int(order), int(volume_correction))
+        m = cls(h, dim, order)
+        m.cracks = None
+        m.planes = None
+        m.force_only = False
+        return m
+
+    def group(self, name):
+        k = self.L.ref_group_size(self.h, name.encode())
+        out = np.zeros(max(1, k), np.int32)
+        self.L.ref_group_get(self.h, name.encode(), _ptr(out, C.c_int))
+        return out[:k]
+
+    def crack_cuts(self, i1, j1):
+        return bool(self.L.ref_crack_cuts(self.h, int(i1), int(j1)))
+
+    def qindices(self):
+        pqr = np.zeros(3 * self.nop, np.int32)
+        fact = np.zeros(self.nop, np.int32)
+        self.L.ref_qindices(self.h, _ptr(pqr, C.c_int), _ptr(fact, C.c_int))
+        return pqr.reshape(-1, 3), fact
+
+    def gbuild(self, nthreads=0):
+        ops = np.zeros(self.nb * self.nop, np.float64)
+        deg = np.zeros(self.n, np.uint8)
+        self.L.ref_gbuild(self.h, _ptr(ops, C.c_double), _ptr(deg, C.c_ubyte), int(nthreads or os.cpu_count()))
+        return ops.reshape(-1, self.nop), deg
+
+    def gbuild_time(self, nthreads=0, reps=1):
+        return self.L.ref_gbuild_time(self.h, int(nthreads or os.cpu_count()), int(reps))
+
+    def apply(self, u, nthreads=0):
+        out = np.zeros(self.n * self.nop, np.float64)
+        self.L.ref_apply(self.h, _ptr(np.ascontiguousarray(u, np.float64), C.c_double), _ptr(out, C.c_double),
+                         int(nthreads or os.cpu_count()))
+        return out.reshape(self.n, self.nop)
+
+    def csr_pattern(self, ndof=1):
+        nnz = self.L.ref_csr_nnz(self.h, int(ndof))
+        rowptr = np.zeros(self.n * ndof + 1, np.int32)
+        cols = np.zeros(nnz, np.int32)
+        self.L.ref_csr_pattern(self.h, int(ndof), _ptr(rowptr, C.c_int), _ptr(cols, C.c_int))
+        return rowptr, cols
+
+    def poisson_assemble(self, sigma, f, u, nthreads=0):
+        nnz = self.L.ref_csr_nnz(self.h, 1)
+        kv = np.zeros(nnz, np.float64)
+        rhs = np.zeros(self.n, np.float64)
+        t = self.L.ref_poisson_assemble(self.h, C.c_double(sigma),
+                                        _ptr(None if f is None else np.ascontiguousarray(f, np.float64), C.c_double),
+                                        _ptr(np.ascontiguousarray(u, np.float64), C.c_double), _ptr(kv, C.c_double),
+                                        _ptr(rhs, C.c_double), int(nthreads or os.cpu_count()))
+        return kv, rhs, t
+
+    def bc_preset(self, bcs, t, u):
+        p = bc_program_arrays(bcs, self.dim)
+        uu = np.ascontiguousarray(u, np.float64).copy()
+        self.L.ref_bc_preset(self.h, p["nbc"], _ptr(p["kind"], C.c_int), _ptr(p["mask"], C.c_int),
+                             _ptr(p["direct"], C.c_int), _ptr(p["val"], C.c_double), _ptr(p["vel"], C.c_double),
+                             _ptr(p["has_box"], C.c_int), _ptr(p["box"], C.c_double), _ptr(p["off"], C.c_int),
+                             _ptr(p["nodes"], C.c_int), C.c_double(t), _ptr(uu, C.c_double))
+        return uu
+
+    def __del__(self):
+        try:
+            self.L.ref_mesh_free(self.h)
+        except Exception:
+            pass
+
+
+class RefEpf:
+    """The reference ExplicitPDDOFracElement bound to a RefMesh."""
+
+    def __init__(self, mesh, E, nu, rho, G0, plane_stress=False, tension_only=True, damage_on=True, b=(0, 0, 0)):
+        self.L = _ref_lib()
+        self.mesh = mesh
+        self.h = C.c_void_p(self.L.ref_epf_create(mesh.h, C.c_double(E), C.c_double(nu), C.c_double(rho),
+                                                  C.c_double(G0), int(plane_stress), int(tension_only),
+                                                  int(damage_on), C.c_double(b[0]), C.c_double(b[1]),
+                                                  C.c_double(b[2])))
+
+    def rate(self, u, nthreads=0):
+        m = self.mesh
+        acc = np.zeros(m.n * m.dim, np.float64)
+        h = np.zeros(m.nb, np.float64)
+        t = self.L.ref_epf_rate(self.h, _ptr(np.ascontiguousarray(u, np.float64), C.c_double), _ptr(acc, C.c_double),
+                                _ptr(h, C.c_double), int(nthreads or os.cpu_count()))
+        return acc, h, t
+
+    def set_health(self, h):
+        self.L.ref_epf_set_health(self.h, _ptr(np.ascontiguousarray(h, np.float64), C.c_double))
+
+    def constants(self):
+        out = np.zeros(5, np.float64)
+        self.L.ref_epf_constants(self.h, _ptr(out, C.c_double))
+        return dict(sc=out[0], C11=out[1], C12=out[2], C66=out[3], stable_dt=out[4])
+
+    def opcache(self):
+        nops = 9 if self.mesh.dim == 3 else 5
+        out = np.zeros(self.mesh.nb * nops, np.float64)
+        self.L.ref_epf_opcache(self.h, _ptr(out, C.c_double))
+        return out.reshape(-1, nops)
+
+    def run(self, u0, v0, dt, nsteps, bcs, nthreads=0):
+        m = self.mesh
+        p = bc_program_arrays(bcs, m.dim)
+        u = np.zeros(m.n * m.dim, np.float64)
+        uo = np.zeros(m.n * m.dim, np.float64)
+        h = np.zeros(m.nb, np.float64)
+        t = self.L.ref_epf_run(self.h, _ptr(np.ascontiguousarray(u0, np.float64), C.c_double),
+                               _ptr(None if v0 is None else np.ascontiguousarray(v0, np.float64), C.c_double),
+                               C.c_double(dt), int(nsteps), p["nbc"], _ptr(p["kind"], C.c_int),
+                               _ptr(p["mask"], C.c_int), _ptr(p["direct"], C.c_int), _ptr(p["val"], C.c_double),
+                               _ptr(p["vel"], C.c_double), _ptr(p["has_box"], C.c_int), _ptr(p["box"], C.c_double),
+                               _ptr(p["off"], C.c_int), _ptr(p["nodes"], C.c_int), _ptr(u, C.c_double),
+                               _ptr(uo, C.c_double), _ptr(h, C.c_double), int(nthreads or os.cpu_count()))
+        return u, uo, h, t
+
+    def __del__(self):
+        try:
+            self.L.ref_epf_free(self.h)
+        except Exception:
+            pass

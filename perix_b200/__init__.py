@@ -1,0 +1,12 @@
+"""perix_b200: B200-native (sm_100a) backend for PeriX's PDDO hot path.
+
+The compute path is ``libperix_b200.so`` (C++20 host + hand-written CUDA kernels) behind the C-ABI declared in
+``include/perix_b200.h``; this package is a thin ctypes mirror of that ABI for Python callers, tests and the
+bench.  It never computes on the CPU: if the library is missing, or no GPU is present, the call fails with
+``PxbError``.
+"""
+from .api import (PxbError, Context, lib, lib_path, lattice, families, crack_cut_mask, csr_pattern,  # noqa: F401
+                  multi_indices, elastic_constants, critical_stretch, FP64, MIXED, BC)
+
+__all__ = ["PxbError", "Context", "lib", "lib_path", "lattice", "families", "crack_cut_mask", "csr_pattern",
+           "multi_indices", "elastic_constants", "critical_stretch", "FP64", "MIXED", "BC"]

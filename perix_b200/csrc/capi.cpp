@@ -1,0 +1,1058 @@
+// The extern "C" layer of perix_b200 (C++20 host code).  Every entry point validates its arguments, drives
+// the kernels on the context stream and reports failures as pxb_status codes; there is no CPU fallback.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "k_kernels.h"
+#include "pxb_context.h"
+
+namespace pxb {
+
+static thread_local std::string t_error;
+
+void set_error(const std::string &msg) { t_error = msg; }
+
+int fail(int status, const std::string &msg) {
+    t_error = msg;
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    t_error = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    return (e == cudaErrorMemoryAllocation) ? PXB_ERR_OOM : PXB_ERR_CUDA;
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+PinnedBuf::~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+}
+
+PinnedBuf &PinnedBuf::operator=(PinnedBuf &&o) noexcept {
+    if (this != &o) {
+        if (p) cudaFreeHost(p);
+        p = o.p;
+        bytes = o.bytes;
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    return *this;
+}
+
+int ensure_pinned(PinnedBuf &b, size_t bytes) {
+    if (b.bytes >= bytes) return PXB_OK;
+    if (b.p) cudaFreeHost(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    PXB_CUDA_TRY(cudaMallocHost(&b.p, bytes));
+    b.bytes = bytes;
+    return PXB_OK;
+}
+
+int dev_alloc(pxb_ctx *c, DevBuf &b, size_t bytes) {
+    (void)c;
+    if (b.p && b.bytes == bytes) return PXB_OK;
+    b.release();
+    if (bytes == 0) return PXB_OK;
+    PXB_CUDA_TRY(cudaMalloc(&b.p, bytes));
+    b.bytes = bytes;
+    return PXB_OK;
+}
+
+int h2d(pxb_ctx *c, void *dst, const void *src, size_t bytes) {
+    if (bytes == 0) return PXB_OK;
+    PXB_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    return PXB_OK;
+}
+
+int d2h(pxb_ctx *c, void *dst, const void *src, size_t bytes) {
+    if (bytes == 0) return PXB_OK;
+    PXB_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return PXB_OK;
+}
+
+int dev_upload(pxb_ctx *c, DevBuf &b, const void *host, size_t bytes) {
+    PXB_TRY(dev_alloc(c, b, bytes));
+    return h2d(c, b.p, host, bytes);
+}
+
+int sync(pxb_ctx *c) {
+    PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PXB_OK;
+}
+
+int check_launch(pxb_ctx *c, const char *what) {
+    c->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    return PXB_OK;
+}
+
+static size_t bufsz(const DevBuf &b) { return b.bytes; }
+
+size_t ctx_bytes(const pxb_ctx *c) {
+    size_t s = 0;
+    const Geometry &g = c->g;
+    s += bufsz(g.off) + bufsz(g.nbr) + bufsz(g.pos) + bufsz(g.vol) + bufsz(g.mirror) + bufsz(g.layer) + bufsz(g.rev);
+    s += bufsz(c->ops.ops) + bufsz(c->ops.degenerate);
+    const EpfState &e = c->epf;
+    s += bufsz(e.G) + bufsz(e.health) + bufsz(e.u[0]) + bufsz(e.u[1]) + bufsz(e.accel) + bufsz(e.counters) +
+         bufsz(e.umax) + bufsz(e.tsched);
+    s += bufsz(e.bc.own) + bufsz(e.bc.src_off) + bufsz(e.bc.tgt) + bufsz(e.bc.comp) + bufsz(e.bc.form) +
+         bufsz(e.bc.vals);
+    const CsrState &k = c->csr;
+    s += bufsz(k.rowptr) + bufsz(k.cols) + bufsz(k.slot) + bufsz(k.diag) + bufsz(k.kvals) + bufsz(k.rhs) +
+         bufsz(k.u) + bufsz(k.uold) + bufsz(k.fnode) + bufsz(k.mnode);
+    s += bufsz(c->ch.rev) + bufsz(c->ch.lap) + bufsz(c->ch.ghost) + bufsz(c->scratch);
+    return s;
+}
+
+// scratch device memory for staging (grown on demand, never shrunk)
+static int scratch(pxb_ctx *c, size_t bytes, void **p) {
+    if (c->scratch.bytes < bytes) {
+        c->scratch.release();
+        PXB_CUDA_TRY(cudaMalloc(&c->scratch.p, bytes));
+        c->scratch.bytes = bytes;
+    }
+    *p = c->scratch.p;
+    return PXB_OK;
+}
+
+static int grid_nodes(int n, int threads) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int wpb = threads / 32;
+    const long long need = ((long long)n + wpb - 1) / wpb;
+    const long long cap = (long long)sms * 16;
+    const long long g = std::min(need, cap);
+    return (int)std::max(1LL, g);
+}
+
+static void destroy_graphs(EpfState &e) {
+    for (auto &kv : e.graphs) cudaGraphExecDestroy(kv.second);
+    e.graphs.clear();
+}
+
+}  // namespace pxb
+
+using namespace pxb;
+
+// =============================================================================================== library / ctx
+extern "C" int pxb_version(void) { return PXB_VERSION; }
+
+extern "C" const char *pxb_last_error(void) { return t_error.c_str(); }
+
+extern "C" int pxb_ctx_create(int device, pxb_ctx **out) {
+    if (!out) return fail(PXB_ERR_INVALID, "pxb_ctx_create: out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= 0)
+        return fail(PXB_ERR_CUDA, std::string("pxb_ctx_create: no CUDA device (") + cudaGetErrorString(e) + ")");
+    if (device < 0 || device >= ndev) return fail(PXB_ERR_INVALID, "pxb_ctx_create: device index out of range");
+    PXB_CUDA_TRY(cudaSetDevice(device));
+    auto *c = new pxb_ctx();
+    c->device = device;
+    e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(e, "cudaStreamCreateWithFlags");
+    }
+    c->stream = c->own;
+    *out = c;
+    return PXB_OK;
+}
+
+extern "C" int pxb_ctx_destroy(pxb_ctx *c) {
+    if (!c) return PXB_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    destroy_graphs(c->epf);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+    return PXB_OK;
+}
+
+extern "C" int pxb_ctx_set_stream(pxb_ctx *c, void *stream) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_ctx_set_stream: NULL context");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->own;
+    if (s != c->stream) destroy_graphs(c->epf);
+    c->stream = s;
+    return PXB_OK;
+}
+
+extern "C" int pxb_ctx_synchronize(pxb_ctx *c) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_ctx_synchronize: NULL context");
+    return sync(c);
+}
+
+extern "C" int pxb_ctx_device_bytes(pxb_ctx *c, size_t *bytes) {
+    if (!c || !bytes) return fail(PXB_ERR_INVALID, "pxb_ctx_device_bytes: NULL argument");
+    *bytes = ctx_bytes(c);
+    return PXB_OK;
+}
+
+extern "C" int pxb_ctx_launch_count(pxb_ctx *c, long long *count) {
+    if (!c || !count) return fail(PXB_ERR_INVALID, "pxb_ctx_launch_count: NULL argument");
+    *count = c->launches;
+    return PXB_OK;
+}
+
+// ==================================================================================================== geometry
+extern "C" int pxb_set_geometry(pxb_ctx *c, int n, int dim, const double *coords3, const double *vols,
+                                const int *neigh_off, const int *neigh_id, double delta, double dx_char,
+                                const int *mirror, const int *layer_index) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_set_geometry: NULL context");
+    if (n <= 0 || (dim != 2 && dim != 3) || !coords3 || !vols || !neigh_off || !neigh_id || !(delta > 0.0))
+        return fail(PXB_ERR_INVALID, "pxb_set_geometry: bad arguments (need n>0, dim 2|3, delta>0, non-NULL arrays)");
+    if (neigh_off[0] != 0) return fail(PXB_ERR_INVALID, "pxb_set_geometry: neigh_off[0] must be 0");
+    int maxf = 0;
+    for (int i = 0; i < n; ++i) {
+        const int f = neigh_off[i + 1] - neigh_off[i];
+        if (f < 0) return fail(PXB_ERR_INVALID, "pxb_set_geometry: neigh_off is not non-decreasing");
+        maxf = std::max(maxf, f);
+    }
+    const long long nb = neigh_off[n];
+    for (long long t = 0; t < nb; ++t)
+        if (neigh_id[t] < 1 || neigh_id[t] > n)
+            return fail(PXB_ERR_INVALID, "pxb_set_geometry: neighbour id out of range (ids are 1-based)");
+    PXB_CUDA_TRY(cudaSetDevice(c->device));
+    PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    destroy_graphs(c->epf);
+    c->ops = OpsCache{};
+    c->epf = EpfState{};
+    c->csr = CsrState{};
+    c->ch = ChState{};
+    Geometry &g = c->g;
+    g = Geometry{};
+    g.n = n;
+    g.dim = dim;
+    g.nb = nb;
+    g.delta = delta;
+    g.dx_char = dx_char;
+    g.max_family = maxf;
+    g.h_off.assign(neigh_off, neigh_off + n + 1);
+    if (mirror) g.h_mirror.assign(mirror, mirror + n);
+    PXB_TRY(dev_upload(c, g.off, neigh_off, sizeof(int) * (size_t)(n + 1)));
+    PXB_TRY(dev_alloc(c, g.nbr, sizeof(int) * (size_t)std::max(1LL, nb)));
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, std::max(sizeof(int) * (size_t)std::max(1LL, nb), sizeof(double) * 3 * (size_t)n), &tmp));
+    PXB_TRY(h2d(c, tmp, neigh_id, sizeof(int) * (size_t)nb));
+    if (nb > 0) {
+        launch_ids_to0(nb, static_cast<const int *>(tmp), g.nbr.as<int>(), c->stream);
+        PXB_TRY(check_launch(c, "ids_to0"));
+    }
+    PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    PXB_TRY(h2d(c, tmp, coords3, sizeof(double) * 3 * (size_t)n));
+    PXB_TRY(dev_alloc(c, g.pos, (dim == 2 ? 16 : 32) * (size_t)n));
+    launch_pos_pack(n, dim, static_cast<const double *>(tmp), g.pos.p, c->stream);
+    PXB_TRY(check_launch(c, "pos_pack"));
+    PXB_TRY(dev_upload(c, g.vol, vols, sizeof(double) * (size_t)n));
+    if (mirror) PXB_TRY(dev_upload(c, g.mirror, mirror, sizeof(int) * (size_t)n));
+    if (layer_index) PXB_TRY(dev_upload(c, g.layer, layer_index, sizeof(int) * (size_t)n));
+    PXB_TRY(sync(c));
+    g.ready = true;
+    return PXB_OK;
+}
+
+static int need_geometry(pxb_ctx *c, const char *who) {
+    if (!c) return fail(PXB_ERR_INVALID, std::string(who) + ": NULL context");
+    if (!c->g.ready) return fail(PXB_ERR_STATE, std::string(who) + ": geometry not set (call pxb_set_geometry)");
+    PXB_CUDA_TRY(cudaSetDevice(c->device));
+    return PXB_OK;
+}
+
+static int ensure_rev(pxb_ctx *c) {
+    Geometry &g = c->g;
+    if (g.rev.p) return PXB_OK;
+    PXB_TRY(dev_alloc(c, g.rev, sizeof(int) * (size_t)std::max(1LL, g.nb)));
+    launch_build_rev(g.n, g.off.as<int>(), g.nbr.as<int>(), g.rev.as<int>(), grid_nodes(g.n, kApplyThreads), c->stream);
+    return check_launch(c, "build_rev");
+}
+
+// ===================================================================================================== g-build
+static int run_gbuild(pxb_ctx *c, int order, bool mixed, void *ops_out, void *G_out, uint8_t *deg_out,
+                      int *n_degenerate, int *first_degenerate) {
+    Geometry &g = c->g;
+    if (!gbuild_supported(g.dim, order))
+        return fail(PXB_ERR_UNSUPPORTED, "pxb_gbuild: order " + std::to_string(order) + " not built for dim " +
+                                             std::to_string(g.dim) + " (2D: 1..3, 3D: 1..2)");
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, 16, &tmp));
+    unsigned int *nd = static_cast<unsigned int *>(tmp);
+    int *first = reinterpret_cast<int *>(static_cast<char *>(tmp) + 8);
+    PXB_CUDA_TRY(cudaMemsetAsync(nd, 0, 4, c->stream));
+    const int big = std::numeric_limits<int>::max();
+    PXB_TRY(h2d(c, first, &big, sizeof(int)));
+    GBuildArgs a;
+    a.n = g.n;
+    a.nb = g.nb;
+    a.off = g.off.as<int>();
+    a.nbr = g.nbr.as<int>();
+    a.pos = g.pos.p;
+    a.vol = g.vol.as<double>();
+    a.layer = g.layer.p ? g.layer.as<int>() : nullptr;
+    a.delta = g.delta;
+    a.dx_char = g.dx_char;
+    a.ops = ops_out;
+    a.G = G_out;
+    a.degenerate = deg_out;
+    a.n_degenerate = nd;
+    a.first_degenerate = first;
+    cudaError_t e = launch_gbuild(a, g.dim, order, mixed, grid_nodes(g.n, kGbuildThreads), c->stream);
+    c->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "gbuild launch");
+    unsigned int hnd = 0;
+    int hfirst = big;
+    PXB_TRY(d2h(c, &hnd, nd, 4));
+    PXB_TRY(d2h(c, &hfirst, first, 4));
+    PXB_TRY(sync(c));
+    if (n_degenerate) *n_degenerate = (int)hnd;
+    if (first_degenerate) *first_degenerate = hnd ? hfirst + 1 : 0;
+    if (hnd)
+        return fail(PXB_ERR_DEGENERATE, "degenerate moment matrix at node " + std::to_string(hfirst + 1) + " (" +
+                                            std::to_string(hnd) + " non-ghost node(s)): the family cannot support "
+                                            "this PDDO order");
+    return PXB_OK;
+}
+
+extern "C" int pxb_gbuild(pxb_ctx *c, int order, int precision, int *n_degenerate, int *first_degenerate) {
+    PXB_TRY(need_geometry(c, "pxb_gbuild"));
+    if (precision != PXB_FP64 && precision != PXB_MIXED) return fail(PXB_ERR_INVALID, "pxb_gbuild: bad precision");
+    OpsCache &o = c->ops;
+    o.ready = false;
+    int nop = 0;
+    for (int k = 1; k <= order; ++k) nop += (c->g.dim == 3) ? (k + 1) * (k + 2) / 2 : (k + 1);
+    const size_t es = precision == PXB_MIXED ? 4 : 8;
+    PXB_TRY(dev_alloc(c, o.ops, es * (size_t)nop * (size_t)std::max(1LL, c->g.nb)));
+    PXB_TRY(dev_alloc(c, o.degenerate, (size_t)c->g.n));
+    o.order = order;
+    o.nop = nop;
+    o.precision = precision;
+    o.pqr.clear();
+    for (int k = 1; k <= order; ++k)
+        for (int p = k; p >= 0; --p) {
+            if (c->g.dim == 3)
+                for (int q = k - p; q >= 0; --q) o.pqr.insert(o.pqr.end(), {p, q, k - p - q});
+            else
+                o.pqr.insert(o.pqr.end(), {p, k - p, 0});
+        }
+    const int st = run_gbuild(c, order, precision == PXB_MIXED, o.ops.p, nullptr, o.degenerate.as<uint8_t>(),
+                              n_degenerate, first_degenerate);
+    if (st == PXB_OK || st == PXB_ERR_DEGENERATE) o.ready = true;  // degenerate rows carry zero operators
+    return st;
+}
+
+extern "C" int pxb_gbuild_info(pxb_ctx *c, int *nop, int *pqr) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_gbuild_info: NULL context");
+    if (!c->ops.ready) return fail(PXB_ERR_STATE, "pxb_gbuild_info: no operator cache (call pxb_gbuild)");
+    if (nop) *nop = c->ops.nop;
+    if (pqr) std::copy(c->ops.pqr.begin(), c->ops.pqr.end(), pqr);
+    return PXB_OK;
+}
+
+extern "C" int pxb_get_ops(pxb_ctx *c, double *ops) {
+    PXB_TRY(need_geometry(c, "pxb_get_ops"));
+    if (!c->ops.ready || !ops) return fail(PXB_ERR_STATE, "pxb_get_ops: no operator cache");
+    const size_t cnt = (size_t)c->ops.nop * (size_t)c->g.nb;
+    if (c->ops.precision == PXB_FP64) {
+        PXB_TRY(d2h(c, ops, c->ops.ops.p, cnt * 8));
+        return sync(c);
+    }
+    std::vector<float> tmp(cnt);
+    PXB_TRY(d2h(c, tmp.data(), c->ops.ops.p, cnt * 4));
+    PXB_TRY(sync(c));
+    for (size_t k = 0; k < cnt; ++k) ops[k] = tmp[k];
+    return PXB_OK;
+}
+
+// ======================================================================================================= apply
+static int apply_args(pxb_ctx *c, int nk, const int *slots, ApplyArgs &a, const char *who) {
+    PXB_TRY(need_geometry(c, who));
+    if (!c->ops.ready) return fail(PXB_ERR_STATE, std::string(who) + ": no operator cache (call pxb_gbuild)");
+    if (nk < 1 || nk > 20 || !slots) return fail(PXB_ERR_INVALID, std::string(who) + ": nk must be 1..20");
+    for (int s = 0; s < nk; ++s)
+        if (slots[s] < 0 || slots[s] >= c->ops.nop) return fail(PXB_ERR_INVALID, std::string(who) + ": slot out of range");
+    a.n = c->g.n;
+    a.nop = c->ops.nop;
+    a.nk = nk;
+    for (int s = 0; s < nk; ++s) a.slots[s] = slots[s];
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.ops = c->ops.ops.p;
+    return PXB_OK;
+}
+
+extern "C" int pxb_apply_d(pxb_ctx *c, const double *u_d, int nk, const int *slots, double *out_d) {
+    ApplyArgs a;
+    PXB_TRY(apply_args(c, nk, slots, a, "pxb_apply"));
+    if (!u_d || !out_d) return fail(PXB_ERR_INVALID, "pxb_apply: NULL buffer");
+    a.u = u_d;
+    a.out = out_d;
+    launch_apply(a, c->ops.precision == PXB_MIXED, grid_nodes(a.n, kApplyThreads), c->stream);
+    return check_launch(c, "apply");
+}
+
+extern "C" int pxb_apply(pxb_ctx *c, const double *u, int nk, const int *slots, double *out) {
+    ApplyArgs a;
+    PXB_TRY(apply_args(c, nk, slots, a, "pxb_apply"));
+    if (!u || !out) return fail(PXB_ERR_INVALID, "pxb_apply: NULL buffer");
+    const size_t n = (size_t)c->g.n;
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, sizeof(double) * n * (1 + nk), &tmp));
+    double *du = static_cast<double *>(tmp), *dout = du + n;
+    PXB_TRY(h2d(c, du, u, sizeof(double) * n));
+    PXB_TRY(pxb_apply_d(c, du, nk, slots, dout));
+    PXB_TRY(d2h(c, out, dout, sizeof(double) * n * nk));
+    return sync(c);
+}
+
+extern "C" int pxb_apply_adjoint_d(pxb_ctx *c, const double *ybar_d, int nk, const int *slots, double *ubar_d) {
+    ApplyArgs a;
+    PXB_TRY(apply_args(c, nk, slots, a, "pxb_apply_adjoint"));
+    if (!ybar_d || !ubar_d) return fail(PXB_ERR_INVALID, "pxb_apply_adjoint: NULL buffer");
+    PXB_TRY(ensure_rev(c));
+    a.rev = c->g.rev.as<int>();
+    a.u = ybar_d;
+    a.out = ubar_d;
+    launch_apply_adjoint(a, c->ops.precision == PXB_MIXED, grid_nodes(a.n, kApplyThreads), c->stream);
+    return check_launch(c, "apply_adjoint");
+}
+
+extern "C" int pxb_apply_adjoint(pxb_ctx *c, const double *ybar, int nk, const int *slots, double *ubar) {
+    ApplyArgs a;
+    PXB_TRY(apply_args(c, nk, slots, a, "pxb_apply_adjoint"));
+    if (!ybar || !ubar) return fail(PXB_ERR_INVALID, "pxb_apply_adjoint: NULL buffer");
+    const size_t n = (size_t)c->g.n;
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, sizeof(double) * n * (1 + nk), &tmp));
+    double *dy = static_cast<double *>(tmp), *dout = dy + n * nk;
+    PXB_TRY(h2d(c, dy, ybar, sizeof(double) * n * nk));
+    PXB_TRY(pxb_apply_adjoint_d(c, dy, nk, slots, dout));
+    PXB_TRY(d2h(c, ubar, dout, sizeof(double) * n));
+    return sync(c);
+}
+
+// =========================================================================================== explicit fracture
+static int need_epf(pxb_ctx *c, const char *who) {
+    PXB_TRY(need_geometry(c, who));
+    if (!c->epf.ready) return fail(PXB_ERR_STATE, std::string(who) + ": call pxb_epf_setup first");
+    return PXB_OK;
+}
+
+static EpfArgs epf_args(pxb_ctx *c) {
+    const Geometry &g = c->g;
+    const EpfState &e = c->epf;
+    EpfArgs a;
+    a.n = g.n;
+    a.nb = g.nb;
+    a.off = g.off.as<int>();
+    a.nbr = g.nbr.as<int>();
+    a.pos = g.pos.p;
+    a.G = e.G.p;
+    a.health = e.health.as<uint8_t>();
+    a.C11 = e.C11;
+    a.C12 = e.C12;
+    a.C66 = e.C66;
+    a.rho = e.rho;
+    for (int d = 0; d < 3; ++d) a.b[d] = e.b[d];
+    a.sc = e.sc;
+    a.sc_hi2 = (1.0 + e.sc) * (1.0 + e.sc);
+    a.sc_lo2 = (e.sc < 1.0) ? (1.0 - e.sc) * (1.0 - e.sc) : 0.0;
+    a.damage = e.sc > 0.0 ? 1 : 0;
+    a.tension_only = e.tension_only;
+    a.n_broken = e.counters.as<unsigned long long>();
+    return a;
+}
+
+extern "C" int pxb_epf_setup(pxb_ctx *c, int precision, double C11, double C12, double C66, double rho,
+                             const double *b, double sc, int tension_only, const uint8_t *health0) {
+    PXB_TRY(need_geometry(c, "pxb_epf_setup"));
+    if (precision != PXB_FP64 && precision != PXB_MIXED) return fail(PXB_ERR_INVALID, "pxb_epf_setup: bad precision");
+    if (!(rho > 0.0)) return fail(PXB_ERR_INVALID, "pxb_epf_setup: rho must be > 0");
+    Geometry &g = c->g;
+    EpfState &e = c->epf;
+    destroy_graphs(e);
+    e = EpfState{};
+    e.precision = precision;
+    e.C11 = C11;
+    e.C12 = C12;
+    e.C66 = C66;
+    e.rho = rho;
+    for (int d = 0; d < g.dim; ++d) e.b[d] = b ? b[d] : 0.0;
+    e.sc = sc;
+    e.tension_only = tension_only ? 1 : 0;
+    const int nc = g.dim == 3 ? 6 : 3;
+    const size_t es = precision == PXB_MIXED ? 4 : 8;
+    const size_t nb1 = (size_t)std::max(1LL, g.nb);
+    PXB_TRY(dev_alloc(c, e.G, es * nc * nb1));
+    PXB_TRY(dev_alloc(c, e.health, nb1));
+    PXB_TRY(dev_alloc(c, e.u[0], sizeof(double) * (size_t)g.n * g.dim));
+    PXB_TRY(dev_alloc(c, e.u[1], sizeof(double) * (size_t)g.n * g.dim));
+    PXB_TRY(dev_alloc(c, e.accel, sizeof(double) * (size_t)g.n * g.dim));
+    PXB_TRY(dev_alloc(c, e.counters, sizeof(unsigned long long) * 4));
+    PXB_CUDA_TRY(cudaMemsetAsync(e.counters.p, 0, sizeof(unsigned long long) * 4, c->stream));
+    PXB_CUDA_TRY(cudaMemsetAsync(e.u[0].p, 0, e.u[0].bytes, c->stream));
+    PXB_CUDA_TRY(cudaMemsetAsync(e.u[1].p, 0, e.u[1].bytes, c->stream));
+    if (health0) PXB_TRY(h2d(c, e.health.p, health0, (size_t)g.nb));
+    else PXB_CUDA_TRY(cudaMemsetAsync(e.health.p, 1, (size_t)g.nb, c->stream));
+    int nd = 0, first = 0;
+    const int st = run_gbuild(c, 2, precision == PXB_MIXED, nullptr, e.G.p, nullptr, &nd, &first);
+    if (st != PXB_OK) return st;
+    e.ready = true;
+    return PXB_OK;
+}
+
+extern "C" int pxb_epf_rate(pxb_ctx *c, const double *u, double *accel, long long *n_broken) {
+    PXB_TRY(need_epf(c, "pxb_epf_rate"));
+    if (!u || !accel) return fail(PXB_ERR_INVALID, "pxb_epf_rate: NULL buffer");
+    EpfState &e = c->epf;
+    const size_t nd = (size_t)c->g.n * c->g.dim;
+    PXB_TRY(h2d(c, e.u[e.cur].p, u, sizeof(double) * nd));
+    unsigned long long before = 0, after = 0;
+    PXB_TRY(d2h(c, &before, e.counters.p, 8));
+    EpfArgs a = epf_args(c);
+    a.u = e.u[e.cur].as<double>();
+    a.accel = e.accel.as<double>();
+    launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_RATE, epf_grid(c->g.n), c->stream);
+    PXB_TRY(check_launch(c, "epf rate"));
+    PXB_TRY(d2h(c, accel, e.accel.p, sizeof(double) * nd));
+    PXB_TRY(d2h(c, &after, e.counters.p, 8));
+    PXB_TRY(sync(c));
+    if (n_broken) *n_broken = (long long)(after - before);
+    return PXB_OK;
+}
+
+// ---- BC program: the reference applies BCs one after another (BCSystem.cpp:114-129); each write either
+//      copies/reflects a mirror value or pins g(t).  Symbolic replay on the host reduces every constrained
+//      (node, component) to one of four closed forms in terms of pre-BC values, executed on the device by the
+//      warp of the node whose integrated value it needs (or by the target's own warp for constants). ----------
+namespace {
+struct Sym {
+    int form = -1;  // -1 untouched (= U(self)), 0 U(src), 1 G, 2 2G-U(src), 3 2G-G2
+    int src = -1;
+    double val = 0, vel = 0, val2 = 0, vel2 = 0;
+};
+}  // namespace
+
+extern "C" int pxb_epf_set_bcs(pxb_ctx *c, int nbc, const int *kind, const int *comp_mask, const int *direct,
+                               const double *value, const double *velocity, const int *has_box, const double *box,
+                               const int *node_off, const int *nodes) {
+    PXB_TRY(need_epf(c, "pxb_epf_set_bcs"));
+    Geometry &g = c->g;
+    EpfState &e = c->epf;
+    destroy_graphs(e);
+    e.has_bc = false;
+    e.bc = BcDevice{};
+    if (nbc <= 0) return PXB_OK;
+    if (!kind || !comp_mask || !node_off || !nodes) return fail(PXB_ERR_INVALID, "pxb_epf_set_bcs: NULL array");
+    const int dim = g.dim;
+    // host coordinates are needed for the box test: fetch positions back once
+    std::vector<double> pos((size_t)g.n * (dim == 2 ? 2 : 4));
+    PXB_TRY(d2h(c, pos.data(), g.pos.p, pos.size() * sizeof(double)));
+    PXB_TRY(sync(c));
+    auto X = [&](int i, int a) { return pos[(size_t)i * (dim == 2 ? 2 : 4) + a]; };
+    const std::vector<int> &mir = g.h_mirror;
+    std::vector<Sym> sym((size_t)g.n * dim);
+    auto cur = [&](int node, int comp) -> Sym {
+        Sym s = sym[(size_t)node * dim + comp];
+        if (s.form < 0) { s.form = 0; s.src = node; }
+        return s;
+    };
+    for (int b = 0; b < nbc; ++b) {
+        for (int p = node_off[b]; p < node_off[b + 1]; ++p) {
+            const int id = nodes[p];
+            if (id < 1 || id > g.n) return fail(PXB_ERR_INVALID, "pxb_epf_set_bcs: node id out of range");
+            const int i = id - 1;
+            const int mb = mir.empty() ? 0 : mir[(size_t)i];
+            if (kind[b] == 0) {
+                if (has_box && has_box[b]) {
+                    bool inside = true;
+                    for (int a = 0; a < dim; ++a) {
+                        const double x = X(i, a);
+                        if (x < box[6 * b + 2 * a] || x > box[6 * b + 2 * a + 1]) inside = false;
+                    }
+                    if (!inside) continue;
+                }
+                for (int a = 0; a < dim; ++a) {
+                    if (!((comp_mask[b] >> a) & 1)) continue;
+                    Sym s;
+                    const double v = value ? value[b * dim + a] : 0.0, w = velocity ? velocity[b * dim + a] : 0.0;
+                    if (mb >= 1 && !(direct && direct[b])) {
+                        const Sym m = cur(mb - 1, a);
+                        if (m.form == 0) { s.form = 2; s.src = m.src; s.val = v; s.vel = w; }
+                        else if (m.form == 1) { s.form = 3; s.val = v; s.vel = w; s.val2 = m.val; s.vel2 = m.vel; }
+                        else return fail(PXB_ERR_UNSUPPORTED, "pxb_epf_set_bcs: reflection off a reflected node");
+                    } else {
+                        s.form = 1; s.val = v; s.vel = w;
+                    }
+                    sym[(size_t)i * dim + a] = s;
+                }
+            } else {
+                if (mb < 1) continue;
+                for (int a = 0; a < dim; ++a)
+                    if ((comp_mask[b] >> a) & 1) sym[(size_t)i * dim + a] = cur(mb - 1, a);
+            }
+        }
+    }
+    // group entries by executor node
+    std::vector<uint8_t> own((size_t)g.n, 0);
+    std::vector<std::vector<int>> by((size_t)g.n);
+    int nent = 0;
+    for (int i = 0; i < g.n; ++i)
+        for (int a = 0; a < dim; ++a) {
+            const Sym &s = sym[(size_t)i * dim + a];
+            if (s.form < 0) continue;
+            if (s.form == 0 && s.src == i) continue;  // identity
+            own[(size_t)i] |= (uint8_t)(1u << a);
+            const int ex = (s.form == 0 || s.form == 2) ? s.src : i;
+            by[(size_t)ex].push_back(i * dim + a);
+            ++nent;
+        }
+    std::vector<int> off((size_t)g.n + 1, 0), tgt, comp, form;
+    std::vector<double> val, vel, val2, vel2;
+    for (int i = 0; i < g.n; ++i) {
+        for (int key : by[(size_t)i]) {
+            const Sym &s = sym[(size_t)key];
+            tgt.push_back(key / dim);
+            comp.push_back(key % dim);
+            form.push_back(s.form);
+            val.push_back(s.val);
+            vel.push_back(s.vel);
+            val2.push_back(s.val2);
+            vel2.push_back(s.vel2);
+        }
+        off[(size_t)i + 1] = (int)tgt.size();
+    }
+    BcDevice &d = e.bc;
+    d.n_entries = nent;
+    PXB_TRY(dev_upload(c, d.own, own.data(), own.size()));
+    PXB_TRY(dev_upload(c, d.src_off, off.data(), off.size() * sizeof(int)));
+    if (nent > 0) {
+        PXB_TRY(dev_upload(c, d.tgt, tgt.data(), tgt.size() * sizeof(int)));
+        PXB_TRY(dev_upload(c, d.comp, comp.data(), comp.size() * sizeof(int)));
+        std::vector<double> packed;
+        packed.reserve((size_t)nent * 4);
+        packed.insert(packed.end(), val.begin(), val.end());
+        packed.insert(packed.end(), vel.begin(), vel.end());
+        packed.insert(packed.end(), val2.begin(), val2.end());
+        packed.insert(packed.end(), vel2.begin(), vel2.end());
+        PXB_TRY(dev_upload(c, d.vals, packed.data(), packed.size() * sizeof(double)));
+        PXB_TRY(dev_upload(c, d.form, form.data(), form.size() * sizeof(int)));
+    }
+    PXB_TRY(sync(c));
+    e.has_bc = true;
+    return PXB_OK;
+}
+
+static void fill_bc(const pxb_ctx *c, EpfArgs &a) {
+    const EpfState &e = c->epf;
+    if (!e.has_bc) return;
+    const BcDevice &d = e.bc;
+    const int ne = d.n_entries;
+    a.bc_own = d.own.as<uint8_t>();
+    a.bc_off = d.src_off.as<int>();
+    if (ne > 0) {
+        a.bc_tgt = d.tgt.as<int>();
+        a.bc_comp = d.comp.as<int>();
+        a.bc_form = d.form.as<int>();
+        const double *p = d.vals.as<double>();
+        a.bc_val = p;
+        a.bc_vel = p + ne;
+        a.bc_val2 = p + 2 * (size_t)ne;
+        a.bc_vel2 = p + 3 * (size_t)ne;
+    }
+}
+
+extern "C" int pxb_epf_start(pxb_ctx *c, const double *u0, const double *v0, double dt) {
+    PXB_TRY(need_epf(c, "pxb_epf_start"));
+    if (!u0 || !(dt > 0.0)) return fail(PXB_ERR_INVALID, "pxb_epf_start: need u0 and dt > 0");
+    EpfState &e = c->epf;
+    const size_t nd = (size_t)c->g.n * c->g.dim;
+    e.cur = 0;
+    PXB_TRY(h2d(c, e.u[0].p, u0, sizeof(double) * nd));
+    void *tmp = nullptr;
+    const double *dv0 = nullptr;
+    if (v0) {
+        PXB_TRY(scratch(c, sizeof(double) * nd, &tmp));
+        PXB_TRY(h2d(c, tmp, v0, sizeof(double) * nd));
+        dv0 = static_cast<const double *>(tmp);
+    }
+    EpfArgs a = epf_args(c);
+    a.u = e.u[0].as<double>();
+    a.u_other = e.u[1].as<double>();
+    a.v0 = dv0;
+    a.dt = dt;
+    a.dt2 = 0.5 * dt * dt;
+    launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_START, epf_grid(c->g.n), c->stream);
+    PXB_TRY(check_launch(c, "epf start"));
+    PXB_TRY(sync(c));
+    e.dt = dt;
+    e.t = 0.0;
+    e.step = 0;
+    e.umax_hist.clear();
+    e.started = true;
+    return PXB_OK;
+}
+
+// one STEP launch on stream s: reads u[par], writes u[par^1]
+static int launch_step(pxb_ctx *c, int par, int q, cudaStream_t s) {
+    EpfState &e = c->epf;
+    EpfArgs a = epf_args(c);
+    fill_bc(c, a);
+    a.u = e.u[par].as<double>();
+    a.u_other = e.u[par ^ 1].as<double>();
+    a.dt = e.dt;
+    a.dt2 = e.dt * e.dt;
+    a.t_sched = e.tsched.as<double>();
+    a.step_in_chunk = q;
+    a.umax = e.umax.as<unsigned long long>();
+    const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_STEP, epf_grid(c->g.n), s);
+    if (err != cudaSuccess) return cuda_fail(err, "epf step launch");
+    return PXB_OK;
+}
+
+static int get_graph(pxb_ctx *c, int steps, cudaGraphExec_t *out) {
+    EpfState &e = c->epf;
+    const GraphKey key{steps, e.cur, e.precision};
+    auto it = e.graphs.find(key);
+    if (it != e.graphs.end()) { *out = it->second; return PXB_OK; }
+    // captured on the context's own stream (never the legacy default stream), replayed on c->stream
+    cudaGraph_t graph = nullptr;
+    PXB_CUDA_TRY(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
+    int par = e.cur, st = PXB_OK;
+    for (int q = 0; q < steps && st == PXB_OK; ++q) {
+        st = launch_step(c, par, q, c->own);
+        par ^= 1;
+    }
+    cudaError_t ce = cudaStreamEndCapture(c->own, &graph);
+    if (st != PXB_OK) { if (graph) cudaGraphDestroy(graph); return st; }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    cudaGraphExec_t exec = nullptr;
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+    e.graphs[key] = exec;
+    *out = exec;
+    return PXB_OK;
+}
+
+// reference blow-up guard (TimeStepping.cpp:550-573): 50-step window, x1e3 growth, non-finite
+static int check_blowup(EpfState &e, const unsigned long long *keys, int steps, int *bad_step) {
+    for (int q = 0; q < steps; ++q) {
+        double umax;
+        std::memcpy(&umax, &keys[q], sizeof(double));
+        const long long step = e.step + q + 1;
+        const bool finite = umax <= std::numeric_limits<double>::max();
+        double cap = std::numeric_limits<double>::infinity();
+        if (step > 50) cap = 1.0e3 * std::max(1.0, e.umax_hist[(size_t)(step - 1 - 50)]);
+        if (!finite || umax > cap) {
+            if (bad_step) *bad_step = (int)step;
+            return fail(PXB_ERR_BLOWUP, "explicit loop blew up at step " + std::to_string(step) +
+                                            (finite ? " (max|U| grew more than 1e3x in 50 steps)" : " (non-finite U)") +
+                                            ": reduce dt below the CFL limit");
+        }
+        e.umax_hist.push_back(umax);
+    }
+    return PXB_OK;
+}
+
+extern "C" int pxb_epf_advance(pxb_ctx *c, int nsteps, int chunk, int *bad_step) {
+    PXB_TRY(need_epf(c, "pxb_epf_advance"));
+    EpfState &e = c->epf;
+    if (!e.started) return fail(PXB_ERR_STATE, "pxb_epf_advance: call pxb_epf_start first");
+    if (nsteps < 0) return fail(PXB_ERR_INVALID, "pxb_epf_advance: nsteps < 0");
+    if (bad_step) *bad_step = 0;
+    if (chunk <= 0) chunk = 200;
+    chunk = std::min(chunk, std::max(1, nsteps));
+    if (e.graph_chunk < chunk) {
+        PXB_TRY(dev_alloc(c, e.umax, sizeof(unsigned long long) * (size_t)chunk));
+        PXB_TRY(dev_alloc(c, e.tsched, sizeof(double) * (size_t)chunk));
+        PXB_TRY(ensure_pinned(e.tsched_h, sizeof(double) * (size_t)chunk * 2 + 16));
+        destroy_graphs(e);
+        e.graph_chunk = chunk;
+    }
+    int done = 0;
+    std::vector<unsigned long long> keys((size_t)chunk);
+    while (done < nsteps) {
+        const int s = std::min(chunk, nsteps - done);
+        double *th = static_cast<double *>(e.tsched_h.p);
+        double t = e.t;
+        for (int q = 0; q < s; ++q) { t = t + e.dt; th[q] = t; }
+        PXB_TRY(h2d(c, e.tsched.p, th, sizeof(double) * (size_t)s));
+        PXB_CUDA_TRY(cudaMemsetAsync(e.umax.p, 0, sizeof(unsigned long long) * (size_t)s, c->stream));
+        cudaGraphExec_t exec = nullptr;
+        PXB_TRY(get_graph(c, s, &exec));
+        PXB_CUDA_TRY(cudaGraphLaunch(exec, c->stream));
+        c->launches += s;
+        PXB_TRY(d2h(c, keys.data(), e.umax.p, sizeof(unsigned long long) * (size_t)s));
+        PXB_TRY(sync(c));
+        const int st = check_blowup(e, keys.data(), s, bad_step);
+        e.cur ^= (s & 1);
+        e.t = t;
+        e.step += s;
+        done += s;
+        if (st != PXB_OK) return st;
+    }
+    return PXB_OK;
+}
+
+extern "C" int pxb_epf_get_state(pxb_ctx *c, double *u, double *u_prev, uint8_t *health, double *t) {
+    PXB_TRY(need_epf(c, "pxb_epf_get_state"));
+    EpfState &e = c->epf;
+    const size_t nd = (size_t)c->g.n * c->g.dim;
+    if (u) PXB_TRY(d2h(c, u, e.u[e.cur].p, sizeof(double) * nd));
+    if (u_prev) PXB_TRY(d2h(c, u_prev, e.u[e.cur ^ 1].p, sizeof(double) * nd));
+    if (health) PXB_TRY(d2h(c, health, e.health.p, (size_t)c->g.nb));
+    if (t) *t = e.t;
+    return sync(c);
+}
+
+extern "C" int pxb_epf_set_state(pxb_ctx *c, const double *u, const double *u_prev, const uint8_t *health, double t) {
+    PXB_TRY(need_epf(c, "pxb_epf_set_state"));
+    EpfState &e = c->epf;
+    const size_t nd = (size_t)c->g.n * c->g.dim;
+    if (u) PXB_TRY(h2d(c, e.u[e.cur].p, u, sizeof(double) * nd));
+    if (u_prev) PXB_TRY(h2d(c, e.u[e.cur ^ 1].p, u_prev, sizeof(double) * nd));
+    if (health) PXB_TRY(h2d(c, e.health.p, health, (size_t)c->g.nb));
+    e.t = t;
+    if (u && u_prev) e.started = true;
+    return sync(c);
+}
+
+extern "C" int pxb_epf_broken_count(pxb_ctx *c, long long *n_broken) {
+    PXB_TRY(need_epf(c, "pxb_epf_broken_count"));
+    if (!n_broken) return fail(PXB_ERR_INVALID, "pxb_epf_broken_count: NULL");
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, 8, &tmp));
+    PXB_CUDA_TRY(cudaMemsetAsync(tmp, 0, 8, c->stream));
+    launch_count_zero(c->g.nb, c->epf.health.as<uint8_t>(), static_cast<unsigned long long *>(tmp), c->stream);
+    PXB_TRY(check_launch(c, "count_zero"));
+    unsigned long long h = 0;
+    PXB_TRY(d2h(c, &h, tmp, 8));
+    PXB_TRY(sync(c));
+    *n_broken = (long long)h;
+    return PXB_OK;
+}
+
+extern "C" int pxb_epf_force_frozen_d(pxb_ctx *c, const double *u_d, double *a_d) {
+    PXB_TRY(need_epf(c, "pxb_epf_force_frozen"));
+    if (!u_d || !a_d) return fail(PXB_ERR_INVALID, "pxb_epf_force_frozen: NULL buffer");
+    EpfArgs a = epf_args(c);
+    a.u = u_d;
+    a.accel = a_d;
+    a.damage = 0;
+    launch_epf(a, c->g.dim, c->epf.precision == PXB_MIXED, EPF_FORCE_FROZEN, epf_grid(c->g.n), c->stream);
+    return check_launch(c, "epf force (frozen mask)");
+}
+
+extern "C" int pxb_epf_force_adjoint_d(pxb_ctx *c, const double *u_d, const double *abar_d, double *ubar_d,
+                                       double *dC_d) {
+    PXB_TRY(need_epf(c, "pxb_epf_force_adjoint"));
+    if (!u_d || !abar_d || !ubar_d) return fail(PXB_ERR_INVALID, "pxb_epf_force_adjoint: NULL buffer");
+    PXB_TRY(ensure_rev(c));
+    const EpfState &e = c->epf;
+    EpfAdjArgs a;
+    a.n = c->g.n;
+    a.nb = c->g.nb;
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.rev = c->g.rev.as<int>();
+    a.G = e.G.p;
+    a.health = e.health.as<uint8_t>();
+    a.C11 = e.C11;
+    a.C12 = e.C12;
+    a.C66 = e.C66;
+    a.inv_rho = 1.0 / e.rho;
+    a.u = u_d;
+    a.abar = abar_d;
+    a.ubar = ubar_d;
+    a.dC = dC_d;
+    if (dC_d) PXB_CUDA_TRY(cudaMemsetAsync(dC_d, 0, 3 * sizeof(double), c->stream));
+    launch_epf_adjoint(a, c->g.dim, e.precision == PXB_MIXED, epf_grid(c->g.n), c->stream);
+    return check_launch(c, "epf adjoint");
+}
+
+extern "C" int pxb_epf_force_adjoint(pxb_ctx *c, const double *u, const double *abar, double *ubar, double *dC) {
+    PXB_TRY(need_epf(c, "pxb_epf_force_adjoint"));
+    if (!u || !abar || !ubar) return fail(PXB_ERR_INVALID, "pxb_epf_force_adjoint: NULL buffer");
+    const size_t nd = (size_t)c->g.n * c->g.dim;
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, sizeof(double) * (3 * nd + 4), &tmp));
+    double *du = static_cast<double *>(tmp), *da = du + nd, *dub = da + nd, *ddc = dub + nd;
+    PXB_TRY(h2d(c, du, u, sizeof(double) * nd));
+    PXB_TRY(h2d(c, da, abar, sizeof(double) * nd));
+    PXB_TRY(pxb_epf_force_adjoint_d(c, du, da, dub, ddc));
+    PXB_TRY(d2h(c, ubar, dub, sizeof(double) * nd));
+    double hdc[3];
+    PXB_TRY(d2h(c, hdc, ddc, sizeof(double) * 3));
+    PXB_TRY(sync(c));
+    if (dC) std::copy(hdc, hdc + 3, dC);
+    return PXB_OK;
+}
+
+// ============================================================================================== CSR assembly
+extern "C" int pxb_csr_set_pattern(pxb_ctx *c, int ndof, const int *rowptr, const int *cols, long long nnz) {
+    PXB_TRY(need_geometry(c, "pxb_csr_set_pattern"));
+    if (ndof < 1 || ndof > 5 || !rowptr || !cols || nnz <= 0) return fail(PXB_ERR_INVALID, "pxb_csr_set_pattern: bad arguments");
+    if (rowptr[(size_t)c->g.n * ndof] != nnz) return fail(PXB_ERR_INVALID, "pxb_csr_set_pattern: rowptr[rows] != nnz");
+    CsrState &k = c->csr;
+    k = CsrState{};
+    k.ndof = ndof;
+    k.nnz = nnz;
+    const size_t rows = (size_t)c->g.n * ndof;
+    PXB_TRY(dev_upload(c, k.rowptr, rowptr, sizeof(int) * (rows + 1)));
+    PXB_TRY(dev_upload(c, k.cols, cols, sizeof(int) * (size_t)nnz));
+    PXB_TRY(dev_alloc(c, k.slot, sizeof(int) * (size_t)std::max(1LL, c->g.nb) * ndof * ndof));
+    PXB_TRY(dev_alloc(c, k.diag, sizeof(int) * (size_t)c->g.n * ndof * ndof));
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, 8, &tmp));
+    PXB_CUDA_TRY(cudaMemsetAsync(tmp, 0, 4, c->stream));
+    CsrMapArgs a;
+    a.n = c->g.n;
+    a.ndof = ndof;
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.rowptr = k.rowptr.as<int>();
+    a.cols = k.cols.as<int>();
+    a.slot = k.slot.as<int>();
+    a.diag = k.diag.as<int>();
+    a.missing = static_cast<int *>(tmp);
+    launch_csr_map(a, c->stream);
+    PXB_TRY(check_launch(c, "csr_map"));
+    int missing = 0;
+    PXB_TRY(d2h(c, &missing, tmp, 4));
+    PXB_TRY(sync(c));
+    if (missing) return fail(PXB_ERR_INVALID, "pxb_csr_set_pattern: pattern lacks " + std::to_string(missing) +
+                                                  " entries required by the families");
+    PXB_TRY(dev_alloc(c, k.kvals, sizeof(double) * (size_t)nnz));
+    PXB_TRY(dev_alloc(c, k.rhs, sizeof(double) * rows));
+    PXB_TRY(dev_alloc(c, k.u, sizeof(double) * rows));
+    PXB_TRY(dev_alloc(c, k.uold, sizeof(double) * rows));
+    k.ready = true;
+    return PXB_OK;
+}
+
+extern "C" int pxb_assemble_scalar_d(pxb_ctx *c, int type, double coef, double f, const double *f_node_d, double dt,
+                                     const double *u_d, const double *uold_d, double *kvals_d, double *rhs_d) {
+    PXB_TRY(need_geometry(c, "pxb_assemble_scalar"));
+    CsrState &k = c->csr;
+    if (!k.ready || k.ndof != 1) return fail(PXB_ERR_STATE, "pxb_assemble_scalar: set a 1-dof pattern first");
+    if (!c->ops.ready || c->ops.order < 2) return fail(PXB_ERR_STATE, "pxb_assemble_scalar: needs a g-build of order >= 2");
+    if (type != 0 && type != 1) return fail(PXB_ERR_INVALID, "pxb_assemble_scalar: type must be 0 (Poisson) or 1 (diffusion)");
+    if (type == 1 && (!(dt > 0.0) || !uold_d)) return fail(PXB_ERR_INVALID, "pxb_assemble_scalar: diffusion is transient-only (dt>0, uold)");
+    if (!u_d || !kvals_d || !rhs_d) return fail(PXB_ERR_INVALID, "pxb_assemble_scalar: NULL buffer");
+    const auto &q = c->ops.pqr;
+    auto slot = [&](int p, int qq, int r) {
+        for (size_t s = 0; s < q.size() / 3; ++s)
+            if (q[3 * s] == p && q[3 * s + 1] == qq && q[3 * s + 2] == r) return (int)s;
+        return -1;
+    };
+    ScalarAsmArgs a;
+    a.n = c->g.n;
+    a.dim = c->g.dim;
+    a.nop = c->ops.nop;
+    a.type = type;
+    a.mixed = c->ops.precision == PXB_MIXED;
+    a.s_xx = slot(2, 0, 0);
+    a.s_yy = slot(0, 2, 0);
+    a.s_zz = c->g.dim == 3 ? slot(0, 0, 2) : -1;
+    a.coef = coef;
+    a.f = f;
+    a.dt = dt;
+    a.f_node = f_node_d;
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.rowptr = k.rowptr.as<int>();
+    a.slot = k.slot.as<int>();
+    a.diag = k.diag.as<int>();
+    a.ops = c->ops.ops.p;
+    a.degenerate = c->ops.degenerate.as<uint8_t>();
+    a.u = u_d;
+    a.uold = uold_d;
+    a.kvals = kvals_d;
+    a.rhs = rhs_d;
+    launch_assemble_scalar(a, c->stream);
+    return check_launch(c, "assemble_scalar");
+}
+
+extern "C" int pxb_assemble_scalar(pxb_ctx *c, int type, double coef, double f, const double *f_node, double dt,
+                                   const double *u, const double *uold, double *kvals, double *rhs) {
+    PXB_TRY(need_geometry(c, "pxb_assemble_scalar"));
+    CsrState &k = c->csr;
+    if (!k.ready) return fail(PXB_ERR_STATE, "pxb_assemble_scalar: set a pattern first");
+    if (!u || !kvals || !rhs) return fail(PXB_ERR_INVALID, "pxb_assemble_scalar: NULL buffer");
+    const size_t n = (size_t)c->g.n;
+    PXB_TRY(h2d(c, k.u.p, u, sizeof(double) * n));
+    if (uold) PXB_TRY(h2d(c, k.uold.p, uold, sizeof(double) * n));
+    if (f_node) {
+        PXB_TRY(dev_alloc(c, k.fnode, sizeof(double) * n));
+        PXB_TRY(h2d(c, k.fnode.p, f_node, sizeof(double) * n));
+    }
+    PXB_TRY(pxb_assemble_scalar_d(c, type, coef, f, f_node ? k.fnode.as<double>() : nullptr, dt, k.u.as<double>(),
+                                  uold ? k.uold.as<double>() : nullptr, k.kvals.as<double>(), k.rhs.as<double>()));
+    PXB_TRY(d2h(c, kvals, k.kvals.p, sizeof(double) * (size_t)k.nnz));
+    PXB_TRY(d2h(c, rhs, k.rhs.p, sizeof(double) * n));
+    return sync(c);
+}
+
+extern "C" int pxb_ch_set_geometry(pxb_ctx *c, const int *rev, const double *lapbond, const char *isghost) {
+    PXB_TRY(need_geometry(c, "pxb_ch_set_geometry"));
+    if (!rev || !lapbond) return fail(PXB_ERR_INVALID, "pxb_ch_set_geometry: NULL array");
+    ChState &h = c->ch;
+    const size_t nb = (size_t)std::max(1LL, c->g.nb);
+    PXB_TRY(dev_upload(c, h.rev, rev, sizeof(int) * (size_t)c->g.nb));
+    if (c->g.nb == 0) PXB_TRY(dev_alloc(c, h.rev, sizeof(int) * nb));
+    PXB_TRY(dev_upload(c, h.lap, lapbond, sizeof(double) * (size_t)c->g.nb));
+    if (isghost) PXB_TRY(dev_upload(c, h.ghost, isghost, (size_t)c->g.n));
+    PXB_TRY(sync(c));
+    h.ready = true;
+    return PXB_OK;
+}
+
+extern "C" int pxb_assemble_ch(pxb_ctx *c, double kappa, double chi, double dt, const double *mnode,
+                               const double *u, const double *uold, double *kvals, double *rhs) {
+    PXB_TRY(need_geometry(c, "pxb_assemble_ch"));
+    CsrState &k = c->csr;
+    if (!k.ready || k.ndof != 2) return fail(PXB_ERR_STATE, "pxb_assemble_ch: set a 2-dof pattern first");
+    if (!c->ch.ready) return fail(PXB_ERR_STATE, "pxb_assemble_ch: call pxb_ch_set_geometry first");
+    if (!(dt > 0.0) || !mnode || !u || !uold || !kvals || !rhs) return fail(PXB_ERR_INVALID, "pxb_assemble_ch: bad arguments (transient-only)");
+    const size_t n = (size_t)c->g.n;
+    PXB_TRY(dev_alloc(c, k.mnode, sizeof(double) * n));
+    PXB_TRY(h2d(c, k.mnode.p, mnode, sizeof(double) * n));
+    PXB_TRY(h2d(c, k.u.p, u, sizeof(double) * 2 * n));
+    PXB_TRY(h2d(c, k.uold.p, uold, sizeof(double) * 2 * n));
+    ChAsmArgs a;
+    a.n = c->g.n;
+    a.kappa = kappa;
+    a.chi = chi;
+    a.dt = dt;
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.rev = c->ch.rev.as<int>();
+    a.lap = c->ch.lap.as<double>();
+    a.vol = c->g.vol.as<double>();
+    a.mnode = k.mnode.as<double>();
+    a.ghost = c->ch.ghost.p ? c->ch.ghost.as<char>() : nullptr;
+    a.rowptr = k.rowptr.as<int>();
+    a.slot = k.slot.as<int>();
+    a.diag = k.diag.as<int>();
+    a.u = k.u.as<double>();
+    a.uold = k.uold.as<double>();
+    a.kvals = k.kvals.as<double>();
+    a.rhs = k.rhs.as<double>();
+    launch_assemble_ch(a, c->stream);
+    PXB_TRY(check_launch(c, "assemble_ch"));
+    PXB_TRY(d2h(c, kvals, k.kvals.p, sizeof(double) * (size_t)k.nnz));
+    PXB_TRY(d2h(c, rhs, k.rhs.p, sizeof(double) * 2 * n));
+    return sync(c);
+}

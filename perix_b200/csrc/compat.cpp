@@ -1,0 +1,188 @@
+// perix_cuda:: drop-in shim over the pxb_* C-ABI (the boundary of reference include/PDSystem/CudaAssemble.h).
+// Structure uploads are cached and redone only when the sizes change, like the reference
+// (src/PDSystem/CudaAssembleKernels.cu:1121-1146); results are copied back into the caller's host arrays.
+#include "../../include/perix_cuda_compat.h"
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+#include "../../include/perix_b200.h"
+
+namespace {
+
+struct ShimState {
+    pxb_ctx *ctx = nullptr;
+    // which structure is resident (0 none, 1 scalar assembly, 2 explicit fracture, 3 Cahn-Hilliard)
+    int kind = 0;
+    int n = 0, nnz = 0, nbtot = 0, nop = 0, ndof = 0, dim = 0;
+    int precision = PXB_FP64;
+};
+
+ShimState g_shim;
+
+bool report(const char *who) {
+    std::fprintf(stderr, "[perix_b200] %s: %s\n", who, pxb_last_error());
+    return false;
+}
+
+bool ensure_ctx() {
+    if (g_shim.ctx) return true;
+    if (pxb_ctx_create(0, &g_shim.ctx) != PXB_OK) return report("context");
+    return true;
+}
+
+int order_of(const perix_cuda::AssembleMesh &m) {
+    int o = 0;
+    for (int k = 0; k < m.nop; ++k) o = std::max(o, m.qp[k] + m.qq[k] + (m.qr ? m.qr[k] : 0));
+    return o;
+}
+
+// the multi-index table the caller passes must be the one the device kernels are compiled for
+// (reference order, src/PDOperators/PDOperators.cpp:51-75)
+bool qtable_matches(const perix_cuda::AssembleMesh &m, int order) {
+    int k = 0;
+    auto check = [&](int p, int q, int r) {
+        const bool ok = k < m.nop && m.qp[k] == p && m.qq[k] == q && (m.qr ? m.qr[k] : 0) == r;
+        ++k;
+        return ok;
+    };
+    for (int o = 1; o <= order; ++o)
+        for (int p = o; p >= 0; --p) {
+            if (m.dim == 3) {
+                for (int q = o - p; q >= 0; --q)
+                    if (!check(p, q, o - p - q)) return false;
+            } else if (!check(p, o - p, 0)) {
+                return false;
+            }
+        }
+    return k == m.nop;
+}
+
+bool upload_mesh(const perix_cuda::AssembleMesh &m, int order) {
+    if (pxb_set_geometry(g_shim.ctx, m.N, m.dim, m.coords, m.vols, m.neigh_off, m.neigh_id, m.delta, m.dx_char,
+                         nullptr, nullptr) != PXB_OK)
+        return report("set_geometry");
+    (void)order;
+    return true;
+}
+
+}  // namespace
+
+namespace perix_cuda {
+
+void shutdown() {
+    if (g_shim.ctx) pxb_ctx_destroy(g_shim.ctx);
+    g_shim = ShimState{};
+}
+
+bool assemble(const AssembleMesh &m, const ElmtParams &p, const OpSlots &s, const double *u, const double *uold,
+              double *out_Kvals, double *out_rhs) {
+    if (m.N <= 0 || p.ndof != 1 || s.dxx < 0 || s.dyy < 0) return false;
+    if (m.nodeHorizon) {
+        std::fprintf(stderr, "[perix_b200] assemble: variable horizon is not supported by this backend\n");
+        return false;
+    }
+    if (!ensure_ctx()) return false;
+    const int order = order_of(m);
+    if (!qtable_matches(m, order)) {
+        std::fprintf(stderr, "[perix_b200] assemble: unexpected multi-index table\n");
+        return false;
+    }
+    const int nbtot = m.neigh_off[m.N];
+    if (g_shim.kind != 1 || g_shim.n != m.N || g_shim.nnz != m.nnz || g_shim.nbtot != nbtot || g_shim.nop != m.nop) {
+        if (!upload_mesh(m, order)) return false;
+        int ndeg = 0, first = 0;
+        const int st = pxb_gbuild(g_shim.ctx, order, PXB_FP64, &ndeg, &first);
+        if (st == PXB_ERR_DEGENERATE)
+            std::fprintf(stderr, "[perix_b200] assemble: %s (rows of those nodes are zeroed)\n", pxb_last_error());
+        else if (st != PXB_OK)
+            return report("gbuild");
+        if (pxb_csr_set_pattern(g_shim.ctx, 1, m.csr_off, m.csr_col, m.nnz) != PXB_OK) return report("csr pattern");
+        g_shim.kind = 1;
+        g_shim.n = m.N;
+        g_shim.nnz = m.nnz;
+        g_shim.nbtot = nbtot;
+        g_shim.nop = m.nop;
+    }
+    const bool diffusion = (p.type == ELMT_DIFFUSION);
+    const int st = pxb_assemble_scalar(g_shim.ctx, diffusion ? 1 : 0, diffusion ? p.D : p.sigma, p.f, nullptr,
+                                       diffusion ? p.dt : 0.0, u, uold, out_Kvals, out_rhs);
+    if (st != PXB_OK) return report("assemble");
+    return true;
+}
+
+bool assembleCahnHilliard(const CahnHilliardMesh &m, const CahnHilliardParams &p, const int *csr_off,
+                          const int *csr_col, int nnz, const double *u, const double *uold, double *out_Kvals,
+                          double *out_rhs) {
+    if (m.N <= 0 || !(p.dt > 0.0)) return false;
+    if (!ensure_ctx()) return false;
+    if (g_shim.kind != 3 || g_shim.n != m.N || g_shim.nnz != nnz || g_shim.nbtot != m.nbtot) {
+        // the conservative CH kernel needs topology, volumes and the host-built Laplacian, not coordinates
+        std::vector<double> zeros((size_t)m.N * 3, 0.0);
+        if (pxb_set_geometry(g_shim.ctx, m.N, 2, zeros.data(), m.vol, m.off, m.nbr, 1.0, 0.0, nullptr, nullptr) != PXB_OK)
+            return report("set_geometry");
+        if (pxb_ch_set_geometry(g_shim.ctx, m.rev, m.lapbond, m.isghost) != PXB_OK) return report("ch geometry");
+        if (pxb_csr_set_pattern(g_shim.ctx, 2, csr_off, csr_col, nnz) != PXB_OK) return report("csr pattern");
+        g_shim.kind = 3;
+        g_shim.n = m.N;
+        g_shim.nnz = nnz;
+        g_shim.nbtot = m.nbtot;
+    }
+    if (pxb_assemble_ch(g_shim.ctx, p.kappa, p.chi, p.dt, m.mnode, u, uold, out_Kvals, out_rhs) != PXB_OK)
+        return report("assembleCahnHilliard");
+    return true;
+}
+
+bool assembleStressCahnHilliard(const AssembleMesh &, const StressCahnHilliardParams &, const OpSlots &, const int *,
+                                const double *, const char *, const double *, const double *, const double *,
+                                const double *, const double *, double *, double *) {
+    std::fprintf(stderr, "[perix_b200] assembleStressCahnHilliard is not implemented by this backend\n");
+    return false;
+}
+
+bool assembleCached(const AssembleMesh &, const CachedParams &, const OpSlots &, const double *, const double *,
+                    const double *, const double *, double *, double *) {
+    std::fprintf(stderr, "[perix_b200] assembleCached is not implemented by this backend\n");
+    return false;
+}
+
+bool assembleExplicitPDDOFracAccel(const AssembleMesh &m, const ExplicitPDDOFracParams &p, const OpSlots &s,
+                                   const double *u, double *health_inout, double *accel_out, int *health_changed) {
+    (void)s;
+    if (health_changed) *health_changed = 0;
+    if (m.N <= 0 || (p.dim != 2 && p.dim != 3)) return false;
+    if (m.nodeHorizon) {
+        std::fprintf(stderr, "[perix_b200] assembleExplicitPDDOFracAccel: variable horizon is not supported\n");
+        return false;
+    }
+    if (!ensure_ctx()) return false;
+    const int nbtot = m.neigh_off[m.N];
+    if (g_shim.kind != 2 || g_shim.n != m.N || g_shim.nbtot != nbtot || g_shim.dim != p.dim) {
+        if (pxb_set_geometry(g_shim.ctx, m.N, p.dim, m.coords, m.vols, m.neigh_off, m.neigh_id, m.delta, m.dx_char,
+                             nullptr, nullptr) != PXB_OK)
+            return report("set_geometry");
+        std::vector<uint8_t> h0((size_t)nbtot);
+        for (int t = 0; t < nbtot; ++t) h0[(size_t)t] = health_inout[t] > 0.0 ? 1 : 0;
+        const double b[3] = {p.bx, p.by, p.bz};
+        const double sc = p.damage_on ? p.sc : 0.0;
+        if (pxb_epf_setup(g_shim.ctx, PXB_FP64, p.C11, p.C12, p.C66, p.rho, b, sc, p.tension_only, h0.data()) != PXB_OK)
+            return report("epf setup");
+        g_shim.kind = 2;
+        g_shim.n = m.N;
+        g_shim.nbtot = nbtot;
+        g_shim.dim = p.dim;
+    }
+    long long broken = 0;
+    if (pxb_epf_rate(g_shim.ctx, u, accel_out, &broken) != PXB_OK) return report("assembleExplicitPDDOFracAccel");
+    if (broken > 0) {
+        std::vector<uint8_t> h((size_t)nbtot);
+        if (pxb_epf_get_state(g_shim.ctx, nullptr, nullptr, h.data(), nullptr) != PXB_OK) return report("health readback");
+        for (int t = 0; t < nbtot; ++t) health_inout[t] = h[(size_t)t] ? 1.0 : 0.0;
+        if (health_changed) *health_changed = 1;
+    }
+    return true;
+}
+
+}  // namespace perix_cuda

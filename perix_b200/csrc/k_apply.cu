@@ -1,0 +1,203 @@
+// Family-sum derivative apply D^k u_i = sum_j g^k_ij (u_j - u_i) and its transpose (reference pattern:
+// PoissonElement::computeNodalProjection, src/ElmtSystem/PoissonElement.cpp:67-105; V_j is baked into g).
+// Plus the small utility kernels (reverse-bond map, layout packing, health conversion, L2 flush).
+#include "k_kernels.h"
+#include "pxb_common.cuh"
+
+namespace pxb {
+
+constexpr int kMaxK = 20;
+
+template <bool MIXED>
+__global__ void __launch_bounds__(kApplyThreads) apply_kernel(ApplyArgs a) {
+    constexpr int WPB = kApplyThreads / kWarp;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
+        const int b0 = a.off[i], b1 = a.off[i + 1];
+        const double ui = a.u[i];
+        double acc[kMaxK];
+        CompF cacc[MIXED ? kMaxK : 1];
+#pragma unroll
+        for (int s = 0; s < kMaxK; ++s) acc[s] = 0.0;
+        for (int t = b0 + lane; t < b1; t += kWarp) {
+            const int j = __ldg(a.nbr + t);
+            const double du = a.u[j] - ui;
+            if constexpr (MIXED) {
+                const float *g = static_cast<const float *>(a.ops) + (size_t)t * a.nop;
+                const float duf = (float)du;
+#pragma unroll
+                for (int s = 0; s < kMaxK; ++s)
+                    if (s < a.nk) cacc[s].add(__ldg(g + a.slots[s]) * duf);
+            } else {
+                const double *g = static_cast<const double *>(a.ops) + (size_t)t * a.nop;
+#pragma unroll
+                for (int s = 0; s < kMaxK; ++s)
+                    if (s < a.nk) acc[s] += __ldg(g + a.slots[s]) * du;
+            }
+        }
+        if constexpr (MIXED) {
+#pragma unroll
+            for (int s = 0; s < kMaxK; ++s) acc[s] = cacc[s].value();
+        }
+        double mine = 0.0;
+#pragma unroll
+        for (int s = 0; s < kMaxK; ++s) {
+            if (s < a.nk) {
+                const double v = group_sum<kWarp>(acc[s]);
+                if (lane == s) mine = v;
+            }
+        }
+        if (lane < a.nk) a.out[(size_t)i * a.nk + lane] = mine;
+    }
+}
+
+// ubar_m = sum_{t in fam(m)} [ sum_s g_{rev t}^s ybar_{j,s} - sum_s g_t^s ybar_{m,s} ]
+template <bool MIXED>
+__global__ void __launch_bounds__(kApplyThreads) apply_adjoint_kernel(ApplyArgs a) {
+    constexpr int WPB = kApplyThreads / kWarp;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    for (int m = blockIdx.x * WPB + wib; m < a.n; m += gridDim.x * WPB) {
+        const int b0 = a.off[m], b1 = a.off[m + 1];
+        double ym[kMaxK];
+#pragma unroll
+        for (int s = 0; s < kMaxK; ++s) ym[s] = (s < a.nk) ? a.u[(size_t)m * a.nk + s] : 0.0;
+        double acc = 0.0;
+        for (int t = b0 + lane; t < b1; t += kWarp) {
+            const int j = __ldg(a.nbr + t);
+            const int r = __ldg(a.rev + t);
+#pragma unroll
+            for (int s = 0; s < kMaxK; ++s) {
+                if (s < a.nk) {
+                    double gt, gr = 0.0;
+                    if constexpr (MIXED) {
+                        gt = (double)__ldg(static_cast<const float *>(a.ops) + (size_t)t * a.nop + a.slots[s]);
+                        if (r >= 0) gr = (double)__ldg(static_cast<const float *>(a.ops) + (size_t)r * a.nop + a.slots[s]);
+                    } else {
+                        gt = __ldg(static_cast<const double *>(a.ops) + (size_t)t * a.nop + a.slots[s]);
+                        if (r >= 0) gr = __ldg(static_cast<const double *>(a.ops) + (size_t)r * a.nop + a.slots[s]);
+                    }
+                    acc += gr * a.u[(size_t)j * a.nk + s] - gt * ym[s];
+                }
+            }
+        }
+        acc = group_sum<kWarp>(acc);
+        if (lane == 0) a.out[m] = acc;
+    }
+}
+
+cudaError_t launch_apply(const ApplyArgs &a, bool mixed, int grid, cudaStream_t s) {
+    if (a.nk > kMaxK) return cudaErrorInvalidValue;
+    if (mixed) apply_kernel<true><<<grid, kApplyThreads, 0, s>>>(a);
+    else apply_kernel<false><<<grid, kApplyThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_apply_adjoint(const ApplyArgs &a, bool mixed, int grid, cudaStream_t s) {
+    if (a.nk > kMaxK) return cudaErrorInvalidValue;
+    if (mixed) apply_adjoint_kernel<true><<<grid, kApplyThreads, 0, s>>>(a);
+    else apply_adjoint_kernel<false><<<grid, kApplyThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// ---- reverse bond: rev[t] = position of i in fam(j) for t = (i -> j), -1 when absent ------------------
+__global__ void build_rev_kernel(int n, const int *off, const int *nbr, int *rev) {
+    constexpr int WPB = kApplyThreads / kWarp;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    for (int i = blockIdx.x * WPB + wib; i < n; i += gridDim.x * WPB) {
+        for (int t = off[i] + lane; t < off[i + 1]; t += kWarp) {
+            const int j = nbr[t];
+            int found = -1;
+            for (int q = off[j]; q < off[j + 1]; ++q)
+                if (nbr[q] == i) { found = q; break; }
+            rev[t] = found;
+        }
+    }
+}
+
+cudaError_t launch_build_rev(int n, const int *off, const int *nbr, int *rev, int grid, cudaStream_t s) {
+    build_rev_kernel<<<grid, kApplyThreads, 0, s>>>(n, off, nbr, rev);
+    return cudaGetLastError();
+}
+
+// ---- layout packing -------------------------------------------------------------------------------------
+__global__ void pos_pack_kernel(int n, int dim, const double *c3, void *pos) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (dim == 2) static_cast<double2 *>(pos)[i] = make_double2(c3[3 * i], c3[3 * i + 1]);
+        else static_cast<double4 *>(pos)[i] = make_double4(c3[3 * i], c3[3 * i + 1], c3[3 * i + 2], 0.0);
+    }
+}
+
+cudaError_t launch_pos_pack(int n, int dim, const double *coords3, void *pos, cudaStream_t s) {
+    const int g = (n + 255) / 256;
+    pos_pack_kernel<<<g > 0 ? g : 1, 256, 0, s>>>(n, dim, coords3, pos);
+    return cudaGetLastError();
+}
+
+__global__ void ids_to0_kernel(long long nb, const int *ids1, int *ids0) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb; t += (long long)gridDim.x * blockDim.x)
+        ids0[t] = ids1[t] - 1;
+}
+
+cudaError_t launch_ids_to0(long long nb, const int *ids1, int *ids0, cudaStream_t s) {
+    long long g = (nb + 255) / 256;
+    if (g > 65535LL * 8) g = 65535LL * 8;
+    ids_to0_kernel<<<(int)(g > 0 ? g : 1), 256, 0, s>>>(nb, ids1, ids0);
+    return cudaGetLastError();
+}
+
+__global__ void health_from_double_kernel(long long nb, const double *h, uint8_t *out) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb; t += (long long)gridDim.x * blockDim.x)
+        out[t] = h[t] > 0.0 ? 1 : 0;
+}
+
+__global__ void health_to_double_kernel(long long nb, const uint8_t *h, double *out) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb; t += (long long)gridDim.x * blockDim.x)
+        out[t] = h[t] ? 1.0 : 0.0;
+}
+
+__global__ void count_zero_kernel(long long nb, const uint8_t *h, unsigned long long *count) {
+    unsigned long long c = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb; t += (long long)gridDim.x * blockDim.x)
+        c += (h[t] == 0);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
+static int grid_for(long long nb) {
+    long long g = (nb + 255) / 256;
+    if (g > 4096) g = 4096;
+    return (int)(g > 0 ? g : 1);
+}
+
+cudaError_t launch_health_from_double(long long nb, const double *h, uint8_t *out, cudaStream_t s) {
+    health_from_double_kernel<<<grid_for(nb), 256, 0, s>>>(nb, h, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_health_to_double(long long nb, const uint8_t *h, double *out, cudaStream_t s) {
+    health_to_double_kernel<<<grid_for(nb), 256, 0, s>>>(nb, h, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_zero(long long nb, const uint8_t *h, unsigned long long *count, cudaStream_t s) {
+    count_zero_kernel<<<grid_for(nb), 256, 0, s>>>(nb, h, count);
+    return cudaGetLastError();
+}
+
+// Writes `bytes` (a multiple of 16) so that the previous working set is evicted from L2.
+__global__ void l2_flush_kernel(uint4 *buf, size_t n16, unsigned seed) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n16; k += (size_t)gridDim.x * blockDim.x)
+        buf[k] = make_uint4(seed, (unsigned)k, seed ^ 0x9e3779b9u, 0u);
+}
+
+cudaError_t launch_l2_flush(void *buf, size_t bytes, cudaStream_t s) {
+    static unsigned seed = 1;
+    l2_flush_kernel<<<1184, 256, 0, s>>>(static_cast<uint4 *>(buf), bytes / 16, seed++);
+    return cudaGetLastError();
+}
+
+}  // namespace pxb

@@ -1,0 +1,171 @@
+// CSR Jacobian value assembly (reference PDSystem::formResidualAndJacobianParallel,
+// src/PDSystem/FormResidualAndJacobianParallel.cpp:114-171, with the element callbacks of
+// src/ElmtSystem/PoissonElement.cpp:26-58, DiffusionElement.cpp and CahnHilliardElement.cpp:178-292).
+//
+// Row ownership: node i owns its ndof rows, so no atomics.  The bond -> CSR slot map is computed once
+// (csr_map_kernel, a binary search per bond at setup), replacing the per-assembly binary search of the
+// reference (devFindSlot, src/PDSystem/CudaAssembleKernels.cu:157-168).  Sign convention K = -dF/dU,
+// RHS = +F.
+#include "k_kernels.h"
+#include "pxb_common.cuh"
+
+namespace pxb {
+
+__device__ __forceinline__ int find_slot(const int *cols, int lo, int hi, int target) {
+    int l = lo, h = hi - 1;
+    while (l <= h) {
+        const int mid = l + ((h - l) >> 1);
+        const int c = cols[mid];
+        if (c == target) return mid;
+        if (c < target) l = mid + 1; else h = mid - 1;
+    }
+    return -1;
+}
+
+__global__ void csr_map_kernel(CsrMapArgs a) {
+    const int nd = a.ndof;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        for (int r = 0; r < nd; ++r) {
+            const int row = i * nd + r;
+            const int lo = a.rowptr[row], hi = a.rowptr[row + 1];
+            for (int c = 0; c < nd; ++c) {
+                const int s = find_slot(a.cols, lo, hi, i * nd + c);
+                a.diag[(size_t)i * nd * nd + r * nd + c] = s;
+                if (s < 0) atomicAdd(a.missing, 1);
+            }
+            for (int t = a.off[i]; t < a.off[i + 1]; ++t) {
+                const int j = a.nbr[t];
+                for (int c = 0; c < nd; ++c) {
+                    const int s = find_slot(a.cols, lo, hi, j * nd + c);
+                    a.slot[(size_t)t * nd * nd + r * nd + c] = s;
+                    if (s < 0) atomicAdd(a.missing, 1);
+                }
+            }
+        }
+    }
+}
+
+cudaError_t launch_csr_map(const CsrMapArgs &a, cudaStream_t s) {
+    const int g = (a.n + 127) / 128;
+    csr_map_kernel<<<g > 0 ? g : 1, 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// ---- scalar elements: Poisson (type 0): coeff = sigma*Lap, R_n = f;  diffusion (type 1): coeff = -D*Lap,
+//      R_n = (u-uold)/dt - f, K_n = 1/dt.  Bond: R = coeff (u_j-u_i), K_II = -coeff, K_IJ = coeff. ----------
+template <bool MIXED>
+__global__ void __launch_bounds__(256) assemble_scalar_kernel(ScalarAsmArgs a) {
+    constexpr int WPB = 256 / kWarp;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
+        const int r0 = a.rowptr[i], r1 = a.rowptr[i + 1];
+        for (int s = r0 + lane; s < r1; s += kWarp) a.kvals[s] = 0.0;
+        __syncwarp();
+        if (a.degenerate && a.degenerate[i]) {  // reference GPU: a singular moment system zeroes the row
+            if (lane == 0) a.rhs[i] = 0.0;
+            continue;
+        }
+        const double ui = a.u[i];
+        const int b0 = a.off[i], b1 = a.off[i + 1];
+        double rsum = 0.0, dsum = 0.0;
+        for (int t = b0 + lane; t < b1; t += kWarp) {
+            const int j = __ldg(a.nbr + t);
+            double lap;
+            if constexpr (MIXED) {
+                const float *g = static_cast<const float *>(a.ops) + (size_t)t * a.nop;
+                lap = (double)g[a.s_xx] + (double)g[a.s_yy];
+                if (a.dim >= 3) lap += (double)g[a.s_zz];
+            } else {
+                const double *g = static_cast<const double *>(a.ops) + (size_t)t * a.nop;
+                lap = g[a.s_xx] + g[a.s_yy];
+                if (a.dim >= 3) lap += g[a.s_zz];
+            }
+            const double coeff = (a.type == 0) ? a.coef * lap : -a.coef * lap;
+            rsum += coeff * (a.u[j] - ui);
+            dsum += coeff;                       // -K_II
+            a.kvals[a.slot[t]] = -coeff;         // -K_IJ
+        }
+        rsum = group_sum<kWarp>(rsum);
+        dsum = group_sum<kWarp>(dsum);
+        if (lane == 0) {
+            double rn, kn;
+            const double fi = a.f_node ? a.f_node[i] : a.f;
+            if (a.type == 0) { rn = fi; kn = 0.0; }
+            else { rn = (ui - a.uold[i]) / a.dt - fi; kn = 1.0 / a.dt; }
+            a.kvals[a.diag[i]] = -kn + dsum;
+            a.rhs[i] = rn + rsum;
+        }
+    }
+}
+
+cudaError_t launch_assemble_scalar(const ScalarAsmArgs &a, cudaStream_t s) {
+    const int g = (a.n + 7) / 8;
+    if (a.mixed) assemble_scalar_kernel<true><<<g > 0 ? g : 1, 256, 0, s>>>(a);
+    else assemble_scalar_kernel<false><<<g > 0 ? g : 1, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// ---- conservative Cahn-Hilliard (2 dof: c, mu) ------------------------------------------------------------
+__device__ __forceinline__ double ch_clamp(double c) { return fmax(1.0e-8, fmin(1.0 - 1.0e-8, c)); }
+
+__global__ void __launch_bounds__(256) assemble_ch_kernel(ChAsmArgs a) {
+    constexpr int WPB = 256 / kWarp;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
+        const int rc = 2 * i, rm = 2 * i + 1;
+        for (int s = a.rowptr[rc] + lane; s < a.rowptr[rm + 1]; s += kWarp) a.kvals[s] = 0.0;
+        __syncwarp();
+        const double c = a.u[rc], mu = a.u[rm], cold = a.uold[rc];
+        const double Vi = a.vol[i], Mi = a.mnode[i];
+        double rcs = 0.0, rms = 0.0, k12 = 0.0, k21 = 0.0;
+        for (int t = a.off[i] + lane; t < a.off[i + 1]; t += kWarp) {
+            const int j = __ldg(a.nbr + t);
+            const bool ghostJ = a.ghost && a.ghost[j];
+            const double g2 = a.lap[t];
+            double coeff_c = 0.0;
+            if (!ghostJ) {
+                const int r = a.rev[t];
+                double w;
+                if (r >= 0 && Vi > 0.0) w = 0.5 * (Mi * g2 + (a.vol[j] / Vi) * a.mnode[j] * a.lap[r]);
+                else w = Mi * g2;
+                coeff_c = -w;
+            }
+            const double coeff_mu = ghostJ ? 0.0 : a.kappa * g2;
+            rcs += coeff_c * (a.u[2 * j + 1] - mu);
+            rms += coeff_mu * (a.u[2 * j] - c);
+            k12 += coeff_c;
+            k21 += coeff_mu;
+            const int *sl = a.slot + (size_t)t * 4;
+            a.kvals[sl[0]] = -0.0;        // (c,  c_j)
+            a.kvals[sl[1]] = -coeff_c;    // (c,  mu_j)
+            a.kvals[sl[2]] = -coeff_mu;   // (mu, c_j)
+            a.kvals[sl[3]] = -0.0;        // (mu, mu_j)
+        }
+        rcs = group_sum<kWarp>(rcs);
+        rms = group_sum<kWarp>(rms);
+        k12 = group_sum<kWarp>(k12);
+        k21 = group_sum<kWarp>(k21);
+        if (lane == 0) {
+            const double cc = ch_clamp(c);
+            const double fp = log(cc / (1.0 - cc)) + a.chi * (1.0 - 2.0 * cc);
+            const double fpp = 1.0 / (cc * (1.0 - cc)) - 2.0 * a.chi;
+            const int *dg = a.diag + (size_t)i * 4;
+            a.kvals[dg[0]] = -(1.0 / a.dt);
+            a.kvals[dg[1]] = -0.0 + k12;
+            a.kvals[dg[2]] = fpp + k21;
+            a.kvals[dg[3]] = -1.0;
+            a.rhs[rc] = (c - cold) / a.dt + rcs;
+            a.rhs[rm] = mu - fp + rms;
+        }
+    }
+}
+
+cudaError_t launch_assemble_ch(const ChAsmArgs &a, cudaStream_t s) {
+    const int g = (a.n + 7) / 8;
+    assemble_ch_kernel<<<g > 0 ? g : 1, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace pxb

@@ -1,0 +1,348 @@
+// explicit_pddo_frac on the device (reference ExplicitPDDOFracElement::preprocessIteration,
+// src/ElmtSystem/ExplicitPDDOFracElement.cpp:239-299, and the central-difference loop of
+// src/TimeStepping/TimeStepping.cpp:479-547).
+//
+// One warp per source node; lanes walk the node's contiguous family (bond id, health byte and the SoA
+// Navier operator streams are read fully coalesced; neighbour positions/displacements are gathers that hit
+// L1/L2 because families are spatially local).  Per step, a single launch does
+//   damage   irreversible tensile (or |s|) critical-stretch failure of every live bond, decided in FP64;
+//   force    L_i = sum_j h_ij P_ij (u_j - u_i) with P from the cached Gxx,Gyy,(Gzz),Gxy,(Gxz,Gyz);
+//   update   a_i = (L_i + b)/rho, u^{n+1} = 2u^n - u^{n-1} + dt^2 a_i  (STEP), written into the u^{n-1}
+//            buffer (ping-pong: every thread reads u^n only, so no grid-wide sync is needed);
+//   BC pass  ghost/boundary targets whose final value derives from this node's freshly integrated value
+//            (reflection, Neumann copy) or from constants (direct pins) are written by this node's warp,
+//            reproducing the reference's sequential BC application (compiled on the host);
+//   guard    the per-step max |u^{n+1}| (NaN-propagating) for the reference blow-up test.
+#include "k_kernels.h"
+#include "pxb_common.cuh"
+
+namespace pxb {
+
+namespace {
+
+// reference stretch s = (|xi+eta| - |xi|)/|xi| with the reference's operation order (no contraction)
+__device__ __forceinline__ double ref_stretch(double y2, double r2) {
+    const double r = sqrt(r2);
+    return __ddiv_rn(__dsub_rn(sqrt(y2), r), r);
+}
+
+template <int DIM>
+__device__ __forceinline__ double dot_rn(const double *a, const double *b) {
+    double s = __dmul_rn(a[0], b[0]);
+    s = __dadd_rn(s, __dmul_rn(a[1], b[1]));
+    if constexpr (DIM == 3) s = __dadd_rn(s, __dmul_rn(a[2], b[2]));
+    return s;
+}
+
+template <int DIM, bool MIXED>
+__device__ __forceinline__ void load_G(const void *G, long long nb, long long t, double *g) {
+    constexpr int NC = (DIM == 3) ? 6 : 3;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        if constexpr (MIXED) g[c] = (double)__ldg(static_cast<const float *>(G) + (size_t)c * nb + t);
+        else g[c] = __ldg(static_cast<const double *>(G) + (size_t)c * nb + t);
+    }
+}
+
+// P * eta with the reference's coefficient formulas (ExplicitPDDOFracElement.cpp:276-295)
+template <int DIM>
+__device__ __forceinline__ void navier_apply(const double *g, double C11, double C12, double C66, const double *e,
+                                             double *out) {
+    if constexpr (DIM == 3) {
+        const double Gxx = g[0], Gyy = g[1], Gzz = g[2], Gxy = g[3], Gxz = g[4], Gyz = g[5];
+        const double p11 = C11 * Gxx + C66 * (Gyy + Gzz);
+        const double p22 = C11 * Gyy + C66 * (Gxx + Gzz);
+        const double p33 = C11 * Gzz + C66 * (Gxx + Gyy);
+        const double ac = C12 + C66;
+        const double p12 = ac * Gxy, p13 = ac * Gxz, p23 = ac * Gyz;
+        out[0] = p11 * e[0] + p12 * e[1] + p13 * e[2];
+        out[1] = p12 * e[0] + p22 * e[1] + p23 * e[2];
+        out[2] = p13 * e[0] + p23 * e[1] + p33 * e[2];
+    } else {
+        const double Gxx = g[0], Gyy = g[1], Gxy = g[2];
+        const double p11 = C11 * Gxx + C66 * Gyy;
+        const double p22 = C66 * Gxx + C11 * Gyy;
+        const double pxy = (C12 + C66) * Gxy;
+        out[0] = p11 * e[0] + pxy * e[1];
+        out[1] = pxy * e[0] + p22 * e[1];
+    }
+}
+
+template <int DIM>
+__device__ __forceinline__ double pick(const double *v, int d) {
+    double r = v[0];
+#pragma unroll
+    for (int k = 1; k < DIM; ++k)
+        if (d == k) r = v[k];
+    return r;
+}
+
+}  // namespace
+
+template <int DIM, bool MIXED, int MODE>
+__global__ void __launch_bounds__(kEpfThreads) epf_kernel(EpfArgs a) {
+    using PosT = typename Vec<DIM>::T;
+    constexpr int WPB = kEpfThreads / kWarp;
+    __shared__ unsigned long long s_umax[WPB];
+    __shared__ unsigned long long s_broken[WPB];
+
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const PosT *pos = static_cast<const PosT *>(a.pos);
+    double t_new = 0.0;
+    if constexpr (MODE == EPF_STEP) t_new = a.t_sched[a.step_in_chunk];
+
+    unsigned long long broken = 0;
+    double umax = 0.0;
+
+    for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
+        const int b0 = a.off[i], b1 = a.off[i + 1];
+        const PosT xi = pos[i];
+        double ui[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) ui[d] = a.u[(size_t)i * DIM + d];
+        double L[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) L[d] = 0.0;
+
+        for (int t = b0 + lane; t < b1; t += kWarp) {
+            if (a.health[t] == 0) continue;
+            const int j = __ldg(a.nbr + t);
+            const PosT xj = pos[j];
+            double e[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) e[d] = __dsub_rn(a.u[(size_t)j * DIM + d], ui[d]);
+            if constexpr (MODE != EPF_FORCE_FROZEN) {
+                if (a.damage) {
+                    double xv[DIM], yv[DIM];
+                    xv[0] = __dsub_rn(xj.x, xi.x);
+                    xv[1] = __dsub_rn(xj.y, xi.y);
+                    if constexpr (DIM == 3) xv[2] = __dsub_rn(xj.z, xi.z);
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
+                    const double r2 = dot_rn<DIM>(xv, xv);
+                    if (r2 > 0.0) {
+                        const double y2 = dot_rn<DIM>(yv, yv);
+                        // fast squared test; the reference's own arithmetic decides bonds near the threshold
+                        const double band = 1.0e-6 * r2;
+                        const double qh = y2 - a.sc_hi2 * r2;
+                        bool brk;
+                        if (a.tension_only) {
+                            if (qh > band) brk = true;
+                            else if (qh < -band) brk = false;
+                            else brk = ref_stretch(y2, r2) > a.sc;
+                        } else {
+                            const double ql = a.sc_lo2 * r2 - y2;
+                            if (qh > band || ql > band) brk = true;
+                            else if (qh < -band && ql < -band) brk = false;
+                            else brk = fabs(ref_stretch(y2, r2)) > a.sc;
+                        }
+                        if (brk) {
+                            a.health[t] = 0;
+                            ++broken;
+                            continue;
+                        }
+                    }
+                }
+            }
+            double g[(DIM == 3) ? 6 : 3];
+            load_G<DIM, MIXED>(a.G, a.nb, t, g);
+            double f[DIM];
+            navier_apply<DIM>(g, a.C11, a.C12, a.C66, e, f);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) L[d] += f[d];
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) L[d] = group_sum<kWarp>(L[d]);
+
+        // node update: lane d owns component d
+        double unew = 0.0;
+        if (lane < DIM) {
+            const int d = lane;
+            const double acc = __ddiv_rn(__dadd_rn(pick<DIM>(L, d), a.b[d]), a.rho);
+            const size_t k = (size_t)i * DIM + d;
+            if constexpr (MODE == EPF_RATE || MODE == EPF_FORCE_FROZEN) {
+                a.accel[k] = acc;
+            } else if constexpr (MODE == EPF_START) {
+                const double v = a.v0 ? a.v0[k] : 0.0;
+                a.u_other[k] = __dadd_rn(__dsub_rn(ui[d], __dmul_rn(a.dt, v)), __dmul_rn(a.dt2, acc));
+            } else {
+                const double uprev = a.u_other[k];
+                unew = __dadd_rn(__dsub_rn(__dmul_rn(2.0, pick<DIM>(ui, d)), uprev), __dmul_rn(a.dt2, acc));
+                const bool owned = a.bc_own && ((a.bc_own[i] >> d) & 1);
+                if (!owned) {
+                    a.u_other[k] = unew;
+                    umax = fmax(umax, fabs(unew));
+                }
+            }
+        }
+        if constexpr (MODE == EPF_STEP) {
+            if (a.bc_off) {
+                const int e0 = a.bc_off[i], e1 = a.bc_off[i + 1];
+                if (e0 < e1) {
+                    double un[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) un[d] = __shfl_sync(kFull, unew, d);
+                    for (int e = e0 + lane; e < e1; e += kWarp) {
+                        const int comp = a.bc_comp[e];
+                        const int form = a.bc_form[e];
+                        // g = value + velocity*t in the reference's order (DirichletBC.cpp:135-137)
+                        const double g1 = __dadd_rn(a.bc_val[e], __dmul_rn(a.bc_vel[e], t_new));
+                        double v;
+                        if (form == 0) {
+                            v = pick<DIM>(un, comp);
+                        } else if (form == 1) {
+                            v = g1;
+                        } else if (form == 2) {
+                            v = __dsub_rn(__dmul_rn(2.0, g1), pick<DIM>(un, comp));
+                        } else {
+                            const double g2 = __dadd_rn(a.bc_val2[e], __dmul_rn(a.bc_vel2[e], t_new));
+                            v = __dsub_rn(__dmul_rn(2.0, g1), g2);
+                        }
+                        a.u_other[(size_t)a.bc_tgt[e] * DIM + comp] = v;
+                        umax = fmax(umax, fabs(v));
+                    }
+                }
+            }
+        }
+    }
+
+    // block reductions, one atomic per block
+    if constexpr (MODE == EPF_STEP) {
+        umax = group_max<kWarp>(umax);
+        if (lane == 0) s_umax[wib] = dbl_key(umax);
+    }
+    unsigned long long bsum = broken;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bsum += __shfl_xor_sync(kFull, bsum, o);
+    if (lane == 0) s_broken[wib] = bsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long bb = 0, mm = 0;
+        for (int w = 0; w < WPB; ++w) {
+            bb += s_broken[w];
+            if constexpr (MODE == EPF_STEP) mm = s_umax[w] > mm ? s_umax[w] : mm;
+        }
+        if (bb && a.n_broken) atomicAdd(a.n_broken, bb);
+        if constexpr (MODE == EPF_STEP) {
+            if (a.umax) atomicMax(a.umax + a.step_in_chunk, mm);
+        }
+    }
+}
+
+// ---- bond-force adjoint with a frozen damage mask ---------------------------------------------------------
+// Forward: a_i = (L_i + b)/rho, L_i = sum_t h_t P_t (u_j - u_i) with P_t symmetric.  For abar = dJ/da,
+// Lbar = abar/rho and
+//   ubar_m = sum_{t in fam(m)} ( h_rev(t) P_rev(t) Lbar_{j_t} - h_t P_t Lbar_m )      (gather via rev)
+//   dJ/dC_k = sum_i sum_t h_t Lbar_i . (dP_t/dC_k) eta_t
+template <int DIM, bool MIXED>
+__global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) {
+    constexpr int WPB = kEpfThreads / kWarp;
+    constexpr int NC = (DIM == 3) ? 6 : 3;
+    __shared__ double s_dC[WPB][3];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    double dC[3] = {0.0, 0.0, 0.0};
+    for (int m = blockIdx.x * WPB + wib; m < a.n; m += gridDim.x * WPB) {
+        double Lm[DIM], um[DIM], U[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            Lm[d] = a.abar[(size_t)m * DIM + d] * a.inv_rho;
+            um[d] = a.u[(size_t)m * DIM + d];
+            U[d] = 0.0;
+        }
+        for (int t = a.off[m] + lane; t < a.off[m + 1]; t += kWarp) {
+            const int j = __ldg(a.nbr + t);
+            const int r = __ldg(a.rev + t);
+            double g[NC], f[DIM];
+            if (r >= 0 && a.health[r]) {
+                double Lj[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) Lj[d] = a.abar[(size_t)j * DIM + d] * a.inv_rho;
+                load_G<DIM, MIXED>(a.G, a.nb, r, g);
+                navier_apply<DIM>(g, a.C11, a.C12, a.C66, Lj, f);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) U[d] += f[d];
+            }
+            if (a.health[t]) {
+                load_G<DIM, MIXED>(a.G, a.nb, t, g);
+                navier_apply<DIM>(g, a.C11, a.C12, a.C66, Lm, f);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) U[d] -= f[d];
+                double e[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) e[d] = a.u[(size_t)j * DIM + d] - um[d];
+                if constexpr (DIM == 3) {
+                    const double Gxx = g[0], Gyy = g[1], Gzz = g[2], Gxy = g[3], Gxz = g[4], Gyz = g[5];
+                    dC[0] += Lm[0] * Gxx * e[0] + Lm[1] * Gyy * e[1] + Lm[2] * Gzz * e[2];
+                    dC[1] += Lm[0] * (Gxy * e[1] + Gxz * e[2]) + Lm[1] * (Gxy * e[0] + Gyz * e[2]) +
+                             Lm[2] * (Gxz * e[0] + Gyz * e[1]);
+                    dC[2] += Lm[0] * ((Gyy + Gzz) * e[0] + Gxy * e[1] + Gxz * e[2]) +
+                             Lm[1] * (Gxy * e[0] + (Gxx + Gzz) * e[1] + Gyz * e[2]) +
+                             Lm[2] * (Gxz * e[0] + Gyz * e[1] + (Gxx + Gyy) * e[2]);
+                } else {
+                    const double Gxx = g[0], Gyy = g[1], Gxy = g[2];
+                    dC[0] += Lm[0] * Gxx * e[0] + Lm[1] * Gyy * e[1];
+                    dC[1] += Lm[0] * Gxy * e[1] + Lm[1] * Gxy * e[0];
+                    dC[2] += Lm[0] * (Gyy * e[0] + Gxy * e[1]) + Lm[1] * (Gxy * e[0] + Gxx * e[1]);
+                }
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) U[d] = group_sum<kWarp>(U[d]);
+        if (lane < DIM) a.ubar[(size_t)m * DIM + lane] = pick<DIM>(U, lane);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) dC[k] = group_sum<kWarp>(dC[k]);
+    if (lane == 0) { s_dC[wib][0] = dC[0]; s_dC[wib][1] = dC[1]; s_dC[wib][2] = dC[2]; }
+    __syncthreads();
+    if (threadIdx.x < 3 && a.dC) {
+        double v = 0.0;
+        for (int w = 0; w < WPB; ++w) v += s_dC[w][threadIdx.x];
+        atomicAdd(a.dC + threadIdx.x, v);
+    }
+}
+
+cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int grid, cudaStream_t s) {
+    if (dim == 2) {
+        if (mixed) epf_adjoint_kernel<2, true><<<grid, kEpfThreads, 0, s>>>(a);
+        else epf_adjoint_kernel<2, false><<<grid, kEpfThreads, 0, s>>>(a);
+    } else {
+        if (mixed) epf_adjoint_kernel<3, true><<<grid, kEpfThreads, 0, s>>>(a);
+        else epf_adjoint_kernel<3, false><<<grid, kEpfThreads, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template <int DIM, bool MIXED>
+static cudaError_t launch_dm(const EpfArgs &a, int mode, int grid, cudaStream_t s) {
+    switch (mode) {
+        case EPF_RATE: epf_kernel<DIM, MIXED, EPF_RATE><<<grid, kEpfThreads, 0, s>>>(a); break;
+        case EPF_START: epf_kernel<DIM, MIXED, EPF_START><<<grid, kEpfThreads, 0, s>>>(a); break;
+        case EPF_STEP: epf_kernel<DIM, MIXED, EPF_STEP><<<grid, kEpfThreads, 0, s>>>(a); break;
+        case EPF_FORCE_FROZEN: epf_kernel<DIM, MIXED, EPF_FORCE_FROZEN><<<grid, kEpfThreads, 0, s>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int grid, cudaStream_t s) {
+    if (dim == 2) return mixed ? launch_dm<2, true>(a, mode, grid, s) : launch_dm<2, false>(a, mode, grid, s);
+    return mixed ? launch_dm<3, true>(a, mode, grid, s) : launch_dm<3, false>(a, mode, grid, s);
+}
+
+int epf_grid(int n) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const int wpb = kEpfThreads / kWarp;
+    const long long need = ((long long)n + wpb - 1) / wpb;
+    const long long cap = (long long)sms * 8;
+    return (int)(need < cap ? need : cap) > 0 ? (int)(need < cap ? need : cap) : 1;
+}
+
+}  // namespace pxb

@@ -1,0 +1,289 @@
+// g-function build: per node i, the PDDO moment matrix over the horizon family, a small dense solve, and the
+// per-bond operator values (reference PDOperators::calcAMatrixCompute / calcOperatorsCompute,
+// src/PDOperators/CalcPDOperators.cpp:108-226 and 307-354).
+//
+// Schedule: one warp per node (families are contiguous in the CSR, so lanes read consecutive bonds).
+//   pass 1  lanes accumulate the upper triangle of A = sum_j bw * m m^T over a lane-strided slice of the
+//           family; a butterfly reduction leaves the full A in every lane.
+//   solve   every lane factors A = L D L^T redundantly in registers (nop <= 9 at order 2, so this is ~120
+//           FMAs) and solves for column k = lane of X = A^-1 diag(q!), followed by one step of iterative
+//           refinement against A kept in shared memory and the reference's max-norm consistency test
+//           (src/MathUtils/MatrixXd.cpp:40-47).
+//   pass 2  X goes to shared memory; lanes evaluate op_k(i,j) = (sum_a X[a][k] eta^{q_a}) * bw / delta^|q_k|
+//           for their bonds and write the full op vector (AoS, [bond][nop]) and/or the Navier subset
+//           (SoA, [c][bond]) used by the explicit fracture step.
+// MIXED: bond weights, monomials and moment products in FP32 with two-sum compensated accumulation on
+// delta-scaled bond vectors (the bond vector itself is formed in FP64); the factorisation, refinement and
+// g-evaluation stay in FP64; g is stored in FP32.
+#include <cfloat>
+
+#include "k_kernels.h"
+#include "pxb_common.cuh"
+
+namespace pxb {
+
+template <int DIM, int ORDER, bool MIXED>
+__global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
+    constexpr QTable<DIM, ORDER> Q{};
+    constexpr int NOP = Q.NOP;
+    constexpr int NE = NOP * (NOP + 1) / 2;
+    constexpr int WPB = kGbuildThreads / kWarp;
+    using PosT = typename Vec<DIM>::T;
+
+    __shared__ double sA[WPB][NOP * NOP];
+    __shared__ double sX[WPB][NOP * NOP];
+
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const PosT *pos = static_cast<const PosT *>(a.pos);
+    const double inv_delta = 1.0 / a.delta;
+
+    double idpow[NOP];
+#pragma unroll
+    for (int k = 0; k < NOP; ++k) {
+        double v = 1.0;
+#pragma unroll
+        for (int t = 0; t < Q.p[k] + Q.q[k] + Q.r[k]; ++t) v *= inv_delta;
+        idpow[k] = v;
+    }
+
+    for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
+        const int b0 = a.off[i], b1 = a.off[i + 1];
+        const PosT xi = pos[i];
+
+        // ---- pass 1: moment sums ----
+        double acc[NE];
+        CompF cacc[MIXED ? NE : 1];
+#pragma unroll
+        for (int e = 0; e < NE; ++e) acc[e] = 0.0;
+        int usable = 0;
+        for (int t = b0 + lane; t < b1; t += kWarp) {
+            const int j = a.nbr[t];
+            const PosT xj = pos[j];
+            const double dx = xj.x - xi.x, dy = xj.y - xi.y;
+            double dz = 0.0;
+            if constexpr (DIM == 3) dz = xj.z - xi.z;
+            const double xn = sqrt(dx * dx + dy * dy + dz * dz);
+            if (xn <= 0.0) continue;
+            if constexpr (MIXED) {
+                const float r = 2.0f * (float)(xn * inv_delta);
+                const float w = expf(-r * r);
+                float vc = 1.0f;
+                if (a.dx_char > 0.0 && xn > a.delta - 0.5 * a.dx_char)
+                    vc = fminf(fmaxf((float)((a.delta - xn + 0.5 * a.dx_char) / a.dx_char), 0.f), 1.f);
+                const float bw = w * vc * (float)a.vol[j];
+                if (!(bw > 0.f)) continue;
+                ++usable;
+                float m[NOP];
+                monomials<DIM, ORDER, float>((float)(dx * inv_delta), (float)(dy * inv_delta),
+                                             (float)(dz * inv_delta), m);
+                int e = 0;
+#pragma unroll
+                for (int p = 0; p < NOP; ++p)
+#pragma unroll
+                    for (int q = p; q < NOP; ++q) cacc[e++].add(bw * m[p] * m[q]);
+            } else {
+                const double bw = bond_weight(xn, a.delta) * rim_correction(xn, a.delta, a.dx_char) * a.vol[j];
+                if (!(bw > 0.0)) continue;
+                ++usable;
+                double m[NOP];
+                monomials<DIM, ORDER, double>(dx * inv_delta, dy * inv_delta, dz * inv_delta, m);
+                int e = 0;
+#pragma unroll
+                for (int p = 0; p < NOP; ++p)
+#pragma unroll
+                    for (int q = p; q < NOP; ++q) acc[e++] += bw * m[p] * m[q];
+            }
+        }
+        if constexpr (MIXED) {
+#pragma unroll
+            for (int e = 0; e < NE; ++e) acc[e] = cacc[e].value();
+        }
+#pragma unroll
+        for (int e = 0; e < NE; ++e) acc[e] = group_sum<kWarp>(acc[e]);
+        usable = group_sum_int<kWarp>(usable);
+
+        // keep A (full, row-major) in shared memory for the refinement residual and the consistency test
+        if (lane == 0) {
+            int e = 0;
+#pragma unroll
+            for (int p = 0; p < NOP; ++p)
+#pragma unroll
+                for (int q = p; q < NOP; ++q) {
+                    sA[wib][p * NOP + q] = acc[e];
+                    sA[wib][q * NOP + p] = acc[e];
+                    ++e;
+                }
+        }
+        __syncwarp();
+
+        // ---- solve: in-place L D L^T of the packed upper triangle (acc[e] holds row p, col q>=p) ----
+        // index of (p,q), q>=p, in the packed upper triangle
+        auto U = [&](int p, int q) -> int { return p * NOP - p * (p - 1) / 2 + (q - p); };
+#pragma unroll
+        for (int j = 0; j < NOP; ++j) {
+            double d = acc[U(j, j)];
+#pragma unroll
+            for (int k = 0; k < j; ++k) d -= acc[U(k, j)] * acc[U(k, j)] * acc[U(k, k)];
+            acc[U(j, j)] = d;
+            const double invd = 1.0 / d;
+#pragma unroll
+            for (int i2 = j + 1; i2 < NOP; ++i2) {
+                double s = acc[U(j, i2)];
+#pragma unroll
+                for (int k = 0; k < j; ++k) s -= acc[U(k, i2)] * acc[U(k, j)] * acc[U(k, k)];
+                acc[U(j, i2)] = s * invd;  // L[i2][j] stored at packed (j, i2)
+            }
+        }
+        const int kcol = (lane < NOP) ? lane : 0;
+        double fk = 0.0;
+#pragma unroll
+        for (int q = 0; q < NOP; ++q)
+            if (q == kcol) fk = Q.fact[q];
+        auto ldl_solve = [&](double *x) {
+            // x holds the rhs on entry
+#pragma unroll
+            for (int i2 = 0; i2 < NOP; ++i2) {
+#pragma unroll
+                for (int j = 0; j < i2; ++j) x[i2] -= acc[U(j, i2)] * x[j];
+            }
+#pragma unroll
+            for (int i2 = 0; i2 < NOP; ++i2) x[i2] /= acc[U(i2, i2)];
+#pragma unroll
+            for (int i2 = NOP - 1; i2 >= 0; --i2) {
+#pragma unroll
+                for (int j = i2 + 1; j < NOP; ++j) x[i2] -= acc[U(i2, j)] * x[j];
+            }
+        };
+        double x[NOP];
+#pragma unroll
+        for (int q = 0; q < NOP; ++q) x[q] = (q == kcol) ? fk : 0.0;
+        ldl_solve(x);
+        // one step of iterative refinement: x += A^-1 (b - A x)
+        double r[NOP];
+#pragma unroll
+        for (int p = 0; p < NOP; ++p) {
+            double s = (p == kcol) ? fk : 0.0;
+#pragma unroll
+            for (int q = 0; q < NOP; ++q) s -= sA[wib][p * NOP + q] * x[q];
+            r[p] = s;
+        }
+        ldl_solve(r);
+#pragma unroll
+        for (int q = 0; q < NOP; ++q) x[q] += r[q];
+        // consistency test (MatrixXd.cpp:40-47): max|A X - B| <= 1e-8 * max(max|B|, max|A| max|X|)
+        double res = 0.0, maxA = 0.0, maxX = 0.0;
+#pragma unroll
+        for (int p = 0; p < NOP; ++p) {
+            double s = -((p == kcol) ? fk : 0.0);
+#pragma unroll
+            for (int q = 0; q < NOP; ++q) {
+                s += sA[wib][p * NOP + q] * x[q];
+                maxA = fmax(maxA, fabs(sA[wib][p * NOP + q]));
+            }
+            res = fmax(res, fabs(s));
+            maxX = fmax(maxX, fabs(x[p]));
+        }
+        if (lane >= NOP) { res = 0.0; maxX = 0.0; }
+        res = group_max<kWarp>(res);
+        maxX = group_max<kWarp>(maxX);
+        double maxB = 0.0;
+#pragma unroll
+        for (int q = 0; q < NOP; ++q) maxB = fmax(maxB, Q.fact[q]);
+        const double scale = fmax(fmax(maxB, maxA * maxX), DBL_MIN);
+        const bool consistent = (res <= 1.0e-8 * scale);  // NaN-safe: NaN fails
+        const bool degenerate = (usable < NOP) || !consistent;
+        const bool deep_ghost = (a.layer != nullptr) && (a.layer[i] > 1);
+        const bool zero_ops = degenerate;
+        if (lane == 0) {
+            if (a.degenerate) a.degenerate[i] = degenerate ? 1 : 0;
+            if (degenerate && !deep_ghost) {
+                atomicAdd(a.n_degenerate, 1u);
+                atomicMin(a.first_degenerate, i);
+            }
+        }
+        // X (column kcol in lane kcol) to shared memory: sX[a][k]
+        if (lane < NOP) {
+#pragma unroll
+            for (int p = 0; p < NOP; ++p) sX[wib][p * NOP + lane] = zero_ops ? 0.0 : x[p];
+        }
+        __syncwarp();
+
+        // ---- pass 2: per-bond operators ----
+        for (int t = b0 + lane; t < b1; t += kWarp) {
+            const int j = a.nbr[t];
+            const PosT xj = pos[j];
+            const double dx = xj.x - xi.x, dy = xj.y - xi.y;
+            double dz = 0.0;
+            if constexpr (DIM == 3) dz = xj.z - xi.z;
+            const double xn = sqrt(dx * dx + dy * dy + dz * dz);
+            double bw = 0.0;
+            if (xn > 0.0) bw = bond_weight(xn, a.delta) * rim_correction(xn, a.delta, a.dx_char) * a.vol[j];
+            const bool live = (xn > 0.0) && (bw > 0.0);
+            double m[NOP];
+            monomials<DIM, ORDER, double>(dx * inv_delta, dy * inv_delta, dz * inv_delta, m);
+            auto op = [&](int k) -> double {
+                if (!live) return 0.0;
+                double s = 0.0;
+#pragma unroll
+                for (int p = 0; p < NOP; ++p) s += sX[wib][p * NOP + k] * m[p];
+                return s * bw * idpow[k];
+            };
+            if (a.ops) {
+                if constexpr (MIXED) {
+                    float *o = static_cast<float *>(a.ops) + (size_t)t * NOP;
+#pragma unroll
+                    for (int k = 0; k < NOP; ++k) o[k] = (float)op(k);
+                } else {
+                    double *o = static_cast<double *>(a.ops) + (size_t)t * NOP;
+#pragma unroll
+                    for (int k = 0; k < NOP; ++k) o[k] = op(k);
+                }
+            }
+            if (a.G) {
+                constexpr int NC = (DIM == 3) ? 6 : 3;
+                int sl[NC];
+                if constexpr (DIM == 3) {
+                    sl[0] = Q.slot(2, 0, 0); sl[1] = Q.slot(0, 2, 0); sl[2] = Q.slot(0, 0, 2);
+                    sl[3] = Q.slot(1, 1, 0); sl[4] = Q.slot(1, 0, 1); sl[5] = Q.slot(0, 1, 1);
+                } else {
+                    sl[0] = Q.slot(2, 0, 0); sl[1] = Q.slot(0, 2, 0); sl[2] = Q.slot(1, 1, 0);
+                }
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    const double v = op(sl[c]);
+                    if constexpr (MIXED) static_cast<float *>(a.G)[(size_t)c * a.nb + t] = (float)v;
+                    else static_cast<double *>(a.G)[(size_t)c * a.nb + t] = v;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <int DIM, int ORDER>
+static cudaError_t launch_order(const GBuildArgs &a, bool mixed, int grid, cudaStream_t s) {
+    if (mixed) gbuild_kernel<DIM, ORDER, true><<<grid, kGbuildThreads, 0, s>>>(a);
+    else gbuild_kernel<DIM, ORDER, false><<<grid, kGbuildThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, int grid, cudaStream_t s) {
+    if (dim == 2) {
+        switch (order) {
+            case 1: return launch_order<2, 1>(a, mixed, grid, s);
+            case 2: return launch_order<2, 2>(a, mixed, grid, s);
+            case 3: return launch_order<2, 3>(a, mixed, grid, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (order) {
+        case 1: return launch_order<3, 1>(a, mixed, grid, s);
+        case 2: return launch_order<3, 2>(a, mixed, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+bool gbuild_supported(int dim, int order) { return (dim == 2 && order >= 1 && order <= 3) || (dim == 3 && order >= 1 && order <= 2); }
+
+}  // namespace pxb

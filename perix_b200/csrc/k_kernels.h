@@ -1,0 +1,153 @@
+// Kernel argument blocks and launchers shared between the .cu kernels and the C++ host code.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pxb {
+
+constexpr int kGbuildThreads = 128;
+constexpr int kEpfThreads = 256;
+constexpr int kApplyThreads = 256;
+
+// ---------------------------------------------------------------------------------------------------- g-build
+struct GBuildArgs {
+    int n = 0;
+    long long nb = 0;
+    const int *off = nullptr;
+    const int *nbr = nullptr;
+    const void *pos = nullptr;  // double2 / double4
+    const double *vol = nullptr;
+    const int *layer = nullptr;
+    double delta = 0.0, dx_char = 0.0;
+    void *ops = nullptr;  // AoS [nb][nop] (double, or float when mixed); may be null
+    void *G = nullptr;    // SoA Navier [c][nb] (double, or float when mixed); may be null
+    uint8_t *degenerate = nullptr;
+    unsigned int *n_degenerate = nullptr;
+    int *first_degenerate = nullptr;
+};
+cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, int grid, cudaStream_t s);
+bool gbuild_supported(int dim, int order);
+
+// ---------------------------------------------------------------------------------------- explicit fracture
+enum EpfMode { EPF_RATE = 0, EPF_START = 1, EPF_STEP = 2, EPF_FORCE_FROZEN = 3 };
+
+struct EpfArgs {
+    int n = 0;
+    long long nb = 0;
+    const int *off = nullptr;
+    const int *nbr = nullptr;
+    const void *pos = nullptr;
+    const void *G = nullptr;  // SoA [c][nb]
+    uint8_t *health = nullptr;
+    double C11 = 0, C12 = 0, C66 = 0, rho = 1, b[3] = {0, 0, 0};
+    double sc = 0;                  // critical stretch
+    double sc_hi2 = 0, sc_lo2 = 0;  // (1+sc)^2 and (1-sc)^2 (0 when 1-sc <= 0)
+    int damage = 0, tension_only = 1;
+    const double *u = nullptr;    // u^n (N*dim)
+    double *u_other = nullptr;    // STEP: u^{n-1} in, u^{n+1} out; START: u^{-1} out
+    const double *v0 = nullptr;   // START
+    double *accel = nullptr;      // RATE / FORCE_FROZEN
+    double dt = 0, dt2 = 0;  // START: dt2 = 0.5*dt*dt; STEP: dt2 = dt*dt
+    // time of the new state for the BC pass: t_sched[step_in_chunk]
+    const double *t_sched = nullptr;
+    int step_in_chunk = 0;
+    // BC program (STEP only)
+    // entry e (executed by the warp of its source node): target node, component, form
+    //   0: U(src)   1: G   2: 2G - U(src)   3: 2G - G2,   G = val + vel*t, G2 = val2 + vel2*t
+    const uint8_t *bc_own = nullptr;
+    const int *bc_off = nullptr;
+    const int *bc_tgt = nullptr;
+    const int *bc_comp = nullptr;
+    const int *bc_form = nullptr;
+    const double *bc_val = nullptr, *bc_vel = nullptr, *bc_val2 = nullptr, *bc_vel2 = nullptr;
+    unsigned long long *umax = nullptr;     // per-step max|u| keys
+    unsigned long long *n_broken = nullptr; // broken-bond counter
+};
+cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int grid, cudaStream_t s);
+int epf_grid(int n);
+
+struct EpfAdjArgs {
+    int n = 0;
+    long long nb = 0;
+    const int *off = nullptr;
+    const int *nbr = nullptr;
+    const int *rev = nullptr;
+    const void *G = nullptr;
+    const uint8_t *health = nullptr;
+    double C11 = 0, C12 = 0, C66 = 0, inv_rho = 1;
+    const double *u = nullptr;
+    const double *abar = nullptr;
+    double *ubar = nullptr;
+    double *dC = nullptr;  // 3 doubles, atomically accumulated (must be zeroed)
+};
+cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int grid, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- apply
+struct ApplyArgs {
+    int n = 0;
+    int nop = 0;
+    int nk = 0;
+    int slots[32];
+    const int *off = nullptr;
+    const int *nbr = nullptr;
+    const int *rev = nullptr;
+    const void *ops = nullptr;  // AoS [nb][nop]
+    const double *u = nullptr;  // forward: u (N); adjoint: ybar (N*nk)
+    double *out = nullptr;      // forward: N*nk; adjoint: N
+};
+cudaError_t launch_apply(const ApplyArgs &a, bool mixed, int grid, cudaStream_t s);
+cudaError_t launch_apply_adjoint(const ApplyArgs &a, bool mixed, int grid, cudaStream_t s);
+
+// ------------------------------------------------------------------------------------------------------- misc
+cudaError_t launch_build_rev(int n, const int *off, const int *nbr, int *rev, int grid, cudaStream_t s);
+cudaError_t launch_pos_pack(int n, int dim, const double *coords3, void *pos, cudaStream_t s);
+cudaError_t launch_ids_to0(long long nb, const int *ids1, int *ids0, cudaStream_t s);
+cudaError_t launch_health_from_double(long long nb, const double *h, uint8_t *out, cudaStream_t s);
+cudaError_t launch_health_to_double(long long nb, const uint8_t *h, double *out, cudaStream_t s);
+cudaError_t launch_count_zero(long long nb, const uint8_t *h, unsigned long long *count, cudaStream_t s);
+cudaError_t launch_l2_flush(void *buf, size_t bytes, cudaStream_t s);
+
+// ------------------------------------------------------------------------------------------------ CSR assembly
+struct CsrMapArgs {
+    int n = 0, ndof = 1;
+    const int *off = nullptr;
+    const int *nbr = nullptr;
+    const int *rowptr = nullptr;
+    const int *cols = nullptr;
+    int *slot = nullptr;   // [nb*ndof*ndof]
+    int *diag = nullptr;   // [n*ndof*ndof]
+    int *missing = nullptr;
+};
+cudaError_t launch_csr_map(const CsrMapArgs &a, cudaStream_t s);
+
+struct ScalarAsmArgs {
+    int n = 0, dim = 2, nop = 0, type = 0, mixed = 0;
+    int s_xx = -1, s_yy = -1, s_zz = -1;
+    double coef = 0, f = 0, dt = 0;
+    const double *f_node = nullptr;
+    const int *off = nullptr;
+    const int *nbr = nullptr;
+    const int *rowptr = nullptr;
+    const int *slot = nullptr;
+    const int *diag = nullptr;
+    const void *ops = nullptr;
+    const uint8_t *degenerate = nullptr;
+    const double *u = nullptr, *uold = nullptr;
+    double *kvals = nullptr, *rhs = nullptr;
+};
+cudaError_t launch_assemble_scalar(const ScalarAsmArgs &a, cudaStream_t s);
+
+struct ChAsmArgs {
+    int n = 0;
+    double kappa = 0, chi = 0, dt = 1;
+    const int *off = nullptr, *nbr = nullptr, *rev = nullptr;
+    const double *lap = nullptr, *vol = nullptr, *mnode = nullptr;
+    const char *ghost = nullptr;
+    const int *rowptr = nullptr, *slot = nullptr, *diag = nullptr;
+    const double *u = nullptr, *uold = nullptr;
+    double *kvals = nullptr, *rhs = nullptr;
+};
+cudaError_t launch_assemble_ch(const ChAsmArgs &a, cudaStream_t s);
+
+}  // namespace pxb

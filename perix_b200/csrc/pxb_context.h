@@ -1,0 +1,170 @@
+// Host-side (C++20) state of a perix_b200 context: device-resident geometry, operator caches, explicit-loop
+// state, CSR maps and captured graphs.  One context = one device, one stream, no globals.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/perix_b200.h"
+
+namespace pxb {
+
+// ---- error plumbing ----------------------------------------------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int status, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define PXB_CUDA_TRY(expr)                                           \
+    do {                                                             \
+        cudaError_t _e = (expr);                                     \
+        if (_e != cudaSuccess) return ::pxb::cuda_fail(_e, #expr);   \
+    } while (0)
+
+#define PXB_TRY(expr)                   \
+    do {                                \
+        int _s = (expr);                \
+        if (_s != PXB_OK) return _s;    \
+    } while (0)
+
+// ---- device buffer ---------------------------------------------------------------------------------------------
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf &operator=(DevBuf &&o) noexcept {
+        if (this != &o) { release(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void release();
+    template <typename T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+// Pinned host staging buffer (grown on demand).
+struct PinnedBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf &) = delete;
+    PinnedBuf &operator=(const PinnedBuf &) = delete;
+    PinnedBuf(PinnedBuf &&o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    PinnedBuf &operator=(PinnedBuf &&o) noexcept;
+    ~PinnedBuf();
+};
+
+struct Geometry {
+    bool ready = false;
+    int n = 0, dim = 2;
+    long long nb = 0;
+    double delta = 0.0, dx_char = 0.0;
+    DevBuf off;     // int32 [n+1]
+    DevBuf nbr;     // int32 [nb], 0-based
+    DevBuf pos;     // double2 [n] (2D) or double4 [n] (3D)
+    DevBuf vol;     // double [n]
+    DevBuf mirror;  // int32 [n], 1-based mirror bulk, 0 none (may be empty)
+    DevBuf layer;   // int32 [n] ghost layer index (may be empty)
+    DevBuf rev;     // int32 [nb] reverse bond index (built lazily)
+    int max_family = 0;
+    std::vector<int> h_off, h_mirror;
+};
+
+struct OpsCache {
+    bool ready = false;
+    int order = 0, nop = 0, precision = PXB_FP64;
+    DevBuf ops;         // AoS [nb][nop], double or float
+    DevBuf degenerate;  // uint8 [n]
+    std::vector<int> pqr;
+};
+
+struct BcDevice {
+    int n_entries = 0;
+    DevBuf own;      // uint8 [n]: bitmask of components whose final value comes from the BC pass
+    DevBuf src_off;  // int32 [n+1]: BC target entries grouped by the node whose warp executes them
+    DevBuf tgt;      // int32 [n_entries]: target node (0-based)
+    DevBuf comp;     // int32 [n_entries]: component
+    DevBuf form;     // int32 [n_entries]: closed form (see EpfArgs)
+    DevBuf vals;     // double [4*n_entries]: val | vel | val2 | vel2 blocks
+};
+
+struct GraphKey {
+    int steps, parity, prec;
+    bool operator<(const GraphKey &o) const {
+        if (steps != o.steps) return steps < o.steps;
+        if (parity != o.parity) return parity < o.parity;
+        return prec < o.prec;
+    }
+};
+
+struct EpfState {
+    bool ready = false, started = false;
+    int precision = PXB_FP64;
+    double C11 = 0, C12 = 0, C66 = 0, rho = 1, b[3] = {0, 0, 0}, sc = 0;
+    int tension_only = 1;
+    DevBuf G;          // SoA Navier operators [c][nb], double or float (c = 3 in 2D, 6 in 3D)
+    DevBuf health;     // uint8 [nb]
+    DevBuf u[2];       // double [n*dim] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
+    DevBuf accel;      // double [n*dim]
+    DevBuf counters;   // unsigned long long [4]: broken-bond counter, ...
+    DevBuf umax;       // unsigned long long [chunk] per-step max |u| keys
+    DevBuf tsched;     // double [chunk] t_{n+1} of each step in the chunk
+    PinnedBuf tsched_h;
+    int cur = 0;
+    double t = 0.0, dt = 0.0;
+    long long step = 0;
+    std::vector<double> umax_hist;  // host history for the windowed blow-up guard
+    BcDevice bc;
+    bool has_bc = false;
+    std::map<GraphKey, cudaGraphExec_t> graphs;
+    int graph_chunk = 0;
+};
+
+struct CsrState {
+    bool ready = false;
+    int ndof = 1;
+    long long nnz = 0;
+    DevBuf rowptr, cols;
+    DevBuf slot;       // int32 [nb*ndof*ndof]: CSR slot of (row i*ndof+a, col j*ndof+b) for bond t
+    DevBuf diag;       // int32 [n*ndof*ndof]: slot of the diagonal block entries
+    DevBuf kvals, rhs, u, uold, fnode, mnode;
+};
+
+struct ChState {
+    bool ready = false;
+    DevBuf rev, lap, ghost;
+};
+
+}  // namespace pxb
+
+struct pxb_ctx {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    long long launches = 0;
+    pxb::Geometry g;
+    pxb::OpsCache ops;
+    pxb::EpfState epf;
+    pxb::CsrState csr;
+    pxb::ChState ch;
+    pxb::DevBuf scratch;
+    pxb::PinnedBuf pinned;
+};
+
+namespace pxb {
+// device allocation helpers (track bytes per context)
+int dev_alloc(pxb_ctx *c, DevBuf &b, size_t bytes);
+int dev_upload(pxb_ctx *c, DevBuf &b, const void *host, size_t bytes);
+int h2d(pxb_ctx *c, void *dst, const void *src, size_t bytes);
+int d2h(pxb_ctx *c, void *dst, const void *src, size_t bytes);
+int ensure_pinned(PinnedBuf &b, size_t bytes);
+int sync(pxb_ctx *c);
+int check_launch(pxb_ctx *c, const char *what);
+size_t ctx_bytes(const pxb_ctx *c);
+}  // namespace pxb
