@@ -1,0 +1,409 @@
+"""Benchmark: explicit PDDO fracture bond-updates/s (and g-build nodes/s) on the 2D notched plate
+(400x200 nodes, h = 0.5 mm, delta = 3.015h, plane strain, E = 190 GPa, nu = 0.3, rho = 8000, s_c = 0.01, two
+force-only slits of 50h at y = 0.05 +- 25h, 16.5 m/s pull on the left ghosts between the slits,
+dt = 0.8 h / sqrt(C11/rho)).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl perix|reference] [--precision mixed|fp64]
+
+A step is one explicit time step (damage + Navier force + central difference + BC pass, one fused kernel),
+timed alone with CUDA events on the launching stream; the L2 is flushed (256 MiB write) before every timed
+step, and the state is restored from a snapshot taken 100 steps into the run every 100 steps, so every timed
+step works on the same physical regime (after ~200 further steps the plate's wall mode grows).
+Multi-GPU runs (torchrun) are independent replicas of the plate (weak scaling); the time is the max over ranks.
+Prints one JSON line on rank 0.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FLUSH_BYTES = 256 << 20
+EPISODE = 100          # steps between snapshot restores
+S0 = 100               # steps run before the snapshot is taken
+
+
+# ------------------------------------------------------------------------------------------------- workload
+def c2_setup(px):
+    nx, ny, h = 400, 200, 5e-4
+    L = px.lattice(2, nx, ny, 0, [0.0, nx * h, 0.0, ny * h])
+    delta = 3.015 * L.dxyz[0] * (1.0 + 1e-6)
+    y1, y2 = 0.05 - 25 * h, 0.05 + 25 * h
+    cracks = [[0.0, y1, 50 * h, y1], [0.0, y2, 50 * h, y2]]
+    off, ids = px.families(L.coords, delta, False, cracks=cracks, mirror=L.mirror, force_only=True)
+    health0 = (1 - px.crack_cut_mask(L.coords, L.mirror, off, ids, cracks=cracks)).astype(np.uint8)
+    E, nu, rho = 190e9, 0.3, 8000.0
+    C11, C12, C66 = px.elastic_constants(2, False, E, nu)
+    sc_target = 0.01
+    G0 = sc_target ** 2 * 12.0 * E * delta / (5.0 * math.pi)
+    sc = px.critical_stretch(2, False, G0, E, delta)
+    dt = 0.8 * h / math.sqrt(C11 / rho)
+    bcs = [px.BC("neumann", [0, 1], L.group(w + "nodes_ghost")) for w in ("left", "right", "bottom", "top")]
+    bcs.append(px.BC("dirichlet", [0], L.group("leftnodes_ghost"), value=[0, 0], velocity=[16.5, 0], direct=True,
+                     box=[-1, 1, y1, y2, -1, 1]))
+    return dict(L=L, off=off, ids=ids, delta=delta, health0=health0, C=(C11, C12, C66), rho=rho, sc=sc, dt=dt,
+                bcs=bcs, E=E, nu=nu, G0=G0, cracks=cracks, n=L.n, nb=int(off[-1]), h=h)
+
+
+def algorithmic_bytes(n, nb, dim, prec):
+    """Per step: nb*(4 B id + c*s B operators + 1 B health) + N*(x, u^n, u^{n-1}, u^{n+1}: 4*dim*8 B)."""
+    c = 6 if dim == 3 else 3
+    s = 4 if prec == "mixed" else 8
+    return nb * (4 + c * s + 1) + n * (4 * dim * 8)
+
+
+# ------------------------------------------------------------------------------------------------- helpers
+class ClockSampler:
+    """nvidia-smi samples (SM clock, max clock, throttle reasons) while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap,utilization.gpu")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no-samples"], "samples": 0}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[4 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def reduce_max(value, ws):
+    """Max over ranks (the slowest rank sets the job time)."""
+    if ws <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def read_traffic(prec):
+    """DRAM bytes per step-kernel launch from the committed ncu summary (None until captured)."""
+    path = os.path.join(ROOT, "profiles", "epf_step_c2_plate.md")
+    if not os.path.exists(path):
+        return None
+    key = "traffic_bytes_per_launch_%s:" % prec
+    for line in open(path):
+        if line.strip().startswith(key):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------------------------- reference arm
+def cpu_reference(w, steps, warmup, threads=None):
+    """The reference's own OpenMP CPU path (oracle/_ref, built from the reference sources): per step the
+    element sweep (damage + force) plus the host central difference and BC preset."""
+    from oracle import RefEpf, RefMesh, ref_available
+    if not ref_available():
+        return None
+    nx, ny, h = 400, 200, 5e-4
+    m = RefMesh.structured(2, nx, ny, 0, [0, nx * h, 0, ny * h], 3.015, 2, cracks=w["cracks"], force_only=True)
+    threads = threads or os.cpu_count()
+    bcs = [bc.as_dict() for bc in w["bcs"]]
+    el = RefEpf(m, w["E"], w["nu"], w["rho"], w["G0"], plane_stress=False)
+    el.run(np.zeros(2 * m.n), None, w["dt"], max(1, warmup), bcs, nthreads=threads)
+    el = RefEpf(m, w["E"], w["nu"], w["rho"], w["G0"], plane_stress=False)
+    _, _, _, t0 = el.run(np.zeros(2 * m.n), None, w["dt"], 0, bcs, nthreads=threads)
+    el = RefEpf(m, w["E"], w["nu"], w["rho"], w["G0"], plane_stress=False)
+    _, _, _, tk = el.run(np.zeros(2 * m.n), None, w["dt"], steps, bcs, nthreads=threads)
+    t = max(tk - t0, 1e-9)
+    return dict(value=m.nb * steps / t, seconds=t, steps=steps, cores=threads, nb=m.nb)
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import perix_b200 as px
+    w = c2_setup(px)
+    steps = max(1, args.steps)
+    r = cpu_reference(w, steps, args.warmup)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference sources) not built"}))
+        return
+    sample = "%d explicit steps of the 400x200 plate (element sweep + central difference + BC preset)" % steps
+    line = {"impl": "reference", "metric": "bond-updates/s (explicit frac)", "value": r["value"],
+            "unit": "bond-updates/s", "n_gpus": ws, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * r["seconds"] / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "explicit_pddo_frac 2D notched plate 400x200 (81,200 PD nodes, %d bonds)" % r["nb"],
+                       "threads": r["cores"]},
+            "cpu_baseline": {"value": r["value"], "unit": "bond-updates/s", "cores": r["cores"], "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": r["value"], "unit": "bond-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------------------------------------ perix arm
+def measure_precision(px, w, prec, steps, warmup, ws, device):
+    ctx = px.Context(device)
+    L = w["L"]
+    ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
+    p = px.MIXED if prec == "mixed" else px.FP64
+    C11, C12, C66 = w["C"]
+    ctx.epf_setup(C11, C12, C66, w["rho"], (0.0, 0.0), w["sc"], True, health0=w["health0"], precision=p)
+    ctx.epf_set_bcs(w["bcs"])
+    ctx.epf_start(np.zeros(2 * L.n), None, w["dt"])
+    ctx.epf_advance(S0)
+    snap(ctx)
+    ms = np.zeros(max(warmup, 1), np.float32)
+    time_steps(ctx, max(warmup, 1), ms)
+    restore(ctx)
+    barrier(ws)
+    launches0 = ctx.launch_count()
+    t_wall = time.perf_counter()
+    ms = np.zeros(steps, np.float32)
+    time_steps(ctx, steps, ms)
+    t_wall = time.perf_counter() - t_wall
+    launches = ctx.launch_count() - launches0
+    barrier(ws)
+    return ctx, ms, launches, t_wall
+
+
+def snap(ctx):
+    import ctypes as C
+    st = ctx.L.pxb_epf_snapshot(ctx.h)
+    if st:
+        raise RuntimeError(ctx.L.pxb_last_error().decode())
+
+
+def restore(ctx):
+    st = ctx.L.pxb_epf_restore(ctx.h)
+    if st:
+        raise RuntimeError(ctx.L.pxb_last_error().decode())
+
+
+def time_steps(ctx, nsteps, ms_out):
+    import ctypes as C
+    st = ctx.L.pxb_epf_time_steps(ctx.h, int(nsteps), C.c_size_t(FLUSH_BYTES), EPISODE,
+                                  ms_out.ctypes.data_as(C.POINTER(C.c_float)))
+    if st:
+        raise RuntimeError(ctx.L.pxb_last_error().decode())
+
+
+def gbuild_rate(px, ctx, prec, reps=5):
+    import ctypes as C
+    p = px.MIXED if prec == "mixed" else px.FP64
+    ctx.gbuild(2, p)
+    ms = np.zeros(reps, np.float32)
+    st = ctx.L.pxb_gbuild_time(ctx.h, 2, p, reps, C.c_size_t(FLUSH_BYTES), ms.ctypes.data_as(C.POINTER(C.c_float)))
+    if st:
+        raise RuntimeError(ctx.L.pxb_last_error().decode())
+    return ctx.n / (float(np.mean(ms)) * 1e-3), float(np.mean(ms))
+
+
+def e2e_rate(px, ctx, w, steps):
+    """The drop-in per-step call (reference assembleExplicitPDDOFracAccel semantics): pinned host u in,
+    pinned host acceleration out, every step."""
+    import torch
+    n2 = 2 * w["n"]
+    u_h = torch.empty(n2, dtype=torch.float64, pin_memory=True)
+    a_h = torch.empty(n2, dtype=torch.float64, pin_memory=True)
+    u, _, _, _ = ctx.epf_state()
+    u_h.copy_(torch.from_numpy(u))
+    import ctypes as C
+    nbk = C.c_longlong(0)
+    up = C.cast(C.c_void_p(u_h.data_ptr()), C.POINTER(C.c_double))
+    ap = C.cast(C.c_void_p(a_h.data_ptr()), C.POINTER(C.c_double))
+    for _ in range(3):
+        ctx.L.pxb_epf_rate(ctx.h, up, ap, C.byref(nbk))
+    t = time.perf_counter()
+    for _ in range(steps):
+        st = ctx.L.pxb_epf_rate(ctx.h, up, ap, C.byref(nbk))
+        if st:
+            raise RuntimeError(ctx.L.pxb_last_error().decode())
+    t = time.perf_counter() - t
+    return w["nb"] * steps / t, n2 * 8, n2 * 8 + 16
+
+
+def mixed_error(px, w, device):
+    """max|u_mixed - u_fp64| / max|u_fp64| after 100 graph-captured steps from the same 100-step state."""
+    res = {}
+    for prec in ("fp64", "mixed"):
+        ctx = px.Context(device)
+        L = w["L"]
+        ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
+        C11, C12, C66 = w["C"]
+        ctx.epf_setup(C11, C12, C66, w["rho"], (0.0, 0.0), w["sc"], True, health0=w["health0"],
+                      precision=px.MIXED if prec == "mixed" else px.FP64)
+        ctx.epf_set_bcs(w["bcs"])
+        ctx.epf_start(np.zeros(2 * L.n), None, w["dt"])
+        ctx.epf_advance(2 * S0)
+        res[prec] = ctx.epf_state()
+        ctx.close()
+    u64, u32 = res["fp64"][0], res["mixed"][0]
+    return float(np.abs(u32 - u64).max() / np.abs(u64).max()), int((res["fp64"][2] != res["mixed"][2]).sum())
+
+
+def run_perix(args):
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import perix_b200 as px
+    w = c2_setup(px)
+    hbm, peak_kind = peaks()
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with ClockSampler(local) as clk:
+            ctx, ms, launches, wall = measure_precision(px, w, prec, args.steps, args.warmup, ws, local)
+        t = reduce_max(float(ms.sum()) * 1e-3, ws)
+        steady = None
+        # graph-captured chunk from the snapshot (L2-warm, the production loop)
+        restore(ctx)
+        t0 = time.perf_counter()
+        ctx.epf_advance(EPISODE, chunk=EPISODE)
+        steady = w["nb"] * EPISODE / (time.perf_counter() - t0)
+        gb, gb_ms = gbuild_rate(px, ctx, prec)
+        out[prec] = dict(ctx=ctx, ms=ms, t=t, launches=launches, wall=wall, clocks=clk.summary(), steady=steady,
+                         gbuild=gb, gbuild_ms=gb_ms)
+    err, hdiff = mixed_error(px, w, local)
+    head = "mixed" if err <= 1e-6 else "fp64"
+    r = out[head]
+    steps = args.steps
+    value = ws * w["nb"] * steps / r["t"]
+    mean_s = float(np.mean(r["ms"])) * 1e-3
+    B = algorithmic_bytes(w["n"], w["nb"], 2, head)
+    achieved = B / mean_s / 1e9
+    traffic = read_traffic(head)
+    e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, max(10, min(steps, 200)))
+    cpu = None
+    if rank == 0 and ws == 1:
+        cpu = cpu_reference(w, 20, 2)
+    if rank != 0:
+        return
+    line = {
+        "metric": "bond-updates/s (explicit frac)",
+        "value": value,
+        "unit": "bond-updates/s",
+        "n_gpus": ws,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * r["t"] / steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "precision": head + (" (f32 operator storage, f64 arithmetic and state)" if head == "mixed" else ""),
+        "data": "synthetic",
+        "config": {"workload": "explicit_pddo_frac 2D notched plate 400x200 (81,200 PD nodes, %d directed bonds), "
+                               "dt=0.8h/c" % w["nb"],
+                   "nodes": w["n"], "bonds": w["nb"], "parallelism": "replicas" if ws > 1 else "single-gpu",
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "state": "snapshot after %d steps, restored every %d steps" % (S0, EPISODE)},
+        "e2e": {"value": ws * e2e, "unit": "bond-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "pxb_epf_rate (drop-in per-step call, pinned host u in / acceleration out)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": B, "kernel": "pxb::epf_kernel<2,%s,EPF_STEP>" % (
+                         "true" if head == "mixed" else "false")},
+        "cpu_baseline": ({"value": cpu["value"], "unit": "bond-updates/s", "cores": cpu["cores"],
+                          "kind": "reference",
+                          "sample": "20 explicit steps of the same plate through the reference's OpenMP CPU path"}
+                         if cpu else None),
+        "gpu_launches": int(r["launches"]),
+        "clocks": {k: r["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "fp64": {"value": ws * w["nb"] * steps / out["fp64"]["t"], "ms_per_step": 1e3 * out["fp64"]["t"] / steps},
+        "mixed": {"value": ws * w["nb"] * steps / out["mixed"]["t"], "ms_per_step": 1e3 * out["mixed"]["t"] / steps,
+                  "rel_err_vs_fp64_after_100_steps": err, "health_differs": hdiff},
+        "steady_state_graph": {"fp64": out["fp64"]["steady"], "mixed": out["mixed"]["steady"],
+                               "note": "100-step CUDA-graph chunk, L2-warm (wall clock incl. host sync)"},
+        "gbuild_nodes_per_s": {"fp64": out["fp64"]["gbuild"], "mixed": out["mixed"]["gbuild"],
+                               "ms": {"fp64": out["fp64"]["gbuild_ms"], "mixed": out["mixed"]["gbuild_ms"]},
+                               "workload": "order-2 g-build of the same plate (81,200 nodes, all 5 operators stored)"},
+    }
+    print(json.dumps(line))
+    for p in out.values():
+        p["ctx"].close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="perix", choices=["perix", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_perix(args)
+
+
+if __name__ == "__main__":
+    main()

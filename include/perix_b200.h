@@ -152,6 +152,18 @@ int pxb_epf_force_adjoint_d(pxb_ctx *ctx, const double *u_d, const double *abar_
 /* Force (rate) with a frozen mask, device pointers, no damage update: a = (L(u)+b)/rho. */
 int pxb_epf_force_frozen_d(pxb_ctx *ctx, const double *u_d, double *a_d);
 
+/* ---- measurement support -----------------------------------------------------------------------------------
+ * Device-side copy of the explicit state (u, u_prev, health, t) and its restore. */
+int pxb_epf_snapshot(pxb_ctx *ctx);
+int pxb_epf_restore(pxb_ctx *ctx);
+/* nsteps explicit steps launched one at a time; before each launch the L2 is flushed by writing flush_bytes
+ * (0 = none) and every restore_every steps (0 = never) the snapshot is restored; ms[s] = CUDA-event duration
+ * of step s's kernel alone.  The blow-up guard is not evaluated. */
+int pxb_epf_time_steps(pxb_ctx *ctx, int nsteps, size_t flush_bytes, int restore_every, float *ms);
+/* reps g-builds into the existing operator cache (same order/precision as the last pxb_gbuild), L2 flushed
+ * before each; ms[r] = CUDA-event duration of build r. */
+int pxb_gbuild_time(pxb_ctx *ctx, int order, int precision, int reps, size_t flush_bytes, float *ms);
+
 /* ---- CSR Jacobian value assembly ---------------------------------------------------------------------------
  * Sets the matrix pattern (from pxb_csr_pattern or the caller) and precomputes the bond -> CSR-slot map
  * on the device (no binary search per assembly). */

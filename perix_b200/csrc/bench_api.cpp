@@ -1,0 +1,162 @@
+// Measurement support in the C-ABI: device-side state snapshots and CUDA-event timing of individual kernel
+// launches on the context stream (so a caller can time exactly the step kernel, with the L2 flushed before
+// each launch, without host work inside the measured interval).
+#include <algorithm>
+#include <vector>
+
+#include "k_kernels.h"
+#include "pxb_context.h"
+
+namespace pxb {
+int step_args(pxb_ctx *c, int par, EpfArgs *out);
+int gbuild_launch_only(pxb_ctx *c, int order, int precision);
+}  // namespace pxb
+
+using namespace pxb;
+
+namespace {
+
+struct Snapshot {
+    DevBuf u0, u1, health;
+    int cur = 0;
+    double t = 0.0;
+    long long step = 0;
+    bool valid = false;
+};
+
+// one snapshot per context, kept outside pxb_ctx so the hot-path state stays lean
+std::vector<std::pair<pxb_ctx *, Snapshot>> g_snaps;
+
+Snapshot &snap_of(pxb_ctx *c) {
+    for (auto &kv : g_snaps)
+        if (kv.first == c) return kv.second;
+    g_snaps.emplace_back(c, Snapshot{});
+    return g_snaps.back().second;
+}
+
+int d2d(pxb_ctx *c, void *dst, const void *src, size_t bytes) {
+    PXB_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    return PXB_OK;
+}
+
+struct Events {
+    std::vector<cudaEvent_t> ev;
+    ~Events() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+    int make(size_t n) {
+        ev.resize(n, nullptr);
+        for (auto &e : ev) PXB_CUDA_TRY(cudaEventCreate(&e));
+        return PXB_OK;
+    }
+};
+
+int flush_l2(pxb_ctx *c, size_t bytes, DevBuf &buf) {
+    if (bytes == 0) return PXB_OK;
+    if (buf.bytes < bytes) PXB_TRY(dev_alloc(c, buf, bytes));
+    launch_l2_flush(buf.p, bytes, c->stream);
+    return check_launch(c, "l2 flush");
+}
+
+DevBuf g_flush;
+
+}  // namespace
+
+namespace pxb {
+// called when a context is destroyed: release its snapshot
+void drop_snapshot(pxb_ctx *c) {
+    for (auto it = g_snaps.begin(); it != g_snaps.end(); ++it)
+        if (it->first == c) {
+            g_snaps.erase(it);
+            return;
+        }
+}
+}  // namespace pxb
+
+extern "C" int pxb_epf_snapshot(pxb_ctx *c) {
+    if (!c || !c->epf.ready || !c->epf.started) return fail(PXB_ERR_STATE, "pxb_epf_snapshot: no running explicit state");
+    EpfState &e = c->epf;
+    Snapshot &s = snap_of(c);
+    PXB_TRY(dev_alloc(c, s.u0, e.u[0].bytes));
+    PXB_TRY(dev_alloc(c, s.u1, e.u[1].bytes));
+    PXB_TRY(dev_alloc(c, s.health, e.health.bytes));
+    PXB_TRY(d2d(c, s.u0.p, e.u[0].p, e.u[0].bytes));
+    PXB_TRY(d2d(c, s.u1.p, e.u[1].p, e.u[1].bytes));
+    PXB_TRY(d2d(c, s.health.p, e.health.p, e.health.bytes));
+    s.cur = e.cur;
+    s.t = e.t;
+    s.step = e.step;
+    s.valid = true;
+    return sync(c);
+}
+
+extern "C" int pxb_epf_restore(pxb_ctx *c) {
+    if (!c || !c->epf.ready) return fail(PXB_ERR_STATE, "pxb_epf_restore: no explicit state");
+    Snapshot &s = snap_of(c);
+    if (!s.valid) return fail(PXB_ERR_STATE, "pxb_epf_restore: no snapshot taken");
+    EpfState &e = c->epf;
+    PXB_TRY(d2d(c, e.u[0].p, s.u0.p, s.u0.bytes));
+    PXB_TRY(d2d(c, e.u[1].p, s.u1.p, s.u1.bytes));
+    PXB_TRY(d2d(c, e.health.p, s.health.p, s.health.bytes));
+    e.cur = s.cur;
+    e.t = s.t;
+    e.step = s.step;
+    e.umax_hist.resize((size_t)std::min<long long>(s.step, (long long)e.umax_hist.size()));
+    return PXB_OK;
+}
+
+// Runs nsteps explicit steps one launch at a time; before each launch the L2 is flushed by writing
+// flush_bytes (0 = no flush) and, every restore_every steps (0 = never), the snapshot is restored.  ms[s]
+// receives the CUDA-event duration of step s's kernel alone.  The blow-up guard is not evaluated here.
+extern "C" int pxb_epf_time_steps(pxb_ctx *c, int nsteps, size_t flush_bytes, int restore_every, float *ms) {
+    if (!c || !c->epf.ready || !c->epf.started) return fail(PXB_ERR_STATE, "pxb_epf_time_steps: call pxb_epf_start first");
+    if (nsteps <= 0 || !ms) return fail(PXB_ERR_INVALID, "pxb_epf_time_steps: bad arguments");
+    EpfState &e = c->epf;
+    if (e.graph_chunk < 1) {
+        PXB_TRY(dev_alloc(c, e.umax, sizeof(unsigned long long)));
+        PXB_TRY(dev_alloc(c, e.tsched, sizeof(double)));
+        PXB_TRY(ensure_pinned(e.tsched_h, 64));
+        e.graph_chunk = 1;
+    }
+    Events ev;
+    PXB_TRY(ev.make(2 * (size_t)nsteps));
+    double *th = static_cast<double *>(e.tsched_h.p);
+    for (int s = 0; s < nsteps; ++s) {
+        if (restore_every > 0 && s > 0 && s % restore_every == 0) PXB_TRY(pxb_epf_restore(c));
+        // t_{n+1} for this step (host-accumulated exactly like the reference loop)
+        PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        th[0] = e.t + e.dt;
+        PXB_TRY(h2d(c, e.tsched.p, th, sizeof(double)));
+        PXB_TRY(flush_l2(c, flush_bytes, g_flush));
+        EpfArgs a;
+        PXB_TRY(step_args(c, e.cur, &a));
+        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)s], c->stream));
+        const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_STEP, epf_grid(c->g.n), c->stream);
+        if (err != cudaSuccess) return cuda_fail(err, "epf step launch");
+        c->launches++;
+        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)s + 1], c->stream));
+        e.cur ^= 1;
+        e.t = th[0];
+        e.step++;
+    }
+    PXB_TRY(sync(c));
+    for (int s = 0; s < nsteps; ++s) PXB_CUDA_TRY(cudaEventElapsedTime(&ms[s], ev.ev[2 * (size_t)s], ev.ev[2 * (size_t)s + 1]));
+    return PXB_OK;
+}
+
+// Times `reps` g-builds (order, precision) of the current geometry, L2 flushed before each; ms[r] per build.
+extern "C" int pxb_gbuild_time(pxb_ctx *c, int order, int precision, int reps, size_t flush_bytes, float *ms) {
+    if (!c || !c->g.ready) return fail(PXB_ERR_STATE, "pxb_gbuild_time: geometry not set");
+    if (reps <= 0 || !ms) return fail(PXB_ERR_INVALID, "pxb_gbuild_time: bad arguments");
+    Events ev;
+    PXB_TRY(ev.make(2 * (size_t)reps));
+    for (int r = 0; r < reps; ++r) {
+        PXB_TRY(flush_l2(c, flush_bytes, g_flush));
+        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r], c->stream));
+        PXB_TRY(gbuild_launch_only(c, order, precision));
+        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r + 1], c->stream));
+    }
+    PXB_TRY(sync(c));
+    for (int r = 0; r < reps; ++r) PXB_CUDA_TRY(cudaEventElapsedTime(&ms[r], ev.ev[2 * (size_t)r], ev.ev[2 * (size_t)r + 1]));
+    return PXB_OK;
+}

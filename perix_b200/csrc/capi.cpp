@@ -172,10 +172,15 @@ extern "C" int pxb_ctx_create(int device, pxb_ctx **out) {
     return PXB_OK;
 }
 
+namespace pxb {
+void drop_snapshot(pxb_ctx *c);
+}
+
 extern "C" int pxb_ctx_destroy(pxb_ctx *c) {
     if (!c) return PXB_OK;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    drop_snapshot(c);
     destroy_graphs(c->epf);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
@@ -280,19 +285,9 @@ static int ensure_rev(pxb_ctx *c) {
 }
 
 // ===================================================================================================== g-build
-static int run_gbuild(pxb_ctx *c, int order, bool mixed, void *ops_out, void *G_out, uint8_t *deg_out,
-                      int *n_degenerate, int *first_degenerate) {
+static GBuildArgs gbuild_args(pxb_ctx *c, void *ops_out, void *G_out, uint8_t *deg_out, unsigned int *nd,
+                              int *first) {
     Geometry &g = c->g;
-    if (!gbuild_supported(g.dim, order))
-        return fail(PXB_ERR_UNSUPPORTED, "pxb_gbuild: order " + std::to_string(order) + " not built for dim " +
-                                             std::to_string(g.dim) + " (2D: 1..3, 3D: 1..2)");
-    void *tmp = nullptr;
-    PXB_TRY(scratch(c, 16, &tmp));
-    unsigned int *nd = static_cast<unsigned int *>(tmp);
-    int *first = reinterpret_cast<int *>(static_cast<char *>(tmp) + 8);
-    PXB_CUDA_TRY(cudaMemsetAsync(nd, 0, 4, c->stream));
-    const int big = std::numeric_limits<int>::max();
-    PXB_TRY(h2d(c, first, &big, sizeof(int)));
     GBuildArgs a;
     a.n = g.n;
     a.nb = g.nb;
@@ -308,6 +303,23 @@ static int run_gbuild(pxb_ctx *c, int order, bool mixed, void *ops_out, void *G_
     a.degenerate = deg_out;
     a.n_degenerate = nd;
     a.first_degenerate = first;
+    return a;
+}
+
+static int run_gbuild(pxb_ctx *c, int order, bool mixed, void *ops_out, void *G_out, uint8_t *deg_out,
+                      int *n_degenerate, int *first_degenerate) {
+    Geometry &g = c->g;
+    if (!gbuild_supported(g.dim, order))
+        return fail(PXB_ERR_UNSUPPORTED, "pxb_gbuild: order " + std::to_string(order) + " not built for dim " +
+                                             std::to_string(g.dim) + " (2D: 1..3, 3D: 1..2)");
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, 16, &tmp));
+    unsigned int *nd = static_cast<unsigned int *>(tmp);
+    int *first = reinterpret_cast<int *>(static_cast<char *>(tmp) + 8);
+    PXB_CUDA_TRY(cudaMemsetAsync(nd, 0, 4, c->stream));
+    const int big = std::numeric_limits<int>::max();
+    PXB_TRY(h2d(c, first, &big, sizeof(int)));
+    const GBuildArgs a = gbuild_args(c, ops_out, G_out, deg_out, nd, first);
     cudaError_t e = launch_gbuild(a, g.dim, order, mixed, grid_nodes(g.n, kGbuildThreads), c->stream);
     c->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "gbuild launch");
@@ -351,6 +363,24 @@ extern "C" int pxb_gbuild(pxb_ctx *c, int order, int precision, int *n_degenerat
     if (st == PXB_OK || st == PXB_ERR_DEGENERATE) o.ready = true;  // degenerate rows carry zero operators
     return st;
 }
+
+namespace pxb {
+// relaunch the g-build into the existing operator cache (same order/precision), no host synchronisation
+int gbuild_launch_only(pxb_ctx *c, int order, int precision) {
+    if (!c->ops.ready || c->ops.order != order || c->ops.precision != precision)
+        return fail(PXB_ERR_STATE, "g-build timing needs a prior pxb_gbuild with the same order and precision");
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, 16, &tmp));
+    const GBuildArgs a = gbuild_args(c, c->ops.ops.p, nullptr, c->ops.degenerate.as<uint8_t>(),
+                                     static_cast<unsigned int *>(tmp),
+                                     reinterpret_cast<int *>(static_cast<char *>(tmp) + 8));
+    cudaError_t e = launch_gbuild(a, c->g.dim, order, precision == PXB_MIXED, grid_nodes(c->g.n, kGbuildThreads),
+                                  c->stream);
+    c->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "gbuild launch");
+    return PXB_OK;
+}
+}  // namespace pxb
 
 extern "C" int pxb_gbuild_info(pxb_ctx *c, int *nop, int *pqr) {
     if (!c) return fail(PXB_ERR_INVALID, "pxb_gbuild_info: NULL context");
@@ -704,8 +734,9 @@ extern "C" int pxb_epf_start(pxb_ctx *c, const double *u0, const double *v0, dou
     return PXB_OK;
 }
 
-// one STEP launch on stream s: reads u[par], writes u[par^1]
-static int launch_step(pxb_ctx *c, int par, int q, cudaStream_t s) {
+namespace pxb {
+// argument block of one STEP launch at ping-pong parity par (reads u[par], writes u[par^1])
+int step_args(pxb_ctx *c, int par, EpfArgs *out) {
     EpfState &e = c->epf;
     EpfArgs a = epf_args(c);
     fill_bc(c, a);
@@ -714,8 +745,19 @@ static int launch_step(pxb_ctx *c, int par, int q, cudaStream_t s) {
     a.dt = e.dt;
     a.dt2 = e.dt * e.dt;
     a.t_sched = e.tsched.as<double>();
-    a.step_in_chunk = q;
+    a.step_in_chunk = 0;
     a.umax = e.umax.as<unsigned long long>();
+    *out = a;
+    return PXB_OK;
+}
+}  // namespace pxb
+
+// one STEP launch on stream s: reads u[par], writes u[par^1]
+static int launch_step(pxb_ctx *c, int par, int q, cudaStream_t s) {
+    EpfState &e = c->epf;
+    EpfArgs a;
+    step_args(c, par, &a);
+    a.step_in_chunk = q;
     const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_STEP, epf_grid(c->g.n), s);
     if (err != cudaSuccess) return cuda_fail(err, "epf step launch");
     return PXB_OK;
