@@ -214,6 +214,7 @@ def measure_precision(px, w, prec, steps, warmup, ws, device):
     ctx.epf_start(np.zeros(2 * L.n), None, w["dt"])
     ctx.epf_advance(S0)
     snap(ctx)
+    tuned = autotune(ctx)
     ms = np.zeros(max(warmup, 1), np.float32)
     time_steps(ctx, max(warmup, 1), ms)
     restore(ctx)
@@ -225,7 +226,22 @@ def measure_precision(px, w, prec, steps, warmup, ws, device):
     t_wall = time.perf_counter() - t_wall
     launches = ctx.launch_count() - launches0
     barrier(ws)
-    return ctx, ms, launches, t_wall
+    return ctx, ms, launches, t_wall, tuned
+
+
+def autotune(ctx, steps=20):
+    """pxb_epf_autotune: time each schedule variant on this plate from the snapshot state, keep the fastest."""
+    import ctypes as C
+    best = C.c_int(0)
+    ms = np.zeros(3, np.float32)
+    st = ctx.L.pxb_epf_autotune(ctx.h, steps, C.c_size_t(FLUSH_BYTES), 0, C.byref(best),
+                                ms.ctypes.data_as(C.POINTER(C.c_float)))
+    if st:
+        raise RuntimeError(ctx.L.pxb_last_error().decode())
+    lpn = C.c_int(0)
+    v = C.c_int(0)
+    ctx.L.pxb_epf_get_variant(ctx.h, C.byref(v), C.byref(lpn))
+    return {"variant": best.value, "lanes_per_node": lpn.value, "ms_per_variant": [round(float(x), 5) for x in ms]}
 
 
 def snap(ctx):
@@ -318,7 +334,7 @@ def run_perix(args):
     out = {}
     for prec in ("fp64", "mixed"):
         with ClockSampler(local) as clk:
-            ctx, ms, launches, wall = measure_precision(px, w, prec, args.steps, args.warmup, ws, local)
+            ctx, ms, launches, wall, tuned = measure_precision(px, w, prec, args.steps, args.warmup, ws, local)
         t = reduce_max(float(ms.sum()) * 1e-3, ws)
         steady = None
         # graph-captured chunk from the snapshot (L2-warm, the production loop)
@@ -328,7 +344,7 @@ def run_perix(args):
         steady = w["nb"] * EPISODE / (time.perf_counter() - t0)
         gb, gb_ms = gbuild_rate(px, ctx, prec)
         out[prec] = dict(ctx=ctx, ms=ms, t=t, launches=launches, wall=wall, clocks=clk.summary(), steady=steady,
-                         gbuild=gb, gbuild_ms=gb_ms)
+                         gbuild=gb, gbuild_ms=gb_ms, tuned=tuned)
     err, hdiff = mixed_error(px, w, local)
     head = "mixed" if err <= 1e-6 else "fp64"
     r = out[head]
@@ -367,17 +383,18 @@ def run_perix(args):
                 "api": "pxb_epf_rate (drop-in per-step call, pinned host u in / acceleration out)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": B, "kernel": "pxb::epf_kernel<2,%s,EPF_STEP>" % (
-                         "true" if head == "mixed" else "false")},
+                     "algorithmic_bytes_per_launch": B, "kernel": "pxb::epf_kernel<2,%s,EPF_STEP,LPN=%d>" % (
+                         "true" if head == "mixed" else "false", out[head]["tuned"]["lanes_per_node"])},
         "cpu_baseline": ({"value": cpu["value"], "unit": "bond-updates/s", "cores": cpu["cores"],
                           "kind": "reference",
                           "sample": "20 explicit steps of the same plate through the reference's OpenMP CPU path"}
                          if cpu else None),
         "gpu_launches": int(r["launches"]),
         "clocks": {k: r["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
-        "fp64": {"value": ws * w["nb"] * steps / out["fp64"]["t"], "ms_per_step": 1e3 * out["fp64"]["t"] / steps},
+        "fp64": {"value": ws * w["nb"] * steps / out["fp64"]["t"], "ms_per_step": 1e3 * out["fp64"]["t"] / steps,
+                 "autotune": out["fp64"]["tuned"]},
         "mixed": {"value": ws * w["nb"] * steps / out["mixed"]["t"], "ms_per_step": 1e3 * out["mixed"]["t"] / steps,
-                  "rel_err_vs_fp64_after_100_steps": err, "health_differs": hdiff},
+                  "rel_err_vs_fp64_after_100_steps": err, "health_differs": hdiff, "autotune": out["mixed"]["tuned"]},
         "steady_state_graph": {"fp64": out["fp64"]["steady"], "mixed": out["mixed"]["steady"],
                                "note": "100-step CUDA-graph chunk, L2-warm (wall clock incl. host sync)"},
         "gbuild_nodes_per_s": {"fp64": out["fp64"]["gbuild"], "mixed": out["mixed"]["gbuild"],

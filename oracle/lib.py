@@ -102,7 +102,7 @@ class PortOracle:
         mir = None if mirror is None else np.ascontiguousarray(mirror, np.int32)
         return bool(self.L.orc_crack_cuts(coords3.size // 3, _ptr(coords3, C.c_double), _ptr(mir, C.c_int),
                                           0 if cr is None else cr.size // 4, _ptr(cr, C.c_double),
-                                          0 if pl is None else pl.size // 12, _ptr(pl, C.c_double), i1, j1))
+                                          0 if pl is None else pl.size // 12, _ptr(pl, C.c_double), int(i1), int(j1)))
 
     def gbuild(self, dim, order, coords3, vols, off, ids, delta, dx_char, volume_correction=True):
         coords3 = np.ascontiguousarray(coords3, np.float64).reshape(-1)

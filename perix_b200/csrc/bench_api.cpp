@@ -2,6 +2,8 @@
 // launches on the context stream (so a caller can time exactly the step kernel, with the L2 flushed before
 // each launch, without host work inside the measured interval).
 #include <algorithm>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "k_kernels.h"
@@ -60,6 +62,76 @@ int flush_l2(pxb_ctx *c, size_t bytes, DevBuf &buf) {
 
 DevBuf g_flush;
 
+int save_state(pxb_ctx *c, Snapshot &s) {
+    EpfState &e = c->epf;
+    PXB_TRY(dev_alloc(c, s.u0, e.u[0].bytes));
+    PXB_TRY(dev_alloc(c, s.u1, e.u[1].bytes));
+    PXB_TRY(dev_alloc(c, s.health, e.health.bytes));
+    PXB_TRY(d2d(c, s.u0.p, e.u[0].p, e.u[0].bytes));
+    PXB_TRY(d2d(c, s.u1.p, e.u[1].p, e.u[1].bytes));
+    PXB_TRY(d2d(c, s.health.p, e.health.p, e.health.bytes));
+    s.cur = e.cur;
+    s.t = e.t;
+    s.step = e.step;
+    s.valid = true;
+    return sync(c);
+}
+
+int load_state(pxb_ctx *c, const Snapshot &s) {
+    EpfState &e = c->epf;
+    PXB_TRY(d2d(c, e.u[0].p, s.u0.p, s.u0.bytes));
+    PXB_TRY(d2d(c, e.u[1].p, s.u1.p, s.u1.bytes));
+    PXB_TRY(d2d(c, e.health.p, s.health.p, s.health.bytes));
+    e.cur = s.cur;
+    e.t = s.t;
+    e.step = s.step;
+    e.umax_hist.resize((size_t)std::min<long long>(s.step, (long long)e.umax_hist.size()));
+    return PXB_OK;
+}
+
+// nsteps single-kernel steps of the current schedule variant, each timed alone (see pxb_epf_time_steps)
+int timed_steps(pxb_ctx *c, int nsteps, size_t flush_bytes, int restore_every, const Snapshot *snap, float *ms) {
+    EpfState &e = c->epf;
+    if (e.graph_chunk < 1) {
+        PXB_TRY(dev_alloc(c, e.umax, sizeof(unsigned long long)));
+        PXB_TRY(dev_alloc(c, e.tsched, sizeof(double)));
+        PXB_TRY(ensure_pinned(e.tsched_h, 64));
+        e.graph_chunk = 1;
+    }
+    Events ev;
+    PXB_TRY(ev.make(2 * (size_t)nsteps));
+    double *th = static_cast<double *>(e.tsched_h.p);
+    for (int s = 0; s < nsteps; ++s) {
+        if (snap && restore_every > 0 && s > 0 && s % restore_every == 0) PXB_TRY(load_state(c, *snap));
+        // t_{n+1} for this step (host-accumulated exactly like the reference loop)
+        PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        th[0] = e.t + e.dt;
+        PXB_TRY(h2d(c, e.tsched.p, th, sizeof(double)));
+        PXB_TRY(flush_l2(c, flush_bytes, g_flush));
+        EpfArgs a;
+        PXB_TRY(step_args(c, e.cur, &a));
+        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)s], c->stream));
+        const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_STEP, e.variant, c->stream);
+        if (err != cudaSuccess) return cuda_fail(err, "epf step launch");
+        c->launches++;
+        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)s + 1], c->stream));
+        e.cur ^= 1;
+        e.t = th[0];
+        e.step++;
+    }
+    PXB_TRY(sync(c));
+    for (int s = 0; s < nsteps; ++s) PXB_CUDA_TRY(cudaEventElapsedTime(&ms[s], ev.ev[2 * (size_t)s], ev.ev[2 * (size_t)s + 1]));
+    return PXB_OK;
+}
+
+// process-wide cache of autotuned schedule choices, keyed by problem signature
+std::map<std::string, int> g_tuned;
+
+std::string signature(const pxb_ctx *c) {
+    return std::to_string(c->g.dim) + ":" + std::to_string(c->epf.precision) + ":" + std::to_string(c->g.n) + ":" +
+           std::to_string(c->g.nb) + ":" + std::to_string(c->g.max_family);
+}
+
 }  // namespace
 
 namespace pxb {
@@ -75,33 +147,63 @@ void drop_snapshot(pxb_ctx *c) {
 
 extern "C" int pxb_epf_snapshot(pxb_ctx *c) {
     if (!c || !c->epf.ready || !c->epf.started) return fail(PXB_ERR_STATE, "pxb_epf_snapshot: no running explicit state");
-    EpfState &e = c->epf;
-    Snapshot &s = snap_of(c);
-    PXB_TRY(dev_alloc(c, s.u0, e.u[0].bytes));
-    PXB_TRY(dev_alloc(c, s.u1, e.u[1].bytes));
-    PXB_TRY(dev_alloc(c, s.health, e.health.bytes));
-    PXB_TRY(d2d(c, s.u0.p, e.u[0].p, e.u[0].bytes));
-    PXB_TRY(d2d(c, s.u1.p, e.u[1].p, e.u[1].bytes));
-    PXB_TRY(d2d(c, s.health.p, e.health.p, e.health.bytes));
-    s.cur = e.cur;
-    s.t = e.t;
-    s.step = e.step;
-    s.valid = true;
-    return sync(c);
+    return save_state(c, snap_of(c));
 }
 
 extern "C" int pxb_epf_restore(pxb_ctx *c) {
     if (!c || !c->epf.ready) return fail(PXB_ERR_STATE, "pxb_epf_restore: no explicit state");
     Snapshot &s = snap_of(c);
     if (!s.valid) return fail(PXB_ERR_STATE, "pxb_epf_restore: no snapshot taken");
-    EpfState &e = c->epf;
-    PXB_TRY(d2d(c, e.u[0].p, s.u0.p, s.u0.bytes));
-    PXB_TRY(d2d(c, e.u[1].p, s.u1.p, s.u1.bytes));
-    PXB_TRY(d2d(c, e.health.p, s.health.p, s.health.bytes));
-    e.cur = s.cur;
-    e.t = s.t;
-    e.step = s.step;
-    e.umax_hist.resize((size_t)std::min<long long>(s.step, (long long)e.umax_hist.size()));
+    return load_state(c, s);
+}
+
+extern "C" int pxb_epf_set_variant(pxb_ctx *c, int variant) {
+    if (!c || !c->epf.ready) return fail(PXB_ERR_STATE, "pxb_epf_set_variant: call pxb_epf_setup first");
+    if (variant < 0 || variant >= kEpfVariants) return fail(PXB_ERR_INVALID, "pxb_epf_set_variant: no such variant");
+    c->epf.variant = variant;
+    return PXB_OK;
+}
+
+extern "C" int pxb_epf_get_variant(pxb_ctx *c, int *variant, int *lanes_per_node) {
+    if (!c || !c->epf.ready || !variant) return fail(PXB_ERR_STATE, "pxb_epf_get_variant: call pxb_epf_setup first");
+    *variant = c->epf.variant;
+    if (lanes_per_node) *lanes_per_node = epf_lanes_per_node(c->g.dim, c->epf.variant);
+    return PXB_OK;
+}
+
+// Times every schedule variant for `steps` steps (L2 flushed before each) from a private copy of the current
+// state, restores the state, selects the fastest and caches the choice for this problem signature.
+extern "C" int pxb_epf_autotune(pxb_ctx *c, int steps, size_t flush_bytes, int use_cache, int *best,
+                                float *ms_per_variant) {
+    if (!c || !c->epf.ready || !c->epf.started) return fail(PXB_ERR_STATE, "pxb_epf_autotune: call pxb_epf_start first");
+    if (steps <= 0) return fail(PXB_ERR_INVALID, "pxb_epf_autotune: steps must be > 0");
+    const std::string key = signature(c);
+    auto hit = g_tuned.find(key);
+    if (use_cache && hit != g_tuned.end()) {
+        c->epf.variant = hit->second;
+        if (best) *best = hit->second;
+        return PXB_OK;
+    }
+    Snapshot keep;
+    PXB_TRY(save_state(c, keep));
+    std::vector<float> ms((size_t)steps);
+    float best_ms = 1e30f;
+    int best_v = c->epf.variant;
+    for (int v = 0; v < kEpfVariants; ++v) {
+        c->epf.variant = v;
+        PXB_TRY(load_state(c, keep));
+        PXB_TRY(timed_steps(c, steps, flush_bytes, 0, nullptr, ms.data()));
+        float mean = 0.f;
+        for (float x : ms) mean += x;
+        mean /= (float)steps;
+        if (ms_per_variant) ms_per_variant[v] = mean;
+        if (mean < best_ms) { best_ms = mean; best_v = v; }
+    }
+    PXB_TRY(load_state(c, keep));
+    PXB_TRY(sync(c));
+    c->epf.variant = best_v;
+    g_tuned[key] = best_v;
+    if (best) *best = best_v;
     return PXB_OK;
 }
 
@@ -111,37 +213,8 @@ extern "C" int pxb_epf_restore(pxb_ctx *c) {
 extern "C" int pxb_epf_time_steps(pxb_ctx *c, int nsteps, size_t flush_bytes, int restore_every, float *ms) {
     if (!c || !c->epf.ready || !c->epf.started) return fail(PXB_ERR_STATE, "pxb_epf_time_steps: call pxb_epf_start first");
     if (nsteps <= 0 || !ms) return fail(PXB_ERR_INVALID, "pxb_epf_time_steps: bad arguments");
-    EpfState &e = c->epf;
-    if (e.graph_chunk < 1) {
-        PXB_TRY(dev_alloc(c, e.umax, sizeof(unsigned long long)));
-        PXB_TRY(dev_alloc(c, e.tsched, sizeof(double)));
-        PXB_TRY(ensure_pinned(e.tsched_h, 64));
-        e.graph_chunk = 1;
-    }
-    Events ev;
-    PXB_TRY(ev.make(2 * (size_t)nsteps));
-    double *th = static_cast<double *>(e.tsched_h.p);
-    for (int s = 0; s < nsteps; ++s) {
-        if (restore_every > 0 && s > 0 && s % restore_every == 0) PXB_TRY(pxb_epf_restore(c));
-        // t_{n+1} for this step (host-accumulated exactly like the reference loop)
-        PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        th[0] = e.t + e.dt;
-        PXB_TRY(h2d(c, e.tsched.p, th, sizeof(double)));
-        PXB_TRY(flush_l2(c, flush_bytes, g_flush));
-        EpfArgs a;
-        PXB_TRY(step_args(c, e.cur, &a));
-        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)s], c->stream));
-        const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_STEP, epf_grid(c->g.n), c->stream);
-        if (err != cudaSuccess) return cuda_fail(err, "epf step launch");
-        c->launches++;
-        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)s + 1], c->stream));
-        e.cur ^= 1;
-        e.t = th[0];
-        e.step++;
-    }
-    PXB_TRY(sync(c));
-    for (int s = 0; s < nsteps; ++s) PXB_CUDA_TRY(cudaEventElapsedTime(&ms[s], ev.ev[2 * (size_t)s], ev.ev[2 * (size_t)s + 1]));
-    return PXB_OK;
+    Snapshot &s = snap_of(c);
+    return timed_steps(c, nsteps, flush_bytes, restore_every, s.valid ? &s : nullptr, ms);
 }
 
 // Times `reps` g-builds (order, precision) of the current geometry, L2 flushed before each; ms[r] per build.

@@ -553,7 +553,7 @@ extern "C" int pxb_epf_rate(pxb_ctx *c, const double *u, double *accel, long lon
     EpfArgs a = epf_args(c);
     a.u = e.u[e.cur].as<double>();
     a.accel = e.accel.as<double>();
-    launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_RATE, epf_grid(c->g.n), c->stream);
+    launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_RATE, e.variant, c->stream);
     PXB_TRY(check_launch(c, "epf rate"));
     PXB_TRY(d2h(c, accel, e.accel.p, sizeof(double) * nd));
     PXB_TRY(d2h(c, &after, e.counters.p, 8));
@@ -723,7 +723,7 @@ extern "C" int pxb_epf_start(pxb_ctx *c, const double *u0, const double *v0, dou
     a.v0 = dv0;
     a.dt = dt;
     a.dt2 = 0.5 * dt * dt;
-    launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_START, epf_grid(c->g.n), c->stream);
+    launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_START, e.variant, c->stream);
     PXB_TRY(check_launch(c, "epf start"));
     PXB_TRY(sync(c));
     e.dt = dt;
@@ -758,14 +758,14 @@ static int launch_step(pxb_ctx *c, int par, int q, cudaStream_t s) {
     EpfArgs a;
     step_args(c, par, &a);
     a.step_in_chunk = q;
-    const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_STEP, epf_grid(c->g.n), s);
+    const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_STEP, e.variant, s);
     if (err != cudaSuccess) return cuda_fail(err, "epf step launch");
     return PXB_OK;
 }
 
 static int get_graph(pxb_ctx *c, int steps, cudaGraphExec_t *out) {
     EpfState &e = c->epf;
-    const GraphKey key{steps, e.cur, e.precision};
+    const GraphKey key{steps, e.cur, e.precision, e.variant};
     auto it = e.graphs.find(key);
     if (it != e.graphs.end()) { *out = it->second; return PXB_OK; }
     // captured on the context's own stream (never the legacy default stream), replayed on c->stream
@@ -893,7 +893,7 @@ extern "C" int pxb_epf_force_frozen_d(pxb_ctx *c, const double *u_d, double *a_d
     a.u = u_d;
     a.accel = a_d;
     a.damage = 0;
-    launch_epf(a, c->g.dim, c->epf.precision == PXB_MIXED, EPF_FORCE_FROZEN, epf_grid(c->g.n), c->stream);
+    launch_epf(a, c->g.dim, c->epf.precision == PXB_MIXED, EPF_FORCE_FROZEN, c->epf.variant, c->stream);
     return check_launch(c, "epf force (frozen mask)");
 }
 
@@ -920,7 +920,7 @@ extern "C" int pxb_epf_force_adjoint_d(pxb_ctx *c, const double *u_d, const doub
     a.ubar = ubar_d;
     a.dC = dC_d;
     if (dC_d) PXB_CUDA_TRY(cudaMemsetAsync(dC_d, 0, 3 * sizeof(double), c->stream));
-    launch_epf_adjoint(a, c->g.dim, e.precision == PXB_MIXED, epf_grid(c->g.n), c->stream);
+    launch_epf_adjoint(a, c->g.dim, e.precision == PXB_MIXED, epf_grid(c->g.n, c->g.dim, 0), c->stream);
     return check_launch(c, "epf adjoint");
 }
 

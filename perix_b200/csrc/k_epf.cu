@@ -13,6 +13,8 @@
 //            (reflection, Neumann copy) or from constants (direct pins) are written by this node's warp,
 //            reproducing the reference's sequential BC application (compiled on the host);
 //   guard    the per-step max |u^{n+1}| (NaN-propagating) for the reference blow-up test.
+#include <type_traits>
+
 #include "k_kernels.h"
 #include "pxb_common.cuh"
 
@@ -79,93 +81,135 @@ __device__ __forceinline__ double pick(const double *v, int d) {
 
 }  // namespace
 
-template <int DIM, bool MIXED, int MODE>
+// Schedule: LPN lanes per node (GPW = 32/LPN nodes per warp in flight) and UNR bonds per lane per pass.
+// Every per-bond stream (health byte, neighbour id, operator values) of the UNR bonds is loaded before any
+// branch, then the neighbour gathers of all UNR bonds are issued together, so a node costs about one DRAM
+// round trip plus one (mostly L2-resident) gather round trip, and GPW*UNR*LPN bonds per warp are in flight.
+template <int DIM, bool MIXED, int MODE, int LPN, int UNR>
 __global__ void __launch_bounds__(kEpfThreads) epf_kernel(EpfArgs a) {
     using PosT = typename Vec<DIM>::T;
+    using GT = typename std::conditional<MIXED, float, double>::type;
+    constexpr int NC = (DIM == 3) ? 6 : 3;
     constexpr int WPB = kEpfThreads / kWarp;
+    constexpr int GPW = kWarp / LPN;
     __shared__ unsigned long long s_umax[WPB];
     __shared__ unsigned long long s_broken[WPB];
 
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
+    const int gl = lane & (LPN - 1);   // lane within the node group
+    const int grp = lane / LPN;        // node group within the warp
     const PosT *pos = static_cast<const PosT *>(a.pos);
+    const GT *G = static_cast<const GT *>(a.G);
     double t_new = 0.0;
     if constexpr (MODE == EPF_STEP) t_new = a.t_sched[a.step_in_chunk];
 
     unsigned long long broken = 0;
     double umax = 0.0;
+    const long long stride = (long long)gridDim.x * WPB * GPW;
 
-    for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
-        const int b0 = a.off[i], b1 = a.off[i + 1];
-        const PosT xi = pos[i];
+    for (long long base = ((long long)blockIdx.x * WPB + wib) * GPW; base < a.n; base += stride) {
+        const int i = (int)(base + grp);
+        const bool act = i < a.n;
+        int b0 = 0, b1 = 0;
+        PosT xi{};
         double ui[DIM];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) ui[d] = a.u[(size_t)i * DIM + d];
+        for (int d = 0; d < DIM; ++d) ui[d] = 0.0;
+        if (act) {
+            b0 = __ldg(a.off + i);
+            b1 = __ldg(a.off + i + 1);
+            xi = pos[i];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) ui[d] = a.u[(size_t)i * DIM + d];
+        }
         double L[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) L[d] = 0.0;
 
-        for (int t = b0 + lane; t < b1; t += kWarp) {
-            if (a.health[t] == 0) continue;
-            const int j = __ldg(a.nbr + t);
-            const PosT xj = pos[j];
-            double e[DIM];
+        for (int t0 = b0; t0 < b1; t0 += LPN * UNR) {
+            uint8_t h[UNR];
+            int j[UNR];
+            GT g[UNR][NC];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) e[d] = __dsub_rn(a.u[(size_t)j * DIM + d], ui[d]);
-            if constexpr (MODE != EPF_FORCE_FROZEN) {
-                if (a.damage) {
-                    double xv[DIM], yv[DIM];
-                    xv[0] = __dsub_rn(xj.x, xi.x);
-                    xv[1] = __dsub_rn(xj.y, xi.y);
-                    if constexpr (DIM == 3) xv[2] = __dsub_rn(xj.z, xi.z);
+            for (int q = 0; q < UNR; ++q) {
+                const int t = t0 + q * LPN + gl;
+                const bool ok = t < b1;
+                h[q] = ok ? a.health[t] : (uint8_t)0;
+                j[q] = ok ? __ldg(a.nbr + t) : i;
 #pragma unroll
-                    for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
-                    const double r2 = dot_rn<DIM>(xv, xv);
-                    if (r2 > 0.0) {
-                        const double y2 = dot_rn<DIM>(yv, yv);
-                        // fast squared test; the reference's own arithmetic decides bonds near the threshold
-                        const double band = 1.0e-6 * r2;
-                        const double qh = y2 - a.sc_hi2 * r2;
-                        bool brk;
-                        if (a.tension_only) {
-                            if (qh > band) brk = true;
-                            else if (qh < -band) brk = false;
-                            else brk = ref_stretch(y2, r2) > a.sc;
-                        } else {
-                            const double ql = a.sc_lo2 * r2 - y2;
-                            if (qh > band || ql > band) brk = true;
-                            else if (qh < -band && ql < -band) brk = false;
-                            else brk = fabs(ref_stretch(y2, r2)) > a.sc;
-                        }
-                        if (brk) {
-                            a.health[t] = 0;
-                            ++broken;
-                            continue;
+                for (int c = 0; c < NC; ++c) g[q][c] = ok ? __ldg(G + (size_t)c * a.nb + t) : GT(0);
+            }
+            PosT xj[UNR];
+            double uj[UNR][DIM];
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                xj[q] = pos[j[q]];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) uj[q][d] = a.u[(size_t)j[q] * DIM + d];
+            }
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                if (h[q] == 0) continue;
+                double e[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) e[d] = __dsub_rn(uj[q][d], ui[d]);
+                if constexpr (MODE != EPF_FORCE_FROZEN) {
+                    if (a.damage) {
+                        double xv[DIM], yv[DIM];
+                        xv[0] = __dsub_rn(xj[q].x, xi.x);
+                        xv[1] = __dsub_rn(xj[q].y, xi.y);
+                        if constexpr (DIM == 3) xv[2] = __dsub_rn(xj[q].z, xi.z);
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
+                        const double r2 = dot_rn<DIM>(xv, xv);
+                        if (r2 > 0.0) {
+                            const double y2 = dot_rn<DIM>(yv, yv);
+                            // fast squared test; the reference's own arithmetic decides bonds near threshold
+                            const double band = 1.0e-6 * r2;
+                            const double qh = y2 - a.sc_hi2 * r2;
+                            bool brk;
+                            if (a.tension_only) {
+                                if (qh > band) brk = true;
+                                else if (qh < -band) brk = false;
+                                else brk = ref_stretch(y2, r2) > a.sc;
+                            } else {
+                                const double ql = a.sc_lo2 * r2 - y2;
+                                if (qh > band || ql > band) brk = true;
+                                else if (qh < -band && ql < -band) brk = false;
+                                else brk = fabs(ref_stretch(y2, r2)) > a.sc;
+                            }
+                            if (brk) {
+                                a.health[t0 + q * LPN + gl] = 0;
+                                ++broken;
+                                continue;
+                            }
                         }
                     }
                 }
-            }
-            double g[(DIM == 3) ? 6 : 3];
-            load_G<DIM, MIXED>(a.G, a.nb, t, g);
-            double f[DIM];
-            navier_apply<DIM>(g, a.C11, a.C12, a.C66, e, f);
+                double gd[NC];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) L[d] += f[d];
+                for (int c = 0; c < NC; ++c) gd[c] = (double)g[q][c];
+                double f[DIM];
+                navier_apply<DIM>(gd, a.C11, a.C12, a.C66, e, f);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) L[d] += f[d];
+            }
         }
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) L[d] = group_sum<kWarp>(L[d]);
+        for (int d = 0; d < DIM; ++d) L[d] = group_sum<LPN>(L[d]);
 
-        // node update: lane d owns component d
+        // node update: lane d of the group owns component d
         double unew = 0.0;
-        if (lane < DIM) {
-            const int d = lane;
+        if (act && gl < DIM) {
+            const int d = gl;
             const double acc = __ddiv_rn(__dadd_rn(pick<DIM>(L, d), a.b[d]), a.rho);
             const size_t k = (size_t)i * DIM + d;
             if constexpr (MODE == EPF_RATE || MODE == EPF_FORCE_FROZEN) {
                 a.accel[k] = acc;
             } else if constexpr (MODE == EPF_START) {
                 const double v = a.v0 ? a.v0[k] : 0.0;
-                a.u_other[k] = __dadd_rn(__dsub_rn(ui[d], __dmul_rn(a.dt, v)), __dmul_rn(a.dt2, acc));
+                a.u_other[k] = __dadd_rn(__dsub_rn(pick<DIM>(ui, d), __dmul_rn(a.dt, v)), __dmul_rn(a.dt2, acc));
             } else {
                 const double uprev = a.u_other[k];
                 unew = __dadd_rn(__dsub_rn(__dmul_rn(2.0, pick<DIM>(ui, d)), uprev), __dmul_rn(a.dt2, acc));
@@ -178,30 +222,28 @@ __global__ void __launch_bounds__(kEpfThreads) epf_kernel(EpfArgs a) {
         }
         if constexpr (MODE == EPF_STEP) {
             if (a.bc_off) {
-                const int e0 = a.bc_off[i], e1 = a.bc_off[i + 1];
-                if (e0 < e1) {
-                    double un[DIM];
+                double un[DIM];
 #pragma unroll
-                    for (int d = 0; d < DIM; ++d) un[d] = __shfl_sync(kFull, unew, d);
-                    for (int e = e0 + lane; e < e1; e += kWarp) {
-                        const int comp = a.bc_comp[e];
-                        const int form = a.bc_form[e];
-                        // g = value + velocity*t in the reference's order (DirichletBC.cpp:135-137)
-                        const double g1 = __dadd_rn(a.bc_val[e], __dmul_rn(a.bc_vel[e], t_new));
-                        double v;
-                        if (form == 0) {
-                            v = pick<DIM>(un, comp);
-                        } else if (form == 1) {
-                            v = g1;
-                        } else if (form == 2) {
-                            v = __dsub_rn(__dmul_rn(2.0, g1), pick<DIM>(un, comp));
-                        } else {
-                            const double g2 = __dadd_rn(a.bc_val2[e], __dmul_rn(a.bc_vel2[e], t_new));
-                            v = __dsub_rn(__dmul_rn(2.0, g1), g2);
-                        }
-                        a.u_other[(size_t)a.bc_tgt[e] * DIM + comp] = v;
-                        umax = fmax(umax, fabs(v));
+                for (int d = 0; d < DIM; ++d) un[d] = __shfl_sync(kFull, unew, grp * LPN + d);
+                const int e0 = act ? a.bc_off[i] : 0, e1 = act ? a.bc_off[i + 1] : 0;
+                for (int e = e0 + gl; e < e1; e += LPN) {
+                    const int comp = a.bc_comp[e];
+                    const int form = a.bc_form[e];
+                    // g = value + velocity*t in the reference's order (DirichletBC.cpp:135-137)
+                    const double g1 = __dadd_rn(a.bc_val[e], __dmul_rn(a.bc_vel[e], t_new));
+                    double v;
+                    if (form == 0) {
+                        v = pick<DIM>(un, comp);
+                    } else if (form == 1) {
+                        v = g1;
+                    } else if (form == 2) {
+                        v = __dsub_rn(__dmul_rn(2.0, g1), pick<DIM>(un, comp));
+                    } else {
+                        const double g2 = __dadd_rn(a.bc_val2[e], __dmul_rn(a.bc_vel2[e], t_new));
+                        v = __dsub_rn(__dmul_rn(2.0, g1), g2);
                     }
+                    a.u_other[(size_t)a.bc_tgt[e] * DIM + comp] = v;
+                    umax = fmax(umax, fabs(v));
                 }
             }
         }
@@ -314,24 +356,70 @@ cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int gri
     return cudaGetLastError();
 }
 
-template <int DIM, bool MIXED>
-static cudaError_t launch_dm(const EpfArgs &a, int mode, int grid, cudaStream_t s) {
-    switch (mode) {
-        case EPF_RATE: epf_kernel<DIM, MIXED, EPF_RATE><<<grid, kEpfThreads, 0, s>>>(a); break;
-        case EPF_START: epf_kernel<DIM, MIXED, EPF_START><<<grid, kEpfThreads, 0, s>>>(a); break;
-        case EPF_STEP: epf_kernel<DIM, MIXED, EPF_STEP><<<grid, kEpfThreads, 0, s>>>(a); break;
-        case EPF_FORCE_FROZEN: epf_kernel<DIM, MIXED, EPF_FORCE_FROZEN><<<grid, kEpfThreads, 0, s>>>(a); break;
-        default: return cudaErrorInvalidValue;
+// schedule variants (LPN lanes per node, UNR bonds per lane per pass); index = EpfArgs-independent id
+// persistent grid: every block resident (SM count x occupancy of this instantiation), capped by the work
+template <typename K>
+static int resident_grid(K kernel, int n, int nodes_per_block) {
+    static int cap = 0;  // one cache per kernel instantiation
+    if (cap == 0) {
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kEpfThreads, 0);
+        cap = sms * (per_sm > 0 ? per_sm : 1);
     }
+    const long long need = ((long long)n + nodes_per_block - 1) / nodes_per_block;
+    return (int)(need < cap ? (need > 0 ? need : 1) : cap);
+}
+
+template <int DIM, bool MIXED, int MODE, int LPN, int UNR>
+static cudaError_t launch_m(const EpfArgs &a, cudaStream_t s) {
+    auto k = epf_kernel<DIM, MIXED, MODE, LPN, UNR>;
+    const int grid = resident_grid(k, a.n, (kEpfThreads / kWarp) * (kWarp / LPN));
+    k<<<grid, kEpfThreads, 0, s>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int grid, cudaStream_t s) {
-    if (dim == 2) return mixed ? launch_dm<2, true>(a, mode, grid, s) : launch_dm<2, false>(a, mode, grid, s);
-    return mixed ? launch_dm<3, true>(a, mode, grid, s) : launch_dm<3, false>(a, mode, grid, s);
+template <int DIM, bool MIXED, int LPN, int UNR>
+static cudaError_t launch_v(const EpfArgs &a, int mode, cudaStream_t s) {
+    switch (mode) {
+        case EPF_RATE: return launch_m<DIM, MIXED, EPF_RATE, LPN, UNR>(a, s);
+        case EPF_START: return launch_m<DIM, MIXED, EPF_START, LPN, UNR>(a, s);
+        case EPF_STEP: return launch_m<DIM, MIXED, EPF_STEP, LPN, UNR>(a, s);
+        case EPF_FORCE_FROZEN: return launch_m<DIM, MIXED, EPF_FORCE_FROZEN, LPN, UNR>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
-int epf_grid(int n) {
+// 2D: families of ~12..30 bonds; 3D: ~40..122
+static constexpr int kLpn2[kEpfVariants] = {32, 16, 8};
+static constexpr int kLpn3[kEpfVariants] = {32, 32, 16};
+
+template <int DIM, bool MIXED>
+static cudaError_t launch_dm(const EpfArgs &a, int mode, int variant, cudaStream_t s) {
+    if constexpr (DIM == 2) {
+        switch (variant) {
+            case 0: return launch_v<2, MIXED, 32, 1>(a, mode, s);
+            case 1: return launch_v<2, MIXED, 16, 2>(a, mode, s);
+            default: return launch_v<2, MIXED, 8, 4>(a, mode, s);
+        }
+    } else {
+        switch (variant) {
+            case 0: return launch_v<3, MIXED, 32, 1>(a, mode, s);
+            case 1: return launch_v<3, MIXED, 32, 2>(a, mode, s);
+            default: return launch_v<3, MIXED, 16, 2>(a, mode, s);
+        }
+    }
+}
+
+cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s) {
+    if (dim == 2) return mixed ? launch_dm<2, true>(a, mode, variant, s) : launch_dm<2, false>(a, mode, variant, s);
+    return mixed ? launch_dm<3, true>(a, mode, variant, s) : launch_dm<3, false>(a, mode, variant, s);
+}
+
+int epf_lanes_per_node(int dim, int variant) { return dim == 3 ? kLpn3[variant] : kLpn2[variant]; }
+
+int epf_grid(int n, int dim, int variant) {
     static int sms = 0;
     if (sms == 0) {
         int dev = 0;
@@ -339,10 +427,11 @@ int epf_grid(int n) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (sms <= 0) sms = 148;
     }
-    const int wpb = kEpfThreads / kWarp;
-    const long long need = ((long long)n + wpb - 1) / wpb;
+    const int nodes_per_block = (kEpfThreads / kWarp) * (kWarp / epf_lanes_per_node(dim, variant));
+    const long long need = ((long long)n + nodes_per_block - 1) / nodes_per_block;
     const long long cap = (long long)sms * 8;
-    return (int)(need < cap ? need : cap) > 0 ? (int)(need < cap ? need : cap) : 1;
+    const long long g = need < cap ? need : cap;
+    return (int)(g > 0 ? g : 1);
 }
 
 }  // namespace pxb

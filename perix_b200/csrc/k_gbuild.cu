@@ -2,11 +2,12 @@
 // per-bond operator values (reference PDOperators::calcAMatrixCompute / calcOperatorsCompute,
 // src/PDOperators/CalcPDOperators.cpp:108-226 and 307-354).
 //
-// Schedule: one warp per node (families are contiguous in the CSR, so lanes read consecutive bonds).
+// Schedule: a group of LPN lanes per node, 32/LPN nodes per warp (families are contiguous in the CSR, so the
+// lanes of a group read consecutive bonds).
 //   pass 1  lanes accumulate the upper triangle of A = sum_j bw * m m^T over a lane-strided slice of the
-//           family; a butterfly reduction leaves the full A in every lane.
+//           family; a butterfly reduction within the group leaves the full A in every lane of the group.
 //   solve   every lane factors A = L D L^T redundantly in registers (nop <= 9 at order 2, so this is ~120
-//           FMAs) and solves for column k = lane of X = A^-1 diag(q!), followed by one step of iterative
+//           FMAs) and solves for column k = its group lane of X = A^-1 diag(q!), followed by one step of iterative
 //           refinement against A kept in shared memory and the reference's max-norm consistency test
 //           (src/MathUtils/MatrixXd.cpp:40-47).
 //   pass 2  X goes to shared memory; lanes evaluate op_k(i,j) = (sum_a X[a][k] eta^{q_a}) * bw / delta^|q_k|
@@ -22,19 +23,23 @@
 
 namespace pxb {
 
-template <int DIM, int ORDER, bool MIXED>
+// LPN lanes per node (a power of two >= nop): GPW = 32/LPN nodes per warp are built concurrently.
+template <int DIM, int ORDER, bool MIXED, int LPN>
 __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
     constexpr QTable<DIM, ORDER> Q{};
     constexpr int NOP = Q.NOP;
     constexpr int NE = NOP * (NOP + 1) / 2;
-    constexpr int WPB = kGbuildThreads / kWarp;
+    constexpr int GPW = kWarp / LPN;
+    constexpr int GPB = (kGbuildThreads / kWarp) * GPW;  // node groups per block
+    static_assert(LPN >= NOP, "one lane per solve column");
     using PosT = typename Vec<DIM>::T;
 
-    __shared__ double sA[WPB][NOP * NOP];
-    __shared__ double sX[WPB][NOP * NOP];
+    __shared__ double sA[GPB][NOP * NOP];
+    __shared__ double sX[GPB][NOP * NOP];
 
     const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
+    const int gl = lane & (LPN - 1);
+    const int wib = (threadIdx.x >> 5) * GPW + lane / LPN;  // node group index within the block
     const PosT *pos = static_cast<const PosT *>(a.pos);
     const double inv_delta = 1.0 / a.delta;
 
@@ -47,9 +52,12 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
         idpow[k] = v;
     }
 
-    for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
-        const int b0 = a.off[i], b1 = a.off[i + 1];
-        const PosT xi = pos[i];
+    const long long stride = (long long)gridDim.x * GPB;
+    for (long long base = (long long)blockIdx.x * GPB + (threadIdx.x >> 5) * GPW; base < a.n + 0LL; base += stride) {
+        const int i = (int)(base + lane / LPN);
+        const bool act = i < a.n;
+        const int b0 = act ? a.off[i] : 0, b1 = act ? a.off[i + 1] : 0;
+        const PosT xi = act ? pos[i] : PosT{};
 
         // ---- pass 1: moment sums ----
         double acc[NE];
@@ -57,7 +65,7 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
 #pragma unroll
         for (int e = 0; e < NE; ++e) acc[e] = 0.0;
         int usable = 0;
-        for (int t = b0 + lane; t < b1; t += kWarp) {
+        for (int t = b0 + gl; t < b1; t += LPN) {
             const int j = a.nbr[t];
             const PosT xj = pos[j];
             const double dx = xj.x - xi.x, dy = xj.y - xi.y;
@@ -100,11 +108,11 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
             for (int e = 0; e < NE; ++e) acc[e] = cacc[e].value();
         }
 #pragma unroll
-        for (int e = 0; e < NE; ++e) acc[e] = group_sum<kWarp>(acc[e]);
-        usable = group_sum_int<kWarp>(usable);
+        for (int e = 0; e < NE; ++e) acc[e] = group_sum<LPN>(acc[e]);
+        usable = group_sum_int<LPN>(usable);
 
         // keep A (full, row-major) in shared memory for the refinement residual and the consistency test
-        if (lane == 0) {
+        if (gl == 0) {
             int e = 0;
 #pragma unroll
             for (int p = 0; p < NOP; ++p)
@@ -135,7 +143,7 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
                 acc[U(j, i2)] = s * invd;  // L[i2][j] stored at packed (j, i2)
             }
         }
-        const int kcol = (lane < NOP) ? lane : 0;
+        const int kcol = (gl < NOP) ? gl : 0;
         double fk = 0.0;
 #pragma unroll
         for (int q = 0; q < NOP; ++q)
@@ -184,18 +192,18 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
             res = fmax(res, fabs(s));
             maxX = fmax(maxX, fabs(x[p]));
         }
-        if (lane >= NOP) { res = 0.0; maxX = 0.0; }
-        res = group_max<kWarp>(res);
-        maxX = group_max<kWarp>(maxX);
+        if (gl >= NOP) { res = 0.0; maxX = 0.0; }
+        res = group_max<LPN>(res);
+        maxX = group_max<LPN>(maxX);
         double maxB = 0.0;
 #pragma unroll
         for (int q = 0; q < NOP; ++q) maxB = fmax(maxB, Q.fact[q]);
         const double scale = fmax(fmax(maxB, maxA * maxX), DBL_MIN);
         const bool consistent = (res <= 1.0e-8 * scale);  // NaN-safe: NaN fails
         const bool degenerate = (usable < NOP) || !consistent;
-        const bool deep_ghost = (a.layer != nullptr) && (a.layer[i] > 1);
+        const bool deep_ghost = act && (a.layer != nullptr) && (a.layer[i] > 1);
         const bool zero_ops = degenerate;
-        if (lane == 0) {
+        if (act && gl == 0) {
             if (a.degenerate) a.degenerate[i] = degenerate ? 1 : 0;
             if (degenerate && !deep_ghost) {
                 atomicAdd(a.n_degenerate, 1u);
@@ -203,14 +211,14 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
             }
         }
         // X (column kcol in lane kcol) to shared memory: sX[a][k]
-        if (lane < NOP) {
+        if (gl < NOP) {
 #pragma unroll
-            for (int p = 0; p < NOP; ++p) sX[wib][p * NOP + lane] = zero_ops ? 0.0 : x[p];
+            for (int p = 0; p < NOP; ++p) sX[wib][p * NOP + gl] = zero_ops ? 0.0 : x[p];
         }
         __syncwarp();
 
         // ---- pass 2: per-bond operators ----
-        for (int t = b0 + lane; t < b1; t += kWarp) {
+        for (int t = b0 + gl; t < b1; t += LPN) {
             const int j = a.nbr[t];
             const PosT xj = pos[j];
             const double dx = xj.x - xi.x, dy = xj.y - xi.y;
@@ -261,25 +269,30 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
     }
 }
 
-template <int DIM, int ORDER>
+template <int DIM, int ORDER, int LPN>
 static cudaError_t launch_order(const GBuildArgs &a, bool mixed, int grid, cudaStream_t s) {
-    if (mixed) gbuild_kernel<DIM, ORDER, true><<<grid, kGbuildThreads, 0, s>>>(a);
-    else gbuild_kernel<DIM, ORDER, false><<<grid, kGbuildThreads, 0, s>>>(a);
+    constexpr int GPB = (kGbuildThreads / kWarp) * (kWarp / LPN);
+    const long long need = ((long long)a.n + GPB - 1) / GPB;
+    const int g = (int)(need < grid ? (need > 0 ? need : 1) : grid);
+    if (mixed) gbuild_kernel<DIM, ORDER, true, LPN><<<g, kGbuildThreads, 0, s>>>(a);
+    else gbuild_kernel<DIM, ORDER, false, LPN><<<g, kGbuildThreads, 0, s>>>(a);
     return cudaGetLastError();
 }
 
+// lanes per node: 8 for 2D order <= 2 (families of ~12-30 bonds: ~4 bonds per lane, 4 nodes per warp), 16 when
+// nop > 8, 32 for 3D order 2 (families of ~40-122 bonds)
 cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, int grid, cudaStream_t s) {
     if (dim == 2) {
         switch (order) {
-            case 1: return launch_order<2, 1>(a, mixed, grid, s);
-            case 2: return launch_order<2, 2>(a, mixed, grid, s);
-            case 3: return launch_order<2, 3>(a, mixed, grid, s);
+            case 1: return launch_order<2, 1, 8>(a, mixed, grid, s);
+            case 2: return launch_order<2, 2, 8>(a, mixed, grid, s);
+            case 3: return launch_order<2, 3, 16>(a, mixed, grid, s);
             default: return cudaErrorInvalidValue;
         }
     }
     switch (order) {
-        case 1: return launch_order<3, 1>(a, mixed, grid, s);
-        case 2: return launch_order<3, 2>(a, mixed, grid, s);
+        case 1: return launch_order<3, 1, 8>(a, mixed, grid, s);
+        case 2: return launch_order<3, 2, 32>(a, mixed, grid, s);
         default: return cudaErrorInvalidValue;
     }
 }

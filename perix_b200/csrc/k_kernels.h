@@ -64,8 +64,11 @@ struct EpfArgs {
     unsigned long long *umax = nullptr;     // per-step max|u| keys
     unsigned long long *n_broken = nullptr; // broken-bond counter
 };
-cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int grid, cudaStream_t s);
-int epf_grid(int n);
+// schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
+constexpr int kEpfVariants = 3;
+cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s);
+int epf_grid(int n, int dim, int variant);
+int epf_lanes_per_node(int dim, int variant);
 
 struct EpfAdjArgs {
     int n = 0;

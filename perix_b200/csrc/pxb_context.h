@@ -95,11 +95,12 @@ struct BcDevice {
 };
 
 struct GraphKey {
-    int steps, parity, prec;
+    int steps, parity, prec, variant;
     bool operator<(const GraphKey &o) const {
         if (steps != o.steps) return steps < o.steps;
         if (parity != o.parity) return parity < o.parity;
-        return prec < o.prec;
+        if (prec != o.prec) return prec < o.prec;
+        return variant < o.variant;
     }
 };
 
@@ -124,6 +125,7 @@ struct EpfState {
     bool has_bc = false;
     std::map<GraphKey, cudaGraphExec_t> graphs;
     int graph_chunk = 0;
+    int variant = 1;   // schedule variant of the explicit kernel (set by the autotuner or pxb_epf_set_variant)
 };
 
 struct CsrState {
