@@ -160,6 +160,8 @@ extern "C" int pxb_epf_restore(pxb_ctx *c) {
 extern "C" int pxb_epf_set_variant(pxb_ctx *c, int variant) {
     if (!c || !c->epf.ready) return fail(PXB_ERR_STATE, "pxb_epf_set_variant: call pxb_epf_setup first");
     if (variant < 0 || variant >= kEpfVariants) return fail(PXB_ERR_INVALID, "pxb_epf_set_variant: no such variant");
+    if (!epf_variant_fits(c->g.dim, variant, c->g.max_family))
+        return fail(PXB_ERR_UNSUPPORTED, "pxb_epf_set_variant: families too large for this tile size");
     c->epf.variant = variant;
     return PXB_OK;
 }
@@ -190,6 +192,10 @@ extern "C" int pxb_epf_autotune(pxb_ctx *c, int steps, size_t flush_bytes, int u
     float best_ms = 1e30f;
     int best_v = c->epf.variant;
     for (int v = 0; v < kEpfVariants; ++v) {
+        if (!epf_variant_fits(c->g.dim, v, c->g.max_family)) {
+            if (ms_per_variant) ms_per_variant[v] = -1.f;
+            continue;
+        }
         c->epf.variant = v;
         PXB_TRY(load_state(c, keep));
         PXB_TRY(timed_steps(c, steps, flush_bytes, 0, nullptr, ms.data()));

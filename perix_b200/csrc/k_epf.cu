@@ -272,6 +272,200 @@ __global__ void __launch_bounds__(kEpfThreads) epf_kernel(EpfArgs a) {
     }
 }
 
+// ---- CSR-stream schedule ---------------------------------------------------------------------------------
+// A block takes a tile of NB consecutive nodes; their families form one contiguous bond range, which all
+// threads stream flat (bond t -> thread t mod blockDim), UNR bonds per thread per pass with every per-bond load
+// issued before any branch.  A shared-memory map gives each bond its tile-local node; partial forces go to
+// shared-memory FP64 accumulators.  A short node phase then does the update and the BC pass.  Every bond is
+// independent, so registers stay low and many bonds are in flight per SM.
+constexpr int kStreamMap = 4096;   // max bonds per tile (host checks NB * max family <= this)
+
+template <int DIM, bool MIXED, int MODE, int NB, int UNR>
+__global__ void __launch_bounds__(kEpfThreads) epf_stream_kernel(EpfArgs a) {
+    using PosT = typename Vec<DIM>::T;
+    using GT = typename std::conditional<MIXED, float, double>::type;
+    constexpr int NC = (DIM == 3) ? 6 : 3;
+    constexpr int WPB = kEpfThreads / kWarp;
+    __shared__ int s_off[NB + 1];
+    __shared__ PosT s_x[NB];
+    __shared__ double s_u[NB][DIM];
+    __shared__ double s_L[NB][DIM];
+    __shared__ double s_un[NB][DIM];
+    __shared__ unsigned char s_node[kStreamMap];
+    __shared__ unsigned long long s_umax[WPB];
+    __shared__ unsigned long long s_broken[WPB];
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int wib = tid >> 5;
+    const PosT *pos = static_cast<const PosT *>(a.pos);
+    const GT *G = static_cast<const GT *>(a.G);
+    double t_new = 0.0;
+    if constexpr (MODE == EPF_STEP) t_new = a.t_sched[a.step_in_chunk];
+    unsigned long long broken = 0;
+    double umax = 0.0;
+    const int ntiles = (a.n + NB - 1) / NB;
+
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int n0 = tile * NB;
+        const int cnt = min(NB, a.n - n0);
+        // ---- phase A: node data of the tile ----
+        if (tid <= cnt) s_off[tid] = __ldg(a.off + n0 + tid);
+        if (tid < cnt) {
+            s_x[tid] = pos[n0 + tid];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                s_u[tid][d] = a.u[(size_t)(n0 + tid) * DIM + d];
+                s_L[tid][d] = 0.0;
+            }
+        }
+        __syncthreads();
+        const int tb = s_off[0], te = s_off[cnt];
+        // bond -> tile-local node map (warp per node, lanes over its bonds)
+        for (int k = wib; k < cnt; k += WPB)
+            for (int t = s_off[k] + lane; t < s_off[k + 1]; t += kWarp) s_node[t - tb] = (unsigned char)k;
+        __syncthreads();
+        // ---- phase B: the tile's bonds, flat ----
+        for (int t0 = tb + tid; t0 < te; t0 += kEpfThreads * UNR) {
+            uint8_t h[UNR];
+            int j[UNR];
+            GT g[UNR][NC];
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                const int t = t0 + q * kEpfThreads;
+                const bool ok = t < te;
+                h[q] = ok ? a.health[t] : (uint8_t)0;
+                j[q] = ok ? __ldg(a.nbr + t) : n0;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) g[q][c] = ok ? __ldg(G + (size_t)c * a.nb + t) : GT(0);
+            }
+            PosT xj[UNR];
+            double uj[UNR][DIM];
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                xj[q] = pos[j[q]];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) uj[q][d] = a.u[(size_t)j[q] * DIM + d];
+            }
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                if (h[q] == 0) continue;
+                const int t = t0 + q * kEpfThreads;
+                const int k = s_node[t - tb];
+                const PosT xi = s_x[k];
+                double e[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) e[d] = __dsub_rn(uj[q][d], s_u[k][d]);
+                if constexpr (MODE != EPF_FORCE_FROZEN) {
+                    if (a.damage) {
+                        double xv[DIM], yv[DIM];
+                        xv[0] = __dsub_rn(xj[q].x, xi.x);
+                        xv[1] = __dsub_rn(xj[q].y, xi.y);
+                        if constexpr (DIM == 3) xv[2] = __dsub_rn(xj[q].z, xi.z);
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
+                        const double r2 = dot_rn<DIM>(xv, xv);
+                        if (r2 > 0.0) {
+                            const double y2 = dot_rn<DIM>(yv, yv);
+                            const double band = 1.0e-6 * r2;
+                            const double qh = y2 - a.sc_hi2 * r2;
+                            bool brk;
+                            if (a.tension_only) {
+                                if (qh > band) brk = true;
+                                else if (qh < -band) brk = false;
+                                else brk = ref_stretch(y2, r2) > a.sc;
+                            } else {
+                                const double ql = a.sc_lo2 * r2 - y2;
+                                if (qh > band || ql > band) brk = true;
+                                else if (qh < -band && ql < -band) brk = false;
+                                else brk = fabs(ref_stretch(y2, r2)) > a.sc;
+                            }
+                            if (brk) {
+                                a.health[t] = 0;
+                                ++broken;
+                                continue;
+                            }
+                        }
+                    }
+                }
+                double gd[NC];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) gd[c] = (double)g[q][c];
+                double f[DIM];
+                navier_apply<DIM>(gd, a.C11, a.C12, a.C66, e, f);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) atomicAdd(&s_L[k][d], f[d]);
+            }
+        }
+        __syncthreads();
+        // ---- phase C: node update, one thread per (node, component) ----
+        if (tid < cnt * DIM) {
+            const int k = tid / DIM, d = tid - k * DIM;
+            const int i = n0 + k;
+            const double acc = __ddiv_rn(__dadd_rn(s_L[k][d], a.b[d]), a.rho);
+            const size_t idx = (size_t)i * DIM + d;
+            if constexpr (MODE == EPF_RATE || MODE == EPF_FORCE_FROZEN) {
+                a.accel[idx] = acc;
+            } else if constexpr (MODE == EPF_START) {
+                const double v = a.v0 ? a.v0[idx] : 0.0;
+                a.u_other[idx] = __dadd_rn(__dsub_rn(s_u[k][d], __dmul_rn(a.dt, v)), __dmul_rn(a.dt2, acc));
+            } else {
+                const double uprev = a.u_other[idx];
+                const double unew = __dadd_rn(__dsub_rn(__dmul_rn(2.0, s_u[k][d]), uprev), __dmul_rn(a.dt2, acc));
+                s_un[k][d] = unew;
+                const bool owned = a.bc_own && ((a.bc_own[i] >> d) & 1);
+                if (!owned) {
+                    a.u_other[idx] = unew;
+                    umax = fmax(umax, fabs(unew));
+                }
+            }
+        }
+        if constexpr (MODE == EPF_STEP) {
+            if (a.bc_off) {
+                __syncthreads();
+                // BC entries executed by the tile: thread per node walks its (few) entries
+                if (tid < cnt) {
+                    const int i = n0 + tid;
+                    for (int e = a.bc_off[i]; e < a.bc_off[i + 1]; ++e) {
+                        const int comp = a.bc_comp[e];
+                        const int form = a.bc_form[e];
+                        const double g1 = __dadd_rn(a.bc_val[e], __dmul_rn(a.bc_vel[e], t_new));
+                        double v;
+                        if (form == 0) v = s_un[tid][comp];
+                        else if (form == 1) v = g1;
+                        else if (form == 2) v = __dsub_rn(__dmul_rn(2.0, g1), s_un[tid][comp]);
+                        else v = __dsub_rn(__dmul_rn(2.0, g1), __dadd_rn(a.bc_val2[e], __dmul_rn(a.bc_vel2[e], t_new)));
+                        a.u_other[(size_t)a.bc_tgt[e] * DIM + comp] = v;
+                        umax = fmax(umax, fabs(v));
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    if constexpr (MODE == EPF_STEP) {
+        umax = group_max<kWarp>(umax);
+        if (lane == 0) s_umax[wib] = dbl_key(umax);
+    }
+    unsigned long long bsum = broken;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bsum += __shfl_xor_sync(kFull, bsum, o);
+    if (lane == 0) s_broken[wib] = bsum;
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long bb = 0, mm = 0;
+        for (int w = 0; w < WPB; ++w) {
+            bb += s_broken[w];
+            if constexpr (MODE == EPF_STEP) mm = s_umax[w] > mm ? s_umax[w] : mm;
+        }
+        if (bb && a.n_broken) atomicAdd(a.n_broken, bb);
+        if constexpr (MODE == EPF_STEP) {
+            if (a.umax) atomicMax(a.umax + a.step_in_chunk, mm);
+        }
+    }
+}
+
 // ---- bond-force adjoint with a frozen damage mask ---------------------------------------------------------
 // Forward: a_i = (L_i + b)/rho, L_i = sum_t h_t P_t (u_j - u_i) with P_t symmetric.  For abar = dJ/da,
 // Lbar = abar/rho and
@@ -380,6 +574,25 @@ static cudaError_t launch_m(const EpfArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int DIM, bool MIXED, int MODE, int NB, int UNR>
+static cudaError_t launch_s(const EpfArgs &a, cudaStream_t s) {
+    auto k = epf_stream_kernel<DIM, MIXED, MODE, NB, UNR>;
+    const int grid = resident_grid(k, a.n, NB);
+    k<<<grid, kEpfThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int DIM, bool MIXED, int NB, int UNR>
+static cudaError_t launch_sv(const EpfArgs &a, int mode, cudaStream_t s) {
+    switch (mode) {
+        case EPF_RATE: return launch_s<DIM, MIXED, EPF_RATE, NB, UNR>(a, s);
+        case EPF_START: return launch_s<DIM, MIXED, EPF_START, NB, UNR>(a, s);
+        case EPF_STEP: return launch_s<DIM, MIXED, EPF_STEP, NB, UNR>(a, s);
+        case EPF_FORCE_FROZEN: return launch_s<DIM, MIXED, EPF_FORCE_FROZEN, NB, UNR>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 template <int DIM, bool MIXED, int LPN, int UNR>
 static cudaError_t launch_v(const EpfArgs &a, int mode, cudaStream_t s) {
     switch (mode) {
@@ -391,9 +604,12 @@ static cudaError_t launch_v(const EpfArgs &a, int mode, cudaStream_t s) {
     }
 }
 
-// 2D: families of ~12..30 bonds; 3D: ~40..122
-static constexpr int kLpn2[kEpfVariants] = {32, 16, 8};
-static constexpr int kLpn3[kEpfVariants] = {32, 32, 16};
+// 2D: families of ~12..30 bonds; 3D: ~40..122.  Variants 3/4 are the CSR-stream schedule (lanes per node
+// reported as 0; tile sizes in nodes below).
+static constexpr int kLpn2[kEpfVariants] = {32, 16, 8, 0, 0};
+static constexpr int kLpn3[kEpfVariants] = {32, 32, 16, 0, 0};
+static constexpr int kTile2[kEpfVariants] = {0, 0, 0, 64, 128};
+static constexpr int kTile3[kEpfVariants] = {0, 0, 0, 16, 32};
 
 template <int DIM, bool MIXED>
 static cudaError_t launch_dm(const EpfArgs &a, int mode, int variant, cudaStream_t s) {
@@ -401,13 +617,17 @@ static cudaError_t launch_dm(const EpfArgs &a, int mode, int variant, cudaStream
         switch (variant) {
             case 0: return launch_v<2, MIXED, 32, 1>(a, mode, s);
             case 1: return launch_v<2, MIXED, 16, 2>(a, mode, s);
-            default: return launch_v<2, MIXED, 8, 4>(a, mode, s);
+            case 2: return launch_v<2, MIXED, 8, 4>(a, mode, s);
+            case 3: return launch_sv<2, MIXED, 64, 2>(a, mode, s);
+            default: return launch_sv<2, MIXED, 128, 2>(a, mode, s);
         }
     } else {
         switch (variant) {
             case 0: return launch_v<3, MIXED, 32, 1>(a, mode, s);
             case 1: return launch_v<3, MIXED, 32, 2>(a, mode, s);
-            default: return launch_v<3, MIXED, 16, 2>(a, mode, s);
+            case 2: return launch_v<3, MIXED, 16, 2>(a, mode, s);
+            case 3: return launch_sv<3, MIXED, 16, 2>(a, mode, s);
+            default: return launch_sv<3, MIXED, 32, 2>(a, mode, s);
         }
     }
 }
@@ -419,6 +639,13 @@ cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int vari
 
 int epf_lanes_per_node(int dim, int variant) { return dim == 3 ? kLpn3[variant] : kLpn2[variant]; }
 
+int epf_tile_nodes(int dim, int variant) { return dim == 3 ? kTile3[variant] : kTile2[variant]; }
+
+bool epf_variant_fits(int dim, int variant, int max_family) {
+    const int nb = epf_tile_nodes(dim, variant);
+    return nb == 0 || (long long)nb * max_family <= kStreamMap;
+}
+
 int epf_grid(int n, int dim, int variant) {
     static int sms = 0;
     if (sms == 0) {
@@ -427,7 +654,8 @@ int epf_grid(int n, int dim, int variant) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (sms <= 0) sms = 148;
     }
-    const int nodes_per_block = (kEpfThreads / kWarp) * (kWarp / epf_lanes_per_node(dim, variant));
+    const int lpn = epf_lanes_per_node(dim, variant);
+    const int nodes_per_block = lpn ? (kEpfThreads / kWarp) * (kWarp / lpn) : epf_tile_nodes(dim, variant);
     const long long need = ((long long)n + nodes_per_block - 1) / nodes_per_block;
     const long long cap = (long long)sms * 8;
     const long long g = need < cap ? need : cap;

@@ -17,6 +17,7 @@
 // delta-scaled bond vectors (the bond vector itself is formed in FP64); the factorisation, refinement and
 // g-evaluation stay in FP64; g is stored in FP32.
 #include <cfloat>
+#include <type_traits>
 
 #include "k_kernels.h"
 #include "pxb_common.cuh"
@@ -34,8 +35,9 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
     static_assert(LPN >= NOP, "one lane per solve column");
     using PosT = typename Vec<DIM>::T;
 
+    using ETs = typename std::conditional<MIXED, float, double>::type;
     __shared__ double sA[GPB][NOP * NOP];
-    __shared__ double sX[GPB][NOP * NOP];
+    __shared__ ETs sX[GPB][NOP * NOP];
 
     const int lane = threadIdx.x & 31;
     const int gl = lane & (LPN - 1);
@@ -65,7 +67,14 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
 #pragma unroll
         for (int e = 0; e < NE; ++e) acc[e] = 0.0;
         int usable = 0;
-        for (int t = b0 + gl; t < b1; t += LPN) {
+        // weights of this lane's first KC bonds, reused by pass 2 (0 marks a skipped bond)
+        constexpr int KC = 4;
+        using ET = typename std::conditional<MIXED, float, double>::type;
+        ET wcache[KC];
+#pragma unroll
+        for (int c = 0; c < KC; ++c) wcache[c] = ET(0);
+        int cidx = 0;
+        for (int t = b0 + gl; t < b1; t += LPN, ++cidx) {
             const int j = a.nbr[t];
             const PosT xj = pos[j];
             const double dx = xj.x - xi.x, dy = xj.y - xi.y;
@@ -82,6 +91,9 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
                 const float bw = w * vc * (float)a.vol[j];
                 if (!(bw > 0.f)) continue;
                 ++usable;
+#pragma unroll
+                for (int c = 0; c < KC; ++c)
+                    if (c == cidx) wcache[c] = bw;
                 float m[NOP];
                 monomials<DIM, ORDER, float>((float)(dx * inv_delta), (float)(dy * inv_delta),
                                              (float)(dz * inv_delta), m);
@@ -94,6 +106,9 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
                 const double bw = bond_weight(xn, a.delta) * rim_correction(xn, a.delta, a.dx_char) * a.vol[j];
                 if (!(bw > 0.0)) continue;
                 ++usable;
+#pragma unroll
+                for (int c = 0; c < KC; ++c)
+                    if (c == cidx) wcache[c] = bw;
                 double m[NOP];
                 monomials<DIM, ORDER, double>(dx * inv_delta, dy * inv_delta, dz * inv_delta, m);
                 int e = 0;
@@ -167,31 +182,27 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
 #pragma unroll
         for (int q = 0; q < NOP; ++q) x[q] = (q == kcol) ? fk : 0.0;
         ldl_solve(x);
-        // one step of iterative refinement: x += A^-1 (b - A x)
+        // consistency test of the direct solution (MatrixXd.cpp:40-47):
+        //   max|A X - B| <= 1e-8 * max(max|B|, max|A| max|X|)
+        // its residual r = b - A x then drives one step of iterative refinement: x += A^-1 r
         double r[NOP];
+        double res = 0.0, maxA = 0.0, maxX = 0.0;
 #pragma unroll
         for (int p = 0; p < NOP; ++p) {
-            double s = (p == kcol) ? fk : 0.0;
+            double sres = (p == kcol) ? fk : 0.0;
 #pragma unroll
-            for (int q = 0; q < NOP; ++q) s -= sA[wib][p * NOP + q] * x[q];
-            r[p] = s;
+            for (int q = 0; q < NOP; ++q) {
+                const double apq = sA[wib][p * NOP + q];
+                sres -= apq * x[q];
+                maxA = fmax(maxA, fabs(apq));
+            }
+            r[p] = sres;
+            res = fmax(res, fabs(sres));
+            maxX = fmax(maxX, fabs(x[p]));
         }
         ldl_solve(r);
 #pragma unroll
         for (int q = 0; q < NOP; ++q) x[q] += r[q];
-        // consistency test (MatrixXd.cpp:40-47): max|A X - B| <= 1e-8 * max(max|B|, max|A| max|X|)
-        double res = 0.0, maxA = 0.0, maxX = 0.0;
-#pragma unroll
-        for (int p = 0; p < NOP; ++p) {
-            double s = -((p == kcol) ? fk : 0.0);
-#pragma unroll
-            for (int q = 0; q < NOP; ++q) {
-                s += sA[wib][p * NOP + q] * x[q];
-                maxA = fmax(maxA, fabs(sA[wib][p * NOP + q]));
-            }
-            res = fmax(res, fabs(s));
-            maxX = fmax(maxX, fabs(x[p]));
-        }
         if (gl >= NOP) { res = 0.0; maxX = 0.0; }
         res = group_max<LPN>(res);
         maxX = group_max<LPN>(maxX);
@@ -210,32 +221,49 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
                 atomicMin(a.first_degenerate, i);
             }
         }
-        // X (column kcol in lane kcol) to shared memory: sX[a][k]
+        // X (column kcol in lane kcol) to shared memory: sX[a][k] (FP32 copy for the mixed evaluation)
         if (gl < NOP) {
 #pragma unroll
-            for (int p = 0; p < NOP; ++p) sX[wib][p * NOP + gl] = zero_ops ? 0.0 : x[p];
+            for (int p = 0; p < NOP; ++p) sX[wib][p * NOP + gl] = zero_ops ? ET(0) : (ET)x[p];
         }
         __syncwarp();
 
-        // ---- pass 2: per-bond operators ----
-        for (int t = b0 + gl; t < b1; t += LPN) {
+        // ---- pass 2: per-bond operators (FP64; FP32 in mixed mode, where g is stored in FP32) ----
+        cidx = 0;
+        for (int t = b0 + gl; t < b1; t += LPN, ++cidx) {
             const int j = a.nbr[t];
             const PosT xj = pos[j];
             const double dx = xj.x - xi.x, dy = xj.y - xi.y;
             double dz = 0.0;
             if constexpr (DIM == 3) dz = xj.z - xi.z;
-            const double xn = sqrt(dx * dx + dy * dy + dz * dz);
-            double bw = 0.0;
-            if (xn > 0.0) bw = bond_weight(xn, a.delta) * rim_correction(xn, a.delta, a.dx_char) * a.vol[j];
-            const bool live = (xn > 0.0) && (bw > 0.0);
-            double m[NOP];
-            monomials<DIM, ORDER, double>(dx * inv_delta, dy * inv_delta, dz * inv_delta, m);
+            ET bw = ET(0);
+            if (cidx < KC) {
+#pragma unroll
+                for (int c = 0; c < KC; ++c)
+                    if (c == cidx) bw = wcache[c];
+            } else {
+                const double xn = sqrt(dx * dx + dy * dy + dz * dz);
+                if (xn > 0.0) {
+                    if constexpr (MIXED) {
+                        const float rr = 2.0f * (float)(xn * inv_delta);
+                        float vc = 1.0f;
+                        if (a.dx_char > 0.0 && xn > a.delta - 0.5 * a.dx_char)
+                            vc = fminf(fmaxf((float)((a.delta - xn + 0.5 * a.dx_char) / a.dx_char), 0.f), 1.f);
+                        bw = expf(-rr * rr) * vc * (float)a.vol[j];
+                    } else {
+                        bw = bond_weight(xn, a.delta) * rim_correction(xn, a.delta, a.dx_char) * a.vol[j];
+                    }
+                }
+            }
+            const bool live = bw > ET(0);
+            ET m[NOP];
+            monomials<DIM, ORDER, ET>((ET)(dx * inv_delta), (ET)(dy * inv_delta), (ET)(dz * inv_delta), m);
             auto op = [&](int k) -> double {
                 if (!live) return 0.0;
-                double s = 0.0;
+                ET sum = ET(0);
 #pragma unroll
-                for (int p = 0; p < NOP; ++p) s += sX[wib][p * NOP + k] * m[p];
-                return s * bw * idpow[k];
+                for (int p = 0; p < NOP; ++p) sum += sX[wib][p * NOP + k] * m[p];
+                return (double)(sum * bw * (ET)idpow[k]);
             };
             if (a.ops) {
                 if constexpr (MIXED) {

@@ -65,10 +65,13 @@ struct EpfArgs {
     unsigned long long *n_broken = nullptr; // broken-bond counter
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
-constexpr int kEpfVariants = 3;
+constexpr int kEpfVariants = 5;
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s);
 int epf_grid(int n, int dim, int variant);
 int epf_lanes_per_node(int dim, int variant);
+int epf_tile_nodes(int dim, int variant);
+// the CSR-stream variants map at most 4096 bonds per tile
+bool epf_variant_fits(int dim, int variant, int max_family);
 
 struct EpfAdjArgs {
     int n = 0;
