@@ -35,9 +35,8 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
     static_assert(LPN >= NOP, "one lane per solve column");
     using PosT = typename Vec<DIM>::T;
 
-    using ETs = typename std::conditional<MIXED, float, double>::type;
     __shared__ double sA[GPB][NOP * NOP];
-    __shared__ ETs sX[GPB][NOP * NOP];
+    __shared__ double sX[GPB][NOP * NOP];
 
     const int lane = threadIdx.x & 31;
     const int gl = lane & (LPN - 1);
@@ -221,14 +220,15 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
                 atomicMin(a.first_degenerate, i);
             }
         }
-        // X (column kcol in lane kcol) to shared memory: sX[a][k] (FP32 copy for the mixed evaluation)
+        // X (column kcol in lane kcol) to shared memory: sX[a][k]
         if (gl < NOP) {
 #pragma unroll
-            for (int p = 0; p < NOP; ++p) sX[wib][p * NOP + gl] = zero_ops ? ET(0) : (ET)x[p];
+            for (int p = 0; p < NOP; ++p) sX[wib][p * NOP + gl] = zero_ops ? 0.0 : x[p];
         }
         __syncwarp();
 
-        // ---- pass 2: per-bond operators (FP64; FP32 in mixed mode, where g is stored in FP32) ----
+        // ---- pass 2: per-bond operators, evaluated in FP64 (mixed mode stores them in FP32; its weights are
+        //      the FP32 ones the moment sums used) ----
         cidx = 0;
         for (int t = b0 + gl; t < b1; t += LPN, ++cidx) {
             const int j = a.nbr[t];
@@ -256,14 +256,15 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
                 }
             }
             const bool live = bw > ET(0);
-            ET m[NOP];
-            monomials<DIM, ORDER, ET>((ET)(dx * inv_delta), (ET)(dy * inv_delta), (ET)(dz * inv_delta), m);
+            const double bwd = (double)bw;
+            double m[NOP];
+            monomials<DIM, ORDER, double>(dx * inv_delta, dy * inv_delta, dz * inv_delta, m);
             auto op = [&](int k) -> double {
                 if (!live) return 0.0;
-                ET sum = ET(0);
+                double sum = 0.0;
 #pragma unroll
                 for (int p = 0; p < NOP; ++p) sum += sX[wib][p * NOP + k] * m[p];
-                return (double)(sum * bw * (ET)idpow[k]);
+                return sum * bwd * idpow[k];
             };
             if (a.ops) {
                 if constexpr (MIXED) {
