@@ -102,6 +102,22 @@ int pxb_gbuild_info(pxb_ctx *ctx, int *nop, int *pqr);
 /* Copy the operator cache to host (always returned as double). */
 int pxb_get_ops(pxb_ctx *ctx, double *ops);
 
+/* g-build without any device allocation.  No counterpart in the reference: it serves callers that cannot
+ * call cudaMalloc (their device memory belongs to another allocator, or they cannot afford its implicit
+ * synchronisation).  Inputs and outputs are device memory owned by the caller: neigh_off_d (n+1),
+ * neigh_id0_d (nbtot, 0-BASED ids), coords3_d (3n, xyz), vols_d (n), ops_d (nbtot*nop, double, or float with
+ * PXB_MIXED), degenerate_d (n bytes, may be NULL); stream is a cudaStream_t (NULL = legacy default stream).
+ * Working memory is one fixed 4 MiB device array shared by all calls on a device, which limits n to
+ * pxb_gbuild_noalloc_max_nodes(dim) (262,128 nodes in 2D, 131,064 in 3D); larger n is rejected with
+ * PXB_ERR_INVALID.  The first call on a device resolves the array's address, so make it before any stream
+ * capture; calls that overlap on the GPU race on the shared array.  Synchronises the stream before returning
+ * (the degenerate counters are read back). */
+int pxb_gbuild_noalloc_d(int dim, int order, int precision, int n, long long nbtot, const int *neigh_off_d,
+                         const int *neigh_id0_d, const double *coords3_d, const double *vols_d, double delta,
+                         double dx_char, void *ops_d, uint8_t *degenerate_d, int *n_degenerate, int *first_degenerate,
+                         void *stream);
+int pxb_gbuild_noalloc_max_nodes(int dim);
+
 /* ---- family-sum derivative apply ---------------------------------------------------------------------------
  * out[i*nk + s] = sum_t g^{k_s}_it (u_j - u_i) for the nk operator slots in `slots` (0-based into the
  * multi-index table), for a scalar field u (N).  The adjoint maps ybar (N*nk) to ubar (N) (transpose). */

@@ -1,0 +1,109 @@
+// g-function build for callers that cannot allocate device memory.
+//
+// Some callers must not call cudaMalloc: an application whose device memory belongs to another allocator
+// (a framework's caching pool, or a solver that reserves the whole GPU up front and hands out slices), or a
+// time-stepping loop that cannot afford the implicit device synchronisation cudaMalloc/cudaFree may perform.
+// pxb_gbuild_noalloc_d serves them: the caller passes every input and output as device memory it already
+// owns, and the build's working memory (the packed node positions the kernel gathers from and the two
+// degenerate-family counters) lives in one file-scope __device__ array of fixed size, kNoallocScratchBytes
+// (4 MiB), which every GPU that loads this library holds until the process exits.  The first call on a
+// device looks up that array's device address (cudaGetSymbolAddress); make that first call before any stream
+// capture begins.  All calls share the one array, so calls that overlap on the GPU (different streams or
+// host threads at the same time) race on it and must be serialised by the caller.
+#include <climits>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "k_kernels.h"
+#include "pxb_context.h"
+
+namespace {
+
+constexpr size_t kNoallocScratchBytes = 4u << 20;  // 4 MiB per device
+constexpr size_t kCounterBytes = 256;              // n_degenerate (u32) and first_degenerate (i32), aligned
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+void *g_scratch_addr[kMaxDevices] = {};
+
+// Resolve the device address of the scratch array on the current device (once per device).  In host code
+// `g_noalloc_scratch` is only a host-side stand-in for the symbol, so a kernel must be given this address.
+int scratch_address(int device, void **out) {
+    if (device < 0 || device >= kMaxDevices) return pxb::fail(PXB_ERR_INVALID, "pxb_gbuild_noalloc_d: device index too large");
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_addr[device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return pxb::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_scratch_addr[device] = p;
+    }
+    *out = g_scratch_addr[device];
+    return PXB_OK;
+}
+
+}  // namespace
+
+extern "C" int pxb_gbuild_noalloc_max_nodes(int dim) {
+    const size_t per_node = dim == 3 ? 32 : 16;
+    return (int)((kNoallocScratchBytes - kCounterBytes) / per_node);
+}
+
+extern "C" int pxb_gbuild_noalloc_d(int dim, int order, int precision, int n, long long nbtot, const int *neigh_off_d,
+                                    const int *neigh_id0_d, const double *coords3_d, const double *vols_d, double delta,
+                                    double dx_char, void *ops_d, uint8_t *degenerate_d, int *n_degenerate,
+                                    int *first_degenerate, void *stream) {
+    using namespace pxb;
+    if ((dim != 2 && dim != 3) || n <= 0 || nbtot < 0 || !neigh_off_d || !neigh_id0_d || !coords3_d || !vols_d ||
+        !ops_d || !(delta > 0.0) || (precision != PXB_FP64 && precision != PXB_MIXED))
+        return fail(PXB_ERR_INVALID, "pxb_gbuild_noalloc_d: bad arguments");
+    if (!gbuild_supported(dim, order)) return fail(PXB_ERR_UNSUPPORTED, "pxb_gbuild_noalloc_d: order not built for this dimension");
+    if (n > pxb_gbuild_noalloc_max_nodes(dim))
+        return fail(PXB_ERR_INVALID, "pxb_gbuild_noalloc_d: " + std::to_string(n) + " nodes exceed the " +
+                                         std::to_string(pxb_gbuild_noalloc_max_nodes(dim)) + "-node limit of the " +
+                                         std::to_string(kNoallocScratchBytes >> 20) + " MiB scratch array (" +
+                                         std::to_string(dim) + "D)");
+    int device = 0;
+    PXB_CUDA_TRY(cudaGetDevice(&device));
+    void *base = nullptr;
+    PXB_TRY(scratch_address(device, &base));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char *scr = static_cast<unsigned char *>(base);
+    unsigned int *nd = reinterpret_cast<unsigned int *>(scr);
+    int *first = reinterpret_cast<int *>(scr + 8);
+    void *pos = scr + kCounterBytes;
+    // the array keeps the previous call's contents: reset the counters (first_degenerate to 0x7f7f7f7f, above
+    // any node index); the packed positions are fully rewritten below
+    PXB_CUDA_TRY(cudaMemsetAsync(nd, 0, sizeof(unsigned int), s));
+    PXB_CUDA_TRY(cudaMemsetAsync(first, 0x7f, sizeof(int), s));
+    PXB_CUDA_TRY(launch_pos_pack(n, dim, coords3_d, pos, s));
+    GBuildArgs a;
+    a.n = n;
+    a.nb = nbtot;
+    a.off = neigh_off_d;
+    a.nbr = neigh_id0_d;
+    a.pos = pos;
+    a.vol = vols_d;
+    a.delta = delta;
+    a.dx_char = dx_char;
+    a.ops = ops_d;
+    a.degenerate = degenerate_d;
+    a.n_degenerate = nd;
+    a.first_degenerate = first;
+    int sms = 148;
+    PXB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    PXB_CUDA_TRY(launch_gbuild(a, dim, order, precision == PXB_MIXED, sms * 16, s));
+    unsigned int hnd = 0;
+    int hfirst = 0;
+    PXB_CUDA_TRY(cudaMemcpyAsync(&hnd, nd, sizeof(hnd), cudaMemcpyDeviceToHost, s));
+    PXB_CUDA_TRY(cudaMemcpyAsync(&hfirst, first, sizeof(hfirst), cudaMemcpyDeviceToHost, s));
+    PXB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (n_degenerate) *n_degenerate = (int)hnd;
+    if (first_degenerate) *first_degenerate = hnd ? hfirst + 1 : 0;
+    if (hnd)
+        return fail(PXB_ERR_DEGENERATE, "degenerate moment matrix at node " + std::to_string(hfirst + 1) + " (" +
+                                            std::to_string(hnd) + " non-ghost node(s))");
+    return PXB_OK;
+}
