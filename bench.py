@@ -233,7 +233,7 @@ def autotune(ctx, steps=20):
     """pxb_epf_autotune: time each schedule variant on this plate from the snapshot state, keep the fastest."""
     import ctypes as C
     best = C.c_int(0)
-    ms = np.zeros(5, np.float32)
+    ms = np.zeros(7, np.float32)
     st = ctx.L.pxb_epf_autotune(ctx.h, steps, C.c_size_t(FLUSH_BYTES), 0, C.byref(best),
                                 ms.ctypes.data_as(C.POINTER(C.c_float)))
     if st:

@@ -394,6 +394,21 @@ class Context:
         _check(self.L.pxb_epf_broken_count(self.h, C.byref(v)))
         return v.value
 
+    def epf_set_variant(self, variant):
+        _check(self.L.pxb_epf_set_variant(self.h, int(variant)))
+
+    def epf_variant(self):
+        v, lpn = C.c_int(0), C.c_int(0)
+        _check(self.L.pxb_epf_get_variant(self.h, C.byref(v), C.byref(lpn)))
+        return v.value, lpn.value
+
+    def epf_autotune(self, steps=10, flush_bytes=256 << 20, use_cache=False):
+        best = C.c_int(0)
+        ms = np.zeros(16, np.float32)
+        _check(self.L.pxb_epf_autotune(self.h, int(steps), C.c_size_t(flush_bytes), int(bool(use_cache)),
+                                       C.byref(best), ms.ctypes.data_as(C.POINTER(C.c_float))))
+        return best.value, ms
+
     def epf_force_adjoint(self, u, abar):
         ub = np.zeros(self.n * self.dim, np.float64)
         dC = np.zeros(3, np.float64)

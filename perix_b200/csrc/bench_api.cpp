@@ -120,6 +120,9 @@ int timed_steps(pxb_ctx *c, int nsteps, size_t flush_bytes, int restore_every, c
         e.step++;
     }
     PXB_TRY(sync(c));
+    unsigned int werr = 0;
+    PXB_CUDA_TRY(cudaMemcpy(&werr, e.counters.as<unsigned long long>() + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost));
+    if (werr) return fail(PXB_ERR_CUDA, "explicit step: a staged-copy wait ran out");
     for (int s = 0; s < nsteps; ++s) PXB_CUDA_TRY(cudaEventElapsedTime(&ms[s], ev.ev[2 * (size_t)s], ev.ev[2 * (size_t)s + 1]));
     return PXB_OK;
 }

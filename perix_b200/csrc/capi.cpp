@@ -247,8 +247,12 @@ extern "C" int pxb_set_geometry(pxb_ctx *c, int n, int dim, const double *coords
     g.max_family = maxf;
     g.h_off.assign(neigh_off, neigh_off + n + 1);
     if (mirror) g.h_mirror.assign(mirror, mirror + n);
-    PXB_TRY(dev_upload(c, g.off, neigh_off, sizeof(int) * (size_t)(n + 1)));
-    PXB_TRY(dev_alloc(c, g.nbr, sizeof(int) * (size_t)std::max(1LL, nb)));
+    g.ldb = ((nb + 16 + 15) / 16) * 16;
+    PXB_TRY(dev_alloc(c, g.off, sizeof(int) * (size_t)(n + 1 + 16)));
+    PXB_CUDA_TRY(cudaMemsetAsync(g.off.p, 0, g.off.bytes, c->stream));
+    PXB_TRY(h2d(c, g.off.p, neigh_off, sizeof(int) * (size_t)(n + 1)));
+    PXB_TRY(dev_alloc(c, g.nbr, sizeof(int) * (size_t)g.ldb));
+    PXB_CUDA_TRY(cudaMemsetAsync(g.nbr.p, 0, g.nbr.bytes, c->stream));
     void *tmp = nullptr;
     PXB_TRY(scratch(c, std::max(sizeof(int) * (size_t)std::max(1LL, nb), sizeof(double) * 3 * (size_t)n), &tmp));
     PXB_TRY(h2d(c, tmp, neigh_id, sizeof(int) * (size_t)nb));
@@ -290,7 +294,6 @@ static GBuildArgs gbuild_args(pxb_ctx *c, void *ops_out, void *G_out, uint8_t *d
     Geometry &g = c->g;
     GBuildArgs a;
     a.n = g.n;
-    a.nb = g.nb;
     a.off = g.off.as<int>();
     a.nbr = g.nbr.as<int>();
     a.pos = g.pos.p;
@@ -298,6 +301,7 @@ static GBuildArgs gbuild_args(pxb_ctx *c, void *ops_out, void *G_out, uint8_t *d
     a.layer = g.layer.p ? g.layer.as<int>() : nullptr;
     a.delta = g.delta;
     a.dx_char = g.dx_char;
+    a.nb = g.ldb;  // SoA stride of the Navier operator streams
     a.ops = ops_out;
     a.G = G_out;
     a.degenerate = deg_out;
@@ -484,7 +488,7 @@ static EpfArgs epf_args(pxb_ctx *c) {
     const EpfState &e = c->epf;
     EpfArgs a;
     a.n = g.n;
-    a.nb = g.nb;
+    a.nb = g.ldb;  // SoA stride of the operator streams
     a.off = g.off.as<int>();
     a.nbr = g.nbr.as<int>();
     a.pos = g.pos.p;
@@ -501,6 +505,8 @@ static EpfArgs epf_args(pxb_ctx *c) {
     a.damage = e.sc > 0.0 ? 1 : 0;
     a.tension_only = e.tension_only;
     a.n_broken = e.counters.as<unsigned long long>();
+    a.err = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 2);
+    if (epf_is_tma(e.variant)) a.maxb = epf_tma_maxb(g.dim, e.variant, g.max_family);
     return a;
 }
 
@@ -523,11 +529,13 @@ extern "C" int pxb_epf_setup(pxb_ctx *c, int precision, double C11, double C12, 
     e.tension_only = tension_only ? 1 : 0;
     const int nc = g.dim == 3 ? 6 : 3;
     const size_t es = precision == PXB_MIXED ? 4 : 8;
-    const size_t nb1 = (size_t)std::max(1LL, g.nb);
-    PXB_TRY(dev_alloc(c, e.G, es * nc * nb1));
-    PXB_TRY(dev_alloc(c, e.health, nb1));
-    PXB_TRY(dev_alloc(c, e.u[0], sizeof(double) * (size_t)g.n * g.dim));
-    PXB_TRY(dev_alloc(c, e.u[1], sizeof(double) * (size_t)g.n * g.dim));
+    const size_t ldb = (size_t)g.ldb;
+    PXB_TRY(dev_alloc(c, e.G, es * nc * ldb));
+    PXB_CUDA_TRY(cudaMemsetAsync(e.G.p, 0, e.G.bytes, c->stream));
+    PXB_TRY(dev_alloc(c, e.health, ldb));
+    PXB_CUDA_TRY(cudaMemsetAsync(e.health.p, 0, e.health.bytes, c->stream));
+    PXB_TRY(dev_alloc(c, e.u[0], sizeof(double) * ((size_t)g.n * g.dim + 8)));
+    PXB_TRY(dev_alloc(c, e.u[1], sizeof(double) * ((size_t)g.n * g.dim + 8)));
     PXB_TRY(dev_alloc(c, e.accel, sizeof(double) * (size_t)g.n * g.dim));
     PXB_TRY(dev_alloc(c, e.counters, sizeof(unsigned long long) * 4));
     PXB_CUDA_TRY(cudaMemsetAsync(e.counters.p, 0, sizeof(unsigned long long) * 4, c->stream));
@@ -837,7 +845,10 @@ extern "C" int pxb_epf_advance(pxb_ctx *c, int nsteps, int chunk, int *bad_step)
         PXB_CUDA_TRY(cudaGraphLaunch(exec, c->stream));
         c->launches += s;
         PXB_TRY(d2h(c, keys.data(), e.umax.p, sizeof(unsigned long long) * (size_t)s));
+        unsigned int werr = 0;
+        PXB_TRY(d2h(c, &werr, e.counters.as<unsigned long long>() + 2, sizeof(unsigned int)));
         PXB_TRY(sync(c));
+        if (werr) return fail(PXB_ERR_CUDA, "explicit step: a staged-copy wait ran out (" + std::to_string(werr) + " blocks)");
         const int st = check_blowup(e, keys.data(), s, bad_step);
         e.cur ^= (s & 1);
         e.t = t;
@@ -905,7 +916,7 @@ extern "C" int pxb_epf_force_adjoint_d(pxb_ctx *c, const double *u_d, const doub
     const EpfState &e = c->epf;
     EpfAdjArgs a;
     a.n = c->g.n;
-    a.nb = c->g.nb;
+    a.nb = c->g.ldb;  // SoA stride of the operator streams
     a.off = c->g.off.as<int>();
     a.nbr = c->g.nbr.as<int>();
     a.rev = c->g.rev.as<int>();

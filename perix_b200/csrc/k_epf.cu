@@ -606,10 +606,10 @@ static cudaError_t launch_v(const EpfArgs &a, int mode, cudaStream_t s) {
 
 // 2D: families of ~12..30 bonds; 3D: ~40..122.  Variants 3/4 are the CSR-stream schedule (lanes per node
 // reported as 0; tile sizes in nodes below).
-static constexpr int kLpn2[kEpfVariants] = {32, 16, 8, 0, 0};
-static constexpr int kLpn3[kEpfVariants] = {32, 32, 16, 0, 0};
-static constexpr int kTile2[kEpfVariants] = {0, 0, 0, 64, 128};
-static constexpr int kTile3[kEpfVariants] = {0, 0, 0, 16, 32};
+static constexpr int kLpn2[kEpfVariants] = {32, 16, 8, 0, 0, 16, 8};
+static constexpr int kLpn3[kEpfVariants] = {32, 32, 16, 0, 0, 32, 32};
+static constexpr int kTile2[kEpfVariants] = {0, 0, 0, 64, 128, 0, 0};
+static constexpr int kTile3[kEpfVariants] = {0, 0, 0, 16, 32, 0, 0};
 
 template <int DIM, bool MIXED>
 static cudaError_t launch_dm(const EpfArgs &a, int mode, int variant, cudaStream_t s) {
@@ -632,7 +632,19 @@ static cudaError_t launch_dm(const EpfArgs &a, int mode, int variant, cudaStream
     }
 }
 
+bool epf_is_tma(int variant) { return variant >= 5; }
+
+int epf_tma_maxb(int dim, int variant, int max_family) {
+    const int nt = epf_tma_tile_nodes(dim, variant - 5);
+    const long long b = (long long)nt * max_family + 32;
+    return (int)((b + 31) / 32 * 32);
+}
+
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s) {
+    if (epf_is_tma(variant)) {
+        if (mode == EPF_STEP) return launch_epf_tma(a, dim, mixed, variant - 5, s);
+        variant = 1;  // the staged kernel implements the time step only; other modes use the lane-group kernel
+    }
     if (dim == 2) return mixed ? launch_dm<2, true>(a, mode, variant, s) : launch_dm<2, false>(a, mode, variant, s);
     return mixed ? launch_dm<3, true>(a, mode, variant, s) : launch_dm<3, false>(a, mode, variant, s);
 }
@@ -642,6 +654,10 @@ int epf_lanes_per_node(int dim, int variant) { return dim == 3 ? kLpn3[variant] 
 int epf_tile_nodes(int dim, int variant) { return dim == 3 ? kTile3[variant] : kTile2[variant]; }
 
 bool epf_variant_fits(int dim, int variant, int max_family) {
+    if (epf_is_tma(variant)) {
+        const int maxb = epf_tma_maxb(dim, variant, max_family);
+        return epf_tma_smem(dim, false, variant - 5, maxb) <= 227u * 1024u;
+    }
     const int nb = epf_tile_nodes(dim, variant);
     return nb == 0 || (long long)nb * max_family <= kStreamMap;
 }

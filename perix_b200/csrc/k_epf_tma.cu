@@ -1,0 +1,394 @@
+// explicit_pddo_frac step with the bond streams staged through shared memory by TMA bulk copies.
+//
+// Each block cycles through tiles of NT consecutive nodes (grid-stride).  A tile's families form one
+// contiguous bond range, so its per-bond streams (health byte, neighbour id, the c Navier operator streams)
+// and its per-node rows (offsets, positions, u^n, u^{n-1}) are each one contiguous span of global memory.
+// Thread 0 fetches them with cp.async.bulk 1D copies (16-byte aligned starts and sizes: the bond range is
+// widened to multiples of 16 bonds, the allocations carry the padding) into an S-stage ring, completing on a
+// per-stage mbarrier.  Consumers wait on the stage's mbarrier, so DRAM streaming for the next S-1 tiles runs
+// while the current tile computes; only the neighbour gathers (mostly L2 hits) remain ordinary loads.
+// The compute is the lanes-per-node schedule of k_epf.cu (LPN lanes per node, NT = 8 warps * 32/LPN nodes).
+//
+// Every wait is bounded: a thread that gives up sets a flag, the block leaves the tile loop together, thread 0
+// waits (bounded) for its copies still in flight, and the kernel records the failure in err[0].  No TMA
+// multicast is used.
+#include <type_traits>
+
+#include "k_kernels.h"
+#include "pxb_common.cuh"
+
+namespace pxb {
+
+namespace {
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+        "r"(bytes)
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait: false if the phase did not complete within the iteration budget
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+    for (int it = 0; it < (1 << 20); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ unsigned up16(unsigned b) { return (b + 15u) & ~15u; }
+
+__device__ __forceinline__ double ref_stretch_t(double y2, double r2) {
+    const double r = sqrt(r2);
+    return __ddiv_rn(__dsub_rn(sqrt(y2), r), r);
+}
+
+template <int DIM>
+__device__ __forceinline__ double dot_rn_t(const double *a, const double *b) {
+    double s = __dmul_rn(a[0], b[0]);
+    s = __dadd_rn(s, __dmul_rn(a[1], b[1]));
+    if constexpr (DIM == 3) s = __dadd_rn(s, __dmul_rn(a[2], b[2]));
+    return s;
+}
+
+template <int DIM>
+__device__ __forceinline__ void navier_apply_t(const double *g, double C11, double C12, double C66, const double *e,
+                                               double *out) {
+    if constexpr (DIM == 3) {
+        const double Gxx = g[0], Gyy = g[1], Gzz = g[2], Gxy = g[3], Gxz = g[4], Gyz = g[5];
+        const double p11 = C11 * Gxx + C66 * (Gyy + Gzz);
+        const double p22 = C11 * Gyy + C66 * (Gxx + Gzz);
+        const double p33 = C11 * Gzz + C66 * (Gxx + Gyy);
+        const double ac = C12 + C66;
+        const double p12 = ac * Gxy, p13 = ac * Gxz, p23 = ac * Gyz;
+        out[0] = p11 * e[0] + p12 * e[1] + p13 * e[2];
+        out[1] = p12 * e[0] + p22 * e[1] + p23 * e[2];
+        out[2] = p13 * e[0] + p23 * e[1] + p33 * e[2];
+    } else {
+        const double Gxx = g[0], Gyy = g[1], Gxy = g[2];
+        const double p11 = C11 * Gxx + C66 * Gyy;
+        const double p22 = C66 * Gxx + C11 * Gyy;
+        const double pxy = (C12 + C66) * Gxy;
+        out[0] = p11 * e[0] + pxy * e[1];
+        out[1] = pxy * e[0] + p22 * e[1];
+    }
+}
+
+template <int DIM>
+__device__ __forceinline__ double pick_t(const double *v, int d) {
+    double r = v[0];
+#pragma unroll
+    for (int k = 1; k < DIM; ++k)
+        if (d == k) r = v[k];
+    return r;
+}
+
+// stage layout (bytes, all sections 16-aligned): G[NC][maxb] | nbr[maxb] | health[maxb] | off[NT+16] |
+// pos[NT] | u[NT*DIM + 2] | uprev[NT*DIM + 2]
+template <int DIM, bool MIXED, int NT>
+struct StageLayout {
+    static constexpr int NC = (DIM == 3) ? 6 : 3;
+    static constexpr int ES = MIXED ? 4 : 8;
+    static constexpr int PS = (DIM == 3) ? 32 : 16;
+    __host__ __device__ static unsigned g_off(int) { return 0; }
+    __host__ __device__ static unsigned nbr_off(int maxb) { return (unsigned)(NC * maxb * ES); }
+    __host__ __device__ static unsigned h_off(int maxb) { return nbr_off(maxb) + (unsigned)maxb * 4u; }
+    __host__ __device__ static unsigned off_off(int maxb) { return h_off(maxb) + (unsigned)maxb; }
+    __host__ __device__ static unsigned pos_off(int maxb) { return off_off(maxb) + (unsigned)(NT + 16) * 4u; }
+    __host__ __device__ static unsigned u_off(int maxb) { return pos_off(maxb) + (unsigned)NT * PS; }
+    __host__ __device__ static unsigned up_off(int maxb) {
+        return u_off(maxb) + (((unsigned)(NT * DIM + 2) * 8u + 15u) & ~15u);
+    }
+    __host__ __device__ static unsigned bytes(int maxb) {
+        return up_off(maxb) + (((unsigned)(NT * DIM + 2) * 8u + 15u) & ~15u);
+    }
+};
+
+}  // namespace
+
+template <int DIM, bool MIXED, int LPN, int S>
+__global__ void __launch_bounds__(kEpfThreads) epf_tma_kernel(EpfArgs a) {
+    using PosT = typename Vec<DIM>::T;
+    using GT = typename std::conditional<MIXED, float, double>::type;
+    constexpr int WPB = kEpfThreads / kWarp;
+    constexpr int GPW = kWarp / LPN;
+    constexpr int NT = WPB * GPW;
+    using SL = StageLayout<DIM, MIXED, NT>;
+    constexpr int NC = SL::NC;
+
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ unsigned long long bar[S];
+    __shared__ int s_t0a[S];
+    __shared__ unsigned long long s_umax[WPB];
+    __shared__ unsigned long long s_broken[WPB];
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int wib = tid >> 5;
+    const int gl = lane & (LPN - 1);
+    const int grp = lane / LPN;
+    const int maxb = a.maxb;
+    const unsigned stage_bytes = SL::bytes(maxb);
+    const PosT *pos = static_cast<const PosT *>(a.pos);
+    const GT *Gg = static_cast<const GT *>(a.G);
+    const double t_new = a.t_sched[a.step_in_chunk];
+
+    const int ntiles = (a.n + NT - 1) / NT;
+    const int mycount = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    // thread 0: fetch tile number k (k-th of this block) into stage k % S
+    auto issue = [&](int k) {
+        const int st = k % S;
+        const int tile = (int)blockIdx.x + k * (int)gridDim.x;
+        const int n0 = tile * NT;
+        const int cnt = min(NT, a.n - n0);
+        const int t0 = __ldg(a.off + n0), t1 = __ldg(a.off + n0 + cnt);
+        const int t0a = t0 & ~15;
+        const unsigned nbond = up16((unsigned)(t1 - t0a));
+        unsigned char *base = smem + (size_t)st * stage_bytes;
+        const unsigned bytes_g = nbond * SL::ES, bytes_n = nbond * 4u, bytes_h = nbond;
+        const unsigned bytes_off = up16((unsigned)(cnt + 1) * 4u);
+        const unsigned bytes_pos = (unsigned)cnt * SL::PS;
+        const unsigned bytes_u = up16((unsigned)cnt * DIM * 8u);
+        const unsigned total = NC * bytes_g + bytes_n + bytes_h + bytes_off + bytes_pos + bytes_u * 2u;
+        s_t0a[st] = t0a;
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&bar[st], total);
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+            bulk_g2s(base + (size_t)c * maxb * SL::ES, Gg + (size_t)c * a.nb + t0a, bytes_g, &bar[st]);
+        bulk_g2s(base + SL::nbr_off(maxb), a.nbr + t0a, bytes_n, &bar[st]);
+        bulk_g2s(base + SL::h_off(maxb), a.health + t0a, bytes_h, &bar[st]);
+        bulk_g2s(base + SL::off_off(maxb), a.off + n0, bytes_off, &bar[st]);
+        bulk_g2s(base + SL::pos_off(maxb), pos + n0, bytes_pos, &bar[st]);
+        bulk_g2s(base + SL::u_off(maxb), a.u + (size_t)n0 * DIM, bytes_u, &bar[st]);
+        bulk_g2s(base + SL::up_off(maxb), a.u_other + (size_t)n0 * DIM, bytes_u, &bar[st]);
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int k = 0; k < S && k < mycount; ++k) issue(k);
+
+    unsigned long long broken = 0;
+    double umax = 0.0;
+    int failed_at = -1;
+
+    for (int k = 0; k < mycount; ++k) {
+        const int st = k % S;
+        const bool ok_wait = mbar_wait(&bar[st], (unsigned)((k / S) & 1));
+        if (__syncthreads_or(!ok_wait)) {
+            failed_at = k;
+            break;
+        }
+        unsigned char *base = smem + (size_t)st * stage_bytes;
+        const GT *sG = reinterpret_cast<const GT *>(base);
+        const int *sN = reinterpret_cast<const int *>(base + SL::nbr_off(maxb));
+        unsigned char *sH = base + SL::h_off(maxb);
+        const int *sOff = reinterpret_cast<const int *>(base + SL::off_off(maxb));
+        const PosT *sPos = reinterpret_cast<const PosT *>(base + SL::pos_off(maxb));
+        const double *sU = reinterpret_cast<const double *>(base + SL::u_off(maxb));
+        const double *sUp = reinterpret_cast<const double *>(base + SL::up_off(maxb));
+        const int t0a = s_t0a[st];
+
+        const int tile = (int)blockIdx.x + k * (int)gridDim.x;
+        const int n0 = tile * NT;
+        const int cnt = min(NT, a.n - n0);
+        const int li = wib * GPW + grp;  // tile-local node of this group
+        const bool act = li < cnt;
+        const int i = n0 + li;
+        int b0 = 0, b1 = 0;
+        PosT xi{};
+        double ui[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) ui[d] = 0.0;
+        if (act) {
+            b0 = sOff[li] - t0a;
+            b1 = sOff[li + 1] - t0a;
+            xi = sPos[li];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) ui[d] = sU[li * DIM + d];
+        }
+        double L[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) L[d] = 0.0;
+        for (int t = b0 + gl; t < b1; t += LPN) {
+            if (sH[t] == 0) continue;
+            const int j = sN[t];
+            const PosT xj = pos[j];
+            double e[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) e[d] = __dsub_rn(a.u[(size_t)j * DIM + d], ui[d]);
+            if (a.damage) {
+                double xv[DIM], yv[DIM];
+                xv[0] = __dsub_rn(xj.x, xi.x);
+                xv[1] = __dsub_rn(xj.y, xi.y);
+                if constexpr (DIM == 3) xv[2] = __dsub_rn(xj.z, xi.z);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
+                const double r2 = dot_rn_t<DIM>(xv, xv);
+                if (r2 > 0.0) {
+                    const double y2 = dot_rn_t<DIM>(yv, yv);
+                    const double band = 1.0e-6 * r2;
+                    const double qh = y2 - a.sc_hi2 * r2;
+                    bool brk;
+                    if (a.tension_only) {
+                        if (qh > band) brk = true;
+                        else if (qh < -band) brk = false;
+                        else brk = ref_stretch_t(y2, r2) > a.sc;
+                    } else {
+                        const double ql = a.sc_lo2 * r2 - y2;
+                        if (qh > band || ql > band) brk = true;
+                        else if (qh < -band && ql < -band) brk = false;
+                        else brk = fabs(ref_stretch_t(y2, r2)) > a.sc;
+                    }
+                    if (brk) {
+                        a.health[t0a + t] = 0;
+                        ++broken;
+                        continue;
+                    }
+                }
+            }
+            double gd[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) gd[c] = (double)sG[(size_t)c * maxb + t];
+            double f[DIM];
+            navier_apply_t<DIM>(gd, a.C11, a.C12, a.C66, e, f);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) L[d] += f[d];
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) L[d] = group_sum<LPN>(L[d]);
+
+        double unew = 0.0;
+        if (act && gl < DIM) {
+            const int d = gl;
+            const double acc = __ddiv_rn(__dadd_rn(pick_t<DIM>(L, d), a.b[d]), a.rho);
+            const size_t kk = (size_t)i * DIM + d;
+            unew = __dadd_rn(__dsub_rn(__dmul_rn(2.0, pick_t<DIM>(ui, d)), sUp[li * DIM + d]), __dmul_rn(a.dt2, acc));
+            const bool owned = a.bc_own && ((a.bc_own[i] >> d) & 1);
+            if (!owned) {
+                a.u_other[kk] = unew;
+                umax = fmax(umax, fabs(unew));
+            }
+        }
+        if (a.bc_off) {
+            double un[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) un[d] = __shfl_sync(kFull, unew, grp * LPN + d);
+            const int e0 = act ? a.bc_off[i] : 0, e1 = act ? a.bc_off[i + 1] : 0;
+            for (int e = e0 + gl; e < e1; e += LPN) {
+                const int comp = a.bc_comp[e];
+                const int form = a.bc_form[e];
+                const double g1 = __dadd_rn(a.bc_val[e], __dmul_rn(a.bc_vel[e], t_new));
+                double v;
+                if (form == 0) v = pick_t<DIM>(un, comp);
+                else if (form == 1) v = g1;
+                else if (form == 2) v = __dsub_rn(__dmul_rn(2.0, g1), pick_t<DIM>(un, comp));
+                else v = __dsub_rn(__dmul_rn(2.0, g1), __dadd_rn(a.bc_val2[e], __dmul_rn(a.bc_vel2[e], t_new)));
+                a.u_other[(size_t)a.bc_tgt[e] * DIM + comp] = v;
+                umax = fmax(umax, fabs(v));
+            }
+        }
+        __syncthreads();  // stage st fully consumed by every thread
+        if (tid == 0 && k + S < mycount) issue(k + S);
+    }
+
+    if (failed_at >= 0 && tid == 0) {
+        // tiles failed_at .. failed_at+S-1 were issued but not consumed: wait (bounded) for their copies
+        for (int k = failed_at; k < mycount && k < failed_at + S; ++k) mbar_wait(&bar[k % S], (unsigned)((k / S) & 1));
+        if (a.err) atomicAdd(a.err, 1u);
+    }
+
+    umax = group_max<kWarp>(umax);
+    if (lane == 0) s_umax[wib] = dbl_key(umax);
+    unsigned long long bsum = broken;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bsum += __shfl_xor_sync(kFull, bsum, o);
+    if (lane == 0) s_broken[wib] = bsum;
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long bb = 0, mm = 0;
+        for (int w = 0; w < WPB; ++w) {
+            bb += s_broken[w];
+            mm = s_umax[w] > mm ? s_umax[w] : mm;
+        }
+        if (bb && a.n_broken) atomicAdd(a.n_broken, bb);
+        if (a.umax) atomicMax(a.umax + a.step_in_chunk, mm);
+    }
+}
+
+template <int DIM, bool MIXED, int LPN, int S>
+static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
+    constexpr int NT = (kEpfThreads / kWarp) * (kWarp / LPN);
+    using SL = StageLayout<DIM, MIXED, NT>;
+    auto k = epf_tma_kernel<DIM, MIXED, LPN, S>;
+    const size_t smem = (size_t)S * SL::bytes(a.maxb);
+    static size_t configured = 0;
+    if (smem > configured) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = smem;
+    }
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kEpfThreads, smem);
+    const long long ntiles = ((long long)a.n + NT - 1) / NT;
+    const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    k<<<grid > 0 ? grid : 1, kEpfThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// Variants: 2D LPN 16 (NT 16) with 4 stages / LPN 8 (NT 32) with 3 stages; 3D LPN 32 (NT 8) with 2 stages.
+int epf_tma_tile_nodes(int dim, int which) {
+    if (dim == 3) return 8;
+    return which == 0 ? 16 : 32;
+}
+
+size_t epf_tma_smem(int dim, bool mixed, int which, int maxb) {
+    if (dim == 3) return mixed ? 2 * StageLayout<3, true, 8>::bytes(maxb) : 2 * StageLayout<3, false, 8>::bytes(maxb);
+    if (which == 0)
+        return mixed ? 4 * StageLayout<2, true, 16>::bytes(maxb) : 4 * StageLayout<2, false, 16>::bytes(maxb);
+    return mixed ? 3 * StageLayout<2, true, 32>::bytes(maxb) : 3 * StageLayout<2, false, 32>::bytes(maxb);
+}
+
+cudaError_t launch_epf_tma(const EpfArgs &a, int dim, bool mixed, int which, cudaStream_t s) {
+    if (dim == 3) return mixed ? launch_tma<3, true, 32, 2>(a, s) : launch_tma<3, false, 32, 2>(a, s);
+    if (which == 0) return mixed ? launch_tma<2, true, 16, 4>(a, s) : launch_tma<2, false, 16, 4>(a, s);
+    return mixed ? launch_tma<2, true, 8, 3>(a, s) : launch_tma<2, false, 8, 3>(a, s);
+}
+
+}  // namespace pxb

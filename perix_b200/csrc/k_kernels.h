@@ -63,15 +63,23 @@ struct EpfArgs {
     const double *bc_val = nullptr, *bc_vel = nullptr, *bc_val2 = nullptr, *bc_vel2 = nullptr;
     unsigned long long *umax = nullptr;     // per-step max|u| keys
     unsigned long long *n_broken = nullptr; // broken-bond counter
+    int maxb = 0;                           // TMA variants: staged bonds per tile (multiple of 32)
+    unsigned int *err = nullptr;            // TMA variants: pipeline waits that ran out
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
-constexpr int kEpfVariants = 5;
+constexpr int kEpfVariants = 7;
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s);
 int epf_grid(int n, int dim, int variant);
 int epf_lanes_per_node(int dim, int variant);
 int epf_tile_nodes(int dim, int variant);
 // the CSR-stream variants map at most 4096 bonds per tile
 bool epf_variant_fits(int dim, int variant, int max_family);
+// TMA-staged step (k_epf_tma.cu): STEP mode only; `which` 0/1 selects the 2D schedule
+bool epf_is_tma(int variant);
+int epf_tma_maxb(int dim, int variant, int max_family);
+int epf_tma_tile_nodes(int dim, int which);
+size_t epf_tma_smem(int dim, bool mixed, int which, int maxb);
+cudaError_t launch_epf_tma(const EpfArgs &a, int dim, bool mixed, int which, cudaStream_t s);
 
 struct EpfAdjArgs {
     int n = 0;

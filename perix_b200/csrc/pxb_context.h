@@ -64,9 +64,11 @@ struct Geometry {
     bool ready = false;
     int n = 0, dim = 2;
     long long nb = 0;
+    long long ldb = 0;  // padded per-bond stride: nb rounded up past nb+16 to a multiple of 16 elements, so
+                        // 16-byte-aligned bulk copies of any bond range stay inside the allocation
     double delta = 0.0, dx_char = 0.0;
-    DevBuf off;     // int32 [n+1]
-    DevBuf nbr;     // int32 [nb], 0-based
+    DevBuf off;     // int32 [n+1+16] (zero tail)
+    DevBuf nbr;     // int32 [ldb], 0-based (zero tail)
     DevBuf pos;     // double2 [n] (2D) or double4 [n] (3D)
     DevBuf vol;     // double [n]
     DevBuf mirror;  // int32 [n], 1-based mirror bulk, 0 none (may be empty)
@@ -109,9 +111,9 @@ struct EpfState {
     int precision = PXB_FP64;
     double C11 = 0, C12 = 0, C66 = 0, rho = 1, b[3] = {0, 0, 0}, sc = 0;
     int tension_only = 1;
-    DevBuf G;          // SoA Navier operators [c][nb], double or float (c = 3 in 2D, 6 in 3D)
-    DevBuf health;     // uint8 [nb]
-    DevBuf u[2];       // double [n*dim] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
+    DevBuf G;          // SoA Navier operators [c][ldb], double or float (c = 3 in 2D, 6 in 3D)
+    DevBuf health;     // uint8 [ldb] (zero tail)
+    DevBuf u[2];       // double [n*dim + 8] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
     DevBuf accel;      // double [n*dim]
     DevBuf counters;   // unsigned long long [4]: broken-bond counter, ...
     DevBuf umax;       // unsigned long long [chunk] per-step max |u| keys

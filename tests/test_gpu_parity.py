@@ -151,11 +151,18 @@ def test_epf_rate_matches_reference(ctx, name, dim):
     assert np.abs(a - d["a_rand"]).max() <= 1e-12 * np.abs(d["a_rand"]).max()
 
 
+@pytest.mark.parametrize("variant", list(range(7)))
 @pytest.mark.parametrize("name,dim", [("epf2d", 2), ("epf3d", 3)])
-def test_epf_trajectory_matches_reference(ctx, name, dim):
+def test_epf_trajectory_matches_reference(ctx, name, dim, variant):
+    """Every schedule variant of the step kernel (lane groups, CSR-stream tiles, TMA-staged tiles)."""
     import perix_b200 as px
     d = load_golden(name)
     epf_context(ctx, d, dim)
+    try:
+        ctx.epf_set_variant(variant)
+    except px.PxbError as e:
+        assert e.status == 7  # families too large for this tile size
+        pytest.skip("variant %d does not fit these families" % variant)
     n = d["coords"].size // 3
     bcs = plate_bcs(d, px) if dim == 2 else slab_bcs(d, px, n)
     ctx.epf_set_bcs(bcs)
