@@ -150,6 +150,17 @@ def read_traffic(prec):
     return None
 
 
+def kernel_name(prec, tuned):
+    """The 2D step kernel the autotuner picked (variants 0-2 lane groups, 3-4 CSR tiles, 5 and up TMA-staged)."""
+    v, lpn = tuned["variant"], tuned["lanes_per_node"]
+    mixed = "true" if prec == "mixed" else "false"
+    if v >= 5:
+        return "pxb::epf_tma_kernel<2,%s,LPN=%d,...> (variant %d)" % (mixed, lpn, v)
+    if v >= 3:
+        return "pxb::epf_stream_kernel<2,%s,EPF_STEP,...> (variant %d)" % (mixed, v)
+    return "pxb::epf_kernel<2,%s,EPF_STEP,LPN=%d,...> (variant %d)" % (mixed, lpn, v)
+
+
 def peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"], "measured"
@@ -233,7 +244,7 @@ def autotune(ctx, steps=20):
     """pxb_epf_autotune: time each schedule variant on this plate from the snapshot state, keep the fastest."""
     import ctypes as C
     best = C.c_int(0)
-    ms = np.zeros(7, np.float32)
+    ms = np.zeros(ctx.L.pxb_epf_variant_count(), np.float32)
     st = ctx.L.pxb_epf_autotune(ctx.h, steps, C.c_size_t(FLUSH_BYTES), 0, C.byref(best),
                                 ms.ctypes.data_as(C.POINTER(C.c_float)))
     if st:
@@ -383,8 +394,7 @@ def run_perix(args):
                 "api": "pxb_epf_rate (drop-in per-step call, pinned host u in / acceleration out)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": B, "kernel": "pxb::epf_kernel<2,%s,EPF_STEP,LPN=%d>" % (
-                         "true" if head == "mixed" else "false", out[head]["tuned"]["lanes_per_node"])},
+                     "algorithmic_bytes_per_launch": B, "kernel": kernel_name(head, out[head]["tuned"])},
         "cpu_baseline": ({"value": cpu["value"], "unit": "bond-updates/s", "cores": cpu["cores"],
                           "kind": "reference",
                           "sample": "20 explicit steps of the same plate through the reference's OpenMP CPU path"}
@@ -409,14 +419,50 @@ def run_perix(args):
         dist.destroy_process_group()
 
 
+def run_profile(args):
+    """One kernel family on the plate, for profiler captures.  --profile step: the plate runs 100 steps with
+    variant 1, then --steps timed steps of variant --variant from that state (so that variant's step kernel is
+    the only kernel of its name launched); --profile gbuild: --steps order-2 g-builds."""
+    import perix_b200 as px
+    w = c2_setup(px)
+    ctx = px.Context(0)
+    L = w["L"]
+    ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
+    if args.profile == "gbuild":
+        gb, ms = gbuild_rate(px, ctx, args.precision, reps=args.steps)
+        print(json.dumps({"profile": "gbuild", "precision": args.precision, "nodes_per_s": gb, "ms": ms}))
+        ctx.close()
+        return
+    C11, C12, C66 = w["C"]
+    p = px.MIXED if args.precision == "mixed" else px.FP64
+    ctx.epf_setup(C11, C12, C66, w["rho"], (0.0, 0.0), w["sc"], True, health0=w["health0"], precision=p)
+    ctx.epf_set_bcs(w["bcs"])
+    ctx.epf_start(np.zeros(2 * L.n), None, w["dt"])
+    ctx.epf_set_variant(1)
+    ctx.epf_advance(S0)
+    snap(ctx)
+    ctx.epf_set_variant(args.variant)
+    ms = np.zeros(args.steps, np.float32)
+    time_steps(ctx, args.steps, ms)
+    print(json.dumps({"profile": "step", "precision": args.precision, "variant": args.variant,
+                      "ms_per_step": float(np.mean(ms)), "bond_updates_per_s": w["nb"] / (float(np.mean(ms)) * 1e-3)}))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="perix", choices=["perix", "reference"])
+    ap.add_argument("--profile", choices=["step", "gbuild"], default=None,
+                    help="run one kernel family only (for profiler captures); prints its own JSON line")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--variant", type=int, default=8)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_perix(args)

@@ -176,11 +176,14 @@ int pxb_epf_restore(pxb_ctx *ctx);
  * (0 = none) and every restore_every steps (0 = never) the snapshot is restored; ms[s] = CUDA-event duration
  * of step s's kernel alone.  The blow-up guard is not evaluated. */
 int pxb_epf_time_steps(pxb_ctx *ctx, int nsteps, size_t flush_bytes, int restore_every, float *ms);
-/* Schedule variants of the explicit kernel (lanes per node x bonds per lane per pass).  pxb_epf_autotune
- * times every variant for `steps` steps from a private copy of the current state (L2 flushed before each
- * step), restores the state, selects the fastest and caches the choice per problem signature (dim,
- * precision, nodes, bonds, largest family); use_cache=1 returns a cached choice without timing.
- * ms_per_variant (may be NULL) receives the mean step time of each variant. */
+/* Schedule variants of the explicit kernel: 0-2 lane groups (lanes per node x bonds per lane per pass), 3-4
+ * CSR-stream tiles, 5 and up TMA-staged tiles (time step only; the other modes of a staged variant run
+ * variant 1).  pxb_epf_variant_count() gives their number.  pxb_epf_autotune times every variant that fits
+ * for `steps` steps from a private copy of the current state (L2 flushed before each step), restores the
+ * state, selects the fastest and caches the choice per problem signature (dim, precision, nodes, bonds,
+ * largest family); use_cache=1 returns a cached choice without timing.  ms_per_variant (may be NULL;
+ * pxb_epf_variant_count() entries) receives the mean step time of each variant, -1 for one that does not fit. */
+int pxb_epf_variant_count(void);
 int pxb_epf_autotune(pxb_ctx *ctx, int steps, size_t flush_bytes, int use_cache, int *best, float *ms_per_variant);
 int pxb_epf_set_variant(pxb_ctx *ctx, int variant);
 int pxb_epf_get_variant(pxb_ctx *ctx, int *variant, int *lanes_per_node);

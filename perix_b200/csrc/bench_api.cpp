@@ -169,6 +169,8 @@ extern "C" int pxb_epf_set_variant(pxb_ctx *c, int variant) {
     return PXB_OK;
 }
 
+extern "C" int pxb_epf_variant_count(void) { return kEpfVariants; }
+
 extern "C" int pxb_epf_get_variant(pxb_ctx *c, int *variant, int *lanes_per_node) {
     if (!c || !c->epf.ready || !variant) return fail(PXB_ERR_STATE, "pxb_epf_get_variant: call pxb_epf_setup first");
     *variant = c->epf.variant;

@@ -606,10 +606,10 @@ static cudaError_t launch_v(const EpfArgs &a, int mode, cudaStream_t s) {
 
 // 2D: families of ~12..30 bonds; 3D: ~40..122.  Variants 3/4 are the CSR-stream schedule (lanes per node
 // reported as 0; tile sizes in nodes below).
-static constexpr int kLpn2[kEpfVariants] = {32, 16, 8, 0, 0, 16, 8};
-static constexpr int kLpn3[kEpfVariants] = {32, 32, 16, 0, 0, 32, 32};
-static constexpr int kTile2[kEpfVariants] = {0, 0, 0, 64, 128, 0, 0};
-static constexpr int kTile3[kEpfVariants] = {0, 0, 0, 16, 32, 0, 0};
+static constexpr int kLpn2[5] = {32, 16, 8, 0, 0};
+static constexpr int kLpn3[5] = {32, 32, 16, 0, 0};
+static constexpr int kTile2[5] = {0, 0, 0, 64, 128};
+static constexpr int kTile3[5] = {0, 0, 0, 16, 32};
 
 template <int DIM, bool MIXED>
 static cudaError_t launch_dm(const EpfArgs &a, int mode, int variant, cudaStream_t s) {
@@ -649,9 +649,15 @@ cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int vari
     return mixed ? launch_dm<3, true>(a, mode, variant, s) : launch_dm<3, false>(a, mode, variant, s);
 }
 
-int epf_lanes_per_node(int dim, int variant) { return dim == 3 ? kLpn3[variant] : kLpn2[variant]; }
+int epf_lanes_per_node(int dim, int variant) {
+    if (epf_is_tma(variant)) return epf_tma_lanes(dim, variant - 5);
+    return dim == 3 ? kLpn3[variant] : kLpn2[variant];
+}
 
-int epf_tile_nodes(int dim, int variant) { return dim == 3 ? kTile3[variant] : kTile2[variant]; }
+int epf_tile_nodes(int dim, int variant) {
+    if (epf_is_tma(variant)) return 0;
+    return dim == 3 ? kTile3[variant] : kTile2[variant];
+}
 
 bool epf_variant_fits(int dim, int variant, int max_family) {
     if (epf_is_tma(variant)) {

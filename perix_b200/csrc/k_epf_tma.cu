@@ -3,15 +3,19 @@
 // Each block cycles through tiles of NT consecutive nodes (grid-stride).  A tile's families form one
 // contiguous bond range, so its per-bond streams (health byte, neighbour id, the c Navier operator streams)
 // and its per-node rows (offsets, positions, u^n, u^{n-1}) are each one contiguous span of global memory.
-// Thread 0 fetches them with cp.async.bulk 1D copies (16-byte aligned starts and sizes: the bond range is
+// One thread fetches them with cp.async.bulk 1D copies (16-byte aligned starts and sizes: the bond range is
 // widened to multiples of 16 bonds, the allocations carry the padding) into an S-stage ring, completing on a
-// per-stage mbarrier.  Consumers wait on the stage's mbarrier, so DRAM streaming for the next S-1 tiles runs
+// per-stage "full" mbarrier.  Consumers wait on that mbarrier, so DRAM streaming for the next S-1 tiles runs
 // while the current tile computes; only the neighbour gathers (mostly L2 hits) remain ordinary loads.
-// The compute is the lanes-per-node schedule of k_epf.cu (LPN lanes per node, NT = 8 warps * 32/LPN nodes).
+// There is no block-wide barrier per tile: each warp, when done with a stage, counts itself in a shared
+// counter; the warp that completes the count refills the stage with the block's tile k+S.  Warps therefore
+// drift up to S tiles apart, which hides the gather latency of one warp behind the arithmetic of another.
+// The compute is the lanes-per-node schedule of k_epf.cu (LPN lanes per node, UNR bonds per lane per pass,
+// NT = 8 warps * 32/LPN nodes per tile).
 //
-// Every wait is bounded: a thread that gives up sets a flag, the block leaves the tile loop together, thread 0
-// waits (bounded) for its copies still in flight, and the kernel records the failure in err[0].  No TMA
-// multicast is used.
+// Every wait is bounded: a warp that gives up raises a shared flag and leaves the tile loop, the others leave
+// at their next tile, the block's copies still in flight are waited for (bounded), and the kernel records
+// the failure in err[0].  No TMA multicast is used.
 #include <type_traits>
 
 #include "k_kernels.h"
@@ -134,8 +138,8 @@ struct StageLayout {
 
 }  // namespace
 
-template <int DIM, bool MIXED, int LPN, int S>
-__global__ void __launch_bounds__(kEpfThreads) epf_tma_kernel(EpfArgs a) {
+template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB>
+__global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
     using PosT = typename Vec<DIM>::T;
     using GT = typename std::conditional<MIXED, float, double>::type;
     constexpr int WPB = kEpfThreads / kWarp;
@@ -147,6 +151,9 @@ __global__ void __launch_bounds__(kEpfThreads) epf_tma_kernel(EpfArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned long long bar[S];
     __shared__ int s_t0a[S];
+    __shared__ unsigned s_done[S];  // warps finished with the stage's current tile
+    __shared__ int s_last[S];       // last tile (block-local index) issued into the stage
+    __shared__ int s_fail;
     __shared__ unsigned long long s_umax[WPB];
     __shared__ unsigned long long s_broken[WPB];
 
@@ -180,6 +187,7 @@ __global__ void __launch_bounds__(kEpfThreads) epf_tma_kernel(EpfArgs a) {
         const unsigned bytes_u = up16((unsigned)cnt * DIM * 8u);
         const unsigned total = NC * bytes_g + bytes_n + bytes_h + bytes_off + bytes_pos + bytes_u * 2u;
         s_t0a[st] = t0a;
+        s_last[st] = k;
         fence_proxy_async();
         mbar_arrive_expect_tx(&bar[st], total);
 #pragma unroll
@@ -194,7 +202,12 @@ __global__ void __launch_bounds__(kEpfThreads) epf_tma_kernel(EpfArgs a) {
     };
 
     if (tid == 0) {
-        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&bar[s], 1);
+            s_done[s] = 0;
+            s_last[s] = -1;
+        }
+        s_fail = 0;
         fence_mbar_init();
     }
     __syncthreads();
@@ -203,13 +216,13 @@ __global__ void __launch_bounds__(kEpfThreads) epf_tma_kernel(EpfArgs a) {
 
     unsigned long long broken = 0;
     double umax = 0.0;
-    int failed_at = -1;
 
     for (int k = 0; k < mycount; ++k) {
         const int st = k % S;
-        const bool ok_wait = mbar_wait(&bar[st], (unsigned)((k / S) & 1));
-        if (__syncthreads_or(!ok_wait)) {
-            failed_at = k;
+        if (*(volatile int *)&s_fail) break;
+        const bool ok_wait = __all_sync(kFull, mbar_wait(&bar[st], (unsigned)((k / S) & 1)));
+        if (!ok_wait) {
+            if (lane == 0) atomicExch(&s_fail, 1);
             break;
         }
         unsigned char *base = smem + (size_t)st * stage_bytes;
@@ -243,50 +256,78 @@ __global__ void __launch_bounds__(kEpfThreads) epf_tma_kernel(EpfArgs a) {
         double L[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) L[d] = 0.0;
-        for (int t = b0 + gl; t < b1; t += LPN) {
-            if (sH[t] == 0) continue;
-            const int j = sN[t];
-            const PosT xj = pos[j];
-            double e[DIM];
+        // UNR bonds per lane per pass: staged reads, then all neighbour gathers, then the arithmetic
+        for (int t0 = b0 + gl; t0 < b1; t0 += LPN * UNR) {
+            uint8_t h[UNR];
+            int j[UNR];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) e[d] = __dsub_rn(a.u[(size_t)j * DIM + d], ui[d]);
-            if (a.damage) {
-                double xv[DIM], yv[DIM];
-                xv[0] = __dsub_rn(xj.x, xi.x);
-                xv[1] = __dsub_rn(xj.y, xi.y);
-                if constexpr (DIM == 3) xv[2] = __dsub_rn(xj.z, xi.z);
+            for (int q = 0; q < UNR; ++q) {
+                const int t = t0 + q * LPN;
+                const bool ok = t < b1;
+                h[q] = ok ? sH[t] : (uint8_t)0;
+                j[q] = ok ? sN[t] : 0;
+            }
+            PosT xj[UNR];
+            double uj[UNR][DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
-                const double r2 = dot_rn_t<DIM>(xv, xv);
-                if (r2 > 0.0) {
-                    const double y2 = dot_rn_t<DIM>(yv, yv);
-                    const double band = 1.0e-6 * r2;
-                    const double qh = y2 - a.sc_hi2 * r2;
-                    bool brk;
-                    if (a.tension_only) {
-                        if (qh > band) brk = true;
-                        else if (qh < -band) brk = false;
-                        else brk = ref_stretch_t(y2, r2) > a.sc;
+            for (int q = 0; q < UNR; ++q) {
+                if (h[q]) {
+                    xj[q] = ldg_vec(pos + j[q]);
+                    if constexpr (DIM == 2) {
+                        const double2 v = __ldg(reinterpret_cast<const double2 *>(a.u) + j[q]);
+                        uj[q][0] = v.x;
+                        uj[q][1] = v.y;
                     } else {
-                        const double ql = a.sc_lo2 * r2 - y2;
-                        if (qh > band || ql > band) brk = true;
-                        else if (qh < -band && ql < -band) brk = false;
-                        else brk = fabs(ref_stretch_t(y2, r2)) > a.sc;
-                    }
-                    if (brk) {
-                        a.health[t0a + t] = 0;
-                        ++broken;
-                        continue;
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) uj[q][d] = __ldg(a.u + (size_t)j[q] * DIM + d);
                     }
                 }
             }
-            double gd[NC];
 #pragma unroll
-            for (int c = 0; c < NC; ++c) gd[c] = (double)sG[(size_t)c * maxb + t];
-            double f[DIM];
-            navier_apply_t<DIM>(gd, a.C11, a.C12, a.C66, e, f);
+            for (int q = 0; q < UNR; ++q) {
+                if (h[q] == 0) continue;
+                const int t = t0 + q * LPN;
+                double e[DIM];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) L[d] += f[d];
+                for (int d = 0; d < DIM; ++d) e[d] = __dsub_rn(uj[q][d], ui[d]);
+                if (a.damage) {
+                    double xv[DIM], yv[DIM];
+                    xv[0] = __dsub_rn(xj[q].x, xi.x);
+                    xv[1] = __dsub_rn(xj[q].y, xi.y);
+                    if constexpr (DIM == 3) xv[2] = __dsub_rn(xj[q].z, xi.z);
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
+                    const double r2 = dot_rn_t<DIM>(xv, xv);
+                    if (r2 > 0.0) {
+                        const double y2 = dot_rn_t<DIM>(yv, yv);
+                        const double band = 1.0e-6 * r2;
+                        const double qh = y2 - a.sc_hi2 * r2;
+                        bool brk;
+                        if (a.tension_only) {
+                            if (qh > band) brk = true;
+                            else if (qh < -band) brk = false;
+                            else brk = ref_stretch_t(y2, r2) > a.sc;
+                        } else {
+                            const double ql = a.sc_lo2 * r2 - y2;
+                            if (qh > band || ql > band) brk = true;
+                            else if (qh < -band && ql < -band) brk = false;
+                            else brk = fabs(ref_stretch_t(y2, r2)) > a.sc;
+                        }
+                        if (brk) {
+                            a.health[t0a + t] = 0;
+                            ++broken;
+                            continue;
+                        }
+                    }
+                }
+                double gd[NC];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) gd[c] = (double)sG[(size_t)c * maxb + t];
+                double f[DIM];
+                navier_apply_t<DIM>(gd, a.C11, a.C12, a.C66, e, f);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) L[d] += f[d];
+            }
         }
 #pragma unroll
         for (int d = 0; d < DIM; ++d) L[d] = group_sum<LPN>(L[d]);
@@ -321,13 +362,22 @@ __global__ void __launch_bounds__(kEpfThreads) epf_tma_kernel(EpfArgs a) {
                 umax = fmax(umax, fabs(v));
             }
         }
-        __syncthreads();  // stage st fully consumed by every thread
-        if (tid == 0 && k + S < mycount) issue(k + S);
+        // stage st consumed by this warp; the warp that completes the count refills it with tile k+S
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            if (atomicAdd(&s_done[st], 1u) == (unsigned)(WPB - 1)) {
+                atomicExch(&s_done[st], 0u);
+                __threadfence_block();
+                if (k + S < mycount) issue(k + S);
+            }
+        }
     }
-
-    if (failed_at >= 0 && tid == 0) {
-        // tiles failed_at .. failed_at+S-1 were issued but not consumed: wait (bounded) for their copies
-        for (int k = failed_at; k < mycount && k < failed_at + S; ++k) mbar_wait(&bar[k % S], (unsigned)((k / S) & 1));
+    __syncthreads();
+    if (s_fail && tid == 0) {
+        // the last tile issued into each stage may still be in flight: wait (bounded) for its copies
+        for (int s = 0; s < S; ++s)
+            if (s_last[s] >= 0) mbar_wait(&bar[s], (unsigned)((s_last[s] / S) & 1));
         if (a.err) atomicAdd(a.err, 1u);
     }
 
@@ -349,11 +399,11 @@ __global__ void __launch_bounds__(kEpfThreads) epf_tma_kernel(EpfArgs a) {
     }
 }
 
-template <int DIM, bool MIXED, int LPN, int S>
+template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB>
 static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
     constexpr int NT = (kEpfThreads / kWarp) * (kWarp / LPN);
     using SL = StageLayout<DIM, MIXED, NT>;
-    auto k = epf_tma_kernel<DIM, MIXED, LPN, S>;
+    auto k = epf_tma_kernel<DIM, MIXED, LPN, UNR, S, MINB>;
     const size_t smem = (size_t)S * SL::bytes(a.maxb);
     static size_t configured = 0;
     if (smem > configured) {
@@ -372,23 +422,63 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// Variants: 2D LPN 16 (NT 16) with 4 stages / LPN 8 (NT 32) with 3 stages; 3D LPN 32 (NT 8) with 2 stages.
-int epf_tma_tile_nodes(int dim, int which) {
-    if (dim == 3) return 8;
-    return which == 0 ? 16 : 32;
+// Staged configurations (lanes per node, bonds per lane per pass, stages; minimum resident blocks in the
+// launch bounds):
+//   2D  0: 16,2,4;1  1: 8,1,3;1  2: 8,4,3;1  3: 8,2,2;3  4: 8,1,2;4  5: 8,2,2;4
+//   3D  0: 32,2,2;1  1: 32,4,2;1 2: 32,1,3;1 3: 16,2,2;1 4: 16,1,2;2 5: 32,2,2;2
+struct TmaCfg {
+    int lpn, unr, stages;
+};
+static constexpr TmaCfg kTma2[kEpfTmaConfigs] = {{16, 2, 4}, {8, 1, 3}, {8, 4, 3}, {8, 2, 2}, {8, 1, 2}, {8, 2, 2}};
+static constexpr TmaCfg kTma3[kEpfTmaConfigs] = {{32, 2, 2}, {32, 4, 2}, {32, 1, 3}, {16, 2, 2}, {16, 1, 2}, {32, 2, 2}};
+
+int epf_tma_lanes(int dim, int which) { return dim == 3 ? kTma3[which].lpn : kTma2[which].lpn; }
+
+int epf_tma_tile_nodes(int dim, int which) { return (kEpfThreads / kWarp) * (kWarp / epf_tma_lanes(dim, which)); }
+
+template <int DIM, bool MIXED>
+static size_t tma_smem_dm(int which, int maxb) {
+    const TmaCfg c = DIM == 3 ? kTma3[which] : kTma2[which];
+    size_t per = 0;
+    switch ((kEpfThreads / kWarp) * (kWarp / c.lpn)) {
+        case 8: per = StageLayout<DIM, MIXED, 8>::bytes(maxb); break;
+        case 16: per = StageLayout<DIM, MIXED, 16>::bytes(maxb); break;
+        default: per = StageLayout<DIM, MIXED, 32>::bytes(maxb); break;
+    }
+    return (size_t)c.stages * per;
 }
 
 size_t epf_tma_smem(int dim, bool mixed, int which, int maxb) {
-    if (dim == 3) return mixed ? 2 * StageLayout<3, true, 8>::bytes(maxb) : 2 * StageLayout<3, false, 8>::bytes(maxb);
-    if (which == 0)
-        return mixed ? 4 * StageLayout<2, true, 16>::bytes(maxb) : 4 * StageLayout<2, false, 16>::bytes(maxb);
-    return mixed ? 3 * StageLayout<2, true, 32>::bytes(maxb) : 3 * StageLayout<2, false, 32>::bytes(maxb);
+    if (dim == 3) return mixed ? tma_smem_dm<3, true>(which, maxb) : tma_smem_dm<3, false>(which, maxb);
+    return mixed ? tma_smem_dm<2, true>(which, maxb) : tma_smem_dm<2, false>(which, maxb);
+}
+
+template <int DIM, bool MIXED>
+static cudaError_t launch_tma_dm(const EpfArgs &a, int which, cudaStream_t s) {
+    if constexpr (DIM == 3) {
+        switch (which) {
+            case 0: return launch_tma<3, MIXED, 32, 2, 2, 1>(a, s);
+            case 1: return launch_tma<3, MIXED, 32, 4, 2, 1>(a, s);
+            case 2: return launch_tma<3, MIXED, 32, 1, 3, 1>(a, s);
+            case 3: return launch_tma<3, MIXED, 16, 2, 2, 1>(a, s);
+            case 4: return launch_tma<3, MIXED, 16, 1, 2, 2>(a, s);
+            default: return launch_tma<3, MIXED, 32, 2, 2, 2>(a, s);
+        }
+    } else {
+        switch (which) {
+            case 0: return launch_tma<2, MIXED, 16, 2, 4, 1>(a, s);
+            case 1: return launch_tma<2, MIXED, 8, 1, 3, 1>(a, s);
+            case 2: return launch_tma<2, MIXED, 8, 4, 3, 1>(a, s);
+            case 3: return launch_tma<2, MIXED, 8, 2, 2, 3>(a, s);
+            case 4: return launch_tma<2, MIXED, 8, 1, 2, 4>(a, s);
+            default: return launch_tma<2, MIXED, 8, 2, 2, 4>(a, s);
+        }
+    }
 }
 
 cudaError_t launch_epf_tma(const EpfArgs &a, int dim, bool mixed, int which, cudaStream_t s) {
-    if (dim == 3) return mixed ? launch_tma<3, true, 32, 2>(a, s) : launch_tma<3, false, 32, 2>(a, s);
-    if (which == 0) return mixed ? launch_tma<2, true, 16, 4>(a, s) : launch_tma<2, false, 16, 4>(a, s);
-    return mixed ? launch_tma<2, true, 8, 3>(a, s) : launch_tma<2, false, 8, 3>(a, s);
+    if (dim == 3) return mixed ? launch_tma_dm<3, true>(a, which, s) : launch_tma_dm<3, false>(a, which, s);
+    return mixed ? launch_tma_dm<2, true>(a, which, s) : launch_tma_dm<2, false>(a, which, s);
 }
 
 }  // namespace pxb

@@ -67,18 +67,20 @@ struct EpfArgs {
     unsigned int *err = nullptr;            // TMA variants: pipeline waits that ran out
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
-constexpr int kEpfVariants = 7;
+constexpr int kEpfTmaConfigs = 6;                 // staged (TMA) configurations per dimension
+constexpr int kEpfVariants = 5 + kEpfTmaConfigs;  // 0-2 lane groups, 3-4 CSR tiles, 5.. staged
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s);
 int epf_grid(int n, int dim, int variant);
 int epf_lanes_per_node(int dim, int variant);
 int epf_tile_nodes(int dim, int variant);
 // the CSR-stream variants map at most 4096 bonds per tile
 bool epf_variant_fits(int dim, int variant, int max_family);
-// TMA-staged step (k_epf_tma.cu): STEP mode only; `which` 0/1 selects the 2D schedule
+// TMA-staged step (k_epf_tma.cu): STEP mode only; `which` selects one of kEpfTmaConfigs configurations
 bool epf_is_tma(int variant);
 int epf_tma_maxb(int dim, int variant, int max_family);
 int epf_tma_tile_nodes(int dim, int which);
 size_t epf_tma_smem(int dim, bool mixed, int which, int maxb);
+int epf_tma_lanes(int dim, int which);
 cudaError_t launch_epf_tma(const EpfArgs &a, int dim, bool mixed, int which, cudaStream_t s);
 
 struct EpfAdjArgs {

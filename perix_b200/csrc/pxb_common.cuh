@@ -135,6 +135,14 @@ struct Vec<3> {
     __device__ __forceinline__ static double c(const double4 &v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
 };
 
+// read-only gathers of node positions (the 3D double4 as two 16-byte loads)
+__device__ __forceinline__ double2 ldg_vec(const double2 *p) { return __ldg(p); }
+__device__ __forceinline__ double4 ldg_vec(const double4 *p) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    const double2 lo = __ldg(q), hi = __ldg(q + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
 // order-preserving key for atomicMax on non-negative doubles (NaN sorts above +inf)
 __device__ __forceinline__ unsigned long long dbl_key(double v) { return (unsigned long long)__double_as_longlong(v); }
 
