@@ -104,7 +104,7 @@ size_t ctx_bytes(const pxb_ctx *c) {
     s += bufsz(g.off) + bufsz(g.nbr) + bufsz(g.pos) + bufsz(g.vol) + bufsz(g.mirror) + bufsz(g.layer) + bufsz(g.rev);
     s += bufsz(c->ops.ops) + bufsz(c->ops.degenerate);
     const EpfState &e = c->epf;
-    s += bufsz(e.G) + bufsz(e.health) + bufsz(e.u[0]) + bufsz(e.u[1]) + bufsz(e.accel) + bufsz(e.counters) +
+    s += bufsz(e.G) + bufsz(e.P) + bufsz(e.health) + bufsz(e.u[0]) + bufsz(e.u[1]) + bufsz(e.accel) + bufsz(e.counters) +
          bufsz(e.umax) + bufsz(e.tsched);
     s += bufsz(e.bc.own) + bufsz(e.bc.src_off) + bufsz(e.bc.tgt) + bufsz(e.bc.comp) + bufsz(e.bc.form) +
          bufsz(e.bc.vals);
@@ -506,6 +506,8 @@ static EpfArgs epf_args(pxb_ctx *c) {
     a.tension_only = e.tension_only;
     a.n_broken = e.counters.as<unsigned long long>();
     a.err = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 2);
+    a.sched = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 3);
+    a.P = e.P.p;
     if (epf_is_tma(e.variant)) a.maxb = epf_tma_maxb(g.dim, e.variant, g.max_family);
     return a;
 }
@@ -546,6 +548,10 @@ extern "C" int pxb_epf_setup(pxb_ctx *c, int precision, double C11, double C12, 
     int nd = 0, first = 0;
     const int st = run_gbuild(c, 2, precision == PXB_MIXED, nullptr, e.G.p, nullptr, &nd, &first);
     if (st != PXB_OK) return st;
+    PXB_TRY(dev_alloc(c, e.P, e.G.bytes));
+    PXB_CUDA_TRY(launch_navier_pack(e.G.p, e.P.p, (long long)ldb, g.dim, precision == PXB_MIXED, C11, C12, C66,
+                                    c->stream));
+    PXB_TRY(check_launch(c, "navier pack"));
     e.ready = true;
     return PXB_OK;
 }

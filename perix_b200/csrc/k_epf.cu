@@ -15,6 +15,8 @@
 //   guard    the per-step max |u^{n+1}| (NaN-propagating) for the reference blow-up test.
 #include <type_traits>
 
+#include <algorithm>
+
 #include "k_kernels.h"
 #include "pxb_common.cuh"
 
@@ -537,6 +539,44 @@ __global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) 
         for (int w = 0; w < WPB; ++w) v += s_dC[w][threadIdx.x];
         atomicAdd(a.dC + threadIdx.x, v);
     }
+}
+
+// ---- packed Navier coefficients for the staged step kernels ----------------------------------------------
+// Per bond the 2D operator is [[p11, pxy], [pxy, p22]] (3D: symmetric 3x3); the step kernels read it directly
+// instead of forming it from (Gxx, Gyy, Gxy) and (C11, C12, C66) on every step.  The sums are evaluated in
+// FP64 from the stored G and rounded once to the storage type.
+template <int DIM, typename T>
+__global__ void navier_pack_kernel(const T *G, T *P, long long ldb, double C11, double C12, double C66) {
+    const double ac = C12 + C66;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ldb; t += (long long)gridDim.x * blockDim.x) {
+        if constexpr (DIM == 3) {
+            const double Gxx = G[t], Gyy = G[ldb + t], Gzz = G[2 * ldb + t];
+            P[t] = (T)(C11 * Gxx + C66 * (Gyy + Gzz));
+            P[ldb + t] = (T)(C11 * Gyy + C66 * (Gxx + Gzz));
+            P[2 * ldb + t] = (T)(C11 * Gzz + C66 * (Gxx + Gyy));
+            P[3 * ldb + t] = (T)(ac * (double)G[3 * ldb + t]);
+            P[4 * ldb + t] = (T)(ac * (double)G[4 * ldb + t]);
+            P[5 * ldb + t] = (T)(ac * (double)G[5 * ldb + t]);
+        } else {
+            const double Gxx = G[t], Gyy = G[ldb + t];
+            P[t] = (T)(C11 * Gxx + C66 * Gyy);
+            P[ldb + t] = (T)(C66 * Gxx + C11 * Gyy);
+            P[2 * ldb + t] = (T)(ac * (double)G[2 * ldb + t]);
+        }
+    }
+}
+
+cudaError_t launch_navier_pack(const void *G, void *P, long long ldb, int dim, bool mixed, double C11, double C12,
+                               double C66, cudaStream_t s) {
+    const int grid = (int)std::min<long long>((ldb + 255) / 256, 148LL * 16);
+    if (dim == 3) {
+        if (mixed) navier_pack_kernel<3, float><<<grid, 256, 0, s>>>((const float *)G, (float *)P, ldb, C11, C12, C66);
+        else navier_pack_kernel<3, double><<<grid, 256, 0, s>>>((const double *)G, (double *)P, ldb, C11, C12, C66);
+    } else {
+        if (mixed) navier_pack_kernel<2, float><<<grid, 256, 0, s>>>((const float *)G, (float *)P, ldb, C11, C12, C66);
+        else navier_pack_kernel<2, double><<<grid, 256, 0, s>>>((const double *)G, (double *)P, ldb, C11, C12, C66);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int grid, cudaStream_t s) {

@@ -1,6 +1,8 @@
 // explicit_pddo_frac step with the bond streams staged through shared memory by TMA bulk copies.
 //
-// Each block cycles through tiles of NT consecutive nodes (grid-stride).  A tile's families form one
+// Blocks take tiles of NT consecutive nodes from a launch-wide counter (a.sched[0], one atomic per tile; the
+// last block to finish resets it and its companion a.sched[1] for the next launch on the stream), so no block
+// is left with an extra tile while the others idle.  A tile's families form one
 // contiguous bond range, so its per-bond streams (health byte, neighbour id, the c Navier operator streams)
 // and its per-node rows (offsets, positions, u^n, u^{n-1}) are each one contiguous span of global memory.
 // One thread fetches them with cp.async.bulk 1D copies (16-byte aligned starts and sizes: the bond range is
@@ -36,6 +38,14 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, u
         "{\n\t.reg .b64 st;\n\t"
         "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
         "r"(bytes)
+        : "memory");
+}
+
+// plain arrival (count 1): completes a phase that carries no copies
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
         : "memory");
 }
 
@@ -83,26 +93,17 @@ __device__ __forceinline__ double dot_rn_t(const double *a, const double *b) {
     return s;
 }
 
+// P = packed Navier coefficients of the bond (navier_pack_kernel): 2D (p11, p22, pxy), 3D (p11, p22, p33,
+// p12, p13, p23); f = P e with P symmetric
 template <int DIM>
-__device__ __forceinline__ void navier_apply_t(const double *g, double C11, double C12, double C66, const double *e,
-                                               double *out) {
+__device__ __forceinline__ void navier_packed_t(const double *p, const double *e, double *out) {
     if constexpr (DIM == 3) {
-        const double Gxx = g[0], Gyy = g[1], Gzz = g[2], Gxy = g[3], Gxz = g[4], Gyz = g[5];
-        const double p11 = C11 * Gxx + C66 * (Gyy + Gzz);
-        const double p22 = C11 * Gyy + C66 * (Gxx + Gzz);
-        const double p33 = C11 * Gzz + C66 * (Gxx + Gyy);
-        const double ac = C12 + C66;
-        const double p12 = ac * Gxy, p13 = ac * Gxz, p23 = ac * Gyz;
-        out[0] = p11 * e[0] + p12 * e[1] + p13 * e[2];
-        out[1] = p12 * e[0] + p22 * e[1] + p23 * e[2];
-        out[2] = p13 * e[0] + p23 * e[1] + p33 * e[2];
+        out[0] = p[0] * e[0] + p[3] * e[1] + p[4] * e[2];
+        out[1] = p[3] * e[0] + p[1] * e[1] + p[5] * e[2];
+        out[2] = p[4] * e[0] + p[5] * e[1] + p[2] * e[2];
     } else {
-        const double Gxx = g[0], Gyy = g[1], Gxy = g[2];
-        const double p11 = C11 * Gxx + C66 * Gyy;
-        const double p22 = C66 * Gxx + C11 * Gyy;
-        const double pxy = (C12 + C66) * Gxy;
-        out[0] = p11 * e[0] + pxy * e[1];
-        out[1] = pxy * e[0] + p22 * e[1];
+        out[0] = p[0] * e[0] + p[2] * e[1];
+        out[1] = p[2] * e[0] + p[1] * e[1];
     }
 }
 
@@ -152,7 +153,8 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
     __shared__ unsigned long long bar[S];
     __shared__ int s_t0a[S];
     __shared__ unsigned s_done[S];  // warps finished with the stage's current tile
-    __shared__ int s_last[S];       // last tile (block-local index) issued into the stage
+    __shared__ int s_last[S];       // block-local sequence number of the last copy issued into the stage
+    __shared__ int s_tile[S];       // the stage's current tile (-1: no tiles left)
     __shared__ int s_fail;
     __shared__ unsigned long long s_umax[WPB];
     __shared__ unsigned long long s_broken[WPB];
@@ -165,16 +167,21 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
     const int maxb = a.maxb;
     const unsigned stage_bytes = SL::bytes(maxb);
     const PosT *pos = static_cast<const PosT *>(a.pos);
-    const GT *Gg = static_cast<const GT *>(a.G);
+    const GT *Pg = static_cast<const GT *>(a.P);
     const double t_new = a.t_sched[a.step_in_chunk];
 
     const int ntiles = (a.n + NT - 1) / NT;
-    const int mycount = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
-    // thread 0: fetch tile number k (k-th of this block) into stage k % S
-    auto issue = [&](int k) {
+    // one thread: fetch `tile` into stage k % S for the block's k-th stage phase; past the last tile the phase
+    // completes with no bytes and the stage reads -1
+    auto issue = [&](int k, int tile) {
         const int st = k % S;
-        const int tile = (int)blockIdx.x + k * (int)gridDim.x;
+        if (tile >= ntiles) {
+            s_tile[st] = -1;
+            mbar_arrive(&bar[st]);
+            return;
+        }
+        s_tile[st] = tile;
         const int n0 = tile * NT;
         const int cnt = min(NT, a.n - n0);
         const int t0 = __ldg(a.off + n0), t1 = __ldg(a.off + n0 + cnt);
@@ -192,7 +199,7 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
         mbar_arrive_expect_tx(&bar[st], total);
 #pragma unroll
         for (int c = 0; c < NC; ++c)
-            bulk_g2s(base + (size_t)c * maxb * SL::ES, Gg + (size_t)c * a.nb + t0a, bytes_g, &bar[st]);
+            bulk_g2s(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st]);
         bulk_g2s(base + SL::nbr_off(maxb), a.nbr + t0a, bytes_n, &bar[st]);
         bulk_g2s(base + SL::h_off(maxb), a.health + t0a, bytes_h, &bar[st]);
         bulk_g2s(base + SL::off_off(maxb), a.off + n0, bytes_off, &bar[st]);
@@ -211,13 +218,15 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
         fence_mbar_init();
     }
     __syncthreads();
-    if (tid == 0)
-        for (int k = 0; k < S && k < mycount; ++k) issue(k);
+    if (tid == 0) {
+        const int first = (int)atomicAdd(a.sched, (unsigned)S);
+        for (int k = 0; k < S; ++k) issue(k, first + k);
+    }
 
     unsigned long long broken = 0;
     double umax = 0.0;
 
-    for (int k = 0; k < mycount; ++k) {
+    for (int k = 0;; ++k) {
         const int st = k % S;
         if (*(volatile int *)&s_fail) break;
         const bool ok_wait = __all_sync(kFull, mbar_wait(&bar[st], (unsigned)((k / S) & 1)));
@@ -226,16 +235,16 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
             break;
         }
         unsigned char *base = smem + (size_t)st * stage_bytes;
-        const GT *sG = reinterpret_cast<const GT *>(base);
+        const GT *sP = reinterpret_cast<const GT *>(base);
         const int *sN = reinterpret_cast<const int *>(base + SL::nbr_off(maxb));
         unsigned char *sH = base + SL::h_off(maxb);
         const int *sOff = reinterpret_cast<const int *>(base + SL::off_off(maxb));
         const PosT *sPos = reinterpret_cast<const PosT *>(base + SL::pos_off(maxb));
         const double *sU = reinterpret_cast<const double *>(base + SL::u_off(maxb));
         const double *sUp = reinterpret_cast<const double *>(base + SL::up_off(maxb));
+        const int tile = s_tile[st];
+        if (tile < 0) break;  // tiles exhausted (every later stage phase reads -1 too)
         const int t0a = s_t0a[st];
-
-        const int tile = (int)blockIdx.x + k * (int)gridDim.x;
         const int n0 = tile * NT;
         const int cnt = min(NT, a.n - n0);
         const int li = wib * GPW + grp;  // tile-local node of this group
@@ -320,11 +329,11 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
                         }
                     }
                 }
-                double gd[NC];
+                double pd[NC];
 #pragma unroll
-                for (int c = 0; c < NC; ++c) gd[c] = (double)sG[(size_t)c * maxb + t];
+                for (int c = 0; c < NC; ++c) pd[c] = (double)sP[(size_t)c * maxb + t];
                 double f[DIM];
-                navier_apply_t<DIM>(gd, a.C11, a.C12, a.C66, e, f);
+                navier_packed_t<DIM>(pd, e, f);
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) L[d] += f[d];
             }
@@ -369,7 +378,7 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
             if (atomicAdd(&s_done[st], 1u) == (unsigned)(WPB - 1)) {
                 atomicExch(&s_done[st], 0u);
                 __threadfence_block();
-                if (k + S < mycount) issue(k + S);
+                issue(k + S, (int)atomicAdd(a.sched, 1u));
             }
         }
     }
@@ -396,6 +405,12 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
         }
         if (bb && a.n_broken) atomicAdd(a.n_broken, bb);
         if (a.umax) atomicMax(a.umax + a.step_in_chunk, mm);
+        // the last block out resets the tile counter for the next launch (no block takes tiles any more)
+        __threadfence();
+        if (atomicAdd(a.sched + 1, 1u) == gridDim.x - 1) {
+            atomicExch(a.sched, 0u);
+            atomicExch(a.sched + 1, 0u);
+        }
     }
 }
 

@@ -39,6 +39,7 @@ struct EpfArgs {
     const int *nbr = nullptr;
     const void *pos = nullptr;
     const void *G = nullptr;  // SoA [c][nb]
+    const void *P = nullptr;  // TMA variants: packed Navier coefficients SoA [c][nb] (navier_pack)
     uint8_t *health = nullptr;
     double C11 = 0, C12 = 0, C66 = 0, rho = 1, b[3] = {0, 0, 0};
     double sc = 0;                  // critical stretch
@@ -65,11 +66,16 @@ struct EpfArgs {
     unsigned long long *n_broken = nullptr; // broken-bond counter
     int maxb = 0;                           // TMA variants: staged bonds per tile (multiple of 32)
     unsigned int *err = nullptr;            // TMA variants: pipeline waits that ran out
+    unsigned int *sched = nullptr;          // TMA variants: [0] next tile, [1] finished blocks (zero between launches)
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
 constexpr int kEpfTmaConfigs = 6;                 // staged (TMA) configurations per dimension
 constexpr int kEpfVariants = 5 + kEpfTmaConfigs;  // 0-2 lane groups, 3-4 CSR tiles, 5.. staged
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s);
+// P[c][t] from G[c][t] (t < ldb, SoA stride ldb): 2D p11 = C11 Gxx + C66 Gyy, p22 = C66 Gxx + C11 Gyy,
+// pxy = (C12 + C66) Gxy; 3D p11/p22/p33 and (C12 + C66) times Gxy, Gxz, Gyz
+cudaError_t launch_navier_pack(const void *G, void *P, long long ldb, int dim, bool mixed, double C11, double C12,
+                               double C66, cudaStream_t s);
 int epf_grid(int n, int dim, int variant);
 int epf_lanes_per_node(int dim, int variant);
 int epf_tile_nodes(int dim, int variant);

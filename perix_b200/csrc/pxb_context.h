@@ -112,10 +112,12 @@ struct EpfState {
     double C11 = 0, C12 = 0, C66 = 0, rho = 1, b[3] = {0, 0, 0}, sc = 0;
     int tension_only = 1;
     DevBuf G;          // SoA Navier operators [c][ldb], double or float (c = 3 in 2D, 6 in 3D)
+    DevBuf P;          // SoA packed Navier coefficients [c][ldb] (same type): the staged step kernels' stream
     DevBuf health;     // uint8 [ldb] (zero tail)
     DevBuf u[2];       // double [n*dim + 8] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
     DevBuf accel;      // double [n*dim]
-    DevBuf counters;   // unsigned long long [4]: broken-bond counter, ...
+    DevBuf counters;   // unsigned long long [4]: [0] broken bonds, [2] staged-kernel wait failures (u32),
+                       // [3] staged-kernel tile counter + finished blocks (2 x u32, zero between launches)
     DevBuf umax;       // unsigned long long [chunk] per-step max |u| keys
     DevBuf tsched;     // double [chunk] t_{n+1} of each step in the chunk
     PinnedBuf tsched_h;
