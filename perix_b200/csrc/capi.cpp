@@ -506,7 +506,6 @@ static EpfArgs epf_args(pxb_ctx *c) {
     a.tension_only = e.tension_only;
     a.n_broken = e.counters.as<unsigned long long>();
     a.err = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 2);
-    a.sched = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 3);
     a.P = e.P.p;
     if (epf_is_tma(e.variant)) a.maxb = epf_tma_maxb(g.dim, e.variant, g.max_family);
     return a;

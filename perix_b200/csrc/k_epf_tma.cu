@@ -1,8 +1,6 @@
 // explicit_pddo_frac step with the bond streams staged through shared memory by TMA bulk copies.
 //
-// Blocks take tiles of NT consecutive nodes from a launch-wide counter (a.sched[0], one atomic per tile; the
-// last block to finish resets it and its companion a.sched[1] for the next launch on the stream), so no block
-// is left with an extra tile while the others idle.  A tile's families form one
+// Each block cycles through tiles of NT consecutive nodes (grid-stride).  A tile's families form one
 // contiguous bond range, so its per-bond streams (health byte, neighbour id, the c Navier operator streams)
 // and its per-node rows (offsets, positions, u^n, u^{n-1}) are each one contiguous span of global memory.
 // One thread fetches them with cp.async.bulk 1D copies (16-byte aligned starts and sizes: the bond range is
@@ -38,14 +36,6 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, u
         "{\n\t.reg .b64 st;\n\t"
         "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
         "r"(bytes)
-        : "memory");
-}
-
-// plain arrival (count 1): completes a phase that carries no copies
-__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
-    asm volatile(
-        "{\n\t.reg .b64 st;\n\t"
-        "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
         : "memory");
 }
 
@@ -154,7 +144,6 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
     __shared__ int s_t0a[S];
     __shared__ unsigned s_done[S];  // warps finished with the stage's current tile
     __shared__ int s_last[S];       // block-local sequence number of the last copy issued into the stage
-    __shared__ int s_tile[S];       // the stage's current tile (-1: no tiles left)
     __shared__ int s_fail;
     __shared__ unsigned long long s_umax[WPB];
     __shared__ unsigned long long s_broken[WPB];
@@ -171,17 +160,12 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
     const double t_new = a.t_sched[a.step_in_chunk];
 
     const int ntiles = (a.n + NT - 1) / NT;
+    const int mycount = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
-    // one thread: fetch `tile` into stage k % S for the block's k-th stage phase; past the last tile the phase
-    // completes with no bytes and the stage reads -1
-    auto issue = [&](int k, int tile) {
+    // one thread: fetch the block's k-th tile into stage k % S
+    auto issue = [&](int k) {
         const int st = k % S;
-        if (tile >= ntiles) {
-            s_tile[st] = -1;
-            mbar_arrive(&bar[st]);
-            return;
-        }
-        s_tile[st] = tile;
+        const int tile = (int)blockIdx.x + k * (int)gridDim.x;
         const int n0 = tile * NT;
         const int cnt = min(NT, a.n - n0);
         const int t0 = __ldg(a.off + n0), t1 = __ldg(a.off + n0 + cnt);
@@ -218,15 +202,13 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
         fence_mbar_init();
     }
     __syncthreads();
-    if (tid == 0) {
-        const int first = (int)atomicAdd(a.sched, (unsigned)S);
-        for (int k = 0; k < S; ++k) issue(k, first + k);
-    }
+    if (tid == 0)
+        for (int k = 0; k < S && k < mycount; ++k) issue(k);
 
     unsigned long long broken = 0;
     double umax = 0.0;
 
-    for (int k = 0;; ++k) {
+    for (int k = 0; k < mycount; ++k) {
         const int st = k % S;
         if (*(volatile int *)&s_fail) break;
         const bool ok_wait = __all_sync(kFull, mbar_wait(&bar[st], (unsigned)((k / S) & 1)));
@@ -242,10 +224,8 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
         const PosT *sPos = reinterpret_cast<const PosT *>(base + SL::pos_off(maxb));
         const double *sU = reinterpret_cast<const double *>(base + SL::u_off(maxb));
         const double *sUp = reinterpret_cast<const double *>(base + SL::up_off(maxb));
-        const int tile = s_tile[st];
-        if (tile < 0) break;  // tiles exhausted (every later stage phase reads -1 too)
         const int t0a = s_t0a[st];
-        const int n0 = tile * NT;
+        const int n0 = ((int)blockIdx.x + k * (int)gridDim.x) * NT;
         const int cnt = min(NT, a.n - n0);
         const int li = wib * GPW + grp;  // tile-local node of this group
         const bool act = li < cnt;
@@ -378,7 +358,7 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
             if (atomicAdd(&s_done[st], 1u) == (unsigned)(WPB - 1)) {
                 atomicExch(&s_done[st], 0u);
                 __threadfence_block();
-                issue(k + S, (int)atomicAdd(a.sched, 1u));
+                if (k + S < mycount) issue(k + S);
             }
         }
     }
@@ -405,12 +385,6 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
         }
         if (bb && a.n_broken) atomicAdd(a.n_broken, bb);
         if (a.umax) atomicMax(a.umax + a.step_in_chunk, mm);
-        // the last block out resets the tile counter for the next launch (no block takes tiles any more)
-        __threadfence();
-        if (atomicAdd(a.sched + 1, 1u) == gridDim.x - 1) {
-            atomicExch(a.sched, 0u);
-            atomicExch(a.sched + 1, 0u);
-        }
     }
 }
 

@@ -66,7 +66,6 @@ struct EpfArgs {
     unsigned long long *n_broken = nullptr; // broken-bond counter
     int maxb = 0;                           // TMA variants: staged bonds per tile (multiple of 32)
     unsigned int *err = nullptr;            // TMA variants: pipeline waits that ran out
-    unsigned int *sched = nullptr;          // TMA variants: [0] next tile, [1] finished blocks (zero between launches)
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
 constexpr int kEpfTmaConfigs = 6;                 // staged (TMA) configurations per dimension

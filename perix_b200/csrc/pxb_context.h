@@ -116,8 +116,7 @@ struct EpfState {
     DevBuf health;     // uint8 [ldb] (zero tail)
     DevBuf u[2];       // double [n*dim + 8] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
     DevBuf accel;      // double [n*dim]
-    DevBuf counters;   // unsigned long long [4]: [0] broken bonds, [2] staged-kernel wait failures (u32),
-                       // [3] staged-kernel tile counter + finished blocks (2 x u32, zero between launches)
+    DevBuf counters;   // unsigned long long [4]: [0] broken bonds, [2] staged-kernel wait failures (u32)
     DevBuf umax;       // unsigned long long [chunk] per-step max |u| keys
     DevBuf tsched;     // double [chunk] t_{n+1} of each step in the chunk
     PinnedBuf tsched_h;
