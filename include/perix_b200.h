@@ -167,6 +167,11 @@ int pxb_epf_force_adjoint(pxb_ctx *ctx, const double *u, const double *abar, dou
 int pxb_epf_force_adjoint_d(pxb_ctx *ctx, const double *u_d, const double *abar_d, double *ubar_d, double *dC_d);
 /* Force (rate) with a frozen mask, device pointers, no damage update: a = (L(u)+b)/rho. */
 int pxb_epf_force_frozen_d(pxb_ctx *ctx, const double *u_d, double *a_d);
+/* Replaces C11, C12, C66 and rho of the explicit element without rebuilding the g-functions (the packed
+ * per-bond coefficients are recomputed; captured step graphs are dropped).  No counterpart in the reference,
+ * which reads the constants from the element parameters (ExplicitPDDOFracElement.cpp:38-53); it serves
+ * sweeps and finite-difference checks of d/dE. */
+int pxb_epf_set_constants(pxb_ctx *ctx, double C11, double C12, double C66, double rho);
 
 /* ---- measurement support -----------------------------------------------------------------------------------
  * Device-side copy of the explicit state (u, u_prev, health, t) and its restore. */

@@ -418,6 +418,10 @@ class Context:
     def epf_force_adjoint_d(self, u_ptr, abar_ptr, ubar_ptr, dC_ptr):
         _check(self.L.pxb_epf_force_adjoint_d(self.h, _p(u_ptr), _p(abar_ptr), _p(ubar_ptr), _p(dC_ptr)))
 
+    def epf_set_constants(self, C11, C12, C66, rho):
+        _check(self.L.pxb_epf_set_constants(self.h, C.c_double(C11), C.c_double(C12), C.c_double(C66),
+                                            C.c_double(rho)))
+
     def epf_force_frozen_d(self, u_ptr, a_ptr):
         _check(self.L.pxb_epf_force_frozen_d(self.h, _p(u_ptr), _p(a_ptr)))
 

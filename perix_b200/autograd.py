@@ -1,0 +1,201 @@
+"""torch.autograd wrappers over the adjoint kernels of the C-ABI.
+
+- ``pddo_apply(ctx, u, slots)``: the family-sum derivative apply D^k u (reference PoissonElement.cpp:67-105,
+  ExplicitPDDOFracElement.cpp:348-366); its backward is the transpose family-scatter ``pxb_apply_adjoint_d``.
+- ``frozen_force(ctx, u, C)``: the explicit element's acceleration a = (L(u) + b)/rho with the damage mask held
+  fixed (reference ExplicitPDDOFracElement.cpp:239-299 without the breaking test); its backward is the
+  bond-force adjoint ``pxb_epf_force_adjoint_d``, which returns dJ/du and dJ/d(C11, C12, C66).
+- ``explicit_loop(ctx, u0, v0, dt, nsteps, C, plan)``: the central-difference loop of the reference
+  (TimeStepping.cpp:479-536) with the ghost BC preset after every step (DirichletBC.cpp:107-147,
+  NeumannBC.cpp:88-105), written in torch around ``frozen_force``.  Segments of ``checkpoint_every`` steps are
+  wrapped in torch.utils.checkpoint, so the backward pass keeps one state per segment and recomputes the
+  steps inside a segment.
+- ``elastic_constants_t``: C11, C12, C66 as torch functions of E and nu (ExplicitPDDOFracElement.cpp:38-53).
+
+The perix context does the arithmetic; torch supplies the tape, the device memory and the stream (each call
+puts the context on torch's current stream).  All tensors are float64 on the context's GPU.
+"""
+import numpy as np
+import torch
+from torch.utils.checkpoint import checkpoint
+
+from .api import BC, Context  # noqa: F401  (BC for type hints in callers)
+
+
+def _on_stream(pctx, t):
+    pctx.set_stream(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def _f64c(t):
+    return t.detach().to(torch.float64).contiguous()
+
+
+class _Apply(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, u, pctx, slots):
+        u = _f64c(u)
+        out = torch.empty((u.numel(), len(slots)), dtype=torch.float64, device=u.device)
+        _on_stream(pctx, u)
+        pctx.apply_d(u.data_ptr(), slots, out.data_ptr())
+        fctx.pctx, fctx.slots = pctx, list(slots)
+        return out
+
+    @staticmethod
+    def backward(fctx, gout):
+        g = _f64c(gout)
+        ub = torch.empty(g.shape[0], dtype=torch.float64, device=g.device)
+        _on_stream(fctx.pctx, g)
+        fctx.pctx.apply_adjoint_d(g.data_ptr(), fctx.slots, ub.data_ptr())
+        return ub, None, None
+
+
+def pddo_apply(pctx, u, slots):
+    """(N,) scalar field -> (N, len(slots)) derivatives for the multi-index slots (0-based) of the context's
+    operator cache; differentiable in u."""
+    return _Apply.apply(u, pctx, list(slots))
+
+
+class _FrozenForce(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, u, C, pctx):
+        u = _f64c(u)
+        a = torch.empty_like(u)
+        _on_stream(pctx, u)
+        pctx.epf_force_frozen_d(u.data_ptr(), a.data_ptr())
+        fctx.save_for_backward(u)
+        fctx.pctx = pctx
+        return a
+
+    @staticmethod
+    def backward(fctx, abar):
+        (u,) = fctx.saved_tensors
+        ab = _f64c(abar)
+        ub = torch.empty_like(u)
+        dC = torch.empty(3, dtype=torch.float64, device=u.device)
+        _on_stream(fctx.pctx, u)
+        fctx.pctx.epf_force_adjoint_d(u.data_ptr(), ab.data_ptr(), ub.data_ptr(), dC.data_ptr())
+        return ub, dC, None
+
+
+def frozen_force(pctx, u, C):
+    """a = (L(u) + b)/rho (N*dim, interleaved) with the context's current health mask held fixed.  C is the
+    (3,) tensor (C11, C12, C66) that the context was set up with (``epf_set_constants``); it only routes the
+    gradient dJ/dC."""
+    return _FrozenForce.apply(u, C, pctx)
+
+
+def elastic_constants_t(dim, plane_stress, E, nu):
+    """(C11, C12, C66) as a (3,) tensor, differentiable in E (and nu)."""
+    if dim >= 3 or not plane_stress:
+        d = (1.0 + nu) * (1.0 - 2.0 * nu)
+        return torch.stack([E * (1.0 - nu) / d, E * nu / d, E / (2.0 * (1.0 + nu))])
+    d = 1.0 - nu * nu
+    return torch.stack([E / d, E * nu / d, E / (2.0 * (1.0 + nu))])
+
+
+class BcPlan:
+    """The BC list compiled to index tensors: entries are applied in list order (reference semantics); within
+    an entry every target is written from values read before the entry (no target of an entry is the mirror of
+    another of its targets, which holds for ghost layers and boxed groups; checked here).
+
+    Dirichlet: u[g,a] = 2 G(t) - u[mirror(g),a] (reflection) or G(t) (direct or no mirror), G = value + velocity*t,
+    nodes filtered by the optional box; Neumann: u[g,a] = u[mirror(g),a] for ghosts with a mirror."""
+
+    def __init__(self, bcs, coords3, mirror, dim, device):
+        xyz = np.asarray(coords3, np.float64).reshape(-1, 3)
+        mir = np.zeros(xyz.shape[0], np.int64) if mirror is None else np.asarray(mirror, np.int64)
+        self.dim = dim
+        self.ops = []
+        for bc in bcs:
+            ids = np.unique(np.asarray(bc.nodes, np.int64))  # 1-based; a repeated id writes the same value
+            comps = [int(c) for c in bc.comps]
+            if bc.kind == "dirichlet":
+                if bc.box is not None:
+                    box = np.asarray(bc.box, np.float64)
+                    inside = np.ones(ids.size, bool)
+                    for a in range(dim):
+                        x = xyz[ids - 1, a]
+                        inside &= (x >= box[2 * a]) & (x <= box[2 * a + 1])
+                    ids = ids[inside]
+                mb = mir[ids - 1]
+                refl = (mb >= 1) & (not bc.direct)
+                for kind, sel in (("reflect", refl), ("direct", ~refl)):
+                    if not sel.any():
+                        continue
+                    tg, sr, va, ve = [], [], [], []
+                    for a in comps:
+                        tg.append((ids[sel] - 1) * dim + a)
+                        sr.append((mb[sel] - 1) * dim + a)
+                        va.append(np.full(sel.sum(), float(bc.value[a])))
+                        ve.append(np.full(sel.sum(), float(bc.velocity[a])))
+                    tgt, src = np.concatenate(tg), np.concatenate(sr)
+                    if kind == "reflect":
+                        assert not np.intersect1d(tgt, src).size, "a BC target mirrors another target"
+                    self.ops.append((kind, torch.from_numpy(tgt).to(device), torch.from_numpy(src).to(device),
+                                     torch.from_numpy(np.concatenate(va)).to(device),
+                                     torch.from_numpy(np.concatenate(ve)).to(device)))
+            else:
+                mb = mir[ids - 1]
+                ids, mb = ids[mb >= 1], mb[mb >= 1]
+                if not ids.size:
+                    continue
+                tgt = np.concatenate([(ids - 1) * dim + a for a in comps])
+                src = np.concatenate([(mb - 1) * dim + a for a in comps])
+                assert not np.intersect1d(tgt, src).size, "a BC target mirrors another target"
+                self.ops.append(("copy", torch.from_numpy(tgt).to(device), torch.from_numpy(src).to(device),
+                                 None, None))
+
+    def apply(self, u, t):
+        for kind, tgt, src, val, vel in self.ops:
+            if kind == "copy":
+                u = u.index_put((tgt,), u[src])
+            else:
+                g = val + vel * t
+                u = u.index_put((tgt,), 2.0 * g - u[src] if kind == "reflect" else g)
+        return u
+
+
+def _segment(pctx, C, plan, dt2, times, force, u, uold):
+    for tn in times:
+        a = force(pctx, u, C)
+        un = 2.0 * u - uold + dt2 * a
+        un = plan.apply(un, tn)
+        uold, u = u, un
+    return u, uold
+
+
+def explicit_loop(pctx, u0, v0, dt, nsteps, C, plan, checkpoint_every=100, t0=0.0, force=None):
+    """nsteps central-difference steps from (u0, v0) at t0 with a frozen damage mask; returns (u^N, u^{N-1}).
+
+    u^{-1} = u0 - dt v0 + dt^2/2 a(u0); u^{n+1} = 2u^n - u^{n-1} + dt^2 a(u^n), then the BC preset at t_{n+1}
+    (t accumulated as t + dt like the reference loop).  The context's constants must equal C (see
+    ``set_constants``).  With checkpoint_every > 0 each segment of that many steps is recomputed in the
+    backward pass instead of stored.  ``force(pctx, u, C)`` replaces ``frozen_force`` (e.g. by a plain-torch
+    restatement for reference gradients)."""
+    force = force or frozen_force
+    a0 = force(pctx, u0, C)
+    if v0 is None:
+        v0 = torch.zeros_like(u0)
+    uold = u0 - dt * v0 + (0.5 * dt * dt) * a0
+    u = u0
+    dt2 = dt * dt
+    t = t0
+    done = 0
+    while done < nsteps:
+        k = min(checkpoint_every if checkpoint_every > 0 else nsteps, nsteps - done)
+        times = []
+        for _ in range(k):
+            t = t + dt
+            times.append(t)
+        if checkpoint_every > 0 and torch.is_grad_enabled():
+            u, uold = checkpoint(_segment, pctx, C, plan, dt2, times, force, u, uold, use_reentrant=False)
+        else:
+            u, uold = _segment(pctx, C, plan, dt2, times, force, u, uold)
+        done += k
+    return u, uold
+
+
+def set_constants(pctx, C, rho):
+    """Puts the values of the (3,) tensor C into the context (one device-to-host read)."""
+    c11, c12, c66 = (float(x) for x in C.detach().cpu())
+    pctx.epf_set_constants(c11, c12, c66, rho)

@@ -913,6 +913,20 @@ extern "C" int pxb_epf_force_frozen_d(pxb_ctx *c, const double *u_d, double *a_d
     return check_launch(c, "epf force (frozen mask)");
 }
 
+extern "C" int pxb_epf_set_constants(pxb_ctx *c, double C11, double C12, double C66, double rho) {
+    PXB_TRY(need_epf(c, "pxb_epf_set_constants"));
+    if (!(rho > 0.0)) return fail(PXB_ERR_INVALID, "pxb_epf_set_constants: rho must be > 0");
+    EpfState &e = c->epf;
+    destroy_graphs(e);  // captured launches carry the old constants
+    e.C11 = C11;
+    e.C12 = C12;
+    e.C66 = C66;
+    e.rho = rho;
+    PXB_CUDA_TRY(launch_navier_pack(e.G.p, e.P.p, (long long)c->g.ldb, c->g.dim, e.precision == PXB_MIXED, C11, C12,
+                                    C66, c->stream));
+    return check_launch(c, "navier pack");
+}
+
 extern "C" int pxb_epf_force_adjoint_d(pxb_ctx *c, const double *u_d, const double *abar_d, double *ubar_d,
                                        double *dC_d) {
     PXB_TRY(need_epf(c, "pxb_epf_force_adjoint"));
