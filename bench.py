@@ -54,6 +54,66 @@ def c2_setup(px):
                 bcs=bcs, E=E, nu=nu, G0=G0, cracks=cracks, n=L.n, nb=int(off[-1]), h=h)
 
 
+def c3_clouds(px, nclouds=256, nmin=1000, nmax=200000, seed=2024):
+    """Batched-cloud workload: clouds alternate 2D / 3D (half each), node counts log-uniform in [nmin, nmax]
+    (seeded), cell-centred lattice of spacing h = 1 mm jittered by U(-0.2h, 0.2h) per coordinate, no ghosts
+    (families truncated at the cloud boundary), delta = 3.015h, unit-cell volumes, dx_char = h."""
+    rng = np.random.default_rng(seed)
+    h = 1e-3
+    clouds = []
+    for k in range(nclouds):
+        dim = 2 if k % 2 == 0 else 3
+        target = math.exp(rng.uniform(math.log(nmin), math.log(nmax)))
+        if dim == 2:
+            nx = max(2, int(round(math.sqrt(target))))
+            ny = max(2, int(round(target / nx)))
+            g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij"), -1).reshape(-1, 2)
+            xyz = np.zeros((g.shape[0], 3))
+            xyz[:, :2] = (g + 0.5) * h
+        else:
+            m = max(2, int(round(target ** (1.0 / 3.0))))
+            g = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 3)
+            xyz = (g + 0.5) * h
+        xyz[:, :dim] += rng.uniform(-0.2 * h, 0.2 * h, size=(xyz.shape[0], dim))
+        delta = 3.015 * h * (1.0 + 1e-6)
+        off, ids = px.families(xyz, delta, dim == 3)
+        clouds.append(dict(dim=dim, coords3=xyz, vols=np.full(xyz.shape[0], h ** dim), off=off, ids=ids,
+                           delta=delta, dx_char=h))
+    return clouds
+
+
+def cubic_field(clouds, seed=7):
+    """Random cubic polynomial per cloud (N(0,1) coefficients on coordinates scaled to the cloud's extent) and
+    its exact order-2 derivatives in the multi-index order of the operators."""
+    rng = np.random.default_rng(seed)
+    u, exact = [], []
+    for c in clouds:
+        dim = c["dim"]
+        x = c["coords3"][:, :dim]
+        L = float(x.max() - x.min())
+        xs = x / L
+        exps = [e for e in np.ndindex(*(4,) * dim) if sum(e) <= 3]
+        coef = rng.standard_normal(len(exps))
+        f = np.zeros(x.shape[0])
+        for a, e in zip(coef, exps):
+            f += a * np.prod(xs ** np.asarray(e), axis=1)
+        slots = [(1, 0), (0, 1), (2, 0), (1, 1), (0, 2)] if dim == 2 else \
+            [(1, 0, 0), (0, 1, 0), (0, 0, 1), (2, 0, 0), (1, 1, 0), (1, 0, 1), (0, 2, 0), (0, 1, 1), (0, 0, 2)]
+        d = np.zeros((x.shape[0], len(slots)))
+        for s, q in enumerate(slots):
+            for a, e in zip(coef, exps):
+                if all(ei >= qi for ei, qi in zip(e, q)):
+                    term = np.full(x.shape[0], a)
+                    for ax in range(dim):
+                        for r in range(q[ax]):
+                            term = term * (e[ax] - r)
+                        term = term * xs[:, ax] ** (e[ax] - q[ax])
+                    d[:, s] += term / L ** sum(q)
+        u.append(f)
+        exact.append(d)
+    return u, exact
+
+
 def algorithmic_bytes(n, nb, dim, prec):
     """Per step: nb*(4 B id + c*s B operators + 1 B health) + N*(x, u^n, u^{n-1}, u^{n+1}: 4*dim*8 B)."""
     c = 6 if dim == 3 else 3

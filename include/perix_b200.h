@@ -196,6 +196,37 @@ int pxb_epf_get_variant(pxb_ctx *ctx, int *variant, int *lanes_per_node);
  * before each; ms[r] = CUDA-event duration of build r. */
 int pxb_gbuild_time(pxb_ctx *ctx, int order, int precision, int reps, size_t flush_bytes, float *ms);
 
+/* ---- batched clouds ----------------------------------------------------------------------------------------
+ * Many independent node clouds (2D and 3D mixed, boundary-truncated families of uneven size) in one
+ * concatenated numbering: cloud k owns nodes [node_off[k], node_off[k+1]); neigh_off is the CSR over all nodes
+ * (neigh_off[N] bonds); neigh_id holds 1-based ids WITHIN the node's own cloud (the reference's per-mesh
+ * convention, PDMeshData per cloud as in tests/ExplicitPDDOFracElementTests.cpp:35-64); coords3 is xyz per
+ * node; delta / dx_char per cloud (PDOperators::calcAMatrixCompute, CalcPDOperators.cpp:108-226).
+ * pxb_batch_gbuild builds the order-2 g-functions of every cloud (nop 5 in 2D, 9 in 3D) in one persistent
+ * launch (or one per dimension, as the schedule says) and fails with PXB_ERR_DEGENERATE naming the cloud and
+ * node of a degenerate family.  pxb_batch_apply computes all nop derivatives of a scalar field (N) per node:
+ * out[out_off(k) + (i - node_off[k]) * nop + s], clouds back to back ([n_k][nop_k]; total length from
+ * pxb_batch_info).  pxb_batch_get_ops returns one cloud's g-functions as double [nb_k][nop_k].
+ * No single counterpart in the reference, which builds and applies one mesh at a time. */
+int pxb_batch_set(pxb_ctx *ctx, int nclouds, const int *dims, const int *node_off, const double *coords3,
+                  const double *vols, const int *neigh_off, const int *neigh_id, const double *delta,
+                  const double *dx_char);
+int pxb_batch_info(pxb_ctx *ctx, long long *nodes, long long *bonds, long long *out_len, long long *ops_len);
+int pxb_batch_gbuild(pxb_ctx *ctx, int precision, int *n_degenerate, int *first_degenerate);
+int pxb_batch_apply(pxb_ctx *ctx, const double *u, double *out);
+int pxb_batch_apply_d(pxb_ctx *ctx, const double *u_d, double *out_d);
+int pxb_batch_get_ops(pxb_ctx *ctx, int cloud, double *ops);
+/* Schedules (which 0: g-build, 1: apply): lanes per node for 2D and 3D clouds and one launch for both
+ * dimensions or one per dimension; pxb_batch_variant_count() of each.  pxb_batch_time times `reps` launches of
+ * the current schedule (L2 flushed before each; the apply on device buffers u_d -> out_d), pxb_batch_autotune
+ * times every schedule and keeps the fastest. */
+int pxb_batch_variant_count(void);
+int pxb_batch_set_variant(pxb_ctx *ctx, int which, int variant);
+int pxb_batch_get_variant(pxb_ctx *ctx, int which, int *variant);
+int pxb_batch_time(pxb_ctx *ctx, int what, int reps, size_t flush_bytes, const double *u_d, double *out_d, float *ms);
+int pxb_batch_autotune(pxb_ctx *ctx, int what, int reps, size_t flush_bytes, const double *u_d, double *out_d,
+                       int *best, float *ms_per_variant);
+
 /* ---- CSR Jacobian value assembly ---------------------------------------------------------------------------
  * Sets the matrix pattern (from pxb_csr_pattern or the caller) and precomputes the bond -> CSR-slot map
  * on the device (no binary search per assembly). */

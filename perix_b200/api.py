@@ -425,6 +425,85 @@ class Context:
     def epf_force_frozen_d(self, u_ptr, a_ptr):
         _check(self.L.pxb_epf_force_frozen_d(self.h, _p(u_ptr), _p(a_ptr)))
 
+    # -- batched clouds
+    def batch_set(self, clouds):
+        """clouds: list of dicts with dim, coords3 (n x 3), vols, off, ids (1-based within the cloud), delta,
+        dx_char.  Concatenates them into the batch numbering."""
+        dims = _i32([c["dim"] for c in clouds])
+        node_off = np.zeros(len(clouds) + 1, np.int64)
+        node_off[1:] = np.cumsum([int(np.asarray(c["vols"]).size) for c in clouds])
+        coords = np.concatenate([_f64(c["coords3"]).reshape(-1) for c in clouds])
+        vols = np.concatenate([_f64(c["vols"]) for c in clouds])
+        offs, base = [np.zeros(1, np.int64)], 0
+        for c in clouds:
+            o = np.asarray(c["off"], np.int64)
+            offs.append(o[1:] + base)
+            base += int(o[-1])
+        neigh_off = np.concatenate(offs)
+        if base >= 2 ** 31 or node_off[-1] >= 2 ** 31:
+            raise ValueError("batch too large for 32-bit offsets")
+        ids = np.concatenate([_i32(c["ids"]) for c in clouds])
+        delta = _f64([c["delta"] for c in clouds])
+        dxc = _f64([c["dx_char"] for c in clouds])
+        _check(self.L.pxb_batch_set(self.h, len(clouds), _p(dims, C.c_int), _p(_i32(node_off), C.c_int), _p(coords),
+                                    _p(vols), _p(_i32(neigh_off), C.c_int), _p(ids, C.c_int), _p(delta), _p(dxc)))
+        self.batch_dims = [int(c["dim"]) for c in clouds]
+        self.batch_node_off = node_off
+        n, nb, ol, opl = C.c_longlong(0), C.c_longlong(0), C.c_longlong(0), C.c_longlong(0)
+        _check(self.L.pxb_batch_info(self.h, C.byref(n), C.byref(nb), C.byref(ol), C.byref(opl)))
+        self.batch_n, self.batch_nb, self.batch_out_len, self.batch_ops_len = n.value, nb.value, ol.value, opl.value
+        self.batch_bond_counts = [int(np.asarray(c["off"])[-1]) for c in clouds]
+
+    def batch_gbuild(self, precision=FP64):
+        nd, first = C.c_int(0), C.c_int(0)
+        _check(self.L.pxb_batch_gbuild(self.h, int(precision), C.byref(nd), C.byref(first)))
+        return nd.value, first.value
+
+    def batch_apply(self, u):
+        out = np.zeros(self.batch_out_len, np.float64)
+        _check(self.L.pxb_batch_apply(self.h, _p(_f64(u)), _p(out)))
+        return out
+
+    def batch_apply_d(self, u_ptr, out_ptr):
+        _check(self.L.pxb_batch_apply_d(self.h, _p(u_ptr), _p(out_ptr)))
+
+    def batch_split(self, out):
+        """Per-cloud views (n_k x nop_k) of a batch apply output."""
+        res, pos = [], 0
+        for k, d in enumerate(self.batch_dims):
+            n = int(self.batch_node_off[k + 1] - self.batch_node_off[k])
+            nop = 9 if d == 3 else 5
+            res.append(out[pos:pos + n * nop].reshape(n, nop))
+            pos += n * nop
+        return res
+
+    def batch_get_ops(self, cloud):
+        nop = 9 if self.batch_dims[cloud] == 3 else 5
+        ops = np.zeros(max(1, self.batch_bond_counts[cloud] * nop), np.float64)
+        _check(self.L.pxb_batch_get_ops(self.h, int(cloud), _p(ops)))
+        return ops[:self.batch_bond_counts[cloud] * nop].reshape(-1, nop)
+
+    def batch_set_variant(self, which, variant):
+        _check(self.L.pxb_batch_set_variant(self.h, int(which), int(variant)))
+
+    def batch_variant(self, which):
+        v = C.c_int(0)
+        _check(self.L.pxb_batch_get_variant(self.h, int(which), C.byref(v)))
+        return v.value
+
+    def batch_time(self, what, reps, flush_bytes=256 << 20, u_ptr=0, out_ptr=0):
+        ms = np.zeros(reps, np.float32)
+        _check(self.L.pxb_batch_time(self.h, int(what), int(reps), C.c_size_t(flush_bytes), _vp(u_ptr), _vp(out_ptr),
+                                     ms.ctypes.data_as(C.POINTER(C.c_float))))
+        return ms
+
+    def batch_autotune(self, what, reps=3, flush_bytes=256 << 20, u_ptr=0, out_ptr=0):
+        best = C.c_int(0)
+        ms = np.zeros(self.L.pxb_batch_variant_count(), np.float32)
+        _check(self.L.pxb_batch_autotune(self.h, int(what), int(reps), C.c_size_t(flush_bytes), _vp(u_ptr),
+                                         _vp(out_ptr), C.byref(best), ms.ctypes.data_as(C.POINTER(C.c_float))))
+        return best.value, ms
+
     # -- CSR assembly
     def csr_set_pattern(self, rowptr, cols, ndof=1):
         r = _i32(rowptr)

@@ -62,6 +62,12 @@ int flush_l2(pxb_ctx *c, size_t bytes, DevBuf &buf) {
 
 DevBuf g_flush;
 
+}  // namespace
+
+int pxb::l2_flush(pxb_ctx *c, size_t bytes) { return flush_l2(c, bytes, g_flush); }
+
+namespace {
+
 int save_state(pxb_ctx *c, Snapshot &s) {
     EpfState &e = c->epf;
     PXB_TRY(dev_alloc(c, s.u0, e.u[0].bytes));

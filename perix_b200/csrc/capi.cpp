@@ -108,6 +108,9 @@ size_t ctx_bytes(const pxb_ctx *c) {
          bufsz(e.umax) + bufsz(e.tsched);
     s += bufsz(e.bc.own) + bufsz(e.bc.src_off) + bufsz(e.bc.tgt) + bufsz(e.bc.comp) + bufsz(e.bc.form) +
          bufsz(e.bc.vals);
+    const BatchState &bt = c->batch;
+    s += bufsz(bt.clouds) + bufsz(bt.tasks) + bufsz(bt.off) + bufsz(bt.nbr) + bufsz(bt.pos) + bufsz(bt.vol) +
+         bufsz(bt.ops) + bufsz(bt.degenerate) + bufsz(bt.counters);
     const CsrState &k = c->csr;
     s += bufsz(k.rowptr) + bufsz(k.cols) + bufsz(k.slot) + bufsz(k.diag) + bufsz(k.kvals) + bufsz(k.rhs) +
          bufsz(k.u) + bufsz(k.uold) + bufsz(k.fnode) + bufsz(k.mnode);

@@ -1,6 +1,8 @@
 // Family-sum derivative apply D^k u_i = sum_j g^k_ij (u_j - u_i) and its transpose (reference pattern:
 // PoissonElement::computeNodalProjection, src/ElmtSystem/PoissonElement.cpp:67-105; V_j is baked into g).
 // Plus the small utility kernels (reverse-bond map, layout packing, health conversion, L2 flush).
+#include <type_traits>
+
 #include "k_kernels.h"
 #include "pxb_common.cuh"
 
@@ -99,6 +101,117 @@ cudaError_t launch_apply_adjoint(const ApplyArgs &a, bool mixed, int grid, cudaS
     if (mixed) apply_adjoint_kernel<true><<<grid, kApplyThreads, 0, s>>>(a);
     else apply_adjoint_kernel<false><<<grid, kApplyThreads, 0, s>>>(a);
     return cudaGetLastError();
+}
+
+// ---- batched clouds: all order-2 derivatives of a scalar field, every cloud in one persistent launch -----------
+// D^k u_i = sum_t g^k_t (u_j - u_i) for k < nop (5 in 2D, 9 in 3D); LPN lanes per node stride the family
+// (coalesced reads of consecutive operator rows), a butterfly over the group reduces the nop sums.  MIXED: g and
+// u_j - u_i in FP32 with two-sum accumulation.
+template <bool MIXED, int DIM, int LPN>
+__device__ __forceinline__ void apply_batch_group(const BatchArgs &b, const BatchCloud &cd, int i, bool act, int gl) {
+    constexpr int NOP = DIM == 3 ? 9 : 5;
+    using GT = typename std::conditional<MIXED, float, double>::type;
+    const GT *ops = static_cast<const GT *>(b.ops) + cd.ops_off;
+    const int b0 = act ? b.off[i] : 0, b1 = act ? b.off[i + 1] : 0;
+    const double ui = act ? b.u[i] : 0.0;
+    double acc[NOP];
+    CompF cacc[MIXED ? NOP : 1];
+#pragma unroll
+    for (int k = 0; k < NOP; ++k) acc[k] = 0.0;
+    for (int t = b0 + gl; t < b1; t += LPN) {
+        const int j = __ldg(b.nbr + t);
+        const double du = __ldg(b.u + j) - ui;
+        const GT *g = ops + (size_t)(t - cd.bond0) * NOP;
+        if constexpr (MIXED) {
+            const float duf = (float)du;
+#pragma unroll
+            for (int k = 0; k < NOP; ++k) cacc[k].add(__ldg(g + k) * duf);
+        } else {
+#pragma unroll
+            for (int k = 0; k < NOP; ++k) acc[k] = fma(__ldg(g + k), du, acc[k]);
+        }
+    }
+    if constexpr (MIXED) {
+#pragma unroll
+        for (int k = 0; k < NOP; ++k) acc[k] = cacc[k].value();
+    }
+    double mine = 0.0;
+#pragma unroll
+    for (int k = 0; k < NOP; ++k) {
+        const double v = group_sum<LPN>(acc[k]);
+        if (gl == k) mine = v;
+    }
+    if (act && gl < NOP) b.out[cd.out_off + (size_t)(i - cd.node0) * NOP + gl] = mine;
+}
+
+template <bool MIXED, int LPN2, int LPN3, int DIMS>
+__global__ void __launch_bounds__(kApplyThreads) apply_batch_kernel(BatchArgs b) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int task = 0;
+        if (lane == 0) task = (int)atomicAdd(b.counter, 1u);
+        task = __shfl_sync(kFull, task, 0);
+        if (task >= b.ntasks) break;
+        const BatchTask tk = b.tasks[b.task0 + task];
+        const BatchCloud cd = b.clouds[tk.cloud];
+        if constexpr ((DIMS & 1) != 0) {
+            if (tk.dim == 2) {
+                constexpr int GPW = kWarp / LPN2;
+                for (int k0 = 0; k0 < tk.count; k0 += GPW) {
+                    const int q = k0 + lane / LPN2;
+                    apply_batch_group<MIXED, 2, LPN2>(b, cd, tk.first + (q < tk.count ? q : 0), q < tk.count,
+                                                      lane & (LPN2 - 1));
+                }
+            }
+        }
+        if constexpr ((DIMS & 2) != 0) {
+            if (tk.dim == 3) {
+                constexpr int GPW = kWarp / LPN3;
+                for (int k0 = 0; k0 < tk.count; k0 += GPW) {
+                    const int q = k0 + lane / LPN3;
+                    apply_batch_group<MIXED, 3, LPN3>(b, cd, tk.first + (q < tk.count ? q : 0), q < tk.count,
+                                                      lane & (LPN3 - 1));
+                }
+            }
+        }
+    }
+}
+
+BatchSchedule batch_apply_schedule(int v) {
+    switch (v) {
+        case 0: return {8, 16, false};
+        case 1: return {4, 16, false};
+        case 2: return {8, 32, false};
+        default: return {8, 16, true};
+    }
+}
+
+template <bool MIXED, int LPN2, int LPN3, int DIMS>
+static cudaError_t launch_ab(const BatchArgs &a, cudaStream_t s) {
+    auto k = apply_batch_kernel<MIXED, LPN2, LPN3, DIMS>;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kApplyThreads, 0);
+    const long long want = ((long long)a.ntasks + (kApplyThreads / kWarp) - 1) / (kApplyThreads / kWarp);
+    const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    const int grid = (int)(want < cap ? (want > 0 ? want : 1) : cap);
+    k<<<grid, kApplyThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <bool MIXED>
+static cudaError_t launch_ab_m(const BatchArgs &a, int variant, int dims, cudaStream_t s) {
+    switch (variant) {
+        case 0: return launch_ab<MIXED, 8, 16, 3>(a, s);
+        case 1: return launch_ab<MIXED, 4, 16, 3>(a, s);
+        case 2: return launch_ab<MIXED, 8, 32, 3>(a, s);
+        default: return dims == 1 ? launch_ab<MIXED, 8, 16, 1>(a, s) : launch_ab<MIXED, 8, 16, 2>(a, s);
+    }
+}
+
+cudaError_t launch_apply_batch(const BatchArgs &a, bool mixed, int variant, int dims, cudaStream_t s) {
+    return mixed ? launch_ab_m<true>(a, variant, dims, s) : launch_ab_m<false>(a, variant, dims, s);
 }
 
 // ---- reverse bond: rev[t] = position of i in fam(j) for t = (i -> j), -1 when absent ------------------

@@ -24,23 +24,17 @@
 
 namespace pxb {
 
-// LPN lanes per node (a power of two >= nop): GPW = 32/LPN nodes per warp are built concurrently.
+// One node per group of LPN lanes (a power of two >= nop; the caller maps 32/LPN groups onto a warp, all
+// lanes of the warp call this together).  i is the node (act false: idle group); sA and sX are this group's
+// nop x nop shared-memory slots.  Positions are read at pos[j - a.node_base] and the AoS operators written at
+// ops[(t - a.bond_base) * nop], so a batch of clouds can address one cloud's slices with global ids.
 template <int DIM, int ORDER, bool MIXED, int LPN>
-__global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
+__device__ __forceinline__ void gbuild_group(const GBuildArgs &a, int i, bool act, int gl, double *sA, double *sX) {
     constexpr QTable<DIM, ORDER> Q{};
     constexpr int NOP = Q.NOP;
     constexpr int NE = NOP * (NOP + 1) / 2;
-    constexpr int GPW = kWarp / LPN;
-    constexpr int GPB = (kGbuildThreads / kWarp) * GPW;  // node groups per block
     static_assert(LPN >= NOP, "one lane per solve column");
     using PosT = typename Vec<DIM>::T;
-
-    __shared__ double sA[GPB][NOP * NOP];
-    __shared__ double sX[GPB][NOP * NOP];
-
-    const int lane = threadIdx.x & 31;
-    const int gl = lane & (LPN - 1);
-    const int wib = (threadIdx.x >> 5) * GPW + lane / LPN;  // node group index within the block
     const PosT *pos = static_cast<const PosT *>(a.pos);
     const double inv_delta = 1.0 / a.delta;
 
@@ -52,13 +46,9 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
         for (int t = 0; t < Q.p[k] + Q.q[k] + Q.r[k]; ++t) v *= inv_delta;
         idpow[k] = v;
     }
-
-    const long long stride = (long long)gridDim.x * GPB;
-    for (long long base = (long long)blockIdx.x * GPB + (threadIdx.x >> 5) * GPW; base < a.n + 0LL; base += stride) {
-        const int i = (int)(base + lane / LPN);
-        const bool act = i < a.n;
+    {
         const int b0 = act ? a.off[i] : 0, b1 = act ? a.off[i + 1] : 0;
-        const PosT xi = act ? pos[i] : PosT{};
+        const PosT xi = act ? pos[i - a.node_base] : PosT{};
 
         // ---- pass 1: moment sums ----
         double acc[NE];
@@ -75,7 +65,7 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
         int cidx = 0;
         for (int t = b0 + gl; t < b1; t += LPN, ++cidx) {
             const int j = a.nbr[t];
-            const PosT xj = pos[j];
+            const PosT xj = pos[j - a.node_base];
             const double dx = xj.x - xi.x, dy = xj.y - xi.y;
             double dz = 0.0;
             if constexpr (DIM == 3) dz = xj.z - xi.z;
@@ -132,8 +122,8 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
             for (int p = 0; p < NOP; ++p)
 #pragma unroll
                 for (int q = p; q < NOP; ++q) {
-                    sA[wib][p * NOP + q] = acc[e];
-                    sA[wib][q * NOP + p] = acc[e];
+                    sA[p * NOP + q] = acc[e];
+                    sA[q * NOP + p] = acc[e];
                     ++e;
                 }
         }
@@ -191,7 +181,7 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
             double sres = (p == kcol) ? fk : 0.0;
 #pragma unroll
             for (int q = 0; q < NOP; ++q) {
-                const double apq = sA[wib][p * NOP + q];
+                const double apq = sA[p * NOP + q];
                 sres -= apq * x[q];
                 maxA = fmax(maxA, fabs(apq));
             }
@@ -223,7 +213,7 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
         // X (column kcol in lane kcol) to shared memory: sX[a][k]
         if (gl < NOP) {
 #pragma unroll
-            for (int p = 0; p < NOP; ++p) sX[wib][p * NOP + gl] = zero_ops ? 0.0 : x[p];
+            for (int p = 0; p < NOP; ++p) sX[p * NOP + gl] = zero_ops ? 0.0 : x[p];
         }
         __syncwarp();
 
@@ -232,7 +222,7 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
         cidx = 0;
         for (int t = b0 + gl; t < b1; t += LPN, ++cidx) {
             const int j = a.nbr[t];
-            const PosT xj = pos[j];
+            const PosT xj = pos[j - a.node_base];
             const double dx = xj.x - xi.x, dy = xj.y - xi.y;
             double dz = 0.0;
             if constexpr (DIM == 3) dz = xj.z - xi.z;
@@ -263,16 +253,16 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
                 if (!live) return 0.0;
                 double sum = 0.0;
 #pragma unroll
-                for (int p = 0; p < NOP; ++p) sum += sX[wib][p * NOP + k] * m[p];
+                for (int p = 0; p < NOP; ++p) sum += sX[p * NOP + k] * m[p];
                 return sum * bwd * idpow[k];
             };
             if (a.ops) {
                 if constexpr (MIXED) {
-                    float *o = static_cast<float *>(a.ops) + (size_t)t * NOP;
+                    float *o = static_cast<float *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
 #pragma unroll
                     for (int k = 0; k < NOP; ++k) o[k] = (float)op(k);
                 } else {
-                    double *o = static_cast<double *>(a.ops) + (size_t)t * NOP;
+                    double *o = static_cast<double *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
 #pragma unroll
                     for (int k = 0; k < NOP; ++k) o[k] = op(k);
                 }
@@ -295,6 +285,24 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
             }
         }
         __syncwarp();
+    }
+}
+
+// single geometry: GPW = 32/LPN nodes per warp, grid-stride over the nodes
+template <int DIM, int ORDER, bool MIXED, int LPN>
+__global__ void __launch_bounds__(kGbuildThreads) gbuild_kernel(GBuildArgs a) {
+    constexpr int NOP = QTable<DIM, ORDER>::NOP;
+    constexpr int GPW = kWarp / LPN;
+    constexpr int GPB = (kGbuildThreads / kWarp) * GPW;  // node groups per block
+    __shared__ double sA[GPB][NOP * NOP];
+    __shared__ double sX[GPB][NOP * NOP];
+    const int lane = threadIdx.x & 31;
+    const int gl = lane & (LPN - 1);
+    const int wib = (threadIdx.x >> 5) * GPW + lane / LPN;  // node group index within the block
+    const long long stride = (long long)gridDim.x * GPB;
+    for (long long base = (long long)blockIdx.x * GPB + (threadIdx.x >> 5) * GPW; base < a.n + 0LL; base += stride) {
+        const int i = (int)(base + lane / LPN);
+        gbuild_group<DIM, ORDER, MIXED, LPN>(a, i, i < a.n, gl, sA[wib], sX[wib]);
     }
 }
 
@@ -324,6 +332,103 @@ cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, i
         case 2: return launch_order<3, 2, 32>(a, mixed, grid, s);
         default: return cudaErrorInvalidValue;
     }
+}
+
+// ---- batched clouds: persistent warps over a task table (order 2) --------------------------------------------
+// DIMS selects the task kinds this instantiation handles (1: 2D, 2: 3D, 3: both); a warp runs its task's nodes
+// 32/LPN at a time with the single-geometry group code, addressing the cloud's slices through node_base /
+// bond_base.
+template <bool MIXED, int LPN2, int LPN3, int DIMS>
+__global__ void __launch_bounds__(kGbuildThreads) gbuild_batch_kernel(BatchArgs b) {
+    constexpr int WPB = kGbuildThreads / kWarp;
+    constexpr int S2 = (kWarp / LPN2) * 25, S3 = (kWarp / LPN3) * 81;
+    constexpr int SLOT = (DIMS & 2) ? ((DIMS & 1) ? (S2 > S3 ? S2 : S3) : S3) : S2;
+    __shared__ double sA[WPB][SLOT];
+    __shared__ double sX[WPB][SLOT];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    for (;;) {
+        int task = 0;
+        if (lane == 0) task = (int)atomicAdd(b.counter, 1u);
+        task = __shfl_sync(kFull, task, 0);
+        if (task >= b.ntasks) break;
+        const BatchTask tk = b.tasks[b.task0 + task];
+        const BatchCloud cd = b.clouds[tk.cloud];
+        GBuildArgs a;
+        a.n = cd.node0 + cd.n;
+        a.off = b.off;
+        a.nbr = b.nbr;
+        a.pos = b.pos + cd.pos_off;
+        a.vol = b.vol;
+        a.delta = cd.delta;
+        a.dx_char = cd.dx_char;
+        a.ops = MIXED ? (void *)(static_cast<float *>(b.ops) + cd.ops_off) : (void *)(static_cast<double *>(b.ops) + cd.ops_off);
+        a.degenerate = b.degenerate;
+        a.n_degenerate = b.n_degenerate;
+        a.first_degenerate = b.first_degenerate;
+        a.node_base = cd.node0;
+        a.bond_base = cd.bond0;
+        if constexpr ((DIMS & 1) != 0) {
+            if (tk.dim == 2) {
+                constexpr int GPW = kWarp / LPN2;
+                const int gl = lane & (LPN2 - 1), grp = lane / LPN2;
+                for (int k0 = 0; k0 < tk.count; k0 += GPW) {
+                    const bool act = k0 + grp < tk.count;
+                    gbuild_group<2, 2, MIXED, LPN2>(a, tk.first + (act ? k0 + grp : 0), act, gl, &sA[w][grp * 25],
+                                                    &sX[w][grp * 25]);
+                }
+            }
+        }
+        if constexpr ((DIMS & 2) != 0) {
+            if (tk.dim == 3) {
+                constexpr int GPW = kWarp / LPN3;
+                const int gl = lane & (LPN3 - 1), grp = lane / LPN3;
+                for (int k0 = 0; k0 < tk.count; k0 += GPW) {
+                    const bool act = k0 + grp < tk.count;
+                    gbuild_group<3, 2, MIXED, LPN3>(a, tk.first + (act ? k0 + grp : 0), act, gl, &sA[w][grp * 81],
+                                                    &sX[w][grp * 81]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+BatchSchedule batch_gbuild_schedule(int v) {
+    switch (v) {
+        case 0: return {8, 32, false};
+        case 1: return {16, 32, false};
+        case 2: return {8, 16, false};
+        default: return {8, 32, true};
+    }
+}
+
+template <bool MIXED, int LPN2, int LPN3, int DIMS>
+static cudaError_t launch_gb(const BatchArgs &a, cudaStream_t s) {
+    auto k = gbuild_batch_kernel<MIXED, LPN2, LPN3, DIMS>;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kGbuildThreads, 0);
+    const long long want = ((long long)a.ntasks + (kGbuildThreads / kWarp) - 1) / (kGbuildThreads / kWarp);
+    const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    const int grid = (int)(want < cap ? (want > 0 ? want : 1) : cap);
+    k<<<grid, kGbuildThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <bool MIXED>
+static cudaError_t launch_gb_m(const BatchArgs &a, int variant, int dims, cudaStream_t s) {
+    switch (variant) {
+        case 0: return launch_gb<MIXED, 8, 32, 3>(a, s);
+        case 1: return launch_gb<MIXED, 16, 32, 3>(a, s);
+        case 2: return launch_gb<MIXED, 8, 16, 3>(a, s);
+        default: return dims == 1 ? launch_gb<MIXED, 8, 32, 1>(a, s) : launch_gb<MIXED, 8, 32, 2>(a, s);
+    }
+}
+
+cudaError_t launch_gbuild_batch(const BatchArgs &a, bool mixed, int variant, int dims, cudaStream_t s) {
+    return mixed ? launch_gb_m<true>(a, variant, dims, s) : launch_gb_m<false>(a, variant, dims, s);
 }
 
 bool gbuild_supported(int dim, int order) { return (dim == 2 && order >= 1 && order <= 3) || (dim == 3 && order >= 1 && order <= 2); }

@@ -25,9 +25,54 @@ struct GBuildArgs {
     uint8_t *degenerate = nullptr;
     unsigned int *n_degenerate = nullptr;
     int *first_degenerate = nullptr;
+    int node_base = 0;       // positions are read at pos[j - node_base] (a batch cloud's slice)
+    long long bond_base = 0; // AoS operators are written at ops[(t - bond_base) * nop]
 };
 cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, int grid, cudaStream_t s);
 bool gbuild_supported(int dim, int order);
+
+// ------------------------------------------------------------------------------------------ batched clouds
+// Many independent clouds (2D and 3D mixed) in one node/bond numbering: cloud c owns nodes [node0, node0+n) and
+// bonds [bond0, bond0+nb) of the global CSR; its operators (order 2: nop 5 in 2D, 9 in 3D, AoS [nb][nop]) start
+// at element ops_off, its apply output ([n][nop]) at element out_off, its positions (double2 in 2D, double4 in
+// 3D) at byte pos_off.  A task is a run of consecutive nodes of one cloud; persistent warps take tasks from a
+// counter (zero at launch).
+struct BatchCloud {
+    int dim = 2, node0 = 0, n = 0, pad = 0;
+    long long bond0 = 0, nb = 0;
+    long long ops_off = 0, out_off = 0, pos_off = 0;
+    double delta = 0.0, dx_char = 0.0;
+};
+struct BatchTask {
+    int cloud = 0, first = 0, count = 0, dim = 2;
+};
+struct BatchArgs {
+    int task0 = 0, ntasks = 0;  // tasks [task0, task0 + ntasks) of the table
+    const BatchTask *tasks = nullptr;
+    const BatchCloud *clouds = nullptr;
+    const int *off = nullptr;
+    const int *nbr = nullptr;  // 0-based global node ids
+    const unsigned char *pos = nullptr;
+    const double *vol = nullptr;
+    void *ops = nullptr;  // double, or float when mixed
+    uint8_t *degenerate = nullptr;
+    unsigned int *n_degenerate = nullptr;
+    int *first_degenerate = nullptr;
+    unsigned int *counter = nullptr;
+    const double *u = nullptr;  // apply: field (N)
+    double *out = nullptr;      // apply: derivatives
+};
+// schedules: lanes per node for 2D / 3D clouds, and whether both dimensions share one launch
+struct BatchSchedule {
+    int lpn2, lpn3;
+    bool split;
+};
+constexpr int kBatchVariants = 4;
+BatchSchedule batch_gbuild_schedule(int variant);
+BatchSchedule batch_apply_schedule(int variant);
+// dims: 1 = 2D tasks only, 2 = 3D tasks only, 3 = both
+cudaError_t launch_gbuild_batch(const BatchArgs &a, bool mixed, int variant, int dims, cudaStream_t s);
+cudaError_t launch_apply_batch(const BatchArgs &a, bool mixed, int variant, int dims, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------- explicit fracture
 enum EpfMode { EPF_RATE = 0, EPF_START = 1, EPF_STEP = 2, EPF_FORCE_FROZEN = 3 };

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/perix_b200.h"
+#include "k_kernels.h"
 
 namespace pxb {
 
@@ -148,6 +149,20 @@ struct ChState {
 
 }  // namespace pxb
 
+namespace pxb {
+// Batched clouds (C-ABI pxb_batch_*): concatenated geometry, task table, operators of every cloud.
+struct BatchState {
+    bool ready = false, built = false;
+    int nclouds = 0, n = 0;
+    long long nb = 0, ops_len = 0, out_len = 0;
+    int ntasks = 0, ntasks3 = 0;  // tasks of 3D clouds first: [0, ntasks3), then 2D
+    int precision = PXB_FP64;
+    int gvariant = 3, avariant = 0;  // schedules (batch_gbuild_schedule / batch_apply_schedule)
+    std::vector<BatchCloud> h_clouds;
+    DevBuf clouds, tasks, off, nbr, pos, vol, ops, degenerate, counters;
+};
+}  // namespace pxb
+
 struct pxb_ctx {
     int device = 0;
     cudaStream_t own = nullptr;
@@ -158,6 +173,7 @@ struct pxb_ctx {
     pxb::EpfState epf;
     pxb::CsrState csr;
     pxb::ChState ch;
+    pxb::BatchState batch;
     pxb::DevBuf scratch;
     pxb::PinnedBuf pinned;
 };
@@ -172,4 +188,5 @@ int ensure_pinned(PinnedBuf &b, size_t bytes);
 int sync(pxb_ctx *c);
 int check_launch(pxb_ctx *c, const char *what);
 size_t ctx_bytes(const pxb_ctx *c);
+int l2_flush(pxb_ctx *c, size_t bytes);  // writes `bytes` through the L2 on the context stream (0: nothing)
 }  // namespace pxb

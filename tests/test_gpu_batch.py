@@ -1,0 +1,113 @@
+"""Batched clouds (pxb_batch_*): 2D and 3D jittered-lattice clouds of uneven size in one launch, against the C
+restatement (oracle) run cloud by cloud.  FP64 g-functions and applies within 1e-12 (family-scaled); mixed
+precision within 1e-6 on g and within the stated per-order bounds on the apply; every schedule gives the same
+result; a degenerate family is reported with its cloud and node."""
+import numpy as np
+import pytest
+
+from conftest import scaled_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def batch(port):
+    import perix_b200 as px
+    from bench import c3_clouds, cubic_field
+    clouds = c3_clouds(px, nclouds=12, nmin=300, nmax=4000, seed=11)
+    u, exact = cubic_field(clouds, seed=3)
+    ref_g, ref_d = [], []
+    for c, f in zip(clouds, u):
+        g, deg = port.gbuild(c["dim"], 2, c["coords3"], c["vols"], c["off"], c["ids"], c["delta"], c["dx_char"])
+        assert deg.sum() == 0
+        ref_g.append(g)
+        ref_d.append(port.apply(c["off"], c["ids"], g, f))
+    return clouds, np.concatenate(u), exact, ref_g, ref_d
+
+
+def _build(ctx, clouds, precision, gvariant=None):
+    ctx.batch_set(clouds)
+    if gvariant is not None:
+        ctx.batch_set_variant(0, gvariant)
+    nd, first = ctx.batch_gbuild(precision)
+    assert nd == 0
+    return ctx
+
+
+@pytest.mark.parametrize("gvariant", [0, 1, 2, 3])
+def test_batch_gbuild_fp64_matches_oracle(ctx, batch, gvariant):
+    clouds, _, _, ref_g, _ = batch
+    _build(ctx, clouds, 0, gvariant)
+    assert {c["dim"] for c in clouds} == {2, 3}
+    for k, c in enumerate(clouds):
+        assert scaled_err(ctx.batch_get_ops(k), ref_g[k], c["off"]) <= 1e-12
+
+
+@pytest.mark.parametrize("avariant", [0, 1, 2, 3])
+def test_batch_apply_fp64_matches_oracle(ctx, batch, avariant):
+    clouds, u, _, _, ref_d = batch
+    _build(ctx, clouds, 0)
+    ctx.batch_set_variant(1, avariant)
+    got = ctx.batch_split(ctx.batch_apply(u))
+    for k in range(len(clouds)):
+        scale = np.abs(ref_d[k]).max(axis=0)
+        assert (np.abs(got[k] - ref_d[k]).max(axis=0) <= 1e-12 * scale + 1e-300).all()
+
+
+def test_batch_mixed_within_bounds(ctx, batch):
+    clouds, u, _, ref_g, ref_d = batch
+    _build(ctx, clouds, 1)
+    for k, c in enumerate(clouds):
+        assert scaled_err(ctx.batch_get_ops(k), ref_g[k], c["off"]) <= 1e-6
+    got = ctx.batch_split(ctx.batch_apply(u))
+    for k, c in enumerate(clouds):
+        nd1 = c["dim"]  # first-derivative slots come first
+        scale = np.abs(ref_d[k]).max(axis=0)
+        err = np.abs(got[k] - ref_d[k]).max(axis=0) / scale
+        assert err[:nd1].max() <= 1e-6
+        assert err[nd1:].max() <= 5e-5
+
+
+def test_batch_derivatives_of_cubics(ctx, batch):
+    """Order-2 PDDO reproduces a cubic's derivatives up to truncation error (measured with the oracle on these
+    clouds): at nodes 4h inside the cloud, first derivatives within 3% and second within 10% of the exact
+    derivative's scale; at every node, including the truncated families at the cloud boundary (the clouds have
+    no ghosts), within 5% and 50%."""
+    clouds, u, exact, _, _ = batch
+    _build(ctx, clouds, 0)
+    got = ctx.batch_split(ctx.batch_apply(u))
+    for k, c in enumerate(clouds):
+        d = c["dim"]
+        scale = np.abs(exact[k]).max(axis=0)
+        x = c["coords3"][:, :d]
+        lo, hi = x.min(axis=0), x.max(axis=0)
+        inner = np.all((x > lo + 4 * c["dx_char"]) & (x < hi - 4 * c["dx_char"]), axis=1)
+        err = np.abs(got[k] - exact[k]).max(axis=0) / scale
+        assert err[:d].max() <= 0.05 and err[d:].max() <= 0.5
+        if inner.any():
+            err = np.abs(got[k][inner] - exact[k][inner]).max(axis=0) / scale
+            assert err[:d].max() <= 0.03 and err[d:].max() <= 0.1
+
+
+def test_batch_reports_degenerate_cloud(ctx, batch):
+    import perix_b200 as px
+    clouds = list(batch[0][:3])
+    # a 2D cloud of three collinear nodes: its families cannot support five order-2 operators
+    xyz = np.array([[0.0, 0.0, 0.0], [1e-3, 0.0, 0.0], [2e-3, 0.0, 0.0]])
+    off, ids = px.families(xyz, 3.015e-3, False)
+    clouds.append(dict(dim=2, coords3=xyz, vols=np.full(3, 1e-6), off=off, ids=ids, delta=3.015e-3, dx_char=1e-3))
+    ctx.batch_set(clouds)
+    with pytest.raises(px.PxbError) as e:
+        ctx.batch_gbuild(0)
+    assert e.value.status == 3 and "cloud 3" in str(e.value)
+
+
+def test_batch_rejects_foreign_ids(ctx, batch):
+    import perix_b200 as px
+    clouds = [dict(c) for c in batch[0][:2]]
+    ids = clouds[1]["ids"].copy()
+    ids[0] = clouds[1]["vols"].size + 1  # beyond its own cloud
+    clouds[1]["ids"] = ids
+    with pytest.raises(px.PxbError) as e:
+        ctx.batch_set(clouds)
+    assert e.value.status == 1 and "cloud 1" in str(e.value)
