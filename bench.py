@@ -479,6 +479,57 @@ def run_perix(args):
         dist.destroy_process_group()
 
 
+def c3_measure(px, nclouds=256, reps=3, device=0):
+    """Batched clouds: one context holds every cloud; the g-build (FP64, then mixed) and the all-derivative apply
+    are autotuned over their schedules and timed with CUDA events (L2 flushed before each launch).  Errors: the
+    mixed g-functions and derivatives against the FP64 ones, and the FP64 derivatives of the random cubics
+    against the exact ones (order-2 truncation error, reported, not a precision claim)."""
+    import torch
+    t0 = time.perf_counter()
+    clouds = c3_clouds(px, nclouds=nclouds)
+    fields, exact = cubic_field(clouds)
+    t_setup = time.perf_counter() - t0
+    ctx = px.Context(device)
+    ctx.batch_set(clouds)
+    dev = torch.device("cuda", device)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    u = torch.from_numpy(np.concatenate(fields)).to(dev)
+    out = torch.empty(ctx.batch_out_len, dtype=torch.float64, device=dev)
+    res = {"clouds": nclouds, "nodes": ctx.batch_n, "bonds": ctx.batch_nb,
+           "dims": {"2d": sum(1 for c in clouds if c["dim"] == 2), "3d": sum(1 for c in clouds if c["dim"] == 3)},
+           "host_setup_s": t_setup}
+    derivs = {}
+    for prec, p in (("fp64", px.FP64), ("mixed", px.MIXED)):
+        ctx.batch_gbuild(p)
+        gbest, gms = ctx.batch_autotune(0, reps=reps, flush_bytes=FLUSH_BYTES)
+        ctx.batch_gbuild(p)
+        abest, ams = ctx.batch_autotune(1, reps=reps, flush_bytes=FLUSH_BYTES, u_ptr=u.data_ptr(), out_ptr=out.data_ptr())
+        ctx.batch_apply_d(u.data_ptr(), out.data_ptr())
+        torch.cuda.synchronize(dev)
+        derivs[prec] = out.cpu().numpy()
+        g_ms, a_ms = float(gms[gbest]), float(ams[abest])
+        res[prec] = {"gbuild_nodes_per_s": ctx.batch_n / (g_ms * 1e-3), "gbuild_ms": g_ms, "gbuild_schedule": gbest,
+                     "gbuild_ms_per_schedule": [round(float(x), 4) for x in gms],
+                     "apply_ms": a_ms, "apply_schedule": abest,
+                     "apply_ms_per_schedule": [round(float(x), 4) for x in ams]}
+    d64 = ctx.batch_split(derivs["fp64"])
+    d32 = ctx.batch_split(derivs["mixed"])
+    mixed_err, trunc = 0.0, {"2d": [0.0, 0.0], "3d": [0.0, 0.0]}
+    for k, c in enumerate(clouds):
+        dim = c["dim"]
+        scale = np.abs(d64[k]).max(axis=0)
+        mixed_err = max(mixed_err, float((np.abs(d32[k] - d64[k]).max(axis=0) / scale)[:dim].max()))
+        esc = np.abs(exact[k]).max(axis=0)
+        e = np.abs(d64[k] - exact[k]).max(axis=0) / esc
+        key = "%dd" % dim
+        trunc[key][0] = max(trunc[key][0], float(e[:dim].max()))
+        trunc[key][1] = max(trunc[key][1], float(e[dim:].max()))
+    res["mixed_first_derivative_rel_err_vs_fp64"] = mixed_err
+    res["truncation_err_vs_exact_cubics"] = {k: {"first": v[0], "second": v[1]} for k, v in trunc.items()}
+    ctx.close()
+    return res
+
+
 def run_profile(args):
     """One kernel family on the plate, for profiler captures.  --profile step: the plate runs 100 steps with
     variant 1, then --steps timed steps of variant --variant from that state (so that variant's step kernel is
@@ -488,6 +539,10 @@ def run_profile(args):
     ctx = px.Context(0)
     L = w["L"]
     ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
+    if args.profile == "c3":
+        print(json.dumps({"profile": "c3", **c3_measure(px, nclouds=args.steps)}))
+        ctx.close()
+        return
     if args.profile == "gbuild":
         gb, ms = gbuild_rate(px, ctx, args.precision, reps=args.steps)
         print(json.dumps({"profile": "gbuild", "precision": args.precision, "nodes_per_s": gb, "ms": ms}))
@@ -515,7 +570,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="perix", choices=["perix", "reference"])
-    ap.add_argument("--profile", choices=["step", "gbuild"], default=None,
+    ap.add_argument("--profile", choices=["step", "gbuild", "c3"], default=None,
                     help="run one kernel family only (for profiler captures); prints its own JSON line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--variant", type=int, default=8)

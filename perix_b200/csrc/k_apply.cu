@@ -135,13 +135,13 @@ __device__ __forceinline__ void apply_batch_group(const BatchArgs &b, const Batc
 #pragma unroll
         for (int k = 0; k < NOP; ++k) acc[k] = cacc[k].value();
     }
-    double mine = 0.0;
+    // lane gl writes the derivatives k = gl, gl + LPN, ... (groups narrower than nop write several)
+    double *o = b.out + cd.out_off + (size_t)(i - cd.node0) * NOP;
 #pragma unroll
     for (int k = 0; k < NOP; ++k) {
         const double v = group_sum<LPN>(acc[k]);
-        if (gl == k) mine = v;
+        if (act && gl == (k & (LPN - 1))) o[k] = v;
     }
-    if (act && gl < NOP) b.out[cd.out_off + (size_t)(i - cd.node0) * NOP + gl] = mine;
 }
 
 template <bool MIXED, int LPN2, int LPN3, int DIMS>
