@@ -508,23 +508,47 @@ def c3_measure(px, nclouds=256, reps=3, device=0):
         torch.cuda.synchronize(dev)
         derivs[prec] = out.cpu().numpy()
         g_ms, a_ms = float(gms[gbest]), float(ams[abest])
+        s_b = 4 if prec == "mixed" else 8
+        # apply bytes per launch: nb*(4 B id + nop*s B g) + N*(8 B u + 8*nop B out) per cloud (u_j gathers: L2);
+        # mixed adds the per-node FP32 first-moment defects of the second-derivative operators
+        a_bytes = sum(int(c["off"][-1]) * (4 + (9 if c["dim"] == 3 else 5) * s_b) +
+                      c["vols"].size * (8 + 8 * (9 if c["dim"] == 3 else 5)) +
+                      (c["vols"].size * (18 if c["dim"] == 3 else 6) * 4 if prec == "mixed" else 0) for c in clouds)
+        hbm, _ = peaks()
         res[prec] = {"gbuild_nodes_per_s": ctx.batch_n / (g_ms * 1e-3), "gbuild_ms": g_ms, "gbuild_schedule": gbest,
                      "gbuild_ms_per_schedule": [round(float(x), 4) for x in gms],
-                     "apply_ms": a_ms, "apply_schedule": abest,
+                     "apply_ms": a_ms, "apply_schedule": abest, "apply_algorithmic_bytes": a_bytes,
+                     "apply_achieved_gbs": a_bytes / (a_ms * 1e-3) / 1e9,
+                     "apply_frac_of_measured_hbm": a_bytes / (a_ms * 1e-3) / 1e9 / hbm,
                      "apply_ms_per_schedule": [round(float(x), 4) for x in ams]}
     d64 = ctx.batch_split(derivs["fp64"])
     d32 = ctx.batch_split(derivs["mixed"])
-    mixed_err, trunc = 0.0, {"2d": [0.0, 0.0], "3d": [0.0, 0.0]}
+    trunc = {"2d": [0.0, 0.0], "3d": [0.0, 0.0]}
+    # mixed vs FP64, first / second derivatives: max |error| over the cloud relative to (a) the same slot's max
+    # |value| over the cloud, (b) the max over the slots of that order (gradient / Hessian magnitude), (c) L2
+    errs = {"per_slot": [0.0, 0.0], "per_order": [0.0, 0.0], "l2": [0.0, 0.0]}
+    worst = None
     for k, c in enumerate(clouds):
         dim = c["dim"]
-        scale = np.abs(d64[k]).max(axis=0)
-        mixed_err = max(mixed_err, float((np.abs(d32[k] - d64[k]).max(axis=0) / scale)[:dim].max()))
+        diff = np.abs(d32[k] - d64[k])
+        for o, sl in enumerate((slice(0, dim), slice(dim, None))):
+            a, b = diff[:, sl], np.abs(d64[k][:, sl])
+            ps = float((a.max(axis=0) / b.max(axis=0)).max())
+            po = float(a.max() / b.max())
+            l2 = float(np.sqrt((a ** 2).sum() / (b ** 2).sum()))
+            if o == 0 and (worst is None or ps > worst[0]):
+                worst = (ps, k, dim, int(c["vols"].size))
+            for key, v in (("per_slot", ps), ("per_order", po), ("l2", l2)):
+                errs[key][o] = max(errs[key][o], v)
+    for k, c in enumerate(clouds):
+        dim = c["dim"]
         esc = np.abs(exact[k]).max(axis=0)
         e = np.abs(d64[k] - exact[k]).max(axis=0) / esc
         key = "%dd" % dim
         trunc[key][0] = max(trunc[key][0], float(e[:dim].max()))
         trunc[key][1] = max(trunc[key][1], float(e[dim:].max()))
-    res["mixed_first_derivative_rel_err_vs_fp64"] = mixed_err
+    res["mixed_rel_err_vs_fp64"] = {key: {"first": v[0], "second": v[1]} for key, v in errs.items()}
+    res["mixed_rel_err_vs_fp64"]["worst_first_per_slot_cloud"] = {"cloud": worst[1], "dim": worst[2], "nodes": worst[3]}
     res["truncation_err_vs_exact_cubics"] = {k: {"first": v[0], "second": v[1]} for k, v in trunc.items()}
     ctx.close()
     return res

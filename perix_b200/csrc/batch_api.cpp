@@ -43,6 +43,7 @@ BatchArgs batch_args(pxb_ctx *c) {
     unsigned *cnt = b.counters.as<unsigned>();
     a.n_degenerate = cnt + 2;
     a.first_degenerate = reinterpret_cast<int *>(cnt + 3);
+    a.defect = (b.precision == PXB_MIXED && b.defect.p) ? b.defect.as<float>() : nullptr;
     return a;
 }
 
@@ -130,7 +131,7 @@ extern "C" int pxb_batch_set(pxb_ctx *c, int nclouds, const int *dims, const int
     b.h_clouds.resize((size_t)nclouds);
     // cloud table, global 0-based neighbour ids, packed positions
     std::vector<int> nbr((size_t)std::max(1LL, nb));
-    long long ops_off = 0, out_off = 0, pos_off = 0;
+    long long ops_off = 0, out_off = 0, pos_off = 0, def_off = 0;
     for (int k = 0; k < nclouds; ++k) {
         BatchCloud &cd = b.h_clouds[(size_t)k];
         cd.dim = dims[k];
@@ -143,7 +144,9 @@ extern "C" int pxb_batch_set(pxb_ctx *c, int nclouds, const int *dims, const int
         cd.ops_off = ops_off;
         cd.out_off = out_off;
         cd.pos_off = pos_off;
+        cd.def_off = def_off;
         const int nop = nop_of_dim(cd.dim);
+        def_off += (long long)cd.n * (nop - cd.dim) * cd.dim;
         ops_off += cd.nb * nop;
         out_off += (long long)cd.n * nop;
         pos_off += ((long long)cd.n * (cd.dim == 3 ? 32 : 16) + 31) / 32 * 32;
@@ -157,6 +160,7 @@ extern "C" int pxb_batch_set(pxb_ctx *c, int nclouds, const int *dims, const int
     }
     b.ops_len = ops_off;
     b.out_len = out_off;
+    b.def_len = def_off;
     std::vector<double> pos((size_t)(pos_off / 8), 0.0);
     for (const BatchCloud &cd : b.h_clouds) {
         double *p = pos.data() + cd.pos_off / 8;
@@ -207,6 +211,11 @@ extern "C" int pxb_batch_gbuild(pxb_ctx *c, int precision, int *n_degenerate, in
     const size_t es = precision == PXB_MIXED ? 4 : 8;
     PXB_TRY(dev_alloc(c, b.ops, es * (size_t)std::max(1LL, b.ops_len)));
     PXB_TRY(dev_alloc(c, b.degenerate, (size_t)b.n));
+    b.defect = DevBuf{};
+    if (precision == PXB_MIXED) {
+        PXB_TRY(dev_alloc(c, b.defect, sizeof(float) * (size_t)std::max(1LL, b.def_len)));
+        PXB_CUDA_TRY(cudaMemsetAsync(b.defect.p, 0, b.defect.bytes, c->stream));
+    }
     unsigned *cnt = b.counters.as<unsigned>();
     const unsigned init[2] = {0u, (unsigned)INT_MAX};
     PXB_TRY(h2d(c, cnt + 2, init, sizeof(init)));

@@ -102,7 +102,7 @@ size_t ctx_bytes(const pxb_ctx *c) {
     size_t s = 0;
     const Geometry &g = c->g;
     s += bufsz(g.off) + bufsz(g.nbr) + bufsz(g.pos) + bufsz(g.vol) + bufsz(g.mirror) + bufsz(g.layer) + bufsz(g.rev);
-    s += bufsz(c->ops.ops) + bufsz(c->ops.degenerate);
+    s += bufsz(c->ops.ops) + bufsz(c->ops.degenerate) + bufsz(c->ops.defect) + bufsz(c->ops.yeff);
     const EpfState &e = c->epf;
     s += bufsz(e.G) + bufsz(e.P) + bufsz(e.health) + bufsz(e.u[0]) + bufsz(e.u[1]) + bufsz(e.accel) + bufsz(e.counters) +
          bufsz(e.umax) + bufsz(e.tsched);
@@ -110,7 +110,7 @@ size_t ctx_bytes(const pxb_ctx *c) {
          bufsz(e.bc.vals);
     const BatchState &bt = c->batch;
     s += bufsz(bt.clouds) + bufsz(bt.tasks) + bufsz(bt.off) + bufsz(bt.nbr) + bufsz(bt.pos) + bufsz(bt.vol) +
-         bufsz(bt.ops) + bufsz(bt.degenerate) + bufsz(bt.counters);
+         bufsz(bt.ops) + bufsz(bt.degenerate) + bufsz(bt.counters) + bufsz(bt.defect);
     const CsrState &k = c->csr;
     s += bufsz(k.rowptr) + bufsz(k.cols) + bufsz(k.slot) + bufsz(k.diag) + bufsz(k.kvals) + bufsz(k.rhs) +
          bufsz(k.u) + bufsz(k.uold) + bufsz(k.fnode) + bufsz(k.mnode);
@@ -293,7 +293,7 @@ static int ensure_rev(pxb_ctx *c) {
 
 // ===================================================================================================== g-build
 static GBuildArgs gbuild_args(pxb_ctx *c, void *ops_out, void *G_out, uint8_t *deg_out, unsigned int *nd,
-                              int *first) {
+                              int *first, float *defect = nullptr) {
     Geometry &g = c->g;
     GBuildArgs a;
     a.n = g.n;
@@ -310,11 +310,12 @@ static GBuildArgs gbuild_args(pxb_ctx *c, void *ops_out, void *G_out, uint8_t *d
     a.degenerate = deg_out;
     a.n_degenerate = nd;
     a.first_degenerate = first;
+    a.defect = defect;
     return a;
 }
 
 static int run_gbuild(pxb_ctx *c, int order, bool mixed, void *ops_out, void *G_out, uint8_t *deg_out,
-                      int *n_degenerate, int *first_degenerate) {
+                      int *n_degenerate, int *first_degenerate, float *defect = nullptr) {
     Geometry &g = c->g;
     if (!gbuild_supported(g.dim, order))
         return fail(PXB_ERR_UNSUPPORTED, "pxb_gbuild: order " + std::to_string(order) + " not built for dim " +
@@ -326,7 +327,7 @@ static int run_gbuild(pxb_ctx *c, int order, bool mixed, void *ops_out, void *G_
     PXB_CUDA_TRY(cudaMemsetAsync(nd, 0, 4, c->stream));
     const int big = std::numeric_limits<int>::max();
     PXB_TRY(h2d(c, first, &big, sizeof(int)));
-    const GBuildArgs a = gbuild_args(c, ops_out, G_out, deg_out, nd, first);
+    const GBuildArgs a = gbuild_args(c, ops_out, G_out, deg_out, nd, first, defect);
     cudaError_t e = launch_gbuild(a, g.dim, order, mixed, grid_nodes(g.n, kGbuildThreads), c->stream);
     c->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "gbuild launch");
@@ -365,8 +366,15 @@ extern "C" int pxb_gbuild(pxb_ctx *c, int order, int precision, int *n_degenerat
             else
                 o.pqr.insert(o.pqr.end(), {p, k - p, 0});
         }
+    float *defect = nullptr;
+    o.defect = DevBuf{};
+    if (precision == PXB_MIXED && order == 2) {
+        PXB_TRY(dev_alloc(c, o.defect, sizeof(float) * (size_t)c->g.n * (size_t)((nop - c->g.dim) * c->g.dim)));
+        PXB_CUDA_TRY(cudaMemsetAsync(o.defect.p, 0, o.defect.bytes, c->stream));
+        defect = o.defect.as<float>();
+    }
     const int st = run_gbuild(c, order, precision == PXB_MIXED, o.ops.p, nullptr, o.degenerate.as<uint8_t>(),
-                              n_degenerate, first_degenerate);
+                              n_degenerate, first_degenerate, defect);
     if (st == PXB_OK || st == PXB_ERR_DEGENERATE) o.ready = true;  // degenerate rows carry zero operators
     return st;
 }
@@ -380,7 +388,8 @@ int gbuild_launch_only(pxb_ctx *c, int order, int precision) {
     PXB_TRY(scratch(c, 16, &tmp));
     const GBuildArgs a = gbuild_args(c, c->ops.ops.p, nullptr, c->ops.degenerate.as<uint8_t>(),
                                      static_cast<unsigned int *>(tmp),
-                                     reinterpret_cast<int *>(static_cast<char *>(tmp) + 8));
+                                     reinterpret_cast<int *>(static_cast<char *>(tmp) + 8),
+                                     c->ops.defect.p ? c->ops.defect.as<float>() : nullptr);
     cudaError_t e = launch_gbuild(a, c->g.dim, order, precision == PXB_MIXED, grid_nodes(c->g.n, kGbuildThreads),
                                   c->stream);
     c->launches++;
@@ -426,6 +435,8 @@ static int apply_args(pxb_ctx *c, int nk, const int *slots, ApplyArgs &a, const 
     a.off = c->g.off.as<int>();
     a.nbr = c->g.nbr.as<int>();
     a.ops = c->ops.ops.p;
+    a.dim = c->g.dim;
+    a.defect = c->ops.defect.p ? c->ops.defect.as<float>() : nullptr;
     return PXB_OK;
 }
 
@@ -461,6 +472,34 @@ extern "C" int pxb_apply_adjoint_d(pxb_ctx *c, const double *ybar_d, int nk, con
     a.rev = c->g.rev.as<int>();
     a.u = ybar_d;
     a.out = ubar_d;
+    bool second = false;
+    for (int s = 0; s < nk; ++s) second |= slots[s] >= c->g.dim;
+    if (a.defect && second) {
+        // transpose of the defect correction: first-derivative slots join the scatter with corrected ybar
+        AdjPrepArgs p;
+        p.n = a.n;
+        p.dim = c->g.dim;
+        p.nop = a.nop;
+        p.nk = nk;
+        p.next = nk;
+        for (int s = 0; s < nk; ++s) p.slots[s] = p.ext[s] = slots[s];
+        for (int m = 0; m < c->g.dim; ++m) {
+            bool have = false;
+            for (int s = 0; s < nk; ++s) have |= slots[s] == m;
+            if (!have) p.ext[p.next++] = m;
+        }
+        if (p.next > 20) return fail(PXB_ERR_INVALID, "pxb_apply_adjoint: too many slots with the defect correction");
+        const size_t need = sizeof(double) * (size_t)a.n * (size_t)p.next;
+        if (c->ops.yeff.bytes < need) PXB_TRY(dev_alloc(c, c->ops.yeff, need));
+        p.defect = a.defect;
+        p.ybar = ybar_d;
+        p.yeff = c->ops.yeff.as<double>();
+        PXB_CUDA_TRY(launch_apply_adjoint_prep(p, c->stream));
+        PXB_TRY(check_launch(c, "apply_adjoint (defect transpose)"));
+        a.nk = p.next;
+        for (int s = 0; s < p.next; ++s) a.slots[s] = p.ext[s];
+        a.u = p.yeff;
+    }
     launch_apply_adjoint(a, c->ops.precision == PXB_MIXED, grid_nodes(a.n, kApplyThreads), c->stream);
     return check_launch(c, "apply_adjoint");
 }

@@ -1,6 +1,7 @@
 // Family-sum derivative apply D^k u_i = sum_j g^k_ij (u_j - u_i) and its transpose (reference pattern:
 // PoissonElement::computeNodalProjection, src/ElmtSystem/PoissonElement.cpp:67-105; V_j is baked into g).
 // Plus the small utility kernels (reverse-bond map, layout packing, health conversion, L2 flush).
+#include <algorithm>
 #include <type_traits>
 
 #include "k_kernels.h"
@@ -10,37 +11,34 @@ namespace pxb {
 
 constexpr int kMaxK = 20;
 
+// MIXED: FP32-stored operators widened to FP64 for the products and sums (HBM-bound: the arithmetic is free);
+// with a.defect (mixed, order 2) every requested second derivative is corrected by the first-moment defect of
+// its stored operator, D^k -= sum_m defect[k][m] D^m, the first derivatives D^m being summed alongside.
 template <bool MIXED>
 __global__ void __launch_bounds__(kApplyThreads) apply_kernel(ApplyArgs a) {
     constexpr int WPB = kApplyThreads / kWarp;
+    using GT = typename std::conditional<MIXED, float, double>::type;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
+    const GT *ops = static_cast<const GT *>(a.ops);
     for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
         const int b0 = a.off[i], b1 = a.off[i + 1];
         const double ui = a.u[i];
-        double acc[kMaxK];
-        CompF cacc[MIXED ? kMaxK : 1];
+        double acc[kMaxK], d1[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int s = 0; s < kMaxK; ++s) acc[s] = 0.0;
         for (int t = b0 + lane; t < b1; t += kWarp) {
             const int j = __ldg(a.nbr + t);
             const double du = a.u[j] - ui;
-            if constexpr (MIXED) {
-                const float *g = static_cast<const float *>(a.ops) + (size_t)t * a.nop;
-                const float duf = (float)du;
+            const GT *g = ops + (size_t)t * a.nop;
 #pragma unroll
-                for (int s = 0; s < kMaxK; ++s)
-                    if (s < a.nk) cacc[s].add(__ldg(g + a.slots[s]) * duf);
-            } else {
-                const double *g = static_cast<const double *>(a.ops) + (size_t)t * a.nop;
+            for (int s = 0; s < kMaxK; ++s)
+                if (s < a.nk) acc[s] = fma((double)__ldg(g + a.slots[s]), du, acc[s]);
+            if (a.defect) {
 #pragma unroll
-                for (int s = 0; s < kMaxK; ++s)
-                    if (s < a.nk) acc[s] += __ldg(g + a.slots[s]) * du;
+                for (int m = 0; m < 3; ++m)
+                    if (m < a.dim) d1[m] = fma((double)__ldg(g + m), du, d1[m]);
             }
-        }
-        if constexpr (MIXED) {
-#pragma unroll
-            for (int s = 0; s < kMaxK; ++s) acc[s] = cacc[s].value();
         }
         double mine = 0.0;
 #pragma unroll
@@ -50,11 +48,45 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(ApplyArgs a) {
                 if (lane == s) mine = v;
             }
         }
+        if (a.defect) {
+#pragma unroll
+            for (int m = 0; m < 3; ++m) d1[m] = (m < a.dim) ? group_sum<kWarp>(d1[m]) : 0.0;
+            if (lane < a.nk && a.slots[lane] >= a.dim) {
+                const int nd = (a.nop - a.dim) * a.dim;
+                const float *dv = a.defect + (size_t)i * nd + (a.slots[lane] - a.dim) * a.dim;
+                for (int m = 0; m < a.dim; ++m) mine -= (double)dv[m] * d1[m];
+            }
+        }
         if (lane < a.nk) a.out[(size_t)i * a.nk + lane] = mine;
     }
 }
 
-// ubar_m = sum_{t in fam(m)} [ sum_s g_{rev t}^s ybar_{j,s} - sum_s g_t^s ybar_{m,s} ]
+// Transpose of the defect correction, ahead of the transpose scatter: the corrected forward is
+// D = G u - C (G1 u) with G1 the first-derivative rows, so ubar = G^T ybar' where ybar' equals ybar on the
+// requested slots and every first-derivative slot m additionally receives -sum_k C[k][m] ybar[k].  p.ext lists
+// the scatter's slots (the requested ones, then any first-derivative slot not requested); yeff is N x next.
+__global__ void apply_adjoint_prep_kernel(AdjPrepArgs p) {
+    const int nd = (p.nop - p.dim) * p.dim;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += gridDim.x * blockDim.x) {
+        double *y = p.yeff + (size_t)i * p.next;
+        for (int e = 0; e < p.next; ++e) y[e] = e < p.nk ? p.ybar[(size_t)i * p.nk + e] : 0.0;
+        for (int s = 0; s < p.nk; ++s) {
+            const int k = p.slots[s];
+            if (k < p.dim) continue;
+            const double yk = p.ybar[(size_t)i * p.nk + s];
+            const float *dv = p.defect + (size_t)i * nd + (k - p.dim) * p.dim;
+            for (int e = 0; e < p.next; ++e)
+                if (p.ext[e] < p.dim) y[e] -= (double)dv[p.ext[e]] * yk;
+        }
+    }
+}
+
+cudaError_t launch_apply_adjoint_prep(const AdjPrepArgs &p, cudaStream_t s) {
+    const int grid = (int)std::min<long long>(((long long)p.n + 255) / 256, 148LL * 8);
+    apply_adjoint_prep_kernel<<<grid > 0 ? grid : 1, 256, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(kApplyThreads) apply_adjoint_kernel(ApplyArgs a) {
     constexpr int WPB = kApplyThreads / kWarp;
@@ -105,43 +137,44 @@ cudaError_t launch_apply_adjoint(const ApplyArgs &a, bool mixed, int grid, cudaS
 
 // ---- batched clouds: all order-2 derivatives of a scalar field, every cloud in one persistent launch -----------
 // D^k u_i = sum_t g^k_t (u_j - u_i) for k < nop (5 in 2D, 9 in 3D); LPN lanes per node stride the family
-// (coalesced reads of consecutive operator rows), a butterfly over the group reduces the nop sums.  MIXED: g and
-// u_j - u_i in FP32 with two-sum accumulation.
+// (coalesced reads of consecutive operator rows), a butterfly over the group reduces the nop sums.
+// MIXED: the operators are stored in FP32 and widened; products and sums stay FP64 (the kernel is HBM-bound,
+// the arithmetic is free), and each second derivative is corrected by the first-moment defect of its stored
+// operator: D^k -= sum_m defect[k][m] D^m (GBuildArgs::defect).
 template <bool MIXED, int DIM, int LPN>
 __device__ __forceinline__ void apply_batch_group(const BatchArgs &b, const BatchCloud &cd, int i, bool act, int gl) {
     constexpr int NOP = DIM == 3 ? 9 : 5;
+    constexpr int ND = (NOP - DIM) * DIM;
     using GT = typename std::conditional<MIXED, float, double>::type;
     const GT *ops = static_cast<const GT *>(b.ops) + cd.ops_off;
     const int b0 = act ? b.off[i] : 0, b1 = act ? b.off[i + 1] : 0;
     const double ui = act ? b.u[i] : 0.0;
     double acc[NOP];
-    CompF cacc[MIXED ? NOP : 1];
 #pragma unroll
     for (int k = 0; k < NOP; ++k) acc[k] = 0.0;
     for (int t = b0 + gl; t < b1; t += LPN) {
         const int j = __ldg(b.nbr + t);
         const double du = __ldg(b.u + j) - ui;
         const GT *g = ops + (size_t)(t - cd.bond0) * NOP;
-        if constexpr (MIXED) {
-            const float duf = (float)du;
 #pragma unroll
-            for (int k = 0; k < NOP; ++k) cacc[k].add(__ldg(g + k) * duf);
-        } else {
-#pragma unroll
-            for (int k = 0; k < NOP; ++k) acc[k] = fma(__ldg(g + k), du, acc[k]);
-        }
+        for (int k = 0; k < NOP; ++k) acc[k] = fma((double)__ldg(g + k), du, acc[k]);
     }
-    if constexpr (MIXED) {
 #pragma unroll
-        for (int k = 0; k < NOP; ++k) acc[k] = cacc[k].value();
+    for (int k = 0; k < NOP; ++k) acc[k] = group_sum<LPN>(acc[k]);
+    if constexpr (MIXED) {
+        if (b.defect && act) {
+            const float *dv = b.defect + cd.def_off + (size_t)(i - cd.node0) * ND;
+#pragma unroll
+            for (int k = DIM; k < NOP; ++k)
+#pragma unroll
+                for (int m = 0; m < DIM; ++m) acc[k] -= (double)__ldg(dv + (k - DIM) * DIM + m) * acc[m];
+        }
     }
     // lane gl writes the derivatives k = gl, gl + LPN, ... (groups narrower than nop write several)
     double *o = b.out + cd.out_off + (size_t)(i - cd.node0) * NOP;
 #pragma unroll
-    for (int k = 0; k < NOP; ++k) {
-        const double v = group_sum<LPN>(acc[k]);
-        if (act && gl == (k & (LPN - 1))) o[k] = v;
-    }
+    for (int k = 0; k < NOP; ++k)
+        if (act && gl == (k & (LPN - 1))) o[k] = acc[k];
 }
 
 template <bool MIXED, int LPN2, int LPN3, int DIMS>
@@ -182,7 +215,9 @@ BatchSchedule batch_apply_schedule(int v) {
         case 0: return {8, 16, false};
         case 1: return {4, 16, false};
         case 2: return {8, 32, false};
-        default: return {8, 16, true};
+        case 3: return {8, 16, true};
+        case 4: return {16, 16, false};
+        default: return {4, 16, true};
     }
 }
 
@@ -206,7 +241,9 @@ static cudaError_t launch_ab_m(const BatchArgs &a, int variant, int dims, cudaSt
         case 0: return launch_ab<MIXED, 8, 16, 3>(a, s);
         case 1: return launch_ab<MIXED, 4, 16, 3>(a, s);
         case 2: return launch_ab<MIXED, 8, 32, 3>(a, s);
-        default: return dims == 1 ? launch_ab<MIXED, 8, 16, 1>(a, s) : launch_ab<MIXED, 8, 16, 2>(a, s);
+        case 3: return dims == 1 ? launch_ab<MIXED, 8, 16, 1>(a, s) : launch_ab<MIXED, 8, 16, 2>(a, s);
+        case 4: return launch_ab<MIXED, 16, 16, 3>(a, s);
+        default: return dims == 1 ? launch_ab<MIXED, 4, 16, 1>(a, s) : launch_ab<MIXED, 4, 16, 2>(a, s);
     }
 }
 

@@ -15,7 +15,12 @@
 //           (SoA, [c][bond]) used by the explicit fracture step.
 // MIXED: bond weights, monomials and moment products in FP32 with two-sum compensated accumulation on
 // delta-scaled bond vectors (the bond vector itself is formed in FP64); the factorisation, refinement and
-// g-evaluation stay in FP64; g is stored in FP32.
+// g-evaluation stay in FP64, the evaluation using the same FP32 weights and monomials that entered the moment
+// sums (so sum_j g_j m(xi_j) reproduces diag(q!) for the matrix actually factored); g is stored in FP32, and
+// at order 2 the first moments of the stored second-derivative operators are kept per node (the apply's
+// defect correction).  MIXED with SUMS64: the same FP32 storage and defects, with the moment sums in FP64
+// (on B200 an FP64 FMA costs less issue than an FP32 two-sum, so this variant is the faster and the more
+// accurate one; the batch autotuner may pick it).
 #include <cfloat>
 #include <type_traits>
 
@@ -28,7 +33,7 @@ namespace pxb {
 // lanes of the warp call this together).  i is the node (act false: idle group); sA and sX are this group's
 // nop x nop shared-memory slots.  Positions are read at pos[j - a.node_base] and the AoS operators written at
 // ops[(t - a.bond_base) * nop], so a batch of clouds can address one cloud's slices with global ids.
-template <int DIM, int ORDER, bool MIXED, int LPN>
+template <int DIM, int ORDER, bool MIXED, int LPN, bool SUMS64 = false>
 __device__ __forceinline__ void gbuild_group(const GBuildArgs &a, int i, bool act, int gl, double *sA, double *sX) {
     constexpr QTable<DIM, ORDER> Q{};
     constexpr int NOP = Q.NOP;
@@ -52,13 +57,13 @@ __device__ __forceinline__ void gbuild_group(const GBuildArgs &a, int i, bool ac
 
         // ---- pass 1: moment sums ----
         double acc[NE];
-        CompF cacc[MIXED ? NE : 1];
+        CompF cacc[(MIXED && !SUMS64) ? NE : 1];
 #pragma unroll
         for (int e = 0; e < NE; ++e) acc[e] = 0.0;
         int usable = 0;
         // weights of this lane's first KC bonds, reused by pass 2 (0 marks a skipped bond)
         constexpr int KC = 4;
-        using ET = typename std::conditional<MIXED, float, double>::type;
+        using ET = typename std::conditional<MIXED && !SUMS64, float, double>::type;
         ET wcache[KC];
 #pragma unroll
         for (int c = 0; c < KC; ++c) wcache[c] = ET(0);
@@ -71,7 +76,7 @@ __device__ __forceinline__ void gbuild_group(const GBuildArgs &a, int i, bool ac
             if constexpr (DIM == 3) dz = xj.z - xi.z;
             const double xn = sqrt(dx * dx + dy * dy + dz * dz);
             if (xn <= 0.0) continue;
-            if constexpr (MIXED) {
+            if constexpr (MIXED && !SUMS64) {
                 const float r = 2.0f * (float)(xn * inv_delta);
                 const float w = expf(-r * r);
                 float vc = 1.0f;
@@ -107,7 +112,7 @@ __device__ __forceinline__ void gbuild_group(const GBuildArgs &a, int i, bool ac
                     for (int q = p; q < NOP; ++q) acc[e++] += bw * m[p] * m[q];
             }
         }
-        if constexpr (MIXED) {
+        if constexpr (MIXED && !SUMS64) {
 #pragma unroll
             for (int e = 0; e < NE; ++e) acc[e] = cacc[e].value();
         }
@@ -219,6 +224,12 @@ __device__ __forceinline__ void gbuild_group(const GBuildArgs &a, int i, bool ac
 
         // ---- pass 2: per-bond operators, evaluated in FP64 (mixed mode stores them in FP32; its weights are
         //      the FP32 ones the moment sums used) ----
+        // mixed, order 2: first moments of the stored second-derivative operators (see GBuildArgs::defect)
+        constexpr bool DEF = MIXED && ORDER == 2;
+        constexpr int ND = DEF ? (NOP - DIM) * DIM : 1;
+        double dsum[ND];
+#pragma unroll
+        for (int e = 0; e < ND; ++e) dsum[e] = 0.0;
         cidx = 0;
         for (int t = b0 + gl; t < b1; t += LPN, ++cidx) {
             const int j = a.nbr[t];
@@ -234,7 +245,7 @@ __device__ __forceinline__ void gbuild_group(const GBuildArgs &a, int i, bool ac
             } else {
                 const double xn = sqrt(dx * dx + dy * dy + dz * dz);
                 if (xn > 0.0) {
-                    if constexpr (MIXED) {
+                    if constexpr (MIXED && !SUMS64) {
                         const float rr = 2.0f * (float)(xn * inv_delta);
                         float vc = 1.0f;
                         if (a.dx_char > 0.0 && xn > a.delta - 0.5 * a.dx_char)
@@ -248,7 +259,16 @@ __device__ __forceinline__ void gbuild_group(const GBuildArgs &a, int i, bool ac
             const bool live = bw > ET(0);
             const double bwd = (double)bw;
             double m[NOP];
-            monomials<DIM, ORDER, double>(dx * inv_delta, dy * inv_delta, dz * inv_delta, m);
+            if constexpr (MIXED && !SUMS64) {
+                // the FP32 monomials pass 1 summed, so the moment conditions hold for the factored matrix
+                float mf[NOP];
+                monomials<DIM, ORDER, float>((float)(dx * inv_delta), (float)(dy * inv_delta), (float)(dz * inv_delta),
+                                             mf);
+#pragma unroll
+                for (int k = 0; k < NOP; ++k) m[k] = (double)mf[k];
+            } else {
+                monomials<DIM, ORDER, double>(dx * inv_delta, dy * inv_delta, dz * inv_delta, m);
+            }
             auto op = [&](int k) -> double {
                 if (!live) return 0.0;
                 double sum = 0.0;
@@ -260,7 +280,17 @@ __device__ __forceinline__ void gbuild_group(const GBuildArgs &a, int i, bool ac
                 if constexpr (MIXED) {
                     float *o = static_cast<float *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
 #pragma unroll
-                    for (int k = 0; k < NOP; ++k) o[k] = (float)op(k);
+                    for (int k = 0; k < NOP; ++k) {
+                        const float gk = (float)op(k);
+                        o[k] = gk;
+                        if constexpr (DEF) {
+                            if (k >= DIM) {
+                                dsum[(k - DIM) * DIM + 0] += (double)gk * dx;
+                                dsum[(k - DIM) * DIM + 1] += (double)gk * dy;
+                                if constexpr (DIM == 3) dsum[(k - DIM) * DIM + 2] += (double)gk * dz;
+                            }
+                        }
+                    }
                 } else {
                     double *o = static_cast<double *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
 #pragma unroll
@@ -281,6 +311,16 @@ __device__ __forceinline__ void gbuild_group(const GBuildArgs &a, int i, bool ac
                     const double v = op(sl[c]);
                     if constexpr (MIXED) static_cast<float *>(a.G)[(size_t)c * a.nb + t] = (float)v;
                     else static_cast<double *>(a.G)[(size_t)c * a.nb + t] = v;
+                }
+            }
+        }
+        if constexpr (DEF) {
+            if (a.defect) {
+                float *dst = a.defect + (size_t)(i - a.node_base) * ND;
+#pragma unroll
+                for (int e = 0; e < ND; ++e) {
+                    const double v = group_sum<LPN>(dsum[e]);
+                    if (act && gl == (e & (LPN - 1))) dst[e] = (float)v;
                 }
             }
         }
@@ -338,7 +378,7 @@ cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, i
 // DIMS selects the task kinds this instantiation handles (1: 2D, 2: 3D, 3: both); a warp runs its task's nodes
 // 32/LPN at a time with the single-geometry group code, addressing the cloud's slices through node_base /
 // bond_base.
-template <bool MIXED, int LPN2, int LPN3, int DIMS>
+template <bool MIXED, int LPN2, int LPN3, int DIMS, bool SUMS64>
 __global__ void __launch_bounds__(kGbuildThreads) gbuild_batch_kernel(BatchArgs b) {
     constexpr int WPB = kGbuildThreads / kWarp;
     constexpr int S2 = (kWarp / LPN2) * 25, S3 = (kWarp / LPN3) * 81;
@@ -368,13 +408,14 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_batch_kernel(BatchArgs 
         a.first_degenerate = b.first_degenerate;
         a.node_base = cd.node0;
         a.bond_base = cd.bond0;
+        a.defect = (MIXED && b.defect) ? b.defect + cd.def_off : nullptr;
         if constexpr ((DIMS & 1) != 0) {
             if (tk.dim == 2) {
                 constexpr int GPW = kWarp / LPN2;
                 const int gl = lane & (LPN2 - 1), grp = lane / LPN2;
                 for (int k0 = 0; k0 < tk.count; k0 += GPW) {
                     const bool act = k0 + grp < tk.count;
-                    gbuild_group<2, 2, MIXED, LPN2>(a, tk.first + (act ? k0 + grp : 0), act, gl, &sA[w][grp * 25],
+                    gbuild_group<2, 2, MIXED, LPN2, SUMS64>(a, tk.first + (act ? k0 + grp : 0), act, gl, &sA[w][grp * 25],
                                                     &sX[w][grp * 25]);
                 }
             }
@@ -385,7 +426,7 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_batch_kernel(BatchArgs 
                 const int gl = lane & (LPN3 - 1), grp = lane / LPN3;
                 for (int k0 = 0; k0 < tk.count; k0 += GPW) {
                     const bool act = k0 + grp < tk.count;
-                    gbuild_group<3, 2, MIXED, LPN3>(a, tk.first + (act ? k0 + grp : 0), act, gl, &sA[w][grp * 81],
+                    gbuild_group<3, 2, MIXED, LPN3, SUMS64>(a, tk.first + (act ? k0 + grp : 0), act, gl, &sA[w][grp * 81],
                                                     &sX[w][grp * 81]);
                 }
             }
@@ -394,18 +435,21 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_batch_kernel(BatchArgs 
     }
 }
 
+// schedules 4 and 5 (mixed only; identical to 2 and 3 in FP64) sum the moments in FP64 (SUMS64)
 BatchSchedule batch_gbuild_schedule(int v) {
     switch (v) {
         case 0: return {8, 32, false};
         case 1: return {16, 32, false};
         case 2: return {8, 16, false};
+        case 3: return {8, 32, true};
+        case 4: return {8, 16, false};
         default: return {8, 32, true};
     }
 }
 
-template <bool MIXED, int LPN2, int LPN3, int DIMS>
+template <bool MIXED, int LPN2, int LPN3, int DIMS, bool SUMS64 = false>
 static cudaError_t launch_gb(const BatchArgs &a, cudaStream_t s) {
-    auto k = gbuild_batch_kernel<MIXED, LPN2, LPN3, DIMS>;
+    auto k = gbuild_batch_kernel<MIXED, LPN2, LPN3, DIMS, SUMS64>;
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -423,7 +467,10 @@ static cudaError_t launch_gb_m(const BatchArgs &a, int variant, int dims, cudaSt
         case 0: return launch_gb<MIXED, 8, 32, 3>(a, s);
         case 1: return launch_gb<MIXED, 16, 32, 3>(a, s);
         case 2: return launch_gb<MIXED, 8, 16, 3>(a, s);
-        default: return dims == 1 ? launch_gb<MIXED, 8, 32, 1>(a, s) : launch_gb<MIXED, 8, 32, 2>(a, s);
+        case 3: return dims == 1 ? launch_gb<MIXED, 8, 32, 1>(a, s) : launch_gb<MIXED, 8, 32, 2>(a, s);
+        case 4: return launch_gb<MIXED, 8, 16, 3, MIXED>(a, s);
+        default:
+            return dims == 1 ? launch_gb<MIXED, 8, 32, 1, MIXED>(a, s) : launch_gb<MIXED, 8, 32, 2, MIXED>(a, s);
     }
 }
 

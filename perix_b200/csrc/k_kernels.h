@@ -27,6 +27,10 @@ struct GBuildArgs {
     int *first_degenerate = nullptr;
     int node_base = 0;       // positions are read at pos[j - node_base] (a batch cloud's slice)
     long long bond_base = 0; // AoS operators are written at ops[(t - bond_base) * nop]
+    // MIXED, order 2: per node the first moments of the stored (FP32-rounded) second-derivative operators,
+    // sum_j g~^k_j xi_j[m] for k = dim..nop-1, m < dim (exactly 0 for exact operators; FP32 is ample for a
+    // correction of that size), at defect[(i - node_base) * (nop - dim) * dim + (k - dim) * dim + m]; may be null
+    float *defect = nullptr;
 };
 cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, int grid, cudaStream_t s);
 bool gbuild_supported(int dim, int order);
@@ -41,6 +45,7 @@ struct BatchCloud {
     int dim = 2, node0 = 0, n = 0, pad = 0;
     long long bond0 = 0, nb = 0;
     long long ops_off = 0, out_off = 0, pos_off = 0;
+    long long def_off = 0;  // element offset of the cloud's defects ([n][(nop - dim) * dim], mixed)
     double delta = 0.0, dx_char = 0.0;
 };
 struct BatchTask {
@@ -58,6 +63,7 @@ struct BatchArgs {
     uint8_t *degenerate = nullptr;
     unsigned int *n_degenerate = nullptr;
     int *first_degenerate = nullptr;
+    float *defect = nullptr;  // mixed: per-cloud first-moment defects at def_off (GBuildArgs::defect)
     unsigned int *counter = nullptr;
     const double *u = nullptr;  // apply: field (N)
     double *out = nullptr;      // apply: derivatives
@@ -67,7 +73,7 @@ struct BatchSchedule {
     int lpn2, lpn3;
     bool split;
 };
-constexpr int kBatchVariants = 4;
+constexpr int kBatchVariants = 6;
 BatchSchedule batch_gbuild_schedule(int variant);
 BatchSchedule batch_apply_schedule(int variant);
 // dims: 1 = 2D tasks only, 2 = 3D tasks only, 3 = both
@@ -161,9 +167,21 @@ struct ApplyArgs {
     const void *ops = nullptr;  // AoS [nb][nop]
     const double *u = nullptr;  // forward: u (N); adjoint: ybar (N*nk)
     double *out = nullptr;      // forward: N*nk; adjoint: N
+    // mixed, order 2: first-moment defects of the second-derivative operators (GBuildArgs::defect); the forward
+    // subtracts sum_m defect[k][m] * D^m u from every second derivative it returns
+    const float *defect = nullptr;
+    int dim = 2;
 };
 cudaError_t launch_apply(const ApplyArgs &a, bool mixed, int grid, cudaStream_t s);
 cudaError_t launch_apply_adjoint(const ApplyArgs &a, bool mixed, int grid, cudaStream_t s);
+struct AdjPrepArgs {
+    int n = 0, dim = 2, nop = 0, nk = 0, next = 0;
+    int slots[32], ext[32];
+    const float *defect = nullptr;
+    const double *ybar = nullptr;
+    double *yeff = nullptr;
+};
+cudaError_t launch_apply_adjoint_prep(const AdjPrepArgs &p, cudaStream_t s);
 
 // ------------------------------------------------------------------------------------------------------- misc
 cudaError_t launch_build_rev(int n, const int *off, const int *nbr, int *rev, int grid, cudaStream_t s);

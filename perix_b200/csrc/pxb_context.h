@@ -84,6 +84,8 @@ struct OpsCache {
     int order = 0, nop = 0, precision = PXB_FP64;
     DevBuf ops;         // AoS [nb][nop], double or float
     DevBuf degenerate;  // uint8 [n]
+    DevBuf defect;      // mixed, order 2: double [n][(nop - dim) * dim] first-moment defects (GBuildArgs::defect)
+    DevBuf yeff;        // adjoint with defects: transposed-correction ybar (grown on demand)
     std::vector<int> pqr;
 };
 
@@ -154,12 +156,13 @@ namespace pxb {
 struct BatchState {
     bool ready = false, built = false;
     int nclouds = 0, n = 0;
-    long long nb = 0, ops_len = 0, out_len = 0;
+    long long nb = 0, ops_len = 0, out_len = 0, def_len = 0;
     int ntasks = 0, ntasks3 = 0;  // tasks of 3D clouds first: [0, ntasks3), then 2D
     int precision = PXB_FP64;
     int gvariant = 3, avariant = 0;  // schedules (batch_gbuild_schedule / batch_apply_schedule)
     std::vector<BatchCloud> h_clouds;
     DevBuf clouds, tasks, off, nbr, pos, vol, ops, degenerate, counters;
+    DevBuf defect;  // mixed: per-cloud first-moment defects of the second-derivative operators
 };
 }  // namespace pxb
 

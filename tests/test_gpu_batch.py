@@ -1,6 +1,6 @@
 """Batched clouds (pxb_batch_*): 2D and 3D jittered-lattice clouds of uneven size in one launch, against the C
 restatement (oracle) run cloud by cloud.  FP64 g-functions and applies within 1e-12 (family-scaled); mixed
-precision within 1e-6 on g and within the stated per-order bounds on the apply; every schedule gives the same
+precision within 1e-6 on g and on the apply (see the test for the norms); every schedule gives the same
 result; a degenerate family is reported with its cloud and node."""
 import numpy as np
 import pytest
@@ -34,7 +34,7 @@ def _build(ctx, clouds, precision, gvariant=None):
     return ctx
 
 
-@pytest.mark.parametrize("gvariant", [0, 1, 2, 3])
+@pytest.mark.parametrize("gvariant", [0, 1, 2, 3, 4, 5])
 def test_batch_gbuild_fp64_matches_oracle(ctx, batch, gvariant):
     clouds, _, _, ref_g, _ = batch
     _build(ctx, clouds, 0, gvariant)
@@ -43,7 +43,7 @@ def test_batch_gbuild_fp64_matches_oracle(ctx, batch, gvariant):
         assert scaled_err(ctx.batch_get_ops(k), ref_g[k], c["off"]) <= 1e-12
 
 
-@pytest.mark.parametrize("avariant", [0, 1, 2, 3])
+@pytest.mark.parametrize("avariant", [0, 1, 2, 3, 4, 5])
 def test_batch_apply_fp64_matches_oracle(ctx, batch, avariant):
     clouds, u, _, _, ref_d = batch
     _build(ctx, clouds, 0)
@@ -54,18 +54,23 @@ def test_batch_apply_fp64_matches_oracle(ctx, batch, avariant):
         assert (np.abs(got[k] - ref_d[k]).max(axis=0) <= 1e-12 * scale + 1e-300).all()
 
 
-def test_batch_mixed_within_bounds(ctx, batch):
+@pytest.mark.parametrize("gvariant,slot_tol", [(2, 5e-6), (4, 1e-6)])
+def test_batch_mixed_within_bounds(ctx, batch, gvariant, slot_tol):
+    """Mixed: g within 1e-6 (family-scaled); every derivative within 1e-6 of the largest derivative of its order
+    (gradient / Hessian magnitude).  Slot by slot (relative to the slot's own largest value) the FP32 two-sum
+    moment sums (schedule 2) stay within 5e-6 and the FP64 moment sums with FP32 storage (schedule 4) within
+    1e-6."""
     clouds, u, _, ref_g, ref_d = batch
-    _build(ctx, clouds, 1)
+    _build(ctx, clouds, 1, gvariant)
     for k, c in enumerate(clouds):
         assert scaled_err(ctx.batch_get_ops(k), ref_g[k], c["off"]) <= 1e-6
     got = ctx.batch_split(ctx.batch_apply(u))
     for k, c in enumerate(clouds):
-        nd1 = c["dim"]  # first-derivative slots come first
-        scale = np.abs(ref_d[k]).max(axis=0)
-        err = np.abs(got[k] - ref_d[k]).max(axis=0) / scale
-        assert err[:nd1].max() <= 1e-6
-        assert err[nd1:].max() <= 5e-5
+        d = c["dim"]  # first-derivative slots come first
+        diff = np.abs(got[k] - ref_d[k])
+        for sl in (slice(0, d), slice(d, None)):
+            assert diff[:, sl].max() <= 1e-6 * np.abs(ref_d[k][:, sl]).max()
+        assert (diff.max(axis=0) / np.abs(ref_d[k]).max(axis=0)).max() <= slot_tol
 
 
 def test_batch_derivatives_of_cubics(ctx, batch):
