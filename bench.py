@@ -427,8 +427,12 @@ def run_perix(args):
     traffic = read_traffic(head)
     e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, max(10, min(steps, 200)))
     cpu = None
+    c3 = None
     if rank == 0 and ws == 1:
         cpu = cpu_reference(w, 20, 2)
+        for p in out.values():
+            p["ctx"].close()
+        c3 = c3_measure(px, device=local)
     if rank != 0:
         return
     line = {
@@ -467,6 +471,7 @@ def run_perix(args):
                   "rel_err_vs_fp64_after_100_steps": err, "health_differs": hdiff, "autotune": out["mixed"]["tuned"]},
         "steady_state_graph": {"fp64": out["fp64"]["steady"], "mixed": out["mixed"]["steady"],
                                "note": "100-step CUDA-graph chunk, L2-warm (wall clock incl. host sync)"},
+        "batched_clouds": c3,
         "gbuild_nodes_per_s": {"fp64": out["fp64"]["gbuild"], "mixed": out["mixed"]["gbuild"],
                                "ms": {"fp64": out["fp64"]["gbuild_ms"], "mixed": out["mixed"]["gbuild_ms"]},
                                "workload": "order-2 g-build of the same plate (81,200 nodes, all 5 operators stored)"},
