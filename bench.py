@@ -54,6 +54,113 @@ def c2_setup(px):
                 bcs=bcs, E=E, nu=nu, G0=G0, cracks=cracks, n=L.n, nb=int(off[-1]), h=h)
 
 
+def c5_setup(px, nx=120, ny=120, nz=24):
+    """3D slab (120x120x24 bulk nodes + one ghost layer per face = 385,920 nodes), h = 1 mm, delta = 3.015h,
+    E = 72 GPa, nu = 0.22, rho = 2440, s_c = 0.004 (G0 = s_c^2 6 E delta / 5), central edge notch of depth 20h
+    as a force-only crack plane at y = Ly/2, zero Neumann on every ghost wall, then +-2 m/s y-velocity pins on
+    the top and bottom three-node layers (box on all nodes), dt = 0.8 h / sqrt(C11 / rho)."""
+    h = 1e-3
+    Lx, Ly, Lz = nx * h, ny * h, nz * h
+    L = px.lattice(3, nx, ny, nz, [0.0, Lx, 0.0, Ly, 0.0, Lz])
+    delta = 3.015 * L.dxyz[0] * (1.0 + 1e-6)
+    plane = [0.0, Ly / 2, -1.0, 20 * h, Ly / 2, -1.0, 20 * h, Ly / 2, 1.0, 0.0, Ly / 2, 1.0]
+    off, ids = px.families(L.coords, delta, True, planes=[plane], mirror=L.mirror, force_only=True)
+    health0 = (1 - px.crack_cut_mask(L.coords, L.mirror, off, ids, planes=[plane])).astype(np.uint8)
+    E, nu, rho, sc_t = 72e9, 0.22, 2440.0, 0.004
+    C11, C12, C66 = px.elastic_constants(3, False, E, nu)
+    G0 = sc_t ** 2 * 6.0 * E * delta / 5.0
+    sc = px.critical_stretch(3, False, G0, E, delta)
+    dt = 0.8 * h / math.sqrt(C11 / rho)
+    bcs = [px.BC("neumann", [0, 1, 2], L.group(w + "nodes_ghost"))
+           for w in ("left", "right", "bottom", "top", "back", "front")]
+    alld = L.group("alldomain")
+    bcs.append(px.BC("dirichlet", [1], alld, value=[0, 0, 0], velocity=[0, 2.0, 0], direct=True,
+                     box=[-1, 1, Ly - 3 * h, 1, -1, 1]))
+    bcs.append(px.BC("dirichlet", [1], alld, value=[0, 0, 0], velocity=[0, -2.0, 0], direct=True,
+                     box=[-1, 1, -1, 3 * h, -1, 1]))
+    return dict(L=L, off=off, ids=ids, delta=delta, health0=health0, C=(C11, C12, C66), rho=rho, sc=sc, dt=dt,
+                bcs=bcs, E=E, nu=nu, n=L.n, nb=int(off[-1]), h=h)
+
+
+def c5_measure(px, device=0, steps=50, adjoint_steps=1000, checkpoint_every=100):
+    """The 3D slab: step throughput (FP64 and mixed, autotuned, CUDA events, L2 flushed, from the state after
+    100 steps) and the frozen-mask adjoint d(misfit)/dE over the first `adjoint_steps` steps with checkpointed
+    recomputation, checked against central finite differences of the device loop."""
+    import torch
+    from perix_b200.autograd import BcPlan, elastic_constants_t, explicit_loop, set_constants
+    t0 = time.perf_counter()
+    w = c5_setup(px)
+    res = {"workload": "3D slab 120x120x24 (+ghosts), edge notch 20h", "nodes": w["n"], "bonds": w["nb"],
+           "host_setup_s": time.perf_counter() - t0}
+    L = w["L"]
+    C11, C12, C66 = w["C"]
+    hbm, _ = peaks()
+    for prec in ("fp64", "mixed"):
+        ctx = px.Context(device)
+        ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 3, mirror=L.mirror)
+        ctx.epf_setup(C11, C12, C66, w["rho"], (0.0, 0.0, 0.0), w["sc"], True, health0=w["health0"],
+                      precision=px.MIXED if prec == "mixed" else px.FP64)
+        ctx.epf_set_bcs(w["bcs"])
+        ctx.epf_start(np.zeros(3 * L.n), None, w["dt"])
+        ctx.epf_advance(S0)
+        snap(ctx)
+        tuned = autotune(ctx, steps=5)
+        ms = np.zeros(steps, np.float32)
+        time_steps(ctx, 3, ms[:3])
+        restore(ctx)
+        time_steps(ctx, steps, ms)
+        mean_ms = float(np.mean(ms))
+        B = algorithmic_bytes(w["n"], w["nb"], 3, prec)
+        res[prec] = {"bond_updates_per_s": w["nb"] / (mean_ms * 1e-3), "ms_per_step": mean_ms, "autotune": tuned,
+                     "achieved_gbs": B / (mean_ms * 1e-3) / 1e9, "frac_of_measured_hbm": B / (mean_ms * 1e-3) / 1e9 / hbm,
+                     "algorithmic_bytes_per_step": B}
+        ctx.close()
+    # adjoint: misfit against the displacement of a 2 % stiffer slab, frozen damage mask (damage off)
+    dev = torch.device("cuda", device)
+    ctx = px.Context(device)
+    ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 3, mirror=L.mirror)
+
+    def device_final(E):
+        c = px.elastic_constants(3, False, E, w["nu"])
+        ctx.epf_setup(c[0], c[1], c[2], w["rho"], (0.0, 0.0, 0.0), 0.0, True, health0=w["health0"])
+        ctx.epf_set_bcs(w["bcs"])
+        ctx.epf_start(np.zeros(3 * L.n), None, w["dt"])
+        ctx.epf_advance(adjoint_steps, chunk=100)
+        return ctx.epf_state()[0]
+
+    u_obs = device_final(1.02 * w["E"])
+    J = lambda uN: 0.5 * float(((uN - u_obs) ** 2).sum())  # noqa: E731
+    def cfd(rel):
+        hE = rel * w["E"]
+        return (J(device_final(w["E"] + hE)) - J(device_final(w["E"] - hE))) / (2 * hE)
+
+    # central differences at two steps; their Richardson extrapolation removes the O(h^2) truncation term,
+    # which 1000 steps of wave propagation make visible at h = 1e-5 E
+    fd1, fd2 = cfd(1e-5), cfd(5e-6)
+    fd = (4.0 * fd2 - fd1) / 3.0
+    device_final(w["E"])  # context state (constants, health) for the differentiable loop
+    plan = BcPlan(w["bcs"], L.coords, L.mirror, 3, dev)
+    E = torch.tensor(w["E"], dtype=torch.float64, device=dev, requires_grad=True)
+    torch.cuda.synchronize(dev)
+    torch.cuda.reset_peak_memory_stats(dev)
+    t0 = time.perf_counter()
+    C = elastic_constants_t(3, False, E, w["nu"])
+    set_constants(ctx, C, w["rho"])
+    uN, _ = explicit_loop(ctx, torch.zeros(3 * L.n, dtype=torch.float64, device=dev), None, w["dt"], adjoint_steps,
+                          C, plan, checkpoint_every=checkpoint_every)
+    Jt = 0.5 * ((uN - torch.from_numpy(u_obs).to(dev)) ** 2).sum()
+    Jt.backward()
+    torch.cuda.synchronize(dev)
+    secs = time.perf_counter() - t0
+    res["adjoint"] = {"steps": adjoint_steps, "checkpoint_every": checkpoint_every, "precision": "fp64",
+                      "dJ_dE": float(E.grad), "dJ_dE_central_fd": {"h=1e-5E": fd1, "h=5e-6E": fd2, "richardson": fd},
+                      "rel_err_vs_fd": abs(float(E.grad) - fd) / abs(fd),
+                      "rel_err_vs_fd_h5e-6": abs(float(E.grad) - fd2) / abs(fd2), "seconds_forward_and_backward": secs,
+                      "peak_torch_gb": torch.cuda.max_memory_allocated(dev) / 1e9}
+    ctx.close()
+    return res
+
+
 def c3_clouds(px, nclouds=256, nmin=1000, nmax=200000, seed=2024):
     """Batched-cloud workload: clouds alternate 2D / 3D (half each), node counts log-uniform in [nmin, nmax]
     (seeded), cell-centred lattice of spacing h = 1 mm jittered by U(-0.2h, 0.2h) per coordinate, no ghosts
@@ -568,6 +675,10 @@ def run_profile(args):
     ctx = px.Context(0)
     L = w["L"]
     ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
+    if args.profile == "c5":
+        print(json.dumps({"profile": "c5", **c5_measure(px)}))
+        ctx.close()
+        return
     if args.profile == "c3":
         print(json.dumps({"profile": "c3", **c3_measure(px, nclouds=args.steps)}))
         ctx.close()
@@ -599,7 +710,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="perix", choices=["perix", "reference"])
-    ap.add_argument("--profile", choices=["step", "gbuild", "c3"], default=None,
+    ap.add_argument("--profile", choices=["step", "gbuild", "c3", "c5"], default=None,
                     help="run one kernel family only (for profiler captures); prints its own JSON line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--variant", type=int, default=8)

@@ -48,7 +48,8 @@ const char *pxb_last_error(void);
 int pxb_ctx_create(int device, pxb_ctx **out);
 int pxb_ctx_destroy(pxb_ctx *ctx);
 /* Use an external stream (cudaStream_t passed as void*), e.g. torch's current stream.  NULL restores the
- * context's own stream. */
+ * context's own stream, which is non-blocking: work on it is NOT ordered against the legacy default stream.
+ * To share the legacy default stream (torch's default stream, handle 0) pass cudaStreamLegacy ((void*)1). */
 int pxb_ctx_set_stream(pxb_ctx *ctx, void *stream);
 int pxb_ctx_synchronize(pxb_ctx *ctx);
 /* Device bytes currently held by the context. */

@@ -280,6 +280,10 @@ class Context:
 
     # -- plumbing
     def set_stream(self, stream_ptr):
+        """Run on an external CUDA stream.  A handle of 0 (torch's default stream) means the legacy default
+        stream and is passed as cudaStreamLegacy; None restores the context's own (non-blocking) stream."""
+        if stream_ptr is not None and int(stream_ptr) == 0:
+            stream_ptr = 1  # cudaStreamLegacy
         _check(self.L.pxb_ctx_set_stream(self.h, _vp(stream_ptr)))
 
     def synchronize(self):

@@ -227,3 +227,60 @@ def test_mixed_adjoint_against_its_forward(ctx, loop_case):
     assert abs(dE32 - fd) <= 1e-6 * abs(fd)
     assert abs(dE32 - dE64) <= 1e-5 * abs(dE64)
     assert np.abs(du32 - du64).max() <= 1e-5 * np.abs(du64).max()
+
+
+def test_explicit_loop_full_plate_matches_device_loop(ctx):
+    """The differentiable loop on the full 400x200 plate (its kernels and torch's ops share torch's default
+    stream: the launches must be ordered with torch's work) against the fused device loop, 30 steps."""
+    torch, dev = _torch()
+    import perix_b200 as px
+    from bench import c2_setup
+    from perix_b200.autograd import BcPlan, elastic_constants_t, explicit_loop, set_constants
+    w = c2_setup(px)
+    L = w["L"]
+    ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
+    C11, C12, C66 = w["C"]
+    ctx.epf_setup(C11, C12, C66, w["rho"], (0.0, 0.0), 0.0, True, health0=w["health0"])
+    ctx.epf_set_bcs(w["bcs"])
+    ctx.epf_start(np.zeros(2 * L.n), None, w["dt"])
+    ctx.epf_advance(30, chunk=10)
+    ref = ctx.epf_state()[0]
+    C = elastic_constants_t(2, False, torch.tensor(w["E"], dtype=torch.float64, device=dev), w["nu"])
+    set_constants(ctx, C, w["rho"])
+    with torch.no_grad():
+        uN, _ = explicit_loop(ctx, torch.zeros(2 * L.n, dtype=torch.float64, device=dev), None, w["dt"], 30, C,
+                              BcPlan(w["bcs"], L.coords, L.mirror, 2, dev))
+    assert np.abs(uN.cpu().numpy() - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+def test_dJ_dE_3d_slab_against_finite_differences(ctx):
+    """3D: a 16x16x6 slab with an edge notch and +-2 m/s pins, 40 steps, checkpoints every 10."""
+    torch, dev = _torch()
+    import perix_b200 as px
+    from bench import c5_setup
+    from perix_b200.autograd import BcPlan, elastic_constants_t, explicit_loop, set_constants
+    w = c5_setup(px, nx=16, ny=16, nz=6)
+    L = w["L"]
+    nsteps = 40
+    ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 3, mirror=L.mirror)
+
+    def device_final(E):
+        c = px.elastic_constants(3, False, E, w["nu"])
+        ctx.epf_setup(c[0], c[1], c[2], w["rho"], (0.0, 0.0, 0.0), 0.0, True, health0=w["health0"])
+        ctx.epf_set_bcs(w["bcs"])
+        ctx.epf_start(np.zeros(3 * L.n), None, w["dt"])
+        ctx.epf_advance(nsteps, chunk=10)
+        return ctx.epf_state()[0]
+
+    u_obs = device_final(1.02 * w["E"])
+    J = lambda u: 0.5 * float(((u - u_obs) ** 2).sum())  # noqa: E731
+    h = 1e-5 * w["E"]
+    fd = (J(device_final(w["E"] + h)) - J(device_final(w["E"] - h))) / (2 * h)
+    device_final(w["E"])
+    E = torch.tensor(w["E"], dtype=torch.float64, device=dev, requires_grad=True)
+    C = elastic_constants_t(3, False, E, w["nu"])
+    set_constants(ctx, C, w["rho"])
+    uN, _ = explicit_loop(ctx, torch.zeros(3 * L.n, dtype=torch.float64, device=dev), None, w["dt"], nsteps, C,
+                          BcPlan(w["bcs"], L.coords, L.mirror, 3, dev), checkpoint_every=10)
+    (0.5 * ((uN - torch.from_numpy(u_obs).to(dev)) ** 2).sum()).backward()
+    assert abs(float(E.grad) - fd) <= 1e-6 * abs(fd)
