@@ -534,12 +534,13 @@ def run_perix(args):
     traffic = read_traffic(head)
     e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, max(10, min(steps, 200)))
     cpu = None
-    c3 = None
+    c3 = c5 = None
     if rank == 0 and ws == 1:
         cpu = cpu_reference(w, 20, 2)
         for p in out.values():
             p["ctx"].close()
         c3 = c3_measure(px, device=local)
+        c5 = c5_measure(px, device=local)
     if rank != 0:
         return
     line = {
@@ -579,6 +580,7 @@ def run_perix(args):
         "steady_state_graph": {"fp64": out["fp64"]["steady"], "mixed": out["mixed"]["steady"],
                                "note": "100-step CUDA-graph chunk, L2-warm (wall clock incl. host sync)"},
         "batched_clouds": c3,
+        "slab_3d": c5,
         "gbuild_nodes_per_s": {"fp64": out["fp64"]["gbuild"], "mixed": out["mixed"]["gbuild"],
                                "ms": {"fp64": out["fp64"]["gbuild_ms"], "mixed": out["mixed"]["gbuild_ms"]},
                                "workload": "order-2 g-build of the same plate (81,200 nodes, all 5 operators stored)"},
@@ -679,6 +681,48 @@ def run_profile(args):
         print(json.dumps({"profile": "c5", **c5_measure(px)}))
         ctx.close()
         return
+    if args.profile == "c5step":
+        # the 3D slab at --size x --size x 24: 100 steps of variant 1, then --steps timed steps of --variant
+        ctx.close()
+        w5 = c5_setup(px, nx=args.size, ny=args.size, nz=24)
+        L5 = w5["L"]
+        ctx = px.Context(0)
+        ctx.set_geometry(L5.coords, L5.vols, w5["off"], w5["ids"], w5["delta"], L5.dxyz[0], 3, mirror=L5.mirror)
+        C11, C12, C66 = w5["C"]
+        ctx.epf_setup(C11, C12, C66, w5["rho"], (0.0, 0.0, 0.0), w5["sc"], True, health0=w5["health0"],
+                      precision=px.MIXED if args.precision == "mixed" else px.FP64)
+        ctx.epf_set_bcs(w5["bcs"])
+        ctx.epf_start(np.zeros(3 * L5.n), None, w5["dt"])
+        ctx.epf_set_variant(1)
+        ctx.epf_advance(S0)
+        snap(ctx)
+        ctx.epf_set_variant(args.variant)
+        ms = np.zeros(args.steps, np.float32)
+        time_steps(ctx, args.steps, ms)
+        print(json.dumps({"profile": "c5step", "size": args.size, "nodes": L5.n, "bonds": w5["nb"],
+                          "precision": args.precision, "variant": args.variant, "ms_per_step": float(np.mean(ms[1:] if
+                          ms.size > 1 else ms))}))
+        ctx.close()
+        return
+    if args.profile == "c3apply":
+        # --steps clouds (log-uniform 1k..200k nodes), one FP64 or mixed g-build, then 3 applies of schedule --variant
+        ctx.close()
+        import torch
+        clouds = c3_clouds(px, nclouds=args.steps)
+        fields, _ = cubic_field(clouds)
+        ctx = px.Context(0)
+        ctx.batch_set(clouds)
+        dev = torch.device("cuda", 0)
+        ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        ctx.batch_gbuild(px.MIXED if args.precision == "mixed" else px.FP64)
+        ctx.batch_set_variant(1, args.variant)
+        u = torch.from_numpy(np.concatenate(fields)).to(dev)
+        out = torch.empty(ctx.batch_out_len, dtype=torch.float64, device=dev)
+        ms = ctx.batch_time(1, 3, FLUSH_BYTES, u.data_ptr(), out.data_ptr())
+        print(json.dumps({"profile": "c3apply", "clouds": args.steps, "nodes": ctx.batch_n, "bonds": ctx.batch_nb,
+                          "precision": args.precision, "schedule": args.variant, "ms": [float(x) for x in ms]}))
+        ctx.close()
+        return
     if args.profile == "c3":
         print(json.dumps({"profile": "c3", **c3_measure(px, nclouds=args.steps)}))
         ctx.close()
@@ -710,10 +754,11 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="perix", choices=["perix", "reference"])
-    ap.add_argument("--profile", choices=["step", "gbuild", "c3", "c5"], default=None,
+    ap.add_argument("--profile", choices=["step", "gbuild", "c3", "c5", "c5step", "c3apply"], default=None,
                     help="run one kernel family only (for profiler captures); prints its own JSON line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--variant", type=int, default=8)
+    ap.add_argument("--size", type=int, default=120, help="--profile c5step: slab of size x size x 24 nodes")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)
