@@ -16,8 +16,8 @@ using namespace pxb;
 
 namespace {
 
-constexpr int kTaskNodes2 = 128;  // nodes per task: ~25 bonds each in 2D
-constexpr int kTaskNodes3 = 32;   // ~100 bonds each in 3D
+constexpr int kTaskNodes2 = 32;  // nodes per task: ~25 bonds each in 2D (small tasks keep small batches parallel)
+constexpr int kTaskNodes3 = 16;  // ~100 bonds each in 3D
 
 int nop_of_dim(int dim) { return dim == 3 ? 9 : 5; }
 
