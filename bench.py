@@ -111,9 +111,10 @@ def c5_measure(px, device=0, steps=50, adjoint_steps=1000, checkpoint_every=100)
         time_steps(ctx, steps, ms)
         mean_ms = float(np.mean(ms))
         B = algorithmic_bytes(w["n"], w["nb"], 3, prec)
+        gb, gb_ms = gbuild_rate(px, ctx, prec, reps=3)
         res[prec] = {"bond_updates_per_s": w["nb"] / (mean_ms * 1e-3), "ms_per_step": mean_ms, "autotune": tuned,
                      "achieved_gbs": B / (mean_ms * 1e-3) / 1e9, "frac_of_measured_hbm": B / (mean_ms * 1e-3) / 1e9 / hbm,
-                     "algorithmic_bytes_per_step": B}
+                     "algorithmic_bytes_per_step": B, "gbuild_nodes_per_s": gb, "gbuild_ms": gb_ms}
         ctx.close()
     # adjoint: misfit against the displacement of a 2 % stiffer slab, frozen damage mask (damage off)
     dev = torch.device("cuda", device)
@@ -356,6 +357,25 @@ def cpu_reference(w, steps, warmup, threads=None):
     return dict(value=m.nb * steps / t, seconds=t, steps=steps, cores=threads, nb=m.nb)
 
 
+def reference_gpu():
+    """The reference's own CUDA explicit path on this GPU (bench.py --profile refgpu, in a child process so that
+    its device state and runtime stay apart from this process's)."""
+    try:
+        r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--profile", "refgpu"], capture_output=True,
+                           text=True, timeout=600)
+        line = [x for x in r.stdout.splitlines() if x.startswith("{")]
+        if r.returncode != 0 or not line:
+            return {"unavailable": "reference GPU run failed: " + (r.stderr.strip().splitlines() or ["?"])[-1][:200]}
+        d = json.loads(line[-1])
+        d.pop("profile", None)
+        d["what"] = ("perix_cuda::assembleExplicitPDDOFracAccel from the reference's CudaAssembleKernels.cu built for "
+                     "sm_100a: call = H2D u + force kernel + D2H accel per step; force kernel alone with CUDA events, "
+                     "L2 flushed; opbuild = its one-off operator build")
+        return d
+    except Exception as e:  # noqa: BLE001
+        return {"unavailable": "reference GPU run failed: %s" % e}
+
+
 def run_reference_arm(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -534,13 +554,14 @@ def run_perix(args):
     traffic = read_traffic(head)
     e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, max(10, min(steps, 200)))
     cpu = None
-    c3 = c5 = None
+    c3 = c5 = refgpu = None
     if rank == 0 and ws == 1:
         cpu = cpu_reference(w, 20, 2)
         for p in out.values():
             p["ctx"].close()
         c3 = c3_measure(px, device=local)
         c5 = c5_measure(px, device=local)
+        refgpu = reference_gpu()
     if rank != 0:
         return
     line = {
@@ -581,6 +602,7 @@ def run_perix(args):
                                "note": "100-step CUDA-graph chunk, L2-warm (wall clock incl. host sync)"},
         "batched_clouds": c3,
         "slab_3d": c5,
+        "reference_gpu": refgpu,
         "gbuild_nodes_per_s": {"fp64": out["fp64"]["gbuild"], "mixed": out["mixed"]["gbuild"],
                                "ms": {"fp64": out["fp64"]["gbuild_ms"], "mixed": out["mixed"]["gbuild_ms"]},
                                "workload": "order-2 g-build of the same plate (81,200 nodes, all 5 operators stored)"},
@@ -681,6 +703,35 @@ def run_profile(args):
         print(json.dumps({"profile": "c5", **c5_measure(px)}))
         ctx.close()
         return
+    if args.profile == "refgpu":
+        # the reference's own GPU explicit path (oracle/_ref/libperix_ref_cuda.so) on the plate and the slab,
+        # from the state after 100 steps; run in a child process of the main bench
+        from oracle import ref_cuda_available, ref_cuda_epf_bench
+        ctx.close()
+        if not ref_cuda_available():
+            print(json.dumps({"profile": "refgpu", "unavailable": "oracle/_ref/libperix_ref_cuda.so not built"}))
+            return
+        res = {"profile": "refgpu"}
+        for name, setup, dim in (("plate_2d", c2_setup, 2), ("slab_3d", c5_setup, 3)):
+            wv = setup(px)
+            Lv = wv["L"]
+            c = px.Context(0)
+            c.set_geometry(Lv.coords, Lv.vols, wv["off"], wv["ids"], wv["delta"], Lv.dxyz[0], dim, mirror=Lv.mirror)
+            C11, C12, C66 = wv["C"]
+            c.epf_setup(C11, C12, C66, wv["rho"], (0.0,) * dim, wv["sc"], True, health0=wv["health0"])
+            c.epf_set_bcs(wv["bcs"])
+            c.epf_start(np.zeros(dim * Lv.n), None, wv["dt"])
+            c.epf_advance(S0)
+            u, _, hh, _ = c.epf_state()
+            c.close()
+            call_ms, kern_ms, ob_ms, _ = ref_cuda_epf_bench(dim, Lv.coords, Lv.vols, wv["off"], wv["ids"], wv["delta"],
+                                                            Lv.dxyz[0], wv["C"], wv["rho"], wv["sc"], u,
+                                                            hh.astype(np.float64), reps=20, flush_bytes=FLUSH_BYTES)
+            res[name] = {"nodes": Lv.n, "bonds": wv["nb"], "call_ms": call_ms, "force_kernel_ms": kern_ms,
+                         "opbuild_ms": ob_ms, "force_kernel_bond_updates_per_s": wv["nb"] / (kern_ms * 1e-3),
+                         "call_bond_updates_per_s": wv["nb"] / (call_ms * 1e-3)}
+        print(json.dumps(res))
+        return
     if args.profile == "c5step":
         # the 3D slab at --size x --size x 24: 100 steps of variant 1, then --steps timed steps of --variant
         ctx.close()
@@ -754,7 +805,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="perix", choices=["perix", "reference"])
-    ap.add_argument("--profile", choices=["step", "gbuild", "c3", "c5", "c5step", "c3apply"], default=None,
+    ap.add_argument("--profile", choices=["step", "gbuild", "c3", "c5", "c5step", "c3apply", "refgpu"], default=None,
                     help="run one kernel family only (for profiler captures); prints its own JSON line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--variant", type=int, default=8)

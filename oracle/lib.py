@@ -1,5 +1,6 @@
 """ctypes bindings for the two oracle libraries (test infrastructure only, see ``oracle/__init__.py``)."""
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -201,6 +202,44 @@ class PortOracle:
                            _ptr(p["has_box"], C.c_int), _ptr(p["box"], C.c_double), _ptr(p["off"], C.c_int),
                            _ptr(p["nodes"], C.c_int), _ptr(u, C.c_double), _ptr(uo, C.c_double), _ptr(h, C.c_double))
         return u, uo, h
+
+
+_REFCU_SO = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "libperix_ref_cuda.so")
+
+
+def ref_cuda_available():
+    return os.path.exists(_REFCU_SO)
+
+
+def ref_cuda_epf_bench(dim, coords3, vols, off, ids, delta, dx_char, Cv, rho, sc, u, health, reps=20,
+                       flush_bytes=256 << 20, tension_only=True):
+    """Times the reference's own GPU explicit path (oracle/ref_cuda_harness.cu): per-step call, force kernel
+    alone, operator build.  Returns (call_ms, kernel_ms, opbuild_ms, accel)."""
+    L = C.CDLL(_REFCU_SO)
+    coords3 = np.ascontiguousarray(coords3, np.float64).reshape(-1)
+    n = coords3.size // 3
+    if dim == 2:
+        q = [(1, 0, 0), (0, 1, 0), (2, 0, 0), (1, 1, 0), (0, 2, 0)]
+    else:
+        q = [(1, 0, 0), (0, 1, 0), (0, 0, 1), (2, 0, 0), (1, 1, 0), (1, 0, 1), (0, 2, 0), (0, 1, 1), (0, 0, 2)]
+    qp = np.array([a for a, _, _ in q], np.int32)
+    qq = np.array([b for _, b, _ in q], np.int32)
+    qr = np.array([c for _, _, c in q], np.int32)
+    fact = np.array([math.factorial(a) * math.factorial(b) * math.factorial(c) for a, b, c in q], np.float64)
+    h = np.ascontiguousarray(health, np.float64).copy()
+    out = np.zeros(4, np.float64)
+    acc = np.zeros(n * dim, np.float64)
+    L.refcu_epf_bench.restype = C.c_int
+    st = L.refcu_epf_bench(n, dim, _ptr(coords3, C.c_double), _ptr(np.ascontiguousarray(vols, np.float64), C.c_double),
+                           _ptr(np.ascontiguousarray(off, np.int32), C.c_int),
+                           _ptr(np.ascontiguousarray(ids, np.int32), C.c_int), _ptr(qp, C.c_int), _ptr(qq, C.c_int),
+                           _ptr(qr, C.c_int), _ptr(fact, C.c_double), len(q), C.c_double(delta), C.c_double(dx_char),
+                           C.c_double(Cv[0]), C.c_double(Cv[1]), C.c_double(Cv[2]), C.c_double(rho), C.c_double(sc),
+                           int(tension_only), _ptr(np.ascontiguousarray(u, np.float64), C.c_double), _ptr(h, C.c_double),
+                           int(reps), C.c_size_t(flush_bytes), _ptr(out, C.c_double), _ptr(acc, C.c_double))
+    if st:
+        raise RuntimeError("reference GPU harness failed with status %d" % st)
+    return float(out[0]), float(out[1]), float(out[2]), acc
 
 
 _REF = None

@@ -1,0 +1,115 @@
+// Measurement infrastructure (not part of the product): the reference's own CUDA assembly translation unit,
+// src/PDSystem/CudaAssembleKernels.cu, compiled unchanged for sm_100a from the reference tree (this file
+// includes it; oracle/Makefile target `refcuda`), plus C-callable timers for its explicit fracture path.
+// It gives the "existing GPU kernel" reference point: the per-step call perix_cuda::assembleExplicitPDDOFracAccel
+// (CudaAssembleKernels.cu:1189-1271: H2D of u, explicitPDDOFracForceKernel, D2H of the acceleration) and the
+// force kernel alone on its cached device state, plus its one-off operator build (explicitPDDOFracOpBuildKernel).
+// Only the oracle loader and bench.py call it.
+#include "PDSystem/CudaAssembleKernels.cu"
+
+#include <chrono>
+#include <vector>
+
+#define REFCU_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+perix_cuda::OpSlots slots_for(int dim) {
+    perix_cuda::OpSlots s;
+    if (dim == 3) {  // multi-index order 100 010 001 200 110 101 020 011 002
+        s.dx = 0; s.dy = 1; s.dz = 2; s.dxx = 3; s.dxy = 4; s.dxz = 5; s.dyy = 6; s.dyz = 7; s.dzz = 8;
+    } else {  // 10 01 20 11 02
+        s.dx = 0; s.dy = 1; s.dxx = 2; s.dxy = 3; s.dyy = 4;
+    }
+    return s;
+}
+
+}  // namespace
+
+// out[0] mean wall ms of one perix_cuda::assembleExplicitPDDOFracAccel call (after one warm call that builds
+// the cache); out[1] mean ms of explicitPDDOFracForceKernel alone (CUDA events, L2 flushed by a flush_bytes
+// write before each launch); out[2] ms of one explicitPDDOFracOpBuildKernel launch (events).  accel_out gets
+// the last call's acceleration.  Returns 0 on success.
+REFCU_API int refcu_epf_bench(int n, int dim, const double *coords, const double *vols, const int *off,
+                              const int *ids, const int *qp, const int *qq, const int *qr, const double *factprod,
+                              int nop, double delta, double dx_char, double C11, double C12, double C66, double rho,
+                              double sc, int tension_only, const double *u, double *health, int reps,
+                              size_t flush_bytes, double *out, double *accel_out) {
+    perix_cuda::AssembleMesh m;
+    m.N = n;
+    m.neigh_off = off;
+    m.neigh_id = ids;
+    m.coords = coords;
+    m.vols = vols;
+    m.qp = qp;
+    m.qq = qq;
+    m.qr = qr;
+    m.factprod = factprod;
+    m.nop = nop;
+    m.dim = dim;
+    m.delta = delta;
+    m.dx_char = dx_char;
+    perix_cuda::ExplicitPDDOFracParams p;
+    p.dim = dim;
+    p.C11 = C11;
+    p.C12 = C12;
+    p.C66 = C66;
+    p.rho = rho;
+    p.sc = sc;
+    p.tension_only = tension_only;
+    p.damage_on = sc > 0.0 ? 1 : 0;
+    const perix_cuda::OpSlots s = slots_for(dim);
+    int changed = 0;
+    if (!perix_cuda::assembleExplicitPDDOFracAccel(m, p, s, u, health, accel_out, &changed)) return 1;
+    auto t0 = std::chrono::steady_clock::now();
+    for (int r = 0; r < reps; ++r)
+        if (!perix_cuda::assembleExplicitPDDOFracAccel(m, p, s, u, health, accel_out, &changed)) return 2;
+    auto t1 = std::chrono::steady_clock::now();
+    out[0] = std::chrono::duration<double, std::milli>(t1 - t0).count() / reps;
+
+    EpfCtx &e = g_epfctx;
+    void *flush = nullptr;
+    if (flush_bytes && cudaMalloc(&flush, flush_bytes) != cudaSuccess) return 3;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int block = 128, grid = (n + block - 1) / block;
+    double kern = 0.0;
+    for (int r = 0; r < reps; ++r) {
+        if (flush) cudaMemsetAsync(flush, r & 0xff, flush_bytes);
+        cudaEventRecord(a);
+        if (dim == 3)
+            explicitPDDOFracForceKernel<3><<<grid, block>>>(n, p, e.coords, nullptr, e.neigh_off, e.neigh_id, e.u,
+                                                            e.nopb, e.opcache, e.health, e.accel, e.anyBroke);
+        else
+            explicitPDDOFracForceKernel<2><<<grid, block>>>(n, p, e.coords, nullptr, e.neigh_off, e.neigh_id, e.u,
+                                                            e.nopb, e.opcache, e.health, e.accel, e.anyBroke);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        kern += ms;
+    }
+    out[1] = kern / reps;
+    if (flush) cudaMemsetAsync(flush, 0, flush_bytes);
+    cudaEventRecord(a);
+    if (dim == 3)
+        explicitPDDOFracOpBuildKernel<3><<<grid, block>>>(n, s, e.coords, e.vols, nullptr, nullptr, e.neigh_off,
+                                                          e.neigh_id, e.qp, e.qq, e.qr, e.factprod, nop, delta, dx_char,
+                                                          e.nopb, e.opcache);
+    else
+        explicitPDDOFracOpBuildKernel<2><<<grid, block>>>(n, s, e.coords, e.vols, nullptr, nullptr, e.neigh_off,
+                                                          e.neigh_id, e.qp, e.qq, e.qr, e.factprod, nop, delta, dx_char,
+                                                          e.nopb, e.opcache);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    out[2] = ms;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (flush) cudaFree(flush);
+    const cudaError_t err = cudaDeviceSynchronize();
+    perix_cuda::shutdown();
+    return err == cudaSuccess ? 0 : 4;
+}
