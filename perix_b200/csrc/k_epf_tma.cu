@@ -129,11 +129,10 @@ struct StageLayout {
 
 }  // namespace
 
-template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB>
-__global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
+template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB>
+__global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     using PosT = typename Vec<DIM>::T;
     using GT = typename std::conditional<MIXED, float, double>::type;
-    constexpr int WPB = kEpfThreads / kWarp;
     constexpr int GPW = kWarp / LPN;
     constexpr int NT = WPB * GPW;
     using SL = StageLayout<DIM, MIXED, NT>;
@@ -388,11 +387,11 @@ __global__ void __launch_bounds__(kEpfThreads, MINB) epf_tma_kernel(EpfArgs a) {
     }
 }
 
-template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB>
+template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB>
 static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
-    constexpr int NT = (kEpfThreads / kWarp) * (kWarp / LPN);
+    constexpr int NT = WPB * (kWarp / LPN);
     using SL = StageLayout<DIM, MIXED, NT>;
-    auto k = epf_tma_kernel<DIM, MIXED, LPN, UNR, S, MINB>;
+    auto k = epf_tma_kernel<DIM, MIXED, LPN, UNR, S, MINB, WPB>;
     const size_t smem = (size_t)S * SL::bytes(a.maxb);
     static size_t configured = 0;
     if (smem > configured) {
@@ -403,36 +402,47 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kEpfThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WPB * kWarp, smem);
     const long long ntiles = ((long long)a.n + NT - 1) / NT;
     const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
     const int grid = (int)(ntiles < cap ? ntiles : cap);
-    k<<<grid > 0 ? grid : 1, kEpfThreads, smem, s>>>(a);
+    k<<<grid > 0 ? grid : 1, WPB * kWarp, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-// Staged configurations (lanes per node, bonds per lane per pass, stages; minimum resident blocks in the
-// launch bounds):
-//   2D  0: 16,2,4;1  1: 8,1,3;1  2: 8,4,3;1  3: 8,2,2;3  4: 8,1,2;4  5: 8,2,2;4
-//   3D  0: 32,2,2;1  1: 32,4,2;1 2: 32,1,3;1 3: 16,2,2;1 4: 16,1,2;2 5: 32,2,2;2
+// Staged configurations: lanes per node, bonds per lane per pass, stages, minimum resident blocks (launch
+// bounds), warps per block.  A tile is WPB * 32/LPN nodes.
 struct TmaCfg {
-    int lpn, unr, stages;
+    int lpn, unr, stages, minb, wpb;
 };
-static constexpr TmaCfg kTma2[kEpfTmaConfigs] = {{16, 2, 4}, {8, 1, 3}, {8, 4, 3}, {8, 2, 2}, {8, 1, 2}, {8, 2, 2}};
-static constexpr TmaCfg kTma3[kEpfTmaConfigs] = {{32, 2, 2}, {32, 4, 2}, {32, 1, 3}, {16, 2, 2}, {16, 1, 2}, {32, 2, 2}};
+#define PXB_TMA2(X)                                                                                   \
+    X(0, 16, 2, 4, 1, 8) X(1, 8, 1, 3, 1, 8) X(2, 8, 4, 3, 1, 8) X(3, 8, 2, 2, 3, 8) X(4, 8, 1, 2, 4, 8) \
+    X(5, 8, 2, 2, 4, 8) X(6, 4, 2, 2, 6, 4) X(7, 4, 4, 2, 4, 4) X(8, 8, 2, 2, 8, 4) X(9, 4, 2, 2, 3, 8)
+#define PXB_TMA3(X)                                                                                     \
+    X(0, 32, 2, 2, 1, 8) X(1, 32, 4, 2, 1, 8) X(2, 32, 1, 3, 1, 8) X(3, 16, 2, 2, 1, 8) X(4, 16, 1, 2, 2, 8) \
+    X(5, 32, 2, 2, 2, 8) X(6, 32, 2, 2, 2, 4) X(7, 32, 1, 2, 4, 4) X(8, 16, 2, 2, 2, 4) X(9, 16, 1, 2, 4, 4)
+#define PXB_CFG(i, l, u, st, mb, w) {l, u, st, mb, w},
+static constexpr TmaCfg kTma2[kEpfTmaConfigs] = {PXB_TMA2(PXB_CFG)};
+static constexpr TmaCfg kTma3[kEpfTmaConfigs] = {PXB_TMA3(PXB_CFG)};
+#undef PXB_CFG
 
 int epf_tma_lanes(int dim, int which) { return dim == 3 ? kTma3[which].lpn : kTma2[which].lpn; }
 
-int epf_tma_tile_nodes(int dim, int which) { return (kEpfThreads / kWarp) * (kWarp / epf_tma_lanes(dim, which)); }
+int epf_tma_tile_nodes(int dim, int which) {
+    const TmaCfg c = dim == 3 ? kTma3[which] : kTma2[which];
+    return c.wpb * (kWarp / c.lpn);
+}
 
 template <int DIM, bool MIXED>
 static size_t tma_smem_dm(int which, int maxb) {
     const TmaCfg c = DIM == 3 ? kTma3[which] : kTma2[which];
     size_t per = 0;
-    switch ((kEpfThreads / kWarp) * (kWarp / c.lpn)) {
+    switch (c.wpb * (kWarp / c.lpn)) {
+        case 4: per = StageLayout<DIM, MIXED, 4>::bytes(maxb); break;
         case 8: per = StageLayout<DIM, MIXED, 8>::bytes(maxb); break;
         case 16: per = StageLayout<DIM, MIXED, 16>::bytes(maxb); break;
-        default: per = StageLayout<DIM, MIXED, 32>::bytes(maxb); break;
+        case 32: per = StageLayout<DIM, MIXED, 32>::bytes(maxb); break;
+        default: per = StageLayout<DIM, MIXED, 64>::bytes(maxb); break;
     }
     return (size_t)c.stages * per;
 }
@@ -442,28 +452,20 @@ size_t epf_tma_smem(int dim, bool mixed, int which, int maxb) {
     return mixed ? tma_smem_dm<2, true>(which, maxb) : tma_smem_dm<2, false>(which, maxb);
 }
 
+#define PXB_CASE2(i, l, u, st, mb, w) \
+    case i: return launch_tma<2, MIXED, l, u, st, mb, w>(a, s);
+#define PXB_CASE3(i, l, u, st, mb, w) \
+    case i: return launch_tma<3, MIXED, l, u, st, mb, w>(a, s);
 template <int DIM, bool MIXED>
 static cudaError_t launch_tma_dm(const EpfArgs &a, int which, cudaStream_t s) {
     if constexpr (DIM == 3) {
-        switch (which) {
-            case 0: return launch_tma<3, MIXED, 32, 2, 2, 1>(a, s);
-            case 1: return launch_tma<3, MIXED, 32, 4, 2, 1>(a, s);
-            case 2: return launch_tma<3, MIXED, 32, 1, 3, 1>(a, s);
-            case 3: return launch_tma<3, MIXED, 16, 2, 2, 1>(a, s);
-            case 4: return launch_tma<3, MIXED, 16, 1, 2, 2>(a, s);
-            default: return launch_tma<3, MIXED, 32, 2, 2, 2>(a, s);
-        }
+        switch (which) { PXB_TMA3(PXB_CASE3) default: return cudaErrorInvalidValue; }
     } else {
-        switch (which) {
-            case 0: return launch_tma<2, MIXED, 16, 2, 4, 1>(a, s);
-            case 1: return launch_tma<2, MIXED, 8, 1, 3, 1>(a, s);
-            case 2: return launch_tma<2, MIXED, 8, 4, 3, 1>(a, s);
-            case 3: return launch_tma<2, MIXED, 8, 2, 2, 3>(a, s);
-            case 4: return launch_tma<2, MIXED, 8, 1, 2, 4>(a, s);
-            default: return launch_tma<2, MIXED, 8, 2, 2, 4>(a, s);
-        }
+        switch (which) { PXB_TMA2(PXB_CASE2) default: return cudaErrorInvalidValue; }
     }
 }
+#undef PXB_CASE2
+#undef PXB_CASE3
 
 cudaError_t launch_epf_tma(const EpfArgs &a, int dim, bool mixed, int which, cudaStream_t s) {
     if (dim == 3) return mixed ? launch_tma_dm<3, true>(a, which, s) : launch_tma_dm<3, false>(a, which, s);

@@ -166,7 +166,7 @@ def test_epf_rate_matches_reference(ctx, name, dim):
     assert np.abs(a - d["a_rand"]).max() <= 1e-12 * np.abs(d["a_rand"]).max()
 
 
-@pytest.mark.parametrize("variant", list(range(11)))
+@pytest.mark.parametrize("variant", list(range(15)))
 @pytest.mark.parametrize("name,dim", [("epf2d", 2), ("epf3d", 3)])
 def test_epf_trajectory_matches_reference(ctx, name, dim, variant):
     """Every schedule variant of the step kernel (lane groups, CSR-stream tiles, TMA-staged tiles)."""

@@ -12,7 +12,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 NSTEPS = 30
-N_VARIANTS = 11
+N_VARIANTS = 15
 
 
 @pytest.fixture(scope="module")
