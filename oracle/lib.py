@@ -261,6 +261,7 @@ def _ref_lib():
         L.ref_gbuild_time.restype = C.c_double
         L.ref_csr_nnz.restype = C.c_int
         L.ref_poisson_assemble.restype = C.c_double
+        L.ref_ch_assemble.restype = C.c_double
         L.ref_epf_create.restype = vp
         L.ref_epf_rate.restype = C.c_double
         L.ref_epf_run.restype = C.c_double
@@ -372,6 +373,24 @@ class RefMesh:
                                         _ptr(np.ascontiguousarray(u, np.float64), C.c_double), _ptr(kv, C.c_double),
                                         _ptr(rhs, C.c_double), int(nthreads or os.cpu_count()))
         return kv, rhs, t
+
+    def ch_assemble(self, chi, kappa, M0, dt, u, uold, nthreads=0):
+        """Cahn-Hilliard (2 dof) K/rhs through the reference element, plus its geometry (lambda-corrected
+        Laplacian per bond, reverse-bond index, ghost flags) and Picard mobility."""
+        nnz = self.L.ref_csr_nnz(self.h, 2)
+        nb = int(self.off[-1])
+        kv = np.zeros(nnz, np.float64)
+        rhs = np.zeros(2 * self.n, np.float64)
+        lap = np.zeros(nb, np.float64)
+        rev = np.zeros(nb, np.int32)
+        ghost = np.zeros(self.n, np.int8)
+        mnode = np.zeros(self.n, np.float64)
+        t = self.L.ref_ch_assemble(self.h, C.c_double(chi), C.c_double(kappa), C.c_double(M0), C.c_double(dt),
+                                   _ptr(np.ascontiguousarray(u, np.float64), C.c_double),
+                                   _ptr(np.ascontiguousarray(uold, np.float64), C.c_double), _ptr(kv, C.c_double),
+                                   _ptr(rhs, C.c_double), _ptr(lap, C.c_double), _ptr(rev, C.c_int),
+                                   _ptr(ghost, C.c_char), _ptr(mnode, C.c_double), int(nthreads or os.cpu_count()))
+        return kv, rhs, dict(lapbond=lap, rev=rev, isghost=ghost, mnode=mnode), t
 
     def bc_preset(self, bcs, t, u):
         p = bc_program_arrays(bcs, self.dim)

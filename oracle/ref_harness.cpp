@@ -310,6 +310,87 @@ double ref_poisson_assemble(void *h, double sigma, const double *fnode, const do
     return std::chrono::duration<double>(t1 - t0).count();
 }
 
+// ---- Cahn-Hilliard element (2 dof) ------------------------------------------------------------------------
+// CahnHilliardElement::preprocessIteration (one-off lambda-corrected Laplacian, reverse bonds, ghost flags,
+// then the Picard-frozen mobility) and its nodal/bond callbacks, accumulated like
+// FormResidualAndJacobianParallel.cpp:100-172 (K = -dF/dU, RHS = +F, row-owned).  Returns the element's geometry
+// (lapbond[nb], rev[nb] 0-based bond index or -1, isghost[n]) and mobility mnode[n] for the device assembler's
+// inputs.  Wall time in seconds of the assembly loop.
+double ref_ch_assemble(void *h, double chi, double kappa, double M0, double dt, const double *u, const double *uold,
+                       double *kvals, double *rhs, double *lapbond, int *rev, char *isghost, double *mnode,
+                       int nthreads) {
+    auto *m = static_cast<RefMesh *>(h);
+    const auto &d = m->pd.getDataConstRef();
+    const int n = d.NodesNum;
+    const int ndof = 2;
+    CahnHilliardElement el;
+    el.setDim(m->dim);
+    el.setChi(chi);
+    el.setKappa(kappa);
+    el.setMobility(M0);
+    VectorXd U(n * ndof), Uo(n * ndof);
+    std::memcpy(U.getDataPtr(), u, sizeof(double) * (size_t)n * ndof);
+    std::memcpy(Uo.getDataPtr(), uold, sizeof(double) * (size_t)n * ndof);
+    LocalElmtInfo info;
+    info.Dt = dt;
+    info.UseParallel = nthreads != 1;
+    PDOperators pops = m->ops;
+    pops.setAbortOnDegenerate(false);
+    el.preprocessIteration(m->pd, pops, info, ndof, U, Uo);
+    SparseMatrix K;
+    K.initFromPDMesh(d, ndof);
+    K.setToZeros();
+    std::vector<double> r((size_t)n * ndof, 0.0);
+    auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+    {
+        PDOperators ops = m->ops;
+        ops.setAbortOnDegenerate(false);
+        VectorXd R(ndof), Rn(ndof), UI(ndof), UJ(ndof), UoI(ndof), UoJ(ndof);
+        MatrixXd KII(ndof, ndof), KIJ(ndof, ndof), Kn(ndof, ndof);
+#pragma omp for schedule(guided)
+        for (int i = 1; i <= n; ++i) {
+            ops.calcAMatrix(i, d);
+            const int bi = (i - 1) * ndof;
+            for (int a = 1; a <= ndof; ++a) {
+                UI(a) = u[bi + a - 1];
+                UoI(a) = uold[bi + a - 1];
+            }
+            el.computeNodalResidualAndJacobian(info, i, UI, UoI, d.NodeVolumes[i - 1], Rn, Kn);
+            for (int a = 1; a <= ndof; ++a) {
+                r[bi + a - 1] += Rn(a);
+                for (int b = 1; b <= ndof; ++b) K.addValue(bi + a, bi + b, -Kn(a, b));
+            }
+            for (int j : d.NodesNeighNodesID[i - 1]) {
+                ops.calcOperators(i, j, d);
+                const int bj = (j - 1) * ndof;
+                for (int a = 1; a <= ndof; ++a) {
+                    UJ(a) = u[bj + a - 1];
+                    UoJ(a) = uold[bj + a - 1];
+                }
+                el.computeBondResidualAndJacobian(ops, info, i, j, UI, UJ, UoI, UoJ, d.NodeVolumes[i - 1], R, KII, KIJ);
+                for (int a = 1; a <= ndof; ++a) {
+                    r[bi + a - 1] += R(a);
+                    for (int b = 1; b <= ndof; ++b) {
+                        K.addValue(bi + a, bi + b, -KII(a, b));
+                        K.addValue(bi + a, bj + b, -KIJ(a, b));
+                    }
+                }
+            }
+        }
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    std::memcpy(kvals, K.getCSRValuesPtr(), sizeof(double) * (size_t)K.getNNZNum());
+    std::memcpy(rhs, r.data(), sizeof(double) * r.size());
+    const size_t nb = el.getLapBond().size();
+    if (lapbond) std::memcpy(lapbond, el.getLapBond().data(), sizeof(double) * nb);
+    if (rev) std::memcpy(rev, el.getRevBond().data(), sizeof(int) * nb);
+    if (isghost)
+        for (int i = 0; i < n; ++i) isghost[i] = el.getGhostFlags().empty() ? 0 : el.getGhostFlags()[(size_t)i];
+    if (mnode) std::memcpy(mnode, el.getNodeMobility().data(), sizeof(double) * (size_t)n);
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
 // ---- explicit_pddo_frac element -------------------------------------------------------------------------
 void *ref_epf_create(void *mesh, double E, double nu, double rho, double G0, int plane_stress, int tension_only,
                      int damage_on, double bx, double by, double bz) {

@@ -417,10 +417,12 @@ struct TmaCfg {
 };
 #define PXB_TMA2(X)                                                                                   \
     X(0, 16, 2, 4, 1, 8) X(1, 8, 1, 3, 1, 8) X(2, 8, 4, 3, 1, 8) X(3, 8, 2, 2, 3, 8) X(4, 8, 1, 2, 4, 8) \
-    X(5, 8, 2, 2, 4, 8) X(6, 4, 2, 2, 6, 4) X(7, 4, 4, 2, 4, 4) X(8, 8, 2, 2, 8, 4) X(9, 4, 2, 2, 3, 8)
+    X(5, 8, 2, 2, 4, 8) X(6, 4, 2, 2, 6, 4) X(7, 4, 4, 2, 4, 4) X(8, 8, 2, 2, 8, 4) X(9, 4, 2, 2, 3, 8) \
+    X(10, 2, 2, 2, 3, 4) X(11, 2, 4, 2, 3, 4) X(12, 4, 2, 3, 4, 4)
 #define PXB_TMA3(X)                                                                                     \
     X(0, 32, 2, 2, 1, 8) X(1, 32, 4, 2, 1, 8) X(2, 32, 1, 3, 1, 8) X(3, 16, 2, 2, 1, 8) X(4, 16, 1, 2, 2, 8) \
-    X(5, 32, 2, 2, 2, 8) X(6, 32, 2, 2, 2, 4) X(7, 32, 1, 2, 4, 4) X(8, 16, 2, 2, 2, 4) X(9, 16, 1, 2, 4, 4)
+    X(5, 32, 2, 2, 2, 8) X(6, 32, 2, 2, 2, 4) X(7, 32, 1, 2, 4, 4) X(8, 16, 2, 2, 2, 4) X(9, 16, 1, 2, 4, 4) \
+    X(10, 16, 2, 3, 2, 4) X(11, 32, 2, 3, 2, 4) X(12, 16, 1, 3, 4, 4)
 #define PXB_CFG(i, l, u, st, mb, w) {l, u, st, mb, w},
 static constexpr TmaCfg kTma2[kEpfTmaConfigs] = {PXB_TMA2(PXB_CFG)};
 static constexpr TmaCfg kTma3[kEpfTmaConfigs] = {PXB_TMA3(PXB_CFG)};
@@ -442,7 +444,7 @@ static size_t tma_smem_dm(int which, int maxb) {
         case 8: per = StageLayout<DIM, MIXED, 8>::bytes(maxb); break;
         case 16: per = StageLayout<DIM, MIXED, 16>::bytes(maxb); break;
         case 32: per = StageLayout<DIM, MIXED, 32>::bytes(maxb); break;
-        default: per = StageLayout<DIM, MIXED, 64>::bytes(maxb); break;
+        default: per = StageLayout<DIM, MIXED, 64>::bytes(maxb); break;  // 64 nodes (LPN 2 x 4 warps, LPN 4 x 8)
     }
     return (size_t)c.stages * per;
 }

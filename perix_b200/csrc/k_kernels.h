@@ -119,7 +119,7 @@ struct EpfArgs {
     unsigned int *err = nullptr;            // TMA variants: pipeline waits that ran out
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
-constexpr int kEpfTmaConfigs = 10;                // staged (TMA) configurations per dimension
+constexpr int kEpfTmaConfigs = 13;                // staged (TMA) configurations per dimension
 constexpr int kEpfVariants = 5 + kEpfTmaConfigs;  // 0-2 lane groups, 3-4 CSR tiles, 5.. staged
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s);
 // P[c][t] from G[c][t] (t < ldb, SoA stride ldb): 2D p11 = C11 Gxx + C66 Gyy, p22 = C66 Gxx + C11 Gyy,

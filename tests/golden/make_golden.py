@@ -51,6 +51,23 @@ def poisson_fixture():
          groups=np.concatenate([m.group(g + "nodes_ghost") for g in ("left", "right", "bottom", "top")]))
 
 
+def ch_fixture():
+    """Scaled C4: 32x32 lattice, h = 1/32, delta = 3.015h, c0 = 0.5 + U(-0.01, 0.01) (seeded), chi = 2.5,
+    M0 = 1, kappa = 1e-4, dt = 1e-6; u = (c, mu) interleaved with mu = f'(c) plus noise; uold = u with c moved."""
+    m = RefMesh.structured(2, 32, 32, 0, [0, 1, 0, 1], 3.015, 2)
+    rp2, cols2 = m.csr_pattern(2)
+    rng = np.random.default_rng(21)
+    chi, kappa, M0, dt = 2.5, 1e-4, 1.0, 1e-6
+    c = 0.5 + rng.uniform(-0.01, 0.01, m.n)
+    mu = np.log(c / (1 - c)) + chi * (1 - 2 * c) + rng.standard_normal(m.n) * 1e-3
+    u = np.stack([c, mu], 1).reshape(-1)
+    uold = u.copy()
+    uold[0::2] -= rng.uniform(-1e-4, 1e-4, m.n)
+    kv, rhs, geo, _ = m.ch_assemble(chi, kappa, M0, dt, u, uold)
+    save("ch32", **mesh_arrays(m), rowptr2=rp2, cols2=cols2, u=u, uold=uold,
+         params=np.array([chi, kappa, M0, dt]), kvals=kv, rhs=rhs, **geo)
+
+
 def lattice3d_fixture():
     m = RefMesh.structured(3, 5, 5, 4, [0, 0.5, 0, 0.5, 0, 0.4], 3.015, 2)
     ops, deg = m.gbuild()
@@ -180,3 +197,4 @@ if __name__ == "__main__":
     cloud_fixture(3, 8, 8)
     epf2d_fixture()
     epf3d_fixture()
+    ch_fixture()

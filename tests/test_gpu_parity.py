@@ -108,6 +108,27 @@ def test_apply_mixed_adjoint_is_transpose(ctx, slots):
     assert abs(lhs - rhs) <= 1e-11 * np.abs(out * y).sum()
 
 
+def test_ch_assembly_matches_reference(ctx):
+    """Conservative Cahn-Hilliard (2 dof) K and rhs against the reference element (CahnHilliardElement
+    preprocess + callbacks in the formResidualAndJacobianParallel accumulation), on the element's own geometry
+    (lambda-corrected Laplacian, reverse bonds, ghost flags) and Picard mobility.  K entries within 1e-12 of the
+    row's largest neighbour-block entry (the 1/dt diagonal would otherwise hide the bond terms), rhs within
+    1e-12 of its largest entry."""
+    d = load_golden("ch32")
+    geometry(ctx, d, 2)
+    ctx.csr_set_pattern(d["rowptr2"], d["cols2"], 2)
+    ctx.ch_set_geometry(d["rev"], d["lapbond"], d["isghost"])
+    chi, kappa, M0, dt = (float(x) for x in d["params"])
+    kv, rhs = ctx.assemble_ch(kappa, chi, dt, d["mnode"], d["u"], d["uold"])
+    rp, cols, ref = d["rowptr2"], d["cols2"], d["kvals"]
+    rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+    nbr_block = (cols // 2) != (rows // 2)
+    scale = np.zeros(rp.size - 1)
+    np.maximum.at(scale, rows[nbr_block], np.abs(ref[nbr_block]))
+    assert (np.abs(kv - ref) <= 1e-12 * scale[rows]).all()
+    assert np.abs(rhs - d["rhs"]).max() <= 1e-12 * np.abs(d["rhs"]).max()
+
+
 def test_poisson_assembly_matches_reference(ctx):
     d = load_golden("poisson16")
     geometry(ctx, d, 2)
@@ -166,7 +187,7 @@ def test_epf_rate_matches_reference(ctx, name, dim):
     assert np.abs(a - d["a_rand"]).max() <= 1e-12 * np.abs(d["a_rand"]).max()
 
 
-@pytest.mark.parametrize("variant", list(range(15)))
+@pytest.mark.parametrize("variant", list(range(18)))
 @pytest.mark.parametrize("name,dim", [("epf2d", 2), ("epf3d", 3)])
 def test_epf_trajectory_matches_reference(ctx, name, dim, variant):
     """Every schedule variant of the step kernel (lane groups, CSR-stream tiles, TMA-staged tiles)."""
