@@ -328,6 +328,8 @@ extern "C" int pxb_batch_autotune(pxb_ctx *c, int what, int reps, size_t flush_b
     int best_v = slot;
     for (int v = 0; v < kBatchVariants; ++v) {
         slot = v;
+        // one untimed launch first: a kernel's first launch in a process also loads its module
+        PXB_TRY(pxb_batch_time(c, what, 1, 0, u_d, out_d, ms.data()));
         PXB_TRY(pxb_batch_time(c, what, reps, flush_bytes, u_d, out_d, ms.data()));
         float mean = 0.f;
         for (float x : ms) mean += x;
