@@ -104,7 +104,7 @@ size_t ctx_bytes(const pxb_ctx *c) {
     s += bufsz(g.off) + bufsz(g.nbr) + bufsz(g.pos) + bufsz(g.vol) + bufsz(g.mirror) + bufsz(g.layer) + bufsz(g.rev);
     s += bufsz(c->ops.ops) + bufsz(c->ops.degenerate) + bufsz(c->ops.defect) + bufsz(c->ops.yeff);
     const EpfState &e = c->epf;
-    s += bufsz(e.G) + bufsz(e.P) + bufsz(e.health) + bufsz(e.u[0]) + bufsz(e.u[1]) + bufsz(e.accel) + bufsz(e.counters) +
+    s += bufsz(e.G) + bufsz(e.P) + bufsz(e.xib) + bufsz(e.health) + bufsz(e.u[0]) + bufsz(e.u[1]) + bufsz(e.accel) + bufsz(e.counters) +
          bufsz(e.umax) + bufsz(e.tsched);
     s += bufsz(e.bc.own) + bufsz(e.bc.src_off) + bufsz(e.bc.tgt) + bufsz(e.bc.comp) + bufsz(e.bc.form) +
          bufsz(e.bc.vals);
@@ -549,6 +549,7 @@ static EpfArgs epf_args(pxb_ctx *c) {
     a.n_broken = e.counters.as<unsigned long long>();
     a.err = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 2);
     a.P = e.P.p;
+    a.xib = e.xib.p ? e.xib.as<float>() : nullptr;
     if (epf_is_tma(e.variant)) a.maxb = epf_tma_maxb(g.dim, e.variant, g.max_family);
     return a;
 }
@@ -593,6 +594,13 @@ extern "C" int pxb_epf_setup(pxb_ctx *c, int precision, double C11, double C12, 
     PXB_CUDA_TRY(launch_navier_pack(e.G.p, e.P.p, (long long)ldb, g.dim, precision == PXB_MIXED, C11, C12, C66,
                                     c->stream));
     PXB_TRY(check_launch(c, "navier pack"));
+    if (precision == PXB_MIXED) {
+        PXB_TRY(dev_alloc(c, e.xib, sizeof(float) * (size_t)g.dim * ldb));
+        PXB_CUDA_TRY(cudaMemsetAsync(e.xib.p, 0, e.xib.bytes, c->stream));
+        PXB_CUDA_TRY(launch_bond_vectors(g.n, g.dim, g.off.as<int>(), g.nbr.as<int>(), g.pos.p, (long long)ldb,
+                                         e.xib.as<float>(), c->stream));
+        PXB_TRY(check_launch(c, "bond vectors"));
+    }
     e.ready = true;
     return PXB_OK;
 }

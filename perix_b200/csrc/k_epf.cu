@@ -566,6 +566,29 @@ __global__ void navier_pack_kernel(const T *G, T *P, long long ldb, double C11, 
     }
 }
 
+template <int DIM>
+__global__ void bond_vector_kernel(int n, const int *off, const int *nbr, const void *pos, long long ldb, float *xib) {
+    using PosT = typename Vec<DIM>::T;
+    const PosT *p = static_cast<const PosT *>(pos);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const PosT xi = p[i];
+        for (int t = off[i]; t < off[i + 1]; ++t) {
+            const PosT xj = p[nbr[t]];
+            xib[t] = (float)(xj.x - xi.x);
+            xib[ldb + t] = (float)(xj.y - xi.y);
+            if constexpr (DIM == 3) xib[2 * ldb + t] = (float)(xj.z - xi.z);
+        }
+    }
+}
+
+cudaError_t launch_bond_vectors(int n, int dim, const int *off, const int *nbr, const void *pos, long long ldb,
+                                float *xib, cudaStream_t s) {
+    const int grid = (int)std::min<long long>(((long long)n + 255) / 256, 148LL * 16);
+    if (dim == 3) bond_vector_kernel<3><<<grid > 0 ? grid : 1, 256, 0, s>>>(n, off, nbr, pos, ldb, xib);
+    else bond_vector_kernel<2><<<grid > 0 ? grid : 1, 256, 0, s>>>(n, off, nbr, pos, ldb, xib);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_navier_pack(const void *G, void *P, long long ldb, int dim, bool mixed, double C11, double C12,
                                double C66, cudaStream_t s) {
     const int grid = (int)std::min<long long>((ldb + 255) / 256, 148LL * 16);

@@ -107,8 +107,8 @@ __device__ __forceinline__ double pick_t(const double *v, int d) {
 }
 
 // stage layout (bytes, all sections 16-aligned): G[NC][maxb] | nbr[maxb] | health[maxb] | off[NT+16] |
-// pos[NT] | u[NT*DIM + 2] | uprev[NT*DIM + 2]
-template <int DIM, bool MIXED, int NT>
+// pos[NT] | u[NT*DIM + 2] | uprev[NT*DIM + 2] | (MIXED and XI) xi[DIM][maxb] FP32 bond vectors
+template <int DIM, bool MIXED, int NT, bool XI = false>
 struct StageLayout {
     static constexpr int NC = (DIM == 3) ? 6 : 3;
     static constexpr int ES = MIXED ? 4 : 8;
@@ -122,20 +122,51 @@ struct StageLayout {
     __host__ __device__ static unsigned up_off(int maxb) {
         return u_off(maxb) + (((unsigned)(NT * DIM + 2) * 8u + 15u) & ~15u);
     }
-    __host__ __device__ static unsigned bytes(int maxb) {
+    __host__ __device__ static unsigned xi_off(int maxb) {
         return up_off(maxb) + (((unsigned)(NT * DIM + 2) * 8u + 15u) & ~15u);
+    }
+    __host__ __device__ static unsigned bytes(int maxb) {
+        return xi_off(maxb) + ((MIXED && XI) ? (unsigned)(DIM * maxb) * 4u : 0u);
     }
 };
 
+// Stretch test of one bond in the reference's FP64 arithmetic (ExplicitPDDOFracElement.cpp:239-299): a squared
+// comparison decides bonds clearly away from the threshold, (sqrt(y2) - r)/r > s_c with rounded ops decides the
+// rest.  Returns 1 (breaks), 0 (holds), or 0 for a zero-length bond (never tested).
+template <int DIM, typename PosT>
+__device__ __forceinline__ int break_fp64(const PosT &xj, const PosT &xi, const double *e, const EpfArgs &a) {
+    double xv[DIM], yv[DIM];
+    xv[0] = __dsub_rn(xj.x, xi.x);
+    xv[1] = __dsub_rn(xj.y, xi.y);
+    if constexpr (DIM == 3) xv[2] = __dsub_rn(xj.z, xi.z);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
+    const double r2 = dot_rn_t<DIM>(xv, xv);
+    if (!(r2 > 0.0)) return 0;
+    const double y2 = dot_rn_t<DIM>(yv, yv);
+    const double band = 1.0e-6 * r2;
+    const double qh = y2 - a.sc_hi2 * r2;
+    if (a.tension_only) {
+        if (qh > band) return 1;
+        if (qh < -band) return 0;
+        return ref_stretch_t(y2, r2) > a.sc ? 1 : 0;
+    }
+    const double ql = a.sc_lo2 * r2 - y2;
+    if (qh > band || ql > band) return 1;
+    if (qh < -band && ql < -band) return 0;
+    return fabs(ref_stretch_t(y2, r2)) > a.sc ? 1 : 0;
+}
+
 }  // namespace
 
-template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB>
+template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB, bool XI>
 __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
+    constexpr bool XS = MIXED && XI;  // staged FP32 bond vectors and the FP32 stretch pre-test
     using PosT = typename Vec<DIM>::T;
     using GT = typename std::conditional<MIXED, float, double>::type;
     constexpr int GPW = kWarp / LPN;
     constexpr int NT = WPB * GPW;
-    using SL = StageLayout<DIM, MIXED, NT>;
+    using SL = StageLayout<DIM, MIXED, NT, XI>;
     constexpr int NC = SL::NC;
 
     extern __shared__ __align__(128) unsigned char smem[];
@@ -157,6 +188,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     const PosT *pos = static_cast<const PosT *>(a.pos);
     const GT *Pg = static_cast<const GT *>(a.P);
     const double t_new = a.t_sched[a.step_in_chunk];
+    const float sc_hi2f = (float)a.sc_hi2, sc_lo2f = (float)a.sc_lo2;
 
     const int ntiles = (a.n + NT - 1) / NT;
     const int mycount = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -175,7 +207,8 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         const unsigned bytes_off = up16((unsigned)(cnt + 1) * 4u);
         const unsigned bytes_pos = (unsigned)cnt * SL::PS;
         const unsigned bytes_u = up16((unsigned)cnt * DIM * 8u);
-        const unsigned total = NC * bytes_g + bytes_n + bytes_h + bytes_off + bytes_pos + bytes_u * 2u;
+        const unsigned total = NC * bytes_g + bytes_n + bytes_h + bytes_off + bytes_pos + bytes_u * 2u +
+                               (XS ? (unsigned)DIM * bytes_n : 0u);
         s_t0a[st] = t0a;
         s_last[st] = k;
         fence_proxy_async();
@@ -189,6 +222,12 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         bulk_g2s(base + SL::pos_off(maxb), pos + n0, bytes_pos, &bar[st]);
         bulk_g2s(base + SL::u_off(maxb), a.u + (size_t)n0 * DIM, bytes_u, &bar[st]);
         bulk_g2s(base + SL::up_off(maxb), a.u_other + (size_t)n0 * DIM, bytes_u, &bar[st]);
+        if constexpr (XS) {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+                bulk_g2s(base + SL::xi_off(maxb) + (size_t)d * maxb * 4u, a.xib + (size_t)d * a.nb + t0a, bytes_n,
+                         &bar[st]);
+        }
     };
 
     if (tid == 0) {
@@ -223,6 +262,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         const PosT *sPos = reinterpret_cast<const PosT *>(base + SL::pos_off(maxb));
         const double *sU = reinterpret_cast<const double *>(base + SL::u_off(maxb));
         const double *sUp = reinterpret_cast<const double *>(base + SL::up_off(maxb));
+        const float *sXi = reinterpret_cast<const float *>(base + SL::xi_off(maxb));
         const int t0a = s_t0a[st];
         const int n0 = ((int)blockIdx.x + k * (int)gridDim.x) * NT;
         const int cnt = min(NT, a.n - n0);
@@ -260,7 +300,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
 #pragma unroll
             for (int q = 0; q < UNR; ++q) {
                 if (h[q]) {
-                    xj[q] = ldg_vec(pos + j[q]);
+                    if constexpr (!XS) xj[q] = ldg_vec(pos + j[q]);
                     if constexpr (DIM == 2) {
                         const double2 v = __ldg(reinterpret_cast<const double2 *>(a.u) + j[q]);
                         uj[q][0] = v.x;
@@ -279,33 +319,43 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) e[d] = __dsub_rn(uj[q][d], ui[d]);
                 if (a.damage) {
-                    double xv[DIM], yv[DIM];
-                    xv[0] = __dsub_rn(xj[q].x, xi.x);
-                    xv[1] = __dsub_rn(xj[q].y, xi.y);
-                    if constexpr (DIM == 3) xv[2] = __dsub_rn(xj[q].z, xi.z);
+                    int brk;
+                    if constexpr (XS) {
+                        // FP32 squared test on the staged FP32 bond vector.  Its error (ξ rounded to FP32, e
+                        // rounded, FP32 sums: < 1e-6 r^2 wherever |y|^2 is near (1 +- s_c)^2 r^2) stays well inside
+                        // the 4e-6 r^2 band; inside the band the reference arithmetic decides on the exact
+                        // positions (gathered only then), so decisions equal the FP64 path's.
+                        float xf[DIM], yf[DIM];
 #pragma unroll
-                    for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
-                    const double r2 = dot_rn_t<DIM>(xv, xv);
-                    if (r2 > 0.0) {
-                        const double y2 = dot_rn_t<DIM>(yv, yv);
-                        const double band = 1.0e-6 * r2;
-                        const double qh = y2 - a.sc_hi2 * r2;
-                        bool brk;
-                        if (a.tension_only) {
-                            if (qh > band) brk = true;
-                            else if (qh < -band) brk = false;
-                            else brk = ref_stretch_t(y2, r2) > a.sc;
-                        } else {
-                            const double ql = a.sc_lo2 * r2 - y2;
-                            if (qh > band || ql > band) brk = true;
-                            else if (qh < -band && ql < -band) brk = false;
-                            else brk = fabs(ref_stretch_t(y2, r2)) > a.sc;
+                        for (int d = 0; d < DIM; ++d) {
+                            xf[d] = sXi[(size_t)d * maxb + t];
+                            yf[d] = xf[d] + (float)e[d];
                         }
-                        if (brk) {
-                            a.health[t0a + t] = 0;
-                            ++broken;
-                            continue;
+                        float r2f = xf[0] * xf[0] + xf[1] * xf[1];
+                        float y2f = yf[0] * yf[0] + yf[1] * yf[1];
+                        if constexpr (DIM == 3) {
+                            r2f += xf[2] * xf[2];
+                            y2f += yf[2] * yf[2];
                         }
+                        brk = 0;
+                        if (r2f > 0.f) {
+                            const float bandf = 4.0e-6f * r2f;
+                            const float qh = y2f - sc_hi2f * r2f;
+                            if (a.tension_only) {
+                                brk = qh > bandf ? 1 : (qh < -bandf ? 0 : -1);
+                            } else {
+                                const float ql = sc_lo2f * r2f - y2f;
+                                brk = (qh > bandf || ql > bandf) ? 1 : ((qh < -bandf && ql < -bandf) ? 0 : -1);
+                            }
+                            if (brk < 0) brk = break_fp64<DIM>(ldg_vec(pos + j[q]), xi, e, a);
+                        }
+                    } else {
+                        brk = break_fp64<DIM>(xj[q], xi, e, a);
+                    }
+                    if (brk) {
+                        a.health[t0a + t] = 0;
+                        ++broken;
+                        continue;
                     }
                 }
                 double pd[NC];
@@ -387,11 +437,11 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     }
 }
 
-template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB>
+template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB, bool XI>
 static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
     constexpr int NT = WPB * (kWarp / LPN);
-    using SL = StageLayout<DIM, MIXED, NT>;
-    auto k = epf_tma_kernel<DIM, MIXED, LPN, UNR, S, MINB, WPB>;
+    using SL = StageLayout<DIM, MIXED, NT, XI>;
+    auto k = epf_tma_kernel<DIM, MIXED, LPN, UNR, S, MINB, WPB, XI>;
     const size_t smem = (size_t)S * SL::bytes(a.maxb);
     static size_t configured = 0;
     if (smem > configured) {
@@ -411,19 +461,22 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
 }
 
 // Staged configurations: lanes per node, bonds per lane per pass, stages, minimum resident blocks (launch
-// bounds), warps per block.  A tile is WPB * 32/LPN nodes.
+// bounds), warps per block, staged FP32 bond vectors (mixed only: the stretch pre-test reads them instead of
+// gathering neighbour positions, for 4 (2D) / 12 (3D) more staged bytes per bond).  A tile is WPB * 32/LPN nodes.
 struct TmaCfg {
-    int lpn, unr, stages, minb, wpb;
+    int lpn, unr, stages, minb, wpb, xi;
 };
-#define PXB_TMA2(X)                                                                                   \
-    X(0, 16, 2, 4, 1, 8) X(1, 8, 1, 3, 1, 8) X(2, 8, 4, 3, 1, 8) X(3, 8, 2, 2, 3, 8) X(4, 8, 1, 2, 4, 8) \
-    X(5, 8, 2, 2, 4, 8) X(6, 4, 2, 2, 6, 4) X(7, 4, 4, 2, 4, 4) X(8, 8, 2, 2, 8, 4) X(9, 4, 2, 2, 3, 8) \
-    X(10, 2, 2, 2, 3, 4) X(11, 2, 4, 2, 3, 4) X(12, 4, 2, 3, 4, 4)
-#define PXB_TMA3(X)                                                                                     \
-    X(0, 32, 2, 2, 1, 8) X(1, 32, 4, 2, 1, 8) X(2, 32, 1, 3, 1, 8) X(3, 16, 2, 2, 1, 8) X(4, 16, 1, 2, 2, 8) \
-    X(5, 32, 2, 2, 2, 8) X(6, 32, 2, 2, 2, 4) X(7, 32, 1, 2, 4, 4) X(8, 16, 2, 2, 2, 4) X(9, 16, 1, 2, 4, 4) \
-    X(10, 16, 2, 3, 2, 4) X(11, 32, 2, 3, 2, 4) X(12, 16, 1, 3, 4, 4)
-#define PXB_CFG(i, l, u, st, mb, w) {l, u, st, mb, w},
+#define PXB_TMA2(X)                                                                                               \
+    X(0, 16, 2, 4, 1, 8, 0) X(1, 8, 1, 3, 1, 8, 0) X(2, 8, 4, 3, 1, 8, 0) X(3, 8, 2, 2, 3, 8, 0)                 \
+    X(4, 8, 1, 2, 4, 8, 0) X(5, 8, 2, 2, 4, 8, 0) X(6, 4, 2, 2, 6, 4, 0) X(7, 4, 4, 2, 4, 4, 0)                  \
+    X(8, 8, 2, 2, 8, 4, 0) X(9, 4, 2, 2, 3, 8, 0) X(10, 4, 2, 2, 6, 4, 1) X(11, 4, 4, 2, 4, 4, 1)                \
+    X(12, 8, 2, 2, 6, 4, 1)
+#define PXB_TMA3(X)                                                                                               \
+    X(0, 32, 2, 2, 1, 8, 0) X(1, 32, 4, 2, 1, 8, 0) X(2, 32, 1, 3, 1, 8, 0) X(3, 16, 2, 2, 1, 8, 0)              \
+    X(4, 16, 1, 2, 2, 8, 0) X(5, 32, 2, 2, 2, 8, 0) X(6, 32, 2, 2, 2, 4, 1) X(7, 32, 1, 2, 4, 4, 1)              \
+    X(8, 16, 2, 2, 2, 4, 1) X(9, 16, 1, 2, 4, 4, 1) X(10, 16, 2, 3, 2, 4, 1) X(11, 32, 2, 3, 2, 4, 1)            \
+    X(12, 16, 1, 3, 4, 4, 1)
+#define PXB_CFG(i, l, u, st, mb, w, x) {l, u, st, mb, w, x},
 static constexpr TmaCfg kTma2[kEpfTmaConfigs] = {PXB_TMA2(PXB_CFG)};
 static constexpr TmaCfg kTma3[kEpfTmaConfigs] = {PXB_TMA3(PXB_CFG)};
 #undef PXB_CFG
@@ -435,17 +488,22 @@ int epf_tma_tile_nodes(int dim, int which) {
     return c.wpb * (kWarp / c.lpn);
 }
 
+template <int DIM, bool MIXED, bool XI>
+static size_t tma_stage_bytes(int nt, int maxb) {
+    switch (nt) {
+        case 4: return StageLayout<DIM, MIXED, 4, XI>::bytes(maxb);
+        case 8: return StageLayout<DIM, MIXED, 8, XI>::bytes(maxb);
+        case 16: return StageLayout<DIM, MIXED, 16, XI>::bytes(maxb);
+        case 32: return StageLayout<DIM, MIXED, 32, XI>::bytes(maxb);
+        default: return StageLayout<DIM, MIXED, 64, XI>::bytes(maxb);  // 64 nodes (LPN 4 x 8 warps)
+    }
+}
+
 template <int DIM, bool MIXED>
 static size_t tma_smem_dm(int which, int maxb) {
     const TmaCfg c = DIM == 3 ? kTma3[which] : kTma2[which];
-    size_t per = 0;
-    switch (c.wpb * (kWarp / c.lpn)) {
-        case 4: per = StageLayout<DIM, MIXED, 4>::bytes(maxb); break;
-        case 8: per = StageLayout<DIM, MIXED, 8>::bytes(maxb); break;
-        case 16: per = StageLayout<DIM, MIXED, 16>::bytes(maxb); break;
-        case 32: per = StageLayout<DIM, MIXED, 32>::bytes(maxb); break;
-        default: per = StageLayout<DIM, MIXED, 64>::bytes(maxb); break;  // 64 nodes (LPN 2 x 4 warps, LPN 4 x 8)
-    }
+    const int nt = c.wpb * (kWarp / c.lpn);
+    const size_t per = c.xi ? tma_stage_bytes<DIM, MIXED, true>(nt, maxb) : tma_stage_bytes<DIM, MIXED, false>(nt, maxb);
     return (size_t)c.stages * per;
 }
 
@@ -454,10 +512,10 @@ size_t epf_tma_smem(int dim, bool mixed, int which, int maxb) {
     return mixed ? tma_smem_dm<2, true>(which, maxb) : tma_smem_dm<2, false>(which, maxb);
 }
 
-#define PXB_CASE2(i, l, u, st, mb, w) \
-    case i: return launch_tma<2, MIXED, l, u, st, mb, w>(a, s);
-#define PXB_CASE3(i, l, u, st, mb, w) \
-    case i: return launch_tma<3, MIXED, l, u, st, mb, w>(a, s);
+#define PXB_CASE2(i, l, u, st, mb, w, x) \
+    case i: return launch_tma<2, MIXED, l, u, st, mb, w, (x != 0)>(a, s);
+#define PXB_CASE3(i, l, u, st, mb, w, x) \
+    case i: return launch_tma<3, MIXED, l, u, st, mb, w, (x != 0)>(a, s);
 template <int DIM, bool MIXED>
 static cudaError_t launch_tma_dm(const EpfArgs &a, int which, cudaStream_t s) {
     if constexpr (DIM == 3) {

@@ -91,6 +91,7 @@ struct EpfArgs {
     const void *pos = nullptr;
     const void *G = nullptr;  // SoA [c][nb]
     const void *P = nullptr;  // TMA variants: packed Navier coefficients SoA [c][nb] (navier_pack)
+    const float *xib = nullptr;  // mixed TMA variants: reference bond vectors x_j - x_i, FP32 SoA [dim][nb]
     uint8_t *health = nullptr;
     double C11 = 0, C12 = 0, C66 = 0, rho = 1, b[3] = {0, 0, 0};
     double sc = 0;                  // critical stretch
@@ -124,6 +125,9 @@ constexpr int kEpfVariants = 5 + kEpfTmaConfigs;  // 0-2 lane groups, 3-4 CSR ti
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s);
 // P[c][t] from G[c][t] (t < ldb, SoA stride ldb): 2D p11 = C11 Gxx + C66 Gyy, p22 = C66 Gxx + C11 Gyy,
 // pxy = (C12 + C66) Gxy; 3D p11/p22/p33 and (C12 + C66) times Gxy, Gxz, Gyz
+// xib[d][t] = (float)(x_j - x_i)[d] for every bond t = (i -> j) (t < off[n]; the tail is left as it is)
+cudaError_t launch_bond_vectors(int n, int dim, const int *off, const int *nbr, const void *pos, long long ldb,
+                                float *xib, cudaStream_t s);
 cudaError_t launch_navier_pack(const void *G, void *P, long long ldb, int dim, bool mixed, double C11, double C12,
                                double C66, cudaStream_t s);
 int epf_grid(int n, int dim, int variant);

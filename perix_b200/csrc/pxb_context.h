@@ -116,6 +116,7 @@ struct EpfState {
     int tension_only = 1;
     DevBuf G;          // SoA Navier operators [c][ldb], double or float (c = 3 in 2D, 6 in 3D)
     DevBuf P;          // SoA packed Navier coefficients [c][ldb] (same type): the staged step kernels' stream
+    DevBuf xib;        // mixed: FP32 reference bond vectors [dim][ldb] (the staged kernels' stretch pre-test)
     DevBuf health;     // uint8 [ldb] (zero tail)
     DevBuf u[2];       // double [n*dim + 8] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
     DevBuf accel;      // double [n*dim]

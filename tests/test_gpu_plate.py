@@ -71,3 +71,32 @@ def test_plate_mixed_within_1e6(ctx, plate, variant):
     assert np.abs(u - u_ref).max() <= 1e-6 * np.abs(u_ref).max()
     # FP32 operator storage may move a bond across the critical stretch only where it sits within round-off
     assert (h != h_ref).sum() <= 1e-4 * h.size
+
+
+@pytest.mark.parametrize("variant", list(range(5, N_VARIANTS)))
+def test_plate_mixed_staged_damage_decisions_exact(ctx, plate, variant):
+    """The staged kernels' mixed stretch pre-test (FP32 bond vectors, 4e-6 r^2 band, exact fallback) must decide
+    every bond like the FP64 reference arithmetic: one step from the random field, against variant 1 (lane
+    groups, exact positions) on the same state."""
+    w, u0, _, _, _ = plate
+    _, _, h_ref, _ = _run_steps(ctx, w, u0, 1, precision=1, variant=1)
+    _, _, h, _ = _run_steps(ctx, w, u0, 1, precision=1, variant=variant)
+    assert (h_ref == 0).sum() > (w["health0"] == 0).sum() + 1000
+    assert np.array_equal(h, h_ref)
+
+
+def _run_steps(ctx, w, u0, nsteps, precision, variant):
+    import perix_b200 as px
+    L = w["L"]
+    ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
+    C11, C12, C66 = w["C"]
+    ctx.epf_setup(C11, C12, C66, w["rho"], (0.0, 0.0), w["sc"], True, health0=w["health0"], precision=precision)
+    try:
+        ctx.epf_set_variant(variant)
+    except px.PxbError as e:
+        assert e.status == 7
+        pytest.skip("variant %d does not fit these families" % variant)
+    ctx.epf_set_bcs(w["bcs"])
+    ctx.epf_start(u0, None, w["dt"])
+    ctx.epf_advance(nsteps, chunk=nsteps)
+    return ctx.epf_state()
