@@ -162,6 +162,86 @@ def c5_measure(px, device=0, steps=50, adjoint_steps=1000, checkpoint_every=100)
     return res
 
 
+def c1_poisson(px, kvals, rhs, L, rowptr, cols):
+    """One static solve of the assembled C1 system (K dU = RHS from U = 0, the Newton step of a linear problem)
+    after the reference's Dirichlet row replacement on the ghost layer (DirichletBC.cpp:176-231: ghost row g
+    becomes s*(dU_g + dU_b) = s*(2*0 - U_g - U_b), reflecting through the wall).  Host direct solve (the solve is
+    not on the hot path); returns U and the relative L2 error against sin(pi x) sin(pi y) over the bulk nodes."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    n = L.n
+    K = sp.csr_matrix((np.asarray(kvals, np.float64), np.asarray(cols), np.asarray(rowptr)), shape=(n, n)).tolil()
+    b = np.asarray(rhs, np.float64).copy()
+    for g in np.nonzero(L.mirror > 0)[0]:
+        K.rows[g] = [g, int(L.mirror[g]) - 1]
+        K.data[g] = [1.0, 1.0]
+        b[g] = 0.0
+    U = spla.spsolve(K.tocsr(), b)
+    x, y = L.coords[0::3], L.coords[1::3]
+    bulk = L.mirror == 0
+    ex = np.sin(math.pi * x) * np.sin(math.pi * y)
+    err = math.sqrt(float(((U - ex)[bulk] ** 2 * L.vols[bulk]).sum()) / float((ex[bulk] ** 2 * L.vols[bulk]).sum()))
+    return U, err
+
+
+def c1_measure(px, device=0, reps=20):
+    """64x64 cell-centred lattice on the unit square, delta = 3.015h, order 2, sigma = 1,
+    f = 2 pi^2 sin(pi x) sin(pi y), reflected Dirichlet 0 on the four ghost groups.  FP64 g-build and Poisson
+    assembly on the GPU (CUDA events), one host solve, L2 error; the reference's OpenMP assembly of the same
+    system through oracle/_ref is timed beside it when present."""
+    import torch
+    L = px.lattice(2, 64, 64, 0, [0.0, 1.0, 0.0, 1.0])
+    delta = 3.015 * L.dxyz[0] * (1.0 + 1e-6)
+    off, ids = px.families(L.coords, delta, False, mirror=L.mirror)
+    rowptr, cols = px.csr_pattern(off, ids, L.mirror, 1)
+    ctx = px.Context(device)
+    ctx.set_geometry(L.coords, L.vols, off, ids, delta, L.dxyz[0], 2, mirror=L.mirror)
+    gb, gb_ms = gbuild_rate(px, ctx, "fp64", reps=5)
+    ctx.gbuild(2, px.FP64)
+    ctx.csr_set_pattern(rowptr, cols, 1)
+    x, y = L.coords[0::3], L.coords[1::3]
+    f = 2 * math.pi ** 2 * np.sin(math.pi * x) * np.sin(math.pi * y)
+    dev = torch.device("cuda", device)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    fd = torch.from_numpy(f).to(dev)
+    ud = torch.zeros(L.n, dtype=torch.float64, device=dev)
+    kd = torch.empty(int(rowptr[-1]), dtype=torch.float64, device=dev)
+    rd = torch.empty(L.n, dtype=torch.float64, device=dev)
+    import ctypes as C
+
+    def assemble():
+        st = ctx.L.pxb_assemble_scalar_d(ctx.h, 0, C.c_double(1.0), C.c_double(0.0), C.c_void_p(fd.data_ptr()),
+                                         C.c_double(0.0), C.c_void_p(ud.data_ptr()), None, C.c_void_p(kd.data_ptr()),
+                                         C.c_void_p(rd.data_ptr()))
+        if st:
+            raise RuntimeError(ctx.L.pxb_last_error().decode())
+
+    for _ in range(3):
+        assemble()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    for _ in range(reps):
+        assemble()
+    ev[1].record()
+    torch.cuda.synchronize(dev)
+    asm_ms = ev[0].elapsed_time(ev[1]) / reps
+    U, err = c1_poisson(px, kd.cpu().numpy(), rd.cpu().numpy(), L, rowptr, cols)
+    res = {"nodes": L.n, "bonds": int(off[-1]), "nnz": int(rowptr[-1]), "gbuild_ms": gb_ms,
+           "assembly_ms": asm_ms, "l2_rel_error_vs_exact": err}
+    try:
+        from oracle import RefMesh, ref_available
+        if ref_available():
+            m = RefMesh.structured(2, 64, 64, 0, [0, 1, 0, 1], 3.015, 2)
+            m.gbuild()
+            _, _, t = m.poisson_assemble(1.0, f, np.zeros(m.n))
+            res["reference_cpu_assembly_ms"] = t * 1e3
+            res["reference_cpu_threads"] = os.cpu_count()
+    except Exception as e:  # noqa: BLE001
+        res["reference_cpu_assembly_ms"] = "unavailable: %s" % e
+    ctx.close()
+    return res
+
+
 def c3_clouds(px, nclouds=256, nmin=1000, nmax=200000, seed=2024):
     """Batched-cloud workload: clouds alternate 2D / 3D (half each), node counts log-uniform in [nmin, nmax]
     (seeded), cell-centred lattice of spacing h = 1 mm jittered by U(-0.2h, 0.2h) per coordinate, no ghosts
@@ -557,7 +637,7 @@ def run_perix(args):
     traffic = read_traffic(head)
     e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, max(10, min(steps, 200)))
     cpu = None
-    c3 = c5 = refgpu = None
+    c3 = c5 = refgpu = c1 = None
     if rank == 0 and ws == 1:
         cpu = cpu_reference(w, 20, 2)
         for p in out.values():
@@ -565,6 +645,7 @@ def run_perix(args):
         c3 = c3_measure(px, device=local)
         c5 = c5_measure(px, device=local)
         refgpu = reference_gpu()
+        c1 = c1_measure(px, device=local)
     if rank != 0:
         return
     line = {
@@ -606,6 +687,7 @@ def run_perix(args):
         "batched_clouds": c3,
         "slab_3d": c5,
         "reference_gpu": refgpu,
+        "poisson_c1": c1,
         "gbuild_nodes_per_s": {"fp64": out["fp64"]["gbuild"], "mixed": out["mixed"]["gbuild"],
                                "ms": {"fp64": out["fp64"]["gbuild_ms"], "mixed": out["mixed"]["gbuild_ms"]},
                                "workload": "order-2 g-build of the same plate (81,200 nodes, all 5 operators stored)"},

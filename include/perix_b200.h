@@ -244,6 +244,17 @@ int pxb_assemble_scalar_d(pxb_ctx *ctx, int type, double coef, double f, const d
  * reverse-bond map rev[nbtot], ghost flags and Picard-frozen mobility (reference
  * src/PDSystem/CudaAssembleKernels.cu:1277-1323 boundary; physics CahnHilliardElement.cpp:178-292). */
 int pxb_ch_set_geometry(pxb_ctx *ctx, const int *rev, const double *lapbond, const char *isghost);
+/* The same geometry built on the device from the order-2 operator cache (the one-off part of
+ * CahnHilliardElement::preprocessIteration, CahnHilliardElement.cpp:93-152): lapbond = g_xx + g_yy (+ g_zz),
+ * times lambda = 2 dim / sum_j g2_ij (|x_j|^2 - |x_i|^2) on bonds to non-ghost nodes; rev = reverse-bond index
+ * (0-based, -1 when absent); isghost from the mirror map.  pxb_ch_get_geometry reads them back. */
+int pxb_ch_build_geometry(pxb_ctx *ctx);
+int pxb_ch_get_geometry(pxb_ctx *ctx, int *rev, double *lapbond, char *isghost);
+/* Picard-frozen mobility M(c) = M0 c (1 - c), c = u[2i] clamped to [1e-8, 1 - 1e-8] (CahnHilliardElement.cpp:45-50),
+ * and the assembly on device buffers (no host copies). */
+int pxb_ch_mobility_d(pxb_ctx *ctx, double M0, const double *u_d, double *mnode_d);
+int pxb_assemble_ch_d(pxb_ctx *ctx, double kappa, double chi, double dt, const double *mnode_d, const double *u_d,
+                      const double *uold_d, double *kvals_d, double *rhs_d);
 int pxb_assemble_ch(pxb_ctx *ctx, double kappa, double chi, double dt, const double *mnode, const double *u,
                     const double *uold, double *kvals, double *rhs);
 

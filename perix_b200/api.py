@@ -527,6 +527,23 @@ class Context:
         g = None if isghost is None else np.ascontiguousarray(isghost, np.int8)
         _check(self.L.pxb_ch_set_geometry(self.h, _p(_i32(rev), C.c_int), _p(_f64(lapbond)), _p(g, C.c_char)))
 
+    def ch_build_geometry(self):
+        _check(self.L.pxb_ch_build_geometry(self.h))
+
+    def ch_get_geometry(self):
+        rev = np.zeros(max(1, self.nb), np.int32)
+        lap = np.zeros(max(1, self.nb), np.float64)
+        ghost = np.zeros(self.n, np.int8)
+        _check(self.L.pxb_ch_get_geometry(self.h, _p(rev, C.c_int), _p(lap), _p(ghost, C.c_char)))
+        return rev[:self.nb], lap[:self.nb], ghost
+
+    def ch_mobility_d(self, M0, u_ptr, mnode_ptr):
+        _check(self.L.pxb_ch_mobility_d(self.h, C.c_double(M0), _p(u_ptr), _p(mnode_ptr)))
+
+    def assemble_ch_d(self, kappa, chi, dt, mnode_ptr, u_ptr, uold_ptr, kvals_ptr, rhs_ptr):
+        _check(self.L.pxb_assemble_ch_d(self.h, C.c_double(kappa), C.c_double(chi), C.c_double(dt), _p(mnode_ptr),
+                                        _p(u_ptr), _p(uold_ptr), _p(kvals_ptr), _p(rhs_ptr)))
+
     def assemble_ch(self, kappa, chi, dt, mnode, u, uold):
         kv = np.zeros(self.nnz, np.float64)
         rhs = np.zeros(2 * self.n, np.float64)

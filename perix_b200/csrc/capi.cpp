@@ -1141,6 +1141,87 @@ extern "C" int pxb_ch_set_geometry(pxb_ctx *c, const int *rev, const double *lap
     return PXB_OK;
 }
 
+extern "C" int pxb_ch_build_geometry(pxb_ctx *c) {
+    PXB_TRY(need_geometry(c, "pxb_ch_build_geometry"));
+    const OpsCache &o = c->ops;
+    if (!o.ready || o.order != 2) return fail(PXB_ERR_STATE, "pxb_ch_build_geometry: needs an order-2 operator cache (pxb_gbuild)");
+    const int dim = c->g.dim;
+    auto slot = [&](int p, int q, int r) {
+        for (int k = 0; k < o.nop; ++k)
+            if (o.pqr[3 * k] == p && o.pqr[3 * k + 1] == q && o.pqr[3 * k + 2] == r) return k;
+        return -1;
+    };
+    const int sxx = slot(2, 0, 0), syy = slot(0, 2, 0), szz = dim == 3 ? slot(0, 0, 2) : 0;
+    ChState &h = c->ch;
+    PXB_TRY(ensure_rev(c));
+    const size_t nb = (size_t)std::max(1LL, c->g.nb);
+    PXB_TRY(dev_alloc(c, h.rev, sizeof(int) * nb));
+    PXB_CUDA_TRY(cudaMemcpyAsync(h.rev.p, c->g.rev.p, sizeof(int) * (size_t)c->g.nb, cudaMemcpyDeviceToDevice, c->stream));
+    PXB_TRY(dev_alloc(c, h.lap, sizeof(double) * nb));
+    PXB_TRY(dev_alloc(c, h.ghost, (size_t)c->g.n));
+    PXB_CUDA_TRY(launch_ch_geometry(c->g.n, dim, c->g.off.as<int>(), c->g.nbr.as<int>(), c->g.pos.p,
+                                    c->g.mirror.p ? c->g.mirror.as<int>() : nullptr, o.ops.p, o.precision == PXB_MIXED,
+                                    o.nop, sxx, syy, szz, h.lap.as<double>(), h.ghost.as<char>(), c->stream));
+    PXB_TRY(check_launch(c, "ch geometry"));
+    PXB_TRY(sync(c));
+    h.ready = true;
+    return PXB_OK;
+}
+
+extern "C" int pxb_ch_get_geometry(pxb_ctx *c, int *rev, double *lapbond, char *isghost) {
+    PXB_TRY(need_geometry(c, "pxb_ch_get_geometry"));
+    if (!c->ch.ready) return fail(PXB_ERR_STATE, "pxb_ch_get_geometry: no CH geometry");
+    const size_t nb = (size_t)c->g.nb;
+    if (rev) PXB_TRY(d2h(c, rev, c->ch.rev.p, sizeof(int) * nb));
+    if (lapbond) PXB_TRY(d2h(c, lapbond, c->ch.lap.p, sizeof(double) * nb));
+    if (isghost && c->ch.ghost.p) PXB_TRY(d2h(c, isghost, c->ch.ghost.p, (size_t)c->g.n));
+    return sync(c);
+}
+
+extern "C" int pxb_ch_mobility_d(pxb_ctx *c, double M0, const double *u_d, double *mnode_d) {
+    PXB_TRY(need_geometry(c, "pxb_ch_mobility"));
+    if (!u_d || !mnode_d) return fail(PXB_ERR_INVALID, "pxb_ch_mobility: NULL buffer");
+    PXB_CUDA_TRY(launch_ch_mobility(c->g.n, M0, u_d, mnode_d, c->stream));
+    return check_launch(c, "ch mobility");
+}
+
+static int ch_args(pxb_ctx *c, double kappa, double chi, double dt, const double *mnode_d, const double *u_d,
+                   const double *uold_d, double *kvals_d, double *rhs_d, ChAsmArgs &a, const char *who) {
+    PXB_TRY(need_geometry(c, who));
+    CsrState &k = c->csr;
+    if (!k.ready || k.ndof != 2) return fail(PXB_ERR_STATE, std::string(who) + ": set a 2-dof pattern first");
+    if (!c->ch.ready) return fail(PXB_ERR_STATE, std::string(who) + ": call pxb_ch_set_geometry or pxb_ch_build_geometry first");
+    if (!(dt > 0.0)) return fail(PXB_ERR_INVALID, std::string(who) + ": dt must be > 0 (transient-only element)");
+    a.n = c->g.n;
+    a.kappa = kappa;
+    a.chi = chi;
+    a.dt = dt;
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.rev = c->ch.rev.as<int>();
+    a.lap = c->ch.lap.as<double>();
+    a.vol = c->g.vol.as<double>();
+    a.mnode = mnode_d;
+    a.ghost = c->ch.ghost.p ? c->ch.ghost.as<char>() : nullptr;
+    a.rowptr = k.rowptr.as<int>();
+    a.slot = k.slot.as<int>();
+    a.diag = k.diag.as<int>();
+    a.u = u_d;
+    a.uold = uold_d;
+    a.kvals = kvals_d;
+    a.rhs = rhs_d;
+    return PXB_OK;
+}
+
+extern "C" int pxb_assemble_ch_d(pxb_ctx *c, double kappa, double chi, double dt, const double *mnode_d,
+                                 const double *u_d, const double *uold_d, double *kvals_d, double *rhs_d) {
+    if (!mnode_d || !u_d || !uold_d || !kvals_d || !rhs_d) return fail(PXB_ERR_INVALID, "pxb_assemble_ch: NULL buffer");
+    ChAsmArgs a;
+    PXB_TRY(ch_args(c, kappa, chi, dt, mnode_d, u_d, uold_d, kvals_d, rhs_d, a, "pxb_assemble_ch"));
+    launch_assemble_ch(a, c->stream);
+    return check_launch(c, "assemble_ch");
+}
+
 extern "C" int pxb_assemble_ch(pxb_ctx *c, double kappa, double chi, double dt, const double *mnode,
                                const double *u, const double *uold, double *kvals, double *rhs) {
     PXB_TRY(need_geometry(c, "pxb_assemble_ch"));

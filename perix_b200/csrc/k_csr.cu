@@ -168,4 +168,64 @@ cudaError_t launch_assemble_ch(const ChAsmArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// ---- Cahn-Hilliard geometry and mobility on the device -------------------------------------------------------
+template <int DIM, typename GT>
+__global__ void ch_geometry_kernel(int n, const int *off, const int *nbr, const void *pos, const int *mirror,
+                                   const GT *ops, int nop, int sxx, int syy, int szz, double *lap, char *ghost) {
+    using PosT = typename Vec<DIM>::T;
+    const PosT *p = static_cast<const PosT *>(pos);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        ghost[i] = (mirror && mirror[i] > 0) ? 1 : 0;
+        const PosT xi = p[i];
+        double qi = xi.x * xi.x + xi.y * xi.y;
+        if constexpr (DIM == 3) qi += xi.z * xi.z;
+        double lapq = 0.0;
+        const int b0 = off[i], b1 = off[i + 1];
+        for (int t = b0; t < b1; ++t) {
+            const GT *g = ops + (size_t)t * nop;
+            double w = (double)g[sxx] + (double)g[syy];
+            if constexpr (DIM == 3) w += (double)g[szz];
+            lap[t] = w;
+            const int j = nbr[t];
+            if (!(mirror && mirror[j] > 0)) {
+                const PosT xj = p[j];
+                double qj = xj.x * xj.x + xj.y * xj.y;
+                if constexpr (DIM == 3) qj += xj.z * xj.z;
+                lapq += w * (qj - qi);
+            }
+        }
+        const double lam = (lapq > 1.0e-12) ? (2.0 * DIM / lapq) : 1.0;
+        for (int t = b0; t < b1; ++t)
+            if (!(mirror && mirror[nbr[t]] > 0)) lap[t] *= lam;
+    }
+}
+
+cudaError_t launch_ch_geometry(int n, int dim, const int *off, const int *nbr, const void *pos, const int *mirror,
+                               const void *ops, bool mixed, int nop, int sxx, int syy, int szz, double *lap,
+                               char *ghost, cudaStream_t s) {
+    const int grid = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
+    const int g = grid > 0 ? grid : 1;
+    if (dim == 3) {
+        if (mixed) ch_geometry_kernel<3, float><<<g, 256, 0, s>>>(n, off, nbr, pos, mirror, (const float *)ops, nop, sxx, syy, szz, lap, ghost);
+        else ch_geometry_kernel<3, double><<<g, 256, 0, s>>>(n, off, nbr, pos, mirror, (const double *)ops, nop, sxx, syy, szz, lap, ghost);
+    } else {
+        if (mixed) ch_geometry_kernel<2, float><<<g, 256, 0, s>>>(n, off, nbr, pos, mirror, (const float *)ops, nop, sxx, syy, szz, lap, ghost);
+        else ch_geometry_kernel<2, double><<<g, 256, 0, s>>>(n, off, nbr, pos, mirror, (const double *)ops, nop, sxx, syy, szz, lap, ghost);
+    }
+    return cudaGetLastError();
+}
+
+__global__ void ch_mobility_kernel(int n, double M0, const double *u, double *mnode) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double c = fmax(1.0e-8, fmin(1.0 - 1.0e-8, u[2 * (size_t)i]));
+        mnode[i] = M0 * c * (1.0 - c);
+    }
+}
+
+cudaError_t launch_ch_mobility(int n, double M0, const double *u, double *mnode, cudaStream_t s) {
+    const int grid = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
+    ch_mobility_kernel<<<grid > 0 ? grid : 1, 256, 0, s>>>(n, M0, u, mnode);
+    return cudaGetLastError();
+}
+
 }  // namespace pxb

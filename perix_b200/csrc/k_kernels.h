@@ -237,5 +237,13 @@ struct ChAsmArgs {
     double *kvals = nullptr, *rhs = nullptr;
 };
 cudaError_t launch_assemble_ch(const ChAsmArgs &a, cudaStream_t s);
+// CH one-off geometry from the order-2 operator cache (CahnHilliardElement.cpp:93-152): per bond the PDDO
+// Laplacian g_xx + g_yy (+ g_zz), lambda-corrected on non-ghost bonds with lambda = 2 dim / sum_j g2_ij
+// (|x_j|^2 - |x_i|^2); ghost flags from the mirror map.  slots: the operator slots of d2/dx2, d2/dy2, d2/dz2.
+cudaError_t launch_ch_geometry(int n, int dim, const int *off, const int *nbr, const void *pos, const int *mirror,
+                               const void *ops, bool mixed, int nop, int sxx, int syy, int szz, double *lap,
+                               char *ghost, cudaStream_t s);
+// mnode[i] = M0 c(1 - c), c = u[2i] clamped to [1e-8, 1 - 1e-8] (CahnHilliardElement.cpp:45-50)
+cudaError_t launch_ch_mobility(int n, double M0, const double *u, double *mnode, cudaStream_t s);
 
 }  // namespace pxb

@@ -129,6 +129,64 @@ def test_ch_assembly_matches_reference(ctx):
     assert np.abs(rhs - d["rhs"]).max() <= 1e-12 * np.abs(d["rhs"]).max()
 
 
+def test_ch_device_geometry_and_mobility(ctx):
+    """The CH geometry and mobility built on the device (pxb_ch_build_geometry, pxb_ch_mobility_d) against the
+    reference element's own arrays, then the whole assembly from them against the reference K and rhs."""
+    import torch
+    d = load_golden("ch32")
+    geometry(ctx, d, 2)
+    ctx.gbuild(2, 0)
+    ctx.ch_build_geometry()
+    rev, lap, ghost = ctx.ch_get_geometry()
+    assert np.array_equal(rev, d["rev"]) and np.array_equal(ghost, d["isghost"])
+    assert scaled_err(lap.reshape(-1, 1), d["lapbond"].reshape(-1, 1), d["off"]) <= 1e-12
+    chi, kappa, M0, dt = (float(x) for x in d["params"])
+    dev = torch.device("cuda", 0)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    u = torch.from_numpy(d["u"]).to(dev)
+    uo = torch.from_numpy(d["uold"]).to(dev)
+    mn = torch.empty(ctx.n, dtype=torch.float64, device=dev)
+    ctx.ch_mobility_d(M0, u.data_ptr(), mn.data_ptr())
+    assert np.abs(mn.cpu().numpy() - d["mnode"]).max() <= 1e-15
+    ctx.csr_set_pattern(d["rowptr2"], d["cols2"], 2)
+    kv = torch.empty(d["kvals"].size, dtype=torch.float64, device=dev)
+    rhs = torch.empty(2 * ctx.n, dtype=torch.float64, device=dev)
+    ctx.assemble_ch_d(kappa, chi, dt, mn.data_ptr(), u.data_ptr(), uo.data_ptr(), kv.data_ptr(), rhs.data_ptr())
+    torch.cuda.synchronize(dev)
+    rp, cols, ref = d["rowptr2"], d["cols2"], d["kvals"]
+    rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+    nbr_block = (cols // 2) != (rows // 2)
+    scale = np.zeros(rp.size - 1)
+    np.maximum.at(scale, rows[nbr_block], np.abs(ref[nbr_block]))
+    assert (np.abs(kv.cpu().numpy() - ref) <= 1e-12 * scale[rows]).all()
+    assert np.abs(rhs.cpu().numpy() - d["rhs"]).max() <= 1e-12 * np.abs(d["rhs"]).max()
+
+
+def test_c1_solve_l2_error(ctx, port):
+    """BASELINE config 1 end to end: 64x64 lattice, order 2, FP64 g-build and Poisson assembly on the GPU, the
+    reference's Dirichlet row replacement on the ghost layer, one solve.  The solution matches the solve of the
+    C restatement's assembly of the same system (1e-9) and the relative L2 error against sin(pi x) sin(pi y) is
+    the reference's (1.44e-3 with the reference's own assembly, tests/test_oracle.py)."""
+    import perix_b200 as px
+    from bench import c1_poisson
+    L = px.lattice(2, 64, 64, 0, [0.0, 1.0, 0.0, 1.0])
+    delta = 3.015 * L.dxyz[0] * (1 + 1e-6)
+    off, ids = px.families(L.coords, delta, False, mirror=L.mirror)
+    rowptr, cols = px.csr_pattern(off, ids, L.mirror, 1)
+    ctx.set_geometry(L.coords, L.vols, off, ids, delta, L.dxyz[0], 2, mirror=L.mirror)
+    ctx.gbuild(2, 0)
+    ctx.csr_set_pattern(rowptr, cols, 1)
+    x, y = L.coords[0::3], L.coords[1::3]
+    f = 2 * math.pi ** 2 * np.sin(math.pi * x) * np.sin(math.pi * y)
+    kv, rhs = ctx.assemble_scalar(0, 1.0, np.zeros(L.n), f_node=f)
+    U, err = c1_poisson(px, kv, rhs, L, rowptr, cols)
+    g, _ = port.gbuild(2, 2, L.coords, L.vols, off, ids, delta, L.dxyz[0])
+    kv_o, rhs_o = port.poisson_assemble(2, off, ids, g, [2, 4], 1.0, f, np.zeros(L.n), rowptr, cols)
+    U_o, err_o = c1_poisson(px, kv_o, rhs_o, L, rowptr, cols)
+    assert np.abs(U - U_o).max() <= 1e-9
+    assert abs(err - 1.4357e-3) <= 1e-6 and abs(err - err_o) <= 1e-9
+
+
 def test_poisson_assembly_matches_reference(ctx):
     d = load_golden("poisson16")
     geometry(ctx, d, 2)

@@ -205,3 +205,22 @@ def test_vs_reference_3d_slab_gbuild(port):
     g_ref, _ = m.gbuild()
     g, _ = port.gbuild(3, 2, m.coords, m.vols, off, ids, m.delta, m.dx_char)
     assert scaled_err(g, g_ref, off) <= 1e-12
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference harness not built here")
+def test_c1_solve_with_reference_assembly():
+    """C1 with the reference's own Poisson assembly: the relative L2 error of the solved field against
+    sin(pi x) sin(pi y) over the bulk nodes (the value the GPU path is held to)."""
+    import math
+    import perix_b200 as px
+    from bench import c1_poisson
+    from oracle import RefMesh
+    m = RefMesh.structured(2, 64, 64, 0, [0, 1, 0, 1], 3.015, 2)
+    m.gbuild()
+    x, y = m.coords[0::3], m.coords[1::3]
+    f = 2 * math.pi ** 2 * np.sin(math.pi * x) * np.sin(math.pi * y)
+    kv, rhs, _ = m.poisson_assemble(1.0, f, np.zeros(m.n))
+    rp, cols = m.csr_pattern(1)
+    L = px.lattice(2, 64, 64, 0, [0.0, 1.0, 0.0, 1.0])
+    _, err = c1_poisson(px, kv, rhs, L, rp, cols)
+    assert abs(err - 1.4357e-3) <= 1e-6
