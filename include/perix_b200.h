@@ -90,6 +90,15 @@ int pxb_csr_pattern(int n, int ndof, const int *neigh_off, const int *neigh_id, 
  * (ghost layer, 0 bulk) may be NULL. */
 int pxb_set_geometry(pxb_ctx *ctx, int n, int dim, const double *coords3, const double *vols, const int *neigh_off,
                      const int *neigh_id, double delta, double dx_char, const int *mirror, const int *layer_index);
+/* The same geometry with the families built on the device: the reference's createNeighborNodes
+ * (src/PDMesh/CreatePDMesh.cpp:910-1082) in its exact order (bit-equal to pxb_families), for meshes without
+ * bond-cutting cracks (force-only cracks keep their bonds and are fine); radius is the family radius (the
+ * reference adds its 1e-6 margin), delta the horizon of the g-build.  nbtot (may be NULL) receives the bond
+ * count; pxb_get_families copies the families out (1-based ids).  PXB_ERR_UNSUPPORTED when a family exceeds
+ * 256 members or a cell of size radius holds 4096 nodes or more. */
+int pxb_set_geometry_points(pxb_ctx *ctx, int n, int dim, const double *coords3, const double *vols, double radius,
+                            double delta, double dx_char, const int *mirror, const int *layer_index, long long *nbtot);
+int pxb_get_families(pxb_ctx *ctx, int *neigh_off, int *neigh_id);
 
 /* ---- g-functions (reference PDOperators::buildGeometryCache, src/PDOperators/CalcPDOperators.cpp:356-463) ----
  * Builds the per-bond operator vectors ops[bond*nop+k] for multi-index order `order` on the device.

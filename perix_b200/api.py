@@ -311,6 +311,23 @@ class Context:
                                        C.c_double(delta), C.c_double(dx_char), _p(m, C.c_int), _p(l_, C.c_int)))
 
     # -- g-functions
+    def set_geometry_points(self, coords3, vols, radius, delta, dx_char, dim, mirror=None, layer=None):
+        """Geometry with the families built on the device (reference order, equal to ``families``)."""
+        c = _f64(coords3).reshape(-1)
+        n = c.size // 3
+        nb = C.c_longlong(0)
+        _check(self.L.pxb_set_geometry_points(self.h, n, int(dim), _p(c), _p(_f64(vols)), C.c_double(radius),
+                                              C.c_double(delta), C.c_double(dx_char), _p(_i32(mirror), C.c_int),
+                                              _p(_i32(layer), C.c_int), C.byref(nb)))
+        self.n, self.dim, self.nb = n, int(dim), nb.value
+        return nb.value
+
+    def get_families(self):
+        off = np.zeros(self.n + 1, np.int32)
+        ids = np.zeros(max(1, self.nb), np.int32)
+        _check(self.L.pxb_get_families(self.h, _p(off, C.c_int), _p(ids, C.c_int)))
+        return off, ids[:self.nb]
+
     def gbuild(self, order=2, precision=FP64, allow_degenerate=False):
         nd = C.c_int(0)
         first = C.c_int(0)

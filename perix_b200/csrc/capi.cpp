@@ -216,6 +216,52 @@ extern "C" int pxb_ctx_launch_count(pxb_ctx *c, long long *count) {
 }
 
 // ==================================================================================================== geometry
+// drop every state that depends on the geometry, then store the CSR offsets (host copy + device) and allocate
+// the zeroed neighbour array (ldb = nb rounded up to 16, plus 16)
+static int geometry_reset(pxb_ctx *c, int n, int dim, const int *neigh_off, int maxf, double delta, double dx_char,
+                          const int *mirror) {
+    PXB_CUDA_TRY(cudaSetDevice(c->device));
+    PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    destroy_graphs(c->epf);
+    c->ops = OpsCache{};
+    c->epf = EpfState{};
+    c->csr = CsrState{};
+    c->ch = ChState{};
+    Geometry &g = c->g;
+    g = Geometry{};
+    const long long nb = neigh_off[n];
+    g.n = n;
+    g.dim = dim;
+    g.nb = nb;
+    g.delta = delta;
+    g.dx_char = dx_char;
+    g.max_family = maxf;
+    g.h_off.assign(neigh_off, neigh_off + n + 1);
+    if (mirror) g.h_mirror.assign(mirror, mirror + n);
+    g.ldb = ((nb + 16 + 15) / 16) * 16;
+    PXB_TRY(dev_alloc(c, g.off, sizeof(int) * (size_t)(n + 1 + 16)));
+    PXB_CUDA_TRY(cudaMemsetAsync(g.off.p, 0, g.off.bytes, c->stream));
+    PXB_TRY(h2d(c, g.off.p, neigh_off, sizeof(int) * (size_t)(n + 1)));
+    PXB_TRY(dev_alloc(c, g.nbr, sizeof(int) * (size_t)g.ldb));
+    PXB_CUDA_TRY(cudaMemsetAsync(g.nbr.p, 0, g.nbr.bytes, c->stream));
+    return PXB_OK;
+}
+
+// positions (packed double2 / double4), volumes, mirror and layer maps; marks the geometry ready
+static int geometry_finish(pxb_ctx *c, const double *coords3_d, const double *vols, const int *mirror,
+                           const int *layer_index) {
+    Geometry &g = c->g;
+    PXB_TRY(dev_alloc(c, g.pos, (g.dim == 2 ? 16 : 32) * (size_t)g.n));
+    launch_pos_pack(g.n, g.dim, coords3_d, g.pos.p, c->stream);
+    PXB_TRY(check_launch(c, "pos_pack"));
+    PXB_TRY(dev_upload(c, g.vol, vols, sizeof(double) * (size_t)g.n));
+    if (mirror) PXB_TRY(dev_upload(c, g.mirror, mirror, sizeof(int) * (size_t)g.n));
+    if (layer_index) PXB_TRY(dev_upload(c, g.layer, layer_index, sizeof(int) * (size_t)g.n));
+    PXB_TRY(sync(c));
+    g.ready = true;
+    return PXB_OK;
+}
+
 extern "C" int pxb_set_geometry(pxb_ctx *c, int n, int dim, const double *coords3, const double *vols,
                                 const int *neigh_off, const int *neigh_id, double delta, double dx_char,
                                 const int *mirror, const int *layer_index) {
@@ -233,29 +279,8 @@ extern "C" int pxb_set_geometry(pxb_ctx *c, int n, int dim, const double *coords
     for (long long t = 0; t < nb; ++t)
         if (neigh_id[t] < 1 || neigh_id[t] > n)
             return fail(PXB_ERR_INVALID, "pxb_set_geometry: neighbour id out of range (ids are 1-based)");
-    PXB_CUDA_TRY(cudaSetDevice(c->device));
-    PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    destroy_graphs(c->epf);
-    c->ops = OpsCache{};
-    c->epf = EpfState{};
-    c->csr = CsrState{};
-    c->ch = ChState{};
+    PXB_TRY(geometry_reset(c, n, dim, neigh_off, maxf, delta, dx_char, mirror));
     Geometry &g = c->g;
-    g = Geometry{};
-    g.n = n;
-    g.dim = dim;
-    g.nb = nb;
-    g.delta = delta;
-    g.dx_char = dx_char;
-    g.max_family = maxf;
-    g.h_off.assign(neigh_off, neigh_off + n + 1);
-    if (mirror) g.h_mirror.assign(mirror, mirror + n);
-    g.ldb = ((nb + 16 + 15) / 16) * 16;
-    PXB_TRY(dev_alloc(c, g.off, sizeof(int) * (size_t)(n + 1 + 16)));
-    PXB_CUDA_TRY(cudaMemsetAsync(g.off.p, 0, g.off.bytes, c->stream));
-    PXB_TRY(h2d(c, g.off.p, neigh_off, sizeof(int) * (size_t)(n + 1)));
-    PXB_TRY(dev_alloc(c, g.nbr, sizeof(int) * (size_t)g.ldb));
-    PXB_CUDA_TRY(cudaMemsetAsync(g.nbr.p, 0, g.nbr.bytes, c->stream));
     void *tmp = nullptr;
     PXB_TRY(scratch(c, std::max(sizeof(int) * (size_t)std::max(1LL, nb), sizeof(double) * 3 * (size_t)n), &tmp));
     PXB_TRY(h2d(c, tmp, neigh_id, sizeof(int) * (size_t)nb));
@@ -265,14 +290,123 @@ extern "C" int pxb_set_geometry(pxb_ctx *c, int n, int dim, const double *coords
     }
     PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
     PXB_TRY(h2d(c, tmp, coords3, sizeof(double) * 3 * (size_t)n));
-    PXB_TRY(dev_alloc(c, g.pos, (dim == 2 ? 16 : 32) * (size_t)n));
-    launch_pos_pack(n, dim, static_cast<const double *>(tmp), g.pos.p, c->stream);
-    PXB_TRY(check_launch(c, "pos_pack"));
-    PXB_TRY(dev_upload(c, g.vol, vols, sizeof(double) * (size_t)n));
-    if (mirror) PXB_TRY(dev_upload(c, g.mirror, mirror, sizeof(int) * (size_t)n));
-    if (layer_index) PXB_TRY(dev_upload(c, g.layer, layer_index, sizeof(int) * (size_t)n));
+    return geometry_finish(c, static_cast<const double *>(tmp), vols, mirror, layer_index);
+}
+
+// Families built on the device (k_families.cu), then the geometry as pxb_set_geometry sets it.
+extern "C" int pxb_set_geometry_points(pxb_ctx *c, int n, int dim, const double *coords3, const double *vols,
+                                       double radius, double delta, double dx_char, const int *mirror,
+                                       const int *layer_index, long long *nbtot) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_set_geometry_points: NULL context");
+    if (n <= 0 || (dim != 2 && dim != 3) || !coords3 || !vols || !(radius > 0.0) || !(delta > 0.0))
+        return fail(PXB_ERR_INVALID, "pxb_set_geometry_points: bad arguments (need n>0, dim 2|3, radius>0, delta>0)");
+    PXB_CUDA_TRY(cudaSetDevice(c->device));
+    PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const bool is3d = dim == 3;
+    FamArgs a;
+    a.n = n;
+    a.is3d = is3d ? 1 : 0;
+    for (int d = 0; d < 3; ++d) a.lo[d] = std::numeric_limits<double>::max();
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) a.lo[d] = std::min(a.lo[d], coords3[3 * (size_t)i + d]);
+    if (!is3d) a.lo[2] = 0.0;
+    a.radius = radius;
+    a.r2 = radius * radius;
+    a.r2tol = 64.0 * std::numeric_limits<double>::epsilon() * a.r2;
+    unsigned slots = 1024;
+    while (slots < 2u * (unsigned)n && slots < (1u << 31)) slots <<= 1;
+    a.mask = slots - 1;
+    DevBuf coords, keys, ccount, cminid, cstart, cfill, members, cell_of, cxyz, pos, fcount, fkey, fval, err;
+    PXB_TRY(dev_upload(c, coords, coords3, sizeof(double) * 3 * (size_t)n));
+    PXB_TRY(dev_alloc(c, keys, sizeof(unsigned long long) * slots));
+    PXB_CUDA_TRY(cudaMemsetAsync(keys.p, 0xff, keys.bytes, c->stream));
+    PXB_TRY(dev_alloc(c, ccount, sizeof(int) * slots));
+    PXB_CUDA_TRY(cudaMemsetAsync(ccount.p, 0, ccount.bytes, c->stream));
+    PXB_TRY(dev_alloc(c, cminid, sizeof(int) * slots));
+    PXB_CUDA_TRY(cudaMemsetAsync(cminid.p, 0x7f, cminid.bytes, c->stream));
+    PXB_TRY(dev_alloc(c, cfill, sizeof(int) * slots));
+    PXB_CUDA_TRY(cudaMemsetAsync(cfill.p, 0, cfill.bytes, c->stream));
+    PXB_TRY(dev_alloc(c, cstart, sizeof(int) * slots));
+    PXB_TRY(dev_alloc(c, members, sizeof(int) * (size_t)n));
+    PXB_TRY(dev_alloc(c, cell_of, sizeof(int) * (size_t)n));
+    PXB_TRY(dev_alloc(c, cxyz, sizeof(int) * 3 * (size_t)n));
+    PXB_TRY(dev_alloc(c, pos, sizeof(int) * (size_t)n));
+    PXB_TRY(dev_alloc(c, fcount, sizeof(int) * (size_t)n));
+    PXB_TRY(dev_alloc(c, err, sizeof(int)));
+    PXB_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), c->stream));
+    a.coords = coords.as<double>();
+    a.keys = keys.as<unsigned long long>();
+    a.ccount = ccount.as<int>();
+    a.cminid = cminid.as<int>();
+    a.cstart = cstart.as<int>();
+    a.cfill = cfill.as<int>();
+    a.members = members.as<int>();
+    a.cell_of = cell_of.as<int>();
+    a.cxyz = cxyz.as<int>();
+    a.pos = pos.as<int>();
+    a.fcount = fcount.as<int>();
+    a.err = err.as<int>();
+    PXB_CUDA_TRY(launch_fam_cells(a, c->stream));
+    int herr = 0;
+    PXB_TRY(d2h(c, &herr, err.p, sizeof(int)));
+    std::vector<int> hcount(slots), hstart(slots);
+    PXB_TRY(d2h(c, hcount.data(), ccount.p, sizeof(int) * slots));
     PXB_TRY(sync(c));
-    g.ready = true;
+    if (herr) return fail(PXB_ERR_INVALID, "pxb_set_geometry_points: cell index out of range or cell table full");
+    long long acc = 0;
+    int maxcell = 0;
+    for (unsigned s = 0; s < slots; ++s) {
+        hstart[s] = (int)acc;
+        acc += hcount[s];
+        maxcell = std::max(maxcell, hcount[s]);
+    }
+    if (maxcell >= kFamCell)
+        return fail(PXB_ERR_UNSUPPORTED, "pxb_set_geometry_points: more than " + std::to_string(kFamCell - 1) +
+                                             " nodes in one cell of size radius (use pxb_families on the host)");
+    PXB_TRY(h2d(c, cstart.p, hstart.data(), sizeof(int) * slots));
+    PXB_CUDA_TRY(launch_fam_members(a, c->stream));
+    PXB_CUDA_TRY(launch_fam_sort_cells(a, c->stream));
+    PXB_CUDA_TRY(launch_fam_candidates(a, false, c->stream));
+    std::vector<int> hfc((size_t)n), hoff((size_t)n + 1);
+    PXB_TRY(d2h(c, hfc.data(), fcount.p, sizeof(int) * (size_t)n));
+    PXB_TRY(sync(c));
+    long long tot = 0;
+    int maxf = 0;
+    hoff[0] = 0;
+    for (int i = 0; i < n; ++i) {
+        tot += hfc[(size_t)i];
+        if (tot > std::numeric_limits<int>::max()) return fail(PXB_ERR_INVALID, "pxb_set_geometry_points: more than 2^31-1 bonds");
+        hoff[(size_t)i + 1] = (int)tot;
+        maxf = std::max(maxf, hfc[(size_t)i]);
+    }
+    if (maxf > kFamMax)
+        return fail(PXB_ERR_UNSUPPORTED, "pxb_set_geometry_points: a family exceeds " + std::to_string(kFamMax) +
+                                             " members (use pxb_families on the host)");
+    PXB_TRY(geometry_reset(c, n, dim, hoff.data(), maxf, delta, dx_char, mirror));
+    Geometry &g = c->g;
+    PXB_TRY(dev_alloc(c, fkey, sizeof(unsigned long long) * (size_t)std::max(1LL, tot)));
+    PXB_TRY(dev_alloc(c, fval, sizeof(int) * (size_t)std::max(1LL, tot)));
+    a.off = g.off.as<int>();
+    a.fkey = fkey.as<unsigned long long>();
+    a.fval = fval.as<int>();
+    a.nbr = g.nbr.as<int>();
+    PXB_CUDA_TRY(launch_fam_candidates(a, true, c->stream));
+    PXB_CUDA_TRY(launch_fam_sort(a, c->stream));
+    PXB_TRY(check_launch(c, "device families"));
+    if (nbtot) *nbtot = tot;
+    return geometry_finish(c, coords.as<double>(), vols, mirror, layer_index);
+}
+
+// The families of the current geometry, 1-based ids (neigh_off: n+1 entries, neigh_id: neigh_off[n]).
+extern "C" int pxb_get_families(pxb_ctx *c, int *neigh_off, int *neigh_id) {
+    if (!c || !c->g.ready) return fail(PXB_ERR_STATE, "pxb_get_families: geometry not set");
+    const Geometry &g = c->g;
+    if (neigh_off) std::copy(g.h_off.begin(), g.h_off.end(), neigh_off);
+    if (neigh_id) {
+        PXB_TRY(d2h(c, neigh_id, g.nbr.p, sizeof(int) * (size_t)g.nb));
+        PXB_TRY(sync(c));
+        for (long long t = 0; t < g.nb; ++t) ++neigh_id[t];
+    }
     return PXB_OK;
 }
 

@@ -35,6 +35,31 @@ struct GBuildArgs {
 cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, int grid, cudaStream_t s);
 bool gbuild_supported(int dim, int order);
 
+// ------------------------------------------------------------------------------ families on the device (A1)
+constexpr int kFamMax = 256;   // largest family the device build sorts
+constexpr int kFamCell = 4096; // largest cell population (12-bit positions in the visit key)
+struct FamArgs {
+    int n = 0, is3d = 0;
+    const double *coords = nullptr;  // xyz per node
+    double lo[3] = {0, 0, 0};
+    double radius = 0, r2 = 0, r2tol = 0;
+    unsigned mask = 0;               // cell table size - 1 (power of two)
+    unsigned long long *keys = nullptr;
+    int *ccount = nullptr, *cminid = nullptr, *cstart = nullptr, *cfill = nullptr, *members = nullptr;
+    int *cell_of = nullptr, *cxyz = nullptr, *pos = nullptr;
+    int *fcount = nullptr;
+    const int *off = nullptr;
+    unsigned long long *fkey = nullptr;
+    int *fval = nullptr;
+    int *nbr = nullptr;  // output, 0-based
+    int *err = nullptr;
+};
+cudaError_t launch_fam_cells(const FamArgs &a, cudaStream_t s);
+cudaError_t launch_fam_members(const FamArgs &a, cudaStream_t s);
+cudaError_t launch_fam_sort_cells(const FamArgs &a, cudaStream_t s);
+cudaError_t launch_fam_candidates(const FamArgs &a, bool write, cudaStream_t s);
+cudaError_t launch_fam_sort(const FamArgs &a, cudaStream_t s);
+
 // ------------------------------------------------------------------------------------------ batched clouds
 // Many independent clouds (2D and 3D mixed) in one node/bond numbering: cloud c owns nodes [node0, node0+n) and
 // bonds [bond0, bond0+nb) of the global CSR; its operators (order 2: nop 5 in 2D, 9 in 3D, AoS [nb][nop]) start

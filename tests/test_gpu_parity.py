@@ -319,3 +319,34 @@ def test_central_difference_start(ctx):
     u, _, _, t = ctx.epf_state()
     assert np.allclose(u, 0.2, atol=1e-14, rtol=0)
     assert abs(t - 0.1) < 1e-15
+
+
+def _device_families_case(name):
+    import perix_b200 as px
+    from bench import c3_clouds
+    if name == "plate2d":
+        from bench import c2_setup
+        w = c2_setup(px)
+        return w["L"].coords, w["L"].vols, w["delta"], 2, w["L"].mirror
+    if name == "slab3d":
+        from bench import c5_setup
+        w = c5_setup(px, nx=30, ny=30, nz=10)
+        return w["L"].coords, w["L"].vols, w["delta"], 3, w["L"].mirror
+    if name == "c1":
+        L = px.lattice(2, 64, 64, 0, [0.0, 1.0, 0.0, 1.0])
+        return L.coords, L.vols, 3.015 * L.dxyz[0] * (1 + 1e-6), 2, L.mirror
+    cl = c3_clouds(px, nclouds=2, nmin=3000, nmax=6000, seed=3)[0 if name == "cloud2d" else 1]
+    return cl["coords3"], cl["vols"], cl["delta"], cl["dim"], None
+
+
+@pytest.mark.parametrize("name", ["plate2d", "slab3d", "c1", "cloud2d", "cloud3d"])
+def test_device_families_equal_host(ctx, name):
+    """Families built on the device (pxb_set_geometry_points) equal the host build (pxb_families, itself bit-equal
+    to the reference's createNeighborNodes): same offsets, same ids in the same order."""
+    import perix_b200 as px
+    coords, vols, delta, dim, mirror = _device_families_case(name)
+    off_h, ids_h = px.families(coords, delta, dim == 3, mirror=mirror)
+    ctx.set_geometry_points(coords, vols, delta, delta, delta / 3.015, dim, mirror=mirror)
+    off_d, ids_d = ctx.get_families()
+    assert np.array_equal(off_d, off_h)
+    assert np.array_equal(ids_d, ids_h)
