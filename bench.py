@@ -242,7 +242,7 @@ def c1_measure(px, device=0, reps=20):
     return res
 
 
-def c3_clouds(px, nclouds=256, nmin=1000, nmax=200000, seed=2024):
+def c3_clouds(px, nclouds=256, nmin=1000, nmax=200000, seed=2024, families=True):
     """Batched-cloud workload: clouds alternate 2D / 3D (half each), node counts log-uniform in [nmin, nmax]
     (seeded), cell-centred lattice of spacing h = 1 mm jittered by U(-0.2h, 0.2h) per coordinate, no ghosts
     (families truncated at the cloud boundary), delta = 3.015h, unit-cell volumes, dx_char = h."""
@@ -264,9 +264,10 @@ def c3_clouds(px, nclouds=256, nmin=1000, nmax=200000, seed=2024):
             xyz = (g + 0.5) * h
         xyz[:, :dim] += rng.uniform(-0.2 * h, 0.2 * h, size=(xyz.shape[0], dim))
         delta = 3.015 * h * (1.0 + 1e-6)
-        off, ids = px.families(xyz, delta, dim == 3)
-        clouds.append(dict(dim=dim, coords3=xyz, vols=np.full(xyz.shape[0], h ** dim), off=off, ids=ids,
-                           delta=delta, dx_char=h))
+        c = dict(dim=dim, coords3=xyz, vols=np.full(xyz.shape[0], h ** dim), delta=delta, dx_char=h)
+        if families:  # host families (reference order); the device builds them itself (batch_set_points)
+            c["off"], c["ids"] = px.families(xyz, delta, dim == 3)
+        clouds.append(c)
     return clouds
 
 
@@ -707,18 +708,20 @@ def c3_measure(px, nclouds=256, reps=3, device=0):
     against the exact ones (order-2 truncation error, reported, not a precision claim)."""
     import torch
     t0 = time.perf_counter()
-    clouds = c3_clouds(px, nclouds=nclouds)
+    clouds = c3_clouds(px, nclouds=nclouds, families=False)
     fields, exact = cubic_field(clouds)
     t_setup = time.perf_counter() - t0
     ctx = px.Context(device)
-    ctx.batch_set(clouds)
+    t0 = time.perf_counter()
+    ctx.batch_set_points(clouds)  # families of every cloud built on the device
+    t_fam = time.perf_counter() - t0
     dev = torch.device("cuda", device)
     ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
     u = torch.from_numpy(np.concatenate(fields)).to(dev)
     out = torch.empty(ctx.batch_out_len, dtype=torch.float64, device=dev)
     res = {"clouds": nclouds, "nodes": ctx.batch_n, "bonds": ctx.batch_nb,
            "dims": {"2d": sum(1 for c in clouds if c["dim"] == 2), "3d": sum(1 for c in clouds if c["dim"] == 3)},
-           "host_setup_s": t_setup}
+           "host_setup_s": t_setup, "batch_set_points_s": t_fam}
     derivs = {}
     for prec, p in (("fp64", px.FP64), ("mixed", px.MIXED)):
         ctx.batch_gbuild(p)
@@ -732,9 +735,10 @@ def c3_measure(px, nclouds=256, reps=3, device=0):
         s_b = 4 if prec == "mixed" else 8
         # apply bytes per launch: nb*(4 B id + nop*s B g) + N*(8 B u + 8*nop B out) per cloud (u_j gathers: L2);
         # mixed adds the per-node FP32 first-moment defects of the second-derivative operators
-        a_bytes = sum(int(c["off"][-1]) * (4 + (9 if c["dim"] == 3 else 5) * s_b) +
+        a_bytes = sum(ctx.batch_bond_counts[k] * (4 + (9 if c["dim"] == 3 else 5) * s_b) +
                       c["vols"].size * (8 + 8 * (9 if c["dim"] == 3 else 5)) +
-                      (c["vols"].size * (18 if c["dim"] == 3 else 6) * 4 if prec == "mixed" else 0) for c in clouds)
+                      (c["vols"].size * (18 if c["dim"] == 3 else 6) * 4 if prec == "mixed" else 0)
+                      for k, c in enumerate(clouds))
         hbm, _ = peaks()
         res[prec] = {"gbuild_nodes_per_s": ctx.batch_n / (g_ms * 1e-3), "gbuild_ms": g_ms, "gbuild_schedule": gbest,
                      "gbuild_ms_per_schedule": [round(float(x), 4) for x in gms],
@@ -844,10 +848,10 @@ def run_profile(args):
         # --steps clouds (log-uniform 1k..200k nodes), one FP64 or mixed g-build, then 3 applies of schedule --variant
         ctx.close()
         import torch
-        clouds = c3_clouds(px, nclouds=args.steps)
+        clouds = c3_clouds(px, nclouds=args.steps, families=False)
         fields, _ = cubic_field(clouds)
         ctx = px.Context(0)
-        ctx.batch_set(clouds)
+        ctx.batch_set_points(clouds)
         dev = torch.device("cuda", 0)
         ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
         ctx.batch_gbuild(px.MIXED if args.precision == "mixed" else px.FP64)

@@ -221,6 +221,12 @@ int pxb_gbuild_time(pxb_ctx *ctx, int order, int precision, int reps, size_t flu
 int pxb_batch_set(pxb_ctx *ctx, int nclouds, const int *dims, const int *node_off, const double *coords3,
                   const double *vols, const int *neigh_off, const int *neigh_id, const double *delta,
                   const double *dx_char);
+/* The same with every cloud's families built on the device (reference order, as pxb_set_geometry_points;
+ * radius[k] is cloud k's family radius); pxb_batch_get_families copies one cloud's families out (1-based ids
+ * within the cloud). */
+int pxb_batch_set_points(pxb_ctx *ctx, int nclouds, const int *dims, const int *node_off, const double *coords3,
+                         const double *vols, const double *radius, const double *delta, const double *dx_char);
+int pxb_batch_get_families(pxb_ctx *ctx, int cloud, int *neigh_off, int *neigh_id);
 int pxb_batch_info(pxb_ctx *ctx, long long *nodes, long long *bonds, long long *out_len, long long *ops_len);
 int pxb_batch_gbuild(pxb_ctx *ctx, int precision, int *n_degenerate, int *first_degenerate);
 int pxb_batch_apply(pxb_ctx *ctx, const double *u, double *out);

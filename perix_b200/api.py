@@ -475,6 +475,38 @@ class Context:
         self.batch_n, self.batch_nb, self.batch_out_len, self.batch_ops_len = n.value, nb.value, ol.value, opl.value
         self.batch_bond_counts = [int(np.asarray(c["off"])[-1]) for c in clouds]
 
+    def batch_set_points(self, clouds):
+        """clouds: list of dicts with dim, coords3, vols, delta, dx_char (and optionally radius, default delta);
+        the families are built on the device."""
+        dims = _i32([c["dim"] for c in clouds])
+        node_off = np.zeros(len(clouds) + 1, np.int64)
+        node_off[1:] = np.cumsum([int(np.asarray(c["vols"]).size) for c in clouds])
+        coords = np.concatenate([_f64(c["coords3"]).reshape(-1) for c in clouds])
+        vols = np.concatenate([_f64(c["vols"]) for c in clouds])
+        radius = _f64([c.get("radius", c["delta"]) for c in clouds])
+        delta = _f64([c["delta"] for c in clouds])
+        dxc = _f64([c["dx_char"] for c in clouds])
+        _check(self.L.pxb_batch_set_points(self.h, len(clouds), _p(dims, C.c_int), _p(_i32(node_off), C.c_int),
+                                           _p(coords), _p(vols), _p(radius), _p(delta), _p(dxc)))
+        self.batch_dims = [int(c["dim"]) for c in clouds]
+        self.batch_node_off = node_off
+        n, nb, ol, opl = C.c_longlong(0), C.c_longlong(0), C.c_longlong(0), C.c_longlong(0)
+        _check(self.L.pxb_batch_info(self.h, C.byref(n), C.byref(nb), C.byref(ol), C.byref(opl)))
+        self.batch_n, self.batch_nb, self.batch_out_len, self.batch_ops_len = n.value, nb.value, ol.value, opl.value
+        counts = []
+        for k in range(len(clouds)):
+            off = np.zeros(int(node_off[k + 1] - node_off[k]) + 1, np.int32)
+            _check(self.L.pxb_batch_get_families(self.h, k, _p(off, C.c_int), None))
+            counts.append(int(off[-1]))
+        self.batch_bond_counts = counts
+
+    def batch_get_families(self, cloud):
+        n = int(self.batch_node_off[cloud + 1] - self.batch_node_off[cloud])
+        off = np.zeros(n + 1, np.int32)
+        ids = np.zeros(max(1, self.batch_bond_counts[cloud]), np.int32)
+        _check(self.L.pxb_batch_get_families(self.h, int(cloud), _p(off, C.c_int), _p(ids, C.c_int)))
+        return off, ids[:self.batch_bond_counts[cloud]]
+
     def batch_gbuild(self, precision=FP64):
         nd, first = C.c_int(0), C.c_int(0)
         _check(self.L.pxb_batch_gbuild(self.h, int(precision), C.byref(nd), C.byref(first)))

@@ -6,11 +6,13 @@
 // PDOperators::calcAMatrixCompute / calcOperatorsCompute (src/PDOperators/CalcPDOperators.cpp:108-354) on it.
 #include <algorithm>
 #include <climits>
+#include <limits>
 #include <string>
 #include <vector>
 
 #include "k_kernels.h"
 #include "pxb_context.h"
+#include "fam_builder.h"
 
 using namespace pxb;
 
@@ -105,21 +107,15 @@ int apply_enqueue(pxb_ctx *c, const double *u_d, double *out_d) {
 
 }  // namespace
 
-extern "C" int pxb_batch_set(pxb_ctx *c, int nclouds, const int *dims, const int *node_off, const double *coords3,
-                             const double *vols, const int *neigh_off, const int *neigh_id, const double *delta,
-                             const double *dx_char) {
-    if (!c) return fail(PXB_ERR_INVALID, "pxb_batch_set: NULL context");
-    if (nclouds <= 0 || !dims || !node_off || !coords3 || !vols || !neigh_off || !neigh_id || !delta || !dx_char)
-        return fail(PXB_ERR_INVALID, "pxb_batch_set: bad arguments");
-    if (node_off[0] != 0 || neigh_off[0] != 0) return fail(PXB_ERR_INVALID, "pxb_batch_set: offsets must start at 0");
-    for (int k = 0; k < nclouds; ++k) {
-        if (dims[k] != 2 && dims[k] != 3) return fail(PXB_ERR_INVALID, "pxb_batch_set: dims must be 2 or 3");
-        if (node_off[k + 1] <= node_off[k]) return fail(PXB_ERR_INVALID, "pxb_batch_set: empty or unordered cloud");
-        if (!(delta[k] > 0.0)) return fail(PXB_ERR_INVALID, "pxb_batch_set: delta must be > 0");
-    }
+namespace {
+
+// The batch tables from concatenated clouds.  neigh_id (1-based within each cloud) may be NULL: the neighbour
+// array is then left zeroed for the device family build to fill.
+int batch_setup(pxb_ctx *c, int nclouds, const int *dims, const int *node_off, const double *coords3, const double *vols,
+                const int *neigh_off, const int *neigh_id, const double *delta, const double *dx_char, const char *who) {
     const int n = node_off[nclouds];
     for (int i = 0; i < n; ++i)
-        if (neigh_off[i + 1] < neigh_off[i]) return fail(PXB_ERR_INVALID, "pxb_batch_set: neigh_off not non-decreasing");
+        if (neigh_off[i + 1] < neigh_off[i]) return fail(PXB_ERR_INVALID, std::string(who) + ": neigh_off not non-decreasing");
     const long long nb = neigh_off[n];
     PXB_CUDA_TRY(cudaSetDevice(c->device));
     PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -130,7 +126,7 @@ extern "C" int pxb_batch_set(pxb_ctx *c, int nclouds, const int *dims, const int
     b.nb = nb;
     b.h_clouds.resize((size_t)nclouds);
     // cloud table, global 0-based neighbour ids, packed positions
-    std::vector<int> nbr((size_t)std::max(1LL, nb));
+    std::vector<int> nbr(neigh_id ? (size_t)std::max(1LL, nb) : 0);
     long long ops_off = 0, out_off = 0, pos_off = 0, def_off = 0;
     for (int k = 0; k < nclouds; ++k) {
         BatchCloud &cd = b.h_clouds[(size_t)k];
@@ -150,10 +146,11 @@ extern "C" int pxb_batch_set(pxb_ctx *c, int nclouds, const int *dims, const int
         ops_off += cd.nb * nop;
         out_off += (long long)cd.n * nop;
         pos_off += ((long long)cd.n * (cd.dim == 3 ? 32 : 16) + 31) / 32 * 32;
+        if (!neigh_id) continue;
         for (long long t = cd.bond0; t < cd.bond0 + cd.nb; ++t) {
             const int id = neigh_id[t];
             if (id < 1 || id > cd.n)
-                return fail(PXB_ERR_INVALID, "pxb_batch_set: cloud " + std::to_string(k) +
+                return fail(PXB_ERR_INVALID, std::string(who) + ": cloud " + std::to_string(k) +
                                                  ": neighbour id out of range (ids are 1-based within the cloud)");
             nbr[(size_t)t] = cd.node0 + id - 1;
         }
@@ -183,12 +180,101 @@ extern "C" int pxb_batch_set(pxb_ctx *c, int nclouds, const int *dims, const int
     PXB_TRY(dev_upload(c, b.clouds, b.h_clouds.data(), sizeof(BatchCloud) * b.h_clouds.size()));
     PXB_TRY(dev_upload(c, b.tasks, tasks.data(), sizeof(BatchTask) * tasks.size()));
     PXB_TRY(dev_upload(c, b.off, neigh_off, sizeof(int) * ((size_t)n + 1)));
-    PXB_TRY(dev_upload(c, b.nbr, nbr.data(), sizeof(int) * nbr.size()));
+    if (neigh_id) {
+        PXB_TRY(dev_upload(c, b.nbr, nbr.data(), sizeof(int) * nbr.size()));
+    } else {
+        PXB_TRY(dev_alloc(c, b.nbr, sizeof(int) * (size_t)std::max(1LL, nb)));
+        PXB_CUDA_TRY(cudaMemsetAsync(b.nbr.p, 0, b.nbr.bytes, c->stream));
+    }
     PXB_TRY(dev_upload(c, b.pos, pos.data(), sizeof(double) * std::max<size_t>(1, pos.size())));
     PXB_TRY(dev_upload(c, b.vol, vols, sizeof(double) * (size_t)n));
     PXB_TRY(dev_alloc(c, b.counters, 4 * sizeof(unsigned)));
     PXB_TRY(sync(c));
+    return PXB_OK;
+}
+
+int check_clouds(int nclouds, const int *dims, const int *node_off, const double *delta, const char *who) {
+    if (node_off[0] != 0) return fail(PXB_ERR_INVALID, std::string(who) + ": node offsets must start at 0");
+    for (int k = 0; k < nclouds; ++k) {
+        if (dims[k] != 2 && dims[k] != 3) return fail(PXB_ERR_INVALID, std::string(who) + ": dims must be 2 or 3");
+        if (node_off[k + 1] <= node_off[k]) return fail(PXB_ERR_INVALID, std::string(who) + ": empty or unordered cloud");
+        if (!(delta[k] > 0.0)) return fail(PXB_ERR_INVALID, std::string(who) + ": delta must be > 0");
+    }
+    return PXB_OK;
+}
+
+}  // namespace
+
+extern "C" int pxb_batch_set(pxb_ctx *c, int nclouds, const int *dims, const int *node_off, const double *coords3,
+                             const double *vols, const int *neigh_off, const int *neigh_id, const double *delta,
+                             const double *dx_char) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_batch_set: NULL context");
+    if (nclouds <= 0 || !dims || !node_off || !coords3 || !vols || !neigh_off || !neigh_id || !delta || !dx_char)
+        return fail(PXB_ERR_INVALID, "pxb_batch_set: bad arguments");
+    if (neigh_off[0] != 0) return fail(PXB_ERR_INVALID, "pxb_batch_set: offsets must start at 0");
+    PXB_TRY(check_clouds(nclouds, dims, node_off, delta, "pxb_batch_set"));
+    PXB_TRY(batch_setup(c, nclouds, dims, node_off, coords3, vols, neigh_off, neigh_id, delta, dx_char, "pxb_batch_set"));
+    c->batch.ready = true;
+    return PXB_OK;
+}
+
+// Families of every cloud built on the device (radius[k] = family radius of cloud k), then the batch as
+// pxb_batch_set sets it.
+extern "C" int pxb_batch_set_points(pxb_ctx *c, int nclouds, const int *dims, const int *node_off,
+                                    const double *coords3, const double *vols, const double *radius,
+                                    const double *delta, const double *dx_char) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_batch_set_points: NULL context");
+    if (nclouds <= 0 || !dims || !node_off || !coords3 || !vols || !radius || !delta || !dx_char)
+        return fail(PXB_ERR_INVALID, "pxb_batch_set_points: bad arguments");
+    PXB_TRY(check_clouds(nclouds, dims, node_off, delta, "pxb_batch_set_points"));
+    for (int k = 0; k < nclouds; ++k)
+        if (!(radius[k] > 0.0)) return fail(PXB_ERR_INVALID, "pxb_batch_set_points: radius must be > 0");
+    PXB_CUDA_TRY(cudaSetDevice(c->device));
+    const int n = node_off[nclouds];
+    std::vector<int> off((size_t)n + 1, 0);
+    long long acc = 0;
+    for (int k = 0; k < nclouds; ++k) {  // counts (the builders are rebuilt for the fill below)
+        FamBuilder fb;
+        std::vector<int> h;
+        int maxf = 0;
+        long long tot = 0;
+        const int n0 = node_off[k], nk = node_off[k + 1] - n0;
+        PXB_TRY(fb.count(c, nk, dims[k] == 3, coords3 + 3 * (size_t)n0, radius[k], h, maxf, tot));
+        for (int i = 0; i < nk; ++i) off[(size_t)n0 + i + 1] = (int)(acc + h[(size_t)i + 1]);
+        acc += tot;
+        if (acc > std::numeric_limits<int>::max()) return fail(PXB_ERR_INVALID, "pxb_batch_set_points: more than 2^31-1 bonds");
+    }
+    PXB_TRY(batch_setup(c, nclouds, dims, node_off, coords3, vols, off.data(), nullptr, delta, dx_char,
+                        "pxb_batch_set_points"));
+    BatchState &b = c->batch;
+    for (int k = 0; k < nclouds; ++k) {
+        FamBuilder fb;
+        std::vector<int> h;
+        int maxf = 0;
+        long long tot = 0;
+        const int n0 = node_off[k], nk = node_off[k + 1] - n0;
+        PXB_TRY(fb.count(c, nk, dims[k] == 3, coords3 + 3 * (size_t)n0, radius[k], h, maxf, tot));
+        PXB_TRY(fb.fill(c, b.off.as<int>() + n0, b.nbr.as<int>(), n0));
+    }
+    PXB_TRY(sync(c));
     b.ready = true;
+    return PXB_OK;
+}
+
+// One cloud's families (1-based ids within the cloud): neigh_off n_k + 1 entries, neigh_id neigh_off[n_k].
+extern "C" int pxb_batch_get_families(pxb_ctx *c, int cloud, int *neigh_off, int *neigh_id) {
+    PXB_TRY(need_batch(c, "pxb_batch_get_families", false));
+    const BatchState &b = c->batch;
+    if (cloud < 0 || cloud >= b.nclouds) return fail(PXB_ERR_INVALID, "pxb_batch_get_families: no such cloud");
+    const BatchCloud &cd = b.h_clouds[(size_t)cloud];
+    std::vector<int> off((size_t)cd.n + 1);
+    PXB_TRY(d2h(c, off.data(), b.off.as<int>() + cd.node0, sizeof(int) * off.size()));
+    if (neigh_id) PXB_TRY(d2h(c, neigh_id, b.nbr.as<int>() + cd.bond0, sizeof(int) * (size_t)cd.nb));
+    PXB_TRY(sync(c));
+    if (neigh_off)
+        for (size_t i = 0; i < off.size(); ++i) neigh_off[i] = off[i] - off[0];
+    if (neigh_id)
+        for (long long t = 0; t < cd.nb; ++t) neigh_id[t] = neigh_id[t] - cd.node0 + 1;
     return PXB_OK;
 }
 

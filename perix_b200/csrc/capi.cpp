@@ -9,6 +9,7 @@
 
 #include "k_kernels.h"
 #include "pxb_context.h"
+#include "fam_builder.h"
 
 namespace pxb {
 
@@ -293,7 +294,7 @@ extern "C" int pxb_set_geometry(pxb_ctx *c, int n, int dim, const double *coords
     return geometry_finish(c, static_cast<const double *>(tmp), vols, mirror, layer_index);
 }
 
-// Families built on the device (k_families.cu), then the geometry as pxb_set_geometry sets it.
+// Families built on the device (k_families.cu, fam_builder.h), then the geometry as pxb_set_geometry sets it.
 extern "C" int pxb_set_geometry_points(pxb_ctx *c, int n, int dim, const double *coords3, const double *vols,
                                        double radius, double delta, double dx_char, const int *mirror,
                                        const int *layer_index, long long *nbtot) {
@@ -302,99 +303,15 @@ extern "C" int pxb_set_geometry_points(pxb_ctx *c, int n, int dim, const double 
         return fail(PXB_ERR_INVALID, "pxb_set_geometry_points: bad arguments (need n>0, dim 2|3, radius>0, delta>0)");
     PXB_CUDA_TRY(cudaSetDevice(c->device));
     PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    const bool is3d = dim == 3;
-    FamArgs a;
-    a.n = n;
-    a.is3d = is3d ? 1 : 0;
-    for (int d = 0; d < 3; ++d) a.lo[d] = std::numeric_limits<double>::max();
-    for (int i = 0; i < n; ++i)
-        for (int d = 0; d < 3; ++d) a.lo[d] = std::min(a.lo[d], coords3[3 * (size_t)i + d]);
-    if (!is3d) a.lo[2] = 0.0;
-    a.radius = radius;
-    a.r2 = radius * radius;
-    a.r2tol = 64.0 * std::numeric_limits<double>::epsilon() * a.r2;
-    unsigned slots = 1024;
-    while (slots < 2u * (unsigned)n && slots < (1u << 31)) slots <<= 1;
-    a.mask = slots - 1;
-    DevBuf coords, keys, ccount, cminid, cstart, cfill, members, cell_of, cxyz, pos, fcount, fkey, fval, err;
-    PXB_TRY(dev_upload(c, coords, coords3, sizeof(double) * 3 * (size_t)n));
-    PXB_TRY(dev_alloc(c, keys, sizeof(unsigned long long) * slots));
-    PXB_CUDA_TRY(cudaMemsetAsync(keys.p, 0xff, keys.bytes, c->stream));
-    PXB_TRY(dev_alloc(c, ccount, sizeof(int) * slots));
-    PXB_CUDA_TRY(cudaMemsetAsync(ccount.p, 0, ccount.bytes, c->stream));
-    PXB_TRY(dev_alloc(c, cminid, sizeof(int) * slots));
-    PXB_CUDA_TRY(cudaMemsetAsync(cminid.p, 0x7f, cminid.bytes, c->stream));
-    PXB_TRY(dev_alloc(c, cfill, sizeof(int) * slots));
-    PXB_CUDA_TRY(cudaMemsetAsync(cfill.p, 0, cfill.bytes, c->stream));
-    PXB_TRY(dev_alloc(c, cstart, sizeof(int) * slots));
-    PXB_TRY(dev_alloc(c, members, sizeof(int) * (size_t)n));
-    PXB_TRY(dev_alloc(c, cell_of, sizeof(int) * (size_t)n));
-    PXB_TRY(dev_alloc(c, cxyz, sizeof(int) * 3 * (size_t)n));
-    PXB_TRY(dev_alloc(c, pos, sizeof(int) * (size_t)n));
-    PXB_TRY(dev_alloc(c, fcount, sizeof(int) * (size_t)n));
-    PXB_TRY(dev_alloc(c, err, sizeof(int)));
-    PXB_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), c->stream));
-    a.coords = coords.as<double>();
-    a.keys = keys.as<unsigned long long>();
-    a.ccount = ccount.as<int>();
-    a.cminid = cminid.as<int>();
-    a.cstart = cstart.as<int>();
-    a.cfill = cfill.as<int>();
-    a.members = members.as<int>();
-    a.cell_of = cell_of.as<int>();
-    a.cxyz = cxyz.as<int>();
-    a.pos = pos.as<int>();
-    a.fcount = fcount.as<int>();
-    a.err = err.as<int>();
-    PXB_CUDA_TRY(launch_fam_cells(a, c->stream));
-    int herr = 0;
-    PXB_TRY(d2h(c, &herr, err.p, sizeof(int)));
-    std::vector<int> hcount(slots), hstart(slots);
-    PXB_TRY(d2h(c, hcount.data(), ccount.p, sizeof(int) * slots));
-    PXB_TRY(sync(c));
-    if (herr) return fail(PXB_ERR_INVALID, "pxb_set_geometry_points: cell index out of range or cell table full");
-    long long acc = 0;
-    int maxcell = 0;
-    for (unsigned s = 0; s < slots; ++s) {
-        hstart[s] = (int)acc;
-        acc += hcount[s];
-        maxcell = std::max(maxcell, hcount[s]);
-    }
-    if (maxcell >= kFamCell)
-        return fail(PXB_ERR_UNSUPPORTED, "pxb_set_geometry_points: more than " + std::to_string(kFamCell - 1) +
-                                             " nodes in one cell of size radius (use pxb_families on the host)");
-    PXB_TRY(h2d(c, cstart.p, hstart.data(), sizeof(int) * slots));
-    PXB_CUDA_TRY(launch_fam_members(a, c->stream));
-    PXB_CUDA_TRY(launch_fam_sort_cells(a, c->stream));
-    PXB_CUDA_TRY(launch_fam_candidates(a, false, c->stream));
-    std::vector<int> hfc((size_t)n), hoff((size_t)n + 1);
-    PXB_TRY(d2h(c, hfc.data(), fcount.p, sizeof(int) * (size_t)n));
-    PXB_TRY(sync(c));
-    long long tot = 0;
+    FamBuilder fb;
+    std::vector<int> hoff;
     int maxf = 0;
-    hoff[0] = 0;
-    for (int i = 0; i < n; ++i) {
-        tot += hfc[(size_t)i];
-        if (tot > std::numeric_limits<int>::max()) return fail(PXB_ERR_INVALID, "pxb_set_geometry_points: more than 2^31-1 bonds");
-        hoff[(size_t)i + 1] = (int)tot;
-        maxf = std::max(maxf, hfc[(size_t)i]);
-    }
-    if (maxf > kFamMax)
-        return fail(PXB_ERR_UNSUPPORTED, "pxb_set_geometry_points: a family exceeds " + std::to_string(kFamMax) +
-                                             " members (use pxb_families on the host)");
+    long long tot = 0;
+    PXB_TRY(fb.count(c, n, dim == 3, coords3, radius, hoff, maxf, tot));
     PXB_TRY(geometry_reset(c, n, dim, hoff.data(), maxf, delta, dx_char, mirror));
-    Geometry &g = c->g;
-    PXB_TRY(dev_alloc(c, fkey, sizeof(unsigned long long) * (size_t)std::max(1LL, tot)));
-    PXB_TRY(dev_alloc(c, fval, sizeof(int) * (size_t)std::max(1LL, tot)));
-    a.off = g.off.as<int>();
-    a.fkey = fkey.as<unsigned long long>();
-    a.fval = fval.as<int>();
-    a.nbr = g.nbr.as<int>();
-    PXB_CUDA_TRY(launch_fam_candidates(a, true, c->stream));
-    PXB_CUDA_TRY(launch_fam_sort(a, c->stream));
-    PXB_TRY(check_launch(c, "device families"));
+    PXB_TRY(fb.fill(c, c->g.off.as<int>(), c->g.nbr.as<int>(), 0));
     if (nbtot) *nbtot = tot;
-    return geometry_finish(c, coords.as<double>(), vols, mirror, layer_index);
+    return geometry_finish(c, fb.coords_d(), vols, mirror, layer_index);
 }
 
 // The families of the current geometry, 1-based ids (neigh_off: n+1 entries, neigh_id: neigh_off[n]).

@@ -132,7 +132,7 @@ __global__ void fam_candidates_kernel(FamArgs a) {
         const int mycell = a.cell_of[x];
         const int posx = a.pos[x];
         int cnt = 0;
-        long long w = WRITE ? (long long)a.off[x] : 0;
+        long long w = WRITE ? (long long)a.off[x] - a.off_base : 0;
         for (int dz = (a.is3d ? -1 : 0); dz <= (a.is3d ? 1 : 0); ++dz)
             for (int dy = -1; dy <= 1; ++dy)
                 for (int dx = -1; dx <= 1; ++dx) {
@@ -197,8 +197,8 @@ __global__ void __launch_bounds__(128) fam_sort_kernel(FamArgs a) {
         const long long b0 = a.off[x];
         const int len = a.off[x + 1] - a.off[x];
         for (int k = lane; k < CAP; k += 32) {
-            sk[w][k] = k < len ? a.fkey[b0 + k] : kEmpty;
-            sv[w][k] = k < len ? a.fval[b0 + k] : 0;
+            sk[w][k] = k < len ? a.fkey[b0 - a.off_base + k] : kEmpty;
+            sv[w][k] = k < len ? a.fval[b0 - a.off_base + k] : 0;
         }
         __syncwarp();
         int size = 2;
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(128) fam_sort_kernel(FamArgs a) {
                 }
                 __syncwarp();
             }
-        for (int k = lane; k < len; k += 32) a.nbr[b0 + k] = sv[w][k];
+        for (int k = lane; k < len; k += 32) a.nbr[b0 + k] = sv[w][k] + a.id_base;
         __syncwarp();
     }
 }

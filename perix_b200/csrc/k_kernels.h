@@ -48,10 +48,12 @@ struct FamArgs {
     int *ccount = nullptr, *cminid = nullptr, *cstart = nullptr, *cfill = nullptr, *members = nullptr;
     int *cell_of = nullptr, *cxyz = nullptr, *pos = nullptr;
     int *fcount = nullptr;
-    const int *off = nullptr;
+    const int *off = nullptr;  // family offsets (a batch cloud's slice: global bond indices)
+    int off_base = 0;          // off[0]: fkey / fval are indexed from it
     unsigned long long *fkey = nullptr;
     int *fval = nullptr;
-    int *nbr = nullptr;  // output, 0-based
+    int *nbr = nullptr;  // output, 0-based, plus id_base (a batch cloud's first node)
+    int id_base = 0;
     int *err = nullptr;
 };
 cudaError_t launch_fam_cells(const FamArgs &a, cudaStream_t s);

@@ -116,3 +116,19 @@ def test_batch_rejects_foreign_ids(ctx, batch):
     with pytest.raises(px.PxbError) as e:
         ctx.batch_set(clouds)
     assert e.value.status == 1 and "cloud 1" in str(e.value)
+
+
+def test_batch_device_families_equal_host(ctx, batch):
+    """pxb_batch_set_points builds every cloud's families on the device: each equals the host build (reference
+    order), and the g-functions built on them equal those of the host-family batch."""
+    clouds = batch[0]
+    ctx.batch_set([dict(c) for c in clouds])
+    ctx.batch_gbuild(0)
+    g_host = [ctx.batch_get_ops(k) for k in range(len(clouds))]
+    ctx.batch_set_points([{k: v for k, v in c.items() if k not in ("off", "ids")} for c in clouds])
+    for k, c in enumerate(clouds):
+        off, ids = ctx.batch_get_families(k)
+        assert np.array_equal(off, c["off"]) and np.array_equal(ids, c["ids"])
+    ctx.batch_gbuild(0)
+    for k in range(len(clouds)):
+        assert np.array_equal(ctx.batch_get_ops(k), g_host[k])
