@@ -6,8 +6,8 @@ dt = 0.8 h / sqrt(C11/rho)).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl perix|reference] [--precision mixed|fp64]
 
 A step is one explicit time step (damage + Navier force + central difference + BC pass, one fused kernel),
-timed alone with CUDA events on the launching stream; the L2 is flushed (256 MiB write) before every timed
-step, and the state is restored from a snapshot taken 100 steps into the run every 100 steps, so every timed
+timed alone with CUDA events on the launching stream; the L2 is flushed (256 MiB write, then read back) before
+every timed step, and the state is restored from a snapshot taken 100 steps into the run every 100 steps, so every timed
 step works on the same physical regime (after ~200 further steps the plate's wall mode grows).
 Multi-GPU runs (torchrun) are independent replicas of the plate (weak scaling); the time is the max over ranks.
 Prints one JSON line on rank 0.
@@ -666,7 +666,7 @@ def run_perix(args):
         "config": {"workload": "explicit_pddo_frac 2D notched plate 400x200 (81,200 PD nodes, %d directed bonds), "
                                "dt=0.8h/c" % w["nb"],
                    "nodes": w["n"], "bonds": w["nb"], "parallelism": "replicas" if ws > 1 else "single-gpu",
-                   "l2": "flushed (256 MiB write) before every timed step",
+                   "l2": "flushed before every timed step (256 MiB write, then the same 256 MiB read back)",
                    "state": "snapshot after %d steps, restored every %d steps" % (S0, EPISODE)},
         "e2e": {"value": ws * e2e, "unit": "bond-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "pxb_epf_rate (drop-in per-step call, pinned host u in / acceleration out)"},

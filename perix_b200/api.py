@@ -425,7 +425,7 @@ class Context:
 
     def epf_autotune(self, steps=10, flush_bytes=256 << 20, use_cache=False):
         best = C.c_int(0)
-        ms = np.zeros(16, np.float32)
+        ms = np.zeros(self.L.pxb_epf_variant_count(), np.float32)
         _check(self.L.pxb_epf_autotune(self.h, int(steps), C.c_size_t(flush_bytes), int(bool(use_cache)),
                                        C.byref(best), ms.ctypes.data_as(C.POINTER(C.c_float))))
         return best.value, ms

@@ -39,21 +39,26 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, u
         : "memory");
 }
 
+constexpr unsigned kSuspendNs = 1000;  // try_wait suspend-time hint
+constexpr int kTileDesc = 64;          // bond ranges of its first tiles a block loads up front
+
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
     unsigned ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
         : "memory");
     return ok != 0;
 }
 
-// bounded wait: false if the phase did not complete within the iteration budget
+// bounded wait: false if the phase did not complete within the iteration budget.  Each try_wait may suspend
+// the thread for up to kSuspendNs (it resumes as soon as the phase completes), so a waiting warp issues few
+// instructions; the budget is at most 2^19 tries (about half a second).
 __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
-    for (int it = 0; it < (1 << 20); ++it)
+    for (int it = 0; it < (1 << 19); ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -175,6 +180,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     __shared__ unsigned s_done[S];  // warps finished with the stage's current tile
     __shared__ int s_last[S];       // block-local sequence number of the last copy issued into the stage
     __shared__ int s_fail;
+    __shared__ int s_d0[kTileDesc], s_d1[kTileDesc];  // bond range of the block's first tiles
     __shared__ unsigned long long s_umax[WPB];
     __shared__ unsigned long long s_broken[WPB];
 
@@ -199,7 +205,8 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         const int tile = (int)blockIdx.x + k * (int)gridDim.x;
         const int n0 = tile * NT;
         const int cnt = min(NT, a.n - n0);
-        const int t0 = __ldg(a.off + n0), t1 = __ldg(a.off + n0 + cnt);
+        const int t0 = k < kTileDesc ? s_d0[k] : __ldg(a.off + n0);
+        const int t1 = k < kTileDesc ? s_d1[k] : __ldg(a.off + n0 + cnt);
         const int t0a = t0 & ~15;
         const unsigned nbond = up16((unsigned)(t1 - t0a));
         unsigned char *base = smem + (size_t)st * stage_bytes;
@@ -238,6 +245,13 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         }
         s_fail = 0;
         fence_mbar_init();
+    }
+    // the bond ranges of the block's first tiles, all loaded at once: a refill then issues its copies without
+    // first waiting on a global load
+    for (int k = tid; k < mycount && k < kTileDesc; k += WPB * kWarp) {
+        const int n0 = ((int)blockIdx.x + k * (int)gridDim.x) * NT;
+        s_d0[k] = __ldg(a.off + n0);
+        s_d1[k] = __ldg(a.off + min(n0 + NT, a.n));
     }
     __syncthreads();
     if (tid == 0)
@@ -299,6 +313,9 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
             double uj[UNR][DIM];
 #pragma unroll
             for (int q = 0; q < UNR; ++q) {
+                xj[q] = PosT{};
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) uj[q][d] = 0.0;
                 if (h[q]) {
                     if constexpr (!XS) xj[q] = ldg_vec(pos + j[q]);
                     if constexpr (DIM == 2) {
@@ -311,25 +328,30 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
                     }
                 }
             }
+            // every bond of the pass as an independent stream: a squared comparison accepts the bonds that clearly
+            // hold (nearly all of them); the others (breaking, or within the rounding band of the threshold) take
+            // the reference test in a rarely entered branch; then the forces of the held bonds
+            bool hold[UNR], slow[UNR];
+            double e[UNR][DIM];
+            bool any_slow = false;
 #pragma unroll
             for (int q = 0; q < UNR; ++q) {
-                if (h[q] == 0) continue;
                 const int t = t0 + q * LPN;
-                double e[DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) e[d] = __dsub_rn(uj[q][d], ui[d]);
+                for (int d = 0; d < DIM; ++d) e[q][d] = __dsub_rn(uj[q][d], ui[d]);
+                bool fast = true;  // clearly holds
                 if (a.damage) {
-                    int brk;
                     if constexpr (XS) {
                         // FP32 squared test on the staged FP32 bond vector.  Its error (ξ rounded to FP32, e
                         // rounded, FP32 sums: < 1e-6 r^2 wherever |y|^2 is near (1 +- s_c)^2 r^2) stays well inside
-                        // the 4e-6 r^2 band; inside the band the reference arithmetic decides on the exact
-                        // positions (gathered only then), so decisions equal the FP64 path's.
+                        // the 4e-6 r^2 band; outside the clear-hold region the reference arithmetic decides on the
+                        // exact positions (gathered only then), so decisions equal the FP64 path's.
+                        const bool ok = t < b1;
                         float xf[DIM], yf[DIM];
 #pragma unroll
                         for (int d = 0; d < DIM; ++d) {
-                            xf[d] = sXi[(size_t)d * maxb + t];
-                            yf[d] = xf[d] + (float)e[d];
+                            xf[d] = ok ? sXi[(size_t)d * maxb + t] : 0.f;
+                            yf[d] = xf[d] + (float)e[q][d];
                         }
                         float r2f = xf[0] * xf[0] + xf[1] * xf[1];
                         float y2f = yf[0] * yf[0] + yf[1] * yf[1];
@@ -337,32 +359,50 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
                             r2f += xf[2] * xf[2];
                             y2f += yf[2] * yf[2];
                         }
-                        brk = 0;
-                        if (r2f > 0.f) {
-                            const float bandf = 4.0e-6f * r2f;
-                            const float qh = y2f - sc_hi2f * r2f;
-                            if (a.tension_only) {
-                                brk = qh > bandf ? 1 : (qh < -bandf ? 0 : -1);
-                            } else {
-                                const float ql = sc_lo2f * r2f - y2f;
-                                brk = (qh > bandf || ql > bandf) ? 1 : ((qh < -bandf && ql < -bandf) ? 0 : -1);
-                            }
-                            if (brk < 0) brk = break_fp64<DIM>(ldg_vec(pos + j[q]), xi, e, a);
-                        }
+                        const float bandf = 4.0e-6f * r2f;
+                        fast = (y2f - sc_hi2f * r2f < -bandf) && (a.tension_only || sc_lo2f * r2f - y2f < -bandf);
+                        fast = fast || !(r2f > 0.f);
                     } else {
-                        brk = break_fp64<DIM>(xj[q], xi, e, a);
-                    }
-                    if (brk) {
-                        a.health[t0a + t] = 0;
-                        ++broken;
-                        continue;
+                        double xv[DIM], yv[DIM];
+                        xv[0] = __dsub_rn(xj[q].x, xi.x);
+                        xv[1] = __dsub_rn(xj[q].y, xi.y);
+                        if constexpr (DIM == 3) xv[2] = __dsub_rn(xj[q].z, xi.z);
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[q][d]);
+                        const double r2 = dot_rn_t<DIM>(xv, xv), y2 = dot_rn_t<DIM>(yv, yv);
+                        const double band = 1.0e-6 * r2;
+                        fast = (y2 - a.sc_hi2 * r2 < -band) && (a.tension_only || a.sc_lo2 * r2 - y2 < -band);
+                        fast = fast || !(r2 > 0.0);
                     }
                 }
+                hold[q] = h[q] && fast;
+                slow[q] = h[q] && !fast;
+                any_slow = any_slow || slow[q];
+            }
+            if (any_slow) {
+#pragma unroll
+                for (int q = 0; q < UNR; ++q) {
+                    if (!slow[q]) continue;
+                    int brk;
+                    if constexpr (XS) brk = break_fp64<DIM>(ldg_vec(pos + j[q]), xi, e[q], a);
+                    else brk = break_fp64<DIM>(xj[q], xi, e[q], a);
+                    if (brk) {
+                        a.health[t0a + t0 + q * LPN] = 0;
+                        ++broken;
+                    } else {
+                        hold[q] = true;
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                if (!hold[q]) continue;
+                const int t = t0 + q * LPN;
                 double pd[NC];
 #pragma unroll
                 for (int c = 0; c < NC; ++c) pd[c] = (double)sP[(size_t)c * maxb + t];
                 double f[DIM];
-                navier_packed_t<DIM>(pd, e, f);
+                navier_packed_t<DIM>(pd, e[q], f);
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) L[d] += f[d];
             }
