@@ -505,7 +505,21 @@ def measure_precision(px, w, prec, steps, warmup, ws, device):
     t_wall = time.perf_counter() - t_wall
     launches = ctx.launch_count() - launches0
     barrier(ws)
+    tuned["launch_floor"] = launch_floor(ctx) if tuned["variant"] >= 5 else None
     return ctx, ms, launches, t_wall, tuned
+
+
+def launch_floor(ctx, reps=20):
+    """The fixed cost inside each timed step: an empty kernel with the tuned step kernel's launch shape, after
+    the same L2 flush, timed with CUDA events like a step (pxb_epf_launch_floor)."""
+    import ctypes as C
+    ms = np.zeros(reps, np.float32)
+    g, b, sm = C.c_int(0), C.c_int(0), C.c_size_t(0)
+    st = ctx.L.pxb_epf_launch_floor(ctx.h, C.c_size_t(FLUSH_BYTES), reps, ms.ctypes.data_as(C.POINTER(C.c_float)),
+                                    C.byref(g), C.byref(b), C.byref(sm))
+    if st:
+        raise RuntimeError(ctx.L.pxb_last_error().decode())
+    return {"ms": float(np.mean(ms[1:])), "grid": g.value, "block": b.value, "smem_bytes": sm.value}
 
 
 def autotune(ctx, steps=20):
@@ -643,10 +657,11 @@ def run_perix(args):
         cpu = cpu_reference(w, 20, 2)
         for p in out.values():
             p["ctx"].close()
-        c3 = c3_measure(px, device=local)
-        c5 = c5_measure(px, device=local)
-        refgpu = reference_gpu()
-        c1 = c1_measure(px, device=local)
+        if not args.headline_only:
+            c3 = c3_measure(px, device=local)
+            c5 = c5_measure(px, device=local)
+            refgpu = reference_gpu()
+            c1 = c1_measure(px, device=local)
     if rank != 0:
         return
     line = {
@@ -672,7 +687,10 @@ def run_perix(args):
                 "api": "pxb_epf_rate (drop-in per-step call, pinned host u in / acceleration out)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": B, "kernel": kernel_name(head, out[head]["tuned"])},
+                     "algorithmic_bytes_per_launch": B, "kernel": kernel_name(head, out[head]["tuned"]),
+                     "launch_floor_ms": (out[head]["tuned"]["launch_floor"] or {}).get("ms"),
+                     "note": "achieved = algorithmic bytes / CUDA-event step time; launch_floor_ms is an empty "
+                             "kernel of the same launch shape timed the same way (flush, events)"},
         "cpu_baseline": ({"value": cpu["value"], "unit": "bond-updates/s", "cores": cpu["cores"],
                           "kind": "reference",
                           "sample": "20 explicit steps of the same plate through the reference's OpenMP CPU path"}
@@ -899,6 +917,8 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--variant", type=int, default=8)
     ap.add_argument("--size", type=int, default=120, help="--profile c5step: slab of size x size x 24 nodes")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="the plate step line alone (no batched-cloud, slab, reference-GPU and Poisson keys)")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)

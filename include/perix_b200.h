@@ -205,6 +205,12 @@ int pxb_epf_get_variant(pxb_ctx *ctx, int *variant, int *lanes_per_node);
 /* reps g-builds into the existing operator cache (same order/precision as the last pxb_gbuild), L2 flushed
  * before each; ms[r] = CUDA-event duration of build r. */
 int pxb_gbuild_time(pxb_ctx *ctx, int order, int precision, int reps, size_t flush_bytes, float *ms);
+/* The fixed cost inside each timed step: reps launches of an empty kernel with the launch shape (grid, block,
+ * dynamic shared memory, returned) of the last TMA-staged step launch, each after the same L2 flush and timed
+ * with CUDA events exactly like a step; ms[r] per launch.  No counterpart in the reference (measurement
+ * support only). */
+int pxb_epf_launch_floor(pxb_ctx *ctx, size_t flush_bytes, int reps, float *ms, int *grid, int *block,
+                         size_t *smem);
 
 /* ---- batched clouds ----------------------------------------------------------------------------------------
  * Many independent node clouds (2D and 3D mixed, boundary-truncated families of uneven size) in one

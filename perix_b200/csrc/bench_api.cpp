@@ -237,6 +237,29 @@ extern "C" int pxb_epf_time_steps(pxb_ctx *c, int nsteps, size_t flush_bytes, in
     return timed_steps(c, nsteps, flush_bytes, restore_every, s.valid ? &s : nullptr, ms);
 }
 
+// The fixed cost inside a timed step: an empty kernel with the launch shape of the last staged step launch
+// (grid, block, dynamic shared memory), timed exactly like a step (L2 flushed, CUDA events around the launch).
+extern "C" int pxb_epf_launch_floor(pxb_ctx *c, size_t flush_bytes, int reps, float *ms, int *grid, int *block,
+                                    size_t *smem) {
+    if (!c || reps <= 0 || !ms) return fail(PXB_ERR_INVALID, "pxb_epf_launch_floor: bad arguments");
+    const LaunchShape sh = epf_tma_last_shape();
+    if (sh.grid <= 0) return fail(PXB_ERR_STATE, "pxb_epf_launch_floor: no staged step launched yet");
+    Events ev;
+    PXB_TRY(ev.make(2 * (size_t)reps));
+    for (int r = 0; r < reps; ++r) {
+        PXB_TRY(flush_l2(c, flush_bytes, g_flush));
+        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r], c->stream));
+        PXB_CUDA_TRY(launch_empty(sh.grid, sh.block, sh.smem, c->stream));
+        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r + 1], c->stream));
+    }
+    PXB_TRY(sync(c));
+    for (int r = 0; r < reps; ++r) PXB_CUDA_TRY(cudaEventElapsedTime(&ms[r], ev.ev[2 * (size_t)r], ev.ev[2 * (size_t)r + 1]));
+    if (grid) *grid = sh.grid;
+    if (block) *block = sh.block;
+    if (smem) *smem = sh.smem;
+    return PXB_OK;
+}
+
 // Times `reps` g-builds (order, precision) of the current geometry, L2 flushed before each; ms[r] per build.
 extern "C" int pxb_gbuild_time(pxb_ctx *c, int order, int precision, int reps, size_t flush_bytes, float *ms) {
     if (!c || !c->g.ready) return fail(PXB_ERR_STATE, "pxb_gbuild_time: geometry not set");

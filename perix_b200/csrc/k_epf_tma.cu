@@ -477,6 +477,10 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     }
 }
 
+static LaunchShape g_last_shape{0, 0, 0};
+
+LaunchShape epf_tma_last_shape() { return g_last_shape; }
+
 template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB, bool XI>
 static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
     constexpr int NT = WPB * (kWarp / LPN);
@@ -497,6 +501,7 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
     const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
     const int grid = (int)(ntiles < cap ? ntiles : cap);
     k<<<grid > 0 ? grid : 1, WPB * kWarp, smem, s>>>(a);
+    g_last_shape = LaunchShape{grid > 0 ? grid : 1, WPB * kWarp, smem};
     return cudaGetLastError();
 }
 

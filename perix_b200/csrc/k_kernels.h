@@ -169,6 +169,14 @@ int epf_tma_tile_nodes(int dim, int which);
 size_t epf_tma_smem(int dim, bool mixed, int which, int maxb);
 int epf_tma_lanes(int dim, int which);
 cudaError_t launch_epf_tma(const EpfArgs &a, int dim, bool mixed, int which, cudaStream_t s);
+// grid, block and dynamic shared memory of the last staged launch (host bookkeeping for the launch-floor probe)
+struct LaunchShape {
+    int grid, block;
+    size_t smem;
+};
+LaunchShape epf_tma_last_shape();
+// an empty kernel with the given launch shape (the fixed cost of a launch, timed like a step)
+cudaError_t launch_empty(int grid, int block, size_t smem, cudaStream_t s);
 
 struct EpfAdjArgs {
     int n = 0;
