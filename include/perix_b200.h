@@ -279,6 +279,28 @@ int pxb_assemble_ch_d(pxb_ctx *ctx, double kappa, double chi, double dt, const d
 int pxb_assemble_ch(pxb_ctx *ctx, double kappa, double chi, double dt, const double *mnode, const double *u,
                     const double *uold, double *kvals, double *rhs);
 
+/* Stress-coupled (optionally fracturing) Cahn-Hilliard assembly, the boundary of the reference's
+ * perix_cuda::assembleStressCahnHilliard (include/PDSystem/CudaAssemble.h:185-191; kernel
+ * src/PDSystem/CudaAssembleKernels.cu:685-874).  Rows per node: c, mu, u_x, u_y[, u_z] (ndof = dim + 2).
+ * Needs an FP64 order-2 g-build, the CH geometry (pxb_ch_set_geometry / pxb_ch_build_geometry) and a pattern
+ * set with ndof = dim + 2.  health[nbtot] (may be NULL: every bond intact) gates the mechanical bond terms by
+ * 1 or kres; vel[n*dim] (may be NULL) with rho > 0 adds the backward-Euler inertia on the u rows; uold may be
+ * NULL (c_old = u_old = 0).  K = -dF/dU, rhs = +F; rows of degenerate nodes are zero. */
+typedef struct pxb_stress_ch_params {
+    double C11, C12, C66;  /* elastic stiffness */
+    double A, Kh, Ch;      /* chemo-mechanical body force -A grad c; hydrostatic stress Kh tr(eps) + Ch (c - cref) */
+    double Omega, cref;    /* swelling */
+    double chi, kappa;     /* regular-solution interaction, gradient energy */
+    double dt;             /* backward-Euler step */
+    double kres;           /* stiffness floor of a broken bond */
+    double rho;            /* > 0: inertia on the displacement rows */
+} pxb_stress_ch_params;
+int pxb_assemble_stress_ch_d(pxb_ctx *ctx, const pxb_stress_ch_params *p, const double *mnode_d,
+                             const double *health_d, const double *vel_d, const double *u_d, const double *uold_d,
+                             double *kvals_d, double *rhs_d);
+int pxb_assemble_stress_ch(pxb_ctx *ctx, const pxb_stress_ch_params *p, const double *mnode, const double *health,
+                           const double *vel, const double *u, const double *uold, double *kvals, double *rhs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,10 +7,11 @@ Two CPU implementations of PeriX's PDDO hot path, used exclusively as checkers b
 * ``ref``   - ``oracle/_ref/libperix_ref.so``, the reference's own hot-path sources compiled by
   ``oracle/Makefile`` together with ``oracle/ref_harness.cpp``.
 
-plus, for ``bench.py``'s GPU reference point only, ``oracle/_ref/libperix_ref_cuda.so``: the reference's own
-CUDA assembly translation unit compiled for sm_100a with timers (``oracle/ref_cuda_harness.cu``).
+plus ``oracle/_ref/libperix_ref_cuda.so``: the reference's own CUDA assembly translation unit compiled for
+sm_100a (``oracle/ref_cuda_harness.cu``), timed by ``bench.py`` as the GPU reference point and used by the GPU
+tests as a checker for the stress-coupled Cahn-Hilliard assembler.
 
 The product (``perix_b200``) never imports this package.
 """
 from .lib import (PortOracle, RefMesh, RefEpf, port_available, ref_available, bc_program_arrays,  # noqa: F401
-                  ORACLE_DIR, ref_cuda_available, ref_cuda_epf_bench)
+                  ORACLE_DIR, ref_cuda_available, ref_cuda_epf_bench, ref_cuda_stress_ch)

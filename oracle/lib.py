@@ -245,6 +245,42 @@ def ref_cuda_epf_bench(dim, coords3, vols, off, ids, delta, dx_char, Cv, rho, sc
 _REF = None
 
 
+def ref_cuda_stress_ch(dim, coords3, vols, off, ids, delta, dx_char, rowptr, cols, p13, rev, lapbond, isghost,
+                       mnode, u, uold, health=None, vel=None):
+    """The reference's own GPU stress-coupled CH assembler (its CUDA TU built for sm_100a); returns K, rhs."""
+    L = C.CDLL(_REFCU_SO)
+    pqr = []
+    for o in (1, 2):
+        for p in range(o, -1, -1):
+            if dim == 3:
+                for q in range(o - p, -1, -1):
+                    pqr.append((p, q, o - p - q))
+            else:
+                pqr.append((p, o - p, 0))
+    qp = np.array([x[0] for x in pqr], np.int32)
+    qq = np.array([x[1] for x in pqr], np.int32)
+    qr = np.array([x[2] for x in pqr], np.int32)
+    fact = np.array([math.factorial(a) * math.factorial(b) * math.factorial(c) for a, b, c in pqr], np.float64)
+    nd = dim + 2
+    n = np.asarray(vols).size
+    kv = np.zeros(np.asarray(cols).size, np.float64)
+    rhs = np.zeros(n * nd, np.float64)
+    f64 = lambda a: np.ascontiguousarray(a, np.float64)
+    i32 = lambda a: np.ascontiguousarray(a, np.int32)
+    st = L.refcu_stress_ch(int(n), int(dim), _ptr(f64(coords3), C.c_double), _ptr(f64(vols), C.c_double),
+                           _ptr(i32(off), C.c_int), _ptr(i32(ids), C.c_int), _ptr(qp, C.c_int), _ptr(qq, C.c_int),
+                           _ptr(qr, C.c_int), _ptr(fact, C.c_double), int(len(pqr)), C.c_double(delta),
+                           C.c_double(dx_char), _ptr(i32(rowptr), C.c_int), _ptr(i32(cols), C.c_int), int(kv.size),
+                           _ptr(f64(p13), C.c_double), _ptr(i32(rev), C.c_int), _ptr(f64(lapbond), C.c_double),
+                           _ptr(np.ascontiguousarray(isghost, np.int8), C.c_char), _ptr(f64(mnode), C.c_double),
+                           None if health is None else _ptr(f64(health), C.c_double),
+                           None if vel is None else _ptr(f64(vel), C.c_double), _ptr(f64(u), C.c_double),
+                           _ptr(f64(uold), C.c_double), _ptr(kv, C.c_double), _ptr(rhs, C.c_double))
+    if st:
+        raise RuntimeError("reference stress-CH GPU assembly failed")
+    return kv, rhs
+
+
 def _ref_lib():
     global _REF
     if _REF is None:
@@ -262,6 +298,7 @@ def _ref_lib():
         L.ref_csr_nnz.restype = C.c_int
         L.ref_poisson_assemble.restype = C.c_double
         L.ref_ch_assemble.restype = C.c_double
+        L.ref_stress_ch_assemble.restype = C.c_double
         L.ref_epf_create.restype = vp
         L.ref_epf_rate.restype = C.c_double
         L.ref_epf_run.restype = C.c_double
@@ -391,6 +428,28 @@ class RefMesh:
                                    _ptr(rhs, C.c_double), _ptr(lap, C.c_double), _ptr(rev, C.c_int),
                                    _ptr(ghost, C.c_char), _ptr(mnode, C.c_double), int(nthreads or os.cpu_count()))
         return kv, rhs, dict(lapbond=lap, rev=rev, isghost=ghost, mnode=mnode), t
+
+    def stress_ch_assemble(self, E, nu, plane_stress, Omega, cref, D, chi, kappa, dt, u, uold, nthreads=0):
+        """StressCahnHilliardElement (ndof = dim + 2) K, rhs and its own geometry / mobility / derived constants
+        (C11, C12, C66, A, Kh, Ch)."""
+        nd = self.dim + 2
+        nnz = self.L.ref_csr_nnz(self.h, nd)
+        kv = np.zeros(nnz, np.float64)
+        rhs = np.zeros(self.n * nd, np.float64)
+        lap = np.zeros(max(1, self.nb), np.float64)
+        rev = np.zeros(max(1, self.nb), np.int32)
+        ghost = np.zeros(self.n, np.int8)
+        mnode = np.zeros(self.n, np.float64)
+        consts = np.zeros(6, np.float64)
+        t = self.L.ref_stress_ch_assemble(self.h, C.c_double(E), C.c_double(nu), int(plane_stress), C.c_double(Omega),
+                                          C.c_double(cref), C.c_double(D), C.c_double(chi), C.c_double(kappa),
+                                          C.c_double(dt), _ptr(np.ascontiguousarray(u, np.float64), C.c_double),
+                                          _ptr(np.ascontiguousarray(uold, np.float64), C.c_double),
+                                          _ptr(kv, C.c_double), _ptr(rhs, C.c_double), _ptr(lap, C.c_double),
+                                          _ptr(rev, C.c_int), _ptr(ghost, C.c_char), _ptr(mnode, C.c_double),
+                                          _ptr(consts, C.c_double), int(nthreads or os.cpu_count()))
+        return kv, rhs, dict(lapbond=lap[:self.nb], rev=rev[:self.nb], isghost=ghost, mnode=mnode,
+                             consts=consts), t
 
     def bc_preset(self, bcs, t, u):
         p = bc_program_arrays(bcs, self.dim)

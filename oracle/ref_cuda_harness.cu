@@ -134,3 +134,53 @@ REFCU_API int refcu_epf_bench(int n, int dim, const double *coords, const double
     perix_cuda::shutdown();
     return err == cudaSuccess ? 0 : 4;
 }
+
+// The reference's own stress-coupled CH device assembler (perix_cuda::assembleStressCahnHilliard,
+// CudaAssembleKernels.cu:1325-) on one mesh: p13 = C11 C12 C66 A Kh Ch Omega cref chi kappa dt kres rho.
+// health (nbtot) and vel (N*dim) may be NULL.  Returns 0 on success.
+REFCU_API int refcu_stress_ch(int n, int dim, const double *coords, const double *vols, const int *off,
+                              const int *ids, const int *qp, const int *qq, const int *qr, const double *factprod,
+                              int nop, double delta, double dx_char, const int *rowptr, const int *cols, int nnz,
+                              const double *p13, const int *rev, const double *lapbond, const char *isghost,
+                              const double *mnode, const double *health, const double *vel, const double *u,
+                              const double *uold, double *kvals, double *rhs) {
+    perix_cuda::AssembleMesh m;
+    m.N = n;
+    m.nnz = nnz;
+    m.csr_off = rowptr;
+    m.csr_col = cols;
+    m.neigh_off = off;
+    m.neigh_id = ids;
+    m.coords = coords;
+    m.vols = vols;
+    m.qp = qp;
+    m.qq = qq;
+    m.qr = qr;
+    m.factprod = factprod;
+    m.nop = nop;
+    m.dim = dim;
+    m.delta = delta;
+    m.dx_char = dx_char;
+    perix_cuda::StressCahnHilliardParams p;
+    p.dim = dim;
+    p.ndof = dim + 2;
+    p.C11 = p13[0];
+    p.C12 = p13[1];
+    p.C66 = p13[2];
+    p.A = p13[3];
+    p.Kh = p13[4];
+    p.Ch = p13[5];
+    p.Omega = p13[6];
+    p.cref = p13[7];
+    p.chi = p13[8];
+    p.kappa = p13[9];
+    p.dt = p13[10];
+    p.kres = p13[11];
+    p.rho = p13[12];
+    const perix_cuda::OpSlots s = slots_for(dim);
+    const bool ok = perix_cuda::assembleStressCahnHilliard(m, p, s, rev, lapbond, isghost, mnode, health, vel, u,
+                                                           uold, kvals, rhs);
+    const cudaError_t err = cudaDeviceSynchronize();
+    perix_cuda::shutdown();
+    return ok && err == cudaSuccess ? 0 : 1;
+}

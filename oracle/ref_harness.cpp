@@ -11,6 +11,7 @@
 //   Poisson assembly        PoissonElement bond callback in the loop of
 //                           PDSystem::formResidualAndJacobianParallel                 (FormResidualAndJacobianParallel.cpp:102-172)
 //   explicit fracture rate  ExplicitPDDOFracElement::preprocessIteration              (ExplicitPDDOFracElement.cpp:85)
+//   stress-coupled CH       StressCahnHilliardElement preprocess + nodal/bond callbacks (StressCahnHilliardElement.cpp:139-466)
 // The central-difference loop and the ghost BC preset are short restatements of
 // TimeStepping.cpp:479-547 and DirichletBC.cpp:107-147 / NeumannBC.cpp:88-105 (those translation units pull
 // in the JSON/BC registry and are not needed to reproduce their arithmetic).
@@ -34,6 +35,7 @@
 #undef private
 #include "ElmtSystem/CahnHilliardElement.h"
 #include "ElmtSystem/PoissonElement.h"
+#include "ElmtSystem/StressCahnHilliardElement.h"
 #include "MathUtils/SparseMatrix.h"
 #include "Mesh/MeshGenerator.h"
 #include "PDMesh/PDMesh.h"
@@ -388,6 +390,99 @@ double ref_ch_assemble(void *h, double chi, double kappa, double M0, double dt, 
     if (isghost)
         for (int i = 0; i < n; ++i) isghost[i] = el.getGhostFlags().empty() ? 0 : el.getGhostFlags()[(size_t)i];
     if (mnode) std::memcpy(mnode, el.getNodeMobility().data(), sizeof(double) * (size_t)n);
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// Stress-coupled Cahn-Hilliard (ndof = dim + 2: c, mu, u): StressCahnHilliardElement's preprocessIteration and
+// its nodal / bond callbacks accumulated as formResidualAndJacobianParallel does (K = -dF/dU, rhs = +F).
+// consts[6] receives the element's derived C11, C12, C66, A, Kh, Ch; lapbond/rev/isghost/mnode its own arrays.
+double ref_stress_ch_assemble(void *h, double E, double nu, int plane_stress, double Omega, double cref, double D,
+                              double chi, double kappa, double dt, const double *u, const double *uold, double *kvals,
+                              double *rhs, double *lapbond, int *rev, char *isghost, double *mnode, double *consts,
+                              int nthreads) {
+    auto *m = static_cast<RefMesh *>(h);
+    const auto &d = m->pd.getDataConstRef();
+    const int n = d.NodesNum;
+    const int ndof = m->dim + 2;
+    StressCahnHilliardElement el;
+    el.setDim(m->dim);
+    el.setE(E);
+    el.setNu(nu);
+    el.setState(plane_stress ? StressCahnHilliardElement::StressState::PlaneStress
+                             : StressCahnHilliardElement::StressState::PlaneStrain);
+    el.setOmega(Omega);
+    el.setCref(cref);
+    el.setDiffusivity(D);
+    el.setChi(chi);
+    el.setKappa(kappa);
+    VectorXd U(n * ndof), Uo(n * ndof);
+    std::memcpy(U.getDataPtr(), u, sizeof(double) * (size_t)n * ndof);
+    std::memcpy(Uo.getDataPtr(), uold, sizeof(double) * (size_t)n * ndof);
+    LocalElmtInfo info;
+    info.Dt = dt;
+    info.UseParallel = nthreads != 1;
+    PDOperators pops = m->ops;
+    pops.setAbortOnDegenerate(false);
+    el.preprocessIteration(m->pd, pops, info, ndof, U, Uo);
+    SparseMatrix K;
+    K.initFromPDMesh(d, ndof);
+    K.setToZeros();
+    std::vector<double> r((size_t)n * ndof, 0.0);
+    auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+    {
+        PDOperators ops = m->ops;
+        ops.setAbortOnDegenerate(false);
+        VectorXd R(ndof), Rn(ndof), UI(ndof), UJ(ndof), UoI(ndof), UoJ(ndof);
+        MatrixXd KII(ndof, ndof), KIJ(ndof, ndof), Kn(ndof, ndof);
+#pragma omp for schedule(guided)
+        for (int i = 1; i <= n; ++i) {
+            ops.calcAMatrix(i, d);
+            const int bi = (i - 1) * ndof;
+            for (int a = 1; a <= ndof; ++a) {
+                UI(a) = u[bi + a - 1];
+                UoI(a) = uold[bi + a - 1];
+            }
+            el.computeNodalResidualAndJacobian(info, i, UI, UoI, d.NodeVolumes[i - 1], Rn, Kn);
+            for (int a = 1; a <= ndof; ++a) {
+                r[bi + a - 1] += Rn(a);
+                for (int b = 1; b <= ndof; ++b) K.addValue(bi + a, bi + b, -Kn(a, b));
+            }
+            for (int j : d.NodesNeighNodesID[i - 1]) {
+                ops.calcOperators(i, j, d);
+                const int bj = (j - 1) * ndof;
+                for (int a = 1; a <= ndof; ++a) {
+                    UJ(a) = u[bj + a - 1];
+                    UoJ(a) = uold[bj + a - 1];
+                }
+                el.computeBondResidualAndJacobian(ops, info, i, j, UI, UJ, UoI, UoJ, d.NodeVolumes[i - 1], R, KII, KIJ);
+                for (int a = 1; a <= ndof; ++a) {
+                    r[bi + a - 1] += R(a);
+                    for (int b = 1; b <= ndof; ++b) {
+                        K.addValue(bi + a, bi + b, -KII(a, b));
+                        K.addValue(bi + a, bj + b, -KIJ(a, b));
+                    }
+                }
+            }
+        }
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    std::memcpy(kvals, K.getCSRValuesPtr(), sizeof(double) * (size_t)K.getNNZNum());
+    std::memcpy(rhs, r.data(), sizeof(double) * r.size());
+    const size_t nb = el.getLapBond().size();
+    if (lapbond) std::memcpy(lapbond, el.getLapBond().data(), sizeof(double) * nb);
+    if (rev) std::memcpy(rev, el.getRevBond().data(), sizeof(int) * nb);
+    if (isghost)
+        for (int i = 0; i < n; ++i) isghost[i] = el.getGhostFlags().empty() ? 0 : el.getGhostFlags()[(size_t)i];
+    if (mnode) std::memcpy(mnode, el.getNodeMobility().data(), sizeof(double) * (size_t)n);
+    if (consts) {
+        consts[0] = el.getC11();
+        consts[1] = el.getC12();
+        consts[2] = el.getC66();
+        consts[3] = el.getCoupling();
+        consts[4] = el.getKh();
+        consts[5] = el.getCh();
+    }
     return std::chrono::duration<double>(t1 - t0).count();
 }
 

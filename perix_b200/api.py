@@ -247,6 +247,13 @@ def _bc_arrays(bcs: List[BC], dim):
 
 
 # ---------------------------------------------------------------------------------------------- context
+class StressChParams(C.Structure):
+    """pxb_stress_ch_params (include/perix_b200.h)."""
+    _fields_ = [(k, C.c_double) for k in ("C11", "C12", "C66", "A", "Kh", "Ch", "Omega", "cref", "chi", "kappa",
+                                          "dt", "kres", "rho")]
+    DEFAULTS = {"dt": 1.0, "kres": 1e-8}
+
+
 class Context:
     """A perix_b200 device context (one GPU, one stream).  Mirrors the pxb_* entry points."""
 
@@ -592,6 +599,25 @@ class Context:
     def assemble_ch_d(self, kappa, chi, dt, mnode_ptr, u_ptr, uold_ptr, kvals_ptr, rhs_ptr):
         _check(self.L.pxb_assemble_ch_d(self.h, C.c_double(kappa), C.c_double(chi), C.c_double(dt), _p(mnode_ptr),
                                         _p(u_ptr), _p(uold_ptr), _p(kvals_ptr), _p(rhs_ptr)))
+
+    def assemble_stress_ch(self, params, mnode, u, uold=None, health=None, vel=None):
+        """Stress-coupled Cahn-Hilliard (ndof = dim + 2) K and rhs; params: dict with the fields of
+        StressChParams (C11 C12 C66 A Kh Ch Omega cref chi kappa dt kres rho)."""
+        p = StressChParams(**{k: float(params.get(k, StressChParams.DEFAULTS.get(k, 0.0)))
+                              for k, _ in StressChParams._fields_})
+        kv = np.zeros(self.nnz, np.float64)
+        rhs = np.zeros((self.dim + 2) * self.n, np.float64)
+        _check(self.L.pxb_assemble_stress_ch(self.h, C.byref(p), _p(_f64(mnode)), _p(None if health is None else _f64(health)),
+                                             _p(None if vel is None else _f64(vel)), _p(_f64(u)),
+                                             _p(None if uold is None else _f64(uold)), _p(kv), _p(rhs)))
+        return kv, rhs
+
+    def assemble_stress_ch_d(self, params, mnode_ptr, u_ptr, uold_ptr, kvals_ptr, rhs_ptr, health_ptr=None,
+                             vel_ptr=None):
+        p = StressChParams(**{k: float(params.get(k, StressChParams.DEFAULTS.get(k, 0.0)))
+                              for k, _ in StressChParams._fields_})
+        _check(self.L.pxb_assemble_stress_ch_d(self.h, C.byref(p), _p(mnode_ptr), _p(health_ptr), _p(vel_ptr),
+                                               _p(u_ptr), _p(uold_ptr), _p(kvals_ptr), _p(rhs_ptr)))
 
     def assemble_ch(self, kappa, chi, dt, mnode, u, uold):
         kv = np.zeros(self.nnz, np.float64)

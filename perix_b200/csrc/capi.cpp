@@ -1273,6 +1273,89 @@ extern "C" int pxb_assemble_ch_d(pxb_ctx *c, double kappa, double chi, double dt
     return check_launch(c, "assemble_ch");
 }
 
+extern "C" int pxb_assemble_stress_ch_d(pxb_ctx *c, const pxb_stress_ch_params *p, const double *mnode_d,
+                                        const double *health_d, const double *vel_d, const double *u_d,
+                                        const double *uold_d, double *kvals_d, double *rhs_d) {
+    PXB_TRY(need_geometry(c, "pxb_assemble_stress_ch"));
+    const int dim = c->g.dim, nd = dim + 2;
+    CsrState &k = c->csr;
+    if (!k.ready || k.ndof != nd) return fail(PXB_ERR_STATE, "pxb_assemble_stress_ch: set a pattern with ndof = dim + 2 first");
+    if (!c->ch.ready) return fail(PXB_ERR_STATE, "pxb_assemble_stress_ch: needs the CH geometry (pxb_ch_set_geometry)");
+    const OpsCache &o = c->ops;
+    if (!o.ready || o.order != 2 || o.precision != PXB_FP64)
+        return fail(PXB_ERR_STATE, "pxb_assemble_stress_ch: needs an FP64 order-2 g-build (pxb_gbuild)");
+    if (!p || !(p->dt > 0.0) || !mnode_d || !u_d || !kvals_d || !rhs_d)
+        return fail(PXB_ERR_INVALID, "pxb_assemble_stress_ch: bad arguments");
+    auto slot = [&](int pp, int q, int r) {
+        for (int s = 0; s < o.nop; ++s)
+            if (o.pqr[3 * s] == pp && o.pqr[3 * s + 1] == q && o.pqr[3 * s + 2] == r) return s;
+        return -1;
+    };
+    StressChAsmArgs a;
+    a.n = c->g.n;
+    a.dim = dim;
+    a.nop = o.nop;
+    const int mi[9][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0}, {1, 1, 0}, {0, 2, 0}, {1, 0, 1}, {0, 1, 1}, {0, 0, 2}};
+    for (int q = 0; q < 9; ++q) a.sl[q] = (dim == 3 || mi[q][2] == 0) ? slot(mi[q][0], mi[q][1], mi[q][2]) : -1;
+    a.C11 = p->C11;
+    a.C12 = p->C12;
+    a.C66 = p->C66;
+    a.A = p->A;
+    a.Kh = p->Kh;
+    a.Ch = p->Ch;
+    a.Omega = p->Omega;
+    a.cref = p->cref;
+    a.chi = p->chi;
+    a.kappa = p->kappa;
+    a.dt = p->dt;
+    a.kres = p->kres;
+    a.rho = p->rho;
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.rev = c->ch.rev.as<int>();
+    a.lap = c->ch.lap.as<double>();
+    a.vol = c->g.vol.as<double>();
+    a.mnode = mnode_d;
+    a.ghost = c->ch.ghost.p ? c->ch.ghost.as<char>() : nullptr;
+    a.ops = o.ops.as<double>();
+    a.degenerate = o.degenerate.as<uint8_t>();
+    a.health = health_d;
+    a.vel = vel_d;
+    a.rowptr = k.rowptr.as<int>();
+    a.slot = k.slot.as<int>();
+    a.diag = k.diag.as<int>();
+    a.u = u_d;
+    a.uold = uold_d;
+    a.kvals = kvals_d;
+    a.rhs = rhs_d;
+    PXB_CUDA_TRY(launch_assemble_stress_ch(a, c->stream));
+    return check_launch(c, "assemble_stress_ch");
+}
+
+extern "C" int pxb_assemble_stress_ch(pxb_ctx *c, const pxb_stress_ch_params *p, const double *mnode,
+                                      const double *health, const double *vel, const double *u, const double *uold,
+                                      double *kvals, double *rhs) {
+    PXB_TRY(need_geometry(c, "pxb_assemble_stress_ch"));
+    CsrState &k = c->csr;
+    const int dim = c->g.dim, nd = dim + 2;
+    if (!k.ready || k.ndof != nd) return fail(PXB_ERR_STATE, "pxb_assemble_stress_ch: set a pattern with ndof = dim + 2 first");
+    if (!mnode || !u || !kvals || !rhs) return fail(PXB_ERR_INVALID, "pxb_assemble_stress_ch: NULL buffer");
+    const size_t n = (size_t)c->g.n, nb = (size_t)c->g.nb;
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, sizeof(double) * (n + (health ? nb : 0) + (vel ? n * dim : 0) + 1), &tmp));
+    double *dm = static_cast<double *>(tmp), *dh = dm + n, *dv = dh + (health ? nb : 0);
+    PXB_TRY(h2d(c, dm, mnode, sizeof(double) * n));
+    if (health) PXB_TRY(h2d(c, dh, health, sizeof(double) * nb));
+    if (vel) PXB_TRY(h2d(c, dv, vel, sizeof(double) * n * dim));
+    PXB_TRY(h2d(c, k.u.p, u, sizeof(double) * n * nd));
+    if (uold) PXB_TRY(h2d(c, k.uold.p, uold, sizeof(double) * n * nd));
+    PXB_TRY(pxb_assemble_stress_ch_d(c, p, dm, health ? dh : nullptr, vel ? dv : nullptr, k.u.as<double>(),
+                                     uold ? k.uold.as<double>() : nullptr, k.kvals.as<double>(), k.rhs.as<double>()));
+    PXB_TRY(d2h(c, kvals, k.kvals.p, sizeof(double) * (size_t)k.nnz));
+    PXB_TRY(d2h(c, rhs, k.rhs.p, sizeof(double) * n * nd));
+    return sync(c);
+}
+
 extern "C" int pxb_assemble_ch(pxb_ctx *c, double kappa, double chi, double dt, const double *mnode,
                                const double *u, const double *uold, double *kvals, double *rhs) {
     PXB_TRY(need_geometry(c, "pxb_assemble_ch"));

@@ -14,7 +14,7 @@ namespace {
 
 struct ShimState {
     pxb_ctx *ctx = nullptr;
-    // which structure is resident (0 none, 1 scalar assembly, 2 explicit fracture, 3 Cahn-Hilliard)
+    // which structure is resident (0 none, 1 scalar assembly, 2 explicit fracture, 3 Cahn-Hilliard, 4 stress CH)
     int kind = 0;
     int n = 0, nnz = 0, nbtot = 0, nop = 0, ndof = 0, dim = 0;
     int precision = PXB_FP64;
@@ -135,11 +135,45 @@ bool assembleCahnHilliard(const CahnHilliardMesh &m, const CahnHilliardParams &p
     return true;
 }
 
-bool assembleStressCahnHilliard(const AssembleMesh &, const StressCahnHilliardParams &, const OpSlots &, const int *,
-                                const double *, const char *, const double *, const double *, const double *,
-                                const double *, const double *, double *, double *) {
-    std::fprintf(stderr, "[perix_b200] assembleStressCahnHilliard is not implemented by this backend\n");
-    return false;
+bool assembleStressCahnHilliard(const AssembleMesh &m, const StressCahnHilliardParams &p, const OpSlots &s,
+                                const int *rev, const double *lapbond, const char *isghost, const double *mnode,
+                                const double *health, const double *vel, const double *u, const double *uold,
+                                double *out_Kvals, double *out_rhs) {
+    (void)s;  // the operator slots are resolved from the multi-index table, which must be the reference's
+    if (m.N <= 0 || (p.dim != 2 && p.dim != 3) || p.ndof != p.dim + 2 || !(p.dt > 0.0)) return false;
+    if (m.nodeHorizon) {
+        std::fprintf(stderr, "[perix_b200] assembleStressCahnHilliard: variable horizon is not supported\n");
+        return false;
+    }
+    if (!ensure_ctx()) return false;
+    if (order_of(m) != 2 || !qtable_matches(m, 2)) {
+        std::fprintf(stderr, "[perix_b200] assembleStressCahnHilliard: needs the order-2 multi-index table\n");
+        return false;
+    }
+    const int nbtot = m.neigh_off[m.N];
+    if (g_shim.kind != 4 || g_shim.n != m.N || g_shim.nnz != m.nnz || g_shim.nbtot != nbtot || g_shim.dim != p.dim) {
+        if (!upload_mesh(m, 2)) return false;
+        int ndeg = 0, first = 0;
+        const int st = pxb_gbuild(g_shim.ctx, 2, PXB_FP64, &ndeg, &first);
+        if (st == PXB_ERR_DEGENERATE)
+            std::fprintf(stderr, "[perix_b200] assembleStressCahnHilliard: %s (rows of those nodes are zeroed)\n",
+                         pxb_last_error());
+        else if (st != PXB_OK)
+            return report("gbuild");
+        if (pxb_ch_set_geometry(g_shim.ctx, rev, lapbond, isghost) != PXB_OK) return report("ch geometry");
+        if (pxb_csr_set_pattern(g_shim.ctx, p.ndof, m.csr_off, m.csr_col, m.nnz) != PXB_OK) return report("csr pattern");
+        g_shim.kind = 4;
+        g_shim.n = m.N;
+        g_shim.nnz = m.nnz;
+        g_shim.nbtot = nbtot;
+        g_shim.dim = p.dim;
+    } else if (pxb_ch_set_geometry(g_shim.ctx, rev, lapbond, isghost) != PXB_OK) {
+        return report("ch geometry");  // host-built per element; cheap to refresh
+    }
+    const pxb_stress_ch_params q{p.C11, p.C12, p.C66, p.A, p.Kh, p.Ch, p.Omega, p.cref, p.chi, p.kappa, p.dt, p.kres, p.rho};
+    if (pxb_assemble_stress_ch(g_shim.ctx, &q, mnode, health, vel, u, uold, out_Kvals, out_rhs) != PXB_OK)
+        return report("assembleStressCahnHilliard");
+    return true;
 }
 
 bool assembleCached(const AssembleMesh &, const CachedParams &, const OpSlots &, const double *, const double *,

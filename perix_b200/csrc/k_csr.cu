@@ -11,6 +11,8 @@
 
 namespace pxb {
 
+__device__ __forceinline__ double ch_clamp(double c) { return fmax(1.0e-8, fmin(1.0 - 1.0e-8, c)); }
+
 __device__ __forceinline__ int find_slot(const int *cols, int lo, int hi, int target) {
     int l = lo, h = hi - 1;
     while (l <= h) {
@@ -106,9 +108,201 @@ cudaError_t launch_assemble_scalar(const ScalarAsmArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// ---- conservative Cahn-Hilliard (2 dof: c, mu) ------------------------------------------------------------
-__device__ __forceinline__ double ch_clamp(double c) { return fmax(1.0e-8, fmin(1.0 - 1.0e-8, c)); }
+// ---- stress-coupled Cahn-Hilliard (reference src/PDSystem/CudaAssembleKernels.cu:685-874): rows c, mu, u.
+//      Per bond: the species flux w_ij = 0.5 (M_i g2_ij + V_j/V_i M_j g2_ji) (dropped on ghost bonds) on the
+//      c-row, the gradient energy kappa g2_ij and the hydrostatic coupling Omega Kh grad(u) on the mu-row, the
+//      Navier operators and the chemo-mechanical body force -A grad(c) on the u-rows; the mechanical terms are
+//      gated by g = 1 (intact) or kres (broken).  Nodal: (c - c_old)/dt, mu - f'(c) + Omega Ch (c - cref), and
+//      the optional backward-Euler inertia -rho (u - u_old - v dt)/dt^2.  K_IJ is stored per bond; the
+//      diagonal block accumulates the nodal Jacobian plus the sum of K_IJ (K_II = -K_IJ per bond). ----------
+template <int DIM>
+__global__ void __launch_bounds__(256) assemble_stress_ch_kernel(StressChAsmArgs a) {
+    constexpr int WPB = 256 / kWarp;
+    constexpr int ND = DIM + 2;
+    // distinct per-bond coefficients: coeff_c, kappaLap, cmu[DIM], cb[DIM], then the Navier block
+    // 2D: p11 pxy p22;  3D: p11 p22 p33 p12 p13 p23
+    constexpr int NK = 2 + 2 * DIM + (DIM == 3 ? 6 : 3);
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int *sl = a.sl;
+    for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
+        const int rb = i * ND;
+        for (int s = a.rowptr[rb] + lane; s < a.rowptr[rb + ND]; s += kWarp) a.kvals[s] = 0.0;
+        __syncwarp();
+        if (a.degenerate && a.degenerate[i]) {  // singular moment system: the rows stay zero
+            if (lane < ND) a.rhs[rb + lane] = 0.0;
+            continue;
+        }
+        double uI[ND];
+#pragma unroll
+        for (int b = 0; b < ND; ++b) uI[b] = a.u[rb + b];
+        const double Vi = a.vol[i], Mi = a.mnode[i];
+        double R[ND], S[NK];
+#pragma unroll
+        for (int b = 0; b < ND; ++b) R[b] = 0.0;
+#pragma unroll
+        for (int k = 0; k < NK; ++k) S[k] = 0.0;
+        for (int t = a.off[i] + lane; t < a.off[i + 1]; t += kWarp) {
+            const int j = __ldg(a.nbr + t);
+            const double *op = a.ops + (size_t)t * a.nop;
+            const double g = a.health ? (a.health[t] > 0.0 ? 1.0 : a.kres) : 1.0;
+            double G1[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) G1[d] = g * op[sl[d]];
+            const double Gxx = g * op[sl[3]], Gxy = g * op[sl[4]], Gyy = g * op[sl[5]];
+            const bool ghostJ = a.ghost && a.ghost[j];
+            const double g2A = a.lap[t];
+            double coeff_c = 0.0;
+            if (!ghostJ) {
+                const int r = a.rev[t];
+                const double w = (r >= 0 && Vi > 0.0) ? 0.5 * (Mi * g2A + (a.vol[j] / Vi) * a.mnode[j] * a.lap[r])
+                                                      : Mi * g2A;
+                coeff_c = -w;
+            }
+            const double kappaLap = ghostJ ? 0.0 : a.kappa * g2A;
+            double k[NK];
+            k[0] = coeff_c;
+            k[1] = kappaLap;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                k[2 + d] = a.Omega * a.Kh * G1[d];
+                k[2 + DIM + d] = -a.A * G1[d];
+            }
+            double du[DIM];
+            const double dC = a.u[(size_t)j * ND] - uI[0], dMu = a.u[(size_t)j * ND + 1] - uI[1];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) du[d] = a.u[(size_t)j * ND + 2 + d] - uI[2 + d];
+            double Kb[ND][ND];
+#pragma unroll
+            for (int r = 0; r < ND; ++r)
+#pragma unroll
+                for (int c = 0; c < ND; ++c) Kb[r][c] = 0.0;
+            Kb[0][1] = coeff_c;
+            Kb[1][0] = kappaLap;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                Kb[1][2 + d] = k[2 + d];
+                Kb[2 + d][0] = k[2 + DIM + d];
+            }
+            constexpr int P0 = 2 + 2 * DIM;
+            if constexpr (DIM == 2) {
+                k[P0 + 0] = a.C11 * Gxx + a.C66 * Gyy;          // p11
+                k[P0 + 1] = (a.C12 + a.C66) * Gxy;              // pxy
+                k[P0 + 2] = a.C66 * Gxx + a.C11 * Gyy;          // p22
+                Kb[2][2] = k[P0];
+                Kb[2][3] = Kb[3][2] = k[P0 + 1];
+                Kb[3][3] = k[P0 + 2];
+            } else {
+                const double Gzz = g * op[sl[8]], Gxz = g * op[sl[6]], Gyz = g * op[sl[7]];
+                const double cc = a.C12 + a.C66;
+                k[P0 + 0] = a.C11 * Gxx + a.C66 * (Gyy + Gzz);  // p11
+                k[P0 + 1] = a.C11 * Gyy + a.C66 * (Gxx + Gzz);  // p22
+                k[P0 + 2] = a.C11 * Gzz + a.C66 * (Gxx + Gyy);  // p33
+                k[P0 + 3] = cc * Gxy;                           // p12
+                k[P0 + 4] = cc * Gxz;                           // p13
+                k[P0 + 5] = cc * Gyz;                           // p23
+                Kb[2][2] = k[P0];
+                Kb[3][3] = k[P0 + 1];
+                Kb[4][4] = k[P0 + 2];
+                Kb[2][3] = Kb[3][2] = k[P0 + 3];
+                Kb[2][4] = Kb[4][2] = k[P0 + 4];
+                Kb[3][4] = Kb[4][3] = k[P0 + 5];
+            }
+            // residual of this bond: R = K_IJ (u_j - u_i) row by row
+            R[0] += coeff_c * dMu;
+            double r1 = kappaLap * dC;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) r1 += k[2 + d] * du[d];
+            R[1] += r1;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                double rd = k[2 + DIM + d] * dC;
+#pragma unroll
+                for (int e = 0; e < DIM; ++e) rd += Kb[2 + d][2 + e] * du[e];
+                R[2 + d] += rd;
+            }
+#pragma unroll
+            for (int q = 0; q < NK; ++q) S[q] += k[q];
+            const int *st = a.slot + (size_t)t * ND * ND;
+#pragma unroll
+            for (int r = 0; r < ND; ++r)
+#pragma unroll
+                for (int c = 0; c < ND; ++c) a.kvals[st[r * ND + c]] = -Kb[r][c];
+        }
+#pragma unroll
+        for (int b = 0; b < ND; ++b) R[b] = group_sum<kWarp>(R[b]);
+#pragma unroll
+        for (int q = 0; q < NK; ++q) S[q] = group_sum<kWarp>(S[q]);
+        if (lane == 0) {
+            const double c = uI[0], mu = uI[1], cold = a.uold ? a.uold[rb] : 0.0;
+            const double cc = ch_clamp(c);
+            const double fp = log(cc / (1.0 - cc)) + a.chi * (1.0 - 2.0 * cc);
+            const double fpp = 1.0 / (cc * (1.0 - cc)) - 2.0 * a.chi;
+            double rl[ND], kii[ND][ND];
+#pragma unroll
+            for (int r = 0; r < ND; ++r) {
+                rl[r] = 0.0;
+#pragma unroll
+                for (int q = 0; q < ND; ++q) kii[r][q] = 0.0;
+            }
+            rl[0] = (c - cold) / a.dt;
+            rl[1] = mu - fp + a.Omega * a.Ch * (c - a.cref);
+            kii[0][0] = -(1.0 / a.dt);
+            kii[1][0] = -(-fpp + a.Omega * a.Ch);
+            kii[1][1] = -(1.0);
+            if (a.rho > 0.0 && a.vel) {
+                const double c0 = a.rho / (a.dt * a.dt);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    const double uo = a.uold ? a.uold[rb + 2 + d] : 0.0;
+                    rl[2 + d] += -c0 * (uI[2 + d] - uo - a.vel[(size_t)i * DIM + d] * a.dt);
+                    kii[2 + d][2 + d] += c0;
+                }
+            }
+            // kii += sum over bonds of K_IJ (= -K_II)
+            constexpr int P0 = 2 + 2 * DIM;
+            kii[0][1] += S[0];
+            kii[1][0] += S[1];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                kii[1][2 + d] += S[2 + d];
+                kii[2 + d][0] += S[2 + DIM + d];
+            }
+            if constexpr (DIM == 2) {
+                kii[2][2] += S[P0];
+                kii[2][3] += S[P0 + 1];
+                kii[3][2] += S[P0 + 1];
+                kii[3][3] += S[P0 + 2];
+            } else {
+                kii[2][2] += S[P0];
+                kii[3][3] += S[P0 + 1];
+                kii[4][4] += S[P0 + 2];
+                kii[2][3] += S[P0 + 3];
+                kii[3][2] += S[P0 + 3];
+                kii[2][4] += S[P0 + 4];
+                kii[4][2] += S[P0 + 4];
+                kii[3][4] += S[P0 + 5];
+                kii[4][3] += S[P0 + 5];
+            }
+            const int *dg = a.diag + (size_t)i * ND * ND;
+#pragma unroll
+            for (int r = 0; r < ND; ++r) {
+#pragma unroll
+                for (int q = 0; q < ND; ++q) a.kvals[dg[r * ND + q]] = kii[r][q];
+                a.rhs[rb + r] = rl[r] + R[r];
+            }
+        }
+    }
+}
 
+cudaError_t launch_assemble_stress_ch(const StressChAsmArgs &a, cudaStream_t s) {
+    const int g = (a.n + 7) / 8;
+    if (a.dim == 3) assemble_stress_ch_kernel<3><<<g > 0 ? g : 1, 256, 0, s>>>(a);
+    else assemble_stress_ch_kernel<2><<<g > 0 ? g : 1, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// ---- conservative Cahn-Hilliard (2 dof: c, mu) ------------------------------------------------------------
 __global__ void __launch_bounds__(256) assemble_ch_kernel(ChAsmArgs a) {
     constexpr int WPB = 256 / kWarp;
     const int lane = threadIdx.x & 31;

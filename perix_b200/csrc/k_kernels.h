@@ -272,6 +272,26 @@ struct ChAsmArgs {
     double *kvals = nullptr, *rhs = nullptr;
 };
 cudaError_t launch_assemble_ch(const ChAsmArgs &a, cudaStream_t s);
+// Stress-coupled Cahn-Hilliard (rows c, mu, u_x, u_y[, u_z] per node; ndof = dim + 2): the device twin of
+// the reference's stressCahnHilliardKernel (src/PDSystem/CudaAssembleKernels.cu:685-874) on the FP64 order-2
+// operator cache.  sl = operator slots of d/dx d/dy d/dz d2/dx2 d2/dxdy d2/dy2 d2/dxdz d2/dydz d2/dz2 (-1 absent).
+struct StressChAsmArgs {
+    int n = 0, dim = 2, nop = 0;
+    int sl[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};
+    double C11 = 0, C12 = 0, C66 = 0, A = 0, Kh = 0, Ch = 0, Omega = 0, cref = 0, chi = 0, kappa = 0, dt = 1;
+    double kres = 1e-8, rho = 0;
+    const int *off = nullptr, *nbr = nullptr, *rev = nullptr;
+    const double *lap = nullptr, *vol = nullptr, *mnode = nullptr;
+    const char *ghost = nullptr;
+    const double *ops = nullptr;        // FP64 [nb][nop]
+    const uint8_t *degenerate = nullptr;
+    const double *health = nullptr;     // [nb] frozen bond health (NULL: every bond intact)
+    const double *vel = nullptr;        // [n*dim] committed velocity (inertia when rho > 0)
+    const int *rowptr = nullptr, *slot = nullptr, *diag = nullptr;
+    const double *u = nullptr, *uold = nullptr;
+    double *kvals = nullptr, *rhs = nullptr;
+};
+cudaError_t launch_assemble_stress_ch(const StressChAsmArgs &a, cudaStream_t s);
 // CH one-off geometry from the order-2 operator cache (CahnHilliardElement.cpp:93-152): per bond the PDDO
 // Laplacian g_xx + g_yy (+ g_zz), lambda-corrected on non-ghost bonds with lambda = 2 dim / sum_j g2_ij
 // (|x_j|^2 - |x_i|^2); ghost flags from the mirror map.  slots: the operator slots of d2/dx2, d2/dy2, d2/dz2.

@@ -68,6 +68,35 @@ def ch_fixture():
          params=np.array([chi, kappa, M0, dt]), kvals=kv, rhs=rhs, **geo)
 
 
+def stress_ch_fixture(dim):
+    """Stress-coupled Cahn-Hilliard (ndof = dim + 2: c, mu, u) through the reference's StressCahnHilliardElement:
+    2D 24x24 lattice on the unit square, 3D 5x5x4 on [0,0.5]x[0,0.5]x[0,0.4], delta = 3.015h, plane strain,
+    E = 1e3, nu = 0.3, Omega = 0.05, cref = 0.5, D = 1, chi = 2.5, kappa = 1e-4, dt = 1e-6; c = 0.5 + U(+-0.05),
+    mu = f'(c) plus noise, displacements N(0, (1e-3 h)^2) (seeded); uold = u with c moved."""
+    if dim == 2:
+        m = RefMesh.structured(2, 24, 24, 0, [0, 1, 0, 1], 3.015, 2)
+        h = 1.0 / 24
+    else:
+        m = RefMesh.structured(3, 5, 5, 4, [0, 0.5, 0, 0.5, 0, 0.4], 3.015, 2)
+        h = 0.1
+    nd = dim + 2
+    rp, cols = m.csr_pattern(nd)
+    rng = np.random.default_rng(31 + dim)
+    E, nu, Omega, cref, D, chi, kappa, dt = 1e3, 0.3, 0.05, 0.5, 1.0, 2.5, 1e-4, 1e-6
+    c = 0.5 + rng.uniform(-0.05, 0.05, m.n)
+    mu = np.log(c / (1 - c)) + chi * (1 - 2 * c) + rng.standard_normal(m.n) * 1e-3
+    u = np.zeros((m.n, nd))
+    u[:, 0] = c
+    u[:, 1] = mu
+    u[:, 2:] = rng.standard_normal((m.n, dim)) * 1e-3 * h
+    u = u.reshape(-1)
+    uold = u.copy()
+    uold[0::nd] -= rng.uniform(-1e-4, 1e-4, m.n)
+    kv, rhs, geo, _ = m.stress_ch_assemble(E, nu, False, Omega, cref, D, chi, kappa, dt, u, uold)
+    save("stressch%dd" % dim, **mesh_arrays(m), rowptr=rp, cols=cols, u=u, uold=uold,
+         params=np.array([E, nu, Omega, cref, D, chi, kappa, dt]), kvals=kv, rhs=rhs, **geo)
+
+
 def lattice3d_fixture():
     m = RefMesh.structured(3, 5, 5, 4, [0, 0.5, 0, 0.5, 0, 0.4], 3.015, 2)
     ops, deg = m.gbuild()
@@ -198,3 +227,5 @@ if __name__ == "__main__":
     epf2d_fixture()
     epf3d_fixture()
     ch_fixture()
+    stress_ch_fixture(2)
+    stress_ch_fixture(3)

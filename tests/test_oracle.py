@@ -224,3 +224,39 @@ def test_c1_solve_with_reference_assembly():
     L = px.lattice(2, 64, 64, 0, [0.0, 1.0, 0.0, 1.0])
     _, err = c1_poisson(px, kv, rhs, L, rp, cols)
     assert abs(err - 1.4357e-3) <= 1e-6
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_stress_ch_restatement_vs_reference_element(dim):
+    """The numpy restatement of the stress-coupled CH assembly (oracle/stress_ch.py) against the reference's
+    StressCahnHilliardElement on its own operators, and against the committed fixture of the same mesh."""
+    RefMesh = _ref()
+    from conftest import load_golden
+    from oracle.stress_ch import stress_ch_assemble
+    d = load_golden("stressch%dd" % dim)
+    if dim == 2:
+        m = RefMesh.structured(2, 24, 24, 0, [0, 1, 0, 1], 3.015, 2)
+    else:
+        m = RefMesh.structured(3, 5, 5, 4, [0, 0.5, 0, 0.5, 0, 0.4], 3.015, 2)
+    assert np.array_equal(m.off, d["off"]) and np.array_equal(m.ids, d["ids"])
+    ops, _ = m.gbuild()
+    E, nu, Omega, cref, D, chi, kappa, dt = (float(x) for x in d["params"])
+    kv, rhs, geo, _ = m.stress_ch_assemble(E, nu, False, Omega, cref, D, chi, kappa, dt, d["u"], d["uold"])
+    assert np.array_equal(kv, d["kvals"]) and np.array_equal(rhs, d["rhs"])
+    C11, C12, C66, A, Kh, Ch = (float(x) for x in geo["consts"])
+    prm = dict(C11=C11, C12=C12, C66=C66, A=A, Kh=Kh, Ch=Ch, Omega=Omega, cref=cref, chi=chi, kappa=kappa, dt=dt,
+               kres=1e-8, rho=0.0)
+    pqr = m.qindices()[0]
+    ko, ro = stress_ch_assemble(dim, m.off, m.ids, ops, pqr, m.vols, geo["rev"], geo["lapbond"], geo["isghost"],
+                                geo["mnode"], d["u"], d["uold"], d["rowptr"], d["cols"], prm)
+    rp, cols = d["rowptr"], d["cols"]
+    nd = dim + 2
+    rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+    nbr = (cols // nd) != (rows // nd)
+    ks = np.zeros(rp.size - 1)
+    np.maximum.at(ks, rows[nbr], np.abs(kv[nbr]))
+    assert (np.abs(ko - kv) <= 1e-12 * np.maximum(ks[rows], np.abs(kv))).all()
+    du = d["u"][cols] - d["u"][(rows // nd) * nd + (cols % nd)]
+    rs = np.zeros(rp.size - 1)
+    np.maximum.at(rs, rows[nbr], np.abs(kv[nbr] * du[nbr]))
+    assert (np.abs(ro - rhs) <= 1e-12 * np.maximum(rs, np.abs(rhs))).all()
