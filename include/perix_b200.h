@@ -301,6 +301,24 @@ int pxb_assemble_stress_ch_d(pxb_ctx *ctx, const pxb_stress_ch_params *p, const 
 int pxb_assemble_stress_ch(pxb_ctx *ctx, const pxb_stress_ch_params *p, const double *mnode, const double *health,
                            const double *vel, const double *u, const double *uold, double *kvals, double *rhs);
 
+/* Implicit PDDO dynamic fracture, the boundary of the reference's perix_cuda::assembleCached
+ * (include/PDSystem/CudaAssemble.h:216-219; kernel src/PDSystem/CudaAssembleKernels.cu:880-1024; physics
+ * PDDODynamicFracElement.cpp:207-306).  Rows per node: u (ndof = dim).  Needs an FP64 order-2 g-build and a
+ * pattern set with ndof = dim.  nodecache[i*ncache + a] = committed velocity (may be NULL: zero), bondcache
+ * [t*nbcache] = frozen bond health (may be NULL: every bond 1; a bond with health <= 0 carries nothing); uold may
+ * be NULL.  R = b - rho (u - u_old - v dt)/dt^2 + sum of health-scaled Navier bond terms; K = -dF/dU. */
+typedef struct pxb_cached_params {
+    double C11, C12, C66;  /* elastic stiffness */
+    double rho, dt;        /* density, backward-Euler step */
+    double b[3];           /* body force */
+} pxb_cached_params;
+int pxb_assemble_cached_d(pxb_ctx *ctx, const pxb_cached_params *p, const double *nodecache_d, int ncache,
+                          const double *bondcache_d, int nbcache, const double *u_d, const double *uold_d,
+                          double *kvals_d, double *rhs_d);
+int pxb_assemble_cached(pxb_ctx *ctx, const pxb_cached_params *p, const double *nodecache, int ncache,
+                        const double *bondcache, int nbcache, const double *u, const double *uold, double *kvals,
+                        double *rhs);
+
 #ifdef __cplusplus
 }
 #endif

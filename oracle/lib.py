@@ -299,6 +299,7 @@ def _ref_lib():
         L.ref_poisson_assemble.restype = C.c_double
         L.ref_ch_assemble.restype = C.c_double
         L.ref_stress_ch_assemble.restype = C.c_double
+        L.ref_dynfrac_assemble.restype = C.c_double
         L.ref_epf_create.restype = vp
         L.ref_epf_rate.restype = C.c_double
         L.ref_epf_run.restype = C.c_double
@@ -450,6 +451,26 @@ class RefMesh:
                                           _ptr(consts, C.c_double), int(nthreads or os.cpu_count()))
         return kv, rhs, dict(lapbond=lap[:self.nb], rev=rev[:self.nb], isghost=ghost, mnode=mnode,
                              consts=consts), t
+
+    def dynfrac_assemble(self, E, nu, rho, G0, dt, uprev, uold, u, plane_stress=False, tension_only=True,
+                         b=(0.0, 0.0, 0.0)):
+        """PDDODynamicFracElement (ndof = dim): initialised from uprev, committed at uold, assembled at u.
+        Returns K, rhs, the committed velocity [n*dim], bond health [nb] and (C11, C12, C66)."""
+        nd = self.dim
+        nnz = self.L.ref_csr_nnz(self.h, nd)
+        kv = np.zeros(nnz, np.float64)
+        rhs = np.zeros(self.n * nd, np.float64)
+        vel = np.zeros(self.n * nd, np.float64)
+        health = np.zeros(max(1, self.nb), np.float64)
+        consts = np.zeros(3, np.float64)
+        f64 = lambda a: np.ascontiguousarray(a, np.float64)
+        self.L.ref_dynfrac_assemble(self.h, C.c_double(E), C.c_double(nu), C.c_double(rho), C.c_double(G0),
+                                    int(plane_stress), int(tension_only), C.c_double(b[0]), C.c_double(b[1]),
+                                    C.c_double(b[2]), C.c_double(dt), _ptr(f64(uprev), C.c_double),
+                                    _ptr(f64(uold), C.c_double), _ptr(f64(u), C.c_double), _ptr(kv, C.c_double),
+                                    _ptr(rhs, C.c_double), _ptr(vel, C.c_double), _ptr(health, C.c_double),
+                                    _ptr(consts, C.c_double))
+        return kv, rhs, vel, health[:self.nb], consts
 
     def bc_preset(self, bcs, t, u):
         p = bc_program_arrays(bcs, self.dim)

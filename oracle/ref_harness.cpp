@@ -12,6 +12,7 @@
 //                           PDSystem::formResidualAndJacobianParallel                 (FormResidualAndJacobianParallel.cpp:102-172)
 //   explicit fracture rate  ExplicitPDDOFracElement::preprocessIteration              (ExplicitPDDOFracElement.cpp:85)
 //   stress-coupled CH       StressCahnHilliardElement preprocess + nodal/bond callbacks (StressCahnHilliardElement.cpp:139-466)
+//   implicit dyn. fracture  PDDODynamicFracElement preprocess (init + one commit) + callbacks (PDDODynamicFracElement.cpp:82-306)
 // The central-difference loop and the ghost BC preset are short restatements of
 // TimeStepping.cpp:479-547 and DirichletBC.cpp:107-147 / NeumannBC.cpp:88-105 (those translation units pull
 // in the JSON/BC registry and are not needed to reproduce their arithmetic).
@@ -34,6 +35,7 @@
 #include "PDOperators/PDOperators.h"
 #undef private
 #include "ElmtSystem/CahnHilliardElement.h"
+#include "ElmtSystem/PDDODynamicFracElement.h"
 #include "ElmtSystem/PoissonElement.h"
 #include "ElmtSystem/StressCahnHilliardElement.h"
 #include "MathUtils/SparseMatrix.h"
@@ -482,6 +484,99 @@ double ref_stress_ch_assemble(void *h, double E, double nu, int plane_stress, do
         consts[3] = el.getCoupling();
         consts[4] = el.getKh();
         consts[5] = el.getCh();
+    }
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// Implicit PDDO dynamic fracture (ndof = dim): PDDODynamicFracElement initialised at step 1 from uprev, then
+// committed at step 2 from uold (velocity (uold - uprev)/dt, bond failure by stretch at uold), then its nodal and
+// bond callbacks at u accumulated as formResidualAndJacobianParallel does.  vel_out[n*dim] and health_out[nbtot]
+// (family order) receive the committed velocity and health; consts[3] = C11, C12, C66.
+double ref_dynfrac_assemble(void *h, double E, double nu, double rho, double G0, int plane_stress, int tension_only,
+                            double bx, double by, double bz, double dt, const double *uprev, const double *uold,
+                            const double *u, double *kvals, double *rhs, double *vel_out, double *health_out,
+                            double *consts) {
+    auto *m = static_cast<RefMesh *>(h);
+    const auto &d = m->pd.getDataConstRef();
+    const int n = d.NodesNum;
+    const int ndof = m->dim;
+    PDDODynamicFracElement el;
+    el.setDim(m->dim);
+    el.setE(E);
+    el.setNu(nu);
+    el.setRho(rho);
+    el.setG0(G0);
+    el.setState(plane_stress ? PDDODynamicFracElement::StressState::PlaneStress
+                             : PDDODynamicFracElement::StressState::PlaneStrain);
+    el.setTensionOnly(tension_only != 0);
+    el.setDamageOn(true);
+    el.setBodyForce(bx, by, bz);
+    VectorXd U(n * ndof), Uo(n * ndof), Up(n * ndof);
+    std::memcpy(U.getDataPtr(), u, sizeof(double) * (size_t)n * ndof);
+    std::memcpy(Uo.getDataPtr(), uold, sizeof(double) * (size_t)n * ndof);
+    std::memcpy(Up.getDataPtr(), uprev, sizeof(double) * (size_t)n * ndof);
+    LocalElmtInfo info;
+    info.Dt = dt;
+    info.UseParallel = false;
+    info.Timestep = 1;
+    PDOperators pops = m->ops;
+    pops.setAbortOnDegenerate(false);
+    el.preprocessIteration(m->pd, pops, info, ndof, U, Up);
+    info.Timestep = 2;
+    el.preprocessIteration(m->pd, pops, info, ndof, U, Uo);
+    SparseMatrix K;
+    K.initFromPDMesh(d, ndof);
+    K.setToZeros();
+    std::vector<double> r((size_t)n * ndof, 0.0);
+    auto t0 = std::chrono::steady_clock::now();
+    {
+        PDOperators ops = m->ops;
+        ops.setAbortOnDegenerate(false);
+        VectorXd R(ndof), Rn(ndof), UI(ndof), UJ(ndof), UoI(ndof), UoJ(ndof);
+        MatrixXd KII(ndof, ndof), KIJ(ndof, ndof), Kn(ndof, ndof);
+        for (int i = 1; i <= n; ++i) {
+            ops.calcAMatrix(i, d);
+            const int bi = (i - 1) * ndof;
+            for (int a = 1; a <= ndof; ++a) {
+                UI(a) = u[bi + a - 1];
+                UoI(a) = uold[bi + a - 1];
+            }
+            el.computeNodalResidualAndJacobian(info, i, UI, UoI, d.NodeVolumes[i - 1], Rn, Kn);
+            for (int a = 1; a <= ndof; ++a) {
+                r[bi + a - 1] += Rn(a);
+                for (int b = 1; b <= ndof; ++b) K.addValue(bi + a, bi + b, -Kn(a, b));
+            }
+            for (int j : d.NodesNeighNodesID[i - 1]) {
+                ops.calcOperators(i, j, d);
+                const int bj = (j - 1) * ndof;
+                for (int a = 1; a <= ndof; ++a) {
+                    UJ(a) = u[bj + a - 1];
+                    UoJ(a) = uold[bj + a - 1];
+                }
+                el.computeBondResidualAndJacobian(ops, info, i, j, UI, UJ, UoI, UoJ, d.NodeVolumes[i - 1], R, KII, KIJ);
+                for (int a = 1; a <= ndof; ++a) {
+                    r[bi + a - 1] += R(a);
+                    for (int b = 1; b <= ndof; ++b) {
+                        K.addValue(bi + a, bi + b, -KII(a, b));
+                        K.addValue(bi + a, bj + b, -KIJ(a, b));
+                    }
+                }
+            }
+        }
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    std::memcpy(kvals, K.getCSRValuesPtr(), sizeof(double) * (size_t)K.getNNZNum());
+    std::memcpy(rhs, r.data(), sizeof(double) * r.size());
+    if (vel_out) std::memcpy(vel_out, el.getVel().data(), sizeof(double) * el.getVel().size());
+    if (health_out) {
+        size_t t = 0;
+        for (const auto &fam : el.getBondHealth())
+            for (double x : fam) health_out[t++] = x;
+    }
+    if (consts) {
+        consts[0] = el.getC11();
+        consts[1] = el.getC12();
+        consts[2] = el.getC66();
     }
     return std::chrono::duration<double>(t1 - t0).count();
 }

@@ -254,6 +254,12 @@ class StressChParams(C.Structure):
     DEFAULTS = {"dt": 1.0, "kres": 1e-8}
 
 
+class CachedParams(C.Structure):
+    """pxb_cached_params (include/perix_b200.h)."""
+    _fields_ = [("C11", C.c_double), ("C12", C.c_double), ("C66", C.c_double), ("rho", C.c_double),
+                ("dt", C.c_double), ("b", C.c_double * 3)]
+
+
 class Context:
     """A perix_b200 device context (one GPU, one stream).  Mirrors the pxb_* entry points."""
 
@@ -618,6 +624,20 @@ class Context:
                               for k, _ in StressChParams._fields_})
         _check(self.L.pxb_assemble_stress_ch_d(self.h, C.byref(p), _p(mnode_ptr), _p(health_ptr), _p(vel_ptr),
                                                _p(u_ptr), _p(uold_ptr), _p(kvals_ptr), _p(rhs_ptr)))
+
+    def assemble_cached(self, params, u, uold=None, nodecache=None, ncache=3, bondcache=None, nbcache=1):
+        """Implicit PDDO dynamic fracture (ndof = dim) K and rhs; params: dict with C11 C12 C66 rho dt and b
+        (3 values); nodecache [n*ncache] committed velocity, bondcache [nb*nbcache] frozen bond health."""
+        p = CachedParams(C11=float(params["C11"]), C12=float(params["C12"]), C66=float(params["C66"]),
+                         rho=float(params["rho"]), dt=float(params["dt"]),
+                         b=(C.c_double * 3)(*[float(x) for x in params.get("b", (0.0, 0.0, 0.0))]))
+        kv = np.zeros(self.nnz, np.float64)
+        rhs = np.zeros(self.dim * self.n, np.float64)
+        _check(self.L.pxb_assemble_cached(self.h, C.byref(p), _p(None if nodecache is None else _f64(nodecache)),
+                                          int(ncache), _p(None if bondcache is None else _f64(bondcache)),
+                                          int(nbcache), _p(_f64(u)), _p(None if uold is None else _f64(uold)),
+                                          _p(kv), _p(rhs)))
+        return kv, rhs
 
     def assemble_ch(self, kappa, chi, dt, mnode, u, uold):
         kv = np.zeros(self.nnz, np.float64)

@@ -1356,6 +1356,88 @@ extern "C" int pxb_assemble_stress_ch(pxb_ctx *c, const pxb_stress_ch_params *p,
     return sync(c);
 }
 
+extern "C" int pxb_assemble_cached_d(pxb_ctx *c, const pxb_cached_params *p, const double *nodecache_d, int ncache,
+                                     const double *bondcache_d, int nbcache, const double *u_d, const double *uold_d,
+                                     double *kvals_d, double *rhs_d) {
+    PXB_TRY(need_geometry(c, "pxb_assemble_cached"));
+    const int dim = c->g.dim;
+    CsrState &k = c->csr;
+    if (!k.ready || k.ndof != dim) return fail(PXB_ERR_STATE, "pxb_assemble_cached: set a pattern with ndof = dim first");
+    const OpsCache &o = c->ops;
+    if (!o.ready || o.order != 2 || o.precision != PXB_FP64)
+        return fail(PXB_ERR_STATE, "pxb_assemble_cached: needs an FP64 order-2 g-build (pxb_gbuild)");
+    if (!p || !(p->dt > 0.0) || !u_d || !kvals_d || !rhs_d || (nodecache_d && ncache < dim) ||
+        (bondcache_d && nbcache < 1))
+        return fail(PXB_ERR_INVALID, "pxb_assemble_cached: bad arguments");
+    auto slot = [&](int pp, int q, int r) {
+        for (int s = 0; s < o.nop; ++s)
+            if (o.pqr[3 * s] == pp && o.pqr[3 * s + 1] == q && o.pqr[3 * s + 2] == r) return s;
+        return -1;
+    };
+    CachedAsmArgs a;
+    a.n = c->g.n;
+    a.dim = dim;
+    a.nop = o.nop;
+    a.ncache = ncache;
+    a.nbcache = nbcache;
+    a.sl[0] = slot(2, 0, 0);
+    a.sl[1] = slot(1, 1, 0);
+    a.sl[2] = slot(0, 2, 0);
+    if (dim == 3) {
+        a.sl[3] = slot(1, 0, 1);
+        a.sl[4] = slot(0, 1, 1);
+        a.sl[5] = slot(0, 0, 2);
+    }
+    a.C11 = p->C11;
+    a.C12 = p->C12;
+    a.C66 = p->C66;
+    a.rho = p->rho;
+    a.dt = p->dt;
+    for (int d = 0; d < 3; ++d) a.b[d] = p->b[d];
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.pos = c->g.pos.p;
+    a.ops = o.ops.as<double>();
+    a.degenerate = o.degenerate.as<uint8_t>();
+    a.nodecache = nodecache_d;
+    a.bondcache = bondcache_d;
+    a.rowptr = k.rowptr.as<int>();
+    a.slot = k.slot.as<int>();
+    a.diag = k.diag.as<int>();
+    a.u = u_d;
+    a.uold = uold_d;
+    a.kvals = kvals_d;
+    a.rhs = rhs_d;
+    PXB_CUDA_TRY(launch_assemble_cached(a, c->stream));
+    return check_launch(c, "assemble_cached");
+}
+
+extern "C" int pxb_assemble_cached(pxb_ctx *c, const pxb_cached_params *p, const double *nodecache, int ncache,
+                                   const double *bondcache, int nbcache, const double *u, const double *uold,
+                                   double *kvals, double *rhs) {
+    PXB_TRY(need_geometry(c, "pxb_assemble_cached"));
+    CsrState &k = c->csr;
+    const int dim = c->g.dim;
+    if (!k.ready || k.ndof != dim) return fail(PXB_ERR_STATE, "pxb_assemble_cached: set a pattern with ndof = dim first");
+    if (!u || !kvals || !rhs || (nodecache && ncache < dim) || (bondcache && nbcache < 1))
+        return fail(PXB_ERR_INVALID, "pxb_assemble_cached: bad arguments");
+    const size_t n = (size_t)c->g.n, nb = (size_t)c->g.nb;
+    const size_t nn = nodecache ? n * (size_t)ncache : 0, nbb = bondcache ? nb * (size_t)nbcache : 0;
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, sizeof(double) * (nn + nbb + 1), &tmp));
+    double *dn = static_cast<double *>(tmp), *db = dn + nn;
+    if (nodecache) PXB_TRY(h2d(c, dn, nodecache, sizeof(double) * nn));
+    if (bondcache) PXB_TRY(h2d(c, db, bondcache, sizeof(double) * nbb));
+    PXB_TRY(h2d(c, k.u.p, u, sizeof(double) * n * dim));
+    if (uold) PXB_TRY(h2d(c, k.uold.p, uold, sizeof(double) * n * dim));
+    PXB_TRY(pxb_assemble_cached_d(c, p, nodecache ? dn : nullptr, ncache, bondcache ? db : nullptr, nbcache,
+                                  k.u.as<double>(), uold ? k.uold.as<double>() : nullptr, k.kvals.as<double>(),
+                                  k.rhs.as<double>()));
+    PXB_TRY(d2h(c, kvals, k.kvals.p, sizeof(double) * (size_t)k.nnz));
+    PXB_TRY(d2h(c, rhs, k.rhs.p, sizeof(double) * n * dim));
+    return sync(c);
+}
+
 extern "C" int pxb_assemble_ch(pxb_ctx *c, double kappa, double chi, double dt, const double *mnode,
                                const double *u, const double *uold, double *kvals, double *rhs) {
     PXB_TRY(need_geometry(c, "pxb_assemble_ch"));

@@ -14,7 +14,7 @@ namespace {
 
 struct ShimState {
     pxb_ctx *ctx = nullptr;
-    // which structure is resident (0 none, 1 scalar assembly, 2 explicit fracture, 3 Cahn-Hilliard, 4 stress CH)
+    // which structure is resident (0 none, 1 scalar assembly, 2 explicit fracture, 3 Cahn-Hilliard, 4 stress CH, 5 dynamic fracture)
     int kind = 0;
     int n = 0, nnz = 0, nbtot = 0, nop = 0, ndof = 0, dim = 0;
     int precision = PXB_FP64;
@@ -176,10 +176,41 @@ bool assembleStressCahnHilliard(const AssembleMesh &m, const StressCahnHilliardP
     return true;
 }
 
-bool assembleCached(const AssembleMesh &, const CachedParams &, const OpSlots &, const double *, const double *,
-                    const double *, const double *, double *, double *) {
-    std::fprintf(stderr, "[perix_b200] assembleCached is not implemented by this backend\n");
-    return false;
+bool assembleCached(const AssembleMesh &m, const CachedParams &p, const OpSlots &s, const double *nodecache,
+                    const double *bondcache, const double *u, const double *uold, double *out_Kvals,
+                    double *out_rhs) {
+    (void)s;  // the operator slots are resolved from the multi-index table, which must be the reference's
+    if (m.N <= 0 || (p.dim != 2 && p.dim != 3) || p.ndof != p.dim || !(p.dt > 0.0)) return false;
+    if (m.nodeHorizon) {
+        std::fprintf(stderr, "[perix_b200] assembleCached: variable horizon is not supported\n");
+        return false;
+    }
+    if (!ensure_ctx()) return false;
+    if (order_of(m) != 2 || !qtable_matches(m, 2)) {
+        std::fprintf(stderr, "[perix_b200] assembleCached: needs the order-2 multi-index table\n");
+        return false;
+    }
+    const int nbtot = m.neigh_off[m.N];
+    if (g_shim.kind != 5 || g_shim.n != m.N || g_shim.nnz != m.nnz || g_shim.nbtot != nbtot || g_shim.dim != p.dim) {
+        if (!upload_mesh(m, 2)) return false;
+        int ndeg = 0, first = 0;
+        const int st = pxb_gbuild(g_shim.ctx, 2, PXB_FP64, &ndeg, &first);
+        if (st == PXB_ERR_DEGENERATE)
+            std::fprintf(stderr, "[perix_b200] assembleCached: %s (rows of those nodes are zeroed)\n", pxb_last_error());
+        else if (st != PXB_OK)
+            return report("gbuild");
+        if (pxb_csr_set_pattern(g_shim.ctx, p.ndof, m.csr_off, m.csr_col, m.nnz) != PXB_OK) return report("csr pattern");
+        g_shim.kind = 5;
+        g_shim.n = m.N;
+        g_shim.nnz = m.nnz;
+        g_shim.nbtot = nbtot;
+        g_shim.dim = p.dim;
+    }
+    const pxb_cached_params q{p.C11, p.C12, p.C66, p.rho, p.dt, {p.bx, p.by, p.bz}};
+    if (pxb_assemble_cached(g_shim.ctx, &q, nodecache, p.ncache, bondcache, p.nbcache, u, uold, out_Kvals, out_rhs) !=
+        PXB_OK)
+        return report("assembleCached");
+    return true;
 }
 
 bool assembleExplicitPDDOFracAccel(const AssembleMesh &m, const ExplicitPDDOFracParams &p, const OpSlots &s,

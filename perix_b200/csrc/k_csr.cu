@@ -302,6 +302,136 @@ cudaError_t launch_assemble_stress_ch(const StressChAsmArgs &a, cudaStream_t s) 
     return cudaGetLastError();
 }
 
+// ---- implicit PDDO dynamic fracture (reference src/PDSystem/CudaAssembleKernels.cu:880-1024, physics of
+//      PDDODynamicFracElement.cpp:207-306): backward-Euler inertia R = b - rho (u - u_old - v dt)/dt^2 per node,
+//      Navier bond blocks P scaled by the frozen bond health (a broken bond contributes nothing; its slots are
+//      written as zero), zero-length bonds skipped.  K_IJ stored per bond, the diagonal block accumulates
+//      rho/dt^2 plus the sum of K_IJ. -----------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(256) assemble_cached_kernel(CachedAsmArgs a) {
+    constexpr int WPB = 256 / kWarp;
+    constexpr int NP = DIM == 3 ? 6 : 3;  // 2D p11 pxy p22; 3D p11 p22 p33 p12 p13 p23
+    using PosT = typename Vec<DIM>::T;
+    const PosT *pos = static_cast<const PosT *>(a.pos);
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
+        const int rb = i * DIM;
+        for (int s = a.rowptr[rb] + lane; s < a.rowptr[rb + DIM]; s += kWarp) a.kvals[s] = 0.0;
+        __syncwarp();
+        if (a.degenerate && a.degenerate[i]) {  // singular moment system: the rows stay zero
+            if (lane < DIM) a.rhs[rb + lane] = 0.0;
+            continue;
+        }
+        double uI[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) uI[d] = a.u[rb + d];
+        const PosT xi = pos[i];
+        double R[DIM], S[NP];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) R[d] = 0.0;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) S[q] = 0.0;
+        for (int t = a.off[i] + lane; t < a.off[i + 1]; t += kWarp) {
+            const int j = __ldg(a.nbr + t);
+            const PosT xj = pos[j];
+            double r2 = (xj.x - xi.x) * (xj.x - xi.x) + (xj.y - xi.y) * (xj.y - xi.y);
+            if constexpr (DIM == 3) r2 += (xj.z - xi.z) * (xj.z - xi.z);
+            if (!(r2 > 0.0)) continue;
+            const double h = a.bondcache ? a.bondcache[(size_t)t * a.nbcache] : 1.0;
+            double P[NP];
+            if (h > 0.0) {
+                const double *op = a.ops + (size_t)t * a.nop;
+                const double Gxx = op[a.sl[0]], Gxy = op[a.sl[1]], Gyy = op[a.sl[2]];
+                if constexpr (DIM == 2) {
+                    P[0] = h * (a.C11 * Gxx + a.C66 * Gyy);
+                    P[1] = h * (a.C12 + a.C66) * Gxy;
+                    P[2] = h * (a.C66 * Gxx + a.C11 * Gyy);
+                } else {
+                    const double Gxz = op[a.sl[3]], Gyz = op[a.sl[4]], Gzz = op[a.sl[5]];
+                    const double cc = a.C12 + a.C66;
+                    P[0] = h * (a.C11 * Gxx + a.C66 * (Gyy + Gzz));
+                    P[1] = h * (a.C11 * Gyy + a.C66 * (Gxx + Gzz));
+                    P[2] = h * (a.C11 * Gzz + a.C66 * (Gxx + Gyy));
+                    P[3] = h * cc * Gxy;
+                    P[4] = h * cc * Gxz;
+                    P[5] = h * cc * Gyz;
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < NP; ++q) P[q] = 0.0;
+            }
+            double Kb[DIM][DIM];
+            if constexpr (DIM == 2) {
+                Kb[0][0] = P[0];
+                Kb[0][1] = Kb[1][0] = P[1];
+                Kb[1][1] = P[2];
+            } else {
+                Kb[0][0] = P[0];
+                Kb[1][1] = P[1];
+                Kb[2][2] = P[2];
+                Kb[0][1] = Kb[1][0] = P[3];
+                Kb[0][2] = Kb[2][0] = P[4];
+                Kb[1][2] = Kb[2][1] = P[5];
+            }
+            double du[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) du[d] = a.u[(size_t)j * DIM + d] - uI[d];
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) {
+                double rr = 0.0;
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) rr += Kb[r][c] * du[c];
+                R[r] += rr;
+            }
+#pragma unroll
+            for (int q = 0; q < NP; ++q) S[q] += P[q];
+            const int *st = a.slot + (size_t)t * DIM * DIM;
+#pragma unroll
+            for (int r = 0; r < DIM; ++r)
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) a.kvals[st[r * DIM + c]] = -Kb[r][c];
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) R[d] = group_sum<kWarp>(R[d]);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) S[q] = group_sum<kWarp>(S[q]);
+        if (lane == 0) {
+            const double c0 = a.rho / (a.dt * a.dt);
+            double kii[DIM][DIM];
+            if constexpr (DIM == 2) {
+                kii[0][0] = S[0];
+                kii[0][1] = kii[1][0] = S[1];
+                kii[1][1] = S[2];
+            } else {
+                kii[0][0] = S[0];
+                kii[1][1] = S[1];
+                kii[2][2] = S[2];
+                kii[0][1] = kii[1][0] = S[3];
+                kii[0][2] = kii[2][0] = S[4];
+                kii[1][2] = kii[2][1] = S[5];
+            }
+            const int *dg = a.diag + (size_t)i * DIM * DIM;
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) {
+                const double uo = a.uold ? a.uold[rb + r] : 0.0;
+                const double v = a.nodecache ? a.nodecache[(size_t)i * a.ncache + r] : 0.0;
+                kii[r][r] += c0;
+                a.rhs[rb + r] = (a.b[r] - c0 * (uI[r] - uo - v * a.dt)) + R[r];
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) a.kvals[dg[r * DIM + c]] = kii[r][c];
+            }
+        }
+    }
+}
+
+cudaError_t launch_assemble_cached(const CachedAsmArgs &a, cudaStream_t s) {
+    const int g = (a.n + 7) / 8;
+    if (a.dim == 3) assemble_cached_kernel<3><<<g > 0 ? g : 1, 256, 0, s>>>(a);
+    else assemble_cached_kernel<2><<<g > 0 ? g : 1, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 // ---- conservative Cahn-Hilliard (2 dof: c, mu) ------------------------------------------------------------
 __global__ void __launch_bounds__(256) assemble_ch_kernel(ChAsmArgs a) {
     constexpr int WPB = 256 / kWarp;

@@ -292,6 +292,23 @@ struct StressChAsmArgs {
     double *kvals = nullptr, *rhs = nullptr;
 };
 cudaError_t launch_assemble_stress_ch(const StressChAsmArgs &a, cudaStream_t s);
+// Implicit PDDO dynamic fracture (rows u per node; ndof = dim): the device twin of the reference's
+// cachedAssembleKernel (src/PDSystem/CudaAssembleKernels.cu:880-1024) on the FP64 order-2 operator cache.
+// nodecache[i*ncache + a] = committed velocity, bondcache[t*nbcache] = frozen bond health.
+struct CachedAsmArgs {
+    int n = 0, dim = 2, nop = 0, ncache = 3, nbcache = 1;
+    int sl[6] = {-1, -1, -1, -1, -1, -1};  // d2/dx2 d2/dxdy d2/dy2 d2/dxdz d2/dydz d2/dz2
+    double C11 = 0, C12 = 0, C66 = 0, rho = 0, dt = 1, b[3] = {0, 0, 0};
+    const int *off = nullptr, *nbr = nullptr;
+    const void *pos = nullptr;          // double2 / double4
+    const double *ops = nullptr;        // FP64 [nb][nop]
+    const uint8_t *degenerate = nullptr;
+    const double *nodecache = nullptr, *bondcache = nullptr;
+    const int *rowptr = nullptr, *slot = nullptr, *diag = nullptr;
+    const double *u = nullptr, *uold = nullptr;
+    double *kvals = nullptr, *rhs = nullptr;
+};
+cudaError_t launch_assemble_cached(const CachedAsmArgs &a, cudaStream_t s);
 // CH one-off geometry from the order-2 operator cache (CahnHilliardElement.cpp:93-152): per bond the PDDO
 // Laplacian g_xx + g_yy (+ g_zz), lambda-corrected on non-ghost bonds with lambda = 2 dim / sum_j g2_ij
 // (|x_j|^2 - |x_i|^2); ghost flags from the mirror map.  slots: the operator slots of d2/dx2, d2/dy2, d2/dz2.

@@ -97,6 +97,32 @@ def stress_ch_fixture(dim):
          params=np.array([E, nu, Omega, cref, D, chi, kappa, dt]), kvals=kv, rhs=rhs, **geo)
 
 
+def dynfrac_fixture(dim):
+    """Implicit PDDO dynamic fracture (ndof = dim) through the reference's PDDODynamicFracElement: 2D 20x20 on
+    [0,0.2]^2, 3D 5x5x4 on [0,0.5]x[0,0.5]x[0,0.4], delta = 3.015h, plane strain, E = 190e9, nu = 0.3,
+    rho = 8000, G0 = 2e4, dt = 1e-7, body force (1e3, -2e3, 5e2); uprev = 0, uold = a smooth stretch plus
+    noise (amplitude 1.5e-3 in 2D, 5e-4 in 3D; noise 5e-5 h) that breaks part of the bonds at the commit,
+    u = uold plus noise (seeded)."""
+    if dim == 2:
+        m = RefMesh.structured(2, 20, 20, 0, [0, 0.2, 0, 0.2], 3.015, 2)
+        h = 0.01
+    else:
+        m = RefMesh.structured(3, 5, 5, 4, [0, 0.5, 0, 0.5, 0, 0.4], 3.015, 2)
+        h = 0.1
+    rp, cols = m.csr_pattern(dim)
+    rng = np.random.default_rng(41 + dim)
+    E, nu, rho, G0, dt = 190e9, 0.3, 8000.0, 2e4, 1e-7
+    b = (1e3, -2e3, 5e2)
+    x = m.coords.reshape(-1, 3)[:, :dim]
+    uprev = np.zeros(m.n * dim)
+    amp = 1.5e-3 if dim == 2 else 5e-4
+    uold = (amp * x * x / x.max() + rng.standard_normal(x.shape) * 5e-5 * h).reshape(-1)
+    u = uold + rng.standard_normal(m.n * dim) * 1e-4 * h
+    kv, rhs, vel, health, consts = m.dynfrac_assemble(E, nu, rho, G0, dt, uprev, uold, u, b=b)
+    save("dynfrac%dd" % dim, **mesh_arrays(m), rowptr=rp, cols=cols, uprev=uprev, uold=uold, u=u,
+         params=np.array([E, nu, rho, G0, dt] + list(b)), kvals=kv, rhs=rhs, vel=vel, health=health, consts=consts)
+
+
 def lattice3d_fixture():
     m = RefMesh.structured(3, 5, 5, 4, [0, 0.5, 0, 0.5, 0, 0.4], 3.015, 2)
     ops, deg = m.gbuild()
@@ -229,3 +255,5 @@ if __name__ == "__main__":
     ch_fixture()
     stress_ch_fixture(2)
     stress_ch_fixture(3)
+    dynfrac_fixture(2)
+    dynfrac_fixture(3)
