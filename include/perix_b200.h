@@ -147,6 +147,16 @@ int pxb_epf_setup(pxb_ctx *ctx, int precision, double C11, double C12, double C6
 /* One rate evaluation at u (N*dim): damage then force, a = (L+b)/rho (the reference CUDA entry
  * assembleExplicitPDDOFracAccel).  *n_broken = bonds that broke in this call. */
 int pxb_epf_rate(pxb_ctx *ctx, const double *u, double *accel, long long *n_broken);
+/* Output projections of the explicit state, the device twin of ExplicitPDDOFracElement::computeNodalProjection
+ * (src/ElmtSystem/ExplicitPDDOFracElement.cpp:324-405): per node damage = 1 - intact/all bonds, von Mises stress,
+ * Cauchy stress and small strain (3x3 row-major, 9 values per node) from the PDDO displacement gradient over the
+ * whole family, with lambda = C12 and mu = C66; 2D sigma_zz = lambda tr(eps) when plane_strain, else 0.  u (NULL:
+ * the current state u^n) and the current bond health.  Outputs may be NULL.  The first call builds the FP64
+ * order-2 operator cache of the context if it is absent. */
+int pxb_epf_project_d(pxb_ctx *ctx, const double *u_d, int plane_strain, double *damage_d, double *von_mises_d,
+                      double *stress_d, double *strain_d);
+int pxb_epf_project(pxb_ctx *ctx, const double *u, int plane_strain, double *damage, double *von_mises,
+                    double *stress, double *strain);
 
 /* Boundary-condition program applied after every central-difference update, in list order (reference
  * BCSystem::presetSolution, src/BCSystem/BCSystem.cpp:114-129).  Entry e: kind 0 Dirichlet (reflect across

@@ -507,6 +507,14 @@ class RefEpf:
                                 _ptr(h, C.c_double), int(nthreads or os.cpu_count()))
         return acc, h, t
 
+    def project(self, which, u):
+        """computeNodalProjection at u for every node: "damage", "vonMises" (n values), "stress", "strain"
+        (n x 9, row-major 3x3)."""
+        k = {"damage": 0, "vonMises": 1, "stress": 2, "strain": 3}[which]
+        out = np.zeros(self.mesh.n * (1 if k < 2 else 9), np.float64)
+        self.L.ref_epf_project(self.h, k, _ptr(np.ascontiguousarray(u, np.float64), C.c_double), _ptr(out, C.c_double))
+        return out if k < 2 else out.reshape(-1, 9)
+
     def set_health(self, h):
         self.L.ref_epf_set_health(self.h, _ptr(np.ascontiguousarray(h, np.float64), C.c_double))
 

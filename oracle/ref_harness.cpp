@@ -628,6 +628,24 @@ void ref_epf_set_health(void *h, const double *health) {
     std::memcpy(e->el.m_HealthFlat.data(), health, sizeof(double) * e->el.m_HealthFlat.size());
 }
 
+// ExplicitPDDOFracElement::computeNodalProjection (ExplicitPDDOFracElement.cpp:324-405) for every node at u, on
+// the element's current op cache and health: which 0 damage (1 value), 1 vonMises (1), 2 stress (9), 3 strain (9).
+void ref_epf_project(void *h, int which, const double *u, double *out) {
+    auto *e = static_cast<RefEpf *>(h);
+    auto *m = e->mesh;
+    const int n = m->pd.getNodesNum();
+    const int dim = m->dim;
+    static const char *names[4] = {"damage", "vonMises", "stress", "strain"};
+    const int k = which < 2 ? 1 : 9;
+    VectorXd U(n * dim);
+    std::memcpy(U.getDataPtr(), u, sizeof(double) * (size_t)n * dim);
+    std::vector<double> o((size_t)k);
+    for (int i = 1; i <= n; ++i) {
+        e->el.computeNodalProjection(names[which], m->pd, m->ops, U, i, dim, o);
+        std::memcpy(out + (size_t)(i - 1) * k, o.data(), sizeof(double) * (size_t)k);
+    }
+}
+
 // [sc, C11, C12, C66, stable_dt]
 void ref_epf_constants(void *h, double *out) {
     auto *e = static_cast<RefEpf *>(h);

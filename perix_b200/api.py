@@ -625,6 +625,16 @@ class Context:
         _check(self.L.pxb_assemble_stress_ch_d(self.h, C.byref(p), _p(mnode_ptr), _p(health_ptr), _p(vel_ptr),
                                                _p(u_ptr), _p(uold_ptr), _p(kvals_ptr), _p(rhs_ptr)))
 
+    def epf_project(self, u=None, plane_strain=True):
+        """Damage, von Mises, stress and strain (3x3 per node) of u (None: the current state) with the current
+        bond health (pxb_epf_project)."""
+        n = self.n
+        dmg, vm = np.zeros(n), np.zeros(n)
+        st, ep = np.zeros(9 * n), np.zeros(9 * n)
+        _check(self.L.pxb_epf_project(self.h, _p(None if u is None else _f64(u)), int(bool(plane_strain)), _p(dmg),
+                                      _p(vm), _p(st), _p(ep)))
+        return dict(damage=dmg, vonMises=vm, stress=st.reshape(n, 9), strain=ep.reshape(n, 9))
+
     def assemble_cached(self, params, u, uold=None, nodecache=None, ncache=3, bondcache=None, nbcache=1):
         """Implicit PDDO dynamic fracture (ndof = dim) K and rhs; params: dict with C11 C12 C66 rho dt and b
         (3 values); nodecache [n*ncache] committed velocity, bondcache [nb*nbcache] frozen bond health."""

@@ -676,6 +676,71 @@ extern "C" int pxb_epf_rate(pxb_ctx *c, const double *u, double *accel, long lon
     return PXB_OK;
 }
 
+// Output projections (ExplicitPDDOFracElement::computeNodalProjection, ExplicitPDDOFracElement.cpp:324-405) of u_d
+// (NULL: the current state u^n) with the current bond health.  The first-derivative operators come from the
+// context's FP64 order-2 operator cache, built here when absent (the step itself keeps only the Navier streams).
+// the FP64 order-2 operator cache the projections read (built once; it uses the context scratch buffer, so it
+// runs before anything is staged there)
+static int ensure_fp64_ops(pxb_ctx *c) {
+    const OpsCache &o = c->ops;
+    if (o.ready && o.order == 2 && o.precision == PXB_FP64) return PXB_OK;
+    int nd = 0, first = 0;
+    const int st = pxb_gbuild(c, 2, PXB_FP64, &nd, &first);
+    return st == PXB_ERR_DEGENERATE ? PXB_OK : st;  // degenerate rows carry zero operators
+}
+
+extern "C" int pxb_epf_project_d(pxb_ctx *c, const double *u_d, int plane_strain, double *damage_d,
+                                 double *von_mises_d, double *stress_d, double *strain_d) {
+    PXB_TRY(need_epf(c, "pxb_epf_project"));
+    PXB_TRY(ensure_fp64_ops(c));
+    const OpsCache &o = c->ops;
+    const EpfState &e = c->epf;
+    auto slot = [&](int pp, int q, int r) {
+        for (int s = 0; s < o.nop; ++s)
+            if (o.pqr[3 * s] == pp && o.pqr[3 * s + 1] == q && o.pqr[3 * s + 2] == r) return s;
+        return -1;
+    };
+    ProjectArgs a;
+    a.n = c->g.n;
+    a.dim = c->g.dim;
+    a.nop = o.nop;
+    a.plane_strain = plane_strain ? 1 : 0;
+    a.sl[0] = slot(1, 0, 0);
+    a.sl[1] = slot(0, 1, 0);
+    a.sl[2] = c->g.dim == 3 ? slot(0, 0, 1) : -1;
+    a.C12 = e.C12;
+    a.C66 = e.C66;
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.ops = o.ops.as<double>();
+    a.health = e.health.as<uint8_t>();
+    a.u = u_d ? u_d : e.u[e.cur].as<double>();
+    a.damage = damage_d;
+    a.von_mises = von_mises_d;
+    a.stress = stress_d;
+    a.strain = strain_d;
+    PXB_CUDA_TRY(launch_epf_project(a, c->stream));
+    return check_launch(c, "epf project");
+}
+
+extern "C" int pxb_epf_project(pxb_ctx *c, const double *u, int plane_strain, double *damage, double *von_mises,
+                               double *stress, double *strain) {
+    PXB_TRY(need_epf(c, "pxb_epf_project"));
+    PXB_TRY(ensure_fp64_ops(c));
+    const size_t n = (size_t)c->g.n, nd = n * c->g.dim;
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, sizeof(double) * (nd + 20 * n), &tmp));
+    double *du = static_cast<double *>(tmp), *dd = du + nd, *dv = dd + n, *ds = dv + n, *de = ds + 9 * n;
+    if (u) PXB_TRY(h2d(c, du, u, sizeof(double) * nd));
+    PXB_TRY(pxb_epf_project_d(c, u ? du : nullptr, plane_strain, damage ? dd : nullptr, von_mises ? dv : nullptr,
+                              stress ? ds : nullptr, strain ? de : nullptr));
+    if (damage) PXB_TRY(d2h(c, damage, dd, sizeof(double) * n));
+    if (von_mises) PXB_TRY(d2h(c, von_mises, dv, sizeof(double) * n));
+    if (stress) PXB_TRY(d2h(c, stress, ds, sizeof(double) * 9 * n));
+    if (strain) PXB_TRY(d2h(c, strain, de, sizeof(double) * 9 * n));
+    return sync(c);
+}
+
 // ---- BC program: the reference applies BCs one after another (BCSystem.cpp:114-129); each write either
 //      copies/reflects a mirror value or pins g(t).  Symbolic replay on the host reduces every constrained
 //      (node, component) to one of four closed forms in terms of pre-BC values, executed on the device by the

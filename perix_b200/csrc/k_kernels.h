@@ -309,6 +309,19 @@ struct CachedAsmArgs {
     double *kvals = nullptr, *rhs = nullptr;
 };
 cudaError_t launch_assemble_cached(const CachedAsmArgs &a, cudaStream_t s);
+// Output projections of the explicit state (k_project.cu; ExplicitPDDOFracElement.cpp:324-405).  Outputs may be
+// NULL; stress and strain are 3x3 row-major per node.  sl = operator slots of d/dx, d/dy, d/dz.
+struct ProjectArgs {
+    int n = 0, dim = 2, nop = 0, plane_strain = 1;
+    int sl[3] = {-1, -1, -1};
+    double C12 = 0, C66 = 0;
+    const int *off = nullptr, *nbr = nullptr;
+    const double *ops = nullptr;      // FP64 [nb][nop]
+    const uint8_t *health = nullptr;  // [nb]
+    const double *u = nullptr;        // [n*dim]
+    double *damage = nullptr, *von_mises = nullptr, *stress = nullptr, *strain = nullptr;
+};
+cudaError_t launch_epf_project(const ProjectArgs &a, cudaStream_t s);
 // CH one-off geometry from the order-2 operator cache (CahnHilliardElement.cpp:93-152): per bond the PDDO
 // Laplacian g_xx + g_yy (+ g_zz), lambda-corrected on non-ghost bonds with lambda = 2 dim / sum_j g2_ij
 // (|x_j|^2 - |x_i|^2); ghost flags from the mirror map.  slots: the operator slots of d2/dx2, d2/dy2, d2/dz2.
