@@ -185,7 +185,7 @@ def c1_poisson(px, kvals, rhs, L, rowptr, cols):
 
 
 def c1_measure(px, device=0, reps=20):
-    """64x64 cell-centred lattice on the unit square, delta = 3.015h, order 2, sigma = 1,
+    """The 64x64 Poisson workload: 64x64 cell-centred lattice on the unit square, delta = 3.015h, order 2, sigma = 1,
     f = 2 pi^2 sin(pi x) sin(pi y), reflected Dirichlet 0 on the four ghost groups.  FP64 g-build and Poisson
     assembly on the GPU (CUDA events), one host solve, L2 error; the reference's OpenMP assembly of the same
     system through oracle/_ref is timed beside it when present."""

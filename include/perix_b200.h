@@ -289,6 +289,39 @@ int pxb_assemble_ch_d(pxb_ctx *ctx, double kappa, double chi, double dt, const d
 int pxb_assemble_ch(pxb_ctx *ctx, double kappa, double chi, double dt, const double *mnode, const double *u,
                     const double *uold, double *kvals, double *rhs);
 
+/* Implicit Cahn-Hilliard run on the device (spinodal decomposition end to end) and its adjoint.  Backward Euler with the
+ * reference's transient CH solve per step: Newton on the conservative element's residual with the mobility
+ * M0 c (1 - c) frozen per iteration at the current iterate (CahnHilliardElement.cpp:66-292), zero-Neumann ghost
+ * rows as NeumannBC::apply (NeumannBC.cpp:127-150), each linear system solved on the device (BiCGStab, 2x2
+ * block-Jacobi).  Needs a 2D geometry (mirror ghosts for the Neumann walls), an FP64 order-2 g-build, the CH
+ * geometry (pxb_ch_build_geometry) and a 2-dof pattern holding the mirror columns.  c0[n]: initial c (ghost entries
+ * are replaced by their mirror bulk values), mu0 = 0.  E = total free energy of the final state, the sum over bulk
+ * nodes of V_i (f(c_i) + kappa/2 |grad c_i|^2), f(c) = c ln c + (1 - c) ln(1 - c) + chi c (1 - c), grad c the PDDO
+ * first derivatives.  pxb_ch_gradient also returns dE/dkappa and dE/dc0 (bulk entries; ghost entries 0) by the
+ * discrete adjoint of the converged steps (the mobility derivative the Picard Jacobian omits included); it keeps
+ * every step's state on the device (2 n (nsteps + 1) doubles).  No counterpart in the reference (it has no GPU
+ * solver and no gradient). */
+typedef struct pxb_ch_run_params {
+    double chi, kappa, M0, dt;
+    int nsteps;
+    double newton_rtol; /* stop when |F| <= newton_rtol |F| of the step's initial guess */
+    int newton_max;
+    double lin_rtol; /* BiCGStab relative residual */
+    int lin_max;
+} pxb_ch_run_params;
+typedef struct pxb_ch_run_stats {
+    int steps, newton_iters, lin_iters;
+    double max_residual;   /* largest final relative Newton residual */
+    double max_lin_relres; /* largest final BiCGStab relative residual */
+    double energy;
+} pxb_ch_run_stats;
+int pxb_ch_run(pxb_ctx *ctx, const pxb_ch_run_params *p, const double *c0, double *u_final, double *E,
+               pxb_ch_run_stats *stats);
+int pxb_ch_gradient(pxb_ctx *ctx, const pxb_ch_run_params *p, const double *c0, double *E, double *dE_dkappa,
+                    double *dE_dc0, pxb_ch_run_stats *stats);
+/* E of u (2n, rows c, mu) and dE/du (may be NULL) */
+int pxb_ch_energy(pxb_ctx *ctx, double kappa, double chi, const double *u, double *E, double *dE_du);
+
 /* Stress-coupled (optionally fracturing) Cahn-Hilliard assembly, the boundary of the reference's
  * perix_cuda::assembleStressCahnHilliard (include/PDSystem/CudaAssemble.h:185-191; kernel
  * src/PDSystem/CudaAssembleKernels.cu:685-874).  Rows per node: c, mu, u_x, u_y[, u_z] (ndof = dim + 2).

@@ -271,7 +271,7 @@ void ref_csr_pattern(void *h, int ndof, int *rowptr, int *cols) {
 
 // ---- Poisson residual/Jacobian (K=-dF/dU, RHS=+F) with a per-node source f_i --------------------------------
 // The bond term is the reference PoissonElement callback; the nodal term is f_i (the reference element only
-// takes a constant f; a per-node source is what BASELINE's manufactured solution needs).  Accumulation order
+// takes a constant f; a per-node source is what the manufactured Poisson solution needs).  Accumulation order
 // and signs follow FormResidualAndJacobianParallel.cpp:114-171.
 double ref_poisson_assemble(void *h, double sigma, const double *fnode, const double *u, double *kvals,
                             double *rhs, int nthreads) {

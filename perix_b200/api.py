@@ -254,6 +254,19 @@ class StressChParams(C.Structure):
     DEFAULTS = {"dt": 1.0, "kres": 1e-8}
 
 
+class ChRunParams(C.Structure):
+    """pxb_ch_run_params (include/perix_b200.h)."""
+    _fields_ = [("chi", C.c_double), ("kappa", C.c_double), ("M0", C.c_double), ("dt", C.c_double),
+                ("nsteps", C.c_int), ("newton_rtol", C.c_double), ("newton_max", C.c_int), ("lin_rtol", C.c_double),
+                ("lin_max", C.c_int)]
+
+
+class ChRunStats(C.Structure):
+    """pxb_ch_run_stats (include/perix_b200.h)."""
+    _fields_ = [("steps", C.c_int), ("newton_iters", C.c_int), ("lin_iters", C.c_int), ("max_residual", C.c_double),
+                ("max_lin_relres", C.c_double), ("energy", C.c_double)]
+
+
 class CachedParams(C.Structure):
     """pxb_cached_params (include/perix_b200.h)."""
     _fields_ = [("C11", C.c_double), ("C12", C.c_double), ("C66", C.c_double), ("rho", C.c_double),
@@ -624,6 +637,37 @@ class Context:
                               for k, _ in StressChParams._fields_})
         _check(self.L.pxb_assemble_stress_ch_d(self.h, C.byref(p), _p(mnode_ptr), _p(health_ptr), _p(vel_ptr),
                                                _p(u_ptr), _p(uold_ptr), _p(kvals_ptr), _p(rhs_ptr)))
+
+    def _ch_params(self, chi, kappa, M0, dt, nsteps, newton_rtol, newton_max, lin_rtol, lin_max):
+        return ChRunParams(chi=float(chi), kappa=float(kappa), M0=float(M0), dt=float(dt), nsteps=int(nsteps),
+                           newton_rtol=float(newton_rtol), newton_max=int(newton_max), lin_rtol=float(lin_rtol),
+                           lin_max=int(lin_max))
+
+    def ch_run(self, c0, chi, kappa, M0, dt, nsteps, newton_rtol=1e-13, newton_max=40, lin_rtol=1e-12,
+               lin_max=2000):
+        """Backward-Euler Cahn-Hilliard run on the device (pxb_ch_run): returns (u_final [2n], E, stats dict)."""
+        p = self._ch_params(chi, kappa, M0, dt, nsteps, newton_rtol, newton_max, lin_rtol, lin_max)
+        u = np.zeros(2 * self.n, np.float64)
+        E = C.c_double(0.0)
+        st = ChRunStats()
+        _check(self.L.pxb_ch_run(self.h, C.byref(p), _p(_f64(c0)), _p(u), C.byref(E), C.byref(st)))
+        return u, E.value, {k: getattr(st, k) for k, _ in ChRunStats._fields_}
+
+    def ch_gradient(self, c0, chi, kappa, M0, dt, nsteps, newton_rtol=1e-13, newton_max=40, lin_rtol=1e-12,
+                    lin_max=2000):
+        """(E, dE/dkappa, dE/dc0 [n], stats) by the discrete adjoint of the run (pxb_ch_gradient)."""
+        p = self._ch_params(chi, kappa, M0, dt, nsteps, newton_rtol, newton_max, lin_rtol, lin_max)
+        g = np.zeros(self.n, np.float64)
+        E, dk = C.c_double(0.0), C.c_double(0.0)
+        st = ChRunStats()
+        _check(self.L.pxb_ch_gradient(self.h, C.byref(p), _p(_f64(c0)), C.byref(E), C.byref(dk), _p(g), C.byref(st)))
+        return E.value, dk.value, g, {k: getattr(st, k) for k, _ in ChRunStats._fields_}
+
+    def ch_energy(self, kappa, chi, u):
+        E = C.c_double(0.0)
+        g = np.zeros(2 * self.n, np.float64)
+        _check(self.L.pxb_ch_energy(self.h, C.c_double(kappa), C.c_double(chi), _p(_f64(u)), C.byref(E), _p(g)))
+        return E.value, g
 
     def epf_project(self, u=None, plane_strain=True):
         """Damage, von Mises, stress and strain (3x3 per node) of u (None: the current state) with the current

@@ -322,6 +322,40 @@ struct ProjectArgs {
     double *damage = nullptr, *von_mises = nullptr, *stress = nullptr, *strain = nullptr;
 };
 cudaError_t launch_epf_project(const ProjectArgs &a, cudaStream_t s);
+// ---- device linear algebra and Cahn-Hilliard Newton / adjoint pieces (k_linalg.cu) ----
+cudaError_t launch_spmv(int rows, const int *rowptr, const int *cols, const double *val, const double *x, double *y,
+                        bool transpose, cudaStream_t s);
+int dot_scratch_doubles();
+// *out = a . b over n entries (fixed-order reduction; scratch: dot_scratch_doubles() doubles)
+cudaError_t launch_dot(long long n, const double *a, const double *b, double *scratch, double *out, cudaStream_t s);
+cudaError_t launch_axpby(long long n, double alpha, const double *x, double beta, double *y, cudaStream_t s);
+cudaError_t launch_bicg_p(long long n, const double *r, double beta, double omega, const double *v, double *p,
+                          cudaStream_t s);
+cudaError_t launch_block_inv(int n, const int *diag, const double *val, bool transpose, double *binv, cudaStream_t s);
+cudaError_t launch_block_apply(int n, const double *binv, const double *x, double *y, cudaStream_t s);
+cudaError_t launch_ch_ghost_rows(int n, const int *mirror, const int *rowptr, const int *cols, const double *u,
+                                 double *kv, double *rhs, cudaStream_t s);
+struct ChAdjArgs {
+    int n = 0;
+    double M0 = 1.0;
+    const int *off = nullptr, *nbr = nullptr, *rev = nullptr, *mirror = nullptr;
+    const char *ghost = nullptr;
+    const double *lap = nullptr, *vol = nullptr, *u = nullptr, *x = nullptr;
+    double *y = nullptr;
+};
+// y[c rows] -= J_M^T x (mobility derivative the Picard iteration omits); per-node lambda_mu dF_mu/dkappa
+cudaError_t launch_ch_mob_adj(const ChAdjArgs &a, cudaStream_t s);
+cudaError_t launch_ch_dkappa(const ChAdjArgs &a, cudaStream_t s);
+struct ChEnergyArgs {
+    int n = 0, nop = 0, sx = 0, sy = 1;
+    double kappa = 0, chi = 0;
+    const int *off = nullptr, *nbr = nullptr, *rev = nullptr, *mirror = nullptr;
+    const double *vol = nullptr, *ops = nullptr, *u = nullptr;
+    double *e_out = nullptr, *grad_e = nullptr, *gbar = nullptr, *fprime = nullptr;
+};
+cudaError_t launch_ch_energy(const ChEnergyArgs &a, cudaStream_t s);
+cudaError_t launch_ch_energy_grad(const ChEnergyArgs &a, double *dedu, cudaStream_t s);
+cudaError_t launch_ch_prev_cot(int n, const int *mirror, const double *lam, double dt, double *g, cudaStream_t s);
 // CH one-off geometry from the order-2 operator cache (CahnHilliardElement.cpp:93-152): per bond the PDDO
 // Laplacian g_xx + g_yy (+ g_zz), lambda-corrected on non-ghost bonds with lambda = 2 dim / sum_j g2_ij
 // (|x_j|^2 - |x_i|^2); ghost flags from the mirror map.  slots: the operator slots of d2/dx2, d2/dy2, d2/dz2.

@@ -148,6 +148,10 @@ struct CsrState {
 struct ChState {
     bool ready = false;
     DevBuf rev, lap, ghost;
+    // implicit run (ch_solver.cpp): state, Newton / BiCGStab work vectors, block-Jacobi inverse, history
+    DevBuf U, Uold, dU, rhs, kv, mnode, binv, red, ones, hist;
+    DevBuf w[8];
+    DevBuf nodal;  // per-node scratch (energy, dkappa terms)
 };
 
 }  // namespace pxb

@@ -163,7 +163,7 @@ def test_ch_device_geometry_and_mobility(ctx):
 
 
 def test_c1_solve_l2_error(ctx, port):
-    """BASELINE config 1 end to end: 64x64 lattice, order 2, FP64 g-build and Poisson assembly on the GPU, the
+    """The 64x64 Poisson problem end to end: 64x64 lattice, order 2, FP64 g-build and Poisson assembly on the GPU, the
     reference's Dirichlet row replacement on the ghost layer, one solve.  The solution matches the solve of the
     C restatement's assembly of the same system (1e-9) and the relative L2 error against sin(pi x) sin(pi y) is
     the reference's (1.44e-3 with the reference's own assembly, tests/test_oracle.py)."""
