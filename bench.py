@@ -242,6 +242,93 @@ def c1_measure(px, device=0, reps=20):
     return res
 
 
+def c4_measure(px, device=0, nside=256, nsteps=200, reps=20, fd=True):
+    """The 256x256 Cahn-Hilliard spinodal-decomposition workload: h = 1/256, delta = 3.015h, c0 = 0.5 + U(+-0.01)
+    (seeded), chi = 2.5, M0 = 1, kappa = 1e-4, backward Euler dt = 1e-6 for 200 steps, mobility frozen per Newton
+    iteration, zero Neumann on the four ghost walls.  Times the CH assembly kernel (CUDA events, L2 flushed) with
+    its HBM roofline, the whole run on the device (wall clock: the Newton and BiCGStab iterations are steered by
+    dot products read back on the host) and the adjoint gradient of the final free energy in kappa and c0, and
+    checks dE/dkappa against central differences (step 1e-6)."""
+    import ctypes as C
+
+    import torch
+    L = px.lattice(2, nside, nside, 0, [0.0, 1.0, 0.0, 1.0])
+    delta = 3.015 * L.dxyz[0] * (1.0 + 1e-6)
+    off, ids = px.families(L.coords, delta, False, mirror=L.mirror)
+    rowptr, cols = px.csr_pattern(off, ids, L.mirror, 2)
+    ctx = px.Context(device)
+    ctx.set_geometry(L.coords, L.vols, off, ids, delta, L.dxyz[0], 2, mirror=L.mirror)
+    ctx.gbuild(2, px.FP64)
+    ctx.ch_build_geometry()
+    ctx.csr_set_pattern(rowptr, cols, 2)
+    chi, kappa, M0, dt = 2.5, 1e-4, 1.0, 1e-6
+    rng = np.random.default_rng(2024)
+    c0 = 0.5 + rng.uniform(-0.01, 0.01, L.n)
+    nb, nnz = int(off[-1]), int(rowptr[-1])
+    res = {"nodes": L.n, "bonds": nb, "rows": 2 * L.n, "nnz": nnz, "steps": nsteps}
+    # the assembly kernel alone at the initial state
+    dev = torch.device("cuda", device)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    u = np.zeros(2 * L.n)
+    u[0::2] = np.where(L.mirror > 0, c0[np.maximum(L.mirror, 1) - 1], c0)
+    ud = torch.from_numpy(u).to(dev)
+    mn = torch.empty(L.n, dtype=torch.float64, device=dev)
+    ctx.ch_mobility_d(M0, ud.data_ptr(), mn.data_ptr())
+    kd = torch.empty(nnz, dtype=torch.float64, device=dev)
+    rd = torch.empty(2 * L.n, dtype=torch.float64, device=dev)
+    flush = torch.empty(FLUSH_BYTES // 8, dtype=torch.float64, device=dev)
+    ms = []
+    for r in range(reps + 3):
+        flush.fill_(float(r))
+        flush.sum()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ctx.assemble_ch_d(kappa, chi, dt, mn.data_ptr(), ud.data_ptr(), ud.data_ptr(), kd.data_ptr(), rd.data_ptr())
+        b.record()
+        torch.cuda.synchronize(dev)
+        if r >= 3:
+            ms.append(a.elapsed_time(b))
+    asm_ms = float(np.mean(ms))
+    # bytes per assembly: per bond id 4 + g2 8 + reverse index 4 + 4 slot ids 16 + 4 K values 32; per node the
+    # state (c, mu, c_old: 24), mobility 8, volume 8, rhs 16, and the zeroing of the node's two rows
+    B = nb * (4 + 8 + 4 + 16 + 32) + L.n * (24 + 8 + 8 + 16)
+    hbm, _ = peaks()
+    res["assembly_ms"] = asm_ms
+    res["assembly_algorithmic_bytes"] = B
+    res["assembly_achieved_gbs"] = B / (asm_ms * 1e-3) / 1e9
+    res["assembly_frac_of_measured_hbm"] = B / (asm_ms * 1e-3) / 1e9 / hbm
+    ctx.set_stream(None)
+    t0 = time.perf_counter()
+    _, E, st = ctx.ch_run(c0, chi, kappa, M0, dt, nsteps)
+    t_run = time.perf_counter() - t0
+    res.update(run_s=t_run, steps_per_s=nsteps / t_run, energy=E, newton_iters=st["newton_iters"],
+               bicgstab_iters=st["lin_iters"], max_bicgstab_relres=st["max_lin_relres"])
+    t0 = time.perf_counter()
+    E2, dk, g, st2 = ctx.ch_gradient(c0, chi, kappa, M0, dt, nsteps)
+    res.update(gradient_s=time.perf_counter() - t0, dE_dkappa=dk, dE_dc0_norm=float(np.linalg.norm(g)),
+               energy_gradient_run_matches=abs(E2 - E) <= 1e-14 * abs(E))
+    if fd:
+        # central differences with steps h and 2h; their Richardson combination removes the h^2 term, which at
+        # 200 steps of spinodal growth is not small against 1e-6 (the growth rate depends strongly on kappa)
+        def central(f, h):
+            return (f(h) - f(-h)) / (2 * h)
+
+        fk = lambda e: ctx.ch_run(c0, chi, kappa + e, M0, dt, nsteps)[1]
+        d1, d2 = central(fk, 1e-6), central(fk, 2e-6)
+        rk = (4 * d1 - d2) / 3
+        v = np.where(L.mirror == 0, np.random.default_rng(7).standard_normal(L.n), 0.0)
+        fc = lambda e: ctx.ch_run(c0 + e * v, chi, kappa, M0, dt, nsteps)[1]
+        e1, e2 = central(fc, 1e-6), central(fc, 2e-6)
+        rc = (4 * e1 - e2) / 3
+        ad = float(g @ v)
+        res.update(dE_dkappa_central_fd_1e6=d1, dE_dkappa_rel_err_vs_fd_1e6=abs(dk - d1) / abs(d1),
+                   dE_dkappa_richardson=rk, dE_dkappa_rel_err_vs_richardson=abs(dk - rk) / abs(rk),
+                   dE_dc0_dir=ad, dE_dc0_dir_central_fd_1e6=e1, dE_dc0_dir_rel_err_vs_fd_1e6=abs(ad - e1) / abs(e1),
+                   dE_dc0_dir_rel_err_vs_richardson=abs(ad - rc) / abs(rc))
+    ctx.close()
+    return res
+
+
 def c3_clouds(px, nclouds=256, nmin=1000, nmax=200000, seed=2024, families=True):
     """Batched-cloud workload: clouds alternate 2D / 3D (half each), node counts log-uniform in [nmin, nmax]
     (seeded), cell-centred lattice of spacing h = 1 mm jittered by U(-0.2h, 0.2h) per coordinate, no ghosts
@@ -652,7 +739,7 @@ def run_perix(args):
     traffic = read_traffic(head)
     e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, max(10, min(steps, 200)))
     cpu = None
-    c3 = c5 = refgpu = c1 = None
+    c3 = c5 = refgpu = c1 = c4 = None
     if rank == 0 and ws == 1:
         cpu = cpu_reference(w, 20, 2)
         for p in out.values():
@@ -662,6 +749,7 @@ def run_perix(args):
             c5 = c5_measure(px, device=local)
             refgpu = reference_gpu()
             c1 = c1_measure(px, device=local)
+            c4 = c4_measure(px, device=local)
     if rank != 0:
         return
     line = {
@@ -707,6 +795,7 @@ def run_perix(args):
         "slab_3d": c5,
         "reference_gpu": refgpu,
         "poisson_c1": c1,
+        "cahn_hilliard_c4": c4,
         "gbuild_nodes_per_s": {"fp64": out["fp64"]["gbuild"], "mixed": out["mixed"]["gbuild"],
                                "ms": {"fp64": out["fp64"]["gbuild_ms"], "mixed": out["mixed"]["gbuild_ms"]},
                                "workload": "order-2 g-build of the same plate (81,200 nodes, all 5 operators stored)"},
@@ -810,6 +899,10 @@ def run_profile(args):
         print(json.dumps({"profile": "c5", **c5_measure(px)}))
         ctx.close()
         return
+    if args.profile == "c4":
+        ctx.close()
+        print(json.dumps({"profile": "c4", **c4_measure(px, nsteps=args.steps)}))
+        return
     if args.profile == "refgpu":
         # the reference's own GPU explicit path (oracle/_ref/libperix_ref_cuda.so) on the plate and the slab,
         # from the state after 100 steps; run in a child process of the main bench
@@ -912,7 +1005,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="perix", choices=["perix", "reference"])
-    ap.add_argument("--profile", choices=["step", "gbuild", "c3", "c5", "c5step", "c3apply", "refgpu"], default=None,
+    ap.add_argument("--profile", choices=["step", "gbuild", "c3", "c5", "c5step", "c3apply", "refgpu", "c4"], default=None,
                     help="run one kernel family only (for profiler captures); prints its own JSON line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--variant", type=int, default=8)
