@@ -11,6 +11,9 @@
   wrapped in torch.utils.checkpoint, so the backward pass keeps one state per segment and recomputes the
   steps inside a segment.
 - ``elastic_constants_t``: C11, C12, C66 as torch functions of E and nu (ExplicitPDDOFracElement.cpp:38-53).
+- ``ch_free_energy(ctx, c0, kappa, ...)``: the total free energy after a backward-Euler Cahn-Hilliard run on the
+  device (CahnHilliardElement.cpp:66-292 per step); its backward is the discrete adjoint of the run
+  (``pxb_ch_gradient``), which returns dE/dkappa and dE/dc0 together.
 
 The perix context does the arithmetic; torch supplies the tape, the device memory and the stream (each call
 puts the context on torch's current stream).  All tensors are float64 on the context's GPU.
@@ -199,3 +202,29 @@ def set_constants(pctx, C, rho):
     """Puts the values of the (3,) tensor C into the context (one device-to-host read)."""
     c11, c12, c66 = (float(x) for x in C.detach().cpu())
     pctx.epf_set_constants(c11, c12, c66, rho)
+
+
+class _ChEnergy(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, c0, kappa, pctx, chi, M0, dt, nsteps):
+        c = _f64c(c0).cpu().numpy()
+        k = float(kappa)
+        E, dk, g, _ = pctx.ch_gradient(c, chi, k, M0, dt, nsteps)
+        fctx.save_for_backward(torch.from_numpy(g).to(c0.device), torch.tensor(dk, dtype=torch.float64,
+                                                                               device=c0.device))
+        return torch.tensor(E, dtype=torch.float64, device=c0.device)
+
+    @staticmethod
+    def backward(fctx, gE):
+        g, dk = fctx.saved_tensors
+        return gE * g, gE * dk, None, None, None, None, None
+
+
+def ch_free_energy(pctx, c0, kappa, chi, M0, dt, nsteps):
+    """Total free energy of the final state of an implicit Cahn-Hilliard run from c0 (one value per node; ghost
+    entries follow their mirror nodes) as a differentiable function of c0 and kappa (a 0-d tensor).  The forward
+    pass already runs the adjoint (pxb_ch_gradient) and keeps the gradient for the backward pass."""
+    if not torch.is_tensor(kappa):
+        kappa = torch.tensor(float(kappa), dtype=torch.float64, device=c0.device)
+    return _ChEnergy.apply(c0, kappa, pctx, float(chi), float(M0), float(dt), int(nsteps))
+
