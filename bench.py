@@ -307,6 +307,16 @@ def c4_measure(px, device=0, nside=256, nsteps=200, reps=20, fd=True):
     E2, dk, g, st2 = ctx.ch_gradient(c0, chi, kappa, M0, dt, nsteps)
     res.update(gradient_s=time.perf_counter() - t0, dE_dkappa=dk, dE_dc0_norm=float(np.linalg.norm(g)),
                energy_gradient_run_matches=abs(E2 - E) <= 1e-14 * abs(E))
+    try:
+        from oracle import RefMesh, ref_available
+        if ref_available():
+            # the reference's OpenMP assembly of the same system (its element preprocess excluded)
+            m = RefMesh.structured(2, nside, nside, 0, [0, 1, 0, 1], 3.015, 2)
+            _, _, _, t = m.ch_assemble(chi, kappa, M0, dt, u, u)
+            res["reference_cpu_assembly_ms"] = t * 1e3
+            res["reference_cpu_threads"] = os.cpu_count()
+    except Exception as e:  # noqa: BLE001
+        res["reference_cpu_assembly_ms"] = "unavailable: %s" % e
     if fd:
         # central differences with steps h and 2h; their Richardson combination removes the h^2 term, which at
         # 200 steps of spinodal growth is not small against 1e-6 (the growth rate depends strongly on kappa)

@@ -1152,9 +1152,10 @@ extern "C" int pxb_csr_set_pattern(pxb_ctx *c, int ndof, const int *rowptr, cons
     PXB_TRY(dev_upload(c, k.cols, cols, sizeof(int) * (size_t)nnz));
     PXB_TRY(dev_alloc(c, k.slot, sizeof(int) * (size_t)std::max(1LL, c->g.nb) * ndof * ndof));
     PXB_TRY(dev_alloc(c, k.diag, sizeof(int) * (size_t)c->g.n * ndof * ndof));
+    PXB_TRY(dev_alloc(c, k.extra, sizeof(int) * (size_t)c->g.n * ndof * ndof));
     void *tmp = nullptr;
     PXB_TRY(scratch(c, 8, &tmp));
-    PXB_CUDA_TRY(cudaMemsetAsync(tmp, 0, 4, c->stream));
+    PXB_CUDA_TRY(cudaMemsetAsync(tmp, 0, 8, c->stream));
     CsrMapArgs a;
     a.n = c->g.n;
     a.ndof = ndof;
@@ -1165,11 +1166,16 @@ extern "C" int pxb_csr_set_pattern(pxb_ctx *c, int ndof, const int *rowptr, cons
     a.slot = k.slot.as<int>();
     a.diag = k.diag.as<int>();
     a.missing = static_cast<int *>(tmp);
+    a.inexact = static_cast<int *>(tmp) + 1;
+    a.mirror = c->g.mirror.p ? c->g.mirror.as<int>() : nullptr;
+    a.extra = k.extra.as<int>();
     launch_csr_map(a, c->stream);
     PXB_TRY(check_launch(c, "csr_map"));
-    int missing = 0;
-    PXB_TRY(d2h(c, &missing, tmp, 4));
+    int flags[2] = {0, 0};
+    PXB_TRY(d2h(c, flags, tmp, 8));
     PXB_TRY(sync(c));
+    const int missing = flags[0];
+    k.exact = flags[1] == 0;
     if (missing) return fail(PXB_ERR_INVALID, "pxb_csr_set_pattern: pattern lacks " + std::to_string(missing) +
                                                   " entries required by the families");
     PXB_TRY(dev_alloc(c, k.kvals, sizeof(double) * (size_t)nnz));
@@ -1322,6 +1328,7 @@ static int ch_args(pxb_ctx *c, double kappa, double chi, double dt, const double
     a.rowptr = k.rowptr.as<int>();
     a.slot = k.slot.as<int>();
     a.diag = k.diag.as<int>();
+    a.extra = k.exact ? k.extra.as<int>() : nullptr;
     a.u = u_d;
     a.uold = uold_d;
     a.kvals = kvals_d;
@@ -1530,6 +1537,7 @@ extern "C" int pxb_assemble_ch(pxb_ctx *c, double kappa, double chi, double dt, 
     a.rowptr = k.rowptr.as<int>();
     a.slot = k.slot.as<int>();
     a.diag = k.diag.as<int>();
+    a.extra = k.exact ? k.extra.as<int>() : nullptr;
     a.u = k.u.as<double>();
     a.uold = k.uold.as<double>();
     a.kvals = k.kvals.as<double>();

@@ -44,6 +44,21 @@ __global__ void csr_map_kernel(CsrMapArgs a) {
                 }
             }
         }
+        if (a.extra) {
+            // the mirror block, when the mirror node is not a family member, and whether the rows hold anything else
+            const int m = a.mirror ? a.mirror[i] - 1 : -1;
+            bool in_fam = m == i;
+            for (int t = a.off[i]; t < a.off[i + 1] && m >= 0 && !in_fam; ++t) in_fam = a.nbr[t] == m;
+            const bool extra = m >= 0 && !in_fam;
+            const int width = nd * (1 + (a.off[i + 1] - a.off[i]) + (extra ? 1 : 0));
+            for (int r = 0; r < nd; ++r) {
+                const int row = i * nd + r;
+                const int lo = a.rowptr[row], hi = a.rowptr[row + 1];
+                if (hi - lo != width) atomicAdd(a.inexact, 1);
+                for (int c = 0; c < nd; ++c)
+                    a.extra[(size_t)i * nd * nd + r * nd + c] = extra ? find_slot(a.cols, lo, hi, m * nd + c) : -1;
+            }
+        }
     }
 }
 
@@ -433,18 +448,43 @@ cudaError_t launch_assemble_cached(const CachedAsmArgs &a, cudaStream_t s) {
 }
 
 // ---- conservative Cahn-Hilliard (2 dof: c, mu) ------------------------------------------------------------
+// LPN lanes per node (a family of 12..28 bonds fills a group of 8 in a pass or four), so the per-node work (row
+// zeroing, reductions, the nodal free-energy terms) runs for 32/LPN nodes at once instead of one per warp
+template <int LPN>
 __global__ void __launch_bounds__(256) assemble_ch_kernel(ChAsmArgs a) {
-    constexpr int WPB = 256 / kWarp;
+    constexpr int GPW = kWarp / LPN;
     const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    for (int i = blockIdx.x * WPB + wib; i < a.n; i += gridDim.x * WPB) {
+    const int gl = lane & (LPN - 1);
+    const int grp = lane / LPN;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int base = warp * GPW; base < a.n; base += nwarps * GPW) {
+        const int i = base + grp;
+        const bool act = i < a.n;
         const int rc = 2 * i, rm = 2 * i + 1;
-        for (int s = a.rowptr[rc] + lane; s < a.rowptr[rm + 1]; s += kWarp) a.kvals[s] = 0.0;
+        if (act) {
+            if (a.extra) {  // exact pattern: every other entry of the two rows is written below
+                if (gl < 4) {
+                    const int e = a.extra[(size_t)i * 4 + gl];
+                    if (e >= 0) a.kvals[e] = 0.0;
+                }
+            } else {
+                for (int s = a.rowptr[rc] + gl; s < a.rowptr[rm + 1]; s += LPN) a.kvals[s] = 0.0;
+            }
+        }
         __syncwarp();
-        const double c = a.u[rc], mu = a.u[rm], cold = a.uold[rc];
-        const double Vi = a.vol[i], Mi = a.mnode[i];
+        double c = 0.0, mu = 0.0, Vi = 0.0, Mi = 0.0;
+        int b0 = 0, b1 = 0;
+        if (act) {
+            c = a.u[rc];
+            mu = a.u[rm];
+            Vi = a.vol[i];
+            Mi = a.mnode[i];
+            b0 = a.off[i];
+            b1 = a.off[i + 1];
+        }
         double rcs = 0.0, rms = 0.0, k12 = 0.0, k21 = 0.0;
-        for (int t = a.off[i] + lane; t < a.off[i + 1]; t += kWarp) {
+        for (int t = b0 + gl; t < b1; t += LPN) {
             const int j = __ldg(a.nbr + t);
             const bool ghostJ = a.ghost && a.ghost[j];
             const double g2 = a.lap[t];
@@ -457,29 +497,30 @@ __global__ void __launch_bounds__(256) assemble_ch_kernel(ChAsmArgs a) {
                 coeff_c = -w;
             }
             const double coeff_mu = ghostJ ? 0.0 : a.kappa * g2;
-            rcs += coeff_c * (a.u[2 * j + 1] - mu);
-            rms += coeff_mu * (a.u[2 * j] - c);
+            rcs += coeff_c * (a.u[2 * (size_t)j + 1] - mu);  // u may be only 8-byte aligned (a caller's pointer)
+            rms += coeff_mu * (a.u[2 * (size_t)j] - c);
             k12 += coeff_c;
             k21 += coeff_mu;
-            const int *sl = a.slot + (size_t)t * 4;
-            a.kvals[sl[0]] = -0.0;        // (c,  c_j)
-            a.kvals[sl[1]] = -coeff_c;    // (c,  mu_j)
-            a.kvals[sl[2]] = -coeff_mu;   // (mu, c_j)
-            a.kvals[sl[3]] = -0.0;        // (mu, mu_j)
+            const int4 sl = reinterpret_cast<const int4 *>(a.slot)[t];
+            a.kvals[sl.x] = -0.0;        // (c,  c_j)
+            a.kvals[sl.y] = -coeff_c;    // (c,  mu_j)
+            a.kvals[sl.z] = -coeff_mu;   // (mu, c_j)
+            a.kvals[sl.w] = -0.0;        // (mu, mu_j)
         }
-        rcs = group_sum<kWarp>(rcs);
-        rms = group_sum<kWarp>(rms);
-        k12 = group_sum<kWarp>(k12);
-        k21 = group_sum<kWarp>(k21);
-        if (lane == 0) {
+        rcs = group_sum<LPN>(rcs);
+        rms = group_sum<LPN>(rms);
+        k12 = group_sum<LPN>(k12);
+        k21 = group_sum<LPN>(k21);
+        if (act && gl == 0) {
+            const double cold = a.uold[rc];
             const double cc = ch_clamp(c);
             const double fp = log(cc / (1.0 - cc)) + a.chi * (1.0 - 2.0 * cc);
             const double fpp = 1.0 / (cc * (1.0 - cc)) - 2.0 * a.chi;
-            const int *dg = a.diag + (size_t)i * 4;
-            a.kvals[dg[0]] = -(1.0 / a.dt);
-            a.kvals[dg[1]] = -0.0 + k12;
-            a.kvals[dg[2]] = fpp + k21;
-            a.kvals[dg[3]] = -1.0;
+            const int4 dg = reinterpret_cast<const int4 *>(a.diag)[i];
+            a.kvals[dg.x] = -(1.0 / a.dt);
+            a.kvals[dg.y] = -0.0 + k12;
+            a.kvals[dg.z] = fpp + k21;
+            a.kvals[dg.w] = -1.0;
             a.rhs[rc] = (c - cold) / a.dt + rcs;
             a.rhs[rm] = mu - fp + rms;
         }
@@ -487,8 +528,11 @@ __global__ void __launch_bounds__(256) assemble_ch_kernel(ChAsmArgs a) {
 }
 
 cudaError_t launch_assemble_ch(const ChAsmArgs &a, cudaStream_t s) {
-    const int g = (a.n + 7) / 8;
-    assemble_ch_kernel<<<g > 0 ? g : 1, 256, 0, s>>>(a);
+    constexpr int LPN = 8;
+    const long long warps = ((long long)a.n + (kWarp / LPN) - 1) / (kWarp / LPN);
+    const long long g = (warps + 7) / 8;
+    const int grid = (int)(g < 148 * 32 ? (g > 0 ? g : 1) : 148 * 32);
+    assemble_ch_kernel<LPN><<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -241,6 +241,9 @@ struct CsrMapArgs {
     int *slot = nullptr;   // [nb*ndof*ndof]
     int *diag = nullptr;   // [n*ndof*ndof]
     int *missing = nullptr;
+    const int *mirror = nullptr;  // 1-based mirror bulk node, 0 none (may be NULL)
+    int *extra = nullptr;         // [n*ndof*ndof] slots of the mirror block when it is not a family member, else -1
+    int *inexact = nullptr;       // rows holding entries beyond own block + family + mirror block
 };
 cudaError_t launch_csr_map(const CsrMapArgs &a, cudaStream_t s);
 
@@ -263,6 +266,7 @@ cudaError_t launch_assemble_scalar(const ScalarAsmArgs &a, cudaStream_t s);
 
 struct ChAsmArgs {
     int n = 0;
+    const int *extra = nullptr;  // exact pattern: mirror-block slots to clear (rows are not zeroed first)
     double kappa = 0, chi = 0, dt = 1;
     const int *off = nullptr, *nbr = nullptr, *rev = nullptr;
     const double *lap = nullptr, *vol = nullptr, *mnode = nullptr;

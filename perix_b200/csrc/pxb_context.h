@@ -142,6 +142,10 @@ struct CsrState {
     DevBuf rowptr, cols;
     DevBuf slot;       // int32 [nb*ndof*ndof]: CSR slot of (row i*ndof+a, col j*ndof+b) for bond t
     DevBuf diag;       // int32 [n*ndof*ndof]: slot of the diagonal block entries
+    // exact pattern (every row = own block + family blocks + mirror block): the assembly kernels then write every
+    // entry once instead of zeroing the rows first; extra = slots of a mirror block outside the family (-1 none)
+    bool exact = false;
+    DevBuf extra;      // int32 [n*ndof*ndof]
     DevBuf kvals, rhs, u, uold, fnode, mnode;
 };
 
