@@ -1176,6 +1176,11 @@ extern "C" int pxb_csr_set_pattern(pxb_ctx *c, int ndof, const int *rowptr, cons
     PXB_TRY(sync(c));
     const int missing = flags[0];
     k.exact = flags[1] == 0;
+    if (ndof == 2 && block_view(c->g.n, rowptr, cols, k.h_bptr, k.h_bcol)) {
+        PXB_TRY(dev_upload(c, k.bptr, k.h_bptr.data(), sizeof(int) * k.h_bptr.size()));
+        PXB_TRY(dev_upload(c, k.bcol, k.h_bcol.data(), sizeof(int) * std::max<size_t>(1, k.h_bcol.size())));
+        k.blocked2 = true;
+    }
     if (missing) return fail(PXB_ERR_INVALID, "pxb_csr_set_pattern: pattern lacks " + std::to_string(missing) +
                                                   " entries required by the families");
     PXB_TRY(dev_alloc(c, k.kvals, sizeof(double) * (size_t)nnz));

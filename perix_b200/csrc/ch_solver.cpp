@@ -5,8 +5,8 @@
 // iteration at the current iterate (CahnHilliardElement::preprocessIteration, .cpp:66-175) and without its
 // derivative in the Jacobian (a Picard-Newton iteration), zero-Neumann ghost rows replaced as NeumannBC::apply
 // does (NeumannBC.cpp:127-150).  Each linear system K dU = F is solved on the device by BiCGStab with a 2x2
-// block-Jacobi preconditioner; assembly, solve and updates never leave the GPU (dot products come back to the host
-// to steer the iteration).
+// block-Jacobi preconditioner, one cooperative kernel per solve (k_bicg.cu); assembly, solve and updates never leave
+// the GPU, and the host reads the solve's outcome and the residual norm once per Newton iteration.
 //
 // The gradient of the total free energy E(U_N) (k_linalg.cu) with respect to kappa and the initial field c0 is the
 // discrete adjoint of the converged steps: with F_n(U_n, U_{n-1}) = 0, dF_n/dU_n = -K_n + J_M (the mobility term the
@@ -24,6 +24,9 @@ namespace pxb {
 namespace {
 
 constexpr double kUpdateTol = 1e-14;  // Newton stops when |dU| <= kUpdateTol |U|
+constexpr size_t kBicgScalarBytes = 128;  // BicgScalars, then the partial sums
+static_assert(sizeof(BicgScalars) <= kBicgScalarBytes, "BiCGStab scalar block");
+constexpr int kHostDots = 4;  // dot products read back with a solve's outcome
 
 struct RunCtx {
     pxb_ctx *c;
@@ -40,6 +43,8 @@ int need_ch_run(pxb_ctx *c, const char *who) {
         return fail(PXB_ERR_STATE, std::string(who) + ": needs an FP64 order-2 g-build (pxb_gbuild)");
     if (!c->ch.ready) return fail(PXB_ERR_STATE, std::string(who) + ": needs the CH geometry (pxb_ch_build_geometry)");
     if (!c->csr.ready || c->csr.ndof != 2) return fail(PXB_ERR_STATE, std::string(who) + ": set a 2-dof pattern first");
+    if (!c->csr.blocked2)
+        return fail(PXB_ERR_UNSUPPORTED, std::string(who) + ": the pattern must consist of dense 2x2 node blocks");
     return PXB_OK;
 }
 
@@ -63,6 +68,8 @@ int alloc_run(RunCtx &r) {
     PXB_TRY(dev_alloc(c, h.red, sizeof(double) * (size_t)(dot_scratch_doubles() + 8)));
     PXB_TRY(dev_alloc(c, h.nodal, sizeof(double) * 2 * n));
     for (auto &w : h.w) PXB_TRY(dev_alloc(c, w, sizeof(double) * rows));
+    PXB_TRY(dev_alloc(c, h.bicg, kBicgScalarBytes + sizeof(double) * 6 * kBicgParts));
+    PXB_TRY(ensure_pinned(h.bicg_h, kBicgScalarBytes + sizeof(double) * kHostDots));
     if (h.ones.bytes < sizeof(double) * n) {
         std::vector<double> one(n, 1.0);
         PXB_TRY(dev_upload(c, h.ones, one.data(), sizeof(double) * n));
@@ -98,91 +105,101 @@ int assemble(RunCtx &r, const double *U, const double *Uold) {
     return PXB_OK;
 }
 
-// y = A x with A = K (forward) or A = K^T - J_M^T at state U (adjoint)
-int apply_op(RunCtx &r, bool adjoint, const double *U, const double *x, double *y) {
+ChAdjArgs adj_args(RunCtx &r, const double *U, const double *x, double *y) {
     pxb_ctx *c = r.c;
-    PXB_TRY(check(c, launch_spmv((int)r.rows, c->csr.rowptr.as<int>(), c->csr.cols.as<int>(), c->ch.kv.as<double>(), x,
-                                 y, adjoint, c->stream),
-                  "spmv"));
-    if (adjoint) {
-        ChAdjArgs a;
-        a.n = r.n;
-        a.M0 = r.p.M0;
-        a.off = c->g.off.as<int>();
-        a.nbr = c->g.nbr.as<int>();
-        a.rev = c->ch.rev.as<int>();
-        a.mirror = c->g.mirror.p ? c->g.mirror.as<int>() : nullptr;
-        a.ghost = c->ch.ghost.p ? c->ch.ghost.as<char>() : nullptr;
-        a.lap = c->ch.lap.as<double>();
-        a.vol = c->g.vol.as<double>();
-        a.u = U;
-        a.x = x;
-        a.y = y;
-        PXB_TRY(check(c, launch_ch_mob_adj(a, c->stream), "ch mobility adjoint"));
-    }
+    ChAdjArgs a;
+    a.n = r.n;
+    a.M0 = r.p.M0;
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.rev = c->ch.rev.as<int>();
+    a.mirror = c->g.mirror.p ? c->g.mirror.as<int>() : nullptr;
+    a.ghost = c->ch.ghost.p ? c->ch.ghost.as<char>() : nullptr;
+    a.lap = c->ch.lap.as<double>();
+    a.vol = c->g.vol.as<double>();
+    a.u = U;
+    a.x = x;
+    a.y = y;
+    return a;
+}
+
+// Right-preconditioned BiCGStab for A x = b (x starts at 0) on the device, one cooperative kernel (k_bicg.cu); A = K
+// (ch.kv) or, for adjoint solves, K'^T (ch.kvt through the transposed block view); the block-Jacobi inverse of A must
+// be in ch.binv.  Launches only; bicg_outcome reads the result after the caller's next synchronisation.
+int bicgstab_launch(RunCtx &r, bool adjoint, const double *b, double *x) {
+    pxb_ctx *c = r.c;
+    ChState &h = c->ch;
+    BicgArgs a;
+    a.n = r.n;
+    a.bptr = (adjoint ? c->csr.tbptr : c->csr.bptr).as<int>();
+    a.bcol = (adjoint ? c->csr.tbcol : c->csr.bcol).as<int>();
+    a.val = (adjoint ? h.kvt : h.kv).as<double>();
+    a.binv = h.binv.as<double>();
+    a.b = b;
+    a.x = x;
+    a.r = h.w[0].as<double>();
+    a.r0 = h.w[1].as<double>();
+    a.rh = h.w[2].as<double>();
+    a.v = h.w[3].as<double>();
+    a.s = h.w[4].as<double>();
+    a.t = h.w[5].as<double>();
+    a.sh = h.w[6].as<double>();
+    a.ph[0] = h.w[7].as<double>();
+    a.ph[1] = h.w[8].as<double>();
+    a.vh[0] = h.w[9].as<double>();
+    a.vh[1] = h.w[10].as<double>();
+    a.sc = h.bicg.as<BicgScalars>();
+    a.part = reinterpret_cast<double *>(h.bicg.as<char>() + kBicgScalarBytes);
+    PXB_TRY(check(c, launch_bicg_solve(a, r.p.lin_rtol, r.p.lin_max, c->stream), "bicgstab"));
     return PXB_OK;
 }
 
-// right-preconditioned BiCGStab for A x = b (x starts at 0); the block-Jacobi inverse must be in ch.binv
-int bicgstab(RunCtx &r, bool adjoint, const double *U, const double *b, double *x, int *its, double *relres) {
-    pxb_ctx *c = r.c;
+// Host copies of the solve's outcome (pinned: BicgScalars, then kHostDots dot products); queue_readback enqueues the
+// copies of the outcome and of the first ndots entries of ch.red's result slots.
+BicgScalars *host_outcome(ChState &h) { return static_cast<BicgScalars *>(h.bicg_h.p); }
+double *host_dots(ChState &h) { return reinterpret_cast<double *>(static_cast<char *>(h.bicg_h.p) + kBicgScalarBytes); }
+double *dev_dots(ChState &h) { return h.red.as<double>() + dot_scratch_doubles(); }
+
+int queue_readback(pxb_ctx *c, int ndots) {
     ChState &h = c->ch;
-    const long long len = r.rows;
-    double *rr = h.w[0].as<double>(), *r0 = h.w[1].as<double>(), *pp = h.w[2].as<double>(), *v = h.w[3].as<double>();
-    double *sv = h.w[4].as<double>(), *t = h.w[5].as<double>(), *ph = h.w[6].as<double>(), *sh = h.w[7].as<double>();
-    PXB_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)len, c->stream));
-    PXB_TRY(copy(r, rr, b));
-    PXB_TRY(copy(r, r0, b));
-    PXB_CUDA_TRY(cudaMemsetAsync(v, 0, sizeof(double) * (size_t)len, c->stream));
-    PXB_CUDA_TRY(cudaMemsetAsync(pp, 0, sizeof(double) * (size_t)len, c->stream));
-    double bb = 0.0;
-    PXB_TRY(dotp(r, len, b, b, &bb));
-    const double bnorm = std::sqrt(bb);
-    *its = 0;
-    *relres = 0.0;
-    if (!(bnorm > 0.0)) return PXB_OK;
-    double rho = 1.0, alpha = 1.0, omega = 1.0;
-    for (int k = 1; k <= r.p.lin_max; ++k) {
-        double rho1 = 0.0;
-        PXB_TRY(dotp(r, len, r0, rr, &rho1));
-        if (rho1 == 0.0 || !std::isfinite(rho1)) break;
-        if (k == 1) PXB_TRY(copy(r, pp, rr));
-        else PXB_TRY(check(c, launch_bicg_p(len, rr, (rho1 / rho) * (alpha / omega), omega, v, pp, c->stream), "bicg p"));
-        PXB_TRY(check(c, launch_block_apply(r.n, h.binv.as<double>(), pp, ph, c->stream), "precond"));
-        PXB_TRY(apply_op(r, adjoint, U, ph, v));
-        double r0v = 0.0;
-        PXB_TRY(dotp(r, len, r0, v, &r0v));
-        if (r0v == 0.0 || !std::isfinite(r0v)) break;
-        alpha = rho1 / r0v;
-        PXB_TRY(copy(r, sv, rr));
-        PXB_TRY(check(c, launch_axpby(len, -alpha, v, 1.0, sv, c->stream), "axpby"));
-        double ss = 0.0;
-        PXB_TRY(dotp(r, len, sv, sv, &ss));
-        *its = k;
-        if (std::sqrt(ss) <= r.p.lin_rtol * bnorm) {
-            PXB_TRY(check(c, launch_axpby(len, alpha, ph, 1.0, x, c->stream), "axpby"));
-            *relres = std::sqrt(ss) / bnorm;
-            return PXB_OK;
-        }
-        PXB_TRY(check(c, launch_block_apply(r.n, h.binv.as<double>(), sv, sh, c->stream), "precond"));
-        PXB_TRY(apply_op(r, adjoint, U, sh, t));
-        double tt = 0.0, ts = 0.0;
-        PXB_TRY(dotp(r, len, t, t, &tt));
-        PXB_TRY(dotp(r, len, t, sv, &ts));
-        omega = tt > 0.0 ? ts / tt : 0.0;
-        PXB_TRY(check(c, launch_axpby(len, alpha, ph, 1.0, x, c->stream), "axpby"));
-        PXB_TRY(check(c, launch_axpby(len, omega, sh, 1.0, x, c->stream), "axpby"));
-        PXB_TRY(copy(r, rr, sv));
-        PXB_TRY(check(c, launch_axpby(len, -omega, t, 1.0, rr, c->stream), "axpby"));
-        double rn = 0.0;
-        PXB_TRY(dotp(r, len, rr, rr, &rn));
-        *relres = std::sqrt(rn) / bnorm;
-        if (*relres <= r.p.lin_rtol) return PXB_OK;
-        rho = rho1;
-        if (omega == 0.0) break;
-    }
+    PXB_CUDA_TRY(cudaMemcpyAsync(host_outcome(h), h.bicg.p, sizeof(BicgScalars), cudaMemcpyDeviceToHost, c->stream));
+    if (ndots > 0)
+        PXB_CUDA_TRY(cudaMemcpyAsync(host_dots(h), dev_dots(h), sizeof(double) * ndots, cudaMemcpyDeviceToHost,
+                                     c->stream));
+    return PXB_OK;
+}
+
+int bicg_outcome(ChState &h, int *its, double *relres) {
+    const BicgScalars *hs = host_outcome(h);
+    *its = hs->its;
+    *relres = hs->relres;
+    if (hs->status == kBicgDone) return PXB_OK;
+    if (hs->abort) return fail(PXB_ERR_CUDA, "CH linear solve: a grid barrier of the BiCGStab kernel timed out");
+    const char *why = hs->status == kBicgBreakdown ? " (breakdown)" : "";
     return fail(PXB_ERR_STATE, "CH linear solve: BiCGStab stopped at relative residual " + std::to_string(*relres) +
-                                   " after " + std::to_string(*its) + " iterations");
+                                   " after " + std::to_string(*its) + " iterations" + why);
+}
+
+// dot product a . b into result slot k of ch.red (launch only)
+int dot_into(RunCtx &r, long long len, const double *a, const double *b, int k) {
+    pxb_ctx *c = r.c;
+    double *red = c->ch.red.as<double>();
+    return check(c, launch_dot(len, a, b, red, dev_dots(c->ch) + k, c->stream), "dot");
+}
+
+// the transposed block view and value permutation of the pattern, and room for K^T (adjoint solves)
+int ensure_transpose(pxb_ctx *c) {
+    CsrState &k = c->csr;
+    if (!k.transposed) {
+        std::vector<int> tbptr, tbcol, perm;
+        block_transpose(c->g.n, k.h_bptr, k.h_bcol, tbptr, tbcol, perm);
+        PXB_TRY(dev_upload(c, k.tbptr, tbptr.data(), sizeof(int) * tbptr.size()));
+        PXB_TRY(dev_upload(c, k.tbcol, tbcol.data(), sizeof(int) * std::max<size_t>(1, tbcol.size())));
+        PXB_TRY(dev_upload(c, k.tperm, perm.data(), sizeof(int) * std::max<size_t>(1, perm.size())));
+        PXB_TRY(sync(c));
+        k.transposed = true;
+    }
+    return dev_alloc(c, c->ch.kvt, sizeof(double) * (size_t)k.nnz);
 }
 
 // one backward-Euler step: U (in: initial guess, out: converged state) from Uold
@@ -206,15 +223,18 @@ int newton_step(RunCtx &r, double *U, const double *Uold, pxb_ch_run_stats *st) 
         PXB_TRY(check(c, launch_block_inv(r.n, c->csr.diag.as<int>(), h.kv.as<double>(), false, h.binv.as<double>(),
                                           c->stream),
                       "block inverse"));
+        PXB_TRY(bicgstab_launch(r, false, h.rhs.as<double>(), h.dU.as<double>()));
+        PXB_TRY(dot_into(r, r.rows, h.dU.as<double>(), h.dU.as<double>(), 0));
+        PXB_TRY(dot_into(r, r.rows, U, U, 1));
+        PXB_TRY(check(c, launch_axpby(r.rows, 1.0, h.dU.as<double>(), 1.0, U, c->stream), "update"));
+        PXB_TRY(queue_readback(c, 2));
+        PXB_TRY(sync(c));
         int lits = 0;
         double lres = 0.0;
-        PXB_TRY(bicgstab(r, false, U, h.rhs.as<double>(), h.dU.as<double>(), &lits, &lres));
+        PXB_TRY(bicg_outcome(h, &lits, &lres));
         st->lin_iters += lits;
         st->max_lin_relres = std::max(st->max_lin_relres, lres);
-        double dd = 0.0, uu = 0.0;
-        PXB_TRY(dotp(r, r.rows, h.dU.as<double>(), h.dU.as<double>(), &dd));
-        PXB_TRY(dotp(r, r.rows, U, U, &uu));
-        PXB_TRY(check(c, launch_axpby(r.rows, 1.0, h.dU.as<double>(), 1.0, U, c->stream), "update"));
+        const double dd = host_dots(h)[0], uu = host_dots(h)[1];
         // an update at the rounding level of the state ends the iteration (the residual of a small step can sit
         // at its evaluation floor, far above newton_rtol times its initial value)
         if (std::sqrt(dd) <= kUpdateTol * std::sqrt(uu)) {
@@ -328,34 +348,33 @@ extern "C" int pxb_ch_gradient(pxb_ctx *c, const pxb_ch_run_params *p, const dou
     double e = 0.0, dk = 0.0;
     double *g = h.Uold.as<double>(), *lam = h.dU.as<double>();
     PXB_TRY(energy(r, hist + rows * (size_t)p->nsteps, &e, &dk, g));
+    PXB_TRY(ensure_transpose(c));
     for (int s = p->nsteps; s >= 1; --s) {
         const double *Un = hist + rows * (size_t)s;
+        // A = (K - J_M)^T at (U_n, U_{n-1}): fold the mobility derivative into K, then transpose the values
         PXB_TRY(assemble(r, Un, Un - rows));
+        const ChAdjArgs fa = adj_args(r, Un, nullptr, nullptr);
+        PXB_TRY(check(c, launch_ch_fold_mobility(fa, c->csr.slot.as<int>(), c->csr.diag.as<int>(), h.kv.as<double>(),
+                                                 c->stream),
+                      "ch mobility fold"));
+        PXB_TRY(check(c, launch_gather_values(c->csr.nnz, c->csr.tperm.as<int>(), h.kv.as<double>(), h.kvt.as<double>(),
+                                              c->stream),
+                      "transpose values"));
         PXB_TRY(check(c, launch_block_inv(r.n, c->csr.diag.as<int>(), h.kv.as<double>(), true, h.binv.as<double>(),
                                           c->stream),
                       "block inverse"));
+        PXB_TRY(bicgstab_launch(r, true, g, lam));
+        ChAdjArgs a = adj_args(r, Un, lam, h.nodal.as<double>());
+        PXB_TRY(check(c, launch_ch_dkappa(a, c->stream), "ch dkappa"));
+        PXB_TRY(dot_into(r, r.n, h.nodal.as<double>(), h.ones.as<double>(), 0));
+        PXB_TRY(queue_readback(c, 1));
+        PXB_TRY(sync(c));
         int lits = 0;
         double lres = 0.0;
-        PXB_TRY(bicgstab(r, true, Un, g, lam, &lits, &lres));
+        PXB_TRY(bicg_outcome(h, &lits, &lres));
         st.lin_iters += lits;
         st.max_lin_relres = std::max(st.max_lin_relres, lres);
-        ChAdjArgs a;
-        a.n = r.n;
-        a.M0 = p->M0;
-        a.off = c->g.off.as<int>();
-        a.nbr = c->g.nbr.as<int>();
-        a.rev = c->ch.rev.as<int>();
-        a.mirror = c->g.mirror.p ? c->g.mirror.as<int>() : nullptr;
-        a.ghost = c->ch.ghost.p ? c->ch.ghost.as<char>() : nullptr;
-        a.lap = c->ch.lap.as<double>();
-        a.vol = c->g.vol.as<double>();
-        a.u = Un;
-        a.x = lam;
-        a.y = h.nodal.as<double>();
-        PXB_TRY(check(c, launch_ch_dkappa(a, c->stream), "ch dkappa"));
-        double dks = 0.0;
-        PXB_TRY(dotp(r, r.n, h.nodal.as<double>(), h.ones.as<double>(), &dks));
-        dk += dks;
+        dk += host_dots(h)[0];
         PXB_TRY(check(c, launch_ch_prev_cot(r.n, a.mirror, lam, p->dt, g, c->stream), "ch previous cotangent"));
     }
     st.energy = e;

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace pxb {
 
 constexpr int kGbuildThreads = 128;
@@ -327,16 +329,11 @@ struct ProjectArgs {
 };
 cudaError_t launch_epf_project(const ProjectArgs &a, cudaStream_t s);
 // ---- device linear algebra and Cahn-Hilliard Newton / adjoint pieces (k_linalg.cu) ----
-cudaError_t launch_spmv(int rows, const int *rowptr, const int *cols, const double *val, const double *x, double *y,
-                        bool transpose, cudaStream_t s);
 int dot_scratch_doubles();
 // *out = a . b over n entries (fixed-order reduction; scratch: dot_scratch_doubles() doubles)
 cudaError_t launch_dot(long long n, const double *a, const double *b, double *scratch, double *out, cudaStream_t s);
 cudaError_t launch_axpby(long long n, double alpha, const double *x, double beta, double *y, cudaStream_t s);
-cudaError_t launch_bicg_p(long long n, const double *r, double beta, double omega, const double *v, double *p,
-                          cudaStream_t s);
 cudaError_t launch_block_inv(int n, const int *diag, const double *val, bool transpose, double *binv, cudaStream_t s);
-cudaError_t launch_block_apply(int n, const double *binv, const double *x, double *y, cudaStream_t s);
 cudaError_t launch_ch_ghost_rows(int n, const int *mirror, const int *rowptr, const int *cols, const double *u,
                                  double *kv, double *rhs, cudaStream_t s);
 struct ChAdjArgs {
@@ -347,8 +344,37 @@ struct ChAdjArgs {
     const double *lap = nullptr, *vol = nullptr, *u = nullptr, *x = nullptr;
     double *y = nullptr;
 };
-// y[c rows] -= J_M^T x (mobility derivative the Picard iteration omits); per-node lambda_mu dF_mu/dkappa
-cudaError_t launch_ch_mob_adj(const ChAdjArgs &a, cudaStream_t s);
+// device-resident BiCGStab (k_bicg.cu): one cooperative kernel per solve, the host reads the outcome
+enum BicgStatus : int { kBicgRunning = 0, kBicgDone = 2, kBicgBreakdown = 3, kBicgMaxIts = 4 };
+constexpr int kBicgParts = 148 * 8;  // most blocks of the solve kernel (one partial sum slot each)
+struct BicgScalars {
+    double relres;
+    int status, its;                     // status: kBicgRunning until the solve ends (then abort tells a timeout)
+    unsigned int bar_count;              // grid barrier arrivals
+    int abort;                           // set by a barrier wait that gave up
+};
+struct BicgArgs {
+    int n = 0;                                  // node blocks (rows 2i, 2i+1)
+    const int *bptr = nullptr, *bcol = nullptr;  // block view of the pattern (block_view)
+    const double *val = nullptr, *binv = nullptr, *b = nullptr;
+    double *x = nullptr, *r = nullptr, *r0 = nullptr, *rh = nullptr, *v = nullptr, *s = nullptr, *sh = nullptr;
+    double *t = nullptr, *ph[2] = {nullptr, nullptr}, *vh[2] = {nullptr, nullptr};
+    BicgScalars *sc = nullptr;
+    double *part = nullptr;  // 6 * kBicgParts doubles (two alternating sets of three)
+};
+// Block view of a 2-dof CSR pattern (host arrays): false unless rows 2i and 2i+1 share one column list of pairs
+// (2j, 2j+1); then bptr[i] = rowptr[2i] / 4 and bcol lists node i's column nodes.
+bool block_view(int n, const int *rowptr, const int *cols, std::vector<int> &bptr, std::vector<int> &bcol);
+// Block view of the transpose and perm: transposed value q = value perm[q] of the matrix
+void block_transpose(int n, const std::vector<int> &bptr, const std::vector<int> &bcol, std::vector<int> &tbptr,
+                     std::vector<int> &tbcol, std::vector<int> &perm);
+cudaError_t launch_gather_values(long long nnz, const int *perm, const double *v, double *vt, cudaStream_t s);
+// the whole solve A x = b (x from 0) as one cooperative kernel; the outcome is in *a.sc when it ends
+cudaError_t launch_bicg_solve(const BicgArgs &a, double tol, int max_its, cudaStream_t s);
+// K' = K - J_M in place on the (c, c) entries of bulk rows, J_M the mobility derivative the Picard Jacobian omits
+// (the adjoint operator is K'^T); slot: bond slot map, diag: diagonal slots of the 2-dof pattern
+cudaError_t launch_ch_fold_mobility(const ChAdjArgs &a, const int *slot, const int *diag, double *kv, cudaStream_t s);
+// per-node lambda_mu dF_mu/dkappa
 cudaError_t launch_ch_dkappa(const ChAdjArgs &a, cudaStream_t s);
 struct ChEnergyArgs {
     int n = 0, nop = 0, sx = 0, sy = 1;

@@ -145,6 +145,11 @@ struct CsrState {
     // exact pattern (every row = own block + family blocks + mirror block): the assembly kernels then write every
     // entry once instead of zeroing the rows first; extra = slots of a mirror block outside the family (-1 none)
     bool exact = false;
+    // ndof 2 and rows 2i, 2i+1 share one list of column pairs (2j, 2j+1): the block view (block_view) and, built on
+    // first use by an adjoint solve, the block view of the transpose with its value permutation
+    bool blocked2 = false, transposed = false;
+    std::vector<int> h_bptr, h_bcol;
+    DevBuf bptr, bcol, tbptr, tbcol, tperm;
     DevBuf extra;      // int32 [n*ndof*ndof]
     DevBuf kvals, rhs, u, uold, fnode, mnode;
 };
@@ -154,8 +159,11 @@ struct ChState {
     DevBuf rev, lap, ghost;
     // implicit run (ch_solver.cpp): state, Newton / BiCGStab work vectors, block-Jacobi inverse, history
     DevBuf U, Uold, dU, rhs, kv, mnode, binv, red, ones, hist;
-    DevBuf w[8];
+    DevBuf w[11];
     DevBuf nodal;  // per-node scratch (energy, dkappa terms)
+    DevBuf kvt;         // values of K^T (adjoint solves)
+    DevBuf bicg;        // BiCGStab scalars and partial sums (k_bicg.cu)
+    PinnedBuf bicg_h;   // host copy of the scalars
 };
 
 }  // namespace pxb
