@@ -255,17 +255,26 @@ def c4_measure(px, device=0, nside=256, nsteps=200, reps=20, fd=True):
     L = px.lattice(2, nside, nside, 0, [0.0, 1.0, 0.0, 1.0])
     delta = 3.015 * L.dxyz[0] * (1.0 + 1e-6)
     off, ids = px.families(L.coords, delta, False, mirror=L.mirror)
+    t0 = time.perf_counter()
     rowptr, cols = px.csr_pattern(off, ids, L.mirror, 2)
+    t_host_pattern = time.perf_counter() - t0
     ctx = px.Context(device)
     ctx.set_geometry(L.coords, L.vols, off, ids, delta, L.dxyz[0], 2, mirror=L.mirror)
     ctx.gbuild(2, px.FP64)
     ctx.ch_build_geometry()
-    ctx.csr_set_pattern(rowptr, cols, 2)
+    ctx.csr_build_pattern(2)  # warm-up
+    t0 = time.perf_counter()
+    ctx.csr_build_pattern(2)  # the pattern of the run: built on the device, slot map included
+    t_dev_pattern = time.perf_counter() - t0
+    r_d, c_d = ctx.csr_get_pattern()
+    pattern_match = bool(np.array_equal(r_d, rowptr) and np.array_equal(c_d, cols))
     chi, kappa, M0, dt = 2.5, 1e-4, 1.0, 1e-6
     rng = np.random.default_rng(2024)
     c0 = 0.5 + rng.uniform(-0.01, 0.01, L.n)
     nb, nnz = int(off[-1]), int(rowptr[-1])
-    res = {"nodes": L.n, "bonds": nb, "rows": 2 * L.n, "nnz": nnz, "steps": nsteps}
+    res = {"nodes": L.n, "bonds": nb, "rows": 2 * L.n, "nnz": nnz, "steps": nsteps,
+           "pattern_host_ms": t_host_pattern * 1e3, "pattern_device_ms": t_dev_pattern * 1e3,
+           "pattern_device_matches_host": pattern_match}
     # the assembly kernel alone at the initial state
     dev = torch.device("cuda", device)
     ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)

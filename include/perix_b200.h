@@ -263,6 +263,12 @@ int pxb_batch_autotune(pxb_ctx *ctx, int what, int reps, size_t flush_bytes, con
  * Sets the matrix pattern (from pxb_csr_pattern or the caller) and precomputes the bond -> CSR-slot map
  * on the device (no binary search per assembly). */
 int pxb_csr_set_pattern(pxb_ctx *ctx, int ndof, const int *rowptr, const int *cols, long long nnz);
+/* Builds the pattern pxb_csr_pattern computes (SparseMatrix::initFromPDMesh, src/MathUtils/SparseMatrix.cpp:73-185:
+ * per node {i} u family u {mirror}, sorted, unique, ndof x ndof blocks) on the device from the context's families
+ * and mirror map, and sets it as pxb_csr_set_pattern does; *nnz gets its size.  Node lists longer than 256 give
+ * PXB_ERR_UNSUPPORTED.  pxb_csr_get_pattern copies the context's pattern to host arrays (rows + 1 and nnz ints). */
+int pxb_csr_build_pattern(pxb_ctx *ctx, int ndof, long long *nnz);
+int pxb_csr_get_pattern(pxb_ctx *ctx, int *rowptr, int *cols);
 /* Poisson (type 0) / transient diffusion (type 1) residual + Jacobian with K = -dF/dU, RHS = +F (reference
  * PoissonElement.cpp:26-58, DiffusionElement, FormResidualAndJacobianParallel.cpp:114-171).  f_node: per-node
  * source (N) or NULL to use the constant f. uold may be NULL when dt == 0. */

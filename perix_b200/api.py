@@ -590,6 +590,24 @@ class Context:
         self._csr_keep = (r, c)
         _check(self.L.pxb_csr_set_pattern(self.h, int(ndof), _p(r, C.c_int), _p(c, C.c_int), C.c_longlong(c.size)))
         self.nnz = c.size
+        self._csr_ndof = int(ndof)
+
+    def csr_build_pattern(self, ndof=1):
+        """The pattern of csr_pattern, built on the device from the context's families and mirror map and set as
+        the context's pattern (pxb_csr_build_pattern); returns nnz."""
+        nnz = C.c_longlong(0)
+        _check(self.L.pxb_csr_build_pattern(self.h, int(ndof), C.byref(nnz)))
+        self._csr_keep = None
+        self.nnz = int(nnz.value)
+        self._csr_ndof = int(ndof)
+        return self.nnz
+
+    def csr_get_pattern(self):
+        """(rowptr, cols) of the context's pattern, copied from the device."""
+        rowptr = np.zeros(self.n * self._csr_ndof + 1, np.int32)
+        cols = np.zeros(self.nnz, np.int32)
+        _check(self.L.pxb_csr_get_pattern(self.h, _p(rowptr, C.c_int), _p(cols, C.c_int)))
+        return rowptr, cols
 
     def assemble_scalar(self, type_, coef, u, f=0.0, f_node=None, dt=0.0, uold=None):
         kv = np.zeros(self.nnz, np.float64)

@@ -1139,17 +1139,13 @@ extern "C" int pxb_epf_force_adjoint(pxb_ctx *c, const double *u, const double *
 }
 
 // ============================================================================================== CSR assembly
-extern "C" int pxb_csr_set_pattern(pxb_ctx *c, int ndof, const int *rowptr, const int *cols, long long nnz) {
-    PXB_TRY(need_geometry(c, "pxb_csr_set_pattern"));
-    if (ndof < 1 || ndof > 5 || !rowptr || !cols || nnz <= 0) return fail(PXB_ERR_INVALID, "pxb_csr_set_pattern: bad arguments");
-    if (rowptr[(size_t)c->g.n * ndof] != nnz) return fail(PXB_ERR_INVALID, "pxb_csr_set_pattern: rowptr[rows] != nnz");
+namespace pxb {
+// the slot map, diagonal slots, exact-pattern flags and value buffers of the pattern in c->csr (rowptr, cols, ndof,
+// nnz set on the device)
+int csr_finish(pxb_ctx *c, const char *who) {
     CsrState &k = c->csr;
-    k = CsrState{};
-    k.ndof = ndof;
-    k.nnz = nnz;
+    const int ndof = k.ndof;
     const size_t rows = (size_t)c->g.n * ndof;
-    PXB_TRY(dev_upload(c, k.rowptr, rowptr, sizeof(int) * (rows + 1)));
-    PXB_TRY(dev_upload(c, k.cols, cols, sizeof(int) * (size_t)nnz));
     PXB_TRY(dev_alloc(c, k.slot, sizeof(int) * (size_t)std::max(1LL, c->g.nb) * ndof * ndof));
     PXB_TRY(dev_alloc(c, k.diag, sizeof(int) * (size_t)c->g.n * ndof * ndof));
     PXB_TRY(dev_alloc(c, k.extra, sizeof(int) * (size_t)c->g.n * ndof * ndof));
@@ -1176,19 +1172,97 @@ extern "C" int pxb_csr_set_pattern(pxb_ctx *c, int ndof, const int *rowptr, cons
     PXB_TRY(sync(c));
     const int missing = flags[0];
     k.exact = flags[1] == 0;
-    if (ndof == 2 && block_view(c->g.n, rowptr, cols, k.h_bptr, k.h_bcol)) {
-        PXB_TRY(dev_upload(c, k.bptr, k.h_bptr.data(), sizeof(int) * k.h_bptr.size()));
-        PXB_TRY(dev_upload(c, k.bcol, k.h_bcol.data(), sizeof(int) * std::max<size_t>(1, k.h_bcol.size())));
-        k.blocked2 = true;
-    }
-    if (missing) return fail(PXB_ERR_INVALID, "pxb_csr_set_pattern: pattern lacks " + std::to_string(missing) +
+    if (missing) return fail(PXB_ERR_INVALID, std::string(who) + ": pattern lacks " + std::to_string(missing) +
                                                   " entries required by the families");
-    PXB_TRY(dev_alloc(c, k.kvals, sizeof(double) * (size_t)nnz));
+    PXB_TRY(dev_alloc(c, k.kvals, sizeof(double) * (size_t)k.nnz));
     PXB_TRY(dev_alloc(c, k.rhs, sizeof(double) * rows));
     PXB_TRY(dev_alloc(c, k.u, sizeof(double) * rows));
     PXB_TRY(dev_alloc(c, k.uold, sizeof(double) * rows));
     k.ready = true;
     return PXB_OK;
+}
+}  // namespace pxb
+
+extern "C" int pxb_csr_set_pattern(pxb_ctx *c, int ndof, const int *rowptr, const int *cols, long long nnz) {
+    PXB_TRY(need_geometry(c, "pxb_csr_set_pattern"));
+    if (ndof < 1 || ndof > 5 || !rowptr || !cols || nnz <= 0) return fail(PXB_ERR_INVALID, "pxb_csr_set_pattern: bad arguments");
+    if (rowptr[(size_t)c->g.n * ndof] != nnz) return fail(PXB_ERR_INVALID, "pxb_csr_set_pattern: rowptr[rows] != nnz");
+    CsrState &k = c->csr;
+    k = CsrState{};
+    k.ndof = ndof;
+    k.nnz = nnz;
+    const size_t rows = (size_t)c->g.n * ndof;
+    PXB_TRY(dev_upload(c, k.rowptr, rowptr, sizeof(int) * (rows + 1)));
+    PXB_TRY(dev_upload(c, k.cols, cols, sizeof(int) * (size_t)nnz));
+    if (ndof == 2 && block_view(c->g.n, rowptr, cols, k.h_bptr, k.h_bcol)) {
+        PXB_TRY(dev_upload(c, k.bptr, k.h_bptr.data(), sizeof(int) * k.h_bptr.size()));
+        PXB_TRY(dev_upload(c, k.bcol, k.h_bcol.data(), sizeof(int) * std::max<size_t>(1, k.h_bcol.size())));
+        k.blocked2 = true;
+    }
+    return csr_finish(c, "pxb_csr_set_pattern");
+}
+
+extern "C" int pxb_csr_build_pattern(pxb_ctx *c, int ndof, long long *nnz) {
+    PXB_TRY(need_geometry(c, "pxb_csr_build_pattern"));
+    if (ndof < 1 || ndof > 5) return fail(PXB_ERR_INVALID, "pxb_csr_build_pattern: ndof must be 1..5");
+    const int n = c->g.n;
+    if (n < 1) return fail(PXB_ERR_INVALID, "pxb_csr_build_pattern: no nodes");
+    CsrState &k = c->csr;
+    k = CsrState{};
+    k.ndof = ndof;
+    DevBuf count, first, bsum, small;
+    PXB_TRY(dev_alloc(c, count, sizeof(int) * (size_t)n));
+    PXB_TRY(dev_alloc(c, first, sizeof(long long) * ((size_t)n + 1)));
+    PXB_TRY(dev_alloc(c, bsum, sizeof(long long) * (size_t)pattern_scan_blocks(n)));
+    PXB_TRY(dev_alloc(c, small, 16));
+    PXB_CUDA_TRY(cudaMemsetAsync(small.p, 0, 16, c->stream));
+    PatternArgs a;
+    a.n = n;
+    a.ndof = ndof;
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.mirror = c->g.mirror.p ? c->g.mirror.as<int>() : nullptr;
+    a.count = count.as<int>();
+    a.first = first.as<long long>();
+    a.overflow = reinterpret_cast<int *>(small.as<char>() + 8);
+    PXB_CUDA_TRY(launch_pattern_count(a, bsum.as<long long>(), small.as<long long>(), c->stream));
+    c->launches += 4;
+    long long h[2] = {0, 0};
+    PXB_TRY(d2h(c, h, small.p, 16));
+    PXB_TRY(sync(c));
+    const long long blocks = h[0];
+    const int overflow = static_cast<int>(h[1] & 0xffffffffLL);
+    if (overflow)
+        return fail(PXB_ERR_UNSUPPORTED, "pxb_csr_build_pattern: " + std::to_string(overflow) +
+                                             " nodes have more than 256 column nodes (use pxb_csr_pattern)");
+    const long long total = blocks * ndof * ndof;
+    if (total > std::numeric_limits<int>::max())
+        return fail(PXB_ERR_INVALID, "pxb_csr_build_pattern: nnz exceeds 2^31-1");
+    k.nnz = total;
+    PXB_TRY(dev_alloc(c, k.rowptr, sizeof(int) * ((size_t)n * ndof + 1)));
+    PXB_TRY(dev_alloc(c, k.cols, sizeof(int) * (size_t)std::max(1LL, total)));
+    if (ndof == 2) {
+        PXB_TRY(dev_alloc(c, k.bptr, sizeof(int) * ((size_t)n + 1)));
+        PXB_TRY(dev_alloc(c, k.bcol, sizeof(int) * (size_t)std::max(1LL, blocks)));
+        a.bptr = k.bptr.as<int>();
+        a.bcol = k.bcol.as<int>();
+        k.blocked2 = true;
+    }
+    a.rowptr = k.rowptr.as<int>();
+    a.cols = k.cols.as<int>();
+    PXB_CUDA_TRY(launch_pattern_fill(a, c->stream));
+    c->launches++;
+    PXB_TRY(csr_finish(c, "pxb_csr_build_pattern"));
+    if (nnz) *nnz = total;
+    return PXB_OK;
+}
+
+extern "C" int pxb_csr_get_pattern(pxb_ctx *c, int *rowptr, int *cols) {
+    if (!c || !c->csr.ready) return fail(PXB_ERR_STATE, "pxb_csr_get_pattern: no pattern set");
+    const CsrState &k = c->csr;
+    if (rowptr) PXB_TRY(d2h(c, rowptr, k.rowptr.p, sizeof(int) * ((size_t)c->g.n * k.ndof + 1)));
+    if (cols) PXB_TRY(d2h(c, cols, k.cols.p, sizeof(int) * (size_t)k.nnz));
+    return sync(c);
 }
 
 extern "C" int pxb_assemble_scalar_d(pxb_ctx *c, int type, double coef, double f, const double *f_node_d, double dt,

@@ -191,6 +191,14 @@ int dot_into(RunCtx &r, long long len, const double *a, const double *b, int k) 
 int ensure_transpose(pxb_ctx *c) {
     CsrState &k = c->csr;
     if (!k.transposed) {
+        if (k.h_bptr.empty()) {  // a pattern built on the device: its block view comes to the host once
+            k.h_bptr.resize((size_t)c->g.n + 1);
+            PXB_TRY(d2h(c, k.h_bptr.data(), k.bptr.p, sizeof(int) * k.h_bptr.size()));
+            PXB_TRY(sync(c));
+            k.h_bcol.resize((size_t)k.h_bptr.back());
+            if (!k.h_bcol.empty()) PXB_TRY(d2h(c, k.h_bcol.data(), k.bcol.p, sizeof(int) * k.h_bcol.size()));
+            PXB_TRY(sync(c));
+        }
         std::vector<int> tbptr, tbcol, perm;
         block_transpose(c->g.n, k.h_bptr, k.h_bcol, tbptr, tbcol, perm);
         PXB_TRY(dev_upload(c, k.tbptr, tbptr.data(), sizeof(int) * tbptr.size()));

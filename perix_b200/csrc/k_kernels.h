@@ -344,6 +344,20 @@ struct ChAdjArgs {
     const double *lap = nullptr, *vol = nullptr, *u = nullptr, *x = nullptr;
     double *y = nullptr;
 };
+// CSR sparsity pattern on the device (k_pattern.cu): count pass with the node-list scan, then the fill
+struct PatternArgs {
+    int n = 0, ndof = 1;
+    const int *off = nullptr, *nbr = nullptr;  // families, nbr 0-based
+    const int *mirror = nullptr;               // 1-based mirror node, 0 none (may be NULL)
+    int *count = nullptr;                      // [n] unique column nodes per node
+    long long *first = nullptr;                // [n+1] exclusive scan of count
+    int *overflow = nullptr;                   // nodes whose list exceeds the sort capacity
+    int *rowptr = nullptr, *cols = nullptr;    // fill: [n*ndof+1], [nnz]
+    int *bptr = nullptr, *bcol = nullptr;      // fill, optional: block view [n+1], [sum count]
+};
+int pattern_scan_blocks(int n);  // long longs of the scan's block-sum scratch
+cudaError_t launch_pattern_count(const PatternArgs &a, long long *bsum, long long *total, cudaStream_t s);
+cudaError_t launch_pattern_fill(const PatternArgs &a, cudaStream_t s);
 // device-resident BiCGStab (k_bicg.cu): one cooperative kernel per solve, the host reads the outcome
 enum BicgStatus : int { kBicgRunning = 0, kBicgDone = 2, kBicgBreakdown = 3, kBicgMaxIts = 4 };
 constexpr int kBicgParts = 148 * 8;  // most blocks of the solve kernel (one partial sum slot each)
