@@ -632,8 +632,8 @@ extern "C" int pxb_epf_setup(pxb_ctx *c, int precision, double C11, double C12, 
     PXB_TRY(dev_alloc(c, e.u[0], sizeof(double) * ((size_t)g.n * g.dim + 8)));
     PXB_TRY(dev_alloc(c, e.u[1], sizeof(double) * ((size_t)g.n * g.dim + 8)));
     PXB_TRY(dev_alloc(c, e.accel, sizeof(double) * (size_t)g.n * g.dim));
-    PXB_TRY(dev_alloc(c, e.counters, sizeof(unsigned long long) * 4));
-    PXB_CUDA_TRY(cudaMemsetAsync(e.counters.p, 0, sizeof(unsigned long long) * 4, c->stream));
+    PXB_TRY(dev_alloc(c, e.counters, sizeof(unsigned long long) * 6));
+    PXB_CUDA_TRY(cudaMemsetAsync(e.counters.p, 0, sizeof(unsigned long long) * 6, c->stream));
     PXB_CUDA_TRY(cudaMemsetAsync(e.u[0].p, 0, e.u[0].bytes, c->stream));
     PXB_CUDA_TRY(cudaMemsetAsync(e.u[1].p, 0, e.u[1].bytes, c->stream));
     if (health0) PXB_TRY(h2d(c, e.health.p, health0, (size_t)g.nb));
@@ -661,18 +661,23 @@ extern "C" int pxb_epf_rate(pxb_ctx *c, const double *u, double *accel, long lon
     if (!u || !accel) return fail(PXB_ERR_INVALID, "pxb_epf_rate: NULL buffer");
     EpfState &e = c->epf;
     const size_t nd = (size_t)c->g.n * c->g.dim;
+    PXB_TRY(ensure_pinned(e.rate_h, sizeof(unsigned long long) * 5));
+    unsigned long long *cnt = e.counters.as<unsigned long long>();
     PXB_TRY(h2d(c, e.u[e.cur].p, u, sizeof(double) * nd));
-    unsigned long long before = 0, after = 0;
-    PXB_TRY(d2h(c, &before, e.counters.p, 8));
+    // the broken-bond count before the kernel, snapshot on the device: one host synchronisation per call
+    PXB_CUDA_TRY(cudaMemcpyAsync(cnt + 4, cnt, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, c->stream));
     EpfArgs a = epf_args(c);
     a.u = e.u[e.cur].as<double>();
     a.accel = e.accel.as<double>();
     launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_RATE, e.variant, c->stream);
     PXB_TRY(check_launch(c, "epf rate"));
     PXB_TRY(d2h(c, accel, e.accel.p, sizeof(double) * nd));
-    PXB_TRY(d2h(c, &after, e.counters.p, 8));
+    unsigned long long *h = static_cast<unsigned long long *>(e.rate_h.p);
+    PXB_TRY(d2h(c, h, cnt, sizeof(unsigned long long) * 5));
     PXB_TRY(sync(c));
-    if (n_broken) *n_broken = (long long)(after - before);
+    const unsigned int werr = static_cast<unsigned int>(h[2] & 0xffffffffULL);
+    if (werr) return fail(PXB_ERR_CUDA, "explicit rate: a staged-copy wait ran out (" + std::to_string(werr) + " blocks)");
+    if (n_broken) *n_broken = (long long)(h[0] - h[4]);
     return PXB_OK;
 }
 

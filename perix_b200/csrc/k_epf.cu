@@ -706,7 +706,12 @@ int epf_tma_maxb(int dim, int variant, int max_family) {
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s) {
     if (epf_is_tma(variant)) {
         if (mode == EPF_STEP) return launch_epf_tma(a, dim, mixed, variant - 5, s);
-        variant = 1;  // the staged kernel implements the time step only; other modes use the lane-group kernel
+        if (mode == EPF_RATE && a.accel) {
+            EpfArgs r = a;
+            r.rate = 1;
+            return launch_epf_tma(r, dim, mixed, variant - 5, s);
+        }
+        variant = 1;  // the staged kernel implements the step and the rate; START / FORCE_FROZEN use variant 1
     }
     if (dim == 2) return mixed ? launch_dm<2, true>(a, mode, variant, s) : launch_dm<2, false>(a, mode, variant, s);
     return mixed ? launch_dm<3, true>(a, mode, variant, s) : launch_dm<3, false>(a, mode, variant, s);

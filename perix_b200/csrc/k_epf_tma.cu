@@ -193,7 +193,8 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     const unsigned stage_bytes = SL::bytes(maxb);
     const PosT *pos = static_cast<const PosT *>(a.pos);
     const GT *Pg = static_cast<const GT *>(a.P);
-    const double t_new = a.t_sched[a.step_in_chunk];
+    const double t_new = a.t_sched ? a.t_sched[a.step_in_chunk] : 0.0;
+    const bool rate = a.rate != 0;  // RATE: the acceleration out, no u^{n-1} stream, no BC pass
     const float sc_hi2f = (float)a.sc_hi2, sc_lo2f = (float)a.sc_lo2;
 
     const int ntiles = (a.n + NT - 1) / NT;
@@ -214,7 +215,8 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         const unsigned bytes_off = up16((unsigned)(cnt + 1) * 4u);
         const unsigned bytes_pos = (unsigned)cnt * SL::PS;
         const unsigned bytes_u = up16((unsigned)cnt * DIM * 8u);
-        const unsigned total = NC * bytes_g + bytes_n + bytes_h + bytes_off + bytes_pos + bytes_u * 2u +
+        const unsigned bytes_up = rate ? 0u : bytes_u;
+        const unsigned total = NC * bytes_g + bytes_n + bytes_h + bytes_off + bytes_pos + bytes_u + bytes_up +
                                (XS ? (unsigned)DIM * bytes_n : 0u);
         s_t0a[st] = t0a;
         s_last[st] = k;
@@ -228,7 +230,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         bulk_g2s(base + SL::off_off(maxb), a.off + n0, bytes_off, &bar[st]);
         bulk_g2s(base + SL::pos_off(maxb), pos + n0, bytes_pos, &bar[st]);
         bulk_g2s(base + SL::u_off(maxb), a.u + (size_t)n0 * DIM, bytes_u, &bar[st]);
-        bulk_g2s(base + SL::up_off(maxb), a.u_other + (size_t)n0 * DIM, bytes_u, &bar[st]);
+        if (!rate) bulk_g2s(base + SL::up_off(maxb), a.u_other + (size_t)n0 * DIM, bytes_up, &bar[st]);
         if constexpr (XS) {
 #pragma unroll
             for (int d = 0; d < DIM; ++d)
@@ -415,14 +417,19 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
             const int d = gl;
             const double acc = __ddiv_rn(__dadd_rn(pick_t<DIM>(L, d), a.b[d]), a.rho);
             const size_t kk = (size_t)i * DIM + d;
-            unew = __dadd_rn(__dsub_rn(__dmul_rn(2.0, pick_t<DIM>(ui, d)), sUp[li * DIM + d]), __dmul_rn(a.dt2, acc));
-            const bool owned = a.bc_own && ((a.bc_own[i] >> d) & 1);
-            if (!owned) {
-                a.u_other[kk] = unew;
-                umax = fmax(umax, fabs(unew));
+            if (rate) {
+                a.accel[kk] = acc;
+            } else {
+                unew = __dadd_rn(__dsub_rn(__dmul_rn(2.0, pick_t<DIM>(ui, d)), sUp[li * DIM + d]),
+                                 __dmul_rn(a.dt2, acc));
+                const bool owned = a.bc_own && ((a.bc_own[i] >> d) & 1);
+                if (!owned) {
+                    a.u_other[kk] = unew;
+                    umax = fmax(umax, fabs(unew));
+                }
             }
         }
-        if (a.bc_off) {
+        if (a.bc_off && !rate) {
             double un[DIM];
 #pragma unroll
             for (int d = 0; d < DIM; ++d) un[d] = __shfl_sync(kFull, unew, grp * LPN + d);
@@ -493,12 +500,20 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         configured = smem;
     }
-    int dev = 0, sms = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WPB * kWarp, smem);
+    // resident blocks for this shared-memory size, queried once per size (the per-step rate call launches
+    // outside any graph, where these queries would cost more than the launch)
+    static size_t cap_smem = 0;
+    static long long cap_blocks = 0;
+    if (cap_blocks == 0 || cap_smem != smem) {
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WPB * kWarp, smem);
+        cap_blocks = (long long)sms * (per_sm > 0 ? per_sm : 1);
+        cap_smem = smem;
+    }
     const long long ntiles = ((long long)a.n + NT - 1) / NT;
-    const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    const long long cap = cap_blocks;
     const int grid = (int)(ntiles < cap ? ntiles : cap);
     k<<<grid > 0 ? grid : 1, WPB * kWarp, smem, s>>>(a);
     g_last_shape = LaunchShape{grid > 0 ? grid : 1, WPB * kWarp, smem};

@@ -147,6 +147,7 @@ struct EpfArgs {
     unsigned long long *n_broken = nullptr; // broken-bond counter
     int maxb = 0;                           // TMA variants: staged bonds per tile (multiple of 32)
     unsigned int *err = nullptr;            // TMA variants: pipeline waits that ran out
+    int rate = 0;                           // TMA variants: RATE mode (accel out; u_other and BCs unused)
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
 constexpr int kEpfTmaConfigs = 13;                // staged (TMA) configurations per dimension

@@ -120,7 +120,9 @@ struct EpfState {
     DevBuf health;     // uint8 [ldb] (zero tail)
     DevBuf u[2];       // double [n*dim + 8] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
     DevBuf accel;      // double [n*dim]
-    DevBuf counters;   // unsigned long long [4]: [0] broken bonds, [2] staged-kernel wait failures (u32)
+    DevBuf counters;   // unsigned long long [6]: [0] broken bonds, [2] staged-kernel wait failures (u32),
+                       // [4] broken bonds before the last rate call
+    PinnedBuf rate_h;  // host copy of counters[0..4] for the per-step rate call
     DevBuf umax;       // unsigned long long [chunk] per-step max |u| keys
     DevBuf tsched;     // double [chunk] t_{n+1} of each step in the chunk
     PinnedBuf tsched_h;
