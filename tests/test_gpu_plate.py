@@ -100,3 +100,30 @@ def _run_steps(ctx, w, u0, nsteps, precision, variant):
     ctx.epf_start(u0, None, w["dt"])
     ctx.epf_advance(nsteps, chunk=nsteps)
     return ctx.epf_state()
+
+
+@pytest.mark.parametrize("variant", list(range(5, N_VARIANTS)))
+def test_plate_rate_staged_matches_lane_group(ctx, plate, variant):
+    """The per-step rate call on every staged kernel (its RATE epilogue, many tiles per block at this size) gives the
+    bond breaks and the acceleration of the lane-group kernel (variant 1) from the same state: identical health and
+    breaks, acceleration within 1e-12."""
+    import perix_b200 as px
+    w, u0, u, uo, h = plate
+    L = w["L"]
+    C11, C12, C66 = w["C"]
+    ustate = u0 * 5.0  # enough stretch to break bonds in this call
+    out = []
+    for v in (1, variant):
+        ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
+        ctx.epf_setup(C11, C12, C66, w["rho"], (0.0, 0.0), w["sc"], True, health0=w["health0"])
+        try:
+            ctx.epf_set_variant(v)
+        except px.PxbError as e:
+            assert e.status == 7
+            pytest.skip("variant %d does not fit these families" % v)
+        a, nbk = ctx.epf_rate(ustate)
+        out.append((a, nbk, ctx.epf_state()[2].copy()))
+    (a1, n1, h1), (a2, n2, h2) = out
+    assert n1 > 0 and n1 == n2
+    assert np.array_equal(h1, h2)
+    assert np.abs(a2 - a1).max() <= 1e-12 * np.abs(a1).max()
