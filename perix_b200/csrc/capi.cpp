@@ -144,6 +144,23 @@ static int grid_nodes(int n, int threads) {
 static void destroy_graphs(EpfState &e) {
     for (auto &kv : e.graphs) cudaGraphExecDestroy(kv.second);
     e.graphs.clear();
+    if (e.rate_done) cudaEventDestroy(e.rate_done);
+    e.rate_done = nullptr;
+}
+
+// Waits for the work queued so far by polling an event from the calling thread: the per-step call's wait is short
+// (~0.1 ms) and a blocking or yielding synchronisation adds a wake-up latency of the same order on a loaded host.
+// After kSpinPolls polls it falls back to a blocking synchronisation.
+static int sync_polled(pxb_ctx *c, cudaEvent_t &ev) {
+    constexpr long kSpinPolls = 1L << 22;
+    if (!ev) PXB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    PXB_CUDA_TRY(cudaEventRecord(ev, c->stream));
+    for (long k = 0; k < kSpinPolls; ++k) {
+        const cudaError_t q = cudaEventQuery(ev);
+        if (q == cudaSuccess) return PXB_OK;
+        if (q != cudaErrorNotReady) return cuda_fail(q, "event poll");
+    }
+    return sync(c);
 }
 
 }  // namespace pxb
@@ -674,7 +691,7 @@ extern "C" int pxb_epf_rate(pxb_ctx *c, const double *u, double *accel, long lon
     PXB_TRY(d2h(c, accel, e.accel.p, sizeof(double) * nd));
     unsigned long long *h = static_cast<unsigned long long *>(e.rate_h.p);
     PXB_TRY(d2h(c, h, cnt, sizeof(unsigned long long) * 5));
-    PXB_TRY(sync(c));
+    PXB_TRY(sync_polled(c, e.rate_done));
     const unsigned int werr = static_cast<unsigned int>(h[2] & 0xffffffffULL);
     if (werr) return fail(PXB_ERR_CUDA, "explicit rate: a staged-copy wait ran out (" + std::to_string(werr) + " blocks)");
     if (n_broken) *n_broken = (long long)(h[0] - h[4]);

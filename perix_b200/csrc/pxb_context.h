@@ -123,6 +123,7 @@ struct EpfState {
     DevBuf counters;   // unsigned long long [6]: [0] broken bonds, [2] staged-kernel wait failures (u32),
                        // [4] broken bonds before the last rate call
     PinnedBuf rate_h;  // host copy of counters[0..4] for the per-step rate call
+    cudaEvent_t rate_done = nullptr;  // end of a rate call's work (polled by the host)
     DevBuf umax;       // unsigned long long [chunk] per-step max |u| keys
     DevBuf tsched;     // double [chunk] t_{n+1} of each step in the chunk
     PinnedBuf tsched_h;
