@@ -8,7 +8,8 @@ dt = 0.8 h / sqrt(C11/rho)).
 A step is one explicit time step (damage + Navier force + central difference + BC pass, one fused kernel),
 timed alone with CUDA events on the launching stream; the L2 is flushed (256 MiB write, then read back) before
 every timed step, and the state is restored from a snapshot taken 100 steps into the run every 100 steps, so every timed
-step works on the same physical regime (after ~200 further steps the plate's wall mode grows).
+step works on the same physical regime (about 200 steps later a wall mode of the reference scheme starts to grow on
+this plate, in the reference and here alike).
 Multi-GPU runs (torchrun) are independent replicas of the plate (weak scaling); the time is the max over ranks.
 Prints one JSON line on rank 0.
 """
@@ -33,7 +34,7 @@ S0 = 100               # steps run before the snapshot is taken
 
 
 # ------------------------------------------------------------------------------------------------- workload
-def c2_setup(px):
+def plate_setup(px):
     nx, ny, h = 400, 200, 5e-4
     L = px.lattice(2, nx, ny, 0, [0.0, nx * h, 0.0, ny * h])
     delta = 3.015 * L.dxyz[0] * (1.0 + 1e-6)
@@ -54,7 +55,7 @@ def c2_setup(px):
                 bcs=bcs, E=E, nu=nu, G0=G0, cracks=cracks, n=L.n, nb=int(off[-1]), h=h)
 
 
-def c5_setup(px, nx=120, ny=120, nz=24):
+def slab_setup(px, nx=120, ny=120, nz=24):
     """3D slab (120x120x24 bulk nodes + one ghost layer per face = 385,920 nodes), h = 1 mm, delta = 3.015h,
     E = 72 GPa, nu = 0.22, rho = 2440, s_c = 0.004 (G0 = s_c^2 6 E delta / 5), central edge notch of depth 20h
     as a force-only crack plane at y = Ly/2, zero Neumann on every ghost wall, then +-2 m/s y-velocity pins on
@@ -82,14 +83,14 @@ def c5_setup(px, nx=120, ny=120, nz=24):
                 bcs=bcs, E=E, nu=nu, n=L.n, nb=int(off[-1]), h=h)
 
 
-def c5_measure(px, device=0, steps=50, adjoint_steps=1000, checkpoint_every=100):
+def slab_measure(px, device=0, steps=50, adjoint_steps=1000, checkpoint_every=100):
     """The 3D slab: step throughput (FP64 and mixed, autotuned, CUDA events, L2 flushed, from the state after
     100 steps) and the frozen-mask adjoint d(misfit)/dE over the first `adjoint_steps` steps with checkpointed
     recomputation, checked against central finite differences of the device loop."""
     import torch
     from perix_b200.autograd import BcPlan, elastic_constants_t, explicit_loop, set_constants
     t0 = time.perf_counter()
-    w = c5_setup(px)
+    w = slab_setup(px)
     res = {"workload": "3D slab 120x120x24 (+ghosts), edge notch 20h", "nodes": w["n"], "bonds": w["nb"],
            "host_setup_s": time.perf_counter() - t0}
     L = w["L"]
@@ -162,8 +163,8 @@ def c5_measure(px, device=0, steps=50, adjoint_steps=1000, checkpoint_every=100)
     return res
 
 
-def c1_poisson(px, kvals, rhs, L, rowptr, cols):
-    """One static solve of the assembled C1 system (K dU = RHS from U = 0, the Newton step of a linear problem)
+def poisson_solve(px, kvals, rhs, L, rowptr, cols):
+    """One static solve of the assembled 64x64 Poisson system (K dU = RHS from U = 0, the Newton step of a linear problem)
     after the reference's Dirichlet row replacement on the ghost layer (DirichletBC.cpp:176-231: ghost row g
     becomes s*(dU_g + dU_b) = s*(2*0 - U_g - U_b), reflecting through the wall).  Host direct solve (the solve is
     not on the hot path); returns U and the relative L2 error against sin(pi x) sin(pi y) over the bulk nodes."""
@@ -184,7 +185,7 @@ def c1_poisson(px, kvals, rhs, L, rowptr, cols):
     return U, err
 
 
-def c1_measure(px, device=0, reps=20):
+def poisson_measure(px, device=0, reps=20):
     """The 64x64 Poisson workload: 64x64 cell-centred lattice on the unit square, delta = 3.015h, order 2, sigma = 1,
     f = 2 pi^2 sin(pi x) sin(pi y), reflected Dirichlet 0 on the four ghost groups.  FP64 g-build and Poisson
     assembly on the GPU (CUDA events), one host solve, L2 error; the reference's OpenMP assembly of the same
@@ -225,7 +226,7 @@ def c1_measure(px, device=0, reps=20):
     ev[1].record()
     torch.cuda.synchronize(dev)
     asm_ms = ev[0].elapsed_time(ev[1]) / reps
-    U, err = c1_poisson(px, kd.cpu().numpy(), rd.cpu().numpy(), L, rowptr, cols)
+    U, err = poisson_solve(px, kd.cpu().numpy(), rd.cpu().numpy(), L, rowptr, cols)
     res = {"nodes": L.n, "bonds": int(off[-1]), "nnz": int(rowptr[-1]), "gbuild_ms": gb_ms,
            "assembly_ms": asm_ms, "l2_rel_error_vs_exact": err}
     try:
@@ -242,7 +243,7 @@ def c1_measure(px, device=0, reps=20):
     return res
 
 
-def c4_measure(px, device=0, nside=256, nsteps=200, reps=20, fd=True):
+def ch_measure(px, device=0, nside=256, nsteps=200, reps=20, fd=True):
     """The 256x256 Cahn-Hilliard spinodal-decomposition workload: h = 1/256, delta = 3.015h, c0 = 0.5 + U(+-0.01)
     (seeded), chi = 2.5, M0 = 1, kappa = 1e-4, backward Euler dt = 1e-6 for 200 steps, mobility frozen per Newton
     iteration, zero Neumann on the four ghost walls.  Times the CH assembly kernel (CUDA events, L2 flushed) with
@@ -353,7 +354,7 @@ def c4_measure(px, device=0, nside=256, nsteps=200, reps=20, fd=True):
     return res
 
 
-def c3_clouds(px, nclouds=256, nmin=1000, nmax=200000, seed=2024, families=True):
+def clouds_generate(px, nclouds=256, nmin=1000, nmax=200000, seed=2024, families=True):
     """Batched-cloud workload: clouds alternate 2D / 3D (half each), node counts log-uniform in [nmin, nmax]
     (seeded), cell-centred lattice of spacing h = 1 mm jittered by U(-0.2h, 0.2h) per coordinate, no ghosts
     (families truncated at the cloud boundary), delta = 3.015h, unit-cell volumes, dx_char = h."""
@@ -497,7 +498,7 @@ def barrier(ws):
 
 def read_traffic(prec):
     """DRAM bytes per step-kernel launch from the committed ncu summary (None until captured)."""
-    path = os.path.join(ROOT, "profiles", "epf_step_c2_plate.md")
+    path = os.path.join(ROOT, "profiles", "epf_step_plate.md")
     if not os.path.exists(path):
         return None
     key = "traffic_bytes_per_launch_%s:" % prec
@@ -573,7 +574,7 @@ def run_reference_arm(args):
     if rank != 0:
         return
     import perix_b200 as px
-    w = c2_setup(px)
+    w = plate_setup(px)
     steps = max(1, args.steps)
     r = cpu_reference(w, steps, args.warmup)
     if r is None:
@@ -737,7 +738,7 @@ def run_perix(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import perix_b200 as px
-    w = c2_setup(px)
+    w = plate_setup(px)
     hbm, peak_kind = peaks()
     out = {}
     for prec in ("fp64", "mixed"):
@@ -767,17 +768,17 @@ def run_perix(args):
     traffic = read_traffic(head)
     e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, max(10, min(steps, 200)))
     cpu = None
-    c3 = c5 = refgpu = c1 = c4 = None
+    clouds = slab = refgpu = poisson = ch = None
     if rank == 0 and ws == 1:
         cpu = cpu_reference(w, 20, 2)
         for p in out.values():
             p["ctx"].close()
         if not args.headline_only:
-            c3 = c3_measure(px, device=local)
-            c5 = c5_measure(px, device=local)
+            clouds = clouds_measure(px, device=local)
+            slab = slab_measure(px, device=local)
             refgpu = reference_gpu()
-            c1 = c1_measure(px, device=local)
-            c4 = c4_measure(px, device=local)
+            poisson = poisson_measure(px, device=local)
+            ch = ch_measure(px, device=local)
     if rank != 0:
         return
     line = {
@@ -819,11 +820,11 @@ def run_perix(args):
                   "rel_err_vs_fp64_after_100_steps": err, "health_differs": hdiff, "autotune": out["mixed"]["tuned"]},
         "steady_state_graph": {"fp64": out["fp64"]["steady"], "mixed": out["mixed"]["steady"],
                                "note": "100-step CUDA-graph chunk, L2-warm (wall clock incl. host sync)"},
-        "batched_clouds": c3,
-        "slab_3d": c5,
+        "batched_clouds": clouds,
+        "slab_3d": slab,
         "reference_gpu": refgpu,
-        "poisson_c1": c1,
-        "cahn_hilliard_c4": c4,
+        "poisson_64x64": poisson,
+        "cahn_hilliard_256x256": ch,
         "gbuild_nodes_per_s": {"fp64": out["fp64"]["gbuild"], "mixed": out["mixed"]["gbuild"],
                                "ms": {"fp64": out["fp64"]["gbuild_ms"], "mixed": out["mixed"]["gbuild_ms"]},
                                "workload": "order-2 g-build of the same plate (81,200 nodes, all 5 operators stored)"},
@@ -836,14 +837,14 @@ def run_perix(args):
         dist.destroy_process_group()
 
 
-def c3_measure(px, nclouds=256, reps=3, device=0):
+def clouds_measure(px, nclouds=256, reps=3, device=0):
     """Batched clouds: one context holds every cloud; the g-build (FP64, then mixed) and the all-derivative apply
     are autotuned over their schedules and timed with CUDA events (L2 flushed before each launch).  Errors: the
     mixed g-functions and derivatives against the FP64 ones, and the FP64 derivatives of the random cubics
     against the exact ones (order-2 truncation error, reported, not a precision claim)."""
     import torch
     t0 = time.perf_counter()
-    clouds = c3_clouds(px, nclouds=nclouds, families=False)
+    clouds = clouds_generate(px, nclouds=nclouds, families=False)
     fields, exact = cubic_field(clouds)
     t_setup = time.perf_counter() - t0
     ctx = px.Context(device)
@@ -919,17 +920,17 @@ def run_profile(args):
     variant 1, then --steps timed steps of variant --variant from that state (so that variant's step kernel is
     the only kernel of its name launched); --profile gbuild: --steps order-2 g-builds."""
     import perix_b200 as px
-    w = c2_setup(px)
+    w = plate_setup(px)
     ctx = px.Context(0)
     L = w["L"]
     ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
-    if args.profile == "c5":
-        print(json.dumps({"profile": "c5", **c5_measure(px)}))
+    if args.profile == "slab":
+        print(json.dumps({"profile": "slab", **slab_measure(px)}))
         ctx.close()
         return
-    if args.profile == "c4":
+    if args.profile == "ch":
         ctx.close()
-        print(json.dumps({"profile": "c4", **c4_measure(px, nsteps=args.steps)}))
+        print(json.dumps({"profile": "ch", **ch_measure(px, nsteps=args.steps)}))
         return
     if args.profile == "refgpu":
         # the reference's own GPU explicit path (oracle/_ref/libperix_ref_cuda.so) on the plate and the slab,
@@ -940,7 +941,7 @@ def run_profile(args):
             print(json.dumps({"profile": "refgpu", "unavailable": "oracle/_ref/libperix_ref_cuda.so not built"}))
             return
         res = {"profile": "refgpu"}
-        for name, setup, dim in (("plate_2d", c2_setup, 2), ("slab_3d", c5_setup, 3)):
+        for name, setup, dim in (("plate_2d", plate_setup, 2), ("slab_3d", slab_setup, 3)):
             wv = setup(px)
             Lv = wv["L"]
             c = px.Context(0)
@@ -960,10 +961,10 @@ def run_profile(args):
                          "call_bond_updates_per_s": wv["nb"] / (call_ms * 1e-3)}
         print(json.dumps(res))
         return
-    if args.profile == "c5step":
+    if args.profile == "slabstep":
         # the 3D slab at --size x --size x 24: 100 steps of variant 1, then --steps timed steps of --variant
         ctx.close()
-        w5 = c5_setup(px, nx=args.size, ny=args.size, nz=24)
+        w5 = slab_setup(px, nx=args.size, ny=args.size, nz=24)
         L5 = w5["L"]
         ctx = px.Context(0)
         ctx.set_geometry(L5.coords, L5.vols, w5["off"], w5["ids"], w5["delta"], L5.dxyz[0], 3, mirror=L5.mirror)
@@ -978,16 +979,16 @@ def run_profile(args):
         ctx.epf_set_variant(args.variant)
         ms = np.zeros(args.steps, np.float32)
         time_steps(ctx, args.steps, ms)
-        print(json.dumps({"profile": "c5step", "size": args.size, "nodes": L5.n, "bonds": w5["nb"],
+        print(json.dumps({"profile": "slabstep", "size": args.size, "nodes": L5.n, "bonds": w5["nb"],
                           "precision": args.precision, "variant": args.variant, "ms_per_step": float(np.mean(ms[1:] if
                           ms.size > 1 else ms))}))
         ctx.close()
         return
-    if args.profile == "c3apply":
+    if args.profile == "cloudsapply":
         # --steps clouds (log-uniform 1k..200k nodes), one FP64 or mixed g-build, then 3 applies of schedule --variant
         ctx.close()
         import torch
-        clouds = c3_clouds(px, nclouds=args.steps, families=False)
+        clouds = clouds_generate(px, nclouds=args.steps, families=False)
         fields, _ = cubic_field(clouds)
         ctx = px.Context(0)
         ctx.batch_set_points(clouds)
@@ -998,12 +999,12 @@ def run_profile(args):
         u = torch.from_numpy(np.concatenate(fields)).to(dev)
         out = torch.empty(ctx.batch_out_len, dtype=torch.float64, device=dev)
         ms = ctx.batch_time(1, 3, FLUSH_BYTES, u.data_ptr(), out.data_ptr())
-        print(json.dumps({"profile": "c3apply", "clouds": args.steps, "nodes": ctx.batch_n, "bonds": ctx.batch_nb,
+        print(json.dumps({"profile": "cloudsapply", "clouds": args.steps, "nodes": ctx.batch_n, "bonds": ctx.batch_nb,
                           "precision": args.precision, "schedule": args.variant, "ms": [float(x) for x in ms]}))
         ctx.close()
         return
-    if args.profile == "c3":
-        print(json.dumps({"profile": "c3", **c3_measure(px, nclouds=args.steps)}))
+    if args.profile == "clouds":
+        print(json.dumps({"profile": "clouds", **clouds_measure(px, nclouds=args.steps)}))
         ctx.close()
         return
     if args.profile == "gbuild":
@@ -1033,7 +1034,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="perix", choices=["perix", "reference"])
-    ap.add_argument("--profile", choices=["step", "gbuild", "c3", "c5", "c5step", "c3apply", "refgpu", "c4"], default=None,
+    ap.add_argument("--profile", choices=["step", "gbuild", "clouds", "slab", "slabstep", "cloudsapply", "refgpu", "ch"], default=None,
                     help="run one kernel family only (for profiler captures); prints its own JSON line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--variant", type=int, default=8)

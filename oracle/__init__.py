@@ -1,6 +1,6 @@
 """Test infrastructure only: the oracle.
 
-Two CPU implementations of PeriX's PDDO hot path, used exclusively as checkers by ``tests/``,
+Two CPU implementations of PeriX's PDDO hot path, used only to check results in ``tests/``,
 ``__graft_entry__.smoke()`` and the CPU-baseline / reference legs of ``bench.py``:
 
 * ``port``  - ``oracle/_ref/libpddo_oracle.so``, a plain-C restatement (``oracle/pddo_oracle.c``);
@@ -9,7 +9,7 @@ Two CPU implementations of PeriX's PDDO hot path, used exclusively as checkers b
 
 plus ``oracle/_ref/libperix_ref_cuda.so``: the reference's own CUDA assembly translation unit compiled for
 sm_100a (``oracle/ref_cuda_harness.cu``), timed by ``bench.py`` as the GPU reference point and used by the GPU
-tests as a checker for the stress-coupled Cahn-Hilliard assembler.
+tests to check the stress-coupled Cahn-Hilliard assembler.
 
 The product (``perix_b200``) never imports this package.
 """

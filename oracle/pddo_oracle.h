@@ -1,5 +1,5 @@
 /* Test infrastructure only (the oracle).  A plain-C CPU restatement of PeriX's PDDO hot path, used by
- * tests/, the smoke check and bench.py's CPU-baseline leg as the checker.  The product never links it.
+ * tests/, the smoke check and bench.py's CPU-baseline leg to check results.  The product never links it.
  * Node ids are 1-based in family lists (reference convention); everything else is 0-based.
  * Each function cites the reference file:line whose algorithm it restates. */
 #ifndef PDDO_ORACLE_H

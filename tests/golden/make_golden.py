@@ -34,7 +34,7 @@ def mesh_arrays(m):
 
 
 def poisson_fixture():
-    """C1 at 16x16: sigma=1, f=2 pi^2 sin(pi x) sin(pi y), a random u."""
+    """The Poisson workload at 16x16: sigma=1, f=2 pi^2 sin(pi x) sin(pi y), a random u."""
     m = RefMesh.structured(2, 16, 16, 0, [0, 1, 0, 1], 3.015, 2)
     ops, deg = m.gbuild()
     rp1, cols1 = m.csr_pattern(1)
@@ -52,7 +52,7 @@ def poisson_fixture():
 
 
 def ch_fixture():
-    """Scaled C4: 32x32 lattice, h = 1/32, delta = 3.015h, c0 = 0.5 + U(-0.01, 0.01) (seeded), chi = 2.5,
+    """The Cahn-Hilliard workload scaled to a 32x32 lattice, h = 1/32, delta = 3.015h, c0 = 0.5 + U(-0.01, 0.01) (seeded), chi = 2.5,
     M0 = 1, kappa = 1e-4, dt = 1e-6; u = (c, mu) interleaved with mu = f'(c) plus noise; uold = u with c moved."""
     m = RefMesh.structured(2, 32, 32, 0, [0, 1, 0, 1], 3.015, 2)
     rp2, cols2 = m.csr_pattern(2)
@@ -164,7 +164,7 @@ def cubic(c, x, y, z, dim):
 
 
 def plate_bcs(m, dim, y_lo, y_hi, vx):
-    """C2-style BCs, in list order: zero Neumann on every ghost wall, then a prescribed x-velocity (direct
+    """The notched-plate BCs, in list order: zero Neumann on every ghost wall, then a prescribed x-velocity (direct
     pin) on the left ghosts between the slits (it overrides the Neumann copy there)."""
     bcs = [dict(kind="neumann", comps=list(range(dim)), nodes=m.group(g + "nodes_ghost"))
            for g in ("left", "right", "bottom", "top")]
@@ -174,7 +174,7 @@ def plate_bcs(m, dim, y_lo, y_hi, vx):
 
 
 def epf2d_fixture():
-    """Scaled C2: 40x20 plate, h=0.5 mm, two force-only slits of 5h at y = Ly/2 +- 2.5h, 16.5 m/s pull."""
+    """The notched plate scaled to 40x20 nodes, h=0.5 mm, two force-only slits of 5h at y = Ly/2 +- 2.5h, 16.5 m/s pull."""
     nx, ny, h = 40, 20, 5e-4
     Lx, Ly = nx * h, ny * h
     y1, y2 = Ly / 2 - 2.5 * h, Ly / 2 + 2.5 * h
@@ -207,7 +207,7 @@ def epf2d_fixture():
 
 
 def slab_bcs(m, Ly, h):
-    """C5-style BCs, in list order: zero Neumann on every ghost wall, then +-2 m/s y-velocity pins (direct) on
+    """The notched-slab BCs, in list order: zero Neumann on every ghost wall, then +-2 m/s y-velocity pins (direct) on
     every node (bulk and ghost) of the top and bottom three-layer strips."""
     bcs = [dict(kind="neumann", comps=[0, 1, 2], nodes=m.group(g + "nodes_ghost"))
            for g in ("left", "right", "bottom", "top", "back", "front")]
@@ -219,7 +219,7 @@ def slab_bcs(m, Ly, h):
 
 
 def epf3d_fixture():
-    """Scaled C5: 10x10x4 slab, h=1 mm, central edge notch plane (force-only), +-2 m/s on top/bottom layers."""
+    """The notched slab scaled to 10x10x4 nodes, h=1 mm, central edge notch plane (force-only), +-2 m/s on top/bottom layers."""
     nx, ny, nz, h = 10, 10, 4, 1e-3
     Lx, Ly, Lz = nx * h, ny * h, nz * h
     plane = [0.0, Ly / 2, -1.0, 3 * h, Ly / 2, -1.0, 3 * h, Ly / 2, 1.0, 0.0, Ly / 2, 1.0]

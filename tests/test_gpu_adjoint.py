@@ -114,12 +114,12 @@ def test_frozen_force_gradients(ctx, plate):
     a = frozen_force(ctx, u, C)
     (a * abar).sum().backward()
     u2 = u.detach().clone().requires_grad_(True)
-    C2 = C.detach().clone().requires_grad_(True)
-    aref = _torch_force(w, u2, C2)
+    C_ref = C.detach().clone().requires_grad_(True)
+    aref = _torch_force(w, u2, C_ref)
     (aref * abar).sum().backward()
     assert (a.detach() - aref.detach()).abs().max() <= 1e-12 * aref.abs().max()
     assert (u.grad - u2.grad).abs().max() <= 1e-10 * u2.grad.abs().max()
-    assert (C.grad - C2.grad).abs().max() <= 1e-10 * C2.grad.abs().max()
+    assert (C.grad - C_ref.grad).abs().max() <= 1e-10 * C_ref.grad.abs().max()
 
 
 def _device_final(ctx, w, E, u0):
@@ -234,9 +234,9 @@ def test_explicit_loop_full_plate_matches_device_loop(ctx):
     stream: the launches must be ordered with torch's work) against the fused device loop, 30 steps."""
     torch, dev = _torch()
     import perix_b200 as px
-    from bench import c2_setup
+    from bench import plate_setup
     from perix_b200.autograd import BcPlan, elastic_constants_t, explicit_loop, set_constants
-    w = c2_setup(px)
+    w = plate_setup(px)
     L = w["L"]
     ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
     C11, C12, C66 = w["C"]
@@ -257,9 +257,9 @@ def test_dJ_dE_3d_slab_against_finite_differences(ctx):
     """3D: a 16x16x6 slab with an edge notch and +-2 m/s pins, 40 steps, checkpoints every 10."""
     torch, dev = _torch()
     import perix_b200 as px
-    from bench import c5_setup
+    from bench import slab_setup
     from perix_b200.autograd import BcPlan, elastic_constants_t, explicit_loop, set_constants
-    w = c5_setup(px, nx=16, ny=16, nz=6)
+    w = slab_setup(px, nx=16, ny=16, nz=6)
     L = w["L"]
     nsteps = 40
     ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 3, mirror=L.mirror)

@@ -13,8 +13,8 @@ pytestmark = pytest.mark.gpu
 @pytest.fixture(scope="module")
 def batch(port):
     import perix_b200 as px
-    from bench import c3_clouds, cubic_field
-    clouds = c3_clouds(px, nclouds=12, nmin=300, nmax=4000, seed=11)
+    from bench import clouds_generate, cubic_field
+    clouds = clouds_generate(px, nclouds=12, nmin=300, nmax=4000, seed=11)
     u, exact = cubic_field(clouds, seed=3)
     ref_g, ref_d = [], []
     for c, f in zip(clouds, u):

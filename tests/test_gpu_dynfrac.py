@@ -1,7 +1,7 @@
 """Implicit PDDO dynamic-fracture assembly (pxb_assemble_cached; boundary of the reference's
 perix_cuda::assembleCached) against the reference's PDDODynamicFracElement (golden fixtures dynfrac2d/3d from
 tests/golden/make_golden.py): the element is initialised, commits one step (velocity history, bond failure by
-stretch: 22 % / 28 % of the bonds break) and is assembled at a perturbed state; this build gets the element's
+stretch: 22 % / 28 % of the bonds break) and is assembled at a perturbed state; perix_b200 gets the element's
 committed velocity (in a 3-slot node cache, the reference layout) and bond health.  Every K entry within 1e-12
 of the largest neighbour-block entry of its row, every rhs entry within 1e-12 of the largest bond term of its
 row or of the entry itself (the nodal inertia dominates)."""

@@ -1,7 +1,7 @@
 """GPU parity: perix_b200 kernels (through the C-ABI) against the golden fixtures made by the reference's own
 code and against the C restatement (oracle) at sizes it finishes in seconds.
 
-Tolerances (north_star): g-functions and operator applies within 1e-12 relative in FP64 (relative to the
+Tolerances: g-functions and operator applies within 1e-12 relative in FP64 (relative to the
 operator's own magnitude over the family); mixed precision within 1e-6; families/CSR bit-exact; damage sets
 identical except bonds whose stretch lies within 1e-9 of critical; explicit trajectories within 1e-10 relative
 (60 central-difference steps accumulate round-off from the reordered family sums)."""
@@ -43,7 +43,7 @@ def test_gbuild_mixed_within_1e6(ctx, name, dim):
     assert scaled_err(g, d["ops"], d["off"]) <= G_TOLMIX
 
 
-def test_gbuild_c1_full_size_vs_oracle(ctx, port):
+def test_gbuild_poisson64_full_size_vs_oracle(ctx, port):
     import perix_b200 as px
     L = px.lattice(2, 64, 64, 0, [0, 1, 0, 1])
     delta = 3.015 * L.dxyz[0] * (1 + 1e-6)
@@ -162,13 +162,13 @@ def test_ch_device_geometry_and_mobility(ctx):
     assert np.abs(rhs.cpu().numpy() - d["rhs"]).max() <= 1e-12 * np.abs(d["rhs"]).max()
 
 
-def test_c1_solve_l2_error(ctx, port):
+def test_poisson64_solve_l2_error(ctx, port):
     """The 64x64 Poisson problem end to end: 64x64 lattice, order 2, FP64 g-build and Poisson assembly on the GPU, the
     reference's Dirichlet row replacement on the ghost layer, one solve.  The solution matches the solve of the
     C restatement's assembly of the same system (1e-9) and the relative L2 error against sin(pi x) sin(pi y) is
     the reference's (1.44e-3 with the reference's own assembly, tests/test_oracle.py)."""
     import perix_b200 as px
-    from bench import c1_poisson
+    from bench import poisson_solve
     L = px.lattice(2, 64, 64, 0, [0.0, 1.0, 0.0, 1.0])
     delta = 3.015 * L.dxyz[0] * (1 + 1e-6)
     off, ids = px.families(L.coords, delta, False, mirror=L.mirror)
@@ -179,10 +179,10 @@ def test_c1_solve_l2_error(ctx, port):
     x, y = L.coords[0::3], L.coords[1::3]
     f = 2 * math.pi ** 2 * np.sin(math.pi * x) * np.sin(math.pi * y)
     kv, rhs = ctx.assemble_scalar(0, 1.0, np.zeros(L.n), f_node=f)
-    U, err = c1_poisson(px, kv, rhs, L, rowptr, cols)
+    U, err = poisson_solve(px, kv, rhs, L, rowptr, cols)
     g, _ = port.gbuild(2, 2, L.coords, L.vols, off, ids, delta, L.dxyz[0])
     kv_o, rhs_o = port.poisson_assemble(2, off, ids, g, [2, 4], 1.0, f, np.zeros(L.n), rowptr, cols)
-    U_o, err_o = c1_poisson(px, kv_o, rhs_o, L, rowptr, cols)
+    U_o, err_o = poisson_solve(px, kv_o, rhs_o, L, rowptr, cols)
     assert np.abs(U - U_o).max() <= 1e-9
     assert abs(err - 1.4357e-3) <= 1e-6 and abs(err - err_o) <= 1e-9
 
@@ -331,23 +331,23 @@ def test_central_difference_start(ctx):
 
 def _device_families_case(name):
     import perix_b200 as px
-    from bench import c3_clouds
+    from bench import clouds_generate
     if name == "plate2d":
-        from bench import c2_setup
-        w = c2_setup(px)
+        from bench import plate_setup
+        w = plate_setup(px)
         return w["L"].coords, w["L"].vols, w["delta"], 2, w["L"].mirror
     if name == "slab3d":
-        from bench import c5_setup
-        w = c5_setup(px, nx=30, ny=30, nz=10)
+        from bench import slab_setup
+        w = slab_setup(px, nx=30, ny=30, nz=10)
         return w["L"].coords, w["L"].vols, w["delta"], 3, w["L"].mirror
-    if name == "c1":
+    if name == "poisson64":
         L = px.lattice(2, 64, 64, 0, [0.0, 1.0, 0.0, 1.0])
         return L.coords, L.vols, 3.015 * L.dxyz[0] * (1 + 1e-6), 2, L.mirror
-    cl = c3_clouds(px, nclouds=2, nmin=3000, nmax=6000, seed=3)[0 if name == "cloud2d" else 1]
+    cl = clouds_generate(px, nclouds=2, nmin=3000, nmax=6000, seed=3)[0 if name == "cloud2d" else 1]
     return cl["coords3"], cl["vols"], cl["delta"], cl["dim"], None
 
 
-@pytest.mark.parametrize("name", ["plate2d", "slab3d", "c1", "cloud2d", "cloud3d"])
+@pytest.mark.parametrize("name", ["plate2d", "slab3d", "poisson64", "cloud2d", "cloud3d"])
 def test_device_families_equal_host(ctx, name):
     """Families built on the device (pxb_set_geometry_points) equal the host build (pxb_families, itself bit-equal
     to the reference's createNeighborNodes): same offsets, same ids in the same order."""

@@ -18,8 +18,8 @@ N_VARIANTS = 18
 @pytest.fixture(scope="module")
 def plate(port):
     import perix_b200 as px
-    from bench import c2_setup
-    w = c2_setup(px)
+    from bench import plate_setup
+    w = plate_setup(px)
     L = w["L"]
     rng = np.random.default_rng(7)
     u0 = rng.standard_normal(2 * L.n) * 2e-6

@@ -80,7 +80,7 @@ def _check(d, dim, kv, rhs, kr, rr):
 @pytest.mark.parametrize("dim", [2, 3])
 def test_stress_ch_fracture_and_inertia_vs_restatement(ctx, port, dim):
     """Broken bonds (kres) and backward-Euler inertia against the numpy restatement (oracle/stress_ch.py, pinned
-    to the reference element by tests/test_oracle.py) on this build's FP64 operators."""
+    to the reference element by tests/test_oracle.py) on perix_b200's FP64 operators."""
     from oracle.stress_ch import stress_ch_assemble
     d = load_golden("stressch%dd" % dim)
     p = _setup(ctx, d, dim)
@@ -95,7 +95,7 @@ def test_stress_ch_fracture_and_inertia_vs_restatement(ctx, port, dim):
 
 def test_stress_ch_2d_matches_reference_gpu(ctx):
     """The reference's own GPU assembler (its CUDA translation unit for sm_100a), plain and with broken bonds and
-    inertia (2D; on the 3D fixture the reference's GPU path disagrees with its own CPU element, which this build
+    inertia (2D; on the 3D fixture the reference's GPU path disagrees with its own CPU element, which perix_b200
     follows)."""
     from oracle import ref_cuda_available, ref_cuda_stress_ch
     if not ref_cuda_available():

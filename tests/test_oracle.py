@@ -173,7 +173,7 @@ def _ref():
     return RefMesh
 
 
-def test_vs_reference_c1_full(port):
+def test_vs_reference_poisson64_full(port):
     RefMesh = _ref()
     m = RefMesh.structured(2, 64, 64, 0, [0, 1, 0, 1], 3.015, 2)
     assert m.n == 4352 and m.nb == 117172
@@ -187,7 +187,7 @@ def test_vs_reference_c1_full(port):
     assert scaled_err(g, g_ref, off) <= 1e-12
 
 
-def test_vs_reference_c2_plate_families(port):
+def test_vs_reference_plate_families(port):
     RefMesh = _ref()
     h = 5e-4
     cracks = [[0.0, 0.05 - 25 * h, 50 * h, 0.05 - 25 * h], [0.0, 0.05 + 25 * h, 50 * h, 0.05 + 25 * h]]
@@ -208,12 +208,12 @@ def test_vs_reference_3d_slab_gbuild(port):
 
 
 @pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference harness not built here")
-def test_c1_solve_with_reference_assembly():
-    """C1 with the reference's own Poisson assembly: the relative L2 error of the solved field against
+def test_poisson64_solve_with_reference_assembly():
+    """The 64x64 Poisson workload with the reference's own Poisson assembly: the relative L2 error of the solved field against
     sin(pi x) sin(pi y) over the bulk nodes (the value the GPU path is held to)."""
     import math
     import perix_b200 as px
-    from bench import c1_poisson
+    from bench import poisson_solve
     from oracle import RefMesh
     m = RefMesh.structured(2, 64, 64, 0, [0, 1, 0, 1], 3.015, 2)
     m.gbuild()
@@ -222,7 +222,7 @@ def test_c1_solve_with_reference_assembly():
     kv, rhs, _ = m.poisson_assemble(1.0, f, np.zeros(m.n))
     rp, cols = m.csr_pattern(1)
     L = px.lattice(2, 64, 64, 0, [0.0, 1.0, 0.0, 1.0])
-    _, err = c1_poisson(px, kv, rhs, L, rp, cols)
+    _, err = poisson_solve(px, kv, rhs, L, rp, cols)
     assert abs(err - 1.4357e-3) <= 1e-6
 
 
