@@ -529,6 +529,11 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def plate_workload(nb):
+    """The workload name both arms report."""
+    return "explicit_pddo_frac 2D notched plate 400x200 (81,200 PD nodes, %d directed bonds), dt=0.8h/c" % nb
+
+
 # --------------------------------------------------------------------------------------------- reference arm
 def cpu_reference(w, steps, warmup, threads=None):
     """The reference's own OpenMP CPU path (oracle/_ref, built from the reference sources): per step the
@@ -585,8 +590,7 @@ def run_reference_arm(args):
             "unit": "bond-updates/s", "n_gpus": ws, "steps": steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * r["seconds"] / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "explicit_pddo_frac 2D notched plate 400x200 (81,200 PD nodes, %d bonds)" % r["nb"],
-                       "threads": r["cores"]},
+            "config": {"workload": plate_workload(r["nb"]), "nodes": w["n"], "bonds": r["nb"], "threads": r["cores"]},
             "cpu_baseline": {"value": r["value"], "unit": "bond-updates/s", "cores": r["cores"], "kind": "reference",
                              "sample": sample},
             "e2e": {"value": r["value"], "unit": "bond-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -709,6 +713,27 @@ def e2e_rate(px, ctx, w, steps):
     return float(np.median(rates)), n2 * 8, n2 * 8 + 16
 
 
+def pcie_copy_us(nbytes, device, reps=20):
+    """Device time (CUDA events, median of reps) of one pinned host->device and one device->host copy of nbytes:
+    the transfers inside each per-step call, measured alone on this machine's link."""
+    import torch
+    dev = torch.device("cuda", device)
+    h = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+    d = torch.empty(nbytes // 8, dtype=torch.float64, device=dev)
+    out = {}
+    for name, dst, src in (("h2d", d, h), ("d2h", h, d)):
+        ts = []
+        for _ in range(reps + 3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            dst.copy_(src, non_blocking=True)
+            b.record()
+            torch.cuda.synchronize(dev)
+            ts.append(a.elapsed_time(b) * 1e3)
+        out[name] = float(np.median(ts[3:]))
+    return out
+
+
 def mixed_error(px, w, device):
     """max|u_mixed - u_fp64| / max|u_fp64| after 100 graph-captured steps from the same 100-step state."""
     res = {}
@@ -767,6 +792,7 @@ def run_perix(args):
     achieved = B / mean_s / 1e9
     traffic = read_traffic(head)
     e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, max(10, min(steps, 200)))
+    copies = pcie_copy_us(h2d, local)
     cpu = None
     clouds = slab = refgpu = poisson = ch = None
     if rank == 0 and ws == 1:
@@ -795,12 +821,15 @@ def run_perix(args):
         "dtype": "f64",
         "precision": head + (" (f32 operator storage, f64 arithmetic and state)" if head == "mixed" else ""),
         "data": "synthetic",
-        "config": {"workload": "explicit_pddo_frac 2D notched plate 400x200 (81,200 PD nodes, %d directed bonds), "
-                               "dt=0.8h/c" % w["nb"],
+        "config": {"workload": plate_workload(w["nb"]),
                    "nodes": w["n"], "bonds": w["nb"], "parallelism": "replicas" if ws > 1 else "single-gpu",
                    "l2": "flushed before every timed step (256 MiB write, then the same 256 MiB read back)",
                    "state": "snapshot after %d steps, restored every %d steps" % (S0, EPISODE)},
         "e2e": {"value": ws * e2e, "unit": "bond-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "call_us": 1e6 * w["nb"] / e2e,
+                "pcie_copy_us": {"h2d": copies["h2d"], "d2h": copies["d2h"],
+                                 "note": "one pinned copy of the call's u (h2d) or acceleration (d2h) bytes alone, "
+                                         "CUDA events, median of 20: the link speed this machine gave"},
                 "api": "pxb_epf_rate (drop-in per-step call, pinned host u in / acceleration out)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "peak_kind": peak_kind,

@@ -53,13 +53,10 @@ struct Events {
     }
 };
 
-// carveout: see launch_l2_flush.  Before a staged step the flush asks for the maximum shared-memory carveout,
-// the split the staged kernels run with, so that the timed launch does not begin by reconfiguring the SMs' L1 /
-// shared memory, which a loop of consecutive steps never does.
-int flush_l2(pxb_ctx *c, size_t bytes, DevBuf &buf, int carveout = -1) {
+int flush_l2(pxb_ctx *c, size_t bytes, DevBuf &buf) {
     if (bytes == 0) return PXB_OK;
     if (buf.bytes < bytes) PXB_TRY(dev_alloc(c, buf, bytes));
-    PXB_CUDA_TRY(launch_l2_flush(buf.p, bytes, c->stream, carveout));
+    launch_l2_flush(buf.p, bytes, c->stream);
     return check_launch(c, "l2 flush");
 }
 
@@ -116,7 +113,7 @@ int timed_steps(pxb_ctx *c, int nsteps, size_t flush_bytes, int restore_every, c
         PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
         th[0] = e.t + e.dt;
         PXB_TRY(h2d(c, e.tsched.p, th, sizeof(double)));
-        PXB_TRY(flush_l2(c, flush_bytes, g_flush, epf_is_tma(e.variant) ? cudaSharedmemCarveoutMaxShared : -1));
+        PXB_TRY(flush_l2(c, flush_bytes, g_flush));
         EpfArgs a;
         PXB_TRY(step_args(c, e.cur, &a));
         PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)s], c->stream));
@@ -250,7 +247,7 @@ extern "C" int pxb_epf_launch_floor(pxb_ctx *c, size_t flush_bytes, int reps, fl
     Events ev;
     PXB_TRY(ev.make(2 * (size_t)reps));
     for (int r = 0; r < reps; ++r) {
-        PXB_TRY(flush_l2(c, flush_bytes, g_flush, cudaSharedmemCarveoutMaxShared));
+        PXB_TRY(flush_l2(c, flush_bytes, g_flush));
         PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r], c->stream));
         PXB_CUDA_TRY(launch_empty(sh.grid, sh.block, sh.smem, c->stream));
         PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r + 1], c->stream));

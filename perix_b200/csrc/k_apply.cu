@@ -368,18 +368,8 @@ cudaError_t launch_empty(int grid, int block, size_t smem, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_l2_flush(void *buf, size_t bytes, cudaStream_t s, int carveout) {
+cudaError_t launch_l2_flush(void *buf, size_t bytes, cudaStream_t s) {
     static unsigned seed = 1;
-    static int set_carveout = -2;
-    if (carveout != set_carveout) {
-        // the flush kernels use no shared memory; their carveout only decides which L1/shared split the SMs
-        // hold when the next (timed) kernel starts
-        cudaError_t e = cudaFuncSetAttribute(l2_flush_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(l2_flush_read_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
-        if (e != cudaSuccess) return e;
-        set_carveout = carveout;
-    }
     l2_flush_kernel<<<1184, 256, 0, s>>>(static_cast<uint4 *>(buf), bytes / 16, seed);
     l2_flush_read_kernel<<<1184, 256, 0, s>>>(static_cast<uint4 *>(buf), bytes / 16, seed++);
     return cudaGetLastError();

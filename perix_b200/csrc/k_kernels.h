@@ -232,9 +232,7 @@ cudaError_t launch_ids_to0(long long nb, const int *ids1, int *ids0, cudaStream_
 cudaError_t launch_health_from_double(long long nb, const double *h, uint8_t *out, cudaStream_t s);
 cudaError_t launch_health_to_double(long long nb, const uint8_t *h, double *out, cudaStream_t s);
 cudaError_t launch_count_zero(long long nb, const uint8_t *h, unsigned long long *count, cudaStream_t s);
-// carveout: the flush kernels' preferred shared-memory carveout (cudaFuncAttributePreferredSharedMemoryCarveout,
-// -1 = no preference)
-cudaError_t launch_l2_flush(void *buf, size_t bytes, cudaStream_t s, int carveout = -1);
+cudaError_t launch_l2_flush(void *buf, size_t bytes, cudaStream_t s);
 
 // ------------------------------------------------------------------------------------------------ CSR assembly
 struct CsrMapArgs {
