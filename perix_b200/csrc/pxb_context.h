@@ -124,6 +124,12 @@ struct EpfState {
                        // [4] broken bonds before the last rate call
     PinnedBuf rate_h;  // host copy of counters[0..4] for the per-step rate call
     cudaEvent_t rate_done = nullptr;  // end of a rate call's work (polled by the host)
+    // the per-step rate call captured as one graph for one pair of pinned host buffers (u in, acceleration out),
+    // the state slot u[cur] and the schedule variant; rate_last_* are the buffers of the previous call
+    cudaGraphExec_t rate_graph = nullptr;
+    const void *rate_u = nullptr, *rate_last_u = nullptr;
+    void *rate_a = nullptr, *rate_last_a = nullptr;
+    int rate_cur = -1, rate_variant = -1;
     DevBuf umax;       // unsigned long long [chunk] per-step max |u| keys
     DevBuf tsched;     // double [chunk] t_{n+1} of each step in the chunk
     PinnedBuf tsched_h;
