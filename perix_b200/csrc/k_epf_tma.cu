@@ -70,6 +70,23 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
                  : "memory");
 }
 
+// the same copy with an L2 cache-policy operand (createpolicy): the bond streams are read once per step, so they
+// go in as evict-first and leave the node rows the neighbour gathers reuse resident in L2
+__device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, unsigned bytes, unsigned long long *bar,
+                                              unsigned long long policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+
+__device__ __forceinline__ unsigned long long policy_evict_first() {
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
@@ -222,11 +239,12 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         s_last[st] = k;
         fence_proxy_async();
         mbar_arrive_expect_tx(&bar[st], total);
+        const unsigned long long ef = policy_evict_first();
 #pragma unroll
         for (int c = 0; c < NC; ++c)
-            bulk_g2s(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st]);
-        bulk_g2s(base + SL::nbr_off(maxb), a.nbr + t0a, bytes_n, &bar[st]);
-        bulk_g2s(base + SL::h_off(maxb), a.health + t0a, bytes_h, &bar[st]);
+            bulk_g2s_hint(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st], ef);
+        bulk_g2s_hint(base + SL::nbr_off(maxb), a.nbr + t0a, bytes_n, &bar[st], ef);
+        bulk_g2s_hint(base + SL::h_off(maxb), a.health + t0a, bytes_h, &bar[st], ef);
         bulk_g2s(base + SL::off_off(maxb), a.off + n0, bytes_off, &bar[st]);
         bulk_g2s(base + SL::pos_off(maxb), pos + n0, bytes_pos, &bar[st]);
         bulk_g2s(base + SL::u_off(maxb), a.u + (size_t)n0 * DIM, bytes_u, &bar[st]);
@@ -234,8 +252,8 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         if constexpr (XS) {
 #pragma unroll
             for (int d = 0; d < DIM; ++d)
-                bulk_g2s(base + SL::xi_off(maxb) + (size_t)d * maxb * 4u, a.xib + (size_t)d * a.nb + t0a, bytes_n,
-                         &bar[st]);
+                bulk_g2s_hint(base + SL::xi_off(maxb) + (size_t)d * maxb * 4u, a.xib + (size_t)d * a.nb + t0a,
+                              bytes_n, &bar[st], ef);
         }
     };
 
