@@ -623,6 +623,7 @@ static EpfArgs epf_args(pxb_ctx *c) {
     a.P = e.P.p;
     a.xib = e.xib.p ? e.xib.as<float>() : nullptr;
     if (epf_is_tma(e.variant)) a.maxb = epf_tma_maxb(g.dim, e.variant, g.max_family);
+    a.evict_first = e.evict_first ? 1 : 0;
     return a;
 }
 
@@ -673,6 +674,12 @@ extern "C" int pxb_epf_setup(pxb_ctx *c, int precision, double C11, double C12, 
                                          e.xib.as<float>(), c->stream));
         PXB_TRY(check_launch(c, "bond vectors"));
     }
+    // Bond streams larger than the L2 are staged as evict-first, so that the node rows the neighbour gathers reuse
+    // stay resident; streams that fit are left to stay in L2 from one step to the next.
+    int l2 = 0;
+    PXB_CUDA_TRY(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, c->device));
+    const size_t stream_bytes = ldb * (es * nc + 5 + (precision == PXB_MIXED ? 4 * (size_t)g.dim : 0));
+    e.evict_first = stream_bytes > (size_t)l2;
     e.ready = true;
     return PXB_OK;
 }
@@ -1019,11 +1026,12 @@ int step_args(pxb_ctx *c, int par, EpfArgs *out) {
 }  // namespace pxb
 
 // one STEP launch on stream s: reads u[par], writes u[par^1]
-static int launch_step(pxb_ctx *c, int par, int q, cudaStream_t s) {
+static int launch_step(pxb_ctx *c, int par, int q, cudaStream_t s, bool pdl = false) {
     EpfState &e = c->epf;
     EpfArgs a;
     step_args(c, par, &a);
     a.step_in_chunk = q;
+    a.pdl = pdl ? 1 : 0;
     const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_STEP, e.variant, s);
     if (err != cudaSuccess) return cuda_fail(err, "epf step launch");
     return PXB_OK;
@@ -1039,7 +1047,7 @@ static int get_graph(pxb_ctx *c, int steps, cudaGraphExec_t *out) {
     PXB_CUDA_TRY(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
     int par = e.cur, st = PXB_OK;
     for (int q = 0; q < steps && st == PXB_OK; ++q) {
-        st = launch_step(c, par, q, c->own);
+        st = launch_step(c, par, q, c->own, /*pdl=*/q > 0);
         par ^= 1;
     }
     cudaError_t ce = cudaStreamEndCapture(c->own, &graph);

@@ -70,8 +70,8 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
                  : "memory");
 }
 
-// the same copy with an L2 cache-policy operand (createpolicy): the bond streams are read once per step, so they
-// go in as evict-first and leave the node rows the neighbour gathers reuse resident in L2
+// the same copy with an L2 cache-policy operand (createpolicy): bond streams larger than the L2 are read once per
+// step, so they go in as evict-first and leave the node rows the neighbour gathers reuse resident in L2
 __device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, unsigned bytes, unsigned long long *bar,
                                               unsigned long long policy) {
     asm volatile(
@@ -210,7 +210,6 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     const unsigned stage_bytes = SL::bytes(maxb);
     const PosT *pos = static_cast<const PosT *>(a.pos);
     const GT *Pg = static_cast<const GT *>(a.P);
-    const double t_new = a.t_sched ? a.t_sched[a.step_in_chunk] : 0.0;
     const bool rate = a.rate != 0;  // RATE: the acceleration out, no u^{n-1} stream, no BC pass
     const float sc_hi2f = (float)a.sc_hi2, sc_lo2f = (float)a.sc_lo2;
 
@@ -239,12 +238,20 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         s_last[st] = k;
         fence_proxy_async();
         mbar_arrive_expect_tx(&bar[st], total);
-        const unsigned long long ef = policy_evict_first();
+        if (a.evict_first) {
+            const unsigned long long ef = policy_evict_first();
 #pragma unroll
-        for (int c = 0; c < NC; ++c)
-            bulk_g2s_hint(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st], ef);
-        bulk_g2s_hint(base + SL::nbr_off(maxb), a.nbr + t0a, bytes_n, &bar[st], ef);
-        bulk_g2s_hint(base + SL::h_off(maxb), a.health + t0a, bytes_h, &bar[st], ef);
+            for (int c = 0; c < NC; ++c)
+                bulk_g2s_hint(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st], ef);
+            bulk_g2s_hint(base + SL::nbr_off(maxb), a.nbr + t0a, bytes_n, &bar[st], ef);
+            bulk_g2s_hint(base + SL::h_off(maxb), a.health + t0a, bytes_h, &bar[st], ef);
+        } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                bulk_g2s(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st]);
+            bulk_g2s(base + SL::nbr_off(maxb), a.nbr + t0a, bytes_n, &bar[st]);
+            bulk_g2s(base + SL::h_off(maxb), a.health + t0a, bytes_h, &bar[st]);
+        }
         bulk_g2s(base + SL::off_off(maxb), a.off + n0, bytes_off, &bar[st]);
         bulk_g2s(base + SL::pos_off(maxb), pos + n0, bytes_pos, &bar[st]);
         bulk_g2s(base + SL::u_off(maxb), a.u + (size_t)n0 * DIM, bytes_u, &bar[st]);
@@ -252,8 +259,12 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         if constexpr (XS) {
 #pragma unroll
             for (int d = 0; d < DIM; ++d)
-                bulk_g2s_hint(base + SL::xi_off(maxb) + (size_t)d * maxb * 4u, a.xib + (size_t)d * a.nb + t0a,
-                              bytes_n, &bar[st], ef);
+                if (a.evict_first)
+                    bulk_g2s_hint(base + SL::xi_off(maxb) + (size_t)d * maxb * 4u, a.xib + (size_t)d * a.nb + t0a,
+                                  bytes_n, &bar[st], policy_evict_first());
+                else
+                    bulk_g2s(base + SL::xi_off(maxb) + (size_t)d * maxb * 4u, a.xib + (size_t)d * a.nb + t0a,
+                             bytes_n, &bar[st]);
         }
     };
 
@@ -266,14 +277,21 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         s_fail = 0;
         fence_mbar_init();
     }
+    // launched with programmatic serialisation (a captured loop of steps), the next step may start its blocks now:
+    // they only run the set-up above their wait while this grid's blocks finish
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     // the bond ranges of the block's first tiles, all loaded at once: a refill then issues its copies without
-    // first waiting on a global load
+    // first waiting on a global load (family offsets never change during a run)
     for (int k = tid; k < mycount && k < kTileDesc; k += WPB * kWarp) {
         const int n0 = ((int)blockIdx.x + k * (int)gridDim.x) * NT;
         s_d0[k] = __ldg(a.off + n0);
         s_d1[k] = __ldg(a.off + min(n0 + NT, a.n));
     }
     __syncthreads();
+    // nothing a previous step writes (u, health, counters) is read before this point: wait for the previous grid
+    // to complete and its writes to be visible (returns at once when the launch had no programmatic dependency)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const double t_new = a.t_sched ? a.t_sched[a.step_in_chunk] : 0.0;
     if (tid == 0)
         for (int k = 0; k < S && k < mycount; ++k) issue(k);
 
@@ -533,8 +551,23 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
     const long long ntiles = ((long long)a.n + NT - 1) / NT;
     const long long cap = cap_blocks;
     const int grid = (int)(ntiles < cap ? ntiles : cap);
-    k<<<grid > 0 ? grid : 1, WPB * kWarp, smem, s>>>(a);
     g_last_shape = LaunchShape{grid > 0 ? grid : 1, WPB * kWarp, smem};
+    if (a.pdl && !a.rate) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(grid > 0 ? grid : 1));
+        cfg.blockDim = dim3(WPB * kWarp);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const cudaError_t e = cudaLaunchKernelEx(&cfg, k, a);
+        if (e != cudaSuccess) return e;
+        return cudaGetLastError();
+    }
+    k<<<grid > 0 ? grid : 1, WPB * kWarp, smem, s>>>(a);
     return cudaGetLastError();
 }
 

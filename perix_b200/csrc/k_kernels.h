@@ -148,6 +148,10 @@ struct EpfArgs {
     int maxb = 0;                           // TMA variants: staged bonds per tile (multiple of 32)
     unsigned int *err = nullptr;            // TMA variants: pipeline waits that ran out
     int rate = 0;                           // TMA variants: RATE mode (accel out; u_other and BCs unused)
+    // TMA variants, STEP mode: launch with programmatic stream serialisation, so that inside a captured loop of
+    // steps the next step's blocks start their set-up while this step's last blocks finish (host-side only)
+    int pdl = 0;
+    int evict_first = 0;  // TMA variants: stage the bond streams with an L2 evict-first policy
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
 constexpr int kEpfTmaConfigs = 13;                // staged (TMA) configurations per dimension

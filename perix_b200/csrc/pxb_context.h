@@ -142,6 +142,7 @@ struct EpfState {
     std::map<GraphKey, cudaGraphExec_t> graphs;
     int graph_chunk = 0;
     int variant = 1;   // schedule variant of the explicit kernel (set by the autotuner or pxb_epf_set_variant)
+    bool evict_first = false;  // the step's bond streams exceed the L2: stage them with an evict-first policy
 };
 
 struct CsrState {
