@@ -148,6 +148,7 @@ static void destroy_graphs(EpfState &e) {
     e.rate_graph = nullptr;
     e.rate_u = e.rate_last_u = nullptr;
     e.rate_a = e.rate_last_a = nullptr;
+    e.rate_last_variant = -1;
     if (e.rate_done) cudaEventDestroy(e.rate_done);
     e.rate_done = nullptr;
 }
@@ -747,11 +748,13 @@ extern "C" int pxb_epf_rate(pxb_ctx *c, const double *u, double *accel, long lon
     if (!u || !accel) return fail(PXB_ERR_INVALID, "pxb_epf_rate: NULL buffer");
     EpfState &e = c->epf;
     PXB_TRY(ensure_pinned(e.rate_h, sizeof(unsigned long long) * 5));
-    // pinned buffers that the previous call used too: replay (or capture) the call as one graph; otherwise (first
-    // call with these buffers, or pageable memory) queue the operations one by one
-    const bool again = u == e.rate_last_u && accel == e.rate_last_a;
+    // pinned buffers that the previous call used too, with the same schedule: replay (or capture) the call as one
+    // graph; otherwise (first call with these buffers or this schedule, or pageable memory) queue the operations
+    // one by one, which also gives a kernel its first, uncaptured launch
+    const bool again = u == e.rate_last_u && accel == e.rate_last_a && e.variant == e.rate_last_variant;
     e.rate_last_u = u;
     e.rate_last_a = accel;
+    e.rate_last_variant = e.variant;
     if (again && pinned_host(u) && pinned_host(accel)) {
         if (!e.rate_graph || e.rate_u != u || e.rate_a != accel || e.rate_cur != e.cur || e.rate_variant != e.variant)
             PXB_TRY(capture_rate(c, u, accel));

@@ -129,7 +129,7 @@ struct EpfState {
     cudaGraphExec_t rate_graph = nullptr;
     const void *rate_u = nullptr, *rate_last_u = nullptr;
     void *rate_a = nullptr, *rate_last_a = nullptr;
-    int rate_cur = -1, rate_variant = -1;
+    int rate_cur = -1, rate_variant = -1, rate_last_variant = -1;
     DevBuf umax;       // unsigned long long [chunk] per-step max |u| keys
     DevBuf tsched;     // double [chunk] t_{n+1} of each step in the chunk
     PinnedBuf tsched_h;

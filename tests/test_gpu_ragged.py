@@ -153,3 +153,9 @@ def test_rate_repeated_on_pinned_buffers(ctx, case, port, variant):
     assert np.array_equal(h, (h_ref3 > 0).astype(np.uint8))
     assert n3 == int(c["h_ref"].sum() - (h_ref3 > 0).sum()) and n3 > 0
     assert np.abs(a3 - a_ref3).max() <= 1e-12 * np.abs(a_ref3).max()
+    # another schedule on the same buffers: queued once, then captured and replayed again
+    ctx.epf_set_variant(1 if variant != 1 else 5)
+    for _ in range(3):
+        a4, n4 = call()
+        assert n4 == 0
+        assert np.abs(a4 - a_ref3).max() <= 1e-12 * np.abs(a_ref3).max()
