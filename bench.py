@@ -713,6 +713,26 @@ def e2e_rate(px, ctx, w, steps):
     return float(np.median(rates)), n2 * 8, n2 * 8 + 16
 
 
+def pageable_call_us(ctx, w, calls=50):
+    """Median time of the per-step call made with pageable host arrays (numpy), as the reference element passes
+    its std::vector data: the copies go through the driver's staging buffers and no graph is used."""
+    import ctypes as C
+    u, _, _, _ = ctx.epf_state()
+    u = np.ascontiguousarray(u, np.float64)
+    a = np.zeros_like(u)
+    nbk = C.c_longlong(0)
+    up, ap = u.ctypes.data_as(C.POINTER(C.c_double)), a.ctypes.data_as(C.POINTER(C.c_double))
+    ts = []
+    for k in range(calls + 10):
+        t = time.perf_counter()
+        st = ctx.L.pxb_epf_rate(ctx.h, up, ap, C.byref(nbk))
+        if st:
+            raise RuntimeError(ctx.L.pxb_last_error().decode())
+        if k >= 10:
+            ts.append(time.perf_counter() - t)
+    return float(np.median(ts)) * 1e6
+
+
 def pcie_copy_us(nbytes, device, reps=20):
     """Device time (CUDA events, median of reps) of one pinned host->device and one device->host copy of nbytes:
     the transfers inside each per-step call, measured alone on this machine's link."""
@@ -796,6 +816,7 @@ def run_perix(args):
     traffic = read_traffic(head)
     e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, max(10, min(steps, 200)))
     copies = pcie_copy_us(h2d, local)
+    pageable_us = pageable_call_us(r["ctx"], w)
     cpu = None
     clouds = slab = refgpu = poisson = ch = None
     if rank == 0 and ws == 1:
@@ -830,6 +851,7 @@ def run_perix(args):
                    "state": "snapshot after %d steps, restored every %d steps" % (S0, EPISODE)},
         "e2e": {"value": ws * e2e, "unit": "bond-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "call_us": 1e6 * w["nb"] / e2e,
+                "call_us_pageable_buffers": pageable_us,
                 "pcie_copy_us": {"h2d": copies["h2d"], "d2h": copies["d2h"],
                                  "note": "one pinned copy of the call's u (h2d) or acceleration (d2h) bytes alone, "
                                          "CUDA events, median of 20: the link speed this machine gave"},
