@@ -1,16 +1,18 @@
-"""Benchmark: explicit PDDO fracture bond-updates/s (and g-build nodes/s) on the 2D notched plate
-(400x200 nodes, h = 0.5 mm, delta = 3.015h, plane strain, E = 190 GPa, nu = 0.3, rho = 8000, s_c = 0.01, two
-force-only slits of 50h at y = 0.05 +- 25h, 16.5 m/s pull on the left ghosts between the slits,
-dt = 0.8 h / sqrt(C11/rho)).
+"""Benchmark: explicit PDDO fracture bond-updates/s (and g-build nodes/s).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl perix|reference] [--precision mixed|fp64]
+Headline workload: the 3D notched slab (120x120x24 bulk nodes + one ghost layer per face = 385,920 PD nodes,
+44,189,344 directed bonds, h = 1 mm, delta = 3.015h, E = 72 GPa, nu = 0.22, rho = 2440, s_c = 0.004, a central edge
+notch of depth 20h as a force-only crack plane, +-2 m/s pins on the top and bottom three-node layers,
+dt = 0.8 h / sqrt(C11/rho)).  The 2D notched plate (400x200 nodes, h = 0.5 mm, E = 190 GPa, nu = 0.3, rho = 8000,
+s_c = 0.01, two force-only slits of 50h, 16.5 m/s pull) is reported under "plate_2d".
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl perix|reference] [--headline-only]
 
 A step is one explicit time step (damage + Navier force + central difference + BC pass, one fused kernel),
 timed alone with CUDA events on the launching stream; the L2 is flushed (256 MiB write, then read back) before
-every timed step, and the state is restored from a snapshot taken 100 steps into the run every 100 steps, so every timed
-step works on the same physical regime (about 200 steps later a wall mode of the reference scheme starts to grow on
-this plate, in the reference and here alike).
-Multi-GPU runs (torchrun) are independent replicas of the plate (weak scaling); the time is the max over ranks.
+every timed step (the slab's bond streams, 1.3-2.4 GB, exceed the L2 anyway), and the state is restored from a
+snapshot taken 100 steps into the run every 100 steps, so every timed step works on the same physical regime.
+Multi-GPU runs (torchrun) are independent replicas of the slab (weak scaling); the time is the max over ranks.
 Prints one JSON line on rank 0.
 """
 import argparse
@@ -52,7 +54,7 @@ def plate_setup(px):
     bcs.append(px.BC("dirichlet", [0], L.group("leftnodes_ghost"), value=[0, 0], velocity=[16.5, 0], direct=True,
                      box=[-1, 1, y1, y2, -1, 1]))
     return dict(L=L, off=off, ids=ids, delta=delta, health0=health0, C=(C11, C12, C66), rho=rho, sc=sc, dt=dt,
-                bcs=bcs, E=E, nu=nu, G0=G0, cracks=cracks, n=L.n, nb=int(off[-1]), h=h)
+                bcs=bcs, E=E, nu=nu, G0=G0, cracks=cracks, n=L.n, nb=int(off[-1]), h=h, dim=2, kind="plate")
 
 
 def slab_setup(px, nx=120, ny=120, nz=24):
@@ -80,12 +82,12 @@ def slab_setup(px, nx=120, ny=120, nz=24):
     bcs.append(px.BC("dirichlet", [1], alld, value=[0, 0, 0], velocity=[0, -2.0, 0], direct=True,
                      box=[-1, 1, -1, 3 * h, -1, 1]))
     return dict(L=L, off=off, ids=ids, delta=delta, health0=health0, C=(C11, C12, C66), rho=rho, sc=sc, dt=dt,
-                bcs=bcs, E=E, nu=nu, n=L.n, nb=int(off[-1]), h=h)
+                bcs=bcs, E=E, nu=nu, G0=G0, plane=plane, n=L.n, nb=int(off[-1]), h=h, dim=3, kind="slab",
+                size=(nx, ny, nz))
 
 
-def slab_measure(px, device=0, steps=50, adjoint_steps=1000, checkpoint_every=100):
-    """The 3D slab: step throughput (FP64 and mixed, autotuned, CUDA events, L2 flushed, from the state after
-    100 steps) and the frozen-mask adjoint d(misfit)/dE over the first `adjoint_steps` steps with checkpointed
+def slab_adjoint(px, device=0, adjoint_steps=1000, checkpoint_every=100):
+    """The 3D slab's frozen-mask adjoint: d(misfit)/dE over the first `adjoint_steps` steps with checkpointed
     recomputation, checked against central finite differences of the device loop."""
     import torch
     from perix_b200.autograd import BcPlan, elastic_constants_t, explicit_loop, set_constants
@@ -94,29 +96,6 @@ def slab_measure(px, device=0, steps=50, adjoint_steps=1000, checkpoint_every=10
     res = {"workload": "3D slab 120x120x24 (+ghosts), edge notch 20h", "nodes": w["n"], "bonds": w["nb"],
            "host_setup_s": time.perf_counter() - t0}
     L = w["L"]
-    C11, C12, C66 = w["C"]
-    hbm, _ = peaks()
-    for prec in ("fp64", "mixed"):
-        ctx = px.Context(device)
-        ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 3, mirror=L.mirror)
-        ctx.epf_setup(C11, C12, C66, w["rho"], (0.0, 0.0, 0.0), w["sc"], True, health0=w["health0"],
-                      precision=px.MIXED if prec == "mixed" else px.FP64)
-        ctx.epf_set_bcs(w["bcs"])
-        ctx.epf_start(np.zeros(3 * L.n), None, w["dt"])
-        ctx.epf_advance(S0)
-        snap(ctx)
-        tuned = autotune(ctx, steps=5)
-        ms = np.zeros(steps, np.float32)
-        time_steps(ctx, 3, ms[:3])
-        restore(ctx)
-        time_steps(ctx, steps, ms)
-        mean_ms = float(np.mean(ms))
-        B = algorithmic_bytes(w["n"], w["nb"], 3, prec)
-        gb, gb_ms = gbuild_rate(px, ctx, prec, reps=3)
-        res[prec] = {"bond_updates_per_s": w["nb"] / (mean_ms * 1e-3), "ms_per_step": mean_ms, "autotune": tuned,
-                     "achieved_gbs": B / (mean_ms * 1e-3) / 1e9, "frac_of_measured_hbm": B / (mean_ms * 1e-3) / 1e9 / hbm,
-                     "algorithmic_bytes_per_step": B, "gbuild_nodes_per_s": gb, "gbuild_ms": gb_ms}
-        ctx.close()
     # adjoint: misfit against the displacement of a 2 % stiffer slab, frozen damage mask (damage off)
     dev = torch.device("cuda", device)
     ctx = px.Context(device)
@@ -496,9 +475,12 @@ def barrier(ws):
         dist.barrier()
 
 
-def read_traffic(prec):
-    """DRAM bytes per step-kernel launch from the committed ncu summary (None until captured)."""
-    path = os.path.join(ROOT, "profiles", "epf_step_plate.md")
+PROFILE_FILES = {"plate": "epf_step_plate.md", "slab": "epf_step_slab.md"}
+
+
+def read_traffic(kind, prec):
+    """DRAM bytes per step-kernel launch from the committed ncu summary of this workload (None until captured)."""
+    path = os.path.join(ROOT, "profiles", PROFILE_FILES[kind])
     if not os.path.exists(path):
         return None
     key = "traffic_bytes_per_launch_%s:" % prec
@@ -511,15 +493,15 @@ def read_traffic(prec):
     return None
 
 
-def kernel_name(prec, tuned):
-    """The 2D step kernel the autotuner picked (variants 0-2 lane groups, 3-4 CSR tiles, 5 and up TMA-staged)."""
+def kernel_name(dim, prec, tuned):
+    """The step kernel the autotuner picked (variants 0-2 lane groups, 3-4 CSR tiles, 5 and up TMA-staged)."""
     v, lpn = tuned["variant"], tuned["lanes_per_node"]
     mixed = "true" if prec == "mixed" else "false"
     if v >= 5:
-        return "pxb::epf_tma_kernel<2,%s,LPN=%d,...> (variant %d)" % (mixed, lpn, v)
+        return "pxb::epf_tma_kernel<%d,%s,LPN=%d,...> (variant %d)" % (dim, mixed, lpn, v)
     if v >= 3:
-        return "pxb::epf_stream_kernel<2,%s,EPF_STEP,...> (variant %d)" % (mixed, v)
-    return "pxb::epf_kernel<2,%s,EPF_STEP,LPN=%d,...> (variant %d)" % (mixed, lpn, v)
+        return "pxb::epf_stream_kernel<%d,%s,EPF_STEP,...> (variant %d)" % (dim, mixed, v)
+    return "pxb::epf_kernel<%d,%s,EPF_STEP,LPN=%d,...> (variant %d)" % (dim, mixed, lpn, v)
 
 
 def peaks():
@@ -529,30 +511,72 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def plate_workload(nb):
+def workload_name(kind, n, nb):
     """The workload name both arms report."""
-    return "explicit_pddo_frac 2D notched plate 400x200 (81,200 PD nodes, %d directed bonds), dt=0.8h/c" % nb
+    if kind == "plate":
+        return ("explicit_pddo_frac 2D notched plate 400x200 (%d PD nodes, %d directed bonds), dt=0.8h/c" % (n, nb))
+    return ("explicit_pddo_frac 3D notched slab 120x120x24 (+ghosts: %d PD nodes, %d directed bonds), edge notch 20h, "
+            "+-2 m/s pins, dt=0.8h/c" % (n, nb))
 
 
 # --------------------------------------------------------------------------------------------- reference arm
-def cpu_reference(w, steps, warmup, threads=None):
-    """The reference's own OpenMP CPU path (oracle/_ref, built from the reference sources): per step the
-    element sweep (damage + force) plus the host central difference and BC preset."""
+def ref_workload(kind):
+    """The same workload built only from the reference's own code (oracle/_ref): its mesh generator,
+    createNeighborNodes and crack seeding, ExplicitPDDOFracElement (constants and s_c from G0), and the BC list as
+    DirichletBC / NeumannBC entries on its node groups.  Returns None when the harness is not built."""
     from oracle import RefEpf, RefMesh, ref_available
     if not ref_available():
         return None
-    nx, ny, h = 400, 200, 5e-4
-    m = RefMesh.structured(2, nx, ny, 0, [0, nx * h, 0, ny * h], 3.015, 2, cracks=w["cracks"], force_only=True)
+    if kind == "plate":
+        nx, ny, h = 400, 200, 5e-4
+        Lx, Ly = nx * h, ny * h
+        y1, y2 = 0.05 - 25 * h, 0.05 + 25 * h
+        cracks = [[0.0, y1, 50 * h, y1], [0.0, y2, 50 * h, y2]]
+        m = RefMesh.structured(2, nx, ny, 0, [0, Lx, 0, Ly], 3.015, 2, cracks=cracks, force_only=True)
+        E, nu, rho = 190e9, 0.3, 8000.0
+        G0 = 0.01 ** 2 * 12.0 * E * m.delta / (5.0 * math.pi)
+        bcs = [dict(kind="neumann", comps=[0, 1], nodes=m.group(g + "nodes_ghost"))
+               for g in ("left", "right", "bottom", "top")]
+        bcs.append(dict(kind="dirichlet", comps=[0], nodes=m.group("leftnodes_ghost"), value=[0, 0],
+                        velocity=[16.5, 0], direct=True, box=[-1, 1, y1, y2, -1, 1]))
+    else:
+        nx, ny, nz, h = 120, 120, 24, 1e-3
+        Lx, Ly, Lz = nx * h, ny * h, nz * h
+        plane = [0.0, Ly / 2, -1.0, 20 * h, Ly / 2, -1.0, 20 * h, Ly / 2, 1.0, 0.0, Ly / 2, 1.0]
+        m = RefMesh.structured(3, nx, ny, nz, [0, Lx, 0, Ly, 0, Lz], 3.015, 2, planes=[plane], force_only=True)
+        E, nu, rho = 72e9, 0.22, 2440.0
+        G0 = 0.004 ** 2 * 6.0 * E * m.delta / 5.0
+        bcs = [dict(kind="neumann", comps=[0, 1, 2], nodes=m.group(g + "nodes_ghost"))
+               for g in ("left", "right", "bottom", "top", "back", "front")]
+        alld = m.group("alldomain")
+        bcs.append(dict(kind="dirichlet", comps=[1], nodes=alld, value=[0, 0, 0], velocity=[0, 2.0, 0], direct=True,
+                        box=[-1, 1, Ly - 3 * h, 1, -1, 1]))
+        bcs.append(dict(kind="dirichlet", comps=[1], nodes=alld, value=[0, 0, 0], velocity=[0, -2.0, 0], direct=True,
+                        box=[-1, 1, -1, 3 * h, -1, 1]))
+    probe = RefEpf(m, E, nu, rho, G0)
+    probe.rate(np.zeros(m.dim * m.n), nthreads=1 if m.n < 100000 else 0)  # derives C11 (and s_c) from the element
+    dt = 0.8 * h / math.sqrt(probe.constants()["C11"] / rho)
+    return dict(kind=kind, m=m, E=E, nu=nu, rho=rho, G0=G0, bcs=bcs, dt=dt, n=m.n, nb=m.nb, dim=m.dim)
+
+
+def cpu_reference(kind, steps, warmup, threads=None):
+    """The reference's own OpenMP CPU path (oracle/_ref, built from the reference sources) on the workload: per step
+    the element sweep (damage + force) plus the central difference and the BC preset (reference BC objects).  Only
+    the stepping loop is timed: the start's rate call, which on a fresh element also builds its operator cache and
+    starts the OpenMP pool, stays outside; on the plate a separate warm-up run of `warmup` steps comes first."""
+    from oracle import RefEpf
+    r = ref_workload(kind)
+    if r is None:
+        return None
+    m = r["m"]
     threads = threads or os.cpu_count()
-    bcs = [bc.as_dict() for bc in w["bcs"]]
-    el = RefEpf(m, w["E"], w["nu"], w["rho"], w["G0"], plane_stress=False)
-    el.run(np.zeros(2 * m.n), None, w["dt"], max(1, warmup), bcs, nthreads=threads)
-    el = RefEpf(m, w["E"], w["nu"], w["rho"], w["G0"], plane_stress=False)
-    _, _, _, t0 = el.run(np.zeros(2 * m.n), None, w["dt"], 0, bcs, nthreads=threads)
-    el = RefEpf(m, w["E"], w["nu"], w["rho"], w["G0"], plane_stress=False)
-    _, _, _, tk = el.run(np.zeros(2 * m.n), None, w["dt"], steps, bcs, nthreads=threads)
-    t = max(tk - t0, 1e-9)
-    return dict(value=m.nb * steps / t, seconds=t, steps=steps, cores=threads, nb=m.nb)
+    if kind == "plate" and warmup > 0:
+        el = RefEpf(m, r["E"], r["nu"], r["rho"], r["G0"], plane_stress=False)
+        el.run(np.zeros(m.dim * m.n), None, r["dt"], warmup, r["bcs"], nthreads=threads)
+    el = RefEpf(m, r["E"], r["nu"], r["rho"], r["G0"], plane_stress=False)
+    _, _, _, t = el.run(np.zeros(m.dim * m.n), None, r["dt"], steps, r["bcs"], nthreads=threads)
+    t = max(t, 1e-9)
+    return dict(value=m.nb * steps / t, seconds=t, steps=steps, cores=threads, nb=m.nb, n=m.n)
 
 
 def reference_gpu():
@@ -574,23 +598,28 @@ def reference_gpu():
         return {"unavailable": "reference GPU run failed: %s" % e}
 
 
+REF_MAX_STEPS = 40     # bound on the reference arm's timed steps (about 0.2-0.4 s each on the slab)
+
+
 def run_reference_arm(args):
+    """The reference's own CPU implementation of the path (oracle/_ref) on the headline workload; nothing of this
+    backend is loaded.  Rank 0 alone runs it under torchrun."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    import perix_b200 as px
-    w = plate_setup(px)
-    steps = max(1, args.steps)
-    r = cpu_reference(w, steps, args.warmup)
+    steps = max(1, min(args.steps, REF_MAX_STEPS))
+    r = cpu_reference("slab", steps, min(args.warmup, 3))
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference sources) not built"}))
         return
-    sample = "%d explicit steps of the 400x200 plate (element sweep + central difference + BC preset)" % steps
+    sample = ("%d explicit steps of the 3D slab (element sweep + central difference + BC preset), %d threads"
+              % (steps, r["cores"]))
     line = {"impl": "reference", "metric": "bond-updates/s (explicit frac)", "value": r["value"],
             "unit": "bond-updates/s", "n_gpus": ws, "steps": steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * r["seconds"] / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": plate_workload(r["nb"]), "nodes": w["n"], "bonds": r["nb"], "threads": r["cores"]},
+            "config": {"workload": workload_name("slab", r["n"], r["nb"]), "nodes": r["n"], "bonds": r["nb"],
+                       "threads": r["cores"]},
             "cpu_baseline": {"value": r["value"], "unit": "bond-updates/s", "cores": r["cores"], "kind": "reference",
                              "sample": sample},
             "e2e": {"value": r["value"], "unit": "bond-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -598,18 +627,24 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------------------------------------ perix arm
-def measure_precision(px, w, prec, steps, warmup, ws, device):
+def explicit_context(px, w, prec, device):
+    """A context holding the workload's explicit element (FP64 or mixed) with its BC program."""
     ctx = px.Context(device)
-    L = w["L"]
-    ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
-    p = px.MIXED if prec == "mixed" else px.FP64
+    L, dim = w["L"], w["dim"]
+    ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], dim, mirror=L.mirror)
     C11, C12, C66 = w["C"]
-    ctx.epf_setup(C11, C12, C66, w["rho"], (0.0, 0.0), w["sc"], True, health0=w["health0"], precision=p)
+    ctx.epf_setup(C11, C12, C66, w["rho"], (0.0,) * dim, w["sc"], True, health0=w["health0"],
+                  precision=px.MIXED if prec == "mixed" else px.FP64)
     ctx.epf_set_bcs(w["bcs"])
-    ctx.epf_start(np.zeros(2 * L.n), None, w["dt"])
+    return ctx
+
+
+def measure_precision(px, w, prec, steps, warmup, ws, device):
+    ctx = explicit_context(px, w, prec, device)
+    ctx.epf_start(np.zeros(w["dim"] * w["n"]), None, w["dt"])
     ctx.epf_advance(S0)
     snap(ctx)
-    tuned = autotune(ctx)
+    tuned = autotune(ctx, steps=20 if w["kind"] == "plate" else 5)
     ms = np.zeros(max(warmup, 1), np.float32)
     time_steps(ctx, max(warmup, 1), ms)
     restore(ctx)
@@ -691,7 +726,7 @@ def e2e_rate(px, ctx, w, steps):
     calls; the median batch rate (the host's wait on each call varies with the load of the shared machine, the
     device work does not)."""
     import torch
-    n2 = 2 * w["n"]
+    n2 = w["dim"] * w["n"]
     u_h = torch.empty(n2, dtype=torch.float64, pin_memory=True)
     a_h = torch.empty(n2, dtype=torch.float64, pin_memory=True)
     u, _, _, _ = ctx.epf_state()
@@ -760,23 +795,140 @@ def pcie_copy_us(nbytes, device, reps=20):
     return out
 
 
+def shim_call_us(px, w, calls=30):
+    """Median time of the reference boundary's own drop-in call, perix_cuda::assembleExplicitPDDOFracAccel (through
+    its C entry pxb_cuda_explicit_accel), made as the reference element makes it: pageable host arrays (numpy, the
+    element's std::vector data), 1-based families, double health in/out.  The shim's first call of the problem
+    uploads the mesh, builds the operators and times its schedules; the timed calls are the per-step calls that
+    follow, at the displacement of the state after 100 steps.  Returns (us per call, calls whose health changed)."""
+    import ctypes as C
+    L, dim = w["L"], w["dim"]
+    ctx = explicit_context(px, w, "fp64", 0)
+    ctx.epf_start(np.zeros(dim * w["n"]), None, w["dt"])
+    ctx.epf_advance(S0)
+    u, _, h8, _ = ctx.epf_state()
+    ctx.close()
+    lib = px.lib()
+    f64 = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    i32 = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))  # noqa: E731
+    off = np.ascontiguousarray(w["off"], np.int32)
+    ids = np.ascontiguousarray(w["ids"], np.int32)
+    coords = np.ascontiguousarray(L.coords, np.float64)
+    vols = np.ascontiguousarray(L.vols, np.float64)
+    u = np.ascontiguousarray(u, np.float64)
+    health = h8.astype(np.float64)
+    acc = np.zeros_like(u)
+    body = np.zeros(3)
+    changed = C.c_int(0)
+    C11, C12, C66 = w["C"]
+    args = (w["n"], dim, i32(off), i32(ids), f64(coords), f64(vols), C.c_double(w["delta"]), C.c_double(L.dxyz[0]),
+            C.c_double(C11), C.c_double(C12), C.c_double(C66), C.c_double(w["rho"]), f64(body), C.c_double(w["sc"]),
+            1, 1, f64(u), f64(health), f64(acc), C.byref(changed))
+    lib.pxb_cuda_shutdown()
+    ts, nchanged = [], 0
+    for k in range(calls + 5):
+        t = time.perf_counter()
+        if lib.pxb_cuda_explicit_accel(*args) != 1:
+            raise RuntimeError("pxb_cuda_explicit_accel failed: " + lib.pxb_last_error().decode())
+        if k >= 5:
+            ts.append(time.perf_counter() - t)
+            nchanged += int(changed.value)
+    lib.pxb_cuda_shutdown()
+    return float(np.median(ts)) * 1e6, nchanged
+
+
 def mixed_error(px, w, device):
-    """max|u_mixed - u_fp64| / max|u_fp64| after 100 graph-captured steps from the same 100-step state."""
+    """max|u_mixed - u_fp64| / max|u_fp64| after 100 graph-captured steps from the same 100-step state, and the
+    number of bonds whose health differs."""
     res = {}
     for prec in ("fp64", "mixed"):
-        ctx = px.Context(device)
-        L = w["L"]
-        ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
-        C11, C12, C66 = w["C"]
-        ctx.epf_setup(C11, C12, C66, w["rho"], (0.0, 0.0), w["sc"], True, health0=w["health0"],
-                      precision=px.MIXED if prec == "mixed" else px.FP64)
-        ctx.epf_set_bcs(w["bcs"])
-        ctx.epf_start(np.zeros(2 * L.n), None, w["dt"])
+        ctx = explicit_context(px, w, prec, device)
+        ctx.epf_start(np.zeros(w["dim"] * w["n"]), None, w["dt"])
         ctx.epf_advance(2 * S0)
         res[prec] = ctx.epf_state()
         ctx.close()
     u64, u32 = res["fp64"][0], res["mixed"][0]
     return float(np.abs(u32 - u64).max() / np.abs(u64).max()), int((res["fp64"][2] != res["mixed"][2]).sum())
+
+
+def explicit_workload(px, w, steps, warmup, ws, local, e2e_calls):
+    """Both precisions of one explicit workload: CUDA-event step times (L2 flushed), the L2-warm 100-step graph
+    chunk, the g-build rate, and for the headline precision (mixed when within 1e-6 of FP64 after 100 steps) the
+    roofline and the per-step calls from host memory.  Returns the JSON block and the headline's timed launches."""
+    hbm, peak_kind = peaks()
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with ClockSampler(local) as clk:
+            ctx, ms, launches, wall, tuned = measure_precision(px, w, prec, steps, warmup, ws, local)
+        t = reduce_max(float(ms.sum()) * 1e-3, ws)
+        # graph-captured chunk from the snapshot (L2-warm, the production loop); the first advance captures and
+        # instantiates the graph for the tuned variant, the next five are timed
+        restore(ctx)
+        ctx.epf_advance(EPISODE, chunk=EPISODE)
+        chunks = []
+        for _ in range(5):
+            restore(ctx)
+            t0 = time.perf_counter()
+            ctx.epf_advance(EPISODE, chunk=EPISODE)
+            chunks.append(time.perf_counter() - t0)
+        steady = w["nb"] * EPISODE / float(np.median(chunks))
+        gb, gb_ms = gbuild_rate(px, ctx, prec, reps=3)
+        out[prec] = dict(ctx=ctx, ms=ms, t=t, launches=launches, wall=wall, clocks=clk.summary(), steady=steady,
+                         gbuild=gb, gbuild_ms=gb_ms, tuned=tuned)
+    err, hdiff = mixed_error(px, w, local)
+    head = "mixed" if err <= 1e-6 else "fp64"
+    r = out[head]
+    mean_s = float(np.mean(r["ms"])) * 1e-3
+    B = algorithmic_bytes(w["n"], w["nb"], w["dim"], head)
+    achieved = B / mean_s / 1e9
+    e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, e2e_calls)
+    copies = pcie_copy_us(h2d, local)
+    pageable_us = pageable_call_us(r["ctx"], w)
+    for p in out.values():
+        p["ctx"].close()
+    shim_us, shim_changed = shim_call_us(px, w)
+    block = {
+        "value": ws * w["nb"] * steps / r["t"],
+        "ms_per_step": 1e3 * r["t"] / steps,
+        "precision": head,
+        "dtype": "mixed(f32-storage,f64-arith)" if head == "mixed" else "f64",
+        "nodes": w["n"], "bonds": w["nb"],
+        "workload": workload_name(w["kind"], w["n"], w["nb"]),
+        "e2e": {"value": ws * e2e, "unit": "bond-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "call_us": 1e6 * w["nb"] / e2e,
+                "call_us_pageable_buffers": pageable_us,
+                "drop_in_call_us": shim_us,
+                "drop_in_calls_with_health_changed": shim_changed,
+                "pcie_copy_us": {"h2d": copies["h2d"], "d2h": copies["d2h"],
+                                 "note": "one pinned copy of the call's u (h2d) or acceleration (d2h) bytes alone, "
+                                         "CUDA events, median of 20: the link speed this machine gave"},
+                "api": "pxb_epf_rate (per-step call, pinned host u in / acceleration out, headline precision); "
+                       "drop_in_call_us: perix_cuda::assembleExplicitPDDOFracAccel via pxb_cuda_explicit_accel with "
+                       "pageable arrays and double health in/out (FP64, the shim's default)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": read_traffic(w["kind"], head), "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": B, "kernel": kernel_name(w["dim"], head, r["tuned"]),
+                     "launch_floor_ms": (r["tuned"]["launch_floor"] or {}).get("ms"),
+                     "note": "achieved = algorithmic bytes / CUDA-event step time; launch_floor_ms is an empty "
+                             "kernel of the same launch shape timed the same way (flush, events)"},
+        "gpu_launches": int(r["launches"]),
+        "clocks": {k: r["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "fp64": {"value": ws * w["nb"] * steps / out["fp64"]["t"], "ms_per_step": 1e3 * out["fp64"]["t"] / steps,
+                 "frac_of_measured_hbm": algorithmic_bytes(w["n"], w["nb"], w["dim"], "fp64") /
+                 (float(np.mean(out["fp64"]["ms"])) * 1e-3) / 1e9 / hbm,
+                 "autotune": out["fp64"]["tuned"]},
+        "mixed": {"value": ws * w["nb"] * steps / out["mixed"]["t"], "ms_per_step": 1e3 * out["mixed"]["t"] / steps,
+                  "frac_of_measured_hbm": algorithmic_bytes(w["n"], w["nb"], w["dim"], "mixed") /
+                  (float(np.mean(out["mixed"]["ms"])) * 1e-3) / 1e9 / hbm,
+                  "rel_err_vs_fp64_after_100_steps": err, "health_differs": hdiff, "autotune": out["mixed"]["tuned"]},
+        "mixed_over_fp64": out["fp64"]["t"] / out["mixed"]["t"],
+        "steady_state_graph": {"fp64": out["fp64"]["steady"], "mixed": out["mixed"]["steady"],
+                               "note": "100-step CUDA-graph chunk, L2-warm (wall clock incl. host sync, median of 5 chunks)"},
+        "gbuild_nodes_per_s": {"fp64": out["fp64"]["gbuild"], "mixed": out["mixed"]["gbuild"],
+                               "ms": {"fp64": out["fp64"]["gbuild_ms"], "mixed": out["mixed"]["gbuild_ms"]},
+                               "workload": "order-2 g-build of the same mesh (all operators stored)"},
+    }
+    return block
 
 
 def run_perix(args):
@@ -789,109 +941,66 @@ def run_perix(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import perix_b200 as px
-    w = plate_setup(px)
-    hbm, peak_kind = peaks()
-    out = {}
-    for prec in ("fp64", "mixed"):
-        with ClockSampler(local) as clk:
-            ctx, ms, launches, wall, tuned = measure_precision(px, w, prec, args.steps, args.warmup, ws, local)
-        t = reduce_max(float(ms.sum()) * 1e-3, ws)
-        steady = None
-        # graph-captured chunk from the snapshot (L2-warm, the production loop); the first advance captures and
-        # instantiates the graph for the tuned variant, the second is timed
-        restore(ctx)
-        ctx.epf_advance(EPISODE, chunk=EPISODE)
-        chunks = []
-        for _ in range(5):
-            restore(ctx)
-            t0 = time.perf_counter()
-            ctx.epf_advance(EPISODE, chunk=EPISODE)
-            chunks.append(time.perf_counter() - t0)
-        steady = w["nb"] * EPISODE / float(np.median(chunks))
-        gb, gb_ms = gbuild_rate(px, ctx, prec)
-        out[prec] = dict(ctx=ctx, ms=ms, t=t, launches=launches, wall=wall, clocks=clk.summary(), steady=steady,
-                         gbuild=gb, gbuild_ms=gb_ms, tuned=tuned)
-    err, hdiff = mixed_error(px, w, local)
-    head = "mixed" if err <= 1e-6 else "fp64"
-    r = out[head]
     steps = args.steps
-    value = ws * w["nb"] * steps / r["t"]
-    mean_s = float(np.mean(r["ms"])) * 1e-3
-    B = algorithmic_bytes(w["n"], w["nb"], 2, head)
-    achieved = B / mean_s / 1e9
-    traffic = read_traffic(head)
-    e2e, h2d, d2h = e2e_rate(px, r["ctx"], w, max(10, min(steps, 200)))
-    copies = pcie_copy_us(h2d, local)
-    pageable_us = pageable_call_us(r["ctx"], w)
+    slab = explicit_workload(px, slab_setup(px), steps, args.warmup, ws, local, max(10, min(steps, 100)))
+    plate = None
     cpu = None
-    clouds = slab = refgpu = poisson = ch = None
+    clouds = refgpu = poisson = ch = adjoint = None
     if rank == 0 and ws == 1:
-        cpu = cpu_reference(w, 20, 2)
-        for p in out.values():
-            p["ctx"].close()
+        cpu = cpu_reference("slab", 10, 2)
         if not args.headline_only:
+            plate = explicit_workload(px, plate_setup(px), steps, args.warmup, ws, local, max(10, min(steps, 200)))
+            plate["cpu_baseline"] = cpu_reference("plate", 20, 2)
             clouds = clouds_measure(px, device=local)
-            slab = slab_measure(px, device=local)
+            adjoint = slab_adjoint(px, device=local)
             refgpu = reference_gpu()
             poisson = poisson_measure(px, device=local)
             ch = ch_measure(px, device=local)
     if rank != 0:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     line = {
         "metric": "bond-updates/s (explicit frac)",
-        "value": value,
+        "value": slab["value"],
         "unit": "bond-updates/s",
         "n_gpus": ws,
         "steps": steps,
         "warmup": args.warmup,
-        "ms_per_step": 1e3 * r["t"] / steps,
+        "ms_per_step": slab["ms_per_step"],
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
-        "precision": head + (" (f32 operator storage, f64 arithmetic and state)" if head == "mixed" else ""),
+        "dtype": slab["dtype"],
+        "precision": slab["precision"] + (" (f32 Navier-coefficient storage; f64 arithmetic, state and stretch "
+                                          "decisions)" if slab["precision"] == "mixed" else ""),
         "data": "synthetic",
-        "config": {"workload": plate_workload(w["nb"]),
-                   "nodes": w["n"], "bonds": w["nb"], "parallelism": "replicas" if ws > 1 else "single-gpu",
-                   "l2": "flushed before every timed step (256 MiB write, then the same 256 MiB read back)",
+        "config": {"workload": slab["workload"], "nodes": slab["nodes"], "bonds": slab["bonds"],
+                   "parallelism": "replicas" if ws > 1 else "single-gpu",
+                   "l2": "flushed before every timed step (256 MiB write, then the same 256 MiB read back); the "
+                         "step's bond streams exceed the 126 MB L2",
                    "state": "snapshot after %d steps, restored every %d steps" % (S0, EPISODE)},
-        "e2e": {"value": ws * e2e, "unit": "bond-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "call_us": 1e6 * w["nb"] / e2e,
-                "call_us_pageable_buffers": pageable_us,
-                "pcie_copy_us": {"h2d": copies["h2d"], "d2h": copies["d2h"],
-                                 "note": "one pinned copy of the call's u (h2d) or acceleration (d2h) bytes alone, "
-                                         "CUDA events, median of 20: the link speed this machine gave"},
-                "api": "pxb_epf_rate (drop-in per-step call, pinned host u in / acceleration out)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": B, "kernel": kernel_name(head, out[head]["tuned"]),
-                     "launch_floor_ms": (out[head]["tuned"]["launch_floor"] or {}).get("ms"),
-                     "note": "achieved = algorithmic bytes / CUDA-event step time; launch_floor_ms is an empty "
-                             "kernel of the same launch shape timed the same way (flush, events)"},
-        "cpu_baseline": ({"value": cpu["value"], "unit": "bond-updates/s", "cores": cpu["cores"],
-                          "kind": "reference",
-                          "sample": "20 explicit steps of the same plate through the reference's OpenMP CPU path"}
-                         if cpu else None),
-        "gpu_launches": int(r["launches"]),
-        "clocks": {k: r["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
-        "fp64": {"value": ws * w["nb"] * steps / out["fp64"]["t"], "ms_per_step": 1e3 * out["fp64"]["t"] / steps,
-                 "autotune": out["fp64"]["tuned"]},
-        "mixed": {"value": ws * w["nb"] * steps / out["mixed"]["t"], "ms_per_step": 1e3 * out["mixed"]["t"] / steps,
-                  "rel_err_vs_fp64_after_100_steps": err, "health_differs": hdiff, "autotune": out["mixed"]["tuned"]},
-        "steady_state_graph": {"fp64": out["fp64"]["steady"], "mixed": out["mixed"]["steady"],
-                               "note": "100-step CUDA-graph chunk, L2-warm (wall clock incl. host sync, median of 5 chunks)"},
+        "e2e": slab["e2e"],
+        "roofline": slab["roofline"],
+        "cpu_baseline": ({"value": cpu["value"], "unit": "bond-updates/s", "cores": cpu["cores"], "kind": "reference",
+                          "sample": "10 explicit steps of the same slab through the reference's OpenMP CPU path "
+                                    "(element sweep + central difference + BC preset)"} if cpu else None),
+        "gpu_launches": slab["gpu_launches"],
+        "clocks": slab["clocks"],
+        "fp64": slab["fp64"],
+        "mixed": slab["mixed"],
+        "mixed_over_fp64": slab["mixed_over_fp64"],
+        "steady_state_graph": slab["steady_state_graph"],
+        "gbuild_nodes_per_s": slab["gbuild_nodes_per_s"],
+        "slab_adjoint": adjoint,
+        "plate_2d": plate,
         "batched_clouds": clouds,
-        "slab_3d": slab,
         "reference_gpu": refgpu,
         "poisson_64x64": poisson,
         "cahn_hilliard_256x256": ch,
-        "gbuild_nodes_per_s": {"fp64": out["fp64"]["gbuild"], "mixed": out["mixed"]["gbuild"],
-                               "ms": {"fp64": out["fp64"]["gbuild_ms"], "mixed": out["mixed"]["gbuild_ms"]},
-                               "workload": "order-2 g-build of the same plate (81,200 nodes, all 5 operators stored)"},
     }
     print(json.dumps(line))
-    for p in out.values():
-        p["ctx"].close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -985,7 +1094,7 @@ def run_profile(args):
     L = w["L"]
     ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 2, mirror=L.mirror)
     if args.profile == "slab":
-        print(json.dumps({"profile": "slab", **slab_measure(px)}))
+        print(json.dumps({"profile": "slab", **slab_adjoint(px)}))
         ctx.close()
         return
     if args.profile == "ch":

@@ -54,6 +54,10 @@ int pxb_ctx_set_stream(pxb_ctx *ctx, void *stream);
 int pxb_ctx_synchronize(pxb_ctx *ctx);
 /* Device bytes currently held by the context. */
 int pxb_ctx_device_bytes(pxb_ctx *ctx, size_t *bytes);
+/* Caps the device bytes the context may hold (0 = no cap beyond the GPU's own memory), e.g. to share a GPU with
+ * other work: an allocation past the cap fails with PXB_ERR_OOM before reaching the driver, like one the driver
+ * refuses (cudaErrorMemoryAllocation is also reported as PXB_ERR_OOM).  No counterpart in the reference. */
+int pxb_ctx_set_memory_limit(pxb_ctx *ctx, size_t bytes);
 /* Kernel launches issued by this context since creation (graph replays count each captured launch). */
 int pxb_ctx_launch_count(pxb_ctx *ctx, long long *count);
 
@@ -114,18 +118,25 @@ int pxb_get_ops(pxb_ctx *ctx, double *ops);
 
 /* g-build without any device allocation.  No counterpart in the reference: it serves callers that cannot
  * call cudaMalloc (their device memory belongs to another allocator, or they cannot afford its implicit
- * synchronisation).  Inputs and outputs are device memory owned by the caller: neigh_off_d (n+1),
- * neigh_id0_d (nbtot, 0-BASED ids), coords3_d (3n, xyz), vols_d (n), ops_d (nbtot*nop, double, or float with
- * PXB_MIXED), degenerate_d (n bytes, may be NULL); stream is a cudaStream_t (NULL = legacy default stream).
- * Working memory is one fixed 4 MiB device array shared by all calls on a device, which limits n to
+ * synchronisation).  Inputs and outputs are device memory owned by the caller: neigh_off_d (n+1; neigh_off_d[0]
+ * == 0, non-decreasing, neigh_off_d[n] == nbtot), neigh_id0_d (nbtot, 0-BASED ids in [0, n)), coords3_d (3n,
+ * xyz), vols_d (n), layer_d (n ghost layer indices, 0 bulk; may be NULL: then deep ghosts are not told apart and
+ * a degenerate family anywhere is an error, whereas with it nodes of layer > 1 get zero operators as in
+ * pxb_gbuild), ops_d (nbtot*nop, double, or float with PXB_MIXED), defect_d (PXB_MIXED at order 2 only: n *
+ * (nop - dim) * dim floats receiving the per-node first moments of the stored second-derivative operators,
+ * the correction the mixed apply subtracts, laid out [node][k - dim][m]; may be NULL, and then no correction
+ * data is produced, so second derivatives from the FP32 operators alone carry an error of order 1e-7 * L/h),
+ * degenerate_d (n bytes, may be NULL); stream is a cudaStream_t (NULL = legacy default stream).  The family
+ * arrays are checked on the device first; a malformed list gives PXB_ERR_INVALID and no build.  Working memory
+ * is one fixed 4 MiB device array shared by all calls on a device, which limits n to
  * pxb_gbuild_noalloc_max_nodes(dim) (262,128 nodes in 2D, 131,064 in 3D); larger n is rejected with
  * PXB_ERR_INVALID.  The first call on a device resolves the array's address, so make it before any stream
  * capture; calls that overlap on the GPU race on the shared array.  Synchronises the stream before returning
- * (the degenerate counters are read back). */
+ * (the input check and the degenerate counters are read back). */
 int pxb_gbuild_noalloc_d(int dim, int order, int precision, int n, long long nbtot, const int *neigh_off_d,
-                         const int *neigh_id0_d, const double *coords3_d, const double *vols_d, double delta,
-                         double dx_char, void *ops_d, uint8_t *degenerate_d, int *n_degenerate, int *first_degenerate,
-                         void *stream);
+                         const int *neigh_id0_d, const double *coords3_d, const double *vols_d, const int *layer_d,
+                         double delta, double dx_char, void *ops_d, float *defect_d, uint8_t *degenerate_d,
+                         int *n_degenerate, int *first_degenerate, void *stream);
 int pxb_gbuild_noalloc_max_nodes(int dim);
 
 /* ---- family-sum derivative apply ---------------------------------------------------------------------------
@@ -147,6 +158,19 @@ int pxb_epf_setup(pxb_ctx *ctx, int precision, double C11, double C12, double C6
 /* One rate evaluation at u (N*dim): damage then force, a = (L+b)/rho (the reference CUDA entry
  * assembleExplicitPDDOFracAccel).  *n_broken = bonds that broke in this call. */
 int pxb_epf_rate(pxb_ctx *ctx, const double *u, double *accel, long long *n_broken);
+/* The reference boundary's explicit drop-in call perix_cuda::assembleExplicitPDDOFracAccel
+ * (include/PDSystem/CudaAssemble.h:251-254 of the reference; shim in include/perix_cuda_compat.h) as a plain C entry
+ * for FFI callers: mesh (N, dim, 1-based families, xyz coords, volumes, delta, dx_char) and element constants as the
+ * reference's AssembleMesh / ExplicitPDDOFracParams carry them, u (N*dim), health_inout (nbtot doubles, 1/0,
+ * updated when a bond breaks), accel_out (N*dim), *health_changed.  Uses the shim's default context (its schedule is
+ * tuned at the first call of a problem).  Returns 1 on success, 0 where the C++ call returns false (reason on
+ * stderr); pxb_cuda_shutdown releases the shim's context (perix_cuda::shutdown). */
+int pxb_cuda_explicit_accel(int n, int dim, const int *neigh_off, const int *neigh_id, const double *coords,
+                            const double *vols, double delta, double dx_char, double C11, double C12, double C66,
+                            double rho, const double *body, double sc, int tension_only, int damage_on,
+                            const double *u, double *health_inout, double *accel_out, int *health_changed);
+void pxb_cuda_shutdown(void);
+
 /* Output projections of the explicit state, the device twin of ExplicitPDDOFracElement::computeNodalProjection
  * (src/ElmtSystem/ExplicitPDDOFracElement.cpp:324-405): per node damage = 1 - intact/all bonds, von Mises stress,
  * Cauchy stress and small strain (3x3 row-major, 9 values per node) from the PDDO displacement gradient over the
@@ -161,8 +185,11 @@ int pxb_epf_project(pxb_ctx *ctx, const double *u, int plane_strain, double *dam
 /* Boundary-condition program applied after every central-difference update, in list order (reference
  * BCSystem::presetSolution, src/BCSystem/BCSystem.cpp:114-129).  Entry e: kind 0 Dirichlet (reflect across
  * the mirror bulk, or direct when direct[e] or no mirror), kind 1 Neumann copy; comp_mask bit a selects
- * component a; value/velocity dim doubles each (g(t)=value+velocity*t); has_box/box (6 doubles,
- * inclusive, on node coordinates); nodes 1-based in node_off[e]..node_off[e+1]. */
+ * component a; value/velocity dim doubles each (g(t)=value+velocity*t); has_box/box (6 doubles xmin,xmax,
+ * ymin,ymax,zmin,zmax, inclusive, on the xyz node coordinates with z = 0 in 2D; an axis whose min exceeds its max
+ * is unconstrained, as DirichletBC::insideBox, src/BCSystem/DirichletBC.cpp:89-98); nodes 1-based in
+ * node_off[e]..node_off[e+1].  A Neumann entry naming a node without a mirror bulk node is rejected
+ * (PXB_ERR_INVALID), where the reference aborts the run. */
 int pxb_epf_set_bcs(pxb_ctx *ctx, int nbc, const int *kind, const int *comp_mask, const int *direct,
                     const double *value, const double *velocity, const int *has_box, const double *box,
                     const int *node_off, const int *nodes);
@@ -173,6 +200,14 @@ int pxb_epf_start(pxb_ctx *ctx, const double *u0, const double *v0, double dt);
 /* Advance nsteps uniform steps on the device (captured into CUDA graphs of `chunk` steps; chunk<=0 picks a
  * default).  Returns PXB_ERR_BLOWUP with *bad_step (1-based) if the reference blow-up guard trips. */
 int pxb_epf_advance(pxb_ctx *ctx, int nsteps, int chunk, int *bad_step);
+/* Advance to the end time t_end exactly as the reference's explicit loop does (TimeStepping::solveExplicitDynamics,
+ * src/TimeStepping/TimeStepping.cpp:495-599): while t < t_end - 1e-12 t_end, the attempted step is min(dt, t_end - t);
+ * a step of the previous step's length is a uniform central-difference step (graph-captured chunks as in
+ * pxb_epf_advance), any other - the clamped last step - takes the variable-step form
+ * u + (dt/dt_prev)(u - u_prev) + dt (dt + dt_prev)/2 a (TimeStepping.cpp:537-545), with the BC pass at its new time
+ * and the blow-up guard.  *steps_taken (may be NULL) receives the number of steps.  pxb_epf_advance itself always
+ * takes uniform steps of dt. */
+int pxb_epf_advance_to(pxb_ctx *ctx, double t_end, int chunk, int *bad_step, long long *steps_taken);
 /* Read back state: u (N*dim), u_prev (N*dim), health (nbtot, as 1/0 bytes), t.  Any pointer may be NULL. */
 int pxb_epf_get_state(pxb_ctx *ctx, double *u, double *u_prev, uint8_t *health, double *t);
 /* Overwrite state (u, u_prev, health may be NULL to keep). */
@@ -193,14 +228,10 @@ int pxb_epf_force_frozen_d(pxb_ctx *ctx, const double *u_d, double *a_d);
  * sweeps and finite-difference checks of d/dE. */
 int pxb_epf_set_constants(pxb_ctx *ctx, double C11, double C12, double C66, double rho);
 
-/* ---- measurement support -----------------------------------------------------------------------------------
+/* ---- explicit-state snapshot and schedule autotuning --------------------------------------------------------
  * Device-side copy of the explicit state (u, u_prev, health, t) and its restore. */
 int pxb_epf_snapshot(pxb_ctx *ctx);
 int pxb_epf_restore(pxb_ctx *ctx);
-/* nsteps explicit steps launched one at a time; before each launch the L2 is flushed by writing flush_bytes
- * (0 = none) and every restore_every steps (0 = never) the snapshot is restored; ms[s] = CUDA-event duration
- * of step s's kernel alone.  The blow-up guard is not evaluated. */
-int pxb_epf_time_steps(pxb_ctx *ctx, int nsteps, size_t flush_bytes, int restore_every, float *ms);
 /* Schedule variants of the explicit kernel: 0-2 lane groups (lanes per node x bonds per lane per pass), 3-4
  * CSR-stream tiles, 5 and up TMA-staged tiles (time step only; the other modes of a staged variant run
  * variant 1).  pxb_epf_variant_count() gives their number.  pxb_epf_autotune times every variant that fits
@@ -210,17 +241,13 @@ int pxb_epf_time_steps(pxb_ctx *ctx, int nsteps, size_t flush_bytes, int restore
  * pxb_epf_variant_count() entries) receives the mean step time of each variant, -1 for one that does not fit. */
 int pxb_epf_variant_count(void);
 int pxb_epf_autotune(pxb_ctx *ctx, int steps, size_t flush_bytes, int use_cache, int *best, float *ms_per_variant);
+/* The same for the per-step rate call (pxb_epf_rate: damage, force, acceleration out) at the caller's
+ * displacement u (host, N*dim): every fitting variant's kernel is timed over reps launches, the bond health and
+ * counters are restored around them (the state is unchanged), and the choice is cached per signature.  Needs
+ * pxb_epf_setup, not pxb_epf_start; the perix_cuda:: shim runs it once per problem at its first call. */
+int pxb_epf_autotune_rate(pxb_ctx *ctx, const double *u, int reps, int use_cache, int *best, float *ms_per_variant);
 int pxb_epf_set_variant(pxb_ctx *ctx, int variant);
 int pxb_epf_get_variant(pxb_ctx *ctx, int *variant, int *lanes_per_node);
-/* reps g-builds into the existing operator cache (same order/precision as the last pxb_gbuild), L2 flushed
- * before each; ms[r] = CUDA-event duration of build r. */
-int pxb_gbuild_time(pxb_ctx *ctx, int order, int precision, int reps, size_t flush_bytes, float *ms);
-/* The fixed cost inside each timed step: reps launches of an empty kernel with the launch shape (grid, block,
- * dynamic shared memory, returned) of the last TMA-staged step launch, each after the same L2 flush and timed
- * with CUDA events exactly like a step; ms[r] per launch.  No counterpart in the reference (measurement
- * support only). */
-int pxb_epf_launch_floor(pxb_ctx *ctx, size_t flush_bytes, int reps, float *ms, int *grid, int *block,
-                         size_t *smem);
 
 /* ---- batched clouds ----------------------------------------------------------------------------------------
  * Many independent node clouds (2D and 3D mixed, boundary-truncated families of uneven size) in one
@@ -249,13 +276,11 @@ int pxb_batch_apply(pxb_ctx *ctx, const double *u, double *out);
 int pxb_batch_apply_d(pxb_ctx *ctx, const double *u_d, double *out_d);
 int pxb_batch_get_ops(pxb_ctx *ctx, int cloud, double *ops);
 /* Schedules (which 0: g-build, 1: apply): lanes per node for 2D and 3D clouds and one launch for both
- * dimensions or one per dimension; pxb_batch_variant_count() of each.  pxb_batch_time times `reps` launches of
- * the current schedule (L2 flushed before each; the apply on device buffers u_d -> out_d), pxb_batch_autotune
- * times every schedule and keeps the fastest. */
+ * dimensions or one per dimension; pxb_batch_variant_count() of each.  pxb_batch_autotune times every schedule
+ * (`reps` launches, L2 flushed before each; the apply on device buffers u_d -> out_d) and keeps the fastest. */
 int pxb_batch_variant_count(void);
 int pxb_batch_set_variant(pxb_ctx *ctx, int which, int variant);
 int pxb_batch_get_variant(pxb_ctx *ctx, int which, int *variant);
-int pxb_batch_time(pxb_ctx *ctx, int what, int reps, size_t flush_bytes, const double *u_d, double *out_d, float *ms);
 int pxb_batch_autotune(pxb_ctx *ctx, int what, int reps, size_t flush_bytes, const double *u_d, double *out_d,
                        int *best, float *ms_per_variant);
 

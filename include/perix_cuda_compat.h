@@ -5,10 +5,12 @@
  * callers (FormResidualAndJacobianCUDA.cpp, ExplicitPDDOFracElement.cpp:174-235) fill and pass exactly these.
  *
  * Behavioural differences, by design:
- *   - there is no CPU fallback: a device failure prints the reason to stderr and returns false, and the
- *     caller's fallback branch should be replaced by a hard error;
- *   - assembleStressCahnHilliard and assembleCached (the stress-coupled CH and implicit dynamic-fracture
- *     kernels) are not implemented by this backend yet and return false with a message.
+ *   - there is no CPU fallback inside the backend: a device failure prints the reason to stderr and returns
+ *     false, which is where the reference's callers take their CPU path; a build that must never run on the CPU
+ *     replaces that branch by an abort;
+ *   - a mesh with a per-node horizon (AssembleMesh::nodeHorizon set) is refused with a message (return false);
+ *   - assembleExplicitPDDOFracAccel times its schedules once per problem at its first call and keeps FP64
+ *     operators unless the environment sets PERIX_B200_PRECISION=mixed.
  * The device work runs on a lazily created default pxb_ctx (device 0), freed by shutdown().
  */
 #pragma once

@@ -13,5 +13,6 @@ tests to check the stress-coupled Cahn-Hilliard assembler.
 
 The product (``perix_b200``) never imports this package.
 """
-from .lib import (PortOracle, RefMesh, RefEpf, port_available, ref_available, bc_program_arrays,  # noqa: F401
+from .lib import (PortOracle, RefMesh, RefEpf, port_available, ref_available, dropin_available,  # noqa: F401
+                  bc_program_arrays,
                   ORACLE_DIR, ref_cuda_available, ref_cuda_epf_bench, ref_cuda_stress_ch)

@@ -8,6 +8,7 @@ import numpy as np
 ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 _PORT_SO = os.path.join(ORACLE_DIR, "_ref", "libpddo_oracle.so")
 _REF_SO = os.path.join(ORACLE_DIR, "_ref", "libperix_ref.so")
+_DROPIN_SO = os.path.join(ORACLE_DIR, "_ref", "libperix_ref_dropin.so")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -281,44 +282,67 @@ def ref_cuda_stress_ch(dim, coords3, vols, off, ids, delta, dx_char, rowptr, col
     return kv, rhs
 
 
-def _ref_lib():
-    global _REF
+_DROPIN = None
+
+
+def dropin_available():
+    return os.path.exists(_DROPIN_SO)
+
+
+def _ref_lib(dropin=False):
+    """The reference harness library; dropin=True loads the build whose reference callers (compiled with
+    -DPERIX_CUDA_ASSEMBLE) are linked to libperix_b200.so."""
+    global _REF, _DROPIN
+    if dropin:
+        if _DROPIN is None:
+            if not dropin_available():
+                raise RuntimeError("drop-in harness not built: run `make -C oracle dropin` where the reference is present")
+            _DROPIN = _bind_ref(C.CDLL(_DROPIN_SO))
+        return _DROPIN
     if _REF is None:
         if not ref_available():
             raise RuntimeError("reference harness not built: run `make -C oracle ref` where the reference is present")
-        L = C.CDLL(_REF_SO)
-        vp = C.c_void_p
-        L.ref_mesh_structured.restype = vp
-        L.ref_mesh_cloud.restype = vp
-        L.ref_mesh_nodes.restype = C.c_int
-        L.ref_mesh_bonds.restype = C.c_longlong
-        L.ref_group_size.restype = C.c_int
-        L.ref_crack_cuts.restype = C.c_int
-        L.ref_gbuild_time.restype = C.c_double
-        L.ref_csr_nnz.restype = C.c_int
-        L.ref_poisson_assemble.restype = C.c_double
-        L.ref_ch_assemble.restype = C.c_double
-        L.ref_stress_ch_assemble.restype = C.c_double
-        L.ref_dynfrac_assemble.restype = C.c_double
-        L.ref_epf_create.restype = vp
-        L.ref_epf_rate.restype = C.c_double
-        L.ref_epf_run.restype = C.c_double
-        L.ref_max_threads.restype = C.c_int
-        for name in ("ref_mesh_free", "ref_mesh_nodes", "ref_mesh_bonds", "ref_mesh_scalars", "ref_mesh_get",
-                     "ref_group_size", "ref_group_get", "ref_crack_cuts", "ref_qindices", "ref_gbuild",
-                     "ref_gbuild_time", "ref_apply", "ref_csr_nnz", "ref_csr_pattern", "ref_poisson_assemble",
-                     "ref_epf_free", "ref_epf_rate", "ref_epf_set_health", "ref_epf_constants", "ref_epf_opcache",
-                     "ref_bc_preset", "ref_epf_run"):
-            getattr(L, name).argtypes = None
-        _REF = L
+        _REF = _bind_ref(C.CDLL(_REF_SO))
     return _REF
+
+
+def _bind_ref(L):
+    vp = C.c_void_p
+    L.ref_mesh_structured.restype = vp
+    L.ref_mesh_cloud.restype = vp
+    L.ref_mesh_nodes.restype = C.c_int
+    L.ref_mesh_bonds.restype = C.c_longlong
+    L.ref_group_size.restype = C.c_int
+    L.ref_crack_cuts.restype = C.c_int
+    L.ref_gbuild_time.restype = C.c_double
+    L.ref_csr_nnz.restype = C.c_int
+    L.ref_poisson_assemble.restype = C.c_double
+    L.ref_ch_assemble.restype = C.c_double
+    L.ref_stress_ch_assemble.restype = C.c_double
+    L.ref_dynfrac_assemble.restype = C.c_double
+    L.ref_epf_create.restype = vp
+    L.ref_epf_rate.restype = C.c_double
+    L.ref_epf_run.restype = C.c_double
+    L.ref_max_threads.restype = C.c_int
+    for name in ("ref_mesh_free", "ref_mesh_nodes", "ref_mesh_bonds", "ref_mesh_scalars", "ref_mesh_get",
+                 "ref_group_size", "ref_group_get", "ref_crack_cuts", "ref_qindices", "ref_gbuild",
+                 "ref_gbuild_time", "ref_apply", "ref_csr_nnz", "ref_csr_pattern", "ref_poisson_assemble",
+                 "ref_epf_free", "ref_epf_rate", "ref_epf_set_health", "ref_epf_constants", "ref_epf_opcache",
+                 "ref_bc_preset", "ref_epf_run"):
+        getattr(L, name).argtypes = None
+    L.ref_system_assemble.restype = C.c_double
+    L.ref_epf_run_to.restype = C.c_int
+    L.ref_epf_use_cuda.restype = C.c_int
+    L.ref_is_dropin.restype = C.c_int
+    return L
 
 
 class RefMesh:
     """A PD mesh built by the reference's own generators/createPDMesh/createNeighborNodes."""
 
-    def __init__(self, handle, dim, order):
-        self.L = _ref_lib()
+    def __init__(self, handle, dim, order, dropin=False):
+        self.L = _ref_lib(dropin)
+        self.dropin = dropin
         self.h = C.c_void_p(handle)
         self.dim = dim
         self.order = order
@@ -338,15 +362,16 @@ class RefMesh:
         self.ids = self.ids[:self.nb]
 
     @classmethod
-    def structured(cls, dim, nx, ny, nz, box, factor, order=2, cracks=None, planes=None, force_only=False):
-        L = _ref_lib()
+    def structured(cls, dim, nx, ny, nz, box, factor, order=2, cracks=None, planes=None, force_only=False,
+                   dropin=False):
+        L = _ref_lib(dropin)
         b = np.ascontiguousarray(list(box) + [0.0] * (6 - len(box)), np.float64)
         cr = None if not cracks else np.ascontiguousarray(cracks, np.float64).reshape(-1)
         pl = None if not planes else np.ascontiguousarray(planes, np.float64).reshape(-1)
         h = L.ref_mesh_structured(int(dim), int(nx), int(ny), int(nz), _ptr(b, C.c_double), C.c_double(factor),
                                   int(order), int(force_only), 0 if cr is None else cr.size // 4,
                                   _ptr(cr, C.c_double), 0 if pl is None else pl.size // 12, _ptr(pl, C.c_double))
-        m = cls(h, dim, order)
+        m = cls(h, dim, order, dropin)
         m.cracks = cr
         m.planes = pl
         m.force_only = force_only
@@ -472,6 +497,22 @@ class RefMesh:
                                     _ptr(consts, C.c_double))
         return kv, rhs, vel, health[:self.nb], consts
 
+    def system_assemble(self, type_, coef, f, u, dt=0.0, uold=None, use_cuda=False):
+        """K (CSR values on the reference pattern) and rhs of a single PoissonElement (type 0: sigma = coef) or
+        DiffusionElement (type 1: D = coef, transient with dt and uold) through the reference's
+        PDSystem::formResidualAndJacobian, or with use_cuda through its formResidualAndJacobianCUDA caller (the
+        drop-in build, where that caller runs this backend's perix_cuda::assemble).  Returns kv, rhs, seconds."""
+        nnz = self.L.ref_csr_nnz(self.h, 1)
+        kv = np.zeros(nnz, np.float64)
+        rhs = np.zeros(self.n, np.float64)
+        f64 = lambda a: np.ascontiguousarray(a, np.float64)
+        t = self.L.ref_system_assemble(self.h, int(type_), C.c_double(coef), C.c_double(f), C.c_double(dt),
+                                       _ptr(f64(u), C.c_double), _ptr(None if uold is None else f64(uold), C.c_double),
+                                       _ptr(kv, C.c_double), _ptr(rhs, C.c_double), int(bool(use_cuda)))
+        if t < 0:
+            raise RuntimeError("use_cuda needs the drop-in build of the reference harness")
+        return kv, rhs, t
+
     def bc_preset(self, bcs, t, u):
         p = bc_program_arrays(bcs, self.dim)
         uu = np.ascontiguousarray(u, np.float64).copy()
@@ -492,7 +533,7 @@ class RefEpf:
     """The reference ExplicitPDDOFracElement bound to a RefMesh."""
 
     def __init__(self, mesh, E, nu, rho, G0, plane_stress=False, tension_only=True, damage_on=True, b=(0, 0, 0)):
-        self.L = _ref_lib()
+        self.L = _ref_lib(getattr(mesh, "dropin", False))
         self.mesh = mesh
         self.h = C.c_void_p(self.L.ref_epf_create(mesh.h, C.c_double(E), C.c_double(nu), C.c_double(rho),
                                                   C.c_double(G0), int(plane_stress), int(tension_only),
@@ -514,6 +555,12 @@ class RefEpf:
         out = np.zeros(self.mesh.n * (1 if k < 2 else 9), np.float64)
         self.L.ref_epf_project(self.h, k, _ptr(np.ascontiguousarray(u, np.float64), C.c_double), _ptr(out, C.c_double))
         return out if k < 2 else out.reshape(-1, 9)
+
+    def use_cuda(self, on=True):
+        """LocalElmtInfo::UseCuda of the following rate calls: the reference element then runs its
+        perix_cuda::assembleExplicitPDDOFracAccel branch (drop-in build only)."""
+        if self.L.ref_epf_use_cuda(self.h, int(bool(on))) != 0:
+            raise RuntimeError("use_cuda needs the drop-in build of the reference harness")
 
     def set_health(self, h):
         self.L.ref_epf_set_health(self.h, _ptr(np.ascontiguousarray(h, np.float64), C.c_double))
@@ -543,6 +590,27 @@ class RefEpf:
                                _ptr(p["off"], C.c_int), _ptr(p["nodes"], C.c_int), _ptr(u, C.c_double),
                                _ptr(uo, C.c_double), _ptr(h, C.c_double), int(nthreads or os.cpu_count()))
         return u, uo, h, t
+
+    def run_to(self, u0, v0, dt, t_end, bcs, nthreads=0):
+        """The reference loop to t_end (clamped variable-dt last step, BC preset, blow-up guard); returns u, uold,
+        health, the number of completed steps, the 1-based step at which the guard tripped (0 if none), and t."""
+        m = self.mesh
+        p = bc_program_arrays(bcs, m.dim)
+        u = np.zeros(m.n * m.dim, np.float64)
+        uo = np.zeros(m.n * m.dim, np.float64)
+        h = np.zeros(m.nb, np.float64)
+        trip = C.c_int(0)
+        t = C.c_double(0.0)
+        steps = self.L.ref_epf_run_to(self.h, _ptr(np.ascontiguousarray(u0, np.float64), C.c_double),
+                                      _ptr(None if v0 is None else np.ascontiguousarray(v0, np.float64), C.c_double),
+                                      C.c_double(dt), C.c_double(t_end), p["nbc"], _ptr(p["kind"], C.c_int),
+                                      _ptr(p["mask"], C.c_int), _ptr(p["direct"], C.c_int),
+                                      _ptr(p["val"], C.c_double), _ptr(p["vel"], C.c_double),
+                                      _ptr(p["has_box"], C.c_int), _ptr(p["box"], C.c_double),
+                                      _ptr(p["off"], C.c_int), _ptr(p["nodes"], C.c_int), _ptr(u, C.c_double),
+                                      _ptr(uo, C.c_double), _ptr(h, C.c_double), C.byref(trip), C.byref(t),
+                                      int(nthreads or os.cpu_count()))
+        return u, uo, h, int(steps), trip.value, t.value
 
     def __del__(self):
         try:

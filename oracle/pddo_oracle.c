@@ -580,10 +580,14 @@ void orc_bc_preset(int n, int dim, const double *coords3, const int *mirror, int
             const int mb = (mirror && id >= 1 && id <= n) ? mirror[id - 1] : 0;
             if (kind[e] == 0) {
                 if (has_box[e]) {
+                    /* DirichletBC::insideBox (DirichletBC.cpp:89-98): all three axes on the xyz coordinates, an
+                       axis with min > max is unconstrained */
                     int inside = 1;
-                    for (int a = 0; a < dim; ++a) {
+                    for (int a = 0; a < 3; ++a) {
+                        const double lo = box[6 * e + 2 * a], hi = box[6 * e + 2 * a + 1];
+                        if (lo > hi) continue;
                         const double x = coords3[(size_t)(id - 1) * 3 + a];
-                        if (x < box[6 * e + 2 * a] || x > box[6 * e + 2 * a + 1]) inside = 0;
+                        if (x < lo || x > hi) inside = 0;
                     }
                     if (!inside) continue;
                 }

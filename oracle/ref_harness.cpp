@@ -13,14 +13,27 @@
 //   explicit fracture rate  ExplicitPDDOFracElement::preprocessIteration              (ExplicitPDDOFracElement.cpp:85)
 //   stress-coupled CH       StressCahnHilliardElement preprocess + nodal/bond callbacks (StressCahnHilliardElement.cpp:139-466)
 //   implicit dyn. fracture  PDDODynamicFracElement preprocess (init + one commit) + callbacks (PDDODynamicFracElement.cpp:82-306)
-// The central-difference loop and the ghost BC preset are short restatements of
-// TimeStepping.cpp:479-547 and DirichletBC.cpp:107-147 / NeumannBC.cpp:88-105 (those translation units pull
-// in the JSON/BC registry and are not needed to reproduce their arithmetic).
+//   ghost BC preset         DirichletBC::presetSolutionAtTime / NeumannBC::presetSolution, applied in list
+//                           order like BCSystem::presetSolution                       (DirichletBC.cpp:107-147,
+//                                                                                      NeumannBC.cpp:88-105,
+//                                                                                      BCSystem.cpp:114-129)
+//   scalar system assembly  PDSystem::formResidualAndJacobian with a registered PoissonElement or
+//                           DiffusionElement                                          (FormResidualAndJacobian.cpp)
+// The central-difference loop is a short restatement of TimeStepping.cpp:479-547 (that translation unit pulls in
+// the whole run-time system).
+//
+// Built a second time with -DPERIX_CUDA_ASSEMBLE into oracle/_ref/libperix_ref_dropin.so, together with the
+// reference's own callers of the CUDA-assembly boundary (PDSystem::formResidualAndJacobianCUDA and
+// ExplicitPDDOFracElement's UseCuda branch, compiled unchanged against a forwarding PDSystem/CudaAssemble.h) and
+// linked to libperix_b200.so: ref_system_assemble(..., use_cuda=1) and ref_epf_use_cuda then run the reference's
+// callers through this backend's perix_cuda:: shim.
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <string>
 #include <vector>
@@ -34,9 +47,14 @@
 #include "ElmtSystem/ExplicitPDDOFracElement.h"
 #include "PDOperators/PDOperators.h"
 #undef private
+#include "BCSystem/DirichletBC.h"
+#include "BCSystem/NeumannBC.h"
 #include "ElmtSystem/CahnHilliardElement.h"
+#include "ElmtSystem/DiffusionElement.h"
+#include "ElmtSystem/ElmtSystem.h"
 #include "ElmtSystem/PDDODynamicFracElement.h"
 #include "ElmtSystem/PoissonElement.h"
+#include "PDSystem/PDSystem.h"
 #include "ElmtSystem/StressCahnHilliardElement.h"
 #include "MathUtils/SparseMatrix.h"
 #include "Mesh/MeshGenerator.h"
@@ -55,6 +73,7 @@ struct RefMesh {
 struct RefEpf {
     ExplicitPDDOFracElement el;
     RefMesh *mesh = nullptr;
+    bool use_cuda = false;  // LocalElmtInfo::UseCuda of the rate calls (drop-in build only)
 };
 
 void setupOps(RefMesh *m) {
@@ -612,6 +631,7 @@ double ref_epf_rate(void *h, const double *u, double *accel, double *health_out,
     std::memcpy(U.getDataPtr(), u, sizeof(double) * (size_t)n * dim);
     LocalElmtInfo info;
     info.UseParallel = nthreads != 1;
+    info.UseCuda = e->use_cuda;
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
@@ -660,48 +680,57 @@ void ref_epf_opcache(void *h, double *out) {
 }
 
 // ---- ghost BC preset + central-difference loop ------------------------------------------------------------
-// A BC program is a list of entries applied in order (BCSystem.cpp:114-129).  Entry e:
+// A BC program is a list of entries applied in order, as BCSystem::presetSolution does (BCSystem.cpp:114-129),
+// each by the reference's own DirichletBC / NeumannBC object.  Entry e:
 //   kind[e]    0 = Dirichlet (reflect, or direct when direct[e]!=0 or no mirror), 1 = Neumann copy
-//   comp_mask  bit a set => component a (0-based) is constrained
+//   comp_mask  bit a set => component a (0-based) is constrained (the objects take 1-based components)
 //   val/vel    dim values each: g(t) = value + velocity*t
-//   box        has_box[e] and 6 bounds (xlo,xhi,ylo,yhi,zlo,zhi), tested on the node's coords inclusively
+//   box        has_box[e] and 6 bounds (xlo,xhi,ylo,yhi,zlo,zhi): DirichletBC::setBox
 //   nodes      1-based ids (node_off[e]..node_off[e+1])
 void ref_bc_preset(void *h, int nbc, const int *kind, const int *comp_mask, const int *direct, const double *val,
                    const double *vel, const int *has_box, const double *box, const int *node_off, const int *nodes,
                    double t, double *u) {
     auto *m = static_cast<RefMesh *>(h);
-    const auto &d = m->pd.getDataConstRef();
     const int dim = m->dim;
+    const int n = m->pd.getNodesNum();
+    VectorXd U(n * dim);
+    std::memcpy(U.getDataPtr(), u, sizeof(double) * (size_t)n * dim);
     for (int e = 0; e < nbc; ++e) {
-        for (int p = node_off[e]; p < node_off[e + 1]; ++p) {
-            const int id = nodes[p];
-            const int mb = (id - 1 < (int)d.GhostMirrorBulkID.size()) ? d.GhostMirrorBulkID[id - 1] : 0;
-            if (kind[e] == 0) {
-                if (has_box[e]) {
-                    bool inside = true;
-                    for (int a = 0; a < dim; ++a) {
-                        const double x = d.NodeCoords[(size_t)(id - 1) * 3 + a];
-                        if (x < box[6 * e + 2 * a] || x > box[6 * e + 2 * a + 1]) inside = false;
-                    }
-                    if (!inside) continue;
-                }
-                for (int a = 0; a < dim; ++a) {
-                    if (!(comp_mask[e] & (1 << a))) continue;
-                    const double g = val[e * dim + a] + vel[e * dim + a] * t;
-                    u[(size_t)(id - 1) * dim + a] = (mb >= 1 && !direct[e]) ? 2.0 * g - u[(size_t)(mb - 1) * dim + a] : g;
-                }
-            } else {
-                if (mb < 1) continue;
-                for (int a = 0; a < dim; ++a)
-                    if (comp_mask[e] & (1 << a)) u[(size_t)(id - 1) * dim + a] = u[(size_t)(mb - 1) * dim + a];
+        std::vector<int> comps;
+        std::vector<double> v, w;
+        for (int a = 0; a < dim; ++a)
+            if (comp_mask[e] & (1 << a)) {
+                comps.push_back(a + 1);
+                v.push_back(val[e * dim + a]);
+                w.push_back(vel[e * dim + a]);
             }
+        if (comps.empty()) continue;  // an empty list would mean every component to the reference objects
+        const std::vector<int> ids(nodes + node_off[e], nodes + node_off[e + 1]);
+        if (kind[e] == 0) {
+            DirichletBC bc;
+            bc.setValues(v);
+            bc.setVelocity(w);
+            bc.setComponents(comps);
+            bc.setDirect(direct[e] != 0);
+            if (has_box[e]) {
+                std::array<double, 6> b6;
+                for (int k = 0; k < 6; ++k) b6[(size_t)k] = box[6 * e + k];
+                bc.setBox(b6);
+            }
+            bc.presetSolutionAtTime(m->pd, ids, dim, U, t);
+        } else {
+            NeumannBC bc;
+            bc.setComponents(comps);
+            bc.presetSolutionAtTime(m->pd, ids, dim, U, t);
         }
     }
+    std::memcpy(u, U.getDataPtr(), sizeof(double) * (size_t)n * dim);
 }
 
 // Central difference (TimeStepping.cpp:479-547): start u^{-1}=u0-dt v0+dt^2/2 a0, then nsteps uniform steps
 // u^{n+1}=2u^n-u^{n-1}+dt^2 a^n followed by the BC preset at t_{n+1}.  u0 in, u/uold out (post-BC),
-// health_out the per-bond health after the run; returns seconds spent in the whole loop.
+// health_out the per-bond health after the run; returns seconds spent in the nsteps steps (the start, whose rate
+// call also builds the element's operator cache on a fresh element, is not counted).
 double ref_epf_run(void *h, const double *u0, const double *v0, double dt, int nsteps, int nbc, const int *kind,
                    const int *comp_mask, const int *direct, const double *val, const double *vel, const int *has_box,
                    const double *box, const int *node_off, const int *nodes, double *u_out, double *uold_out,
@@ -710,9 +739,9 @@ double ref_epf_run(void *h, const double *u0, const double *v0, double dt, int n
     auto *m = e->mesh;
     const int n = m->pd.getNodesNum() * m->dim;
     std::vector<double> U(u0, u0 + n), Uo(n), A(n);
-    auto t0 = std::chrono::steady_clock::now();
     ref_epf_rate(h, U.data(), A.data(), nullptr, nthreads);
     for (int k = 0; k < n; ++k) Uo[k] = U[k] - dt * (v0 ? v0[k] : 0.0) + 0.5 * dt * dt * A[k];
+    auto t0 = std::chrono::steady_clock::now();
     double t = 0.0;
     const double dt2 = dt * dt;
     for (int s = 0; s < nsteps; ++s) {
@@ -731,6 +760,149 @@ double ref_epf_run(void *h, const double *u0, const double *v0, double dt, int n
     if (uold_out) std::memcpy(uold_out, Uo.data(), sizeof(double) * n);
     if (health_out) std::memcpy(health_out, e->el.m_HealthFlat.data(), sizeof(double) * e->el.m_HealthFlat.size());
     return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// ---- scalar system assembly through the reference's PDSystem --------------------------------------------
+// type 0: PoissonElement(sigma = coef, f), type 1: DiffusionElement(D = coef, f) with Info.Dt = dt and Uold.
+// use_cuda 0 runs PDSystem::formResidualAndJacobian (the reference CPU assembly); use_cuda 1 runs
+// PDSystem::formResidualAndJacobianCUDA, the reference's caller of perix_cuda::assemble (drop-in build only;
+// returns -1 elsewhere).  K = -dF/dU, RHS = +F on the reference CSR pattern (SparseMatrix::initFromPDMesh).
+// Returns seconds spent in the assembly call.
+double ref_system_assemble(void *h, int type, double coef, double f, double dt, const double *u, const double *uold,
+                           double *kvals, double *rhs, int use_cuda) {
+    auto *m = static_cast<RefMesh *>(h);
+    const auto &d = m->pd.getDataConstRef();
+    const int n = d.NodesNum;
+    ElmtSystem es;
+    if (type == 0) {
+        auto el = std::make_unique<PoissonElement>(coef, f);
+        el->setDim(m->dim);
+        es.addElement("poisson", std::move(el));
+    } else {
+        auto el = std::make_unique<DiffusionElement>();
+        el->setDim(m->dim);
+        el->setD(coef);
+        el->setF(f);
+        es.addElement("diffusion", std::move(el));
+    }
+    SparseMatrix K;
+    K.initFromPDMesh(d, 1);
+    K.setToZeros();
+    VectorXd U(n), Uo(n), R(n);
+    std::memcpy(U.getDataPtr(), u, sizeof(double) * (size_t)n);
+    if (uold) std::memcpy(Uo.getDataPtr(), uold, sizeof(double) * (size_t)n);
+    LocalElmtInfo info;
+    info.Dt = dt;
+    PDSystem sys;
+    auto t0 = std::chrono::steady_clock::now();
+    if (use_cuda) {
+#ifdef PERIX_CUDA_ASSEMBLE
+        sys.formResidualAndJacobianCUDA(m->pd, m->ops, es, info, U, Uo, K, R);
+#else
+        return -1.0;
+#endif
+    } else {
+        sys.formResidualAndJacobian(m->pd, m->ops, es, info, U, Uo, K, R);
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    std::memcpy(kvals, K.getCSRValuesPtr(), sizeof(double) * (size_t)K.getNNZNum());
+    std::memcpy(rhs, R.getDataPtr(), sizeof(double) * (size_t)n);
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// LocalElmtInfo::UseCuda for the element's rate calls: the reference element then hands the damage and force
+// to perix_cuda::assembleExplicitPDDOFracAccel (drop-in build only; returns -1 elsewhere).
+int ref_epf_use_cuda(void *h, int on) {
+#ifdef PERIX_CUDA_ASSEMBLE
+    static_cast<RefEpf *>(h)->use_cuda = on != 0;
+    return 0;
+#else
+    (void)h;
+    (void)on;
+    return -1;
+#endif
+}
+
+// 1 when this library is the drop-in build (the reference's callers linked to libperix_b200.so)
+int ref_is_dropin(void) {
+#ifdef PERIX_CUDA_ASSEMBLE
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+// The reference's explicit loop to an end time (TimeStepping.cpp:479-599, restated): the start of ref_epf_run, then
+// while t < t_end - 1e-12 t_end: dt_attempt = min(dt, t_end - t), the uniform step when dt_attempt equals the
+// previous step's dt, else the variable-step form u + (dt/dt_prev)(u - u_prev) + dt (dt + dt_prev)/2 a; the BC
+// preset at the new time; the blow-up guard (50-step window: non-finite U, or max|U| above 1e3 max(1, max|U| 50
+// steps before).  Returns the number of steps completed; *blowup_step receives the 1-based step at which the guard
+// tripped (0 if it did not), and u/uold/health are the state after the last completed step.
+int ref_epf_run_to(void *h, const double *u0, const double *v0, double dt, double t_end, int nbc, const int *kind,
+                   const int *comp_mask, const int *direct, const double *val, const double *vel, const int *has_box,
+                   const double *box, const int *node_off, const int *nodes, double *u_out, double *uold_out,
+                   double *health_out, int *blowup_step, double *t_out, int nthreads) {
+    auto *e = static_cast<RefEpf *>(h);
+    auto *m = e->mesh;
+    const int n = m->pd.getNodesNum() * m->dim;
+    std::vector<double> U(u0, u0 + n), Uo(n), A(n);
+    ref_epf_rate(h, U.data(), A.data(), nullptr, nthreads);
+    for (int k = 0; k < n; ++k) Uo[k] = U[k] - dt * (v0 ? v0[k] : 0.0) + 0.5 * dt * dt * A[k];
+    constexpr int kWindow = 50;
+    double hist[kWindow] = {0.0};
+    double t = 0.0, dt_prev = dt;
+    const double t_eps = 1.0e-12 * t_end;
+    int step = 0, tripped = 0;
+    while (t < t_end - t_eps) {
+        step++;
+        const double dtA = std::min(dt, t_end - t);
+        const double tNew = t + dtA;
+        const double dt2 = dtA * dtA;
+        std::vector<double> Un = U, Uon = Uo;
+        ref_epf_rate(h, Un.data(), A.data(), nullptr, nthreads);
+        if (dtA == dt_prev) {
+            for (int k = 0; k < n; ++k) {
+                const double un = 2.0 * Un[k] - Uon[k] + dt2 * A[k];
+                Uon[k] = Un[k];
+                Un[k] = un;
+            }
+        } else {
+            const double rho = dtA / dt_prev;
+            const double w = 0.5 * dtA * (dtA + dt_prev);
+            for (int k = 0; k < n; ++k) {
+                const double un = Un[k] + rho * (Un[k] - Uon[k]) + w * A[k];
+                Uon[k] = Un[k];
+                Un[k] = un;
+            }
+        }
+        ref_bc_preset(m, nbc, kind, comp_mask, direct, val, vel, has_box, box, node_off, nodes, tNew, Un.data());
+        const int slot = (step - 1) % kWindow;
+        const double past = step > kWindow ? hist[slot] : -1.0;
+        const double cap = past >= 0.0 ? 1.0e3 * std::max(1.0, past) : std::numeric_limits<double>::infinity();
+        double umax = 0.0;
+        bool finite = true;
+        for (int k = 0; k < n; ++k) {
+            const double av = std::fabs(Un[k]);
+            if (!(av <= std::numeric_limits<double>::max())) finite = false;
+            else if (av > umax) umax = av;
+        }
+        if (!finite || umax > cap) {
+            tripped = step;
+            step--;
+            break;
+        }
+        hist[slot] = umax;
+        U.swap(Un);
+        Uo.swap(Uon);
+        t = tNew;
+        dt_prev = dtA;
+    }
+    if (u_out) std::memcpy(u_out, U.data(), sizeof(double) * n);
+    if (uold_out) std::memcpy(uold_out, Uo.data(), sizeof(double) * n);
+    if (health_out) std::memcpy(health_out, e->el.m_HealthFlat.data(), sizeof(double) * e->el.m_HealthFlat.size());
+    if (blowup_step) *blowup_step = tripped;
+    if (t_out) *t_out = t;
+    return step;
 }
 
 int ref_max_threads(void) {

@@ -63,6 +63,13 @@ def _check(status):
         raise PxbError(status, lib().pxb_last_error().decode(errors="replace"))
 
 
+def _check_step(status, bad):
+    if status != 0:
+        e = PxbError(status, lib().pxb_last_error().decode(errors="replace"))
+        e.bad_step = bad.value
+        raise e
+
+
 def _f64(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
 
@@ -421,8 +428,26 @@ class Context:
         _check(self.L.pxb_epf_start(self.h, _p(_f64(u0)), _p(_f64(v0)), C.c_double(dt)))
 
     def epf_advance(self, nsteps, chunk=0):
+        """nsteps uniform steps; a tripped blow-up guard raises PxbError (status 5) with .bad_step set."""
         bad = C.c_int(0)
-        _check(self.L.pxb_epf_advance(self.h, int(nsteps), int(chunk), C.byref(bad)))
+        _check_step(self.L.pxb_epf_advance(self.h, int(nsteps), int(chunk), C.byref(bad)), bad)
+
+    def epf_advance_to(self, t_end, chunk=0):
+        """Advance to t_end with the reference's clamped variable-dt last step; returns the number of steps."""
+        bad = C.c_int(0)
+        steps = C.c_longlong(0)
+        _check_step(self.L.pxb_epf_advance_to(self.h, C.c_double(t_end), int(chunk), C.byref(bad), C.byref(steps)),
+                    bad)
+        return steps.value
+
+    def set_memory_limit(self, nbytes):
+        """Cap the device bytes this context may hold (0: none); allocations past it raise PxbError (status 4)."""
+        _check(self.L.pxb_ctx_set_memory_limit(self.h, C.c_size_t(int(nbytes))))
+
+    def epf_set_wait_budget(self, tries):
+        """Fault-path test hook (include/perix_b200_measure.h): try_wait calls a staged consumer wait may make; -1
+        restores the default."""
+        _check(self.L.pxb_epf_set_wait_budget(self.h, int(tries)))
 
     def epf_state(self):
         u = np.zeros(self.n * self.dim, np.float64)

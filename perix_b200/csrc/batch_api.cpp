@@ -12,6 +12,7 @@
 
 #include "k_kernels.h"
 #include "pxb_context.h"
+#include "tune_internal.h"
 #include "fam_builder.h"
 
 using namespace pxb;
@@ -377,8 +378,7 @@ extern "C" int pxb_batch_get_variant(pxb_ctx *c, int which, int *variant) {
 
 // Times `reps` launches of the current schedule of the g-build (what 0) or the apply (what 1, on the field
 // u_d into out_d, device pointers), the L2 flushed before each; ms[r] per launch group.
-extern "C" int pxb_batch_time(pxb_ctx *c, int what, int reps, size_t flush_bytes, const double *u_d, double *out_d,
-                              float *ms) {
+int pxb::batch_time(pxb_ctx *c, int what, int reps, size_t flush_bytes, const double *u_d, double *out_d, float *ms) {
     PXB_TRY(need_batch(c, "pxb_batch_time", what == 1));
     if (reps <= 0 || !ms || (what == 1 && (!u_d || !out_d)) || (what != 0 && what != 1))
         return fail(PXB_ERR_INVALID, "pxb_batch_time: bad arguments");
@@ -415,8 +415,8 @@ extern "C" int pxb_batch_autotune(pxb_ctx *c, int what, int reps, size_t flush_b
     for (int v = 0; v < kBatchVariants; ++v) {
         slot = v;
         // one untimed launch first: a kernel's first launch in a process also loads its module
-        PXB_TRY(pxb_batch_time(c, what, 1, 0, u_d, out_d, ms.data()));
-        PXB_TRY(pxb_batch_time(c, what, reps, flush_bytes, u_d, out_d, ms.data()));
+        PXB_TRY(batch_time(c, what, 1, 0, u_d, out_d, ms.data()));
+        PXB_TRY(batch_time(c, what, reps, flush_bytes, u_d, out_d, ms.data()));
         float mean = 0.f;
         for (float x : ms) mean += x;
         mean /= (float)reps;

@@ -9,6 +9,7 @@
 
 #include "k_kernels.h"
 #include "pxb_context.h"
+#include "tune_internal.h"
 #include "fam_builder.h"
 
 namespace pxb {
@@ -58,12 +59,25 @@ int ensure_pinned(PinnedBuf &b, size_t bytes) {
     return PXB_OK;
 }
 
+// a failed cudaMalloc is PXB_ERR_OOM (its sticky-free error is cleared so the context stays usable)
+static int malloc_dev(void **p, size_t bytes) {
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) return PXB_OK;
+    *p = nullptr;
+    cudaGetLastError();
+    if (e == cudaErrorMemoryAllocation)
+        return fail(PXB_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed (out of memory)");
+    return cuda_fail(e, "cudaMalloc");
+}
+
 int dev_alloc(pxb_ctx *c, DevBuf &b, size_t bytes) {
-    (void)c;
     if (b.p && b.bytes == bytes) return PXB_OK;
+    if (c && c->mem_limit && bytes > b.bytes && ctx_bytes(c) - b.bytes + bytes > c->mem_limit)
+        return fail(PXB_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes would exceed the context's " +
+                                     std::to_string(c->mem_limit) + "-byte limit (pxb_ctx_set_memory_limit)");
     b.release();
     if (bytes == 0) return PXB_OK;
-    PXB_CUDA_TRY(cudaMalloc(&b.p, bytes));
+    PXB_TRY(malloc_dev(&b.p, bytes));
     b.bytes = bytes;
     return PXB_OK;
 }
@@ -97,6 +111,14 @@ int check_launch(pxb_ctx *c, const char *what) {
     return PXB_OK;
 }
 
+// A staged kernel's consumer wait ran out in `werr` blocks: clear the context's error word (so the next call starts
+// clean) and report the failure.
+int wait_failure(pxb_ctx *c, unsigned int werr, const char *what) {
+    cudaMemsetAsync(c->epf.counters.as<unsigned long long>() + 2, 0, sizeof(unsigned int), c->stream);
+    cudaStreamSynchronize(c->stream);
+    return fail(PXB_ERR_CUDA, std::string(what) + ": a staged-copy wait ran out (" + std::to_string(werr) + " blocks)");
+}
+
 static size_t bufsz(const DevBuf &b) { return b.bytes; }
 
 size_t ctx_bytes(const pxb_ctx *c) {
@@ -121,11 +143,7 @@ size_t ctx_bytes(const pxb_ctx *c) {
 
 // scratch device memory for staging (grown on demand, never shrunk)
 static int scratch(pxb_ctx *c, size_t bytes, void **p) {
-    if (c->scratch.bytes < bytes) {
-        c->scratch.release();
-        PXB_CUDA_TRY(cudaMalloc(&c->scratch.p, bytes));
-        c->scratch.bytes = bytes;
-    }
+    if (c->scratch.bytes < bytes) PXB_TRY(dev_alloc(c, c->scratch, bytes));
     *p = c->scratch.p;
     return PXB_OK;
 }
@@ -453,7 +471,6 @@ extern "C" int pxb_gbuild(pxb_ctx *c, int order, int precision, int *n_degenerat
 }
 
 namespace pxb {
-// relaunch the g-build into the existing operator cache (same order/precision), no host synchronisation
 int gbuild_launch_only(pxb_ctx *c, int order, int precision) {
     if (!c->ops.ready || c->ops.order != order || c->ops.precision != precision)
         return fail(PXB_ERR_STATE, "g-build timing needs a prior pxb_gbuild with the same order and precision");
@@ -625,6 +642,7 @@ static EpfArgs epf_args(pxb_ctx *c) {
     a.xib = e.xib.p ? e.xib.as<float>() : nullptr;
     if (epf_is_tma(e.variant)) a.maxb = epf_tma_maxb(g.dim, e.variant, g.max_family);
     a.evict_first = e.evict_first ? 1 : 0;
+    if (e.wait_tries >= 0) a.wait_tries = e.wait_tries;
     return a;
 }
 
@@ -768,7 +786,7 @@ extern "C" int pxb_epf_rate(pxb_ctx *c, const double *u, double *accel, long lon
     unsigned long long *h = static_cast<unsigned long long *>(e.rate_h.p);
     PXB_TRY(sync_polled(c, e.rate_done));
     const unsigned int werr = static_cast<unsigned int>(h[2] & 0xffffffffULL);
-    if (werr) return fail(PXB_ERR_CUDA, "explicit rate: a staged-copy wait ran out (" + std::to_string(werr) + " blocks)");
+    if (werr) return wait_failure(c, werr, "explicit rate");
     if (n_broken) *n_broken = (long long)(h[0] - h[4]);
     return PXB_OK;
 }
@@ -882,10 +900,14 @@ extern "C" int pxb_epf_set_bcs(pxb_ctx *c, int nbc, const int *kind, const int *
             const int mb = mir.empty() ? 0 : mir[(size_t)i];
             if (kind[b] == 0) {
                 if (has_box && has_box[b]) {
+                    // DirichletBC::insideBox (DirichletBC.cpp:89-98): every axis of the xyz coordinates (z = 0 in
+                    // 2D), an axis whose min exceeds its max leaves that axis unconstrained
                     bool inside = true;
-                    for (int a = 0; a < dim; ++a) {
-                        const double x = X(i, a);
-                        if (x < box[6 * b + 2 * a] || x > box[6 * b + 2 * a + 1]) inside = false;
+                    for (int a = 0; a < 3; ++a) {
+                        const double lo = box[6 * b + 2 * a], hi = box[6 * b + 2 * a + 1];
+                        if (lo > hi) continue;
+                        const double x = a < dim ? X(i, a) : 0.0;
+                        if (x < lo || x > hi) inside = false;
                     }
                     if (!inside) continue;
                 }
@@ -904,7 +926,11 @@ extern "C" int pxb_epf_set_bcs(pxb_ctx *c, int nbc, const int *kind, const int *
                     sym[(size_t)i * dim + a] = s;
                 }
             } else {
-                if (mb < 1) continue;
+                // NeumannBC::presetSolution (NeumannBC.cpp:88-105) copies from the mirror bulk and aborts the run
+                // for a node without one (checkedMirror); here that is an error
+                if (mb < 1)
+                    return fail(PXB_ERR_INVALID, "pxb_epf_set_bcs: Neumann entry " + std::to_string(b) + " names node " +
+                                                     std::to_string(id) + ", which has no mirror bulk node");
                 for (int a = 0; a < dim; ++a)
                     if ((comp_mask[b] >> a) & 1) sym[(size_t)i * dim + a] = cur(mb - 1, a);
             }
@@ -1005,6 +1031,7 @@ extern "C" int pxb_epf_start(pxb_ctx *c, const double *u0, const double *v0, dou
     e.dt = dt;
     e.t = 0.0;
     e.step = 0;
+    e.dt_prev = dt;
     e.umax_hist.clear();
     e.started = true;
     return PXB_OK;
@@ -1023,6 +1050,16 @@ int step_args(pxb_ctx *c, int par, EpfArgs *out) {
     a.t_sched = e.tsched.as<double>();
     a.step_in_chunk = 0;
     a.umax = e.umax.as<unsigned long long>();
+    *out = a;
+    return PXB_OK;
+}
+
+// argument block of one RATE launch of the per-step rate call: reads u[cur], writes the acceleration
+int rate_args(pxb_ctx *c, EpfArgs *out) {
+    EpfState &e = c->epf;
+    EpfArgs a = epf_args(c);
+    a.u = e.u[e.cur].as<double>();
+    a.accel = e.accel.as<double>();
     *out = a;
     return PXB_OK;
 }
@@ -1117,14 +1154,106 @@ extern "C" int pxb_epf_advance(pxb_ctx *c, int nsteps, int chunk, int *bad_step)
         unsigned int werr = 0;
         PXB_TRY(d2h(c, &werr, e.counters.as<unsigned long long>() + 2, sizeof(unsigned int)));
         PXB_TRY(sync(c));
-        if (werr) return fail(PXB_ERR_CUDA, "explicit step: a staged-copy wait ran out (" + std::to_string(werr) + " blocks)");
+        if (werr) return wait_failure(c, werr, "explicit step");
         const int st = check_blowup(e, keys.data(), s, bad_step);
         e.cur ^= (s & 1);
         e.t = t;
         e.step += s;
+        e.dt_prev = e.dt;
         done += s;
         if (st != PXB_OK) return st;
     }
+    return PXB_OK;
+}
+
+// One step of length dtA launched alone, with the BC pass at t + dtA and the blow-up guard: the uniform form with
+// dt^2 = dtA^2 when dtA equals the previous step's dt, else the variable-step central difference
+// (TimeStepping.cpp:529-545).
+static int single_step(pxb_ctx *c, double dtA, int *bad_step) {
+    EpfState &e = c->epf;
+    if (e.graph_chunk < 1) {
+        PXB_TRY(dev_alloc(c, e.umax, sizeof(unsigned long long)));
+        PXB_TRY(dev_alloc(c, e.tsched, sizeof(double)));
+        PXB_TRY(ensure_pinned(e.tsched_h, 64));
+        e.graph_chunk = 1;
+    }
+    const double t_new = e.t + dtA;
+    double *th = static_cast<double *>(e.tsched_h.p);
+    PXB_TRY(sync(c));
+    th[0] = t_new;
+    PXB_TRY(h2d(c, e.tsched.p, th, sizeof(double)));
+    PXB_CUDA_TRY(cudaMemsetAsync(e.umax.p, 0, sizeof(unsigned long long), c->stream));
+    EpfArgs a;
+    PXB_TRY(step_args(c, e.cur, &a));
+    a.step_in_chunk = 0;
+    a.dt2 = dtA * dtA;
+    a.var_step = dtA == e.dt_prev ? 0 : 1;
+    a.cv_rho = dtA / e.dt_prev;
+    a.cv_w = 0.5 * dtA * (dtA + e.dt_prev);
+    const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_STEP, e.variant, c->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "epf variable step launch");
+    c->launches++;
+    unsigned long long key = 0;
+    unsigned int werr = 0;
+    PXB_TRY(d2h(c, &key, e.umax.p, sizeof(key)));
+    PXB_TRY(d2h(c, &werr, e.counters.as<unsigned long long>() + 2, sizeof(unsigned int)));
+    PXB_TRY(sync(c));
+    if (werr) return wait_failure(c, werr, "explicit step");
+    const int st = check_blowup(e, &key, 1, bad_step);
+    e.cur ^= 1;
+    e.t = t_new;
+    e.step += 1;
+    e.dt_prev = dtA;
+    return st;
+}
+
+extern "C" int pxb_epf_advance_to(pxb_ctx *c, double t_end, int chunk, int *bad_step, long long *steps_taken) {
+    PXB_TRY(need_epf(c, "pxb_epf_advance_to"));
+    EpfState &e = c->epf;
+    if (!e.started) return fail(PXB_ERR_STATE, "pxb_epf_advance_to: call pxb_epf_start first");
+    if (!(t_end > 0.0)) return fail(PXB_ERR_INVALID, "pxb_epf_advance_to: t_end must be > 0");
+    if (bad_step) *bad_step = 0;
+    const long long step0 = e.step;
+    // the reference's loop (TimeStepping.cpp:495-599): while t < T - 1e-12 T, dt_attempt = min(dt, T - t); a step
+    // whose dt_attempt equals the previous step's dt is uniform, any other takes the variable-step form
+    const double t_eps = 1.0e-12 * t_end;
+    int st = PXB_OK;
+    while (st == PXB_OK && e.t < t_end - t_eps) {
+        const double dtA = std::min(e.dt, t_end - e.t);
+        if (dtA == e.dt && e.dt_prev == e.dt) {
+            // the run of uniform steps up to the clamp, t accumulated exactly like the reference loop
+            long long k = 0;
+            double t = e.t;
+            while (t < t_end - t_eps && std::min(e.dt, t_end - t) == e.dt) {
+                t = t + e.dt;
+                ++k;
+            }
+            while (st == PXB_OK && k > 0) {
+                const int s = (int)std::min<long long>(k, 1 << 30);
+                st = pxb_epf_advance(c, s, chunk, bad_step);
+                k -= s;
+            }
+        } else {
+            st = single_step(c, dtA, bad_step);
+        }
+    }
+    if (steps_taken) *steps_taken = e.step - step0;
+    return st;
+}
+
+extern "C" int pxb_ctx_set_memory_limit(pxb_ctx *c, size_t bytes) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_ctx_set_memory_limit: NULL context");
+    c->mem_limit = bytes;
+    return PXB_OK;
+}
+
+extern "C" int pxb_epf_set_wait_budget(pxb_ctx *c, int tries) {
+    PXB_TRY(need_epf(c, "pxb_epf_set_wait_budget"));
+    EpfState &e = c->epf;
+    e.wait_tries = tries < 0 ? -1 : tries;
+    destroy_graphs(e);  // captured steps carry the old budget
+    if (e.rate_graph) cudaGraphExecDestroy(e.rate_graph);
+    e.rate_graph = nullptr;
     return PXB_OK;
 }
 

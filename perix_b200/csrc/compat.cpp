@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "../../include/perix_b200.h"
@@ -25,6 +27,13 @@ ShimState g_shim;
 bool report(const char *who) {
     std::fprintf(stderr, "[perix_b200] %s: %s\n", who, pxb_last_error());
     return false;
+}
+
+// Precision of the explicit element's device operators: FP64 unless PERIX_B200_PRECISION=mixed (FP32-stored Navier
+// coefficients with FP64 arithmetic, state and stretch decisions; within 1e-6 of FP64).
+int explicit_precision() {
+    const char *v = std::getenv("PERIX_B200_PRECISION");
+    return (v && (std::strcmp(v, "mixed") == 0 || std::strcmp(v, "MIXED") == 0)) ? PXB_MIXED : PXB_FP64;
 }
 
 bool ensure_ctx() {
@@ -232,8 +241,12 @@ bool assembleExplicitPDDOFracAccel(const AssembleMesh &m, const ExplicitPDDOFrac
         for (int t = 0; t < nbtot; ++t) h0[(size_t)t] = health_inout[t] > 0.0 ? 1 : 0;
         const double b[3] = {p.bx, p.by, p.bz};
         const double sc = p.damage_on ? p.sc : 0.0;
-        if (pxb_epf_setup(g_shim.ctx, PXB_FP64, p.C11, p.C12, p.C66, p.rho, b, sc, p.tension_only, h0.data()) != PXB_OK)
+        const int prec = explicit_precision();
+        if (pxb_epf_setup(g_shim.ctx, prec, p.C11, p.C12, p.C66, p.rho, b, sc, p.tension_only, h0.data()) != PXB_OK)
             return report("epf setup");
+        // the per-step call's schedule, timed once per problem signature at this displacement (state unchanged)
+        if (pxb_epf_autotune_rate(g_shim.ctx, u, 3, 1, nullptr, nullptr) != PXB_OK) return report("epf autotune");
+        g_shim.precision = prec;
         g_shim.kind = 2;
         g_shim.n = m.N;
         g_shim.nbtot = nbtot;
@@ -251,3 +264,38 @@ bool assembleExplicitPDDOFracAccel(const AssembleMesh &m, const ExplicitPDDOFrac
 }
 
 }  // namespace perix_cuda
+
+// C entry over the explicit drop-in call, for callers that bind C rather than C++ (ctypes, other FFIs): the
+// arguments are the members of AssembleMesh / ExplicitPDDOFracParams the call reads, and the behaviour is
+// perix_cuda::assembleExplicitPDDOFracAccel's (1 on success, 0 where that returns false).
+extern "C" int pxb_cuda_explicit_accel(int n, int dim, const int *neigh_off, const int *neigh_id, const double *coords,
+                                       const double *vols, double delta, double dx_char, double C11, double C12,
+                                       double C66, double rho, const double *body, double sc, int tension_only,
+                                       int damage_on, const double *u, double *health_inout, double *accel_out,
+                                       int *health_changed) {
+    perix_cuda::AssembleMesh m;
+    m.N = n;
+    m.dim = dim;
+    m.neigh_off = neigh_off;
+    m.neigh_id = neigh_id;
+    m.coords = coords;
+    m.vols = vols;
+    m.delta = delta;
+    m.dx_char = dx_char;
+    perix_cuda::ExplicitPDDOFracParams p;
+    p.dim = dim;
+    p.C11 = C11;
+    p.C12 = C12;
+    p.C66 = C66;
+    p.rho = rho;
+    p.bx = body ? body[0] : 0.0;
+    p.by = body ? body[1] : 0.0;
+    p.bz = body && dim == 3 ? body[2] : 0.0;
+    p.sc = sc;
+    p.tension_only = tension_only;
+    p.damage_on = damage_on;
+    perix_cuda::OpSlots s;
+    return perix_cuda::assembleExplicitPDDOFracAccel(m, p, s, u, health_inout, accel_out, health_changed) ? 1 : 0;
+}
+
+extern "C" void pxb_cuda_shutdown(void) { perix_cuda::shutdown(); }

@@ -214,11 +214,11 @@ __global__ void __launch_bounds__(kEpfThreads) epf_kernel(EpfArgs a) {
                 a.u_other[k] = __dadd_rn(__dsub_rn(pick<DIM>(ui, d), __dmul_rn(a.dt, v)), __dmul_rn(a.dt2, acc));
             } else {
                 const double uprev = a.u_other[k];
-                unew = __dadd_rn(__dsub_rn(__dmul_rn(2.0, pick<DIM>(ui, d)), uprev), __dmul_rn(a.dt2, acc));
+                unew = cd_next(pick<DIM>(ui, d), uprev, acc, a.dt2, a.var_step, a.cv_rho, a.cv_w);
                 const bool owned = a.bc_own && ((a.bc_own[i] >> d) & 1);
                 if (!owned) {
                     a.u_other[k] = unew;
-                    umax = fmax(umax, fabs(unew));
+                    umax = max_nan(umax, fabs(unew));
                 }
             }
         }
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kEpfThreads) epf_kernel(EpfArgs a) {
                         v = __dsub_rn(__dmul_rn(2.0, g1), g2);
                     }
                     a.u_other[(size_t)a.bc_tgt[e] * DIM + comp] = v;
-                    umax = fmax(umax, fabs(v));
+                    umax = max_nan(umax, fabs(v));
                 }
             }
         }
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kEpfThreads) epf_kernel(EpfArgs a) {
 
     // block reductions, one atomic per block
     if constexpr (MODE == EPF_STEP) {
-        umax = group_max<kWarp>(umax);
+        umax = group_max_nan<kWarp>(umax);
         if (lane == 0) s_umax[wib] = dbl_key(umax);
     }
     unsigned long long bsum = broken;
@@ -413,12 +413,12 @@ __global__ void __launch_bounds__(kEpfThreads) epf_stream_kernel(EpfArgs a) {
                 a.u_other[idx] = __dadd_rn(__dsub_rn(s_u[k][d], __dmul_rn(a.dt, v)), __dmul_rn(a.dt2, acc));
             } else {
                 const double uprev = a.u_other[idx];
-                const double unew = __dadd_rn(__dsub_rn(__dmul_rn(2.0, s_u[k][d]), uprev), __dmul_rn(a.dt2, acc));
+                const double unew = cd_next(s_u[k][d], uprev, acc, a.dt2, a.var_step, a.cv_rho, a.cv_w);
                 s_un[k][d] = unew;
                 const bool owned = a.bc_own && ((a.bc_own[i] >> d) & 1);
                 if (!owned) {
                     a.u_other[idx] = unew;
-                    umax = fmax(umax, fabs(unew));
+                    umax = max_nan(umax, fabs(unew));
                 }
             }
         }
@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(kEpfThreads) epf_stream_kernel(EpfArgs a) {
                         else if (form == 2) v = __dsub_rn(__dmul_rn(2.0, g1), s_un[tid][comp]);
                         else v = __dsub_rn(__dmul_rn(2.0, g1), __dadd_rn(a.bc_val2[e], __dmul_rn(a.bc_vel2[e], t_new)));
                         a.u_other[(size_t)a.bc_tgt[e] * DIM + comp] = v;
-                        umax = fmax(umax, fabs(v));
+                        umax = max_nan(umax, fabs(v));
                     }
                 }
             }
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(kEpfThreads) epf_stream_kernel(EpfArgs a) {
     }
 
     if constexpr (MODE == EPF_STEP) {
-        umax = group_max<kWarp>(umax);
+        umax = group_max_nan<kWarp>(umax);
         if (lane == 0) s_umax[wib] = dbl_key(umax);
     }
     unsigned long long bsum = broken;

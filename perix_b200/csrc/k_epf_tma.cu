@@ -56,9 +56,10 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
 
 // bounded wait: false if the phase did not complete within the iteration budget.  Each try_wait may suspend
 // the thread for up to kSuspendNs (it resumes as soon as the phase completes), so a waiting warp issues few
-// instructions; the budget is at most 2^19 tries (about half a second).
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
-    for (int it = 0; it < (1 << 19); ++it)
+// instructions; the default budget is 2^19 tries (about half a second).
+constexpr int kWaitTries = 1 << 19;
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int tries = kWaitTries) {
+    for (int it = 0; it < tries; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -301,7 +302,9 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     for (int k = 0; k < mycount; ++k) {
         const int st = k % S;
         if (*(volatile int *)&s_fail) break;
-        const bool ok_wait = __all_sync(kFull, mbar_wait(&bar[st], (unsigned)((k / S) & 1)));
+        // the consumers' wait (its budget: EpfArgs::wait_tries, the default unless a test shortens it); the drain
+        // of the copies in flight after a failure below always keeps the default budget
+        const bool ok_wait = __all_sync(kFull, mbar_wait(&bar[st], (unsigned)((k / S) & 1), a.wait_tries));
         if (!ok_wait) {
             if (lane == 0) atomicExch(&s_fail, 1);
             break;
@@ -456,12 +459,11 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
             if (rate) {
                 a.accel[kk] = acc;
             } else {
-                unew = __dadd_rn(__dsub_rn(__dmul_rn(2.0, pick_t<DIM>(ui, d)), sUp[li * DIM + d]),
-                                 __dmul_rn(a.dt2, acc));
+                unew = cd_next(pick_t<DIM>(ui, d), sUp[li * DIM + d], acc, a.dt2, a.var_step, a.cv_rho, a.cv_w);
                 const bool owned = a.bc_own && ((a.bc_own[i] >> d) & 1);
                 if (!owned) {
                     a.u_other[kk] = unew;
-                    umax = fmax(umax, fabs(unew));
+                    umax = max_nan(umax, fabs(unew));
                 }
             }
         }
@@ -480,7 +482,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
                 else if (form == 2) v = __dsub_rn(__dmul_rn(2.0, g1), pick_t<DIM>(un, comp));
                 else v = __dsub_rn(__dmul_rn(2.0, g1), __dadd_rn(a.bc_val2[e], __dmul_rn(a.bc_vel2[e], t_new)));
                 a.u_other[(size_t)a.bc_tgt[e] * DIM + comp] = v;
-                umax = fmax(umax, fabs(v));
+                umax = max_nan(umax, fabs(v));
             }
         }
         // stage st consumed by this warp; the warp that completes the count refills it with tile k+S
@@ -502,7 +504,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         if (a.err) atomicAdd(a.err, 1u);
     }
 
-    umax = group_max<kWarp>(umax);
+    umax = group_max_nan<kWarp>(umax);
     if (lane == 0) s_umax[wib] = dbl_key(umax);
     unsigned long long bsum = broken;
 #pragma unroll

@@ -152,6 +152,10 @@ struct EpfArgs {
     // steps the next step's blocks start their set-up while this step's last blocks finish (host-side only)
     int pdl = 0;
     int evict_first = 0;  // TMA variants: stage the bond streams with an L2 evict-first policy
+    // STEP: a step whose dt differs from the previous one takes the variable-step form (see cd_next)
+    int var_step = 0;
+    double cv_rho = 0, cv_w = 0;
+    int wait_tries = 1 << 19;  // TMA variants: try_wait calls a consumer wait may make before it gives up
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
 constexpr int kEpfTmaConfigs = 13;                // staged (TMA) configurations per dimension

@@ -106,6 +106,25 @@ __device__ __forceinline__ double group_max(double v) {
     return v;
 }
 
+// NaN-propagating maximum of non-negative values (fmax would drop a NaN): the blow-up guard must see a non-finite
+// displacement
+__device__ __forceinline__ double max_nan(double a, double b) { return (b > a || b != b) ? b : a; }
+
+template <int LANES>
+__device__ __forceinline__ double group_max_nan(double v) {
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) v = max_nan(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+
+// u^{n+1} of the central difference in the reference's rounding (TimeStepping.cpp:529-545): the uniform step
+// 2u - u_prev + dt^2 a, or, for a step whose dt differs from the previous step's (var != 0), the variable-step form
+// u + rho (u - u_prev) + w a with rho = dt/dt_prev and w = dt (dt + dt_prev)/2
+__device__ __forceinline__ double cd_next(double u, double up, double acc, double dt2, int var, double rho, double w) {
+    if (var) return __dadd_rn(__dadd_rn(u, __dmul_rn(rho, __dsub_rn(u, up))), __dmul_rn(w, acc));
+    return __dadd_rn(__dsub_rn(__dmul_rn(2.0, u), up), __dmul_rn(dt2, acc));
+}
+
 // ---- compensated FP32 accumulation (Knuth two-sum) ---------------------------------------------------------
 struct CompF {
     float s, c;

@@ -135,6 +135,7 @@ struct EpfState {
     PinnedBuf tsched_h;
     int cur = 0;
     double t = 0.0, dt = 0.0;
+    double dt_prev = 0.0;  // dt of the last step taken (differs from dt after a clamped final step)
     long long step = 0;
     std::vector<double> umax_hist;  // host history for the windowed blow-up guard
     BcDevice bc;
@@ -143,6 +144,7 @@ struct EpfState {
     int graph_chunk = 0;
     int variant = 1;   // schedule variant of the explicit kernel (set by the autotuner or pxb_epf_set_variant)
     bool evict_first = false;  // the step's bond streams exceed the L2: stage them with an evict-first policy
+    int wait_tries = -1;       // staged kernels' consumer waits: try_wait calls allowed (-1: the default bound)
 };
 
 struct CsrState {
@@ -195,6 +197,7 @@ struct BatchState {
 
 struct pxb_ctx {
     int device = 0;
+    size_t mem_limit = 0;  // device bytes the context may hold (0: no limit beyond the GPU's)
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
     long long launches = 0;
@@ -219,4 +222,5 @@ int sync(pxb_ctx *c);
 int check_launch(pxb_ctx *c, const char *what);
 size_t ctx_bytes(const pxb_ctx *c);
 int l2_flush(pxb_ctx *c, size_t bytes);  // writes `bytes` through the L2 on the context stream (0: nothing)
+int wait_failure(pxb_ctx *c, unsigned int werr, const char *what);  // report (and clear) a staged wait that ran out
 }  // namespace pxb

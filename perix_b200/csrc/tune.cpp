@@ -1,6 +1,6 @@
-// Measurement support in the C-ABI: device-side state snapshots and CUDA-event timing of individual kernel
-// launches on the context stream (so a caller can time exactly the step kernel, with the L2 flushed before
-// each launch, without host work inside the measured interval).
+// Schedule autotuners of the explicit kernel (the time step of the device loop and the per-step rate call of the
+// reference boundary) and the device-side explicit-state snapshot they run from.  Each candidate schedule is timed
+// with CUDA events around its kernel launches on the context stream; the choice is cached per problem signature.
 #include <algorithm>
 #include <map>
 #include <string>
@@ -8,10 +8,11 @@
 
 #include "k_kernels.h"
 #include "pxb_context.h"
+#include "tune_internal.h"
 
 namespace pxb {
 int step_args(pxb_ctx *c, int par, EpfArgs *out);
-int gbuild_launch_only(pxb_ctx *c, int order, int precision);
+int rate_args(pxb_ctx *c, EpfArgs *out);
 }  // namespace pxb
 
 using namespace pxb;
@@ -40,18 +41,6 @@ int d2d(pxb_ctx *c, void *dst, const void *src, size_t bytes) {
     PXB_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
     return PXB_OK;
 }
-
-struct Events {
-    std::vector<cudaEvent_t> ev;
-    ~Events() {
-        for (auto e : ev) cudaEventDestroy(e);
-    }
-    int make(size_t n) {
-        ev.resize(n, nullptr);
-        for (auto &e : ev) PXB_CUDA_TRY(cudaEventCreate(&e));
-        return PXB_OK;
-    }
-};
 
 int flush_l2(pxb_ctx *c, size_t bytes, DevBuf &buf) {
     if (bytes == 0) return PXB_OK;
@@ -128,7 +117,7 @@ int timed_steps(pxb_ctx *c, int nsteps, size_t flush_bytes, int restore_every, c
     PXB_TRY(sync(c));
     unsigned int werr = 0;
     PXB_CUDA_TRY(cudaMemcpy(&werr, e.counters.as<unsigned long long>() + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost));
-    if (werr) return fail(PXB_ERR_CUDA, "explicit step: a staged-copy wait ran out");
+    if (werr) return wait_failure(c, werr, "explicit step");
     for (int s = 0; s < nsteps; ++s) PXB_CUDA_TRY(cudaEventElapsedTime(&ms[s], ev.ev[2 * (size_t)s], ev.ev[2 * (size_t)s + 1]));
     return PXB_OK;
 }
@@ -144,6 +133,11 @@ std::string signature(const pxb_ctx *c) {
 }  // namespace
 
 namespace pxb {
+int epf_timed_steps(pxb_ctx *c, int nsteps, size_t flush_bytes, int restore_every, bool from_snapshot, float *ms) {
+    Snapshot &s = snap_of(c);
+    return timed_steps(c, nsteps, flush_bytes, restore_every, from_snapshot && s.valid ? &s : nullptr, ms);
+}
+
 // called when a context is destroyed: release its snapshot
 void drop_snapshot(pxb_ctx *c) {
     for (auto it = g_snaps.begin(); it != g_snaps.end(); ++it)
@@ -227,52 +221,81 @@ extern "C" int pxb_epf_autotune(pxb_ctx *c, int steps, size_t flush_bytes, int u
     return PXB_OK;
 }
 
-// Runs nsteps explicit steps one launch at a time; before each launch the L2 is flushed by writing
-// flush_bytes (0 = no flush) and, every restore_every steps (0 = never), the snapshot is restored.  ms[s]
-// receives the CUDA-event duration of step s's kernel alone.  The blow-up guard is not evaluated here.
-extern "C" int pxb_epf_time_steps(pxb_ctx *c, int nsteps, size_t flush_bytes, int restore_every, float *ms) {
-    if (!c || !c->epf.ready || !c->epf.started) return fail(PXB_ERR_STATE, "pxb_epf_time_steps: call pxb_epf_start first");
-    if (nsteps <= 0 || !ms) return fail(PXB_ERR_INVALID, "pxb_epf_time_steps: bad arguments");
-    Snapshot &s = snap_of(c);
-    return timed_steps(c, nsteps, flush_bytes, restore_every, s.valid ? &s : nullptr, ms);
-}
 
-// The fixed cost inside a timed step: an empty kernel with the launch shape of the last staged step launch
-// (grid, block, dynamic shared memory), timed exactly like a step (L2 flushed, CUDA events around the launch).
-extern "C" int pxb_epf_launch_floor(pxb_ctx *c, size_t flush_bytes, int reps, float *ms, int *grid, int *block,
-                                    size_t *smem) {
-    if (!c || reps <= 0 || !ms) return fail(PXB_ERR_INVALID, "pxb_epf_launch_floor: bad arguments");
-    const LaunchShape sh = epf_tma_last_shape();
-    if (sh.grid <= 0) return fail(PXB_ERR_STATE, "pxb_epf_launch_floor: no staged step launched yet");
+
+
+// Times the per-step rate call's kernel (RATE epilogue: damage, force, acceleration out) of every schedule variant
+// that fits, at the caller's displacement u (host, n*dim), reps launches each after one untimed launch; the bond
+// health and the counters are restored before every launch and at the end, so the state is as before the call.
+// Selects the fastest and caches it per problem signature (separately from the time-step choice).
+extern "C" int pxb_epf_autotune_rate(pxb_ctx *c, const double *u, int reps, int use_cache, int *best,
+                                     float *ms_per_variant) {
+    if (!c || !c->g.ready || !c->epf.ready) return fail(PXB_ERR_STATE, "pxb_epf_autotune_rate: call pxb_epf_setup first");
+    if (!u || reps <= 0) return fail(PXB_ERR_INVALID, "pxb_epf_autotune_rate: need u and reps > 0");
+    EpfState &e = c->epf;
+    const std::string key = signature(c) + ":rate";
+    auto hit = g_tuned.find(key);
+    if (use_cache && hit != g_tuned.end()) {
+        e.variant = hit->second;
+        if (best) *best = hit->second;
+        return PXB_OK;
+    }
+    DevBuf health, counters;
+    PXB_TRY(dev_alloc(c, health, e.health.bytes));
+    PXB_TRY(dev_alloc(c, counters, e.counters.bytes));
+    PXB_TRY(d2d(c, health.p, e.health.p, e.health.bytes));
+    PXB_TRY(d2d(c, counters.p, e.counters.p, e.counters.bytes));
+    PXB_TRY(h2d(c, e.u[e.cur].p, u, sizeof(double) * (size_t)c->g.n * c->g.dim));
+    auto restore = [&]() -> int {
+        PXB_TRY(d2d(c, e.health.p, health.p, health.bytes));
+        return d2d(c, e.counters.p, counters.p, counters.bytes);
+    };
     Events ev;
     PXB_TRY(ev.make(2 * (size_t)reps));
-    for (int r = 0; r < reps; ++r) {
-        PXB_TRY(flush_l2(c, flush_bytes, g_flush));
-        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r], c->stream));
-        PXB_CUDA_TRY(launch_empty(sh.grid, sh.block, sh.smem, c->stream));
-        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r + 1], c->stream));
+    const int keep = e.variant;
+    float best_ms = 1e30f;
+    int best_v = keep;
+    for (int v = 0; v < kEpfVariants; ++v) {
+        if (!epf_variant_fits(c->g.dim, v, c->g.max_family)) {
+            if (ms_per_variant) ms_per_variant[v] = -1.f;
+            continue;
+        }
+        e.variant = v;
+        EpfArgs a;
+        PXB_TRY(rate_args(c, &a));
+        // one untimed launch first: a kernel's first launch in a process also loads its module
+        for (int r = -1; r < reps; ++r) {
+            PXB_TRY(restore());
+            if (r >= 0) PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r], c->stream));
+            const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_RATE, v, c->stream);
+            if (err != cudaSuccess) return cuda_fail(err, "rate autotune launch");
+            c->launches++;
+            if (r >= 0) PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r + 1], c->stream));
+        }
+        PXB_TRY(sync(c));
+        unsigned int werr = 0;
+        PXB_CUDA_TRY(cudaMemcpy(&werr, e.counters.as<unsigned long long>() + 2, sizeof(unsigned int),
+                                cudaMemcpyDeviceToHost));
+        if (werr) {
+            e.variant = keep;
+            PXB_TRY(restore());
+            PXB_TRY(sync(c));
+            return fail(PXB_ERR_CUDA, "pxb_epf_autotune_rate: a staged-copy wait ran out");
+        }
+        float mean = 0.f;
+        for (int r = 0; r < reps; ++r) {
+            float ms = 0.f;
+            PXB_CUDA_TRY(cudaEventElapsedTime(&ms, ev.ev[2 * (size_t)r], ev.ev[2 * (size_t)r + 1]));
+            mean += ms;
+        }
+        mean /= (float)reps;
+        if (ms_per_variant) ms_per_variant[v] = mean;
+        if (mean < best_ms) { best_ms = mean; best_v = v; }
     }
+    PXB_TRY(restore());
     PXB_TRY(sync(c));
-    for (int r = 0; r < reps; ++r) PXB_CUDA_TRY(cudaEventElapsedTime(&ms[r], ev.ev[2 * (size_t)r], ev.ev[2 * (size_t)r + 1]));
-    if (grid) *grid = sh.grid;
-    if (block) *block = sh.block;
-    if (smem) *smem = sh.smem;
-    return PXB_OK;
-}
-
-// Times `reps` g-builds (order, precision) of the current geometry, L2 flushed before each; ms[r] per build.
-extern "C" int pxb_gbuild_time(pxb_ctx *c, int order, int precision, int reps, size_t flush_bytes, float *ms) {
-    if (!c || !c->g.ready) return fail(PXB_ERR_STATE, "pxb_gbuild_time: geometry not set");
-    if (reps <= 0 || !ms) return fail(PXB_ERR_INVALID, "pxb_gbuild_time: bad arguments");
-    Events ev;
-    PXB_TRY(ev.make(2 * (size_t)reps));
-    for (int r = 0; r < reps; ++r) {
-        PXB_TRY(flush_l2(c, flush_bytes, g_flush));
-        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r], c->stream));
-        PXB_TRY(gbuild_launch_only(c, order, precision));
-        PXB_CUDA_TRY(cudaEventRecord(ev.ev[2 * (size_t)r + 1], c->stream));
-    }
-    PXB_TRY(sync(c));
-    for (int r = 0; r < reps; ++r) PXB_CUDA_TRY(cudaEventElapsedTime(&ms[r], ev.ev[2 * (size_t)r], ev.ev[2 * (size_t)r + 1]));
+    e.variant = best_v;
+    g_tuned[key] = best_v;
+    if (best) *best = best_v;
     return PXB_OK;
 }

@@ -1,0 +1,69 @@
+"""The full batched-cloud workload (256 jittered 2D and 3D clouds, node counts log-uniform in [1e3, 2e5], 10.18 M
+nodes, the benchmark's seed) built and applied in one context, with families built on the device, then a seeded
+sample of 32 clouds - always including the largest 2D and the largest 3D cloud - checked against the C restatement
+(oracle) cloud by cloud: families bit-equal to the host build (itself bit-equal to the reference's
+createNeighborNodes), FP64 g-functions within 1e-12 (family-scaled), the all-derivative apply of the cubic field
+within 1e-12, and the mixed build's apply within 1e-6 of the FP64 oracle's."""
+import numpy as np
+import pytest
+
+from conftest import scaled_err
+
+pytestmark = pytest.mark.gpu
+
+NSAMPLE = 32
+
+
+@pytest.fixture(scope="module")
+def full_batch():
+    import perix_b200 as px
+    from bench import clouds_generate, cubic_field
+    clouds = clouds_generate(px, nclouds=256, families=False)
+    u, _ = cubic_field(clouds, seed=7)
+    sizes = np.array([c["coords3"].shape[0] for c in clouds])
+    dims = np.array([c["dim"] for c in clouds])
+    big2 = int(np.argmax(np.where(dims == 2, sizes, -1)))
+    big3 = int(np.argmax(np.where(dims == 3, sizes, -1)))
+    rng = np.random.default_rng(99)
+    rest = [k for k in rng.permutation(len(clouds)) if k not in (big2, big3)]
+    sample = sorted([big2, big3] + [int(k) for k in rest[:NSAMPLE - 2]])
+    return clouds, u, sample, big2, big3
+
+
+def _device(ctx, clouds, u, precision):
+    ctx.batch_set_points(clouds)
+    nd, _ = ctx.batch_gbuild(precision)
+    assert nd == 0
+    return ctx.batch_split(ctx.batch_apply(np.concatenate(u)))
+
+
+def test_full_batch_sample_matches_oracle(ctx, port, full_batch):
+    import perix_b200 as px
+    clouds, u, sample, big2, big3 = full_batch
+    assert sum(c["coords3"].shape[0] for c in clouds) == 10178520
+    got64 = _device(ctx, clouds, u, 0)
+    checked = {2: 0, 3: 0}
+    ref_apply = {}
+    for k in sample:
+        c = clouds[k]
+        off_d, ids_d = ctx.batch_get_families(k)
+        off_h, ids_h = px.families(c["coords3"], c["delta"], c["dim"] == 3)
+        assert np.array_equal(off_d, off_h) and np.array_equal(ids_d, ids_h)
+        g_ref, deg = port.gbuild(c["dim"], 2, c["coords3"], c["vols"], off_h, ids_h, c["delta"], c["dx_char"])
+        assert deg.sum() == 0
+        assert scaled_err(ctx.batch_get_ops(k), g_ref, off_h) <= 1e-12
+        d_ref = port.apply(off_h, ids_h, g_ref, u[k])
+        scale = np.abs(d_ref).max(axis=0)
+        assert (np.abs(got64[k] - d_ref).max(axis=0) <= 1e-12 * scale + 1e-300).all()
+        ref_apply[k] = d_ref
+        checked[c["dim"]] += 1
+    assert checked[2] >= 8 and checked[3] >= 8
+    assert big2 in ref_apply and big3 in ref_apply
+    # the mixed build of the same batch, against the FP64 oracle on the sample: every derivative within 1e-6 of the
+    # largest derivative of its order
+    got32 = _device(ctx, clouds, u, 1)
+    for k in sample:
+        d = clouds[k]["dim"]
+        diff = np.abs(got32[k] - ref_apply[k])
+        for sl in (slice(0, d), slice(d, None)):
+            assert diff[:, sl].max() <= 1e-6 * np.abs(ref_apply[k][:, sl]).max()

@@ -1,0 +1,90 @@
+"""The full 3D slab (120x120x24 bulk nodes + ghosts = 385,920 nodes, 44,189,344 directed bonds, central edge notch
+of depth 20h as a force-only crack plane) against the reference itself (oracle/_ref/libperix_ref.so: the
+reference's mesh generator, createNeighborNodes, ExplicitPDDOFracElement and its DirichletBC / NeumannBC objects,
+with the harness's central difference).
+
+* Families built on the device (pxb_set_geometry_points) equal the reference's createNeighborNodes at full size.
+* Eight explicit steps from a seeded random field (std 1 um against a 4 um critical extension of the shortest
+  bonds, so tens of thousands of bonds break) on several step schedules: FP64 with identical damage sets and u within
+  1e-10 of its magnitude; mixed within 1e-6 with damage sets identical but for bonds at the threshold."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import ref_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not ref_available(), reason="reference harness not built")]
+
+NSTEPS = 8
+
+
+@pytest.fixture(scope="module")
+def slab():
+    import perix_b200 as px
+    from oracle import RefEpf, RefMesh
+    nx, ny, nz, h = 120, 120, 24, 1e-3
+    Lx, Ly, Lz = nx * h, ny * h, nz * h
+    plane = [0.0, Ly / 2, -1.0, 20 * h, Ly / 2, -1.0, 20 * h, Ly / 2, 1.0, 0.0, Ly / 2, 1.0]
+    m = RefMesh.structured(3, nx, ny, nz, [0, Lx, 0, Ly, 0, Lz], 3.015, 2, planes=[plane], force_only=True)
+    E, nu, rho = 72e9, 0.22, 2440.0
+    G0 = 0.004 ** 2 * 6 * E * m.delta / 5
+    el = RefEpf(m, E, nu, rho, G0)
+    el.rate(np.zeros(3 * m.n))  # seeds the notch, derives s_c and the elastic constants
+    k = el.constants()
+    dt = 0.8 * h / math.sqrt(k["C11"] / rho)
+    bcs = [px.BC("neumann", [0, 1, 2], m.group(w + "nodes_ghost"))
+           for w in ("left", "right", "bottom", "top", "back", "front")]
+    alld = m.group("alldomain")
+    bcs.append(px.BC("dirichlet", [1], alld, value=[0, 0, 0], velocity=[0, 2.0, 0], direct=True,
+                     box=[-1, 1, Ly - 3 * h, 1, -1, 1]))
+    bcs.append(px.BC("dirichlet", [1], alld, value=[0, 0, 0], velocity=[0, -2.0, 0], direct=True,
+                     box=[-1, 1, -1, 3 * h, -1, 1]))
+    health0 = (1 - px.crack_cut_mask(m.coords, m.mirror, m.off, m.ids, planes=[plane])).astype(np.uint8)
+    rng = np.random.default_rng(2024)
+    u0 = rng.standard_normal(3 * m.n) * 1e-6
+    u, uo, hh, _ = el.run(u0, None, dt, NSTEPS, [b.as_dict() for b in bcs])
+    return dict(m=m, k=k, rho=rho, dt=dt, bcs=bcs, health0=health0, u0=u0, u=u, uo=uo, h=(hh > 0).astype(np.uint8))
+
+
+def test_slab_families_built_on_device_equal_reference(ctx, slab):
+    m = slab["m"]
+    assert m.n == 385920 and m.nb == 44189344
+    ctx.set_geometry_points(m.coords, m.vols, m.delta, m.delta, m.dx_char, 3, mirror=m.mirror)
+    off, ids = ctx.get_families()
+    assert np.array_equal(off, m.off)
+    assert np.array_equal(ids, m.ids)
+
+
+def _run(ctx, s, variant, precision):
+    import perix_b200 as px
+    m, k = s["m"], s["k"]
+    ctx.set_geometry(m.coords, m.vols, m.off, m.ids, m.delta, m.dx_char, 3, mirror=m.mirror)
+    ctx.epf_setup(k["C11"], k["C12"], k["C66"], s["rho"], (0.0, 0.0, 0.0), k["sc"], True, health0=s["health0"],
+                  precision=precision)
+    try:
+        ctx.epf_set_variant(variant)
+    except px.PxbError as e:
+        assert e.status == 7
+        pytest.skip("variant %d does not fit these families" % variant)
+    ctx.epf_set_bcs(s["bcs"])
+    ctx.epf_start(s["u0"], None, s["dt"])
+    ctx.epf_advance(NSTEPS, chunk=NSTEPS)
+    return ctx.epf_state()
+
+
+@pytest.mark.parametrize("variant", [1, 5, 7, 11, 12, 17])
+def test_slab_fp64_steps_match_reference(ctx, slab, variant):
+    u, uo, h, _ = _run(ctx, slab, variant, 0)
+    assert (slab["h"] == 0).sum() > (slab["health0"] == 0).sum() + 10000
+    assert np.array_equal(h, slab["h"])
+    scale = np.abs(slab["u"]).max()
+    assert np.abs(u - slab["u"]).max() <= 1e-10 * scale
+    assert np.abs(uo - slab["uo"]).max() <= 1e-10 * scale
+
+
+@pytest.mark.parametrize("variant", [1, 11, 17])
+def test_slab_mixed_steps_within_1e6(ctx, slab, variant):
+    u, _, h, _ = _run(ctx, slab, variant, 1)
+    assert np.abs(u - slab["u"]).max() <= 1e-6 * np.abs(slab["u"]).max()
+    assert (h != slab["h"]).sum() <= 1e-5 * h.size

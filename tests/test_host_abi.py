@@ -30,8 +30,13 @@ def test_library_exports_every_declared_symbol(px):
     lib = px.lib()
     names = declared("perix_b200.h")
     assert len(names) >= 40
-    missing = [n for n in names if not hasattr(lib, n)]
-    assert not missing, missing
+    headers = sorted(h for h in os.listdir(os.path.join(ROOT, "include")) if h.startswith("perix_b200") and h.endswith(".h"))
+    assert "perix_b200_measure.h" in headers
+    for h in headers:
+        names = declared(h)
+        assert names, h
+        missing = [n for n in names if not hasattr(lib, n)]
+        assert not missing, (h, missing)
 
 
 def test_dropin_symbols_exported(px):
