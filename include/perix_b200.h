@@ -105,12 +105,18 @@ int pxb_set_geometry_points(pxb_ctx *ctx, int n, int dim, const double *coords3,
 int pxb_get_families(pxb_ctx *ctx, int *neigh_off, int *neigh_id);
 
 /* ---- g-functions (reference PDOperators::buildGeometryCache, src/PDOperators/CalcPDOperators.cpp:356-463) ----
- * Builds the per-bond operator vectors ops[bond*nop+k] for multi-index order `order` on the device.
- * precision PXB_MIXED accumulates the moment sums in FP32 on delta-scaled bond vectors with compensated
- * (two-sum) accumulation, keeps the solve and one refinement step in FP64, and stores g in FP32.
+ * Builds the per-bond operator vectors ops[bond*nop+k] for multi-index order `order` (2D 1..4, 3D 1..3) on the
+ * device.  precision PXB_MIXED stores g in FP32 with the solve and one refinement step in FP64; its moment sums run
+ * in FP32 on delta-scaled bond vectors with compensated (two-sum) accumulation on the lane-group schedule and in FP64
+ * on the warp-per-node schedule (pxb_gbuild_set_schedule).
  * Returns PXB_ERR_DEGENERATE when a non-ghost family is degenerate; *n_degenerate / *first_degenerate
  * (1-based) describe them (either may be NULL).  Deep ghosts (layer > 1) get zero operators. */
 int pxb_gbuild(pxb_ctx *ctx, int order, int precision, int *n_degenerate, int *first_degenerate);
+/* Schedule of the g-build kernels: 0 lane groups (a group of 8-32 lanes per node; at MIXED the moment sums run in
+ * FP32 with two-sum compensation), 1 one warp per node (moment sums in FP64 at both precisions; MIXED stores FP32),
+ * -1 (default) the one this backend picks: warp per node in 3D and above order 2, lane groups for 2D orders 1-2.
+ * Orders 2D 4 and 3D 3 exist only as the warp-per-node schedule. */
+int pxb_gbuild_set_schedule(pxb_ctx *ctx, int schedule);
 /* nop of the current operator cache and its multi-index table (pqr: 3*nop ints, may be NULL). */
 int pxb_gbuild_info(pxb_ctx *ctx, int *nop, int *pqr);
 /* Copy the operator cache to host (always returned as double). */

@@ -361,6 +361,10 @@ class Context:
         _check(self.L.pxb_get_families(self.h, _p(off, C.c_int), _p(ids, C.c_int)))
         return off, ids[:self.nb]
 
+    def gbuild_set_schedule(self, schedule):
+        """-1 default, 0 lane groups, 1 one warp per node (pxb_gbuild_set_schedule)."""
+        _check(self.L.pxb_gbuild_set_schedule(self.h, int(schedule)))
+
     def gbuild(self, order=2, precision=FP64, allow_degenerate=False):
         nd = C.c_int(0)
         first = C.c_int(0)

@@ -405,12 +405,26 @@ static GBuildArgs gbuild_args(pxb_ctx *c, void *ops_out, void *G_out, uint8_t *d
     return a;
 }
 
+// the g-build schedule for this problem: one warp per node (k_gbuild_warp.cu) for 3D and for 2D above order 2,
+// lane groups (k_gbuild.cu) for 2D orders 1-2, unless pxb_gbuild_set_schedule chose one
+static bool gbuild_use_warp(const pxb_ctx *c, int order) {
+    if (!gbuild_warp_supported(c->g.dim, order)) return false;
+    if (!gbuild_supported(c->g.dim, order)) return true;
+    if (c->gbuild_schedule >= 0) return c->gbuild_schedule == 1;
+    return c->g.dim == 3 || order > 2;
+}
+
+static cudaError_t gbuild_launch(pxb_ctx *c, const GBuildArgs &a, int order, bool mixed) {
+    if (gbuild_use_warp(c, order)) return launch_gbuild_warp(a, c->g.dim, order, mixed, c->stream);
+    return launch_gbuild(a, c->g.dim, order, mixed, grid_nodes(c->g.n, kGbuildThreads), c->stream);
+}
+
 static int run_gbuild(pxb_ctx *c, int order, bool mixed, void *ops_out, void *G_out, uint8_t *deg_out,
                       int *n_degenerate, int *first_degenerate, float *defect = nullptr) {
     Geometry &g = c->g;
-    if (!gbuild_supported(g.dim, order))
+    if (!gbuild_supported(g.dim, order) && !gbuild_warp_supported(g.dim, order))
         return fail(PXB_ERR_UNSUPPORTED, "pxb_gbuild: order " + std::to_string(order) + " not built for dim " +
-                                             std::to_string(g.dim) + " (2D: 1..3, 3D: 1..2)");
+                                             std::to_string(g.dim) + " (2D: 1..4, 3D: 1..3)");
     void *tmp = nullptr;
     PXB_TRY(scratch(c, 16, &tmp));
     unsigned int *nd = static_cast<unsigned int *>(tmp);
@@ -419,7 +433,7 @@ static int run_gbuild(pxb_ctx *c, int order, bool mixed, void *ops_out, void *G_
     const int big = std::numeric_limits<int>::max();
     PXB_TRY(h2d(c, first, &big, sizeof(int)));
     const GBuildArgs a = gbuild_args(c, ops_out, G_out, deg_out, nd, first, defect);
-    cudaError_t e = launch_gbuild(a, g.dim, order, mixed, grid_nodes(g.n, kGbuildThreads), c->stream);
+    cudaError_t e = gbuild_launch(c, a, order, mixed);
     c->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "gbuild launch");
     unsigned int hnd = 0;
@@ -480,13 +494,19 @@ int gbuild_launch_only(pxb_ctx *c, int order, int precision) {
                                      static_cast<unsigned int *>(tmp),
                                      reinterpret_cast<int *>(static_cast<char *>(tmp) + 8),
                                      c->ops.defect.p ? c->ops.defect.as<float>() : nullptr);
-    cudaError_t e = launch_gbuild(a, c->g.dim, order, precision == PXB_MIXED, grid_nodes(c->g.n, kGbuildThreads),
-                                  c->stream);
+    cudaError_t e = gbuild_launch(c, a, order, precision == PXB_MIXED);
     c->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "gbuild launch");
     return PXB_OK;
 }
 }  // namespace pxb
+
+extern "C" int pxb_gbuild_set_schedule(pxb_ctx *c, int schedule) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_gbuild_set_schedule: NULL context");
+    if (schedule < -1 || schedule > 1) return fail(PXB_ERR_INVALID, "pxb_gbuild_set_schedule: -1, 0 or 1");
+    c->gbuild_schedule = schedule;
+    return PXB_OK;
+}
 
 extern "C" int pxb_gbuild_info(pxb_ctx *c, int *nop, int *pqr) {
     if (!c) return fail(PXB_ERR_INVALID, "pxb_gbuild_info: NULL context");

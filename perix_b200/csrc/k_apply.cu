@@ -217,7 +217,9 @@ BatchSchedule batch_apply_schedule(int v) {
         case 2: return {8, 32, false};
         case 3: return {8, 16, true};
         case 4: return {16, 16, false};
-        default: return {4, 16, true};
+        case 5: return {4, 16, true};
+        case 6: return {4, 32, false};
+        default: return {16, 32, true};
     }
 }
 

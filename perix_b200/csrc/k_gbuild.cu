@@ -435,7 +435,8 @@ __global__ void __launch_bounds__(kGbuildThreads) gbuild_batch_kernel(BatchArgs 
     }
 }
 
-// schedules 4 and 5 (mixed only; identical to 2 and 3 in FP64) sum the moments in FP64 (SUMS64)
+// schedules 4 and 5 (mixed only; identical to 2 and 3 in FP64) sum the moments in FP64 (SUMS64); 6 and 7 run one
+// warp per node (FP64 moment sums in both precisions), in one launch or one per dimension
 BatchSchedule batch_gbuild_schedule(int v) {
     switch (v) {
         case 0: return {8, 32, false};
@@ -443,7 +444,9 @@ BatchSchedule batch_gbuild_schedule(int v) {
         case 2: return {8, 16, false};
         case 3: return {8, 32, true};
         case 4: return {8, 16, false};
-        default: return {8, 32, true};
+        case 5: return {8, 32, true};
+        case 6: return {32, 32, false, true};
+        default: return {32, 32, true, true};
     }
 }
 
@@ -475,6 +478,8 @@ static cudaError_t launch_gb_m(const BatchArgs &a, int variant, int dims, cudaSt
 }
 
 cudaError_t launch_gbuild_batch(const BatchArgs &a, bool mixed, int variant, int dims, cudaStream_t s) {
+    const BatchSchedule sch = batch_gbuild_schedule(variant);
+    if (sch.warp) return launch_gbuild_batch_warp(a, mixed, sch.split, dims, s);
     return mixed ? launch_gb_m<true>(a, variant, dims, s) : launch_gb_m<false>(a, variant, dims, s);
 }
 

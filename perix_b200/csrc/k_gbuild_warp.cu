@@ -1,0 +1,498 @@
+// g-function build with one warp per node (reference PDOperators::calcAMatrixCompute / calcOperatorsCompute,
+// src/PDOperators/CalcPDOperators.cpp:108-226 and 307-354), for moment systems of up to 32 monomials.
+//
+// The lane-group build (k_gbuild.cu) keeps the whole packed moment matrix in every lane while it accumulates and
+// reduces, which at 3D order 2 (45 entries) takes ~250 registers a thread and leaves 2 blocks per SM.  Here:
+//   pass 1  the family is walked in chunks of 32 bonds, one bond per lane: the lane forms its bond's weight bw
+//           (cached in shared memory for pass 2) and monomials m, and the chunk's contribution to every entry
+//           A[p][q] += (bw m_p) m_q is summed over the warp by a recursive-halving reduce-scatter whose products
+//           are formed as the pairs are exchanged; after the five halvings each lane holds the chunk sums of at
+//           most ceil(NE/32) entries and adds them to its accumulators;
+//   solve   the entries go to shared memory, the warp factors A = L D L^T (right-looking, a row per lane), lane k
+//           solves column k of X = A^-1 diag(q!), takes one step of iterative refinement and the reference's
+//           max-norm consistency test (src/MathUtils/MatrixXd.cpp:40-47) decides degeneracy;
+//   pass 2  one bond per lane again: op_k = (sum_p X[p][k] m_p) bw / delta^|q_k| for every slot k, written as the
+//           AoS operator vector and/or the SoA Navier subset; MIXED stores FP32 (sums stay FP64) and, at order 2,
+//           the per-node first moments of the stored second-derivative operators (GBuildArgs::defect).
+// Per-node horizons (GBuildArgs::node_delta / node_dxc) follow the reference's variable-horizon path: node i
+// uses its own delta_i and spacing, and bonds longer than delta_i stay out of its moment system and get zero
+// operators (CalcPDOperators.cpp:113-147, 307-354).
+#include <cfloat>
+
+#include "k_kernels.h"
+#include "pxb_common.cuh"
+
+namespace pxb {
+
+namespace {
+
+constexpr int kWarpNodeThreads = 128;  // 4 warps (nodes) per block
+constexpr int kBwCache = 256;          // bond weights per node cached for pass 2 (longer families recompute)
+
+// packed upper triangle (p <= q, row-major) of an NOP x NOP symmetric matrix
+template <int NOP>
+struct Tri {
+    static constexpr int NE = NOP * (NOP + 1) / 2;
+    int p[NE], q[NE];
+    __host__ __device__ constexpr Tri() : p{}, q{} {
+        int e = 0;
+        for (int a = 0; a < NOP; ++a)
+            for (int b = a; b < NOP; ++b) {
+                p[e] = a;
+                q[e] = b;
+                ++e;
+            }
+    }
+};
+
+__host__ __device__ constexpr int halve(int n) { return (n + 1) / 2; }
+
+// shared-memory loads the compiler may not hoist out of the bond loops (it would otherwise keep the whole
+// loop-invariant X, A or L D L^T in registers)
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ double lds(const double *p) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(smem_addr(p)));
+    return v;
+}
+__device__ __forceinline__ double2 lds2(const double *p) {
+    double2 v;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(smem_addr(p)));
+    return v;
+}
+
+// one halving of a reduce-scatter: lanes whose bit MASK is clear keep the first half of the list, their partners
+// the second; each sends the other half and adds what it receives (a missing odd element counts as 0)
+template <int N, int MASK>
+__device__ __forceinline__ void rs_level(const double (&in)[N], double (&out)[halve(N)], bool upper) {
+    constexpr int H = halve(N);
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+        const double lo = in[k];
+        const double hi = (H + k < N) ? in[(H + k < N) ? H + k : 0] : 0.0;
+        const double send = upper ? lo : hi;
+        const double keep = upper ? hi : lo;
+        out[k] = keep + __shfl_xor_sync(kFull, send, MASK);
+    }
+}
+
+// entry index held in final slot s by this lane after the five halvings of an NE-long list (-1: padding)
+template <int NE>
+__device__ __forceinline__ int rs_entry(int lane, int s) {
+    constexpr int L0 = NE, L1 = halve(L0), L2 = halve(L1), L3 = halve(L2), L4 = halve(L3);
+    int p = s;
+    p = (lane & 1) ? halve(L4) + p : p;
+    if (p >= L4) return -1;
+    p = (lane & 2) ? halve(L3) + p : p;
+    if (p >= L3) return -1;
+    p = (lane & 4) ? halve(L2) + p : p;
+    if (p >= L2) return -1;
+    p = (lane & 8) ? halve(L1) + p : p;
+    if (p >= L1) return -1;
+    p = (lane & 16) ? halve(L0) + p : p;
+    if (p >= L0) return -1;
+    return p;
+}
+
+struct BondGeo {
+    double dx, dy, dz, bw;
+};
+
+// bond t of node i: the bond vector and the weight bw = w(|xi|) vc(|xi|) V_j (0 when the bond is skipped: zero
+// length, outside the node's own horizon, or a non-positive weight)
+template <int DIM, typename PosT>
+__device__ __forceinline__ BondGeo bond_geo(const GBuildArgs &a, const PosT *pos, const PosT &xi, int t, double delta,
+                                            double dxc, bool own_horizon) {
+    BondGeo g{0.0, 0.0, 0.0, 0.0};
+    const int j = a.nbr[t];
+    const PosT xj = pos[j - a.node_base];
+    g.dx = xj.x - xi.x;
+    g.dy = xj.y - xi.y;
+    if constexpr (DIM == 3) g.dz = xj.z - xi.z;
+    const double xn = sqrt(g.dx * g.dx + g.dy * g.dy + g.dz * g.dz);
+    if (xn > 0.0 && !(own_horizon && xn > delta)) {
+        const double bw = bond_weight(xn, delta) * rim_correction(xn, delta, dxc) * a.vol[j];
+        if (bw > 0.0) g.bw = bw;
+    }
+    return g;
+}
+
+}  // namespace
+
+// Shared memory a warp needs for one node of NOP monomials (doubles): weight cache, A, L D L^T, X (rows padded
+// to an even count so that rows load as double2).
+template <int NOP>
+struct WarpNodeSmem {
+    static constexpr int NP = (NOP + 1) & ~1;
+    double bw[kBwCache];
+    double A[NOP * NOP];
+    double L[NOP * NOP];
+    double X[NOP * NP];
+};
+
+template <int DIM, int ORDER, bool MIXED>
+__device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int lane,
+                                                 WarpNodeSmem<nop_of(DIM, ORDER)> &sm) {
+    constexpr QTable<DIM, ORDER> Q{};
+    constexpr int NOP = Q.NOP;
+    constexpr Tri<NOP> T{};
+    constexpr int NE = Tri<NOP>::NE;
+    constexpr int L1 = halve(NE), L2 = halve(L1), L3 = halve(L2), L4 = halve(L3), L5 = halve(L4);
+    constexpr int NP = WarpNodeSmem<NOP>::NP;
+    static_assert(NOP <= 32, "one lane per solve column");
+    using PosT = typename Vec<DIM>::T;
+    const PosT *pos = static_cast<const PosT *>(a.pos);
+    const bool own_h = a.node_delta != nullptr;
+    const double delta = own_h ? a.node_delta[i - a.node_base] : a.delta;
+    const double dxc = own_h ? a.node_dxc[i - a.node_base] : a.dx_char;
+    const double inv_delta = 1.0 / delta;
+    const int b0 = a.off[i], b1 = a.off[i + 1];
+    const PosT xi = pos[i - a.node_base];
+
+    // ---- pass 1: moment sums, chunk by chunk ----
+    double acc[L5];
+#pragma unroll
+    for (int s = 0; s < L5; ++s) acc[s] = 0.0;
+    int usable = 0;
+    for (int c0 = b0; c0 < b1; c0 += kWarp) {
+        const int t = c0 + lane;
+        BondGeo g{0.0, 0.0, 0.0, 0.0};
+        if (t < b1) g = bond_geo<DIM>(a, pos, xi, t, delta, dxc, own_h);
+        if (t < b1 && t - b0 < kBwCache) sm.bw[t - b0] = g.bw;
+        usable += g.bw > 0.0 ? 1 : 0;
+        double m[NOP], wm[NOP];
+        monomials<DIM, ORDER, double>(g.dx * inv_delta, g.dy * inv_delta, g.dz * inv_delta, m);
+#pragma unroll
+        for (int k = 0; k < NOP; ++k) wm[k] = g.bw * m[k];
+        // first halving with the products formed as they are exchanged
+        double v1[L1];
+        {
+            const bool upper = (lane & 16) != 0;
+#pragma unroll
+            for (int k = 0; k < L1; ++k) {
+                constexpr int dummy = 0;
+                const int kh = (L1 + k < NE) ? L1 + k : dummy;
+                const double lo = wm[T.p[k]] * m[T.q[k]];
+                const double hi = (L1 + k < NE) ? wm[T.p[kh]] * m[T.q[kh]] : 0.0;
+                const double send = upper ? lo : hi;
+                const double keep = upper ? hi : lo;
+                v1[k] = keep + __shfl_xor_sync(kFull, send, 16);
+            }
+        }
+        double v2[L2], v3[L3], v4[L4], v5[L5];
+        rs_level<L1, 8>(v1, v2, (lane & 8) != 0);
+        rs_level<L2, 4>(v2, v3, (lane & 4) != 0);
+        rs_level<L3, 2>(v3, v4, (lane & 2) != 0);
+        rs_level<L4, 1>(v4, v5, (lane & 1) != 0);
+#pragma unroll
+        for (int s = 0; s < L5; ++s) acc[s] += v5[s];
+    }
+    usable = group_sum_int<kWarp>(usable);
+#pragma unroll
+    for (int s = 0; s < L5; ++s) {
+        const int e = rs_entry<NE>(lane, s);
+        if (e >= 0) {
+            sm.A[T.p[e] * NOP + T.q[e]] = acc[s];
+            sm.A[T.q[e] * NOP + T.p[e]] = acc[s];
+            sm.L[T.p[e] * NOP + T.q[e]] = acc[s];
+            sm.L[T.q[e] * NOP + T.p[e]] = acc[s];
+        }
+    }
+    __syncwarp();
+
+    // ---- solve: A = L D L^T right-looking in sm.L (row r in lane r; D on the diagonal, L below) ----
+    for (int j = 0; j < NOP; ++j) {
+        const double d = sm.L[j * NOP + j];
+        const double cr = (lane > j && lane < NOP) ? sm.L[lane * NOP + j] : 0.0;  // column j before scaling
+        __syncwarp();
+        if (lane > j && lane < NOP) {
+            const double l = cr / d;
+            for (int k = j + 1; k <= lane; ++k) sm.L[lane * NOP + k] -= l * sm.L[k * NOP + j];
+        }
+        __syncwarp();
+        if (lane > j && lane < NOP) sm.L[lane * NOP + j] = cr / d;
+        __syncwarp();
+    }
+    // lane k < NOP: column k of X = A^-1 diag(q!), one refinement step, the consistency test's residual
+    const int kc = lane < NOP ? lane : 0;
+    double fk = 0.0;
+#pragma unroll
+    for (int q = 0; q < NOP; ++q)
+        if (q == kc) fk = Q.fact[q];
+    auto solve = [&](double *x) {
+#pragma unroll
+        for (int r = 0; r < NOP; ++r) {
+#pragma unroll
+            for (int l = 0; l < r; ++l) x[r] -= lds(&sm.L[r * NOP + l]) * x[l];
+        }
+#pragma unroll
+        for (int r = 0; r < NOP; ++r) x[r] /= lds(&sm.L[r * NOP + r]);
+#pragma unroll
+        for (int r = NOP - 1; r >= 0; --r) {
+#pragma unroll
+            for (int l = r + 1; l < NOP; ++l) x[r] -= lds(&sm.L[l * NOP + r]) * x[l];
+        }
+    };
+    double x[NOP];
+#pragma unroll
+    for (int q = 0; q < NOP; ++q) x[q] = (q == kc) ? fk : 0.0;
+    solve(x);
+    double r[NOP];
+    double res = 0.0, maxA = 0.0, maxX = 0.0;
+#pragma unroll
+    for (int p = 0; p < NOP; ++p) {
+        double sres = (p == kc) ? fk : 0.0;
+#pragma unroll
+        for (int q = 0; q < NOP; ++q) {
+            const double apq = lds(&sm.A[p * NOP + q]);
+            sres -= apq * x[q];
+            maxA = fmax(maxA, fabs(apq));
+        }
+        r[p] = sres;
+        res = fmax(res, fabs(sres));
+        maxX = fmax(maxX, fabs(x[p]));
+    }
+    solve(r);
+#pragma unroll
+    for (int q = 0; q < NOP; ++q) x[q] += r[q];
+    if (lane >= NOP) { res = 0.0; maxX = 0.0; }
+    res = group_max<kWarp>(res);
+    maxX = group_max<kWarp>(maxX);
+    double maxB = 0.0;
+#pragma unroll
+    for (int q = 0; q < NOP; ++q) maxB = fmax(maxB, Q.fact[q]);
+    const double scale = fmax(fmax(maxB, maxA * maxX), DBL_MIN);
+    const bool consistent = (res <= 1.0e-8 * scale);  // NaN-safe: NaN fails
+    const bool degenerate = (usable < NOP) || !consistent;
+    const bool deep_ghost = (a.layer != nullptr) && (a.layer[i] > 1);
+    if (lane == 0) {
+        if (a.degenerate) a.degenerate[i] = degenerate ? 1 : 0;
+        if (degenerate && !deep_ghost) {
+            atomicAdd(a.n_degenerate, 1u);
+            atomicMin(a.first_degenerate, i);
+        }
+    }
+    if (lane < NP) {
+#pragma unroll
+        for (int p = 0; p < NOP; ++p) sm.X[p * NP + lane] = (degenerate || lane >= NOP) ? 0.0 : x[p];
+    }
+    __syncwarp();
+
+    // ---- pass 2: per-bond operators ----
+    constexpr bool DEF = MIXED && ORDER == 2;
+    constexpr int ND = DEF ? (NOP - DIM) * DIM : 1;
+    double dsum[ND];
+#pragma unroll
+    for (int e = 0; e < ND; ++e) dsum[e] = 0.0;
+    for (int c0 = b0; c0 < b1; c0 += kWarp) {
+        const int t = c0 + lane;
+        if (t >= b1) continue;
+        BondGeo g;
+        if (t - b0 < kBwCache) {
+            const int j = a.nbr[t];
+            const PosT xj = pos[j - a.node_base];
+            g.dx = xj.x - xi.x;
+            g.dy = xj.y - xi.y;
+            g.dz = 0.0;
+            if constexpr (DIM == 3) g.dz = xj.z - xi.z;
+            g.bw = sm.bw[t - b0];
+        } else {
+            g = bond_geo<DIM>(a, pos, xi, t, delta, dxc, own_h);
+        }
+        double m[NOP];
+        monomials<DIM, ORDER, double>(g.dx * inv_delta, g.dy * inv_delta, g.dz * inv_delta, m);
+        double op[NOP];
+#pragma unroll
+        for (int k = 0; k < NOP; k += 2) {
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int p = 0; p < NOP; ++p) {
+                const double2 xr = lds2(&sm.X[p * NP + k]);
+                s0 += xr.x * m[p];
+                s1 += xr.y * m[p];
+            }
+            // op_k = (sum_p X[p][k] m_p) bw / delta^|q_k|
+            double ip0 = 1.0, ip1 = 1.0;
+#pragma unroll
+            for (int t2 = 0; t2 < Q.p[k] + Q.q[k] + Q.r[k]; ++t2) ip0 *= inv_delta;
+            constexpr int dummy = 0;
+            const int k1 = (k + 1 < NOP) ? k + 1 : dummy;
+#pragma unroll
+            for (int t2 = 0; t2 < Q.p[k1] + Q.q[k1] + Q.r[k1]; ++t2) ip1 *= inv_delta;
+            op[k] = g.bw > 0.0 ? s0 * g.bw * ip0 : 0.0;
+            if (k + 1 < NOP) op[k1] = g.bw > 0.0 ? s1 * g.bw * ip1 : 0.0;
+        }
+        if (a.ops) {
+            if constexpr (MIXED) {
+                float *o = static_cast<float *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
+#pragma unroll
+                for (int k = 0; k < NOP; ++k) {
+                    const float gk = (float)op[k];
+                    o[k] = gk;
+                    if constexpr (DEF) {
+                        if (k >= DIM) {
+                            dsum[(k - DIM) * DIM + 0] += (double)gk * g.dx;
+                            dsum[(k - DIM) * DIM + 1] += (double)gk * g.dy;
+                            if constexpr (DIM == 3) dsum[(k - DIM) * DIM + 2] += (double)gk * g.dz;
+                        }
+                    }
+                }
+            } else {
+                double *o = static_cast<double *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
+#pragma unroll
+                for (int k = 0; k < NOP; ++k) o[k] = op[k];
+            }
+        }
+        if constexpr (ORDER >= 2) {
+            if (a.G) {
+                constexpr int NC = (DIM == 3) ? 6 : 3;
+                int sl[NC];
+                if constexpr (DIM == 3) {
+                    sl[0] = Q.slot(2, 0, 0); sl[1] = Q.slot(0, 2, 0); sl[2] = Q.slot(0, 0, 2);
+                    sl[3] = Q.slot(1, 1, 0); sl[4] = Q.slot(1, 0, 1); sl[5] = Q.slot(0, 1, 1);
+                } else {
+                    sl[0] = Q.slot(2, 0, 0); sl[1] = Q.slot(0, 2, 0); sl[2] = Q.slot(1, 1, 0);
+                }
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    const double v = op[sl[c]];
+                    if constexpr (MIXED) static_cast<float *>(a.G)[(size_t)c * a.nb + t] = (float)v;
+                    else static_cast<double *>(a.G)[(size_t)c * a.nb + t] = v;
+                }
+            }
+        }
+    }
+    if constexpr (DEF) {
+        if (a.defect) {
+            float *dst = a.defect + (size_t)(i - a.node_base) * ND;
+#pragma unroll
+            for (int e = 0; e < ND; ++e) {
+                const double v = group_sum<kWarp>(dsum[e]);
+                if (lane == (e & 31)) dst[e] = (float)v;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// single geometry: one warp per node, grid-stride over the nodes; MINB resident blocks bound the registers
+// (128 a thread at 4, where the 3D order-2 node spills a few dozen bytes)
+template <int DIM, int ORDER, bool MIXED, int MINB>
+__global__ void __launch_bounds__(kWarpNodeThreads, MINB) gbuild_warp_kernel(GBuildArgs a) {
+    constexpr int NOP = nop_of(DIM, ORDER);
+    constexpr int WPB = kWarpNodeThreads / kWarp;
+    __shared__ WarpNodeSmem<NOP> sm[WPB];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    for (long long i = (long long)blockIdx.x * WPB + w; i < a.n; i += (long long)gridDim.x * WPB)
+        gbuild_warp_node<DIM, ORDER, MIXED>(a, (int)i, lane, sm[w]);
+}
+
+template <int DIM, int ORDER>
+static cudaError_t launch_warp_order(const GBuildArgs &a, bool mixed, cudaStream_t s) {
+    constexpr int WPB = kWarpNodeThreads / kWarp;
+    constexpr int MINB = nop_of(DIM, ORDER) <= 5 ? 5 : (nop_of(DIM, ORDER) <= 9 ? 4 : 2);
+    auto k = mixed ? gbuild_warp_kernel<DIM, ORDER, true, MINB> : gbuild_warp_kernel<DIM, ORDER, false, MINB>;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kWarpNodeThreads, 0);
+    const long long need = ((long long)a.n + WPB - 1) / WPB;
+    const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    const int grid = (int)(need < cap ? (need > 0 ? need : 1) : cap);
+    k<<<grid, kWarpNodeThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gbuild_warp(const GBuildArgs &a, int dim, int order, bool mixed, cudaStream_t s) {
+    if (dim == 2) {
+        switch (order) {
+            case 1: return launch_warp_order<2, 1>(a, mixed, s);
+            case 2: return launch_warp_order<2, 2>(a, mixed, s);
+            case 3: return launch_warp_order<2, 3>(a, mixed, s);
+            case 4: return launch_warp_order<2, 4>(a, mixed, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (order) {
+        case 1: return launch_warp_order<3, 1>(a, mixed, s);
+        case 2: return launch_warp_order<3, 2>(a, mixed, s);
+        case 3: return launch_warp_order<3, 3>(a, mixed, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---- batched clouds: persistent warps over the task table, one node at a time per warp (order 2) ----------------
+template <int A, int B>
+union BatchWarpSmem {
+    WarpNodeSmem<A> s2;
+    WarpNodeSmem<B> s3;
+};
+
+template <bool MIXED, int DIMS, int MINB>
+__global__ void __launch_bounds__(kWarpNodeThreads, MINB) gbuild_batch_warp_kernel(BatchArgs b) {
+    constexpr int WPB = kWarpNodeThreads / kWarp;
+    __shared__ BatchWarpSmem<5, 9> sm[WPB];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    for (;;) {
+        int task = 0;
+        if (lane == 0) task = (int)atomicAdd(b.counter, 1u);
+        task = __shfl_sync(kFull, task, 0);
+        if (task >= b.ntasks) break;
+        const BatchTask tk = b.tasks[b.task0 + task];
+        const BatchCloud cd = b.clouds[tk.cloud];
+        GBuildArgs a;
+        a.n = cd.node0 + cd.n;
+        a.off = b.off;
+        a.nbr = b.nbr;
+        a.pos = b.pos + cd.pos_off;
+        a.vol = b.vol;
+        a.delta = cd.delta;
+        a.dx_char = cd.dx_char;
+        a.ops = MIXED ? (void *)(static_cast<float *>(b.ops) + cd.ops_off)
+                      : (void *)(static_cast<double *>(b.ops) + cd.ops_off);
+        a.degenerate = b.degenerate;
+        a.n_degenerate = b.n_degenerate;
+        a.first_degenerate = b.first_degenerate;
+        a.node_base = cd.node0;
+        a.bond_base = cd.bond0;
+        a.defect = (MIXED && b.defect) ? b.defect + cd.def_off : nullptr;
+        for (int k = 0; k < tk.count; ++k) {
+            if constexpr ((DIMS & 1) != 0) {
+                if (tk.dim == 2) gbuild_warp_node<2, 2, MIXED>(a, tk.first + k, lane, sm[w].s2);
+            }
+            if constexpr ((DIMS & 2) != 0) {
+                if (tk.dim == 3) gbuild_warp_node<3, 2, MIXED>(a, tk.first + k, lane, sm[w].s3);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <bool MIXED, int DIMS, int MINB>
+static cudaError_t launch_gbw(const BatchArgs &a, cudaStream_t s) {
+    auto k = gbuild_batch_warp_kernel<MIXED, DIMS, MINB>;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kWarpNodeThreads, 0);
+    const long long want = ((long long)a.ntasks + (kWarpNodeThreads / kWarp) - 1) / (kWarpNodeThreads / kWarp);
+    const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    const int grid = (int)(want < cap ? (want > 0 ? want : 1) : cap);
+    k<<<grid, kWarpNodeThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// split: one launch per dimension (dims 1: 2D tasks, 2: 3D tasks) with its own register bound
+cudaError_t launch_gbuild_batch_warp(const BatchArgs &a, bool mixed, bool split, int dims, cudaStream_t s) {
+    if (!split) return mixed ? launch_gbw<true, 3, 4>(a, s) : launch_gbw<false, 3, 4>(a, s);
+    if (dims == 1) return mixed ? launch_gbw<true, 1, 5>(a, s) : launch_gbw<false, 1, 5>(a, s);
+    return mixed ? launch_gbw<true, 2, 4>(a, s) : launch_gbw<false, 2, 4>(a, s);
+}
+
+bool gbuild_warp_supported(int dim, int order) {
+    return (dim == 2 && order >= 1 && order <= 4) || (dim == 3 && order >= 1 && order <= 3);
+}
+
+}  // namespace pxb

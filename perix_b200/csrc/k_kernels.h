@@ -33,9 +33,15 @@ struct GBuildArgs {
     // sum_j g~^k_j xi_j[m] for k = dim..nop-1, m < dim (exactly 0 for exact operators; FP32 is ample for a
     // correction of that size), at defect[(i - node_base) * (nop - dim) * dim + (k - dim) * dim + m]; may be null
     float *defect = nullptr;
+    // per-node horizon and spacing (variable horizon), read at [i - node_base]; null: delta / dx_char for all
+    const double *node_delta = nullptr;
+    const double *node_dxc = nullptr;
 };
 cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, int grid, cudaStream_t s);
 bool gbuild_supported(int dim, int order);
+// one warp per node (k_gbuild_warp.cu): FP64 moment sums; MIXED stores FP32 operators (and the order-2 defects)
+cudaError_t launch_gbuild_warp(const GBuildArgs &a, int dim, int order, bool mixed, cudaStream_t s);
+bool gbuild_warp_supported(int dim, int order);
 
 // ------------------------------------------------------------------------------ families on the device (A1)
 constexpr int kFamMax = 256;   // largest family the device build sorts
@@ -101,8 +107,10 @@ struct BatchArgs {
 struct BatchSchedule {
     int lpn2, lpn3;
     bool split;
+    bool warp = false;  // g-build: one warp per node (k_gbuild_warp.cu) instead of lane groups
 };
-constexpr int kBatchVariants = 6;
+constexpr int kBatchVariants = 8;
+cudaError_t launch_gbuild_batch_warp(const BatchArgs &a, bool mixed, bool split, int dims, cudaStream_t s);
 BatchSchedule batch_gbuild_schedule(int variant);
 BatchSchedule batch_apply_schedule(int variant);
 // dims: 1 = 2D tasks only, 2 = 3D tasks only, 3 = both

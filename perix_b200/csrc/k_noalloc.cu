@@ -82,7 +82,8 @@ extern "C" int pxb_gbuild_noalloc_d(int dim, int order, int precision, int n, lo
     if ((dim != 2 && dim != 3) || n <= 0 || nbtot < 0 || !neigh_off_d || !neigh_id0_d || !coords3_d || !vols_d ||
         !ops_d || !(delta > 0.0) || (precision != PXB_FP64 && precision != PXB_MIXED))
         return fail(PXB_ERR_INVALID, "pxb_gbuild_noalloc_d: bad arguments");
-    if (!gbuild_supported(dim, order)) return fail(PXB_ERR_UNSUPPORTED, "pxb_gbuild_noalloc_d: order not built for this dimension");
+    if (!gbuild_supported(dim, order) && !gbuild_warp_supported(dim, order))
+        return fail(PXB_ERR_UNSUPPORTED, "pxb_gbuild_noalloc_d: order not built for this dimension");
     if (n > pxb_gbuild_noalloc_max_nodes(dim))
         return fail(PXB_ERR_INVALID, "pxb_gbuild_noalloc_d: " + std::to_string(n) + " nodes exceed the " +
                                          std::to_string(pxb_gbuild_noalloc_max_nodes(dim)) + "-node limit of the " +
@@ -132,7 +133,10 @@ extern "C" int pxb_gbuild_noalloc_d(int dim, int order, int precision, int n, lo
     a.n_degenerate = nd;
     a.first_degenerate = first;
     a.defect = with_defect ? defect_d : nullptr;
-    PXB_CUDA_TRY(launch_gbuild(a, dim, order, precision == PXB_MIXED, sms * 16, s));
+    // the schedule pxb_gbuild picks by default: one warp per node in 3D and above order 2, lane groups otherwise
+    const bool warp = !gbuild_supported(dim, order) || dim == 3 || order > 2;
+    if (warp) PXB_CUDA_TRY(launch_gbuild_warp(a, dim, order, precision == PXB_MIXED, s));
+    else PXB_CUDA_TRY(launch_gbuild(a, dim, order, precision == PXB_MIXED, sms * 16, s));
     unsigned int hnd = 0;
     int hfirst = 0;
     PXB_CUDA_TRY(cudaMemcpyAsync(&hnd, nd, sizeof(hnd), cudaMemcpyDeviceToHost, s));

@@ -198,6 +198,7 @@ struct BatchState {
 struct pxb_ctx {
     int device = 0;
     size_t mem_limit = 0;  // device bytes the context may hold (0: no limit beyond the GPU's)
+    int gbuild_schedule = -1;  // g-build: -1 by problem, 0 lane groups, 1 one warp per node
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
     long long launches = 0;

@@ -1,0 +1,103 @@
+"""The warp-per-node g-build schedule (k_gbuild_warp.cu) and the orders it adds, against the reference.
+
+* Both schedules (lane groups and one warp per node) on every golden fixture made by the reference's own code:
+  FP64 within 1e-12 (family-scaled), mixed within 1e-6.
+* Orders above 2 (2D orders 3 and 4 - the 14 monomials of the reference GPU path's kMaxNop = 15 - and 3D order 3)
+  against the reference's PDOperators on a lattice with mirror ghosts and on a jittered cloud
+  (oracle/_ref/libperix_ref.so), and against the C restatement.
+* A degenerate family is reported with its 1-based node id by both schedules."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, scaled_err
+from oracle import ref_available
+
+pytestmark = pytest.mark.gpu
+
+FIXTURES = [("poisson16", 2), ("lattice3d", 3), ("cloud2d", 2), ("cloud3d", 3), ("epf2d", 2), ("epf3d", 3)]
+
+
+def _geometry(ctx, d, dim):
+    s = d["scalars"]
+    ctx.set_geometry(d["coords"], d["vols"], d["off"], d["ids"], s[0], s[4], dim, mirror=d["mirror"])
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("name,dim", FIXTURES)
+def test_schedules_match_reference_goldens(ctx, name, dim, schedule):
+    d = load_golden(name)
+    if "ops" not in d:
+        pytest.skip("fixture without a full operator cache")
+    _geometry(ctx, d, dim)
+    ctx.gbuild_set_schedule(schedule)
+    try:
+        ctx.gbuild(2, 0)
+        assert scaled_err(ctx.get_ops(), d["ops"], d["off"]) <= 1e-12
+        ctx.gbuild(2, 1)
+        assert scaled_err(ctx.get_ops(), d["ops"], d["off"]) <= 1e-6
+    finally:
+        ctx.gbuild_set_schedule(-1)
+
+
+def _ref_mesh(dim, order, kind):
+    from oracle import RefMesh
+    if kind == "lattice":
+        if dim == 2:
+            return RefMesh.structured(2, 16, 12, 0, [0, 1.6, 0, 1.2], 3.015, order)
+        return RefMesh.structured(3, 8, 7, 6, [0, 0.8, 0, 0.7, 0, 0.6], 3.015, order)
+    rng = np.random.default_rng(5 + dim + order)
+    h = 0.1
+    shape = (14, 11) if dim == 2 else (8, 7, 6)
+    g = np.stack(np.meshgrid(*[np.arange(k) for k in shape], indexing="ij"), -1).reshape(-1, dim)
+    xyz = np.zeros((g.shape[0], 3))
+    xyz[:, :dim] = (g + 0.5) * h + rng.uniform(-0.2 * h, 0.2 * h, size=(g.shape[0], dim))
+    return RefMesh.cloud(dim, xyz, np.full(g.shape[0], h ** dim), h, h, h if dim == 3 else 0.0, 3.015 * h, order)
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference harness not built")
+@pytest.mark.parametrize("kind", ["lattice", "cloud"])
+@pytest.mark.parametrize("dim,order", [(2, 3), (2, 4), (3, 3)])
+def test_higher_orders_match_reference(ctx, port, dim, order, kind):
+    m = _ref_mesh(dim, order, kind)
+    g_ref, deg_ref = m.gbuild()
+    if deg_ref[m.mirror == 0].any():
+        pytest.skip("the reference finds degenerate bulk families at this order")
+    ctx.set_geometry(m.coords, m.vols, m.off, m.ids, m.delta, m.dx_char, dim,
+                     mirror=m.mirror if m.mirror.any() else None)
+    nd, _ = ctx.gbuild(order, 0, allow_degenerate=True)
+    g = ctx.get_ops()
+    assert g.shape == g_ref.shape
+    ok = np.repeat(deg_ref == 0, np.diff(m.off))  # rows the reference builds (deep/degenerate ghosts aside)
+    off_ok = np.concatenate([[0], np.cumsum(np.diff(m.off)[deg_ref == 0])])
+    assert scaled_err(g[ok], g_ref[ok], off_ok) <= 1e-12
+    g_port, _ = port.gbuild(dim, order, m.coords, m.vols, m.off, m.ids, m.delta, m.dx_char)
+    assert scaled_err(g[ok], g_port[ok], off_ok) <= 1e-12
+    ctx.gbuild(order, 1, allow_degenerate=True)
+    assert scaled_err(ctx.get_ops()[ok], g_ref[ok], off_ok) <= 1e-6
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_degenerate_family_reported_by_both_schedules(ctx, dim, schedule):
+    import perix_b200 as px
+    d = load_golden("poisson16" if dim == 2 else "lattice3d")
+    off, ids = d["off"], d["ids"]
+    bad = 40
+    lens = np.diff(off).copy()
+    parts = [ids[off[i]:off[i + 1]] if i != bad else ids[off[i]:off[i] + 3] for i in range(off.size - 1)]
+    lens[bad] = 3
+    off2 = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ids2 = np.concatenate(parts).astype(np.int32)
+    s = d["scalars"]
+    ctx.set_geometry(d["coords"], d["vols"], off2, ids2, s[0], s[4], dim, mirror=d["mirror"])
+    ctx.gbuild_set_schedule(schedule)
+    try:
+        with pytest.raises(px.PxbError) as e:
+            ctx.gbuild(2, 0)
+        assert e.value.status == 3 and ("node %d " % (bad + 1)) in str(e.value)
+        nd, first = ctx.gbuild(2, 0, allow_degenerate=True)
+        assert nd == 1 and first == bad + 1
+        g = ctx.get_ops()
+        assert np.all(g[off2[bad]:off2[bad + 1]] == 0.0)
+    finally:
+        ctx.gbuild_set_schedule(-1)
