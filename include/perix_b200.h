@@ -78,6 +78,19 @@ int pxb_families(int n, const double *coords3, double radius, int is3d, int ncra
                  int nplanes, const double *planes, const int *mirror, int force_only, int *neigh_off,
                  int *neigh_id, long long *nbtot);
 
+/* Families with a per-node horizon (the reference's VariableHorizon, CreatePDMesh.cpp:932-938, 1043-1057): the cell
+ * size is the largest horizon and a pair is kept when |x_i - x_j|^2 <= cut^2 (1 + 64 eps), cut = max(delta_i,
+ * delta_j), so each family is the dual family (it may hold j with |x_j - x_i| > delta_i).  Otherwise as
+ * pxb_families. */
+int pxb_families_vh(int n, const double *coords3, const double *node_horizon, int is3d, int ncracks,
+                    const double *cracks, int nplanes, const double *planes, const int *mirror, int force_only,
+                    int *neigh_off, int *neigh_id, long long *nbtot);
+/* Per-node horizon and rim spacing (reference PDMesh::computeVariableHorizon, CreatePDMesh.cpp:828-905):
+ * s_i = V_i^(1/dim), s_ref = median of s_i over bulk nodes (mirror[i] == 0; mirror may be NULL: all bulk),
+ * node_delta[i] = horizon s_i / s_ref, node_spacing[i] = dx_char s_i / s_ref (may be NULL). */
+int pxb_variable_horizon(int n, int dim, const double *vols, const int *mirror, double horizon, double dx_char,
+                         double *node_delta, double *node_spacing);
+
 /* Crack-crossing test for every bond of the family (reference src/PDMesh/PDMesh.cpp:104-159); out[t]=1
  * where bond t is cut.  Used to seed force-only notch health. */
 int pxb_crack_cut_mask(int n, const double *coords3, const int *mirror, const int *neigh_off, const int *neigh_id,
@@ -103,6 +116,11 @@ int pxb_set_geometry(pxb_ctx *ctx, int n, int dim, const double *coords3, const 
 int pxb_set_geometry_points(pxb_ctx *ctx, int n, int dim, const double *coords3, const double *vols, double radius,
                             double delta, double dx_char, const int *mirror, const int *layer_index, long long *nbtot);
 int pxb_get_families(pxb_ctx *ctx, int *neigh_off, int *neigh_id);
+/* Variable horizon for the context's geometry (the reference's NodeHorizon / NodeSpacing): node i's moment system and
+ * operators use delta_i and spacing_i (its rim correction; NULL spacing = 0, no rim correction), and bonds longer
+ * than delta_i get zero operators (CalcPDOperators.cpp:113-147, 307-354).  NULL node_delta clears them.  Call after
+ * pxb_set_geometry and before pxb_gbuild / pxb_epf_setup (the operator and explicit state are dropped). */
+int pxb_set_node_horizons(pxb_ctx *ctx, const double *node_delta, const double *node_spacing);
 
 /* ---- g-functions (reference PDOperators::buildGeometryCache, src/PDOperators/CalcPDOperators.cpp:356-463) ----
  * Builds the per-bond operator vectors ops[bond*nop+k] for multi-index order `order` (2D 1..4, 3D 1..3) on the
@@ -161,6 +179,12 @@ int pxb_apply_adjoint_d(pxb_ctx *ctx, const double *ybar_d, int nk, const int *s
 int pxb_epf_setup(pxb_ctx *ctx, int precision, double C11, double C12, double C66, double rho, const double *b,
                   double sc, int tension_only, const uint8_t *health0);
 
+/* Variable horizon: every bond breaks at its own critical stretch s_c(0.5 (delta_i + delta_j)) from the fracture
+ * energy G0, Young's modulus E and (2D) plane stress (ExplicitPDDOFracElement.cpp:254-261 with
+ * FractureCriterion.h:30-43), instead of the uniform sc of pxb_epf_setup.  Needs pxb_set_node_horizons; call after
+ * pxb_epf_setup.  The staged step kernels do not read per-bond thresholds: their variants then run the lane-group
+ * kernel. */
+int pxb_epf_set_variable_horizon_stretch(pxb_ctx *ctx, double G0, double E, int plane_stress);
 /* One rate evaluation at u (N*dim): damage then force, a = (L+b)/rho (the reference CUDA entry
  * assembleExplicitPDDOFracAccel).  *n_broken = bonds that broke in this call. */
 int pxb_epf_rate(pxb_ctx *ctx, const double *u, double *accel, long long *n_broken);

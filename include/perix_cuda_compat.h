@@ -8,7 +8,9 @@
  *   - there is no CPU fallback inside the backend: a device failure prints the reason to stderr and returns
  *     false, which is where the reference's callers take their CPU path; a build that must never run on the CPU
  *     replaces that branch by an abort;
- *   - a mesh with a per-node horizon (AssembleMesh::nodeHorizon set) is refused with a message (return false);
+ *   - a per-node horizon (AssembleMesh::nodeHorizon / nodeSpacing) is honoured by every entry: the g-build uses
+ *     node i's own horizon and spacing, and the explicit element breaks each bond at s_c(0.5 (delta_i + delta_j))
+ *     computed from ExplicitPDDOFracParams::G0, E and plane_stress;
  *   - assembleExplicitPDDOFracAccel times its schedules once per problem at its first call and keeps FP64
  *     operators unless the environment sets PERIX_B200_PRECISION=mixed.
  * The device work runs on a lazily created default pxb_ctx (device 0), freed by shutdown().

@@ -310,6 +310,7 @@ def _bind_ref(L):
     vp = C.c_void_p
     L.ref_mesh_structured.restype = vp
     L.ref_mesh_cloud.restype = vp
+    L.ref_mesh_cloud_vh.restype = vp
     L.ref_mesh_nodes.restype = C.c_int
     L.ref_mesh_bonds.restype = C.c_longlong
     L.ref_group_size.restype = C.c_int
@@ -388,6 +389,24 @@ class RefMesh:
         m.cracks = None
         m.planes = None
         m.force_only = False
+        return m
+
+    @classmethod
+    def cloud_vh(cls, dim, coords3, vols, dx, dy, dz, horizon, order=2, volume_correction=True, dropin=False):
+        """A cloud with the reference's variable horizon on (NodeHorizon / NodeSpacing from the node volumes, dual
+        families)."""
+        L = _ref_lib(dropin)
+        c = np.ascontiguousarray(coords3, np.float64).reshape(-1)
+        v = np.ascontiguousarray(vols, np.float64)
+        h = L.ref_mesh_cloud_vh(int(dim), c.size // 3, _ptr(c, C.c_double), _ptr(v, C.c_double), C.c_double(dx),
+                                C.c_double(dy), C.c_double(dz), C.c_double(horizon), int(order), int(volume_correction))
+        m = cls(h, dim, order, dropin)
+        m.cracks = None
+        m.planes = None
+        m.force_only = False
+        m.node_delta = np.zeros(m.n)
+        m.node_spacing = np.zeros(m.n)
+        L.ref_mesh_node_horizon(m.h, _ptr(m.node_delta, C.c_double), _ptr(m.node_spacing, C.c_double))
         return m
 
     def group(self, name):

@@ -141,6 +141,39 @@ void *ref_mesh_cloud(int dim, int n, const double *coords3, const double *vols, 
     return m;
 }
 
+// The same free cloud with the reference's variable horizon on (PDMeshData::VariableHorizon): every node is a bulk
+// node (NodesElmtID = 1), PDMesh::computeVariableHorizon sets NodeHorizon / NodeSpacing from the volumes, then
+// createNeighborNodes builds the dual families.
+void *ref_mesh_cloud_vh(int dim, int n, const double *coords3, const double *vols, double dx, double dy, double dz,
+                        double horizon_radius_no_margin, int order, int volume_correction) {
+    auto *m = new RefMesh();
+    m->dim = dim;
+    m->order = order;
+    auto &d = m->pd.getDataRef();
+    d.NodesNum = n;
+    d.BulkElmtsNum = n;
+    d.DX = dx; d.DY = dy; d.DZ = (dim == 3) ? dz : 0.0;
+    d.NodeCoords.assign(coords3, coords3 + 3 * (size_t)n);
+    d.NodeVolumes.assign(vols, vols + n);
+    d.NodesElmtID.assign((size_t)n, 1);
+    d.VolumeCorrection = volume_correction != 0;
+    m->pd.setHorizonRadius(horizon_radius_no_margin);
+    m->pd.setVariableHorizon(true);
+    m->pd.computeVariableHorizon();
+    m->pd.createNeighborNodes();
+    setupOps(m);
+    return m;
+}
+
+// NodeHorizon / NodeSpacing of the mesh (n each; zeros when the variable horizon is off)
+void ref_mesh_node_horizon(void *h, double *delta, double *spacing) {
+    const auto &d = static_cast<RefMesh *>(h)->pd.getDataConstRef();
+    for (int i = 0; i < d.NodesNum; ++i) {
+        delta[i] = d.NodeHorizon.empty() ? 0.0 : d.NodeHorizon[(size_t)i];
+        spacing[i] = d.NodeSpacing.empty() ? 0.0 : d.NodeSpacing[(size_t)i];
+    }
+}
+
 void ref_mesh_free(void *h) { delete static_cast<RefMesh *>(h); }
 
 int ref_mesh_nodes(void *h) { return static_cast<RefMesh *>(h)->pd.getNodesNum(); }

@@ -5,8 +5,9 @@ The compute path is ``libperix_b200.so`` (C++20 host + hand-written CUDA kernels
 bench.  It never computes on the CPU: if the library is missing, or no GPU is present, the call fails with
 ``PxbError``.
 """
-from .api import (PxbError, Context, lib, lib_path, lattice, families, crack_cut_mask, csr_pattern,  # noqa: F401
-                  multi_indices, elastic_constants, critical_stretch, FP64, MIXED, BC)
+from .api import (PxbError, Context, lib, lib_path, lattice, families, families_vh, variable_horizon,  # noqa: F401
+                  crack_cut_mask, csr_pattern, multi_indices, elastic_constants, critical_stretch, FP64, MIXED, BC)
 
-__all__ = ["PxbError", "Context", "lib", "lib_path", "lattice", "families", "crack_cut_mask", "csr_pattern",
-           "multi_indices", "elastic_constants", "critical_stretch", "FP64", "MIXED", "BC"]
+__all__ = ["PxbError", "Context", "lib", "lib_path", "lattice", "families", "families_vh", "variable_horizon",
+           "crack_cut_mask", "csr_pattern", "multi_indices", "elastic_constants", "critical_stretch", "FP64", "MIXED",
+           "BC"]

@@ -182,6 +182,35 @@ def families(coords3, radius, is3d, cracks=None, planes=None, mirror=None, force
     return off, ids[:nb.value]
 
 
+def families_vh(coords3, node_horizon, is3d, cracks=None, planes=None, mirror=None, force_only=False):
+    """Dual families of a variable horizon (pxb_families_vh): pairs within max(delta_i, delta_j)."""
+    L = lib()
+    c = _f64(coords3).reshape(-1)
+    n = c.size // 3
+    h = _f64(node_horizon)
+    cr = None if cracks is None or len(cracks) == 0 else _f64(cracks).reshape(-1)
+    pl = None if planes is None or len(planes) == 0 else _f64(planes).reshape(-1)
+    mir = _i32(mirror)
+    off = np.zeros(n + 1, np.int32)
+    nb = C.c_longlong(0)
+    args = (n, _p(c), _p(h), int(is3d), 0 if cr is None else cr.size // 4, _p(cr),
+            0 if pl is None else pl.size // 12, _p(pl), _p(mir, C.c_int), int(force_only))
+    _check(L.pxb_families_vh(*args, _p(off, C.c_int), None, C.byref(nb)))
+    ids = np.zeros(max(1, nb.value), np.int32)
+    _check(L.pxb_families_vh(*args, _p(off, C.c_int), _p(ids, C.c_int), C.byref(nb)))
+    return off, ids[:nb.value]
+
+
+def variable_horizon(dim, vols, horizon, dx_char, mirror=None):
+    """Per-node horizon and spacing from the node volumes (pxb_variable_horizon)."""
+    v = _f64(vols)
+    d = np.zeros(v.size, np.float64)
+    sp = np.zeros(v.size, np.float64)
+    _check(lib().pxb_variable_horizon(v.size, int(dim), _p(v), _p(_i32(mirror), C.c_int), C.c_double(horizon),
+                                      C.c_double(dx_char), _p(d), _p(sp)))
+    return d, sp
+
+
 def crack_cut_mask(coords3, mirror, off, ids, cracks=None, planes=None):
     L = lib()
     c = _f64(coords3).reshape(-1)
@@ -354,6 +383,15 @@ class Context:
                                               _p(_i32(layer), C.c_int), C.byref(nb)))
         self.n, self.dim, self.nb = n, int(dim), nb.value
         return nb.value
+
+    def set_node_horizons(self, node_delta, node_spacing=None):
+        """Variable horizon: per-node delta and rim spacing (None clears)."""
+        self._vh = (_f64(node_delta), _f64(node_spacing))
+        _check(self.L.pxb_set_node_horizons(self.h, _p(self._vh[0]), _p(self._vh[1])))
+
+    def epf_set_variable_horizon_stretch(self, G0, E, plane_stress=False):
+        """Per-bond critical stretch s_c(0.5 (delta_i + delta_j)) (pxb_epf_set_variable_horizon_stretch)."""
+        _check(self.L.pxb_epf_set_variable_horizon_stretch(self.h, C.c_double(G0), C.c_double(E), int(plane_stress)))
 
     def get_families(self):
         off = np.zeros(self.n + 1, np.int32)

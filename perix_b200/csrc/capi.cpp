@@ -354,6 +354,30 @@ extern "C" int pxb_set_geometry_points(pxb_ctx *c, int n, int dim, const double 
     return geometry_finish(c, fb.coords_d(), vols, mirror, layer_index);
 }
 
+static int need_geometry(pxb_ctx *c, const char *who);
+
+// Per-node horizon and spacing for the g-build (the reference's VariableHorizon; NULL delta clears them).  Drops the
+// operator caches built with the previous horizons.
+extern "C" int pxb_set_node_horizons(pxb_ctx *c, const double *node_delta, const double *node_spacing) {
+    PXB_TRY(need_geometry(c, "pxb_set_node_horizons"));
+    Geometry &g = c->g;
+    c->ops = OpsCache{};
+    destroy_graphs(c->epf);
+    c->epf = EpfState{};
+    g.node_delta = DevBuf{};
+    g.node_dxc = DevBuf{};
+    g.h_node_delta.clear();
+    if (!node_delta) return PXB_OK;
+    for (int i = 0; i < g.n; ++i)
+        if (!(node_delta[i] > 0.0)) return fail(PXB_ERR_INVALID, "pxb_set_node_horizons: delta must be > 0");
+    std::vector<double> sp((size_t)g.n, 0.0);
+    if (node_spacing) sp.assign(node_spacing, node_spacing + g.n);
+    PXB_TRY(dev_upload(c, g.node_delta, node_delta, sizeof(double) * (size_t)g.n));
+    PXB_TRY(dev_upload(c, g.node_dxc, sp.data(), sizeof(double) * (size_t)g.n));
+    g.h_node_delta.assign(node_delta, node_delta + g.n);
+    return sync(c);
+}
+
 // The families of the current geometry, 1-based ids (neigh_off: n+1 entries, neigh_id: neigh_off[n]).
 extern "C" int pxb_get_families(pxb_ctx *c, int *neigh_off, int *neigh_id) {
     if (!c || !c->g.ready) return fail(PXB_ERR_STATE, "pxb_get_families: geometry not set");
@@ -402,6 +426,10 @@ static GBuildArgs gbuild_args(pxb_ctx *c, void *ops_out, void *G_out, uint8_t *d
     a.n_degenerate = nd;
     a.first_degenerate = first;
     a.defect = defect;
+    if (g.node_delta.p) {
+        a.node_delta = g.node_delta.as<double>();
+        a.node_dxc = g.node_dxc.as<double>();
+    }
     return a;
 }
 
@@ -409,6 +437,7 @@ static GBuildArgs gbuild_args(pxb_ctx *c, void *ops_out, void *G_out, uint8_t *d
 // lane groups (k_gbuild.cu) for 2D orders 1-2, unless pxb_gbuild_set_schedule chose one
 static bool gbuild_use_warp(const pxb_ctx *c, int order) {
     if (!gbuild_warp_supported(c->g.dim, order)) return false;
+    if (c->g.node_delta.p) return true;  // per-node horizons: the warp-per-node kernel reads them
     if (!gbuild_supported(c->g.dim, order)) return true;
     if (c->gbuild_schedule >= 0) return c->gbuild_schedule == 1;
     return c->g.dim == 3 || order > 2;
@@ -663,6 +692,10 @@ static EpfArgs epf_args(pxb_ctx *c) {
     if (epf_is_tma(e.variant)) a.maxb = epf_tma_maxb(g.dim, e.variant, g.max_family);
     a.evict_first = e.evict_first ? 1 : 0;
     if (e.wait_tries >= 0) a.wait_tries = e.wait_tries;
+    if (e.sc_bond.p) {
+        a.sc_bond = e.sc_bond.as<double>();
+        a.damage = 1;
+    }
     return a;
 }
 
@@ -1324,6 +1357,40 @@ extern "C" int pxb_epf_force_frozen_d(pxb_ctx *c, const double *u_d, double *a_d
     a.damage = 0;
     launch_epf(a, c->g.dim, c->epf.precision == PXB_MIXED, EPF_FORCE_FROZEN, c->epf.variant, c->stream);
     return check_launch(c, "epf force (frozen mask)");
+}
+
+// s_c from the fracture energy (reference include/ElmtSystem/FractureCriterion.h:30-43): 3D 5 G0 / (6 E delta),
+// plane stress 4 pi G0 / (9 E delta), plane strain 5 pi G0 / (12 E delta); 0 when a value is not positive
+static double critical_stretch(double G0, double E, double delta, int dim, bool plane_stress) {
+    if (G0 <= 0.0 || E <= 0.0 || delta <= 0.0) return 0.0;
+    if (dim >= 3) return std::sqrt(5.0 * G0 / (6.0 * E * delta));
+    if (plane_stress) return std::sqrt(4.0 * M_PI * G0 / (9.0 * E * delta));
+    return std::sqrt(5.0 * M_PI * G0 / (12.0 * E * delta));
+}
+
+extern "C" int pxb_epf_set_variable_horizon_stretch(pxb_ctx *c, double G0, double E, int plane_stress) {
+    PXB_TRY(need_epf(c, "pxb_epf_set_variable_horizon_stretch"));
+    Geometry &g = c->g;
+    EpfState &e = c->epf;
+    if (g.h_node_delta.empty())
+        return fail(PXB_ERR_STATE, "pxb_epf_set_variable_horizon_stretch: no node horizons (pxb_set_node_horizons)");
+    std::vector<int> nbr((size_t)std::max(1LL, g.nb));
+    PXB_TRY(d2h(c, nbr.data(), g.nbr.p, sizeof(int) * (size_t)g.nb));
+    PXB_TRY(sync(c));
+    std::vector<double> sc((size_t)g.ldb, 0.0);
+    const bool ps = g.dim < 3 && plane_stress != 0;
+    for (int i = 0; i < g.n; ++i) {
+        const double di = g.h_node_delta[(size_t)i];
+        for (int t = g.h_off[(size_t)i]; t < g.h_off[(size_t)i + 1]; ++t) {
+            const double db = 0.5 * (di + g.h_node_delta[(size_t)nbr[(size_t)t]]);
+            sc[(size_t)t] = critical_stretch(G0, E, db, g.dim, ps);
+        }
+    }
+    destroy_graphs(e);
+    if (e.rate_graph) cudaGraphExecDestroy(e.rate_graph);
+    e.rate_graph = nullptr;
+    PXB_TRY(dev_upload(c, e.sc_bond, sc.data(), sizeof(double) * sc.size()));
+    return sync(c);
 }
 
 extern "C" int pxb_epf_set_constants(pxb_ctx *c, double C11, double C12, double C66, double rho) {

@@ -20,6 +20,7 @@ struct ShimState {
     int kind = 0;
     int n = 0, nnz = 0, nbtot = 0, nop = 0, ndof = 0, dim = 0;
     int precision = PXB_FP64;
+    const double *vh = nullptr;  // the caller's per-node horizon array of the resident structure (variable horizon)
 };
 
 ShimState g_shim;
@@ -69,10 +70,15 @@ bool qtable_matches(const perix_cuda::AssembleMesh &m, int order) {
     return k == m.nop;
 }
 
+// the mesh, and with a variable horizon (AssembleMesh::nodeHorizon / nodeSpacing, the reference's
+// PDMeshData::NodeHorizon / NodeSpacing) the per-node horizons the g-build uses
 bool upload_mesh(const perix_cuda::AssembleMesh &m, int order) {
     if (pxb_set_geometry(g_shim.ctx, m.N, m.dim, m.coords, m.vols, m.neigh_off, m.neigh_id, m.delta, m.dx_char,
                          nullptr, nullptr) != PXB_OK)
         return report("set_geometry");
+    if (m.nodeHorizon && pxb_set_node_horizons(g_shim.ctx, m.nodeHorizon, m.nodeSpacing) != PXB_OK)
+        return report("node horizons");
+    g_shim.vh = m.nodeHorizon;
     (void)order;
     return true;
 }
@@ -89,10 +95,6 @@ void shutdown() {
 bool assemble(const AssembleMesh &m, const ElmtParams &p, const OpSlots &s, const double *u, const double *uold,
               double *out_Kvals, double *out_rhs) {
     if (m.N <= 0 || p.ndof != 1 || s.dxx < 0 || s.dyy < 0) return false;
-    if (m.nodeHorizon) {
-        std::fprintf(stderr, "[perix_b200] assemble: variable horizon is not supported by this backend\n");
-        return false;
-    }
     if (!ensure_ctx()) return false;
     const int order = order_of(m);
     if (!qtable_matches(m, order)) {
@@ -100,7 +102,8 @@ bool assemble(const AssembleMesh &m, const ElmtParams &p, const OpSlots &s, cons
         return false;
     }
     const int nbtot = m.neigh_off[m.N];
-    if (g_shim.kind != 1 || g_shim.n != m.N || g_shim.nnz != m.nnz || g_shim.nbtot != nbtot || g_shim.nop != m.nop) {
+    if (g_shim.kind != 1 || g_shim.n != m.N || g_shim.nnz != m.nnz || g_shim.nbtot != nbtot || g_shim.nop != m.nop ||
+        g_shim.vh != m.nodeHorizon) {
         if (!upload_mesh(m, order)) return false;
         int ndeg = 0, first = 0;
         const int st = pxb_gbuild(g_shim.ctx, order, PXB_FP64, &ndeg, &first);
@@ -150,17 +153,14 @@ bool assembleStressCahnHilliard(const AssembleMesh &m, const StressCahnHilliardP
                                 double *out_Kvals, double *out_rhs) {
     (void)s;  // the operator slots are resolved from the multi-index table, which must be the reference's
     if (m.N <= 0 || (p.dim != 2 && p.dim != 3) || p.ndof != p.dim + 2 || !(p.dt > 0.0)) return false;
-    if (m.nodeHorizon) {
-        std::fprintf(stderr, "[perix_b200] assembleStressCahnHilliard: variable horizon is not supported\n");
-        return false;
-    }
     if (!ensure_ctx()) return false;
     if (order_of(m) != 2 || !qtable_matches(m, 2)) {
         std::fprintf(stderr, "[perix_b200] assembleStressCahnHilliard: needs the order-2 multi-index table\n");
         return false;
     }
     const int nbtot = m.neigh_off[m.N];
-    if (g_shim.kind != 4 || g_shim.n != m.N || g_shim.nnz != m.nnz || g_shim.nbtot != nbtot || g_shim.dim != p.dim) {
+    if (g_shim.kind != 4 || g_shim.n != m.N || g_shim.nnz != m.nnz || g_shim.nbtot != nbtot || g_shim.dim != p.dim ||
+        g_shim.vh != m.nodeHorizon) {
         if (!upload_mesh(m, 2)) return false;
         int ndeg = 0, first = 0;
         const int st = pxb_gbuild(g_shim.ctx, 2, PXB_FP64, &ndeg, &first);
@@ -190,17 +190,14 @@ bool assembleCached(const AssembleMesh &m, const CachedParams &p, const OpSlots 
                     double *out_rhs) {
     (void)s;  // the operator slots are resolved from the multi-index table, which must be the reference's
     if (m.N <= 0 || (p.dim != 2 && p.dim != 3) || p.ndof != p.dim || !(p.dt > 0.0)) return false;
-    if (m.nodeHorizon) {
-        std::fprintf(stderr, "[perix_b200] assembleCached: variable horizon is not supported\n");
-        return false;
-    }
     if (!ensure_ctx()) return false;
     if (order_of(m) != 2 || !qtable_matches(m, 2)) {
         std::fprintf(stderr, "[perix_b200] assembleCached: needs the order-2 multi-index table\n");
         return false;
     }
     const int nbtot = m.neigh_off[m.N];
-    if (g_shim.kind != 5 || g_shim.n != m.N || g_shim.nnz != m.nnz || g_shim.nbtot != nbtot || g_shim.dim != p.dim) {
+    if (g_shim.kind != 5 || g_shim.n != m.N || g_shim.nnz != m.nnz || g_shim.nbtot != nbtot || g_shim.dim != p.dim ||
+        g_shim.vh != m.nodeHorizon) {
         if (!upload_mesh(m, 2)) return false;
         int ndeg = 0, first = 0;
         const int st = pxb_gbuild(g_shim.ctx, 2, PXB_FP64, &ndeg, &first);
@@ -227,16 +224,16 @@ bool assembleExplicitPDDOFracAccel(const AssembleMesh &m, const ExplicitPDDOFrac
     (void)s;
     if (health_changed) *health_changed = 0;
     if (m.N <= 0 || (p.dim != 2 && p.dim != 3)) return false;
-    if (m.nodeHorizon) {
-        std::fprintf(stderr, "[perix_b200] assembleExplicitPDDOFracAccel: variable horizon is not supported\n");
-        return false;
-    }
     if (!ensure_ctx()) return false;
     const int nbtot = m.neigh_off[m.N];
-    if (g_shim.kind != 2 || g_shim.n != m.N || g_shim.nbtot != nbtot || g_shim.dim != p.dim) {
+    if (g_shim.kind != 2 || g_shim.n != m.N || g_shim.nbtot != nbtot || g_shim.dim != p.dim ||
+        g_shim.vh != m.nodeHorizon) {
         if (pxb_set_geometry(g_shim.ctx, m.N, p.dim, m.coords, m.vols, m.neigh_off, m.neigh_id, m.delta, m.dx_char,
                              nullptr, nullptr) != PXB_OK)
             return report("set_geometry");
+        if (m.nodeHorizon && pxb_set_node_horizons(g_shim.ctx, m.nodeHorizon, m.nodeSpacing) != PXB_OK)
+            return report("node horizons");
+        g_shim.vh = m.nodeHorizon;
         std::vector<uint8_t> h0((size_t)nbtot);
         for (int t = 0; t < nbtot; ++t) h0[(size_t)t] = health_inout[t] > 0.0 ? 1 : 0;
         const double b[3] = {p.bx, p.by, p.bz};
@@ -244,6 +241,10 @@ bool assembleExplicitPDDOFracAccel(const AssembleMesh &m, const ExplicitPDDOFrac
         const int prec = explicit_precision();
         if (pxb_epf_setup(g_shim.ctx, prec, p.C11, p.C12, p.C66, p.rho, b, sc, p.tension_only, h0.data()) != PXB_OK)
             return report("epf setup");
+        // variable horizon: each bond breaks at s_c(0.5 (delta_i + delta_j)) (ExplicitPDDOFracElement.cpp:254-261)
+        if (m.nodeHorizon && p.damage_on &&
+            pxb_epf_set_variable_horizon_stretch(g_shim.ctx, p.G0, p.E, p.plane_stress) != PXB_OK)
+            return report("variable-horizon stretch");
         // the per-step call's schedule, timed once per problem signature at this displacement (state unchanged)
         if (pxb_epf_autotune_rate(g_shim.ctx, u, 3, 1, nullptr, nullptr) != PXB_OK) return report("epf autotune");
         g_shim.precision = prec;

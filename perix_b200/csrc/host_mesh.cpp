@@ -208,10 +208,16 @@ struct CrackSet {
 // ---- families (reference src/PDMesh/CreatePDMesh.cpp:910-1082) ------------------------------------------------
 // Cells of size `radius` are opened in node order; each cell pairs its own members (a<b) and then the
 // members of the forward half of its neighbour cells (4 offsets in 2D, 13 in 3D); every accepted pair
-// appends j to i and i to j.  This reproduces the reference family order exactly.
-extern "C" int pxb_families(int n, const double *coords3, double radius, int is3d, int ncracks,
-                            const double *cracks, int nplanes, const double *planes, const int *mirror,
-                            int force_only, int *neigh_off, int *neigh_id, long long *nbtot) {
+// appends j to i and i to j.  This reproduces the reference family order exactly.  With per-node horizons
+// (node_h, the reference's VariableHorizon) the cells take the largest horizon and a pair is kept when
+// |x_i - x_j|^2 <= cut^2 (1 + 64 eps) with cut = max(delta_i, delta_j) (CreatePDMesh.cpp:932-938, 1043-1057).
+static int families_impl(int n, const double *coords3, double radius, const double *node_h, int is3d, int ncracks,
+                         const double *cracks, int nplanes, const double *planes, const int *mirror, int force_only,
+                         int *neigh_off, int *neigh_id, long long *nbtot) {
+    if (node_h) {
+        radius = 0.0;
+        for (int i = 0; i < n; ++i) radius = std::max(radius, node_h[i]);
+    }
     if (n < 0 || !coords3 || !neigh_off || !(radius > 0.0)) return pxb::fail(PXB_ERR_INVALID, "pxb_families: bad arguments");
     neigh_off[0] = 0;
     if (n == 0) { if (nbtot) *nbtot = 0; return PXB_OK; }
@@ -250,7 +256,13 @@ extern "C" int pxb_families(int n, const double *coords3, double radius, int is3
             const double *a = coords3 + 3 * (size_t)i, *b = coords3 + 3 * (size_t)j;
             const double dx = a[0] - b[0], dy = a[1] - b[1], dz = is3d ? (a[2] - b[2]) : 0.0;
             const double d2 = dx * dx + dy * dy + dz * dz;
-            if (!(d2 <= r2 + r2tol)) return;
+            if (node_h) {
+                const double cut = std::max(node_h[i], node_h[j]);
+                const double cut2 = cut * cut;
+                if (d2 > cut2 + 64.0 * std::numeric_limits<double>::epsilon() * cut2) return;
+            } else if (!(d2 <= r2 + r2tol)) {
+                return;
+            }
             if (cut && cs.cuts(i + 1, j + 1)) return;
             emit(i, j);
         };
@@ -282,6 +294,49 @@ extern "C" int pxb_families(int n, const double *coords3, double radius, int is3
         neigh_id[neigh_off[i] + cnt[(size_t)i]++] = j + 1;
         neigh_id[neigh_off[j] + cnt[(size_t)j]++] = i + 1;
     });
+    return PXB_OK;
+}
+
+extern "C" int pxb_families(int n, const double *coords3, double radius, int is3d, int ncracks,
+                            const double *cracks, int nplanes, const double *planes, const int *mirror,
+                            int force_only, int *neigh_off, int *neigh_id, long long *nbtot) {
+    return families_impl(n, coords3, radius, nullptr, is3d, ncracks, cracks, nplanes, planes, mirror, force_only,
+                         neigh_off, neigh_id, nbtot);
+}
+
+extern "C" int pxb_families_vh(int n, const double *coords3, const double *node_horizon, int is3d, int ncracks,
+                               const double *cracks, int nplanes, const double *planes, const int *mirror,
+                               int force_only, int *neigh_off, int *neigh_id, long long *nbtot) {
+    if (!node_horizon) return pxb::fail(PXB_ERR_INVALID, "pxb_families_vh: node_horizon is NULL");
+    return families_impl(n, coords3, 0.0, node_horizon, is3d, ncracks, cracks, nplanes, planes, mirror, force_only,
+                         neigh_off, neigh_id, nbtot);
+}
+
+// Per-node horizon and spacing (reference PDMesh::computeVariableHorizon, src/PDMesh/CreatePDMesh.cpp:828-905):
+// s_i = V_i^(1/dim); s_ref = the median (upper middle) of s_i over the bulk nodes with V_i > 0 (all such nodes when
+// no bulk node has one); delta_i = horizon (s_i / s_ref) and spacing_i = dx_char (s_i / s_ref), or the global
+// values where V_i <= 0.
+extern "C" int pxb_variable_horizon(int n, int dim, const double *vols, const int *mirror, double horizon,
+                                    double dx_char, double *node_delta, double *node_spacing) {
+    if (n <= 0 || (dim != 2 && dim != 3) || !vols || !node_delta || !(horizon > 0.0))
+        return pxb::fail(PXB_ERR_INVALID, "pxb_variable_horizon: bad arguments");
+    const double inv_dim = dim == 3 ? (1.0 / 3.0) : 0.5;
+    std::vector<double> s((size_t)n, 0.0), sb;
+    for (int i = 0; i < n; ++i) s[(size_t)i] = vols[i] > 0.0 ? std::pow(vols[i], inv_dim) : 0.0;
+    for (int i = 0; i < n; ++i)
+        if ((!mirror || mirror[i] == 0) && s[(size_t)i] > 0.0) sb.push_back(s[(size_t)i]);
+    if (sb.empty())
+        for (int i = 0; i < n; ++i)
+            if (s[(size_t)i] > 0.0) sb.push_back(s[(size_t)i]);
+    if (sb.empty()) return pxb::fail(PXB_ERR_INVALID, "pxb_variable_horizon: no positive node volume");
+    std::sort(sb.begin(), sb.end());
+    const double s_ref = sb[sb.size() / 2];
+    const double inv_ref = 1.0 / s_ref;
+    for (int i = 0; i < n; ++i) {
+        const double ratio = s[(size_t)i] > 0.0 ? s[(size_t)i] * inv_ref : 1.0;
+        node_delta[i] = horizon * ratio;
+        if (node_spacing) node_spacing[i] = dx_char * ratio;
+    }
     return PXB_OK;
 }
 

@@ -25,6 +25,17 @@ namespace pxb {
 namespace {
 
 // reference stretch s = (|xi+eta| - |xi|)/|xi| with the reference's operation order (no contraction)
+// critical stretch of bond t and its squared thresholds (1 +- s_c)^2: the element's uniform s_c, or with a variable
+// horizon the bond's own s_c(0.5 (delta_i + delta_j)) (ExplicitPDDOFracElement.cpp:239-266); s_c <= 0 never breaks
+struct BondStretch {
+    double sc, hi2, lo2;
+};
+__device__ __forceinline__ BondStretch bond_stretch(const EpfArgs &a, long long t) {
+    if (!a.sc_bond) return BondStretch{a.sc, a.sc_hi2, a.sc_lo2};
+    const double sc = a.sc_bond[t];
+    return BondStretch{sc, (1.0 + sc) * (1.0 + sc), sc < 1.0 ? (1.0 - sc) * (1.0 - sc) : 0.0};
+}
+
 __device__ __forceinline__ double ref_stretch(double y2, double r2) {
     const double r = sqrt(r2);
     return __ddiv_rn(__dsub_rn(sqrt(y2), r), r);
@@ -165,21 +176,22 @@ __global__ void __launch_bounds__(kEpfThreads) epf_kernel(EpfArgs a) {
 #pragma unroll
                         for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
                         const double r2 = dot_rn<DIM>(xv, xv);
-                        if (r2 > 0.0) {
+                        const BondStretch bs = bond_stretch(a, t0 + q * LPN + gl);
+                        if (r2 > 0.0 && bs.sc > 0.0) {
                             const double y2 = dot_rn<DIM>(yv, yv);
                             // fast squared test; the reference's own arithmetic decides bonds near threshold
                             const double band = 1.0e-6 * r2;
-                            const double qh = y2 - a.sc_hi2 * r2;
+                            const double qh = y2 - bs.hi2 * r2;
                             bool brk;
                             if (a.tension_only) {
                                 if (qh > band) brk = true;
                                 else if (qh < -band) brk = false;
-                                else brk = ref_stretch(y2, r2) > a.sc;
+                                else brk = ref_stretch(y2, r2) > bs.sc;
                             } else {
-                                const double ql = a.sc_lo2 * r2 - y2;
+                                const double ql = bs.lo2 * r2 - y2;
                                 if (qh > band || ql > band) brk = true;
                                 else if (qh < -band && ql < -band) brk = false;
-                                else brk = fabs(ref_stretch(y2, r2)) > a.sc;
+                                else brk = fabs(ref_stretch(y2, r2)) > bs.sc;
                             }
                             if (brk) {
                                 a.health[t0 + q * LPN + gl] = 0;
@@ -367,20 +379,21 @@ __global__ void __launch_bounds__(kEpfThreads) epf_stream_kernel(EpfArgs a) {
 #pragma unroll
                         for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[d]);
                         const double r2 = dot_rn<DIM>(xv, xv);
-                        if (r2 > 0.0) {
+                        const BondStretch bs = bond_stretch(a, t);
+                        if (r2 > 0.0 && bs.sc > 0.0) {
                             const double y2 = dot_rn<DIM>(yv, yv);
                             const double band = 1.0e-6 * r2;
-                            const double qh = y2 - a.sc_hi2 * r2;
+                            const double qh = y2 - bs.hi2 * r2;
                             bool brk;
                             if (a.tension_only) {
                                 if (qh > band) brk = true;
                                 else if (qh < -band) brk = false;
-                                else brk = ref_stretch(y2, r2) > a.sc;
+                                else brk = ref_stretch(y2, r2) > bs.sc;
                             } else {
-                                const double ql = a.sc_lo2 * r2 - y2;
+                                const double ql = bs.lo2 * r2 - y2;
                                 if (qh > band || ql > band) brk = true;
                                 else if (qh < -band && ql < -band) brk = false;
-                                else brk = fabs(ref_stretch(y2, r2)) > a.sc;
+                                else brk = fabs(ref_stretch(y2, r2)) > bs.sc;
                             }
                             if (brk) {
                                 a.health[t] = 0;
@@ -704,6 +717,7 @@ int epf_tma_maxb(int dim, int variant, int max_family) {
 }
 
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s) {
+    if (a.sc_bond && epf_is_tma(variant)) variant = 1;  // per-bond critical stretch: the lane-group kernels read it
     if (epf_is_tma(variant)) {
         if (mode == EPF_STEP) return launch_epf_tma(a, dim, mixed, variant - 5, s);
         if (mode == EPF_RATE && a.accel) {

@@ -164,6 +164,9 @@ struct EpfArgs {
     int var_step = 0;
     double cv_rho = 0, cv_w = 0;
     int wait_tries = 1 << 19;  // TMA variants: try_wait calls a consumer wait may make before it gives up
+    // variable horizon: per-bond critical stretch [nb] (null: sc for every bond); the staged kernels do not read
+    // it, launch_epf runs the lane-group kernel instead
+    const double *sc_bond = nullptr;
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
 constexpr int kEpfTmaConfigs = 13;                // staged (TMA) configurations per dimension

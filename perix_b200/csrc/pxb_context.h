@@ -75,6 +75,8 @@ struct Geometry {
     DevBuf mirror;  // int32 [n], 1-based mirror bulk, 0 none (may be empty)
     DevBuf layer;   // int32 [n] ghost layer index (may be empty)
     DevBuf rev;     // int32 [nb] reverse bond index (built lazily)
+    DevBuf node_delta, node_dxc;     // double [n] per-node horizon and spacing (variable horizon; empty: global)
+    std::vector<double> h_node_delta;
     int max_family = 0;
     std::vector<int> h_off, h_mirror;
 };
@@ -117,6 +119,7 @@ struct EpfState {
     DevBuf G;          // SoA Navier operators [c][ldb], double or float (c = 3 in 2D, 6 in 3D)
     DevBuf P;          // SoA packed Navier coefficients [c][ldb] (same type): the staged step kernels' stream
     DevBuf xib;        // mixed: FP32 reference bond vectors [dim][ldb] (the staged kernels' stretch pre-test)
+    DevBuf sc_bond;    // variable horizon: per-bond critical stretch s_c(0.5 (delta_i + delta_j)) [ldb]
     DevBuf health;     // uint8 [ldb] (zero tail)
     DevBuf u[2];       // double [n*dim + 8] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
     DevBuf accel;      // double [n*dim]

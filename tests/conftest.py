@@ -64,3 +64,26 @@ def scaled_err(a, b, off):
     if (~mask).any():
         worst = max(worst, float(d[~mask].max()))
     return worst
+
+
+def graded_cloud(dim, n=(24, 16, 8), h0=1e-3, grade=0.6, jitter=0.1, seed=4):
+    """A point cloud whose spacing grows by `grade` across x (cell-centred columns of width h0 (1 + grade x/Lx)),
+    uniform h0 in y (and z), jittered by U(+-jitter h) per coordinate; volumes are the local cell sizes.  Its
+    volumes vary smoothly, so a variable horizon (delta_i ~ V_i^(1/dim)) differs from node to node."""
+    rng = np.random.default_rng(seed)
+    nx = n[0]
+    w = h0 * (1.0 + grade * (np.arange(nx) + 0.5) / nx)
+    xc = np.cumsum(w) - 0.5 * w
+    axes = [np.arange(k) for k in n[1:dim]]
+    grid = np.meshgrid(np.arange(nx), *axes, indexing="ij")
+    idx = np.stack([g.reshape(-1) for g in grid], -1)
+    xyz = np.zeros((idx.shape[0], 3))
+    xyz[:, 0] = xc[idx[:, 0]]
+    for a in range(1, dim):
+        xyz[:, a] = (idx[:, a] + 0.5) * h0
+    hx = w[idx[:, 0]]
+    xyz[:, 0] += rng.uniform(-jitter, jitter, idx.shape[0]) * hx
+    for a in range(1, dim):
+        xyz[:, a] += rng.uniform(-jitter, jitter, idx.shape[0]) * h0
+    vols = hx * h0 ** (dim - 1)
+    return xyz, vols
