@@ -250,6 +250,17 @@ int pxb_epf_broken_count(pxb_ctx *ctx, long long *n_broken);
  * health mask is held fixed (no damage update). Device-pointer variant for torch. */
 int pxb_epf_force_adjoint(pxb_ctx *ctx, const double *u, const double *abar, double *ubar, double *dC);
 int pxb_epf_force_adjoint_d(pxb_ctx *ctx, const double *u_d, const double *abar_d, double *ubar_d, double *dC_d);
+/* Adjoint of the explicit loop with the damage mask frozen at the current health (device pointers, N*dim each):
+ * the forward is the loop of pxb_epf_start + pxb_epf_advance from (u0, v0) (v0 may be NULL) over nsteps steps of dt,
+ * with the context's BC program after every step and no bond breaking.  Given ubar_N = dJ/du^N and ubar_Nm1 =
+ * dJ/du^{N-1} (may be NULL: 0), returns u0bar = dJ/du0, v0bar = dJ/dv0 (may be NULL) and dC = dJ/d(C11, C12, C66)
+ * (3 doubles, may be NULL).  The reverse sweep runs on the device: per step the transpose of the BC pass, then one
+ * kernel for the bond-force adjoint (reverse-bond gather) fused with the central difference's transpose.  The forward
+ * states it needs are recomputed from checkpoints kept every checkpoint_every steps (<= 0: one segment, all states
+ * kept: nsteps * N * dim doubles).  Leaves the context's explicit state unchanged.  No counterpart in the reference. */
+int pxb_epf_adjoint_d(pxb_ctx *ctx, const double *u0_d, const double *v0_d, double dt, int nsteps, int checkpoint_every,
+                      const double *ubar_N_d, const double *ubar_Nm1_d, double *u0bar_d, double *v0bar_d,
+                      double *dC_d);
 /* Force (rate) with a frozen mask, device pointers, no damage update: a = (L(u)+b)/rho. */
 int pxb_epf_force_frozen_d(pxb_ctx *ctx, const double *u_d, double *a_d);
 /* Replaces C11, C12, C66 and rho of the explicit element without rebuilding the g-functions (the packed

@@ -10,6 +10,10 @@
   NeumannBC.cpp:88-105), written in torch around ``frozen_force``.  Segments of ``checkpoint_every`` steps are
   wrapped in torch.utils.checkpoint, so the backward pass keeps one state per segment and recomputes the
   steps inside a segment.
+- ``explicit_run(ctx, u0, v0, C, dt, nsteps)``: the same loop run entirely on the device (the context's fused
+  step kernels and its BC program); its backward is the device adjoint ``pxb_epf_adjoint_d`` (per step the BC
+  transpose and one fused bond-force / central-difference adjoint kernel, forward states recomputed from
+  checkpoints), which returns dJ/du0, dJ/dv0 and dJ/dC.
 - ``elastic_constants_t``: C11, C12, C66 as torch functions of E and nu (ExplicitPDDOFracElement.cpp:38-53).
 - ``ch_free_energy(ctx, c0, kappa, ...)``: the total free energy after a backward-Euler Cahn-Hilliard run on the
   device (CahnHilliardElement.cpp:66-292 per step); its backward is the discrete adjoint of the run
@@ -114,9 +118,12 @@ class BcPlan:
             comps = [int(c) for c in bc.comps]
             if bc.kind == "dirichlet":
                 if bc.box is not None:
-                    box = np.asarray(bc.box, np.float64)
+                    # DirichletBC::insideBox: all three axes, an axis with min > max unconstrained
+                    box = np.asarray(list(bc.box) + [0.0] * (6 - len(bc.box)), np.float64)
                     inside = np.ones(ids.size, bool)
-                    for a in range(dim):
+                    for a in range(3):
+                        if box[2 * a] > box[2 * a + 1]:
+                            continue
                         x = xyz[ids - 1, a]
                         inside &= (x >= box[2 * a]) & (x <= box[2 * a + 1])
                     ids = ids[inside]
@@ -196,6 +203,50 @@ def explicit_loop(pctx, u0, v0, dt, nsteps, C, plan, checkpoint_every=100, t0=0.
             u, uold = _segment(pctx, C, plan, dt2, times, force, u, uold)
         done += k
     return u, uold
+
+
+class _ExplicitRun(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, u0, C, v0, pctx, dt, nsteps, checkpoint_every):
+        u0c = _f64c(u0)
+        v0c = None if v0 is None else _f64c(v0)
+        pctx.set_stream(0)
+        torch.cuda.current_stream(u0c.device).synchronize()
+        pctx.epf_start(u0c.cpu().numpy(), None if v0c is None else v0c.cpu().numpy(), dt)
+        pctx.epf_advance(nsteps)
+        uN, uNm1, _, _ = pctx.epf_state()
+        fctx.save_for_backward(u0c, *(() if v0c is None else (v0c,)))
+        fctx.pctx, fctx.dt, fctx.nsteps, fctx.ck, fctx.has_v0 = pctx, dt, nsteps, checkpoint_every, v0c is not None
+        return (torch.from_numpy(uN).to(u0c.device), torch.from_numpy(uNm1).to(u0c.device))
+
+    @staticmethod
+    def backward(fctx, gN, gNm1):
+        import ctypes as Ct
+        saved = fctx.saved_tensors
+        u0 = saved[0]
+        v0 = saved[1] if fctx.has_v0 else None
+        gN = torch.zeros_like(u0) if gN is None else _f64c(gN)
+        gNm1 = None if gNm1 is None else _f64c(gNm1)
+        u0bar = torch.empty_like(u0)
+        v0bar = torch.empty_like(u0)
+        dC = torch.zeros(3, dtype=torch.float64, device=u0.device)
+        _on_stream(fctx.pctx, u0)
+        p = lambda t: None if t is None else Ct.c_void_p(t.data_ptr())  # noqa: E731
+        st = fctx.pctx.L.pxb_epf_adjoint_d(fctx.pctx.h, p(u0), p(v0), Ct.c_double(fctx.dt), int(fctx.nsteps),
+                                           int(fctx.ck), p(gN), p(gNm1), p(u0bar), p(v0bar), p(dC))
+        if st:
+            from .api import PxbError
+            raise PxbError(st, fctx.pctx.L.pxb_last_error().decode(errors="replace"))
+        return u0bar, dC, (v0bar if fctx.has_v0 else None), None, None, None, None
+
+
+def explicit_run(pctx, u0, v0, C, dt, nsteps, checkpoint_every=0):
+    """(u^N, u^{N-1}) of nsteps central-difference steps from (u0, v0) run on the device (pxb_epf_start +
+    pxb_epf_advance with the context's BC program), differentiable in u0, v0 and C through the device adjoint
+    (pxb_epf_adjoint_d).  The damage mask must be frozen: set the context up with sc = 0 (its current health is the
+    mask), and its constants equal to C (``set_constants``).  checkpoint_every > 0 keeps a state every that many steps
+    and recomputes the others in the backward pass; 0 keeps them all (nsteps * N * dim doubles on the device)."""
+    return _ExplicitRun.apply(u0, C, v0, pctx, float(dt), int(nsteps), int(checkpoint_every))
 
 
 def set_constants(pctx, C, rho):

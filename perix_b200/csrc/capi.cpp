@@ -1434,6 +1434,164 @@ extern "C" int pxb_epf_force_adjoint_d(pxb_ctx *c, const double *u_d, const doub
     return check_launch(c, "epf adjoint");
 }
 
+// ---- adjoint of the explicit loop with a frozen damage mask ------------------------------------------------------
+// Forward (the reference loop, TimeStepping.cpp:479-536, with the context's BC program after every step):
+//   u^{-1} = u0 - dt v0 + dt^2/2 a(u0),  w^n = 2u^n - u^{n-1} + dt^2 a(u^n),  u^{n+1} = P w^n + g(t_{n+1}),
+// a(u) = (L(C) u + b)/rho linear in u for a fixed health mask.  Reverse, with A = dJ/du^{n+1} and R = the part of
+// dJ/du^n carried from step n+1 (where u^n is the previous state):
+//   W = P^T A;  A <- R + 2 W + (da/du)^T (dt^2 W);  R <- -W;  dJ/dC += (da/dC(u^n))^T (dt^2 W)
+// and at the start  dJ/du0 = A + R + (da/du)^T (dt^2/2 R),  dJ/dv0 = -dt R,  dJ/dC += (da/dC(u0))^T (dt^2/2 R).
+// The forward states for dJ/dC come from checkpoints every `checkpoint_every` steps, recomputed segment by segment.
+namespace {
+
+// one STEP launch of the forward loop on explicit buffers: reads cur (u^n) and other (u^{n-1}), writes u^{n+1}
+// into other; the BC pass at t_sched[q]; damage off (frozen mask)
+int adj_step(pxb_ctx *c, double *cur, double *other, const double *tsched, int q, double dt) {
+    EpfState &e = c->epf;
+    EpfArgs a;
+    PXB_TRY(step_args(c, 0, &a));
+    a.dt = dt;
+    a.dt2 = dt * dt;
+    a.u = cur;
+    a.u_other = other;
+    a.t_sched = tsched;
+    a.step_in_chunk = q;
+    a.umax = e.adj_umax.as<unsigned long long>();
+    a.damage = 0;
+    a.sc_bond = nullptr;
+    a.pdl = 0;
+    const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_STEP, e.variant, c->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "adjoint forward step");
+    c->launches++;
+    return PXB_OK;
+}
+
+int adj_kernel(pxb_ctx *c, const double *u, const double *w, double scale, double c_r, const double *rin, double c_w,
+               double *ubar, double c_o, double *rout) {
+    const EpfState &e = c->epf;
+    EpfAdjArgs a;
+    a.n = c->g.n;
+    a.nb = c->g.ldb;
+    a.off = c->g.off.as<int>();
+    a.nbr = c->g.nbr.as<int>();
+    a.rev = c->g.rev.as<int>();
+    a.G = e.G.p;
+    a.health = e.health.as<uint8_t>();
+    a.C11 = e.C11;
+    a.C12 = e.C12;
+    a.C66 = e.C66;
+    a.inv_rho = 1.0 / e.rho;
+    a.u = u;
+    a.abar = w;
+    a.ubar = ubar;
+    a.dC = e.adj_dC.as<double>();
+    a.step = 1;
+    a.scale = scale;
+    a.c_r = c_r;
+    a.rin = rin;
+    a.c_w = c_w;
+    a.c_o = c_o;
+    a.rout = rout;
+    launch_epf_adjoint(a, c->g.dim, e.precision == PXB_MIXED, epf_grid(c->g.n, c->g.dim, 0), c->stream);
+    return check_launch(c, "epf adjoint step");
+}
+
+}  // namespace
+
+extern "C" int pxb_epf_adjoint_d(pxb_ctx *c, const double *u0_d, const double *v0_d, double dt, int nsteps,
+                                 int checkpoint_every, const double *ubar_N_d, const double *ubar_Nm1_d,
+                                 double *u0bar_d, double *v0bar_d, double *dC_d) {
+    PXB_TRY(need_epf(c, "pxb_epf_adjoint_d"));
+    if (!u0_d || !ubar_N_d || !u0bar_d || !(dt > 0.0) || nsteps < 0)
+        return fail(PXB_ERR_INVALID, "pxb_epf_adjoint_d: need u0, dJ/du^N, the dJ/du0 output, dt > 0, nsteps >= 0");
+    PXB_TRY(ensure_rev(c));
+    EpfState &e = c->epf;
+    const size_t nd = (size_t)c->g.n * c->g.dim, bytes = sizeof(double) * nd;
+    const int K = (checkpoint_every <= 0 || checkpoint_every > nsteps) ? std::max(nsteps, 1) : checkpoint_every;
+    const int nseg = nsteps > 0 ? (nsteps + K - 1) / K : 0;
+    PXB_TRY(dev_alloc(c, e.adj_ckpt, 2 * bytes * (size_t)std::max(nseg, 1)));
+    PXB_TRY(dev_alloc(c, e.adj_seg, bytes * (size_t)K));
+    for (int k = 0; k < 2; ++k) PXB_TRY(dev_alloc(c, e.adj_p[k], bytes + 64));
+    PXB_TRY(dev_alloc(c, e.adj_A, bytes));
+    PXB_TRY(dev_alloc(c, e.adj_R, bytes));
+    PXB_TRY(dev_alloc(c, e.adj_W, bytes));
+    PXB_TRY(dev_alloc(c, e.adj_t, sizeof(double) * (size_t)std::max(nsteps, 1)));
+    PXB_TRY(dev_alloc(c, e.adj_dC, 4 * sizeof(double)));
+    PXB_TRY(dev_alloc(c, e.adj_umax, sizeof(unsigned long long) * (size_t)std::max(nsteps, 1)));
+    PXB_CUDA_TRY(cudaMemsetAsync(e.adj_dC.p, 0, 4 * sizeof(double), c->stream));
+    // step times t_{n+1}, accumulated as the forward loop does
+    std::vector<double> th((size_t)std::max(nsteps, 1));
+    double t = 0.0;
+    for (int s = 0; s < nsteps; ++s) { t = t + dt; th[(size_t)s] = t; }
+    PXB_TRY(h2d(c, e.adj_t.p, th.data(), sizeof(double) * th.size()));
+    const double *tdev = e.adj_t.as<double>();
+    double *P[2] = {e.adj_p[0].as<double>(), e.adj_p[1].as<double>()};
+    double *ck = e.adj_ckpt.as<double>();
+    auto d2d = [&](void *dst, const void *src, size_t b) -> int {
+        PXB_CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToDevice, c->stream));
+        return PXB_OK;
+    };
+    // start: u^{-1} = u0 - dt v0 + dt^2/2 a(u0) with the frozen mask (the START mode of the lane-group kernel)
+    {
+        EpfArgs a = epf_args(c);
+        a.u = u0_d;
+        a.u_other = P[1];
+        a.v0 = v0_d;
+        a.dt = dt;
+        a.dt2 = 0.5 * dt * dt;
+        a.damage = 0;
+        a.sc_bond = nullptr;
+        const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_START, 1, c->stream);
+        if (err != cudaSuccess) return cuda_fail(err, "adjoint start");
+        c->launches++;
+        PXB_TRY(d2d(P[0], u0_d, bytes));
+    }
+    // sweep 1: the forward loop, keeping (u^{sK}, u^{sK-1}) at the start of every segment
+    int cur = 0;
+    for (int s = 0; s < nseg; ++s) {
+        PXB_TRY(d2d(ck + (size_t)(2 * s) * nd, P[cur], bytes));
+        PXB_TRY(d2d(ck + (size_t)(2 * s + 1) * nd, P[cur ^ 1], bytes));
+        if (s == nseg - 1) break;  // the last segment is recomputed in the reverse sweep anyway
+        for (int q = s * K; q < (s + 1) * K; ++q) {
+            PXB_TRY(adj_step(c, P[cur], P[cur ^ 1], tdev, q, dt));
+            cur ^= 1;
+        }
+    }
+    // reverse sweep
+    double *A = e.adj_A.as<double>(), *Rv = e.adj_R.as<double>(), *W = e.adj_W.as<double>();
+    double *seg = e.adj_seg.as<double>();
+    PXB_TRY(d2d(A, ubar_N_d, bytes));
+    if (ubar_Nm1_d) PXB_TRY(d2d(Rv, ubar_Nm1_d, bytes));
+    else PXB_CUDA_TRY(cudaMemsetAsync(Rv, 0, bytes, c->stream));
+    EpfArgs bc = epf_args(c);
+    fill_bc(c, bc);
+    const double dt2 = dt * dt;
+    for (int s = nseg - 1; s >= 0; --s) {
+        const int q0 = s * K, q1 = std::min(nsteps, (s + 1) * K);
+        // recompute the segment's states u^{q0} .. u^{q1-1}
+        PXB_TRY(d2d(P[0], ck + (size_t)(2 * s) * nd, bytes));
+        PXB_TRY(d2d(P[1], ck + (size_t)(2 * s + 1) * nd, bytes));
+        cur = 0;
+        for (int q = q0; q < q1; ++q) {
+            PXB_TRY(d2d(seg + (size_t)(q - q0) * nd, P[cur], bytes));
+            if (q + 1 < q1) {
+                PXB_TRY(adj_step(c, P[cur], P[cur ^ 1], tdev, q, dt));
+                cur ^= 1;
+            }
+        }
+        for (int q = q1 - 1; q >= q0; --q) {
+            const cudaError_t err = launch_bc_transpose(bc, c->g.n, c->g.dim, A, W, c->stream);
+            if (err != cudaSuccess) return cuda_fail(err, "bc transpose");
+            c->launches++;
+            PXB_TRY(adj_kernel(c, seg + (size_t)(q - q0) * nd, W, dt2, 1.0, Rv, 2.0, A, -1.0, Rv));
+        }
+    }
+    // the start: dJ/du0 = A + R + (da/du)^T (dt^2/2 R), dJ/dv0 = -dt R
+    PXB_TRY(adj_kernel(c, u0_d, Rv, 0.5 * dt2, 1.0, A, 1.0, u0bar_d, -dt, v0bar_d));
+    if (dC_d) PXB_TRY(d2d(dC_d, e.adj_dC.p, 3 * sizeof(double)));
+    return PXB_OK;
+}
+
 extern "C" int pxb_epf_force_adjoint(pxb_ctx *c, const double *u, const double *abar, double *ubar, double *dC) {
     PXB_TRY(need_epf(c, "pxb_epf_force_adjoint"));
     if (!u || !abar || !ubar) return fail(PXB_ERR_INVALID, "pxb_epf_force_adjoint: NULL buffer");

@@ -496,9 +496,10 @@ __global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) 
     double dC[3] = {0.0, 0.0, 0.0};
     for (int m = blockIdx.x * WPB + wib; m < a.n; m += gridDim.x * WPB) {
         double Lm[DIM], um[DIM], U[DIM];
+        const double lscale = a.scale * a.inv_rho;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
-            Lm[d] = a.abar[(size_t)m * DIM + d] * a.inv_rho;
+            Lm[d] = a.abar[(size_t)m * DIM + d] * lscale;
             um[d] = a.u[(size_t)m * DIM + d];
             U[d] = 0.0;
         }
@@ -509,7 +510,7 @@ __global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) 
             if (r >= 0 && a.health[r]) {
                 double Lj[DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) Lj[d] = a.abar[(size_t)j * DIM + d] * a.inv_rho;
+                for (int d = 0; d < DIM; ++d) Lj[d] = a.abar[(size_t)j * DIM + d] * lscale;
                 load_G<DIM, MIXED>(a.G, a.nb, r, g);
                 navier_apply<DIM>(g, a.C11, a.C12, a.C66, Lj, f);
 #pragma unroll
@@ -541,7 +542,17 @@ __global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) 
         }
 #pragma unroll
         for (int d = 0; d < DIM; ++d) U[d] = group_sum<kWarp>(U[d]);
-        if (lane < DIM) a.ubar[(size_t)m * DIM + lane] = pick<DIM>(U, lane);
+        if (lane < DIM) {
+            const size_t k = (size_t)m * DIM + lane;
+            if (a.step) {
+                const double w = a.abar[k];
+                const double r = a.rin ? a.rin[k] : 0.0;
+                if (a.rout) a.rout[k] = a.c_o * w;
+                a.ubar[k] = a.c_r * r + a.c_w * w + pick<DIM>(U, lane);
+            } else {
+                a.ubar[k] = pick<DIM>(U, lane);
+            }
+        }
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) dC[k] = group_sum<kWarp>(dC[k]);
@@ -552,6 +563,40 @@ __global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) 
         for (int w = 0; w < WPB; ++w) v += s_dC[w][threadIdx.x];
         atomicAdd(a.dC + threadIdx.x, v);
     }
+}
+
+// ---- transpose of the BC program (the adjoint of a step's BC pass) --------------------------------------------
+// The forward pass sets u^{n+1}[target] = coef w[src] + const per entry (form 0: coef +1, form 2: -1, forms 1 and 3:
+// constants) and keeps w elsewhere; entries are grouped by the node that executes them, which for forms 0 and 2 is
+// the source, so the transpose is a gather without atomics: thread per node.
+template <int DIM>
+__global__ void bc_transpose_kernel(EpfArgs b, int n, const double *a, double *w) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned own = b.bc_own ? b.bc_own[i] : 0u;
+        double v[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) v[d] = ((own >> d) & 1u) ? 0.0 : a[(size_t)i * DIM + d];
+        if (b.bc_off) {
+            for (int e = b.bc_off[i]; e < b.bc_off[i + 1]; ++e) {
+                const int form = b.bc_form[e];
+                if (form != 0 && form != 2) continue;
+                const int comp = b.bc_comp[e];
+                const double x = a[(size_t)b.bc_tgt[e] * DIM + comp];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d)
+                    if (d == comp) v[d] += form == 0 ? x : -x;
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) w[(size_t)i * DIM + d] = v[d];
+    }
+}
+
+cudaError_t launch_bc_transpose(const EpfArgs &bc, int n, int dim, const double *a, double *w, cudaStream_t s) {
+    const int grid = (int)std::min<long long>(((long long)n + 255) / 256, 148LL * 16);
+    if (dim == 3) bc_transpose_kernel<3><<<grid > 0 ? grid : 1, 256, 0, s>>>(bc, n, a, w);
+    else bc_transpose_kernel<2><<<grid > 0 ? grid : 1, 256, 0, s>>>(bc, n, a, w);
+    return cudaGetLastError();
 }
 
 // ---- packed Navier coefficients for the staged step kernels ----------------------------------------------

@@ -213,8 +213,17 @@ struct EpfAdjArgs {
     const double *abar = nullptr;
     double *ubar = nullptr;
     double *dC = nullptr;  // 3 doubles, atomically accumulated (must be zeroed)
+    // reverse time step (step != 0): Lbar = scale abar / rho, and per node
+    //   ubar = c_r rin + c_w abar + (da/du)^T (scale abar),   rout = c_o abar   (rin / rout may alias, per node)
+    int step = 0;
+    double scale = 1.0, c_r = 0.0, c_w = 0.0, c_o = 0.0;
+    const double *rin = nullptr;
+    double *rout = nullptr;
 };
 cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int grid, cudaStream_t s);
+// transpose of the BC program's linear part: w[i] = (component owned by the BC pass ? 0 : a[i]) + sum over the
+// entries executed by node i of +-a[target] (form 0: +, form 2: -, constants: none)
+cudaError_t launch_bc_transpose(const EpfArgs &bc, int n, int dim, const double *a, double *w, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- apply
 struct ApplyArgs {

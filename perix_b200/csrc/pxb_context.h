@@ -120,6 +120,9 @@ struct EpfState {
     DevBuf P;          // SoA packed Navier coefficients [c][ldb] (same type): the staged step kernels' stream
     DevBuf xib;        // mixed: FP32 reference bond vectors [dim][ldb] (the staged kernels' stretch pre-test)
     DevBuf sc_bond;    // variable horizon: per-bond critical stretch s_c(0.5 (delta_i + delta_j)) [ldb]
+    // explicit-loop adjoint (pxb_epf_adjoint_d): checkpoints, a segment's states, the two ping-pong states, the
+    // adjoint vectors A (dJ/du^n), R (dJ/du^{n-1} carried), W (BC-transposed A), step times, dC accumulator
+    DevBuf adj_ckpt, adj_seg, adj_p[2], adj_A, adj_R, adj_W, adj_t, adj_dC, adj_umax;
     DevBuf health;     // uint8 [ldb] (zero tail)
     DevBuf u[2];       // double [n*dim + 8] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
     DevBuf accel;      // double [n*dim]
