@@ -739,7 +739,7 @@ extern "C" int pxb_epf_setup(pxb_ctx *c, int precision, double C11, double C12, 
     PXB_CUDA_TRY(launch_navier_pack(e.G.p, e.P.p, (long long)ldb, g.dim, precision == PXB_MIXED, C11, C12, C66,
                                     c->stream));
     PXB_TRY(check_launch(c, "navier pack"));
-    if (precision == PXB_MIXED) {
+    {  // the staged kernels' FP32 bond vectors (the stretch pre-test of the configurations that stage them)
         PXB_TRY(dev_alloc(c, e.xib, sizeof(float) * (size_t)g.dim * ldb));
         PXB_CUDA_TRY(cudaMemsetAsync(e.xib.p, 0, e.xib.bytes, c->stream));
         PXB_CUDA_TRY(launch_bond_vectors(g.n, g.dim, g.off.as<int>(), g.nbr.as<int>(), g.pos.p, (long long)ldb,
@@ -750,7 +750,7 @@ extern "C" int pxb_epf_setup(pxb_ctx *c, int precision, double C11, double C12, 
     // stay resident; streams that fit are left to stay in L2 from one step to the next.
     int l2 = 0;
     PXB_CUDA_TRY(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, c->device));
-    const size_t stream_bytes = ldb * (es * nc + 5 + (precision == PXB_MIXED ? 4 * (size_t)g.dim : 0));
+    const size_t stream_bytes = ldb * (es * nc + 5 + 4 * (size_t)g.dim);
     e.evict_first = stream_bytes > (size_t)l2;
     e.ready = true;
     return PXB_OK;

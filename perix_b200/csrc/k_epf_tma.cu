@@ -149,7 +149,7 @@ struct StageLayout {
         return up_off(maxb) + (((unsigned)(NT * DIM + 2) * 8u + 15u) & ~15u);
     }
     __host__ __device__ static unsigned bytes(int maxb) {
-        return xi_off(maxb) + ((MIXED && XI) ? (unsigned)(DIM * maxb) * 4u : 0u);
+        return xi_off(maxb) + (XI ? (unsigned)(DIM * maxb) * 4u : 0u);
     }
 };
 
@@ -184,7 +184,7 @@ __device__ __forceinline__ int break_fp64(const PosT &xj, const PosT &xi, const 
 
 template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB, bool XI>
 __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
-    constexpr bool XS = MIXED && XI;  // staged FP32 bond vectors and the FP32 stretch pre-test
+    constexpr bool XS = XI;  // staged FP32 bond vectors and the FP32 stretch pre-test (both precisions)
     using PosT = typename Vec<DIM>::T;
     using GT = typename std::conditional<MIXED, float, double>::type;
     constexpr int GPW = kWarp / LPN;
@@ -574,8 +574,8 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
 }
 
 // Staged configurations: lanes per node, bonds per lane per pass, stages, minimum resident blocks (launch
-// bounds), warps per block, staged FP32 bond vectors (mixed only: the stretch pre-test reads them instead of
-// gathering neighbour positions, for 4 (2D) / 12 (3D) more staged bytes per bond).  A tile is WPB * 32/LPN nodes.
+// bounds), warps per block, staged FP32 bond vectors (either precision: the stretch pre-test reads them instead of
+// gathering neighbour positions, for 8 (2D) / 12 (3D) more staged bytes per bond).  A tile is WPB * 32/LPN nodes.
 struct TmaCfg {
     int lpn, unr, stages, minb, wpb, xi;
 };
