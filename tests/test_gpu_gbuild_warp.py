@@ -101,3 +101,21 @@ def test_degenerate_family_reported_by_both_schedules(ctx, dim, schedule):
         assert np.all(g[off2[bad]:off2[bad + 1]] == 0.0)
     finally:
         ctx.gbuild_set_schedule(-1)
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference harness not built")
+@pytest.mark.parametrize("dim,order", [(2, 3), (2, 4), (3, 3)])
+def test_higher_order_poisson_assembly_matches_reference(ctx, dim, order):
+    """Poisson K and rhs (PDSystem::formResidualAndJacobian with a PoissonElement) from operators of order 3 and 4,
+    the Laplacian slots resolved from the multi-index table."""
+    m = _ref_mesh(dim, order, "lattice")
+    rng = np.random.default_rng(60 + dim + order)
+    u = rng.standard_normal(m.n)
+    kv_ref, rhs_ref, _ = m.system_assemble(0, 1.3, 0.7, u)
+    ctx.set_geometry(m.coords, m.vols, m.off, m.ids, m.delta, m.dx_char, dim, mirror=m.mirror)
+    ctx.gbuild(order, 0, allow_degenerate=True)
+    rowptr, cols = m.csr_pattern(1)
+    ctx.csr_set_pattern(rowptr, cols, 1)
+    kv, rhs = ctx.assemble_scalar(0, 1.3, u, f=0.7)
+    assert np.abs(kv - kv_ref).max() <= 1e-12 * np.abs(kv_ref).max()
+    assert np.abs(rhs - rhs_ref).max() <= 1e-12 * np.abs(rhs_ref).max()

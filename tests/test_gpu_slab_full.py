@@ -5,7 +5,7 @@ with the harness's central difference).
 
 * Families built on the device (pxb_set_geometry_points) equal the reference's createNeighborNodes at full size.
 * Eight explicit steps from a seeded random field (std 1 um against a 4 um critical extension of the shortest
-  bonds, so tens of thousands of bonds break) on several step schedules: FP64 with identical damage sets and u within
+  bonds, so thousands of bonds break) on several step schedules: FP64 with identical damage sets and u within
   1e-10 of its magnitude; mixed within 1e-6 with damage sets identical but for bonds at the threshold."""
 import math
 
@@ -76,7 +76,7 @@ def _run(ctx, s, variant, precision):
 @pytest.mark.parametrize("variant", [1, 5, 7, 11, 12, 17])
 def test_slab_fp64_steps_match_reference(ctx, slab, variant):
     u, uo, h, _ = _run(ctx, slab, variant, 0)
-    assert (slab["h"] == 0).sum() > (slab["health0"] == 0).sum() + 10000
+    assert (slab["h"] == 0).sum() > (slab["health0"] == 0).sum() + 1000
     assert np.array_equal(h, slab["h"])
     scale = np.abs(slab["u"]).max()
     assert np.abs(u - slab["u"]).max() <= 1e-10 * scale

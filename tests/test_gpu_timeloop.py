@@ -74,14 +74,17 @@ def test_clamped_last_step_differs_from_a_uniform_one(ctx):
     dt = float(d["dt"])
     rng = np.random.default_rng(3)
     u0 = rng.standard_normal(2 * m.n) * 1e-6
+    # each run from a fresh element (the damage a run commits stays in the context's health)
     _device(ctx, m, d, k, bcs, health0, 1, k["sc"])
     ctx.epf_start(u0, None, dt)
     ctx.epf_advance_to(dt * 37.37)
     u_var = ctx.epf_state()[0]
+    _device(ctx, m, d, k, bcs, health0, 1, k["sc"])
     ctx.epf_start(u0, None, dt)
     ctx.epf_advance(37)
     ctx.epf_advance_to(dt * 37.37)  # the same clamped step after 37 uniform ones: identical
     assert np.array_equal(ctx.epf_state()[0], u_var)
+    _device(ctx, m, d, k, bcs, health0, 1, k["sc"])
     ctx.epf_start(u0, None, dt)
     ctx.epf_advance(38)
     assert np.abs(ctx.epf_state()[0] - u_var).max() > 1e-6 * np.abs(u_var).max()
