@@ -595,10 +595,81 @@ def reference_gpu():
         d.pop("profile", None)
         d["what"] = ("perix_cuda::assembleExplicitPDDOFracAccel from the reference's CudaAssembleKernels.cu built for "
                      "sm_100a: call = H2D u + force kernel + D2H accel per step; force kernel alone with CUDA events, "
-                     "L2 flushed; opbuild = its one-off operator build")
+                     "L2 flushed; opbuild = its one-off operator build; assembly: perix_cuda::assemble (Poisson) "
+                     "with its opsBuildKernel and assembleKernel timed alone beside this backend's g-build and "
+                     "assembly on the same mesh")
         return d
     except Exception as e:  # noqa: BLE001
         return {"unavailable": "reference GPU run failed: %s" % e}
+
+
+def single_cloud(px, dim, nside, seed=11):
+    """One cloud of the batched-cloud workload's recipe at a fixed size: nside^dim cell-centred nodes of spacing
+    h = 1 mm jittered by U(-0.2h, 0.2h), delta = 3.015h, unit-cell volumes, no ghosts."""
+    rng = np.random.default_rng(seed)
+    h = 1e-3
+    g = np.stack(np.meshgrid(*(np.arange(nside),) * dim, indexing="ij"), -1).reshape(-1, dim)
+    xyz = np.zeros((g.shape[0], 3))
+    xyz[:, :dim] = (g + 0.5) * h + rng.uniform(-0.2 * h, 0.2 * h, size=(g.shape[0], dim))
+    delta = 3.015 * h * (1.0 + 1e-6)
+    off, ids = px.families(xyz, delta, dim == 3)
+    return dict(dim=dim, coords3=xyz, vols=np.full(g.shape[0], h ** dim), delta=delta, dx_char=h, off=off, ids=ids)
+
+
+def assembly_pair(px, c, mirror=None, reps=10):
+    """Order-2 g-build + Poisson assembly (sigma = 1, f = 1, u = 0) on one mesh: this backend's g-build and
+    assembly kernels (CUDA events, L2 flushed before each g-build) beside the reference's own GPU path on the same
+    mesh (oracle/_ref/libperix_ref_cuda.so: opsBuildKernel and assembleKernel with CUDA events, L2 flushed, and the
+    whole perix_cuda::assemble call on host buffers).  The two CSR value arrays are compared."""
+    import ctypes as C
+    import torch
+    from oracle import ref_cuda_assemble_bench
+    dim, n = c["dim"], c["vols"].size
+    rowptr, cols = px.csr_pattern(c["off"], c["ids"], mirror, 1)
+    ctx = px.Context(0)
+    ctx.set_geometry(c["coords3"].reshape(-1), c["vols"], c["off"], c["ids"], c["delta"], c["dx_char"], dim,
+                     mirror=mirror)
+    _, gb_ms = gbuild_rate(px, ctx, "fp64", reps=5)
+    ctx.gbuild(2, px.FP64)
+    ctx.csr_set_pattern(rowptr, cols, 1)
+    dev = torch.device("cuda", 0)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    ud = torch.zeros(n, dtype=torch.float64, device=dev)
+    kd = torch.empty(int(rowptr[-1]), dtype=torch.float64, device=dev)
+    rd = torch.empty(n, dtype=torch.float64, device=dev)
+
+    def assemble():
+        st = ctx.L.pxb_assemble_scalar_d(ctx.h, 0, C.c_double(1.0), C.c_double(1.0), None, C.c_double(0.0),
+                                         C.c_void_p(ud.data_ptr()), None, C.c_void_p(kd.data_ptr()),
+                                         C.c_void_p(rd.data_ptr()))
+        if st:
+            raise RuntimeError(ctx.L.pxb_last_error().decode())
+
+    for _ in range(3):
+        assemble()
+    flush = torch.empty(FLUSH_BYTES // 8, dtype=torch.float64, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    tot = 0.0
+    for r in range(reps):
+        flush.fill_(float(r))
+        ev[0].record()
+        assemble()
+        ev[1].record()
+        torch.cuda.synchronize(dev)
+        tot += ev[0].elapsed_time(ev[1])
+    asm_ms = tot / reps
+    ours = kd.cpu().numpy()
+    ctx.close()
+    del flush
+    torch.cuda.empty_cache()
+    call_ms, ob_ms, ak_ms, kv, _ = ref_cuda_assemble_bench(dim, c["coords3"], c["vols"], c["off"], c["ids"], c["delta"],
+                                                           c["dx_char"], rowptr, cols, 1.0, 1.0, np.zeros(n),
+                                                           reps=reps, flush_bytes=FLUSH_BYTES)
+    scale = float(np.abs(kv).max()) or 1.0
+    return {"nodes": n, "bonds": int(c["off"][-1]), "nnz": int(rowptr[-1]), "gbuild_ms": gb_ms, "assembly_ms": asm_ms,
+            "ref_call_ms": call_ms, "ref_opsbuild_ms": ob_ms, "ref_assemble_kernel_ms": ak_ms,
+            "gbuild_speedup_vs_ref_opsbuild": ob_ms / gb_ms, "assembly_speedup_vs_ref_kernel": ak_ms / asm_ms,
+            "kvals_max_rel_diff": float(np.abs(ours - kv).max()) / scale}
 
 
 REF_MAX_STEPS = 40     # bound on the reference arm's timed steps (about 0.2-0.4 s each on the slab)
@@ -1109,6 +1180,9 @@ def run_profile(args):
         # from the state after 100 steps; run in a child process of the main bench
         from oracle import ref_cuda_available, ref_cuda_epf_bench
         ctx.close()
+        # the reference keeps its operator cache at nop 5 (2D implicit) only when PERIX_CUDA_OPCACHE=1; it reads
+        # the variable once, at its first call (this is a child process of the main bench)
+        os.environ["PERIX_CUDA_OPCACHE"] = "1"
         if not ref_cuda_available():
             print(json.dumps({"profile": "refgpu", "unavailable": "oracle/_ref/libperix_ref_cuda.so not built"}))
             return
@@ -1131,6 +1205,16 @@ def run_profile(args):
             res[name] = {"nodes": Lv.n, "bonds": wv["nb"], "call_ms": call_ms, "force_kernel_ms": kern_ms,
                          "opbuild_ms": ob_ms, "force_kernel_bond_updates_per_s": wv["nb"] / (kern_ms * 1e-3),
                          "call_bond_updates_per_s": wv["nb"] / (call_ms * 1e-3)}
+        # the implicit path: order-2 g-build + Poisson assembly on the 64x64 Poisson lattice and on the largest 2D
+        # and 3D clouds of the batched-cloud workload
+        L = px.lattice(2, 64, 64, 0, [0.0, 1.0, 0.0, 1.0])
+        delta = 3.015 * L.dxyz[0] * (1.0 + 1e-6)
+        off, ids = px.families(L.coords, delta, False, mirror=L.mirror)
+        asm = {"poisson_64x64": assembly_pair(px, dict(dim=2, coords3=L.coords, vols=L.vols, delta=delta,
+                                                       dx_char=L.dxyz[0], off=off, ids=ids), mirror=L.mirror)}
+        asm["cloud_2d_447x447"] = assembly_pair(px, single_cloud(px, 2, 447))
+        asm["cloud_3d_58x58x58"] = assembly_pair(px, single_cloud(px, 3, 58))
+        res["assembly"] = asm
         print(json.dumps(res))
         return
     if args.profile == "slabstep":

@@ -15,4 +15,4 @@ The product (``perix_b200``) never imports this package.
 """
 from .lib import (PortOracle, RefMesh, RefEpf, port_available, ref_available, dropin_available,  # noqa: F401
                   bc_program_arrays,
-                  ORACLE_DIR, ref_cuda_available, ref_cuda_epf_bench, ref_cuda_stress_ch)
+                  ORACLE_DIR, ref_cuda_available, ref_cuda_epf_bench, ref_cuda_stress_ch, ref_cuda_assemble_bench)

@@ -282,6 +282,42 @@ def ref_cuda_stress_ch(dim, coords3, vols, off, ids, delta, dx_char, rowptr, col
     return kv, rhs
 
 
+def ref_cuda_assemble_bench(dim, coords3, vols, off, ids, delta, dx_char, rowptr, cols, sigma, f, u, reps=10,
+                            flush_bytes=256 << 20):
+    """Times the reference's own implicit GPU path (oracle/ref_cuda_harness.cu) on a Poisson assembly: the
+    perix_cuda::assemble call, its one-off opsBuildKernel and assembleKernel alone.  The child process should set
+    PERIX_CUDA_OPCACHE=1 so that the reference keeps an operator cache at nop 5 too.  Returns (call_ms,
+    opsbuild_ms, kernel_ms, kvals, rhs)."""
+    L = C.CDLL(_REFCU_SO)
+    coords3 = np.ascontiguousarray(coords3, np.float64).reshape(-1)
+    n = coords3.size // 3
+    if dim == 2:
+        q = [(1, 0, 0), (0, 1, 0), (2, 0, 0), (1, 1, 0), (0, 2, 0)]
+    else:
+        q = [(1, 0, 0), (0, 1, 0), (0, 0, 1), (2, 0, 0), (1, 1, 0), (1, 0, 1), (0, 2, 0), (0, 1, 1), (0, 0, 2)]
+    qp = np.array([a for a, _, _ in q], np.int32)
+    qq = np.array([b for _, b, _ in q], np.int32)
+    qr = np.array([c for _, _, c in q], np.int32)
+    fact = np.array([math.factorial(a) * math.factorial(b) * math.factorial(c) for a, b, c in q], np.float64)
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    cols = np.ascontiguousarray(cols, np.int32)
+    out = np.zeros(4, np.float64)
+    kv = np.zeros(cols.size, np.float64)
+    rhs = np.zeros(n, np.float64)
+    L.refcu_assemble_bench.restype = C.c_int
+    st = L.refcu_assemble_bench(n, dim, _ptr(coords3, C.c_double), _ptr(np.ascontiguousarray(vols, np.float64), C.c_double),
+                                _ptr(np.ascontiguousarray(off, np.int32), C.c_int),
+                                _ptr(np.ascontiguousarray(ids, np.int32), C.c_int), _ptr(qp, C.c_int),
+                                _ptr(qq, C.c_int), _ptr(qr, C.c_int), _ptr(fact, C.c_double), len(q), C.c_double(delta),
+                                C.c_double(dx_char), _ptr(rowptr, C.c_int), _ptr(cols, C.c_int), int(cols.size),
+                                C.c_double(sigma), C.c_double(f), _ptr(np.ascontiguousarray(u, np.float64), C.c_double),
+                                int(reps), C.c_size_t(flush_bytes), _ptr(out, C.c_double), _ptr(kv, C.c_double),
+                                _ptr(rhs, C.c_double))
+    if st:
+        raise RuntimeError("reference GPU assembly harness failed with status %d" % st)
+    return float(out[0]), float(out[1]), float(out[2]), kv, rhs
+
+
 _DROPIN = None
 
 

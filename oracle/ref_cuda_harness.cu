@@ -135,6 +135,90 @@ REFCU_API int refcu_epf_bench(int n, int dim, const double *coords, const double
     return err == cudaSuccess ? 0 : 4;
 }
 
+// The reference's implicit GPU path on one mesh (perix_cuda::assemble, CudaAssembleKernels.cu:1109-1184, Poisson):
+// out[0] mean wall ms of one call after a warm call (H2D u, assembleKernel, D2H K and rhs), out[1] ms of its one-off
+// operator build opsBuildKernel (all nop operators of every bond, CUDA events, L2 flushed first), out[2] mean ms of
+// assembleKernel alone on the cached operators (events, L2 flushed before each).  kvals / rhs get the last call's
+// values.  Returns 0 on success.
+REFCU_API int refcu_assemble_bench(int n, int dim, const double *coords, const double *vols, const int *off,
+                                   const int *ids, const int *qp, const int *qq, const int *qr,
+                                   const double *factprod, int nop, double delta, double dx_char, const int *csr_off,
+                                   const int *csr_col, int nnz, double sigma, double f, const double *u, int reps,
+                                   size_t flush_bytes, double *out, double *kvals, double *rhs) {
+    perix_cuda::AssembleMesh m;
+    m.N = n;
+    m.nnz = nnz;
+    m.csr_off = csr_off;
+    m.csr_col = csr_col;
+    m.neigh_off = off;
+    m.neigh_id = ids;
+    m.coords = coords;
+    m.vols = vols;
+    m.qp = qp;
+    m.qq = qq;
+    m.qr = qr;
+    m.factprod = factprod;
+    m.nop = nop;
+    m.dim = dim;
+    m.delta = delta;
+    m.dx_char = dx_char;
+    perix_cuda::ElmtParams p;
+    p.type = perix_cuda::ELMT_POISSON;
+    p.ndof = 1;
+    p.dim = dim;
+    p.sigma = sigma;
+    p.f = f;
+    const perix_cuda::OpSlots s = slots_for(dim);
+    if (!perix_cuda::assemble(m, p, s, u, nullptr, kvals, rhs)) return 1;
+    auto t0 = std::chrono::steady_clock::now();
+    for (int r = 0; r < reps; ++r)
+        if (!perix_cuda::assemble(m, p, s, u, nullptr, kvals, rhs)) return 2;
+    auto t1 = std::chrono::steady_clock::now();
+    out[0] = std::chrono::duration<double, std::milli>(t1 - t0).count() / reps;
+    Ctx &g = g_ctx;
+    if (!g.bondOps) return 5;  // the operator cache is off for this nop (devOpCacheEnabled)
+    void *flush = nullptr;
+    if (flush_bytes && cudaMalloc(&flush, flush_bytes) != cudaSuccess) return 3;
+    auto do_flush = [&](int r) {
+        if (!flush) return;
+        cudaMemsetAsync(flush, r & 0xff, flush_bytes);
+        refcu_flush_read<<<1184, 256>>>(static_cast<const uint4 *>(flush), flush_bytes / 16,
+                                       static_cast<unsigned *>(flush));
+    };
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int block = 128, grid = (n + block - 1) / block;
+    do_flush(0);
+    cudaEventRecord(a);
+    opsBuildKernel<<<grid, block>>>(n, dim, nop, g.qp, g.qq, g.qr, g.factprod, g.coords, g.vols, g.neigh_off,
+                                    g.neigh_id, nullptr, nullptr, delta, dx_char, g.bondOps, g.opsValid);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    out[1] = ms;
+    double kern = 0.0;
+    for (int r = 0; r < reps; ++r) {
+        do_flush(r + 1);
+        cudaEventRecord(a);
+        assembleKernel<<<grid, block>>>(n, p, s, g.csr_off, g.csr_col, g.neigh_off, g.neigh_id, g.coords, g.vols,
+                                        g.qp, g.qq, g.qr, g.factprod, nop, delta, dx_char, nullptr, nullptr,
+                                        g.bondOps, g.opsValid, g.u, nullptr, g.Kvals, g.rhs);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&ms, a, b);
+        kern += ms;
+    }
+    out[2] = kern / reps;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (flush) cudaFree(flush);
+    const cudaError_t err = cudaDeviceSynchronize();
+    perix_cuda::shutdown();
+    return err == cudaSuccess ? 0 : 4;
+}
+
 // The reference's own stress-coupled CH device assembler (perix_cuda::assembleStressCahnHilliard,
 // CudaAssembleKernels.cu:1325-) on one mesh: p13 = C11 C12 C66 A Kh Ch Omega cref chi kappa dt kres rho.
 // health (nbtot) and vel (N*dim) may be NULL.  Returns 0 on success.
