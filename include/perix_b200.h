@@ -154,9 +154,8 @@ int pxb_get_ops(pxb_ctx *ctx, double *ops);
  * arrays are checked on the device first; a malformed list gives PXB_ERR_INVALID and no build.  Working memory
  * is one fixed 4 MiB device array shared by all calls on a device, which limits n to
  * pxb_gbuild_noalloc_max_nodes(dim) (262,128 nodes in 2D, 131,064 in 3D); larger n is rejected with
- * PXB_ERR_INVALID.  The first call on a device resolves the array's address, so make it before any stream
- * capture; calls that overlap on the GPU race on the shared array.  Synchronises the stream before returning
- * (the input check and the degenerate counters are read back). */
+ * PXB_ERR_INVALID.  Calls that overlap on the GPU race on the shared array.  The call synchronises its stream
+ * (the input check and the degenerate counters are read back), so it cannot be captured into a CUDA graph. */
 int pxb_gbuild_noalloc_d(int dim, int order, int precision, int n, long long nbtot, const int *neigh_off_d,
                          const int *neigh_id0_d, const double *coords3_d, const double *vols_d, const int *layer_d,
                          double delta, double dx_char, void *ops_d, float *defect_d, uint8_t *degenerate_d,

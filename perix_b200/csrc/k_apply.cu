@@ -245,7 +245,10 @@ static cudaError_t launch_ab_m(const BatchArgs &a, int variant, int dims, cudaSt
         case 2: return launch_ab<MIXED, 8, 32, 3>(a, s);
         case 3: return dims == 1 ? launch_ab<MIXED, 8, 16, 1>(a, s) : launch_ab<MIXED, 8, 16, 2>(a, s);
         case 4: return launch_ab<MIXED, 16, 16, 3>(a, s);
-        default: return dims == 1 ? launch_ab<MIXED, 4, 16, 1>(a, s) : launch_ab<MIXED, 4, 16, 2>(a, s);
+        case 5: return dims == 1 ? launch_ab<MIXED, 4, 16, 1>(a, s) : launch_ab<MIXED, 4, 16, 2>(a, s);
+        case 6: return launch_ab<MIXED, 4, 32, 3>(a, s);
+        case 7: return dims == 1 ? launch_ab<MIXED, 16, 32, 1>(a, s) : launch_ab<MIXED, 16, 32, 2>(a, s);
+        default: return cudaErrorInvalidValue;
     }
 }
 

@@ -4,7 +4,12 @@
   FP64 within 1e-12 (family-scaled), mixed within 1e-6.
 * Orders above 2 (2D orders 3 and 4 - the 14 monomials of the reference GPU path's kMaxNop = 15 - and 3D order 3)
   against the reference's PDOperators on a lattice with mirror ghosts and on a jittered cloud
-  (oracle/_ref/libperix_ref.so), and against the C restatement.
+  (oracle/_ref/libperix_ref.so), and against the C restatement.  Order 4 uses a horizon of 4.015 h: at 3.015 h
+  the reference's own build finds degenerate ghost families and exits (calcAMatrix).
+* The FP64 bound is 1e-12 family-scaled up to nine monomials.  The 14- and 19-monomial systems are conditioned so
+  that FP64 itself sets the floor: on these meshes the reference's own FullPivLU result lies 4.4e-12 (2D order 4
+  lattice) and 2.7e-12 (3D order 3 cloud) from an 80-bit solve of the same moment systems, and an FP64 L D L^T
+  with one refinement step lies as far from it; there the bound is 3e-11.
 * A degenerate family is reported with its 1-based node id by both schedules."""
 import numpy as np
 import pytest
@@ -39,19 +44,25 @@ def test_schedules_match_reference_goldens(ctx, name, dim, schedule):
         ctx.gbuild_set_schedule(-1)
 
 
+def _fp64_bound(dim, order):
+    """Family-scaled FP64 bound against the reference (see the module docstring)."""
+    return 1e-12 if (order <= 2 or (dim == 2 and order == 3)) else 3e-11
+
+
 def _ref_mesh(dim, order, kind):
     from oracle import RefMesh
+    hf = 4.015 if order >= 4 else 3.015
     if kind == "lattice":
         if dim == 2:
-            return RefMesh.structured(2, 16, 12, 0, [0, 1.6, 0, 1.2], 3.015, order)
-        return RefMesh.structured(3, 8, 7, 6, [0, 0.8, 0, 0.7, 0, 0.6], 3.015, order)
+            return RefMesh.structured(2, 16, 12, 0, [0, 1.6, 0, 1.2], hf, order)
+        return RefMesh.structured(3, 8, 7, 6, [0, 0.8, 0, 0.7, 0, 0.6], hf, order)
     rng = np.random.default_rng(5 + dim + order)
     h = 0.1
     shape = (14, 11) if dim == 2 else (8, 7, 6)
     g = np.stack(np.meshgrid(*[np.arange(k) for k in shape], indexing="ij"), -1).reshape(-1, dim)
     xyz = np.zeros((g.shape[0], 3))
     xyz[:, :dim] = (g + 0.5) * h + rng.uniform(-0.2 * h, 0.2 * h, size=(g.shape[0], dim))
-    return RefMesh.cloud(dim, xyz, np.full(g.shape[0], h ** dim), h, h, h if dim == 3 else 0.0, 3.015 * h, order)
+    return RefMesh.cloud(dim, xyz, np.full(g.shape[0], h ** dim), h, h, h if dim == 3 else 0.0, hf * h, order)
 
 
 @pytest.mark.skipif(not ref_available(), reason="reference harness not built")
@@ -69,9 +80,10 @@ def test_higher_orders_match_reference(ctx, port, dim, order, kind):
     assert g.shape == g_ref.shape
     ok = np.repeat(deg_ref == 0, np.diff(m.off))  # rows the reference builds (deep/degenerate ghosts aside)
     off_ok = np.concatenate([[0], np.cumsum(np.diff(m.off)[deg_ref == 0])])
-    assert scaled_err(g[ok], g_ref[ok], off_ok) <= 1e-12
+    tol = _fp64_bound(dim, order)
+    assert scaled_err(g[ok], g_ref[ok], off_ok) <= tol
     g_port, _ = port.gbuild(dim, order, m.coords, m.vols, m.off, m.ids, m.delta, m.dx_char)
-    assert scaled_err(g[ok], g_port[ok], off_ok) <= 1e-12
+    assert scaled_err(g[ok], g_port[ok], off_ok) <= tol
     ctx.gbuild(order, 1, allow_degenerate=True)
     assert scaled_err(ctx.get_ops()[ok], g_ref[ok], off_ok) <= 1e-6
 
@@ -109,6 +121,9 @@ def test_higher_order_poisson_assembly_matches_reference(ctx, dim, order):
     """Poisson K and rhs (PDSystem::formResidualAndJacobian with a PoissonElement) from operators of order 3 and 4,
     the Laplacian slots resolved from the multi-index table."""
     m = _ref_mesh(dim, order, "lattice")
+    _, deg_ref = m.gbuild()
+    if deg_ref.any():  # the reference's system assembly exits on a degenerate family
+        pytest.skip("degenerate families at this order")
     rng = np.random.default_rng(60 + dim + order)
     u = rng.standard_normal(m.n)
     kv_ref, rhs_ref, _ = m.system_assemble(0, 1.3, 0.7, u)
@@ -117,5 +132,6 @@ def test_higher_order_poisson_assembly_matches_reference(ctx, dim, order):
     rowptr, cols = m.csr_pattern(1)
     ctx.csr_set_pattern(rowptr, cols, 1)
     kv, rhs = ctx.assemble_scalar(0, 1.3, u, f=0.7)
-    assert np.abs(kv - kv_ref).max() <= 1e-12 * np.abs(kv_ref).max()
-    assert np.abs(rhs - rhs_ref).max() <= 1e-12 * np.abs(rhs_ref).max()
+    tol = _fp64_bound(dim, order)
+    assert np.abs(kv - kv_ref).max() <= tol * np.abs(kv_ref).max()
+    assert np.abs(rhs - rhs_ref).max() <= tol * np.abs(rhs_ref).max()
