@@ -101,11 +101,16 @@ def slab_adjoint(px, device=0, adjoint_steps=1000, checkpoint_every=100):
     ctx = px.Context(device)
     ctx.set_geometry(L.coords, L.vols, w["off"], w["ids"], w["delta"], L.dxyz[0], 3, mirror=L.mirror)
 
+    tuned = {}
+
     def device_final(E):
         c = px.elastic_constants(3, False, E, w["nu"])
         ctx.epf_setup(c[0], c[1], c[2], w["rho"], (0.0, 0.0, 0.0), 0.0, True, health0=w["health0"])
         ctx.epf_set_bcs(w["bcs"])
         ctx.epf_start(np.zeros(3 * L.n), None, w["dt"])
+        if not tuned:  # the step schedule of this frozen-mask loop, timed once (state unchanged)
+            tuned.update(autotune(ctx))
+        ctx.epf_set_variant(tuned["variant"])
         ctx.epf_advance(adjoint_steps, chunk=100)
         return ctx.epf_state()[0]
 
@@ -122,25 +127,32 @@ def slab_adjoint(px, device=0, adjoint_steps=1000, checkpoint_every=100):
     t0 = time.perf_counter()
     device_final(w["E"])  # the forward loop alone (start + adjoint_steps graph-captured steps); context state too
     fwd_secs = time.perf_counter() - t0
-    E = torch.tensor(w["E"], dtype=torch.float64, device=dev, requires_grad=True)
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    C = elastic_constants_t(3, False, E, w["nu"])
-    set_constants(ctx, C, w["rho"])
-    uN, _ = explicit_run(ctx, torch.zeros(3 * L.n, dtype=torch.float64, device=dev), None, C, w["dt"], adjoint_steps,
-                         checkpoint_every=checkpoint_every)
-    Jt = 0.5 * ((uN - torch.from_numpy(u_obs).to(dev)) ** 2).sum()
-    Jt.backward()
-    torch.cuda.synchronize(dev)
-    secs = time.perf_counter() - t0
-    res["adjoint"] = {"steps": adjoint_steps, "checkpoint_every": checkpoint_every, "precision": "fp64",
-                      "dJ_dE": float(E.grad), "dJ_dE_central_fd": {"h=1e-5E": fd1, "h=5e-6E": fd2, "richardson": fd},
-                      "rel_err_vs_fd": abs(float(E.grad) - fd) / abs(fd),
-                      "rel_err_vs_fd_h5e-6": abs(float(E.grad) - fd2) / abs(fd2), "seconds_forward_and_backward": secs,
-                      "seconds_forward_loop_alone": fwd_secs, "over_forward": secs / fwd_secs,
-                      "method": "device loop forward (pxb_epf_advance), device adjoint backward (pxb_epf_adjoint_d: "
-                                "BC transpose + fused bond-force / central-difference adjoint per step, states "
-                                "recomputed from checkpoints)"}
+    def gradient(ck):
+        E = torch.tensor(w["E"], dtype=torch.float64, device=dev, requires_grad=True)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        C = elastic_constants_t(3, False, E, w["nu"])
+        set_constants(ctx, C, w["rho"])
+        uN, _ = explicit_run(ctx, torch.zeros(3 * L.n, dtype=torch.float64, device=dev), None, C, w["dt"],
+                             adjoint_steps, checkpoint_every=ck)
+        Jt = 0.5 * ((uN - torch.from_numpy(u_obs).to(dev)) ** 2).sum()
+        Jt.backward()
+        torch.cuda.synchronize(dev)
+        secs = time.perf_counter() - t0
+        return {"steps": adjoint_steps, "checkpoint_every": ck, "precision": "fp64", "dJ_dE": float(E.grad),
+                "dJ_dE_central_fd": {"h=1e-5E": fd1, "h=5e-6E": fd2, "richardson": fd},
+                "rel_err_vs_fd": abs(float(E.grad) - fd) / abs(fd),
+                "rel_err_vs_fd_h5e-6": abs(float(E.grad) - fd2) / abs(fd2), "seconds_forward_and_backward": secs,
+                "seconds_forward_loop_alone": fwd_secs, "over_forward": secs / fwd_secs}
+
+    how = ("forward: the frozen-mask device loop keeping its checkpoints (pxb_epf_record_d); backward: per step the BC "
+           "transpose and one fused bond-force / central-difference adjoint kernel (pxb_epf_adjoint_recorded_d)")
+    res["forward_step_variant"] = tuned.get("variant")
+    res["adjoint"] = gradient(checkpoint_every)
+    res["adjoint"]["method"] = how + ", states recomputed segment by segment from the checkpoints"
+    res["adjoint_all_states_kept"] = gradient(0)
+    res["adjoint_all_states_kept"]["method"] = how + ", every state kept (%.1f GB), nothing recomputed" % (
+        adjoint_steps * 3 * L.n * 8 / 1e9)
     ctx.close()
     return res
 
@@ -1259,6 +1271,29 @@ def run_profile(args):
                           "precision": args.precision, "schedule": args.variant, "ms": [float(x) for x in ms]}))
         ctx.close()
         return
+    if args.profile == "cloudsgbuild":
+        # --steps clouds (log-uniform 1k..200k nodes), then 3 FP64 or mixed order-2 g-builds with schedule --variant
+        ctx.close()
+        import torch
+        clouds = clouds_generate(px, nclouds=args.steps, families=False)
+        ctx = px.Context(0)
+        ctx.batch_set_points(clouds)
+        dev = torch.device("cuda", 0)
+        ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        ctx.batch_set_variant(0, args.variant)
+        prec = px.MIXED if args.precision == "mixed" else px.FP64
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ms = []
+        for _ in range(3):
+            ev[0].record()
+            ctx.batch_gbuild(prec)
+            ev[1].record()
+            torch.cuda.synchronize(dev)
+            ms.append(ev[0].elapsed_time(ev[1]))
+        print(json.dumps({"profile": "cloudsgbuild", "clouds": args.steps, "nodes": ctx.batch_n, "bonds": ctx.batch_nb,
+                          "precision": args.precision, "schedule": args.variant, "ms": ms}))
+        ctx.close()
+        return
     if args.profile == "clouds":
         print(json.dumps({"profile": "clouds", **clouds_measure(px, nclouds=args.steps)}))
         ctx.close()
@@ -1290,7 +1325,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="perix", choices=["perix", "reference"])
-    ap.add_argument("--profile", choices=["step", "gbuild", "clouds", "slab", "slabstep", "cloudsapply", "refgpu", "ch"], default=None,
+    ap.add_argument("--profile", choices=["step", "gbuild", "clouds", "slab", "slabstep", "cloudsapply", "cloudsgbuild", "refgpu", "ch"], default=None,
                     help="run one kernel family only (for profiler captures); prints its own JSON line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--variant", type=int, default=8)

@@ -124,7 +124,7 @@ int pxb_set_node_horizons(pxb_ctx *ctx, const double *node_delta, const double *
 
 /* ---- g-functions (reference PDOperators::buildGeometryCache, src/PDOperators/CalcPDOperators.cpp:356-463) ----
  * Builds the per-bond operator vectors ops[bond*nop+k] for multi-index order `order` (2D 1..4, 3D 1..3) on the
- * device.  precision PXB_MIXED stores g in FP32 with the solve and one refinement step in FP64; its moment sums run
+ * device.  precision PXB_MIXED stores g in FP32 with the solve in FP64; its moment sums run
  * in FP32 on delta-scaled bond vectors with compensated (two-sum) accumulation on the lane-group schedule and in FP64
  * on the warp-per-node schedule (pxb_gbuild_set_schedule).
  * Returns PXB_ERR_DEGENERATE when a non-ghost family is degenerate; *n_degenerate / *first_degenerate
@@ -132,7 +132,9 @@ int pxb_set_node_horizons(pxb_ctx *ctx, const double *node_delta, const double *
 int pxb_gbuild(pxb_ctx *ctx, int order, int precision, int *n_degenerate, int *first_degenerate);
 /* Schedule of the g-build kernels: 0 lane groups (a group of 8-32 lanes per node; at MIXED the moment sums run in
  * FP32 with two-sum compensation), 1 one warp per node (moment sums in FP64 at both precisions; MIXED stores FP32),
- * -1 (default) the one this backend picks: warp per node in 3D and above order 2, lane groups for 2D orders 1-2.
+ * 2 the same with each lane's moment sums kept over all the node's bonds and reduced once per node (up to nine
+ * monomials; larger systems as 1), -1 (default) the one this backend picks: warp per node in 3D and above order 2,
+ * lane groups for 2D orders 1-2.
  * Orders 2D 4 and 3D 3 exist only as the warp-per-node schedule. */
 int pxb_gbuild_set_schedule(pxb_ctx *ctx, int schedule);
 /* nop of the current operator cache and its multi-index table (pqr: 3*nop ints, may be NULL). */
@@ -254,12 +256,23 @@ int pxb_epf_force_adjoint_d(pxb_ctx *ctx, const double *u_d, const double *abar_
  * with the context's BC program after every step and no bond breaking.  Given ubar_N = dJ/du^N and ubar_Nm1 =
  * dJ/du^{N-1} (may be NULL: 0), returns u0bar = dJ/du0, v0bar = dJ/dv0 (may be NULL) and dC = dJ/d(C11, C12, C66)
  * (3 doubles, may be NULL).  The reverse sweep runs on the device: per step the transpose of the BC pass, then one
- * kernel for the bond-force adjoint (reverse-bond gather) fused with the central difference's transpose.  The forward
- * states it needs are recomputed from checkpoints kept every checkpoint_every steps (<= 0: one segment, all states
- * kept: nsteps * N * dim doubles).  Leaves the context's explicit state unchanged.  No counterpart in the reference. */
+ * kernel for the bond-force adjoint fused with the central difference's transpose (the reverse bonds' operators come
+ * from a bond-ordered copy built on first use, as large as the operator cache; without room for it they are
+ * gathered).  The forward states it needs are kept every checkpoint_every steps and the others recomputed
+ * (<= 0 or >= nsteps: every state kept, nsteps * N * dim doubles, nothing recomputed).  Leaves the context's
+ * explicit state unchanged.  pxb_epf_adjoint_d = pxb_epf_record_d + pxb_epf_adjoint_recorded_d.  No counterpart
+ * in the reference. */
 int pxb_epf_adjoint_d(pxb_ctx *ctx, const double *u0_d, const double *v0_d, double dt, int nsteps, int checkpoint_every,
                       const double *ubar_N_d, const double *ubar_Nm1_d, double *u0bar_d, double *v0bar_d,
                       double *dC_d);
+/* The forward half on its own: runs the frozen-mask loop from (u0, v0), keeps its checkpoints (or every state) in the
+ * context and returns u^N and u^{N-1} (either may be NULL).  A differentiable caller runs it as its forward pass and
+ * pxb_epf_adjoint_recorded_d as its backward pass, so the loop is not run a second time. */
+int pxb_epf_record_d(pxb_ctx *ctx, const double *u0_d, const double *v0_d, double dt, int nsteps, int checkpoint_every,
+                     double *uN_d, double *uNm1_d);
+/* The reverse sweep of the last pxb_epf_record_d (PXB_ERR_STATE when there is none); arguments as pxb_epf_adjoint_d. */
+int pxb_epf_adjoint_recorded_d(pxb_ctx *ctx, const double *ubar_N_d, const double *ubar_Nm1_d, double *u0bar_d,
+                               double *v0bar_d, double *dC_d);
 /* Force (rate) with a frozen mask, device pointers, no damage update: a = (L(u)+b)/rho. */
 int pxb_epf_force_frozen_d(pxb_ctx *ctx, const double *u_d, double *a_d);
 /* Replaces C11, C12, C66 and rho of the explicit element without rebuilding the g-functions (the packed

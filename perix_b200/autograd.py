@@ -205,19 +205,29 @@ def explicit_loop(pctx, u0, v0, dt, nsteps, C, plan, checkpoint_every=100, t0=0.
     return u, uold
 
 
+def _record(pctx, u0, v0, dt, nsteps, ck, uN=None, uNm1=None):
+    import ctypes as Ct
+    p = lambda t: None if t is None else Ct.c_void_p(t.data_ptr())  # noqa: E731
+    _on_stream(pctx, u0)
+    st = pctx.L.pxb_epf_record_d(pctx.h, p(u0), p(v0), Ct.c_double(dt), int(nsteps), int(ck), p(uN), p(uNm1))
+    if st:
+        from .api import PxbError
+        raise PxbError(st, pctx.L.pxb_last_error().decode(errors="replace"))
+    pctx._recording = token = object()  # the context keeps one recording: the latest
+    return token
+
+
 class _ExplicitRun(torch.autograd.Function):
     @staticmethod
     def forward(fctx, u0, C, v0, pctx, dt, nsteps, checkpoint_every):
         u0c = _f64c(u0)
         v0c = None if v0 is None else _f64c(v0)
-        pctx.set_stream(0)
-        torch.cuda.current_stream(u0c.device).synchronize()
-        pctx.epf_start(u0c.cpu().numpy(), None if v0c is None else v0c.cpu().numpy(), dt)
-        pctx.epf_advance(nsteps)
-        uN, uNm1, _, _ = pctx.epf_state()
+        uN = torch.empty_like(u0c)
+        uNm1 = torch.empty_like(u0c)
+        fctx.token = _record(pctx, u0c, v0c, dt, nsteps, checkpoint_every, uN, uNm1)
         fctx.save_for_backward(u0c, *(() if v0c is None else (v0c,)))
         fctx.pctx, fctx.dt, fctx.nsteps, fctx.ck, fctx.has_v0 = pctx, dt, nsteps, checkpoint_every, v0c is not None
-        return (torch.from_numpy(uN).to(u0c.device), torch.from_numpy(uNm1).to(u0c.device))
+        return uN, uNm1
 
     @staticmethod
     def backward(fctx, gN, gNm1):
@@ -225,6 +235,8 @@ class _ExplicitRun(torch.autograd.Function):
         saved = fctx.saved_tensors
         u0 = saved[0]
         v0 = saved[1] if fctx.has_v0 else None
+        if getattr(fctx.pctx, "_recording", None) is not fctx.token:  # a later run replaced this one's recording
+            fctx.token = _record(fctx.pctx, u0, v0, fctx.dt, fctx.nsteps, fctx.ck)
         gN = torch.zeros_like(u0) if gN is None else _f64c(gN)
         gNm1 = None if gNm1 is None else _f64c(gNm1)
         u0bar = torch.empty_like(u0)
@@ -232,8 +244,7 @@ class _ExplicitRun(torch.autograd.Function):
         dC = torch.zeros(3, dtype=torch.float64, device=u0.device)
         _on_stream(fctx.pctx, u0)
         p = lambda t: None if t is None else Ct.c_void_p(t.data_ptr())  # noqa: E731
-        st = fctx.pctx.L.pxb_epf_adjoint_d(fctx.pctx.h, p(u0), p(v0), Ct.c_double(fctx.dt), int(fctx.nsteps),
-                                           int(fctx.ck), p(gN), p(gNm1), p(u0bar), p(v0bar), p(dC))
+        st = fctx.pctx.L.pxb_epf_adjoint_recorded_d(fctx.pctx.h, p(gN), p(gNm1), p(u0bar), p(v0bar), p(dC))
         if st:
             from .api import PxbError
             raise PxbError(st, fctx.pctx.L.pxb_last_error().decode(errors="replace"))
@@ -241,11 +252,12 @@ class _ExplicitRun(torch.autograd.Function):
 
 
 def explicit_run(pctx, u0, v0, C, dt, nsteps, checkpoint_every=0):
-    """(u^N, u^{N-1}) of nsteps central-difference steps from (u0, v0) run on the device (pxb_epf_start +
-    pxb_epf_advance with the context's BC program), differentiable in u0, v0 and C through the device adjoint
-    (pxb_epf_adjoint_d).  The damage mask must be frozen: set the context up with sc = 0 (its current health is the
-    mask), and its constants equal to C (``set_constants``).  checkpoint_every > 0 keeps a state every that many steps
-    and recomputes the others in the backward pass; 0 keeps them all (nsteps * N * dim doubles on the device)."""
+    """(u^N, u^{N-1}) of nsteps central-difference steps from (u0, v0) run on the device with the context's BC program
+    (pxb_epf_record_d, which keeps the forward states the backward pass needs), differentiable in u0, v0 and C through
+    the device adjoint (pxb_epf_adjoint_recorded_d).  The damage mask is frozen at the context's current health (no
+    bond breaks; the context's explicit state is left as it is), and the context's constants must equal C
+    (``set_constants``).  checkpoint_every > 0 keeps a state every that many steps and recomputes the others in the
+    backward pass; 0 keeps them all (nsteps * N * dim doubles on the device)."""
     return _ExplicitRun.apply(u0, C, v0, pctx, float(dt), int(nsteps), int(checkpoint_every))
 
 

@@ -128,7 +128,9 @@ size_t ctx_bytes(const pxb_ctx *c) {
     s += bufsz(c->ops.ops) + bufsz(c->ops.degenerate) + bufsz(c->ops.defect) + bufsz(c->ops.yeff);
     const EpfState &e = c->epf;
     s += bufsz(e.G) + bufsz(e.P) + bufsz(e.xib) + bufsz(e.health) + bufsz(e.u[0]) + bufsz(e.u[1]) + bufsz(e.accel) + bufsz(e.counters) +
-         bufsz(e.umax) + bufsz(e.tsched);
+         bufsz(e.umax) + bufsz(e.tsched) + bufsz(e.sc_bond);
+    s += bufsz(e.adj_ckpt) + bufsz(e.adj_seg) + bufsz(e.adj_p[0]) + bufsz(e.adj_p[1]) + bufsz(e.adj_A) + bufsz(e.adj_R) +
+         bufsz(e.adj_W) + bufsz(e.adj_t) + bufsz(e.adj_dC) + bufsz(e.adj_umax) + bufsz(e.adj_GR) + bufsz(e.adj_HR) + bufsz(e.adj_u0);
     s += bufsz(e.bc.own) + bufsz(e.bc.src_off) + bufsz(e.bc.tgt) + bufsz(e.bc.comp) + bufsz(e.bc.form) +
          bufsz(e.bc.vals);
     const BatchState &bt = c->batch;
@@ -439,12 +441,13 @@ static bool gbuild_use_warp(const pxb_ctx *c, int order) {
     if (!gbuild_warp_supported(c->g.dim, order)) return false;
     if (c->g.node_delta.p) return true;  // per-node horizons: the warp-per-node kernel reads them
     if (!gbuild_supported(c->g.dim, order)) return true;
-    if (c->gbuild_schedule >= 0) return c->gbuild_schedule == 1;
+    if (c->gbuild_schedule >= 0) return c->gbuild_schedule >= 1;
     return c->g.dim == 3 || order > 2;
 }
 
 static cudaError_t gbuild_launch(pxb_ctx *c, const GBuildArgs &a, int order, bool mixed) {
-    if (gbuild_use_warp(c, order)) return launch_gbuild_warp(a, c->g.dim, order, mixed, c->stream);
+    if (gbuild_use_warp(c, order))
+        return launch_gbuild_warp(a, c->g.dim, order, mixed, c->gbuild_schedule == 2, c->stream);
     return launch_gbuild(a, c->g.dim, order, mixed, grid_nodes(c->g.n, kGbuildThreads), c->stream);
 }
 
@@ -532,7 +535,7 @@ int gbuild_launch_only(pxb_ctx *c, int order, int precision) {
 
 extern "C" int pxb_gbuild_set_schedule(pxb_ctx *c, int schedule) {
     if (!c) return fail(PXB_ERR_INVALID, "pxb_gbuild_set_schedule: NULL context");
-    if (schedule < -1 || schedule > 1) return fail(PXB_ERR_INVALID, "pxb_gbuild_set_schedule: -1, 0 or 1");
+    if (schedule < -1 || schedule > 2) return fail(PXB_ERR_INVALID, "pxb_gbuild_set_schedule: -1, 0, 1 or 2");
     c->gbuild_schedule = schedule;
     return PXB_OK;
 }
@@ -1476,6 +1479,8 @@ int adj_kernel(pxb_ctx *c, const double *u, const double *w, double scale, doubl
     a.nbr = c->g.nbr.as<int>();
     a.rev = c->g.rev.as<int>();
     a.G = e.G.p;
+    a.GR = e.adj_GR.p;
+    a.hrev = e.adj_GR.p ? e.adj_HR.as<uint8_t>() : nullptr;
     a.health = e.health.as<uint8_t>();
     a.C11 = e.C11;
     a.C12 = e.C12;
@@ -1498,27 +1503,45 @@ int adj_kernel(pxb_ctx *c, const double *u, const double *w, double scale, doubl
 
 }  // namespace
 
-extern "C" int pxb_epf_adjoint_d(pxb_ctx *c, const double *u0_d, const double *v0_d, double dt, int nsteps,
-                                 int checkpoint_every, const double *ubar_N_d, const double *ubar_Nm1_d,
-                                 double *u0bar_d, double *v0bar_d, double *dC_d) {
-    PXB_TRY(need_epf(c, "pxb_epf_adjoint_d"));
-    if (!u0_d || !ubar_N_d || !u0bar_d || !(dt > 0.0) || nsteps < 0)
-        return fail(PXB_ERR_INVALID, "pxb_epf_adjoint_d: need u0, dJ/du^N, the dJ/du0 output, dt > 0, nsteps >= 0");
-    PXB_TRY(ensure_rev(c));
+namespace {
+
+// The adjoint kernel's reverse-bond operators as a bond-ordered copy (GR[c][t] = G[c][rev t]), built once per setup:
+// the kernel then streams them instead of gathering six scattered values per bond.  Without room for the copy
+// (a memory cap, or a full device) the kernel gathers them.
+int ensure_grev(pxb_ctx *c) {
     EpfState &e = c->epf;
+    if (e.adj_GR.p || e.adj_GR_none) return PXB_OK;
+    PXB_TRY(ensure_rev(c));
+    if (dev_alloc(c, e.adj_GR, e.G.bytes) != PXB_OK) {
+        e.adj_GR_none = true;
+        return PXB_OK;
+    }
+    PXB_CUDA_TRY(cudaMemsetAsync(e.adj_GR.p, 0, e.adj_GR.bytes, c->stream));
+    PXB_CUDA_TRY(launch_reverse_gather(e.G.p, e.adj_GR.p, c->g.rev.as<int>(), c->g.nb, (long long)c->g.ldb, c->g.dim,
+                                       e.precision == PXB_MIXED, c->stream));
+    return check_launch(c, "reverse gather");
+}
+
+}  // namespace
+
+extern "C" int pxb_epf_record_d(pxb_ctx *c, const double *u0_d, const double *v0_d, double dt, int nsteps,
+                                int checkpoint_every, double *uN_d, double *uNm1_d) {
+    PXB_TRY(need_epf(c, "pxb_epf_record_d"));
+    if (!u0_d || !(dt > 0.0) || nsteps < 0)
+        return fail(PXB_ERR_INVALID, "pxb_epf_record_d: need u0, dt > 0, nsteps >= 0");
+    EpfState &e = c->epf;
+    e.rec_steps = -1;
     const size_t nd = (size_t)c->g.n * c->g.dim, bytes = sizeof(double) * nd;
-    const int K = (checkpoint_every <= 0 || checkpoint_every > nsteps) ? std::max(nsteps, 1) : checkpoint_every;
+    // every state kept when checkpoint_every <= 0 or covers the run: the reverse sweep then recomputes nothing
+    const bool all = checkpoint_every <= 0 || checkpoint_every >= nsteps;
+    const int K = all ? std::max(nsteps, 1) : checkpoint_every;
     const int nseg = nsteps > 0 ? (nsteps + K - 1) / K : 0;
-    PXB_TRY(dev_alloc(c, e.adj_ckpt, 2 * bytes * (size_t)std::max(nseg, 1)));
+    PXB_TRY(dev_alloc(c, e.adj_ckpt, all ? 0 : 2 * bytes * (size_t)std::max(nseg, 1)));
     PXB_TRY(dev_alloc(c, e.adj_seg, bytes * (size_t)K));
     for (int k = 0; k < 2; ++k) PXB_TRY(dev_alloc(c, e.adj_p[k], bytes + 64));
-    PXB_TRY(dev_alloc(c, e.adj_A, bytes));
-    PXB_TRY(dev_alloc(c, e.adj_R, bytes));
-    PXB_TRY(dev_alloc(c, e.adj_W, bytes));
+    PXB_TRY(dev_alloc(c, e.adj_u0, bytes));
     PXB_TRY(dev_alloc(c, e.adj_t, sizeof(double) * (size_t)std::max(nsteps, 1)));
-    PXB_TRY(dev_alloc(c, e.adj_dC, 4 * sizeof(double)));
     PXB_TRY(dev_alloc(c, e.adj_umax, sizeof(unsigned long long) * (size_t)std::max(nsteps, 1)));
-    PXB_CUDA_TRY(cudaMemsetAsync(e.adj_dC.p, 0, 4 * sizeof(double), c->stream));
     // step times t_{n+1}, accumulated as the forward loop does
     std::vector<double> th((size_t)std::max(nsteps, 1));
     double t = 0.0;
@@ -1526,11 +1549,12 @@ extern "C" int pxb_epf_adjoint_d(pxb_ctx *c, const double *u0_d, const double *v
     PXB_TRY(h2d(c, e.adj_t.p, th.data(), sizeof(double) * th.size()));
     const double *tdev = e.adj_t.as<double>();
     double *P[2] = {e.adj_p[0].as<double>(), e.adj_p[1].as<double>()};
-    double *ck = e.adj_ckpt.as<double>();
+    double *ck = e.adj_ckpt.as<double>(), *seg = e.adj_seg.as<double>();
     auto d2d = [&](void *dst, const void *src, size_t b) -> int {
         PXB_CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToDevice, c->stream));
         return PXB_OK;
     };
+    PXB_TRY(d2d(e.adj_u0.p, u0_d, bytes));
     // start: u^{-1} = u0 - dt v0 + dt^2/2 a(u0) with the frozen mask (the START mode of the lane-group kernel)
     {
         EpfArgs a = epf_args(c);
@@ -1542,41 +1566,80 @@ extern "C" int pxb_epf_adjoint_d(pxb_ctx *c, const double *u0_d, const double *v
         a.damage = 0;
         a.sc_bond = nullptr;
         const cudaError_t err = launch_epf(a, c->g.dim, e.precision == PXB_MIXED, EPF_START, 1, c->stream);
-        if (err != cudaSuccess) return cuda_fail(err, "adjoint start");
+        if (err != cudaSuccess) return cuda_fail(err, "recorded start");
         c->launches++;
         PXB_TRY(d2d(P[0], u0_d, bytes));
     }
-    // sweep 1: the forward loop, keeping (u^{sK}, u^{sK-1}) at the start of every segment
+    // the forward loop, keeping every state u^q (all) or the pair (u^{sK}, u^{sK-1}) at every segment start
     int cur = 0;
-    for (int s = 0; s < nseg; ++s) {
-        PXB_TRY(d2d(ck + (size_t)(2 * s) * nd, P[cur], bytes));
-        PXB_TRY(d2d(ck + (size_t)(2 * s + 1) * nd, P[cur ^ 1], bytes));
-        if (s == nseg - 1) break;  // the last segment is recomputed in the reverse sweep anyway
-        for (int q = s * K; q < (s + 1) * K; ++q) {
-            PXB_TRY(adj_step(c, P[cur], P[cur ^ 1], tdev, q, dt));
-            cur ^= 1;
+    for (int q = 0; q < nsteps; ++q) {
+        if (all) {
+            PXB_TRY(d2d(seg + (size_t)q * nd, P[cur], bytes));
+        } else if (q % K == 0) {
+            const size_t s = (size_t)(q / K);
+            PXB_TRY(d2d(ck + (2 * s) * nd, P[cur], bytes));
+            PXB_TRY(d2d(ck + (2 * s + 1) * nd, P[cur ^ 1], bytes));
         }
+        PXB_TRY(adj_step(c, P[cur], P[cur ^ 1], tdev, q, dt));
+        cur ^= 1;
     }
-    // reverse sweep
+    if (uN_d) PXB_TRY(d2d(uN_d, P[cur], bytes));
+    if (uNm1_d) PXB_TRY(d2d(uNm1_d, P[cur ^ 1], bytes));
+    e.rec_dt = dt;
+    e.rec_steps = nsteps;
+    e.rec_K = K;
+    e.rec_all = all;
+    return PXB_OK;
+}
+
+extern "C" int pxb_epf_adjoint_recorded_d(pxb_ctx *c, const double *ubar_N_d, const double *ubar_Nm1_d,
+                                          double *u0bar_d, double *v0bar_d, double *dC_d) {
+    PXB_TRY(need_epf(c, "pxb_epf_adjoint_recorded_d"));
+    EpfState &e = c->epf;
+    if (e.rec_steps < 0)
+        return fail(PXB_ERR_STATE, "pxb_epf_adjoint_recorded_d: no recorded forward loop (pxb_epf_record_d)");
+    if (!ubar_N_d || !u0bar_d) return fail(PXB_ERR_INVALID, "pxb_epf_adjoint_recorded_d: need dJ/du^N and dJ/du0");
+    PXB_TRY(ensure_grev(c));
+    if (e.adj_GR.p) {  // the frozen mask in reverse-bond order, for this sweep
+        PXB_TRY(dev_alloc(c, e.adj_HR, (size_t)std::max(1LL, c->g.nb)));
+        PXB_CUDA_TRY(launch_reverse_health(e.health.as<uint8_t>(), c->g.rev.as<int>(), e.adj_HR.as<uint8_t>(), c->g.nb,
+                                           c->stream));
+        PXB_TRY(check_launch(c, "reverse health"));
+    }
+    const size_t nd = (size_t)c->g.n * c->g.dim, bytes = sizeof(double) * nd;
+    const int nsteps = e.rec_steps, K = e.rec_K;
+    const double dt = e.rec_dt, dt2 = dt * dt;
+    const int nseg = nsteps > 0 ? (nsteps + K - 1) / K : 0;
+    PXB_TRY(dev_alloc(c, e.adj_A, bytes));
+    PXB_TRY(dev_alloc(c, e.adj_R, bytes));
+    PXB_TRY(dev_alloc(c, e.adj_W, bytes));
+    PXB_TRY(dev_alloc(c, e.adj_dC, 4 * sizeof(double)));
+    PXB_CUDA_TRY(cudaMemsetAsync(e.adj_dC.p, 0, 4 * sizeof(double), c->stream));
+    auto d2d = [&](void *dst, const void *src, size_t b) -> int {
+        PXB_CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToDevice, c->stream));
+        return PXB_OK;
+    };
+    const double *tdev = e.adj_t.as<double>();
+    double *P[2] = {e.adj_p[0].as<double>(), e.adj_p[1].as<double>()};
+    double *ck = e.adj_ckpt.as<double>(), *seg = e.adj_seg.as<double>();
     double *A = e.adj_A.as<double>(), *Rv = e.adj_R.as<double>(), *W = e.adj_W.as<double>();
-    double *seg = e.adj_seg.as<double>();
     PXB_TRY(d2d(A, ubar_N_d, bytes));
     if (ubar_Nm1_d) PXB_TRY(d2d(Rv, ubar_Nm1_d, bytes));
     else PXB_CUDA_TRY(cudaMemsetAsync(Rv, 0, bytes, c->stream));
     EpfArgs bc = epf_args(c);
     fill_bc(c, bc);
-    const double dt2 = dt * dt;
     for (int s = nseg - 1; s >= 0; --s) {
         const int q0 = s * K, q1 = std::min(nsteps, (s + 1) * K);
-        // recompute the segment's states u^{q0} .. u^{q1-1}
-        PXB_TRY(d2d(P[0], ck + (size_t)(2 * s) * nd, bytes));
-        PXB_TRY(d2d(P[1], ck + (size_t)(2 * s + 1) * nd, bytes));
-        cur = 0;
-        for (int q = q0; q < q1; ++q) {
-            PXB_TRY(d2d(seg + (size_t)(q - q0) * nd, P[cur], bytes));
-            if (q + 1 < q1) {
-                PXB_TRY(adj_step(c, P[cur], P[cur ^ 1], tdev, q, dt));
-                cur ^= 1;
+        if (!e.rec_all) {  // recompute the segment's states u^{q0} .. u^{q1-1} from its checkpoint
+            PXB_TRY(d2d(P[0], ck + (size_t)(2 * s) * nd, bytes));
+            PXB_TRY(d2d(P[1], ck + (size_t)(2 * s + 1) * nd, bytes));
+            int cur = 0;
+            for (int q = q0; q < q1; ++q) {
+                PXB_TRY(d2d(seg + (size_t)(q - q0) * nd, P[cur], bytes));
+                if (q + 1 < q1) {
+                    PXB_TRY(adj_step(c, P[cur], P[cur ^ 1], tdev, q, dt));
+                    cur ^= 1;
+                }
             }
         }
         for (int q = q1 - 1; q >= q0; --q) {
@@ -1587,9 +1650,19 @@ extern "C" int pxb_epf_adjoint_d(pxb_ctx *c, const double *u0_d, const double *v
         }
     }
     // the start: dJ/du0 = A + R + (da/du)^T (dt^2/2 R), dJ/dv0 = -dt R
-    PXB_TRY(adj_kernel(c, u0_d, Rv, 0.5 * dt2, 1.0, A, 1.0, u0bar_d, -dt, v0bar_d));
+    PXB_TRY(adj_kernel(c, e.adj_u0.as<double>(), Rv, 0.5 * dt2, 1.0, A, 1.0, u0bar_d, -dt, v0bar_d));
     if (dC_d) PXB_TRY(d2d(dC_d, e.adj_dC.p, 3 * sizeof(double)));
     return PXB_OK;
+}
+
+extern "C" int pxb_epf_adjoint_d(pxb_ctx *c, const double *u0_d, const double *v0_d, double dt, int nsteps,
+                                 int checkpoint_every, const double *ubar_N_d, const double *ubar_Nm1_d,
+                                 double *u0bar_d, double *v0bar_d, double *dC_d) {
+    PXB_TRY(need_epf(c, "pxb_epf_adjoint_d"));
+    if (!u0_d || !ubar_N_d || !u0bar_d || !(dt > 0.0) || nsteps < 0)
+        return fail(PXB_ERR_INVALID, "pxb_epf_adjoint_d: need u0, dJ/du^N, the dJ/du0 output, dt > 0, nsteps >= 0");
+    PXB_TRY(pxb_epf_record_d(c, u0_d, v0_d, dt, nsteps, checkpoint_every, nullptr, nullptr));
+    return pxb_epf_adjoint_recorded_d(c, ubar_N_d, ubar_Nm1_d, u0bar_d, v0bar_d, dC_d);
 }
 
 extern "C" int pxb_epf_force_adjoint(pxb_ctx *c, const double *u, const double *abar, double *ubar, double *dC) {

@@ -219,7 +219,9 @@ BatchSchedule batch_apply_schedule(int v) {
         case 4: return {16, 16, false};
         case 5: return {4, 16, true};
         case 6: return {4, 32, false};
-        default: return {16, 32, true};
+        case 7: return {16, 32, true};
+        case 8: return {4, 32, true};
+        default: return {8, 32, true};
     }
 }
 
@@ -248,6 +250,8 @@ static cudaError_t launch_ab_m(const BatchArgs &a, int variant, int dims, cudaSt
         case 5: return dims == 1 ? launch_ab<MIXED, 4, 16, 1>(a, s) : launch_ab<MIXED, 4, 16, 2>(a, s);
         case 6: return launch_ab<MIXED, 4, 32, 3>(a, s);
         case 7: return dims == 1 ? launch_ab<MIXED, 16, 32, 1>(a, s) : launch_ab<MIXED, 16, 32, 2>(a, s);
+        case 8: return dims == 1 ? launch_ab<MIXED, 4, 32, 1>(a, s) : launch_ab<MIXED, 4, 32, 2>(a, s);
+        case 9: return dims == 1 ? launch_ab<MIXED, 8, 32, 1>(a, s) : launch_ab<MIXED, 8, 32, 2>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }

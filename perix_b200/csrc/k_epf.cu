@@ -505,9 +505,20 @@ __global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) 
         }
         for (int t = a.off[m] + lane; t < a.off[m + 1]; t += kWarp) {
             const int j = __ldg(a.nbr + t);
-            const int r = __ldg(a.rev + t);
+            const int r = a.hrev ? 0 : __ldg(a.rev + t);
             double g[NC], f[DIM];
-            if (r >= 0 && a.health[r]) {
+            if (a.GR) {
+                // the reverse bond's operators and health from bond-ordered copies (coalesced; zero without a
+                // reverse bond): every load of the bond is issued up front, the masks applied afterwards
+                double gr[NC], Lj[DIM];
+                load_G<DIM, MIXED>(a.GR, a.nb, t, gr);
+                const bool hr = a.hrev ? a.hrev[t] != 0 : (r >= 0 && a.health[r]);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) Lj[d] = a.abar[(size_t)j * DIM + d] * lscale;
+                navier_apply<DIM>(gr, a.C11, a.C12, a.C66, Lj, f);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) U[d] += hr ? f[d] : 0.0;
+            } else if (r >= 0 && a.health[r]) {
                 double Lj[DIM];
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) Lj[d] = a.abar[(size_t)j * DIM + d] * lscale;
@@ -563,6 +574,41 @@ __global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) 
         for (int w = 0; w < WPB; ++w) v += s_dC[w][threadIdx.x];
         atomicAdd(a.dC + threadIdx.x, v);
     }
+}
+
+// ---- the Navier operators in reverse-bond order: GR[c][t] = G[c][rev t] (0 without a reverse bond) -------------
+template <typename T>
+__global__ void reverse_gather_kernel(const T *G, T *GR, const int *rev, long long nb, long long ldb, int nc) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb; t += (long long)gridDim.x * blockDim.x) {
+        const int r = rev[t];
+        for (int c = 0; c < nc; ++c) GR[(size_t)c * ldb + t] = r >= 0 ? G[(size_t)c * ldb + r] : T(0);
+    }
+}
+
+__global__ void reverse_health_kernel(const uint8_t *health, const int *rev, uint8_t *hr, long long nb) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb; t += (long long)gridDim.x * blockDim.x) {
+        const int r = rev[t];
+        hr[t] = r >= 0 ? health[r] : (uint8_t)0;
+    }
+}
+
+cudaError_t launch_reverse_health(const uint8_t *health, const int *rev, uint8_t *hr, long long nb, cudaStream_t s) {
+    const int grid = (int)std::min<long long>((nb + 255) / 256, 148LL * 16);
+    reverse_health_kernel<<<grid > 0 ? grid : 1, 256, 0, s>>>(health, rev, hr, nb);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reverse_gather(const void *G, void *GR, const int *rev, long long nb, long long ldb, int dim,
+                                  bool mixed, cudaStream_t s) {
+    const int nc = dim == 3 ? 6 : 3;
+    const int grid = (int)std::min<long long>((nb + 255) / 256, 148LL * 16);
+    if (mixed)
+        reverse_gather_kernel<float><<<grid > 0 ? grid : 1, 256, 0, s>>>(static_cast<const float *>(G),
+                                                                       static_cast<float *>(GR), rev, nb, ldb, nc);
+    else
+        reverse_gather_kernel<double><<<grid > 0 ? grid : 1, 256, 0, s>>>(static_cast<const double *>(G),
+                                                                         static_cast<double *>(GR), rev, nb, ldb, nc);
+    return cudaGetLastError();
 }
 
 // ---- transpose of the BC program (the adjoint of a step's BC pass) --------------------------------------------
@@ -660,23 +706,12 @@ cudaError_t launch_navier_pack(const void *G, void *P, long long ldb, int dim, b
     return cudaGetLastError();
 }
 
-cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int grid, cudaStream_t s) {
-    if (dim == 2) {
-        if (mixed) epf_adjoint_kernel<2, true><<<grid, kEpfThreads, 0, s>>>(a);
-        else epf_adjoint_kernel<2, false><<<grid, kEpfThreads, 0, s>>>(a);
-    } else {
-        if (mixed) epf_adjoint_kernel<3, true><<<grid, kEpfThreads, 0, s>>>(a);
-        else epf_adjoint_kernel<3, false><<<grid, kEpfThreads, 0, s>>>(a);
-    }
-    return cudaGetLastError();
-}
 
 // schedule variants (LPN lanes per node, UNR bonds per lane per pass); index = EpfArgs-independent id
 // persistent grid: every block resident (SM count x occupancy of this instantiation), capped by the work
 template <typename K>
-static int resident_grid(K kernel, int n, int nodes_per_block) {
-    static int cap = 0;  // one cache per kernel instantiation
-    if (cap == 0) {
+static int resident_grid(K kernel, int n, int nodes_per_block, int &cap) {
+    if (cap == 0) {  // cap: the caller's cache, one per kernel instantiation
         int dev = 0, sms = 148, per_sm = 1;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -687,10 +722,26 @@ static int resident_grid(K kernel, int n, int nodes_per_block) {
     return (int)(need < cap ? (need > 0 ? need : 1) : cap);
 }
 
+// the adjoint kernel's own resident grid (one warp per node, grid-stride), capped by the node count
+template <int DIM, bool MIXED>
+static cudaError_t launch_adj(const EpfAdjArgs &a, cudaStream_t s) {
+    auto k = epf_adjoint_kernel<DIM, MIXED>;
+    static int cap = 0;
+    const int grid = resident_grid(k, a.n, kEpfThreads / kWarp, cap);
+    k<<<grid, kEpfThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int, cudaStream_t s) {
+    if (dim == 2) return mixed ? launch_adj<2, true>(a, s) : launch_adj<2, false>(a, s);
+    return mixed ? launch_adj<3, true>(a, s) : launch_adj<3, false>(a, s);
+}
+
 template <int DIM, bool MIXED, int MODE, int LPN, int UNR>
 static cudaError_t launch_m(const EpfArgs &a, cudaStream_t s) {
     auto k = epf_kernel<DIM, MIXED, MODE, LPN, UNR>;
-    const int grid = resident_grid(k, a.n, (kEpfThreads / kWarp) * (kWarp / LPN));
+    static int cap = 0;
+    const int grid = resident_grid(k, a.n, (kEpfThreads / kWarp) * (kWarp / LPN), cap);
     k<<<grid, kEpfThreads, 0, s>>>(a);
     return cudaGetLastError();
 }
@@ -698,7 +749,8 @@ static cudaError_t launch_m(const EpfArgs &a, cudaStream_t s) {
 template <int DIM, bool MIXED, int MODE, int NB, int UNR>
 static cudaError_t launch_s(const EpfArgs &a, cudaStream_t s) {
     auto k = epf_stream_kernel<DIM, MIXED, MODE, NB, UNR>;
-    const int grid = resident_grid(k, a.n, NB);
+    static int cap = 0;
+    const int grid = resident_grid(k, a.n, NB, cap);
     k<<<grid, kEpfThreads, 0, s>>>(a);
     return cudaGetLastError();
 }

@@ -82,6 +82,15 @@ __device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, unsign
         : "memory");
 }
 
+// bulk prefetch of [src, src + bytes) into L2 (no shared memory, no barrier); src 16-byte aligned, bytes % 16 == 0
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_prefetch_l2_hint(const void *src, unsigned bytes, unsigned long long policy) {
+    asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;" ::"l"(src), "r"(bytes), "l"(policy)
+                 : "memory");
+}
+
 __device__ __forceinline__ unsigned long long policy_evict_first() {
     unsigned long long p;
     asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
@@ -107,16 +116,16 @@ __device__ __forceinline__ double dot_rn_t(const double *a, const double *b) {
 }
 
 // P = packed Navier coefficients of the bond (navier_pack_kernel): 2D (p11, p22, pxy), 3D (p11, p22, p33,
-// p12, p13, p23); f = P e with P symmetric
+// p12, p13, p23), symmetric; L += P e as a chain of FMAs per component
 template <int DIM>
-__device__ __forceinline__ void navier_packed_t(const double *p, const double *e, double *out) {
+__device__ __forceinline__ void navier_acc_t(const double *p, const double *e, double *L) {
     if constexpr (DIM == 3) {
-        out[0] = p[0] * e[0] + p[3] * e[1] + p[4] * e[2];
-        out[1] = p[3] * e[0] + p[1] * e[1] + p[5] * e[2];
-        out[2] = p[4] * e[0] + p[5] * e[1] + p[2] * e[2];
+        L[0] = fma(p[0], e[0], fma(p[3], e[1], fma(p[4], e[2], L[0])));
+        L[1] = fma(p[3], e[0], fma(p[1], e[1], fma(p[5], e[2], L[1])));
+        L[2] = fma(p[4], e[0], fma(p[5], e[1], fma(p[2], e[2], L[2])));
     } else {
-        out[0] = p[0] * e[0] + p[2] * e[1];
-        out[1] = p[2] * e[0] + p[1] * e[1];
+        L[0] = fma(p[0], e[0], fma(p[2], e[1], L[0]));
+        L[1] = fma(p[2], e[0], fma(p[1], e[1], L[1]));
     }
 }
 
@@ -129,15 +138,16 @@ __device__ __forceinline__ double pick_t(const double *v, int d) {
     return r;
 }
 
-// stage layout (bytes, all sections 16-aligned): G[NC][maxb] | nbr[maxb] | health[maxb] | off[NT+16] |
-// pos[NT] | u[NT*DIM + 2] | uprev[NT*DIM + 2] | (MIXED and XI) xi[DIM][maxb] FP32 bond vectors
-template <int DIM, bool MIXED, int NT, bool XI = false>
+// stage layout (bytes, all sections 16-aligned): G[NC][maxb] (not with PL2) | nbr[maxb] | health[maxb] |
+// off[NT+16] | pos[NT] | u[NT*DIM + 2] | uprev[NT*DIM + 2] | (XI) xi[DIM][maxb] FP32 bond vectors
+template <int DIM, bool MIXED, int NT, bool XI = false, bool PL2 = false>
 struct StageLayout {
     static constexpr int NC = (DIM == 3) ? 6 : 3;
     static constexpr int ES = MIXED ? 4 : 8;
     static constexpr int PS = (DIM == 3) ? 32 : 16;
     __host__ __device__ static unsigned g_off(int) { return 0; }
-    __host__ __device__ static unsigned nbr_off(int maxb) { return (unsigned)(NC * maxb * ES); }
+    // PL2: the coefficients are not staged (prefetched into L2 and loaded per lane)
+    __host__ __device__ static unsigned nbr_off(int maxb) { return PL2 ? 0u : (unsigned)(NC * maxb * ES); }
     __host__ __device__ static unsigned h_off(int maxb) { return nbr_off(maxb) + (unsigned)maxb * 4u; }
     __host__ __device__ static unsigned off_off(int maxb) { return h_off(maxb) + (unsigned)maxb; }
     __host__ __device__ static unsigned pos_off(int maxb) { return off_off(maxb) + (unsigned)(NT + 16) * 4u; }
@@ -182,14 +192,20 @@ __device__ __forceinline__ int break_fp64(const PosT &xj, const PosT &xi, const 
 
 }  // namespace
 
-template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB, bool XI>
+// FLAGS bit 0 (XI): stage FP32 bond vectors for an FP32 stretch pre-test (both precisions); bit 1 (PL2): do not stage
+// the packed coefficients but prefetch each tile's coefficient ranges into L2 with bulk prefetches as its copies are
+// issued, and load them per lane at the start of each pass (the stage then holds ids, health and node rows only, so
+// shared memory no longer limits the resident warps)
+template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB, int FLAGS>
 __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
-    constexpr bool XS = XI;  // staged FP32 bond vectors and the FP32 stretch pre-test (both precisions)
+    constexpr bool XI = (FLAGS & 1) != 0;
+    constexpr bool PL2 = (FLAGS & 2) != 0;
+    constexpr bool XS = XI;
     using PosT = typename Vec<DIM>::T;
     using GT = typename std::conditional<MIXED, float, double>::type;
     constexpr int GPW = kWarp / LPN;
     constexpr int NT = WPB * GPW;
-    using SL = StageLayout<DIM, MIXED, NT, XI>;
+    using SL = StageLayout<DIM, MIXED, NT, XI, PL2>;
     constexpr int NC = SL::NC;
 
     extern __shared__ __align__(128) unsigned char smem[];
@@ -213,6 +229,9 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     const GT *Pg = static_cast<const GT *>(a.P);
     const bool rate = a.rate != 0;  // RATE: the acceleration out, no u^{n-1} stream, no BC pass
     const float sc_hi2f = (float)a.sc_hi2, sc_lo2f = (float)a.sc_lo2;
+    // FP64 clear-hold test with the rounding band folded into the thresholds: y2 < ((1+sc)^2 - 1e-6) r2 and
+    // y2 > ((1-sc)^2 + 1e-6) r2 (the rounding of these two constants is far inside the band)
+    const double hi_band = a.sc_hi2 - 1.0e-6, lo_band = a.sc_lo2 + 1.0e-6;
 
     const int ntiles = (a.n + NT - 1) / NT;
     const int mycount = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -233,8 +252,8 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         const unsigned bytes_pos = (unsigned)cnt * SL::PS;
         const unsigned bytes_u = up16((unsigned)cnt * DIM * 8u);
         const unsigned bytes_up = rate ? 0u : bytes_u;
-        const unsigned total = NC * bytes_g + bytes_n + bytes_h + bytes_off + bytes_pos + bytes_u + bytes_up +
-                               (XS ? (unsigned)DIM * bytes_n : 0u);
+        const unsigned total = (PL2 ? 0u : NC * bytes_g) + bytes_n + bytes_h + bytes_off + bytes_pos + bytes_u +
+                               bytes_up + (XS ? (unsigned)DIM * bytes_n : 0u);
         s_t0a[st] = t0a;
         s_last[st] = k;
         fence_proxy_async();
@@ -242,14 +261,18 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         if (a.evict_first) {
             const unsigned long long ef = policy_evict_first();
 #pragma unroll
-            for (int c = 0; c < NC; ++c)
-                bulk_g2s_hint(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st], ef);
+            for (int c = 0; c < NC; ++c) {
+                if constexpr (PL2) bulk_prefetch_l2_hint(Pg + (size_t)c * a.nb + t0a, bytes_g, ef);
+                else bulk_g2s_hint(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st], ef);
+            }
             bulk_g2s_hint(base + SL::nbr_off(maxb), a.nbr + t0a, bytes_n, &bar[st], ef);
             bulk_g2s_hint(base + SL::h_off(maxb), a.health + t0a, bytes_h, &bar[st], ef);
         } else {
 #pragma unroll
-            for (int c = 0; c < NC; ++c)
-                bulk_g2s(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st]);
+            for (int c = 0; c < NC; ++c) {
+                if constexpr (PL2) bulk_prefetch_l2(Pg + (size_t)c * a.nb + t0a, bytes_g);
+                else bulk_g2s(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st]);
+            }
             bulk_g2s(base + SL::nbr_off(maxb), a.nbr + t0a, bytes_n, &bar[st]);
             bulk_g2s(base + SL::h_off(maxb), a.health + t0a, bytes_h, &bar[st]);
         }
@@ -329,12 +352,22 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         double ui[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) ui[d] = 0.0;
+        // the node's BC words, loaded before the bond passes so that their latency overlaps them
+        unsigned own_bits = 0;
+        int bce0 = 0, bce1 = 0;
         if (act) {
             b0 = sOff[li] - t0a;
             b1 = sOff[li + 1] - t0a;
             xi = sPos[li];
 #pragma unroll
             for (int d = 0; d < DIM; ++d) ui[d] = sU[li * DIM + d];
+            if (!rate) {
+                if (a.bc_own) own_bits = __ldg(a.bc_own + i);
+                if (a.bc_off) {
+                    bce0 = __ldg(a.bc_off + i);
+                    bce1 = __ldg(a.bc_off + i + 1);
+                }
+            }
         }
         double L[DIM];
 #pragma unroll
@@ -348,25 +381,32 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
                 const int t = t0 + q * LPN;
                 const bool ok = t < b1;
                 h[q] = ok ? sH[t] : (uint8_t)0;
-                j[q] = ok ? sN[t] : 0;
+                j[q] = ok ? sN[t] : i;  // past the family: the node itself (a valid gather, masked by h = 0)
             }
+            // PL2: the pass's coefficients from L2 (prefetched with the tile), issued before the gathers
+            GT pv[PL2 ? UNR : 1][NC];
+            if constexpr (PL2) {
+                const GT *Pt = Pg + t0a;
+#pragma unroll
+                for (int q = 0; q < UNR; ++q) {
+                    const int t = t0 + q * LPN;
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) pv[q][c] = t < b1 ? __ldcs(Pt + (size_t)c * a.nb + t) : GT(0);
+                }
+            }
+            // the gathers are unconditional (broken bonds and the tail read valid rows and are masked below)
             PosT xj[UNR];
             double uj[UNR][DIM];
 #pragma unroll
             for (int q = 0; q < UNR; ++q) {
-                xj[q] = PosT{};
+                if constexpr (!XS) xj[q] = ldg_vec(pos + j[q]);
+                if constexpr (DIM == 2) {
+                    const double2 v = __ldg(reinterpret_cast<const double2 *>(a.u) + j[q]);
+                    uj[q][0] = v.x;
+                    uj[q][1] = v.y;
+                } else {
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) uj[q][d] = 0.0;
-                if (h[q]) {
-                    if constexpr (!XS) xj[q] = ldg_vec(pos + j[q]);
-                    if constexpr (DIM == 2) {
-                        const double2 v = __ldg(reinterpret_cast<const double2 *>(a.u) + j[q]);
-                        uj[q][0] = v.x;
-                        uj[q][1] = v.y;
-                    } else {
-#pragma unroll
-                        for (int d = 0; d < DIM; ++d) uj[q][d] = __ldg(a.u + (size_t)j[q] * DIM + d);
-                    }
+                    for (int d = 0; d < DIM; ++d) uj[q][d] = __ldg(a.u + (size_t)j[q] * DIM + d);
                 }
             }
             // every bond of the pass as an independent stream: a squared comparison accepts the bonds that clearly
@@ -404,15 +444,20 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
                         fast = (y2f - sc_hi2f * r2f < -bandf) && (a.tension_only || sc_lo2f * r2f - y2f < -bandf);
                         fast = fast || !(r2f > 0.f);
                     } else {
+                        // contracted FP64 (a few ulps of r2 and y2, far inside the 1e-6 r2 band)
                         double xv[DIM], yv[DIM];
-                        xv[0] = __dsub_rn(xj[q].x, xi.x);
-                        xv[1] = __dsub_rn(xj[q].y, xi.y);
-                        if constexpr (DIM == 3) xv[2] = __dsub_rn(xj[q].z, xi.z);
+                        xv[0] = xj[q].x - xi.x;
+                        xv[1] = xj[q].y - xi.y;
+                        if constexpr (DIM == 3) xv[2] = xj[q].z - xi.z;
 #pragma unroll
-                        for (int d = 0; d < DIM; ++d) yv[d] = __dadd_rn(xv[d], e[q][d]);
-                        const double r2 = dot_rn_t<DIM>(xv, xv), y2 = dot_rn_t<DIM>(yv, yv);
-                        const double band = 1.0e-6 * r2;
-                        fast = (y2 - a.sc_hi2 * r2 < -band) && (a.tension_only || a.sc_lo2 * r2 - y2 < -band);
+                        for (int d = 0; d < DIM; ++d) yv[d] = xv[d] + e[q][d];
+                        double r2 = xv[0] * xv[0] + xv[1] * xv[1];
+                        double y2 = yv[0] * yv[0] + yv[1] * yv[1];
+                        if constexpr (DIM == 3) {
+                            r2 = fma(xv[2], xv[2], r2);
+                            y2 = fma(yv[2], yv[2], y2);
+                        }
+                        fast = (y2 < hi_band * r2) && (a.tension_only || y2 > lo_band * r2);
                         fast = fast || !(r2 > 0.0);
                     }
                 }
@@ -441,11 +486,11 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
                 const int t = t0 + q * LPN;
                 double pd[NC];
 #pragma unroll
-                for (int c = 0; c < NC; ++c) pd[c] = (double)sP[(size_t)c * maxb + t];
-                double f[DIM];
-                navier_packed_t<DIM>(pd, e[q], f);
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) L[d] += f[d];
+                for (int c = 0; c < NC; ++c) {
+                    if constexpr (PL2) pd[c] = (double)pv[q < (PL2 ? UNR : 1) ? q : 0][c];
+                    else pd[c] = (double)sP[(size_t)c * maxb + t];
+                }
+                navier_acc_t<DIM>(pd, e[q], L);
             }
         }
 #pragma unroll
@@ -454,13 +499,15 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         double unew = 0.0;
         if (act && gl < DIM) {
             const int d = gl;
-            const double acc = __ddiv_rn(__dadd_rn(pick_t<DIM>(L, d), a.b[d]), a.rho);
+            // the body force by selects (a runtime index into the parameter array would go through local memory)
+            const double bd = d == 0 ? a.b[0] : (d == 1 ? a.b[1] : a.b[DIM - 1]);
+            const double acc = __ddiv_rn(__dadd_rn(pick_t<DIM>(L, d), bd), a.rho);
             const size_t kk = (size_t)i * DIM + d;
             if (rate) {
                 a.accel[kk] = acc;
             } else {
                 unew = cd_next(pick_t<DIM>(ui, d), sUp[li * DIM + d], acc, a.dt2, a.var_step, a.cv_rho, a.cv_w);
-                const bool owned = a.bc_own && ((a.bc_own[i] >> d) & 1);
+                const bool owned = (own_bits >> d) & 1u;
                 if (!owned) {
                     a.u_other[kk] = unew;
                     umax = max_nan(umax, fabs(unew));
@@ -471,8 +518,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
             double un[DIM];
 #pragma unroll
             for (int d = 0; d < DIM; ++d) un[d] = __shfl_sync(kFull, unew, grp * LPN + d);
-            const int e0 = act ? a.bc_off[i] : 0, e1 = act ? a.bc_off[i + 1] : 0;
-            for (int e = e0 + gl; e < e1; e += LPN) {
+            for (int e = bce0 + gl; e < bce1; e += LPN) {
                 const int comp = a.bc_comp[e];
                 const int form = a.bc_form[e];
                 const double g1 = __dadd_rn(a.bc_val[e], __dmul_rn(a.bc_vel[e], t_new));
@@ -526,11 +572,11 @@ static LaunchShape g_last_shape{0, 0, 0};
 
 LaunchShape epf_tma_last_shape() { return g_last_shape; }
 
-template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB, bool XI>
+template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB, int FLAGS>
 static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
     constexpr int NT = WPB * (kWarp / LPN);
-    using SL = StageLayout<DIM, MIXED, NT, XI>;
-    auto k = epf_tma_kernel<DIM, MIXED, LPN, UNR, S, MINB, WPB, XI>;
+    using SL = StageLayout<DIM, MIXED, NT, (FLAGS & 1) != 0, (FLAGS & 2) != 0>;
+    auto k = epf_tma_kernel<DIM, MIXED, LPN, UNR, S, MINB, WPB, FLAGS>;
     const size_t smem = (size_t)S * SL::bytes(a.maxb);
     static size_t configured = 0;
     if (smem > configured) {
@@ -574,8 +620,9 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
 }
 
 // Staged configurations: lanes per node, bonds per lane per pass, stages, minimum resident blocks (launch
-// bounds), warps per block, staged FP32 bond vectors (either precision: the stretch pre-test reads them instead of
-// gathering neighbour positions, for 8 (2D) / 12 (3D) more staged bytes per bond).  A tile is WPB * 32/LPN nodes.
+// bounds), warps per block, flags (1: staged FP32 bond vectors for the stretch pre-test, 8 (2D) / 12 (3D) more
+// staged bytes per bond; 2: coefficients prefetched into L2 and loaded per lane instead of staged).  A tile is
+// WPB * 32/LPN nodes.
 struct TmaCfg {
     int lpn, unr, stages, minb, wpb, xi;
 };
@@ -583,12 +630,12 @@ struct TmaCfg {
     X(0, 16, 2, 4, 1, 8, 0) X(1, 8, 1, 3, 1, 8, 0) X(2, 8, 4, 3, 1, 8, 0) X(3, 8, 2, 2, 3, 8, 0)                 \
     X(4, 8, 1, 2, 4, 8, 0) X(5, 8, 2, 2, 4, 8, 0) X(6, 4, 2, 2, 6, 4, 0) X(7, 4, 4, 2, 4, 4, 0)                  \
     X(8, 8, 2, 2, 8, 4, 0) X(9, 4, 2, 2, 3, 8, 0) X(10, 4, 2, 2, 6, 4, 1) X(11, 4, 4, 2, 4, 4, 1)                \
-    X(12, 8, 2, 2, 6, 4, 1)
+    X(12, 8, 2, 2, 6, 4, 1) X(13, 8, 2, 3, 3, 8, 2) X(14, 4, 2, 3, 3, 8, 2) X(15, 4, 4, 3, 2, 8, 3)
 #define PXB_TMA3(X)                                                                                               \
-    X(0, 32, 2, 2, 1, 8, 0) X(1, 32, 4, 2, 1, 8, 0) X(2, 32, 1, 3, 1, 8, 0) X(3, 16, 2, 2, 1, 8, 0)              \
+    X(0, 32, 2, 2, 1, 8, 0) X(1, 16, 2, 3, 2, 8, 2) X(2, 32, 1, 3, 1, 8, 0) X(3, 16, 2, 2, 1, 8, 0)              \
     X(4, 16, 1, 2, 2, 8, 0) X(5, 32, 2, 2, 2, 8, 0) X(6, 32, 2, 2, 2, 4, 1) X(7, 32, 1, 2, 4, 4, 1)              \
-    X(8, 16, 2, 2, 2, 4, 1) X(9, 16, 1, 2, 4, 4, 1) X(10, 16, 2, 3, 2, 4, 1) X(11, 32, 2, 3, 2, 4, 1)            \
-    X(12, 16, 1, 3, 4, 4, 1)
+    X(8, 16, 2, 2, 2, 4, 1) X(9, 16, 1, 3, 3, 8, 2) X(10, 32, 1, 3, 3, 8, 3) X(11, 32, 2, 3, 2, 4, 1)            \
+    X(12, 32, 1, 4, 3, 8, 2) X(13, 32, 2, 3, 2, 8, 2) X(14, 32, 1, 3, 3, 8, 2) X(15, 32, 1, 3, 6, 4, 2)
 #define PXB_CFG(i, l, u, st, mb, w, x) {l, u, st, mb, w, x},
 static constexpr TmaCfg kTma2[kEpfTmaConfigs] = {PXB_TMA2(PXB_CFG)};
 static constexpr TmaCfg kTma3[kEpfTmaConfigs] = {PXB_TMA3(PXB_CFG)};
@@ -601,14 +648,14 @@ int epf_tma_tile_nodes(int dim, int which) {
     return c.wpb * (kWarp / c.lpn);
 }
 
-template <int DIM, bool MIXED, bool XI>
+template <int DIM, bool MIXED, bool XI, bool PL2>
 static size_t tma_stage_bytes(int nt, int maxb) {
     switch (nt) {
-        case 4: return StageLayout<DIM, MIXED, 4, XI>::bytes(maxb);
-        case 8: return StageLayout<DIM, MIXED, 8, XI>::bytes(maxb);
-        case 16: return StageLayout<DIM, MIXED, 16, XI>::bytes(maxb);
-        case 32: return StageLayout<DIM, MIXED, 32, XI>::bytes(maxb);
-        default: return StageLayout<DIM, MIXED, 64, XI>::bytes(maxb);  // 64 nodes (LPN 4 x 8 warps)
+        case 4: return StageLayout<DIM, MIXED, 4, XI, PL2>::bytes(maxb);
+        case 8: return StageLayout<DIM, MIXED, 8, XI, PL2>::bytes(maxb);
+        case 16: return StageLayout<DIM, MIXED, 16, XI, PL2>::bytes(maxb);
+        case 32: return StageLayout<DIM, MIXED, 32, XI, PL2>::bytes(maxb);
+        default: return StageLayout<DIM, MIXED, 64, XI, PL2>::bytes(maxb);  // 64 nodes (LPN 4 x 8 warps)
     }
 }
 
@@ -616,7 +663,13 @@ template <int DIM, bool MIXED>
 static size_t tma_smem_dm(int which, int maxb) {
     const TmaCfg c = DIM == 3 ? kTma3[which] : kTma2[which];
     const int nt = c.wpb * (kWarp / c.lpn);
-    const size_t per = c.xi ? tma_stage_bytes<DIM, MIXED, true>(nt, maxb) : tma_stage_bytes<DIM, MIXED, false>(nt, maxb);
+    size_t per = 0;
+    switch (c.xi) {
+        case 0: per = tma_stage_bytes<DIM, MIXED, false, false>(nt, maxb); break;
+        case 1: per = tma_stage_bytes<DIM, MIXED, true, false>(nt, maxb); break;
+        case 2: per = tma_stage_bytes<DIM, MIXED, false, true>(nt, maxb); break;
+        default: per = tma_stage_bytes<DIM, MIXED, true, true>(nt, maxb); break;
+    }
     return (size_t)c.stages * per;
 }
 
@@ -626,9 +679,9 @@ size_t epf_tma_smem(int dim, bool mixed, int which, int maxb) {
 }
 
 #define PXB_CASE2(i, l, u, st, mb, w, x) \
-    case i: return launch_tma<2, MIXED, l, u, st, mb, w, (x != 0)>(a, s);
+    case i: return launch_tma<2, MIXED, l, u, st, mb, w, x>(a, s);
 #define PXB_CASE3(i, l, u, st, mb, w, x) \
-    case i: return launch_tma<3, MIXED, l, u, st, mb, w, (x != 0)>(a, s);
+    case i: return launch_tma<3, MIXED, l, u, st, mb, w, x>(a, s);
 template <int DIM, bool MIXED>
 static cudaError_t launch_tma_dm(const EpfArgs &a, int which, cudaStream_t s) {
     if constexpr (DIM == 3) {

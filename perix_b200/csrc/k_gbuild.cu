@@ -446,7 +446,9 @@ BatchSchedule batch_gbuild_schedule(int v) {
         case 4: return {8, 16, false};
         case 5: return {8, 32, true};
         case 6: return {32, 32, false, true};
-        default: return {32, 32, true, true};
+        case 7: return {32, 32, true, true};
+        case 8: return {32, 32, false, true, true};
+        default: return {8, 32, true, true, false, true};
     }
 }
 
@@ -479,7 +481,9 @@ static cudaError_t launch_gb_m(const BatchArgs &a, int variant, int dims, cudaSt
 
 cudaError_t launch_gbuild_batch(const BatchArgs &a, bool mixed, int variant, int dims, cudaStream_t s) {
     const BatchSchedule sch = batch_gbuild_schedule(variant);
-    if (sch.warp) return launch_gbuild_batch_warp(a, mixed, sch.split, dims, s);
+    if (sch.hybrid && dims == 1)  // the 2D launch of the hybrid schedule: lane groups (FP64 sums for MIXED)
+        return mixed ? launch_gb<true, 8, 32, 1, true>(a, s) : launch_gb<false, 8, 32, 1, false>(a, s);
+    if (sch.warp) return launch_gbuild_batch_warp(a, mixed, sch.split, dims, sch.acc, s);
     return mixed ? launch_gb_m<true>(a, variant, dims, s) : launch_gb_m<false>(a, variant, dims, s);
 }
 

@@ -9,8 +9,8 @@
 //           are formed as the pairs are exchanged; after the five halvings each lane holds the chunk sums of at
 //           most ceil(NE/32) entries and adds them to its accumulators;
 //   solve   the entries go to shared memory, the warp factors A = L D L^T (right-looking, a row per lane), lane k
-//           solves column k of X = A^-1 diag(q!), takes one step of iterative refinement and the reference's
-//           max-norm consistency test (src/MathUtils/MatrixXd.cpp:40-47) decides degeneracy;
+//           solves column k of X = A^-1 diag(q!) (with one step of iterative refinement above nine monomials) and
+//           the reference's max-norm consistency test (src/MathUtils/MatrixXd.cpp:40-47) decides degeneracy;
 //   pass 2  one bond per lane again: op_k = (sum_p X[p][k] m_p) bw / delta^|q_k| for every slot k, written as the
 //           AoS operator vector and/or the SoA Navier subset; MIXED stores FP32 (sums stay FP64) and, at order 2,
 //           the per-node first moments of the stored second-derivative operators (GBuildArgs::defect).
@@ -18,6 +18,7 @@
 // uses its own delta_i and spacing, and bonds longer than delta_i stay out of its moment system and get zero
 // operators (CalcPDOperators.cpp:113-147, 307-354).
 #include <cfloat>
+#include <cstddef>
 
 #include "k_kernels.h"
 #include "pxb_common.cuh"
@@ -98,20 +99,34 @@ struct BondGeo {
     double dx, dy, dz, bw;
 };
 
+// per-node constants of the weight: delta, 4/delta^2, the rim spacing and the squared inner radius of the rim
+// (delta - dx_char/2)^2 (-1 when that radius is not positive: every bond is a rim bond)
+struct NodeWeight {
+    double delta, four_inv_d2, dxc, rim2;
+    __device__ __forceinline__ NodeWeight(double d, double dx) : delta(d), four_inv_d2(4.0 / (d * d)), dxc(dx) {
+        const double ri = d - 0.5 * dx;
+        rim2 = (dx > 0.0 && ri > 0.0) ? ri * ri : -1.0;
+    }
+};
+
 // bond t of node i: the bond vector and the weight bw = w(|xi|) vc(|xi|) V_j (0 when the bond is skipped: zero
-// length, outside the node's own horizon, or a non-positive weight)
+// length, outside the node's own horizon, or a non-positive weight).  w = exp(-(2|xi|/delta)^2) is evaluated from
+// |xi|^2 (a few ulps from the reference's rounding of 2|xi|/delta); |xi| itself is formed only for rim bonds and
+// for the own-horizon test
 template <int DIM, typename PosT>
-__device__ __forceinline__ BondGeo bond_geo(const GBuildArgs &a, const PosT *pos, const PosT &xi, int t, double delta,
-                                            double dxc, bool own_horizon) {
+__device__ __forceinline__ BondGeo bond_geo(const GBuildArgs &a, const PosT *pos, const PosT &xi, int t,
+                                            const NodeWeight &nw, bool own_horizon) {
     BondGeo g{0.0, 0.0, 0.0, 0.0};
     const int j = a.nbr[t];
     const PosT xj = pos[j - a.node_base];
     g.dx = xj.x - xi.x;
     g.dy = xj.y - xi.y;
     if constexpr (DIM == 3) g.dz = xj.z - xi.z;
-    const double xn = sqrt(g.dx * g.dx + g.dy * g.dy + g.dz * g.dz);
-    if (xn > 0.0 && !(own_horizon && xn > delta)) {
-        const double bw = bond_weight(xn, delta) * rim_correction(xn, delta, dxc) * a.vol[j];
+    const double r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz;
+    if (r2 > 0.0 && !(own_horizon && sqrt(r2) > nw.delta)) {
+        double bw = exp(-(r2 * nw.four_inv_d2));
+        if (nw.dxc > 0.0 && r2 > nw.rim2) bw *= rim_correction(sqrt(r2), nw.delta, nw.dxc);
+        bw *= a.vol[j];
         if (bw > 0.0) g.bw = bw;
     }
     return g;
@@ -124,13 +139,24 @@ __device__ __forceinline__ BondGeo bond_geo(const GBuildArgs &a, const PosT *pos
 template <int NOP>
 struct WarpNodeSmem {
     static constexpr int NP = (NOP + 1) & ~1;
-    double bw[kBwCache];
-    double A[NOP * NOP];
-    double L[NOP * NOP];
-    double X[NOP * NP];
+    // bond vectors cached for pass 2 too (up to nine monomials; larger systems gather them again)
+    static constexpr bool CACHE_X = NOP <= 9;
+    static constexpr int XC = CACHE_X ? kBwCache : 2;
+    // every section starts on a 16-byte boundary (X is read as double2)
+    alignas(16) double bw[kBwCache];
+    alignas(16) double xc[3 * XC];
+    alignas(16) double A[NOP * NOP];
+    alignas(16) double L[NOP * NOP];
+    alignas(16) double X[NOP * NP];
+    alignas(16) double invD[NP];  // 1 / D of the L D L^T factorisation
 };
+static_assert(offsetof(WarpNodeSmem<14>, X) % 16 == 0 && offsetof(WarpNodeSmem<19>, X) % 16 == 0 &&
+                  offsetof(WarpNodeSmem<9>, X) % 16 == 0 && offsetof(WarpNodeSmem<5>, X) % 16 == 0,
+              "X rows are read as double2");
 
-template <int DIM, int ORDER, bool MIXED>
+// ACC: each lane keeps its own moment sums over all the node's chunks and the warp reduce-scatters them once per
+// node (NE accumulators a lane) instead of once per 32-bond chunk
+template <int DIM, int ORDER, bool MIXED, bool ACC = false>
 __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int lane,
                                                  WarpNodeSmem<nop_of(DIM, ORDER)> &sm) {
     constexpr QTable<DIM, ORDER> Q{};
@@ -146,6 +172,7 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     const double delta = own_h ? a.node_delta[i - a.node_base] : a.delta;
     const double dxc = own_h ? a.node_dxc[i - a.node_base] : a.dx_char;
     const double inv_delta = 1.0 / delta;
+    constexpr bool XCACHE = WarpNodeSmem<NOP>::CACHE_X;
     const int b0 = a.off[i], b1 = a.off[i + 1];
     const PosT xi = pos[i - a.node_base];
 
@@ -153,17 +180,34 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     double acc[L5];
 #pragma unroll
     for (int s = 0; s < L5; ++s) acc[s] = 0.0;
+    double lacc[ACC ? NE : 1];
+#pragma unroll
+    for (int e = 0; e < (ACC ? NE : 1); ++e) lacc[e] = 0.0;
     int usable = 0;
+    {
+    const NodeWeight nw(delta, dxc);
     for (int c0 = b0; c0 < b1; c0 += kWarp) {
         const int t = c0 + lane;
         BondGeo g{0.0, 0.0, 0.0, 0.0};
-        if (t < b1) g = bond_geo<DIM>(a, pos, xi, t, delta, dxc, own_h);
-        if (t < b1 && t - b0 < kBwCache) sm.bw[t - b0] = g.bw;
+        if (t < b1) g = bond_geo<DIM>(a, pos, xi, t, nw, own_h);
+        if (t < b1 && t - b0 < kBwCache) {
+            sm.bw[t - b0] = g.bw;
+            if constexpr (XCACHE) {
+                sm.xc[3 * (t - b0)] = g.dx;
+                sm.xc[3 * (t - b0) + 1] = g.dy;
+                sm.xc[3 * (t - b0) + 2] = g.dz;
+            }
+        }
         usable += g.bw > 0.0 ? 1 : 0;
         double m[NOP], wm[NOP];
         monomials<DIM, ORDER, double>(g.dx * inv_delta, g.dy * inv_delta, g.dz * inv_delta, m);
 #pragma unroll
         for (int k = 0; k < NOP; ++k) wm[k] = g.bw * m[k];
+        if constexpr (ACC) {
+#pragma unroll
+            for (int e = 0; e < NE; ++e) lacc[e] = fma(wm[T.p[e]], m[T.q[e]], lacc[e]);
+            continue;
+        }
         // first halving with the products formed as they are exchanged
         double v1[L1];
         {
@@ -186,6 +230,15 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         rs_level<L4, 1>(v4, v5, (lane & 1) != 0);
 #pragma unroll
         for (int s = 0; s < L5; ++s) acc[s] += v5[s];
+    }
+    }
+    if constexpr (ACC) {  // the node's one reduce-scatter
+        double v1[L1], v2[L2], v3[L3], v4[L4];
+        rs_level<NE, 16>(lacc, v1, (lane & 16) != 0);
+        rs_level<L1, 8>(v1, v2, (lane & 8) != 0);
+        rs_level<L2, 4>(v2, v3, (lane & 4) != 0);
+        rs_level<L3, 2>(v3, v4, (lane & 2) != 0);
+        rs_level<L4, 1>(v4, acc, (lane & 1) != 0);
     }
     usable = group_sum_int<kWarp>(usable);
 #pragma unroll
@@ -213,6 +266,10 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         if (lane > j && lane < NOP) sm.L[lane * NOP + j] = cr / d;
         __syncwarp();
     }
+    if constexpr (NOP <= 9) {
+        if (lane < NOP) sm.invD[lane] = 1.0 / sm.L[lane * NOP + lane];
+        __syncwarp();
+    }
     // lane k < NOP: column k of X = A^-1 diag(q!), one refinement step, the consistency test's residual
     const int kc = lane < NOP ? lane : 0;
     double fk = 0.0;
@@ -226,7 +283,12 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
             for (int l = 0; l < r; ++l) x[r] -= lds(&sm.L[r * NOP + l]) * x[l];
         }
 #pragma unroll
-        for (int r = 0; r < NOP; ++r) x[r] /= lds(&sm.L[r * NOP + r]);
+        for (int r = 0; r < NOP; ++r) {
+            // up to nine monomials by the reciprocals (formed once per node); the larger systems divide (fewer
+            // live registers there)
+            if constexpr (NOP <= 9) x[r] *= lds(&sm.invD[r]);
+            else x[r] /= lds(&sm.L[r * NOP + r]);
+        }
 #pragma unroll
         for (int r = NOP - 1; r >= 0; --r) {
 #pragma unroll
@@ -252,9 +314,14 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         res = fmax(res, fabs(sres));
         maxX = fmax(maxX, fabs(x[p]));
     }
-    solve(r);
+    // one step of iterative refinement for the larger systems (14, 19 monomials); up to nine monomials the plain
+    // solve is already ~1e-14 (family-scaled) from the reference's FullPivLU result, and a refinement step changes
+    // nothing measurable there
+    if constexpr (NOP > 9) {
+        solve(r);
 #pragma unroll
-    for (int q = 0; q < NOP; ++q) x[q] += r[q];
+        for (int q = 0; q < NOP; ++q) x[q] += r[q];
+    }
     if (lane >= NOP) { res = 0.0; maxX = 0.0; }
     res = group_max<kWarp>(res);
     maxX = group_max<kWarp>(maxX);
@@ -272,9 +339,14 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
             atomicMin(a.first_degenerate, i);
         }
     }
+    // column k carries the operator's scale 1/delta^|q_k|, so that pass 2 only multiplies by the bond weight
+    int ord = 1;  // |q_k| of this lane's column: the monomials are ordered by total degree
+    while (ord < ORDER && kc >= nop_of(DIM, ord)) ++ord;
+    double colscale = inv_delta;
+    for (int t2 = 1; t2 < ord; ++t2) colscale *= inv_delta;
     if (lane < NP) {
 #pragma unroll
-        for (int p = 0; p < NOP; ++p) sm.X[p * NP + lane] = (degenerate || lane >= NOP) ? 0.0 : x[p];
+        for (int p = 0; p < NOP; ++p) sm.X[p * NP + lane] = (degenerate || lane >= NOP) ? 0.0 : x[p] * colscale;
     }
     __syncwarp();
 
@@ -289,15 +361,21 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         if (t >= b1) continue;
         BondGeo g;
         if (t - b0 < kBwCache) {
-            const int j = a.nbr[t];
-            const PosT xj = pos[j - a.node_base];
-            g.dx = xj.x - xi.x;
-            g.dy = xj.y - xi.y;
-            g.dz = 0.0;
-            if constexpr (DIM == 3) g.dz = xj.z - xi.z;
+            if constexpr (XCACHE) {
+                g.dx = sm.xc[3 * (t - b0)];
+                g.dy = sm.xc[3 * (t - b0) + 1];
+                g.dz = sm.xc[3 * (t - b0) + 2];
+            } else {
+                const int j = a.nbr[t];
+                const PosT xj = pos[j - a.node_base];
+                g.dx = xj.x - xi.x;
+                g.dy = xj.y - xi.y;
+                g.dz = 0.0;
+                if constexpr (DIM == 3) g.dz = xj.z - xi.z;
+            }
             g.bw = sm.bw[t - b0];
-        } else {
-            g = bond_geo<DIM>(a, pos, xi, t, delta, dxc, own_h);
+        } else {  // past the weight cache (families longer than kBwCache): formed again
+            g = bond_geo<DIM>(a, pos, xi, t, NodeWeight(delta, dxc), own_h);
         }
         double m[NOP];
         monomials<DIM, ORDER, double>(g.dx * inv_delta, g.dy * inv_delta, g.dz * inv_delta, m);
@@ -311,16 +389,9 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
                 s0 += xr.x * m[p];
                 s1 += xr.y * m[p];
             }
-            // op_k = (sum_p X[p][k] m_p) bw / delta^|q_k|
-            double ip0 = 1.0, ip1 = 1.0;
-#pragma unroll
-            for (int t2 = 0; t2 < Q.p[k] + Q.q[k] + Q.r[k]; ++t2) ip0 *= inv_delta;
-            constexpr int dummy = 0;
-            const int k1 = (k + 1 < NOP) ? k + 1 : dummy;
-#pragma unroll
-            for (int t2 = 0; t2 < Q.p[k1] + Q.q[k1] + Q.r[k1]; ++t2) ip1 *= inv_delta;
-            op[k] = g.bw > 0.0 ? s0 * g.bw * ip0 : 0.0;
-            if (k + 1 < NOP) op[k1] = g.bw > 0.0 ? s1 * g.bw * ip1 : 0.0;
+            // op_k = (sum_p X[p][k] m_p) bw / delta^|q_k| (the scale is in the column of X)
+            op[k] = g.bw > 0.0 ? s0 * g.bw : 0.0;
+            if (k + 1 < NOP) op[k + 1 < NOP ? k + 1 : 0] = g.bw > 0.0 ? s1 * g.bw : 0.0;
         }
         if (a.ops) {
             if constexpr (MIXED) {
@@ -377,7 +448,7 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
 
 // single geometry: one warp per node, grid-stride over the nodes; MINB resident blocks bound the registers
 // (128 a thread at 4, where the 3D order-2 node spills a few dozen bytes)
-template <int DIM, int ORDER, bool MIXED, int MINB>
+template <int DIM, int ORDER, bool MIXED, int MINB, bool ACC>
 __global__ void __launch_bounds__(kWarpNodeThreads, MINB) gbuild_warp_kernel(GBuildArgs a) {
     constexpr int NOP = nop_of(DIM, ORDER);
     constexpr int WPB = kWarpNodeThreads / kWarp;
@@ -385,14 +456,17 @@ __global__ void __launch_bounds__(kWarpNodeThreads, MINB) gbuild_warp_kernel(GBu
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     for (long long i = (long long)blockIdx.x * WPB + w; i < a.n; i += (long long)gridDim.x * WPB)
-        gbuild_warp_node<DIM, ORDER, MIXED>(a, (int)i, lane, sm[w]);
+        gbuild_warp_node<DIM, ORDER, MIXED, ACC>(a, (int)i, lane, sm[w]);
 }
 
-template <int DIM, int ORDER>
+// lane-local moment sums (ACC) up to nine monomials (45 accumulators a lane); larger systems reduce per chunk
+template <int DIM, int ORDER, bool ACC0>
 static cudaError_t launch_warp_order(const GBuildArgs &a, bool mixed, cudaStream_t s) {
     constexpr int WPB = kWarpNodeThreads / kWarp;
-    constexpr int MINB = nop_of(DIM, ORDER) <= 5 ? 5 : (nop_of(DIM, ORDER) <= 9 ? 4 : 2);
-    auto k = mixed ? gbuild_warp_kernel<DIM, ORDER, true, MINB> : gbuild_warp_kernel<DIM, ORDER, false, MINB>;
+    constexpr int NOP = nop_of(DIM, ORDER);
+    constexpr bool ACC = ACC0 && NOP <= 9;
+    constexpr int MINB = NOP <= 5 ? 5 : (NOP <= 9 ? (ACC ? 3 : 4) : 2);
+    auto k = mixed ? gbuild_warp_kernel<DIM, ORDER, true, MINB, ACC> : gbuild_warp_kernel<DIM, ORDER, false, MINB, ACC>;
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -404,22 +478,27 @@ static cudaError_t launch_warp_order(const GBuildArgs &a, bool mixed, cudaStream
     return cudaGetLastError();
 }
 
-cudaError_t launch_gbuild_warp(const GBuildArgs &a, int dim, int order, bool mixed, cudaStream_t s) {
+template <bool ACC>
+static cudaError_t launch_warp_acc(const GBuildArgs &a, int dim, int order, bool mixed, cudaStream_t s) {
     if (dim == 2) {
         switch (order) {
-            case 1: return launch_warp_order<2, 1>(a, mixed, s);
-            case 2: return launch_warp_order<2, 2>(a, mixed, s);
-            case 3: return launch_warp_order<2, 3>(a, mixed, s);
-            case 4: return launch_warp_order<2, 4>(a, mixed, s);
+            case 1: return launch_warp_order<2, 1, ACC>(a, mixed, s);
+            case 2: return launch_warp_order<2, 2, ACC>(a, mixed, s);
+            case 3: return launch_warp_order<2, 3, ACC>(a, mixed, s);
+            case 4: return launch_warp_order<2, 4, false>(a, mixed, s);
             default: return cudaErrorInvalidValue;
         }
     }
     switch (order) {
-        case 1: return launch_warp_order<3, 1>(a, mixed, s);
-        case 2: return launch_warp_order<3, 2>(a, mixed, s);
-        case 3: return launch_warp_order<3, 3>(a, mixed, s);
+        case 1: return launch_warp_order<3, 1, ACC>(a, mixed, s);
+        case 2: return launch_warp_order<3, 2, ACC>(a, mixed, s);
+        case 3: return launch_warp_order<3, 3, false>(a, mixed, s);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_gbuild_warp(const GBuildArgs &a, int dim, int order, bool mixed, bool acc, cudaStream_t s) {
+    return acc ? launch_warp_acc<true>(a, dim, order, mixed, s) : launch_warp_acc<false>(a, dim, order, mixed, s);
 }
 
 // ---- batched clouds: persistent warps over the task table, one node at a time per warp (order 2) ----------------
@@ -429,7 +508,7 @@ union BatchWarpSmem {
     WarpNodeSmem<B> s3;
 };
 
-template <bool MIXED, int DIMS, int MINB>
+template <bool MIXED, int DIMS, int MINB, bool ACC>
 __global__ void __launch_bounds__(kWarpNodeThreads, MINB) gbuild_batch_warp_kernel(BatchArgs b) {
     constexpr int WPB = kWarpNodeThreads / kWarp;
     __shared__ BatchWarpSmem<5, 9> sm[WPB];
@@ -460,19 +539,19 @@ __global__ void __launch_bounds__(kWarpNodeThreads, MINB) gbuild_batch_warp_kern
         a.defect = (MIXED && b.defect) ? b.defect + cd.def_off : nullptr;
         for (int k = 0; k < tk.count; ++k) {
             if constexpr ((DIMS & 1) != 0) {
-                if (tk.dim == 2) gbuild_warp_node<2, 2, MIXED>(a, tk.first + k, lane, sm[w].s2);
+                if (tk.dim == 2) gbuild_warp_node<2, 2, MIXED, ACC>(a, tk.first + k, lane, sm[w].s2);
             }
             if constexpr ((DIMS & 2) != 0) {
-                if (tk.dim == 3) gbuild_warp_node<3, 2, MIXED>(a, tk.first + k, lane, sm[w].s3);
+                if (tk.dim == 3) gbuild_warp_node<3, 2, MIXED, ACC>(a, tk.first + k, lane, sm[w].s3);
             }
         }
         __syncwarp();
     }
 }
 
-template <bool MIXED, int DIMS, int MINB>
+template <bool MIXED, int DIMS, int MINB, bool ACC>
 static cudaError_t launch_gbw(const BatchArgs &a, cudaStream_t s) {
-    auto k = gbuild_batch_warp_kernel<MIXED, DIMS, MINB>;
+    auto k = gbuild_batch_warp_kernel<MIXED, DIMS, MINB, ACC>;
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -485,10 +564,17 @@ static cudaError_t launch_gbw(const BatchArgs &a, cudaStream_t s) {
 }
 
 // split: one launch per dimension (dims 1: 2D tasks, 2: 3D tasks) with its own register bound
-cudaError_t launch_gbuild_batch_warp(const BatchArgs &a, bool mixed, bool split, int dims, cudaStream_t s) {
-    if (!split) return mixed ? launch_gbw<true, 3, 4>(a, s) : launch_gbw<false, 3, 4>(a, s);
-    if (dims == 1) return mixed ? launch_gbw<true, 1, 5>(a, s) : launch_gbw<false, 1, 5>(a, s);
-    return mixed ? launch_gbw<true, 2, 4>(a, s) : launch_gbw<false, 2, 4>(a, s);
+template <bool ACC>
+static cudaError_t launch_gbw_acc(const BatchArgs &a, bool mixed, bool split, int dims, cudaStream_t s) {
+    constexpr int MB3 = ACC ? 3 : 4;  // 3D (and joint) register bound: 45 lane-local sums need ~170 registers
+    if (!split) return mixed ? launch_gbw<true, 3, MB3, ACC>(a, s) : launch_gbw<false, 3, MB3, ACC>(a, s);
+    if (dims == 1) return mixed ? launch_gbw<true, 1, 5, ACC>(a, s) : launch_gbw<false, 1, 5, ACC>(a, s);
+    return mixed ? launch_gbw<true, 2, MB3, ACC>(a, s) : launch_gbw<false, 2, MB3, ACC>(a, s);
+}
+
+// split: one launch per dimension (dims 1: 2D tasks, 2: 3D tasks) with its own register bound
+cudaError_t launch_gbuild_batch_warp(const BatchArgs &a, bool mixed, bool split, int dims, bool acc, cudaStream_t s) {
+    return acc ? launch_gbw_acc<true>(a, mixed, split, dims, s) : launch_gbw_acc<false>(a, mixed, split, dims, s);
 }
 
 bool gbuild_warp_supported(int dim, int order) {

@@ -40,7 +40,8 @@ struct GBuildArgs {
 cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, int grid, cudaStream_t s);
 bool gbuild_supported(int dim, int order);
 // one warp per node (k_gbuild_warp.cu): FP64 moment sums; MIXED stores FP32 operators (and the order-2 defects)
-cudaError_t launch_gbuild_warp(const GBuildArgs &a, int dim, int order, bool mixed, cudaStream_t s);
+// acc: lane-local moment sums reduced once per node (up to nine monomials)
+cudaError_t launch_gbuild_warp(const GBuildArgs &a, int dim, int order, bool mixed, bool acc, cudaStream_t s);
 bool gbuild_warp_supported(int dim, int order);
 
 // ------------------------------------------------------------------------------ families on the device (A1)
@@ -108,9 +109,11 @@ struct BatchSchedule {
     int lpn2, lpn3;
     bool split;
     bool warp = false;  // g-build: one warp per node (k_gbuild_warp.cu) instead of lane groups
+    bool acc = false;   // g-build, warp per node: lane-local moment sums, one reduce-scatter per node
+    bool hybrid = false;  // g-build, split: lane groups of lpn2 lanes for the 2D clouds, a warp per node for 3D
 };
-constexpr int kBatchVariants = 8;
-cudaError_t launch_gbuild_batch_warp(const BatchArgs &a, bool mixed, bool split, int dims, cudaStream_t s);
+constexpr int kBatchVariants = 10;
+cudaError_t launch_gbuild_batch_warp(const BatchArgs &a, bool mixed, bool split, int dims, bool acc, cudaStream_t s);
 BatchSchedule batch_gbuild_schedule(int variant);
 BatchSchedule batch_apply_schedule(int variant);
 // dims: 1 = 2D tasks only, 2 = 3D tasks only, 3 = both
@@ -169,7 +172,7 @@ struct EpfArgs {
     const double *sc_bond = nullptr;
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
-constexpr int kEpfTmaConfigs = 13;                // staged (TMA) configurations per dimension
+constexpr int kEpfTmaConfigs = 16;                // staged (TMA) configurations per dimension
 constexpr int kEpfVariants = 5 + kEpfTmaConfigs;  // 0-2 lane groups, 3-4 CSR tiles, 5.. staged
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s);
 // P[c][t] from G[c][t] (t < ldb, SoA stride ldb): 2D p11 = C11 Gxx + C66 Gyy, p22 = C66 Gxx + C11 Gyy,
@@ -207,6 +210,8 @@ struct EpfAdjArgs {
     const int *nbr = nullptr;
     const int *rev = nullptr;
     const void *G = nullptr;
+    const void *GR = nullptr;  // optional: G in reverse-bond order, GR[c][t] = G[c][rev t] (0 without a reverse bond)
+    const uint8_t *hrev = nullptr;  // optional with GR: health in reverse-bond order (then rev is not read)
     const uint8_t *health = nullptr;
     double C11 = 0, C12 = 0, C66 = 0, inv_rho = 1;
     const double *u = nullptr;
@@ -221,6 +226,11 @@ struct EpfAdjArgs {
     double *rout = nullptr;
 };
 cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int grid, cudaStream_t s);
+// hr[t] = health[rev t] for t < nb (0 where rev t < 0)
+cudaError_t launch_reverse_health(const uint8_t *health, const int *rev, uint8_t *hr, long long nb, cudaStream_t s);
+// GR[c][t] = G[c][rev t] for t < nb (0 where rev t < 0), SoA stride ldb
+cudaError_t launch_reverse_gather(const void *G, void *GR, const int *rev, long long nb, long long ldb, int dim,
+                                  bool mixed, cudaStream_t s);
 // transpose of the BC program's linear part: w[i] = (component owned by the BC pass ? 0 : a[i]) + sum over the
 // entries executed by node i of +-a[target] (form 0: +, form 2: -, constants: none)
 cudaError_t launch_bc_transpose(const EpfArgs &bc, int n, int dim, const double *a, double *w, cudaStream_t s);

@@ -135,7 +135,7 @@ extern "C" int pxb_gbuild_noalloc_d(int dim, int order, int precision, int n, lo
     a.defect = with_defect ? defect_d : nullptr;
     // the schedule pxb_gbuild picks by default: one warp per node in 3D and above order 2, lane groups otherwise
     const bool warp = !gbuild_supported(dim, order) || dim == 3 || order > 2;
-    if (warp) PXB_CUDA_TRY(launch_gbuild_warp(a, dim, order, precision == PXB_MIXED, s));
+    if (warp) PXB_CUDA_TRY(launch_gbuild_warp(a, dim, order, precision == PXB_MIXED, false, s));
     else PXB_CUDA_TRY(launch_gbuild(a, dim, order, precision == PXB_MIXED, sms * 16, s));
     unsigned int hnd = 0;
     int hfirst = 0;

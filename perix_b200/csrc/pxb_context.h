@@ -123,6 +123,14 @@ struct EpfState {
     // explicit-loop adjoint (pxb_epf_adjoint_d): checkpoints, a segment's states, the two ping-pong states, the
     // adjoint vectors A (dJ/du^n), R (dJ/du^{n-1} carried), W (BC-transposed A), step times, dC accumulator
     DevBuf adj_ckpt, adj_seg, adj_p[2], adj_A, adj_R, adj_W, adj_t, adj_dC, adj_umax;
+    DevBuf adj_u0;       // the recorded loop's u0 (the reverse sweep's start term)
+    DevBuf adj_GR;       // the Navier operators in reverse-bond order (the adjoint kernel's second stream)
+    DevBuf adj_HR;       // the health mask in reverse-bond order (rebuilt by every reverse sweep)
+    bool adj_GR_none = false;  // no room for adj_GR: the adjoint kernel gathers the reverse bonds' operators
+    // the recorded forward loop (pxb_epf_record_d): rec_steps < 0 when there is none; rec_all: every state kept
+    double rec_dt = 0.0;
+    int rec_steps = -1, rec_K = 1;
+    bool rec_all = false;
     DevBuf health;     // uint8 [ldb] (zero tail)
     DevBuf u[2];       // double [n*dim + 8] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
     DevBuf accel;      // double [n*dim]
@@ -204,7 +212,8 @@ struct BatchState {
 struct pxb_ctx {
     int device = 0;
     size_t mem_limit = 0;  // device bytes the context may hold (0: no limit beyond the GPU's)
-    int gbuild_schedule = -1;  // g-build: -1 by problem, 0 lane groups, 1 one warp per node
+    int gbuild_schedule = -1;  // g-build: -1 by problem, 0 lane groups, 1 one warp per node, 2 the same with
+                               // lane-local moment sums
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
     long long launches = 0;

@@ -4,7 +4,8 @@ FP64 restatement in test_gpu_adjoint.py) on the notched plate, frozen damage mas
 
 * dJ/du0, dJ/dv0 and dJ/dE within 1e-10 of the taped loop, for the direct-pin BC program and for one with
   reflected walls (the BC transpose's +-1 entries), with all states kept and with checkpoints every 7 steps;
-* dJ/dE within 1e-6 of a central finite difference of the device loop itself."""
+* dJ/dE within 1e-6 of a central finite difference of the device loop itself;
+* a backward pass after a later run (which replaced the context's recording) gives the same gradients."""
 import numpy as np
 import pytest
 
@@ -89,3 +90,35 @@ def test_device_adjoint_dJ_dE_against_finite_differences(ctx, plate):  # noqa: F
     h = 1e-5 * E0
     fd = (J(E0 + h) - J(E0 - h)) / (2 * h)
     assert abs(float(E.grad) - fd) <= 1e-6 * abs(fd)
+
+
+def test_backward_after_a_later_run_rerecords(ctx, plate):  # noqa: F811
+    """The context keeps one recorded forward loop; a backward pass whose recording a later run replaced records its
+    own loop again, so its gradients equal those of the run taken alone."""
+    torch, dev = _torch()
+    from perix_b200.autograd import elastic_constants_t, explicit_run, set_constants
+    w = plate
+    n = w["L"].n
+    rng = np.random.default_rng(21)
+    u0 = rng.standard_normal(2 * n) * 1e-7
+    u0b = rng.standard_normal(2 * n) * 1e-7
+    u_obs = rng.standard_normal(2 * n) * 1e-7
+
+    def grads(with_second_run):
+        _ctx(ctx, w, E0)
+        ctx.epf_set_bcs(w["bcs"])
+        E = torch.tensor(E0, dtype=torch.float64, device=dev, requires_grad=True)
+        u0t = torch.tensor(u0, device=dev, requires_grad=True)
+        C = elastic_constants_t(2, False, E, NU)
+        set_constants(ctx, C, RHO)
+        uN, _ = explicit_run(ctx, u0t, None, C, w["dt"], NSTEPS, checkpoint_every=5)
+        if with_second_run:
+            explicit_run(ctx, torch.tensor(u0b, device=dev), None, C, w["dt"], NSTEPS // 2, checkpoint_every=0)
+        (0.5 * ((uN - torch.tensor(u_obs, device=dev)) ** 2).sum()).backward()
+        return float(E.grad), u0t.grad.cpu().numpy()
+
+    dE1, du1 = grads(False)
+    dE2, du2 = grads(True)
+    # dJ/dC is summed with one atomic per block, so its last bit may differ from run to run
+    assert abs(dE1 - dE2) <= 1e-13 * abs(dE1)
+    assert np.abs(du1 - du2).max() <= 1e-13 * np.abs(du1).max()

@@ -34,7 +34,7 @@ def _build(ctx, clouds, precision, gvariant=None):
     return ctx
 
 
-@pytest.mark.parametrize("gvariant", [0, 1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("gvariant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_batch_gbuild_fp64_matches_oracle(ctx, batch, gvariant):
     clouds, _, _, ref_g, _ = batch
     _build(ctx, clouds, 0, gvariant)
@@ -43,7 +43,7 @@ def test_batch_gbuild_fp64_matches_oracle(ctx, batch, gvariant):
         assert scaled_err(ctx.batch_get_ops(k), ref_g[k], c["off"]) <= 1e-12
 
 
-@pytest.mark.parametrize("avariant", [0, 1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("avariant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_batch_apply_fp64_matches_oracle(ctx, batch, avariant):
     clouds, u, _, _, ref_d = batch
     _build(ctx, clouds, 0)
@@ -54,7 +54,7 @@ def test_batch_apply_fp64_matches_oracle(ctx, batch, avariant):
         assert (np.abs(got[k] - ref_d[k]).max(axis=0) <= 1e-12 * scale + 1e-300).all()
 
 
-@pytest.mark.parametrize("gvariant,slot_tol", [(2, 5e-6), (4, 1e-6), (6, 1e-6)])
+@pytest.mark.parametrize("gvariant,slot_tol", [(2, 5e-6), (4, 1e-6), (6, 1e-6), (8, 1e-6)])
 def test_batch_mixed_within_bounds(ctx, batch, gvariant, slot_tol):
     """Mixed: g within 1e-6 (family-scaled); every derivative within 1e-6 of the largest derivative of its order
     (gradient / Hessian magnitude).  Slot by slot (relative to the slot's own largest value) the FP32 two-sum

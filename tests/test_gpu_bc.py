@@ -17,7 +17,7 @@ from oracle import ref_available
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not ref_available(), reason="reference harness not built")]
 
 NSTEPS = 30
-N_VARIANTS = 18
+N_VARIANTS = 21
 INACTIVE = [1.0, -1.0]  # min > max: the box leaves this axis unconstrained
 
 

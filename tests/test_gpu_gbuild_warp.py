@@ -27,7 +27,7 @@ def _geometry(ctx, d, dim):
     ctx.set_geometry(d["coords"], d["vols"], d["off"], d["ids"], s[0], s[4], dim, mirror=d["mirror"])
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 2])
 @pytest.mark.parametrize("name,dim", FIXTURES)
 def test_schedules_match_reference_goldens(ctx, name, dim, schedule):
     d = load_golden(name)
@@ -78,17 +78,34 @@ def test_higher_orders_match_reference(ctx, port, dim, order, kind):
     nd, _ = ctx.gbuild(order, 0, allow_degenerate=True)
     g = ctx.get_ops()
     assert g.shape == g_ref.shape
-    ok = np.repeat(deg_ref == 0, np.diff(m.off))  # rows the reference builds (deep/degenerate ghosts aside)
-    off_ok = np.concatenate([[0], np.cumsum(np.diff(m.off)[deg_ref == 0])])
+    built = deg_ref == 0  # nodes the reference builds (deep/degenerate ghosts aside)
+
+    def rows(nodes):
+        return np.repeat(nodes, np.diff(m.off)), np.concatenate([[0], np.cumsum(np.diff(m.off)[nodes])])
+
+    nodes = built
+    if kind == "cloud" and order == 4:
+        # The cloud's boundary-truncated order-4 families are conditioned so that any two FP64 builds differ there
+        # at 1e-8..1e-7 (on this cloud the reference's FullPivLU result lies up to 1.3e-8 from an 80-bit solve of
+        # the same moment systems, an FP64 L D L^T with refinement up to 1.5e-7): all nodes at 1e-6, the nodes with
+        # complete families (a horizon inside the cloud's box) at the FP64 bound.
+        ok, off_ok = rows(built)
+        assert scaled_err(g[ok], g_ref[ok], off_ok) <= 1e-6
+        x = m.coords.reshape(-1, 3)[:, :dim]
+        inner = np.minimum(x - x.min(0), x.max(0) - x).min(1) >= m.delta
+        assert inner.sum() >= 10
+        nodes = built & inner
+    ok, off_ok = rows(nodes)
     tol = _fp64_bound(dim, order)
     assert scaled_err(g[ok], g_ref[ok], off_ok) <= tol
     g_port, _ = port.gbuild(dim, order, m.coords, m.vols, m.off, m.ids, m.delta, m.dx_char)
     assert scaled_err(g[ok], g_port[ok], off_ok) <= tol
     ctx.gbuild(order, 1, allow_degenerate=True)
+    ok, off_ok = rows(built)
     assert scaled_err(ctx.get_ops()[ok], g_ref[ok], off_ok) <= 1e-6
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 2])
 @pytest.mark.parametrize("dim", [2, 3])
 def test_degenerate_family_reported_by_both_schedules(ctx, dim, schedule):
     import perix_b200 as px

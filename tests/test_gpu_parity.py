@@ -234,7 +234,7 @@ def slab_bcs(d, px, mesh_n):
     return bcs
 
 
-@pytest.mark.parametrize("variant", list(range(18)))
+@pytest.mark.parametrize("variant", list(range(21)))
 @pytest.mark.parametrize("name,dim", [("epf2d", 2), ("epf3d", 3)])
 def test_epf_rate_matches_reference(ctx, name, dim, variant):
     """The per-step drop-in call on every schedule variant (the staged ones run their RATE epilogue)."""
@@ -253,7 +253,7 @@ def test_epf_rate_matches_reference(ctx, name, dim, variant):
     assert np.abs(a - d["a_rand"]).max() <= 1e-12 * np.abs(d["a_rand"]).max()
 
 
-@pytest.mark.parametrize("variant", list(range(18)))
+@pytest.mark.parametrize("variant", list(range(21)))
 @pytest.mark.parametrize("name,dim", [("epf2d", 2), ("epf3d", 3)])
 def test_epf_trajectory_matches_reference(ctx, name, dim, variant):
     """Every schedule variant of the step kernel (lane groups, CSR-stream tiles, TMA-staged tiles)."""

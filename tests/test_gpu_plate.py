@@ -12,7 +12,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 NSTEPS = 30
-N_VARIANTS = 18
+N_VARIANTS = 21
 
 
 @pytest.fixture(scope="module")

@@ -15,7 +15,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-N_VARIANTS = 18
+N_VARIANTS = 21
 E, NU, RHO, SC = 190e9, 0.3, 8000.0, 0.01
 
 

@@ -71,14 +71,16 @@ def _epf_device(ctx, m, k, E, rho, G0, variant):
         pytest.skip("variant %d does not fit these families" % variant)
 
 
-@pytest.mark.parametrize("variant", list(range(18)))
+@pytest.mark.parametrize("variant", list(range(21)))
 @pytest.mark.parametrize("dim", [2, 3])
 def test_vh_explicit_rate_and_steps_match_reference(ctx, dim, variant):
     m = _mesh(dim)
     el, k, E, rho, G0 = _epf_ref(m, dim)
     rng = np.random.default_rng(20 + dim)
-    u = rng.standard_normal(dim * m.n) * (1.5e-6 if dim == 2 else 3e-6)
+    # amplitudes at which the reference breaks ~1.5 % (2D, s_c = 0.01) and ~3.5 % (3D, s_c = 0.004) of the bonds
+    u = rng.standard_normal(dim * m.n) * (5e-6 if dim == 2 else 3e-6)
     a_ref, h_ref, _ = el.rate(u)
+    assert (h_ref == 0).any()
     _epf_device(ctx, m, k, E, rho, G0, variant)
     a, nbk = ctx.epf_rate(u)
     h = ctx.epf_state()[2]
