@@ -262,7 +262,9 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
             const unsigned long long ef = policy_evict_first();
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                if constexpr (PL2) bulk_prefetch_l2_hint(Pg + (size_t)c * a.nb + t0a, bytes_g, ef);
+                // the prefetch keeps the normal priority (the streaming loads that consume it mark it evict-first);
+                // prefetched as evict-first, lines were evicted before use
+                if constexpr (PL2) bulk_prefetch_l2(Pg + (size_t)c * a.nb + t0a, bytes_g);
                 else bulk_g2s_hint(base + (size_t)c * maxb * SL::ES, Pg + (size_t)c * a.nb + t0a, bytes_g, &bar[st], ef);
             }
             bulk_g2s_hint(base + SL::nbr_off(maxb), a.nbr + t0a, bytes_n, &bar[st], ef);
@@ -635,7 +637,7 @@ struct TmaCfg {
     X(0, 32, 2, 2, 1, 8, 0) X(1, 16, 2, 3, 2, 8, 2) X(2, 32, 1, 3, 1, 8, 0) X(3, 16, 2, 2, 1, 8, 0)              \
     X(4, 16, 1, 2, 2, 8, 0) X(5, 32, 2, 2, 2, 8, 0) X(6, 32, 2, 2, 2, 4, 1) X(7, 32, 1, 2, 4, 4, 1)              \
     X(8, 16, 2, 2, 2, 4, 1) X(9, 16, 1, 3, 3, 8, 2) X(10, 32, 1, 3, 3, 8, 3) X(11, 32, 2, 3, 2, 4, 1)            \
-    X(12, 32, 1, 4, 3, 8, 2) X(13, 32, 2, 3, 2, 8, 2) X(14, 32, 1, 3, 3, 8, 2) X(15, 32, 1, 3, 6, 4, 2)
+    X(12, 16, 2, 2, 2, 8, 2) X(13, 16, 2, 3, 3, 8, 3) X(14, 32, 1, 3, 3, 8, 2) X(15, 32, 1, 3, 6, 4, 2)
 #define PXB_CFG(i, l, u, st, mb, w, x) {l, u, st, mb, w, x},
 static constexpr TmaCfg kTma2[kEpfTmaConfigs] = {PXB_TMA2(PXB_CFG)};
 static constexpr TmaCfg kTma3[kEpfTmaConfigs] = {PXB_TMA3(PXB_CFG)};
