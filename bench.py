@@ -230,6 +230,7 @@ def poisson_measure(px, device=0, reps=20):
             m.gbuild()
             _, _, t = m.poisson_assemble(1.0, f, np.zeros(m.n))
             res["reference_cpu_assembly_ms"] = t * 1e3
+            res["reference_cpu_gbuild_ms"] = m.gbuild_time(reps=3) * 1e3
             res["reference_cpu_threads"] = os.cpu_count()
     except Exception as e:  # noqa: BLE001
         res["reference_cpu_assembly_ms"] = "unavailable: %s" % e
@@ -626,6 +627,27 @@ def single_cloud(px, dim, nside, seed=11):
     delta = 3.015 * h * (1.0 + 1e-6)
     off, ids = px.families(xyz, delta, dim == 3)
     return dict(dim=dim, coords3=xyz, vols=np.full(g.shape[0], h ** dim), delta=delta, dx_char=h, off=off, ids=ids)
+
+
+def reference_cpu_gbuild_clouds(px):
+    """The reference's own order-2 g-build (PDOperators::buildGeometryCache, OpenMP on all host cores) on the largest
+    2D and 3D clouds of the batched-cloud recipe, families from its own createNeighborNodes (oracle/_ref).  The
+    same clouds' device g-build is in reference_gpu.assembly."""
+    res = {}
+    try:
+        from oracle import RefMesh, ref_available
+        if not ref_available():
+            return {"unavailable": "oracle/_ref not built"}
+        for name, dim, nside, reps in (("cloud_2d_447x447", 2, 447, 2), ("cloud_3d_58x58x58", 3, 58, 1)):
+            c = single_cloud(px, dim, nside)
+            h = c["dx_char"]
+            m = RefMesh.cloud(dim, c["coords3"], c["vols"], h, h, h if dim == 3 else 0.0, 3.015 * h)
+            secs = m.gbuild_time(reps=reps)
+            res[name] = {"nodes": int(c["vols"].size), "ms": secs * 1e3, "nodes_per_s": c["vols"].size / secs,
+                         "threads": os.cpu_count()}
+    except Exception as e:  # noqa: BLE001
+        res["unavailable"] = "reference g-build failed: %s" % e
+    return res
 
 
 def assembly_pair(px, c, mirror=None, reps=10):
@@ -1038,6 +1060,7 @@ def run_perix(args):
             plate = explicit_workload(px, plate_setup(px), steps, args.warmup, ws, local, max(10, min(steps, 200)))
             plate["cpu_baseline"] = cpu_reference("plate", 20, 2)
             clouds = clouds_measure(px, device=local)
+            clouds["reference_cpu_gbuild"] = reference_cpu_gbuild_clouds(px)
             adjoint = slab_adjoint(px, device=local)
             refgpu = reference_gpu()
             poisson = poisson_measure(px, device=local)
