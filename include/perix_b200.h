@@ -132,8 +132,8 @@ int pxb_set_node_horizons(pxb_ctx *ctx, const double *node_delta, const double *
 int pxb_gbuild(pxb_ctx *ctx, int order, int precision, int *n_degenerate, int *first_degenerate);
 /* Schedule of the g-build kernels: 0 lane groups (a group of 8-32 lanes per node; at MIXED the moment sums run in
  * FP32 with two-sum compensation), 1 one warp per node (moment sums in FP64 at both precisions; MIXED stores FP32),
- * 2 the same with each lane's moment sums kept over all the node's bonds and reduced once per node (up to nine
- * monomials; larger systems as 1), -1 (default) the one this backend picks: warp per node in 3D and above order 2,
+ * 2 the same with its moment sums and per-bond operator products on the FP64 tensor cores (mma m8n8k4; up to nine
+ * monomials, larger systems as 1), -1 (default) the one this backend picks: warp per node in 3D and above order 2,
  * lane groups for 2D orders 1-2.
  * Orders 2D 4 and 3D 3 exist only as the warp-per-node schedule. */
 int pxb_gbuild_set_schedule(pxb_ctx *ctx, int schedule);

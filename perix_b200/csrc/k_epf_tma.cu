@@ -86,10 +86,20 @@ __device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, unsign
 __device__ __forceinline__ void bulk_prefetch_l2(const void *src, unsigned bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ void bulk_prefetch_l2_hint(const void *src, unsigned bytes, unsigned long long policy) {
-    asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;" ::"l"(src), "r"(bytes), "l"(policy)
-                 : "memory");
+
+// per-thread asynchronous copy of one element (4 or 8 bytes, both addresses aligned to it) global -> shared, and
+// its group fences
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ unsigned long long policy_evict_first() {
     unsigned long long p;
@@ -200,6 +210,9 @@ template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB, int F
 __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     constexpr bool XI = (FLAGS & 1) != 0;
     constexpr bool PL2 = (FLAGS & 2) != 0;
+    // CPA (bit 2, with PL2): each lane copies its next pass's coefficients from L2 into a private double buffer in
+    // shared memory (cp.async) while it computes the current pass, instead of holding them in registers
+    constexpr bool CPA = PL2 && (FLAGS & 4) != 0;
     constexpr bool XS = XI;
     using PosT = typename Vec<DIM>::T;
     using GT = typename std::conditional<MIXED, float, double>::type;
@@ -375,7 +388,31 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
 #pragma unroll
         for (int d = 0; d < DIM; ++d) L[d] = 0.0;
         // UNR bonds per lane per pass: staged reads, then all neighbour gathers, then the arithmetic
-        for (int t0 = b0 + gl; t0 < b1; t0 += LPN * UNR) {
+        // CPA: this lane's double buffer, [buf][q][c] with the lane index innermost (conflict-free)
+        GT *cbuf = nullptr;
+        auto cpa_issue = [&](int tb, int buf) {
+            const GT *Pt = Pg + t0a;
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                const int t = tb + q * LPN;
+                if (t < b1) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c)
+                        cp_async_elem(cbuf + ((size_t)(buf * UNR + q) * NC + c) * kWarp, Pt + (size_t)c * a.nb + t);
+                }
+            }
+            cp_async_commit();
+        };
+        if constexpr (CPA) {
+            cbuf = reinterpret_cast<GT *>(smem + (size_t)S * stage_bytes) + (size_t)wib * 2 * UNR * NC * kWarp + lane;
+            cpa_issue(b0 + gl, 0);
+        }
+        int pass = 0;
+        for (int t0 = b0 + gl; t0 < b1; t0 += LPN * UNR, ++pass) {
+            if constexpr (CPA) {  // the next pass's copies go out, this pass's must have landed
+                cpa_issue(t0 + LPN * UNR, (pass + 1) & 1);
+                cp_async_wait<1>();
+            }
             uint8_t h[UNR];
             int j[UNR];
 #pragma unroll
@@ -387,7 +424,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
             }
             // PL2: the pass's coefficients from L2 (prefetched with the tile), issued before the gathers
             GT pv[PL2 ? UNR : 1][NC];
-            if constexpr (PL2) {
+            if constexpr (PL2 && !CPA) {
                 const GT *Pt = Pg + t0a;
 #pragma unroll
                 for (int q = 0; q < UNR; ++q) {
@@ -489,12 +526,14 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
                 double pd[NC];
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
-                    if constexpr (PL2) pd[c] = (double)pv[q < (PL2 ? UNR : 1) ? q : 0][c];
+                    if constexpr (CPA) pd[c] = (double)cbuf[((size_t)((pass & 1) * UNR + q) * NC + c) * kWarp];
+                    else if constexpr (PL2) pd[c] = (double)pv[q < (PL2 ? UNR : 1) ? q : 0][c];
                     else pd[c] = (double)sP[(size_t)c * maxb + t];
                 }
                 navier_acc_t<DIM>(pd, e[q], L);
             }
         }
+        if constexpr (CPA) cp_async_wait<0>();  // nothing of this lane's may still land in its buffer
 #pragma unroll
         for (int d = 0; d < DIM; ++d) L[d] = group_sum<LPN>(L[d]);
 
@@ -574,12 +613,18 @@ static LaunchShape g_last_shape{0, 0, 0};
 
 LaunchShape epf_tma_last_shape() { return g_last_shape; }
 
+// the per-lane coefficient double buffers of the CPA configurations (after the ring)
+constexpr size_t cpa_bytes(int dim, bool mixed, int unr, int wpb, int flags) {
+    return ((flags & 6) == 6) ? (size_t)wpb * 2 * unr * (dim == 3 ? 6 : 3) * kWarp * (mixed ? 4 : 8) : 0;
+}
+
 template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB, int FLAGS>
 static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
     constexpr int NT = WPB * (kWarp / LPN);
     using SL = StageLayout<DIM, MIXED, NT, (FLAGS & 1) != 0, (FLAGS & 2) != 0>;
     auto k = epf_tma_kernel<DIM, MIXED, LPN, UNR, S, MINB, WPB, FLAGS>;
-    const size_t smem = (size_t)S * SL::bytes(a.maxb);
+    constexpr size_t cpa = cpa_bytes(DIM, MIXED, UNR, WPB, FLAGS);
+    const size_t smem = (size_t)S * SL::bytes(a.maxb) + cpa;
     static size_t configured = 0;
     if (smem > configured) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -623,7 +668,8 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
 
 // Staged configurations: lanes per node, bonds per lane per pass, stages, minimum resident blocks (launch
 // bounds), warps per block, flags (1: staged FP32 bond vectors for the stretch pre-test, 8 (2D) / 12 (3D) more
-// staged bytes per bond; 2: coefficients prefetched into L2 and loaded per lane instead of staged).  A tile is
+// staged bytes per bond; 2: coefficients prefetched into L2 and loaded per lane instead of staged; 4 (with 2): those
+// loads go through a per-lane double buffer in shared memory filled by cp.async one pass ahead).  A tile is
 // WPB * 32/LPN nodes.
 struct TmaCfg {
     int lpn, unr, stages, minb, wpb, xi;
@@ -637,7 +683,7 @@ struct TmaCfg {
     X(0, 32, 2, 2, 1, 8, 0) X(1, 16, 2, 3, 2, 8, 2) X(2, 32, 1, 3, 1, 8, 0) X(3, 16, 2, 2, 1, 8, 0)              \
     X(4, 16, 1, 2, 2, 8, 0) X(5, 32, 2, 2, 2, 8, 0) X(6, 32, 2, 2, 2, 4, 1) X(7, 32, 1, 2, 4, 4, 1)              \
     X(8, 16, 2, 2, 2, 4, 1) X(9, 16, 1, 3, 3, 8, 2) X(10, 32, 1, 3, 3, 8, 3) X(11, 32, 2, 3, 2, 4, 1)            \
-    X(12, 16, 2, 2, 2, 8, 2) X(13, 16, 2, 3, 3, 8, 3) X(14, 32, 1, 3, 3, 8, 2) X(15, 32, 1, 3, 6, 4, 2)
+    X(12, 16, 2, 2, 2, 8, 2) X(13, 16, 2, 3, 3, 8, 6) X(14, 32, 1, 3, 3, 8, 2) X(15, 32, 1, 3, 6, 4, 2)
 #define PXB_CFG(i, l, u, st, mb, w, x) {l, u, st, mb, w, x},
 static constexpr TmaCfg kTma2[kEpfTmaConfigs] = {PXB_TMA2(PXB_CFG)};
 static constexpr TmaCfg kTma3[kEpfTmaConfigs] = {PXB_TMA3(PXB_CFG)};
@@ -670,9 +716,11 @@ static size_t tma_smem_dm(int which, int maxb) {
         case 0: per = tma_stage_bytes<DIM, MIXED, false, false>(nt, maxb); break;
         case 1: per = tma_stage_bytes<DIM, MIXED, true, false>(nt, maxb); break;
         case 2: per = tma_stage_bytes<DIM, MIXED, false, true>(nt, maxb); break;
-        default: per = tma_stage_bytes<DIM, MIXED, true, true>(nt, maxb); break;
+        case 3: per = tma_stage_bytes<DIM, MIXED, true, true>(nt, maxb); break;
+        case 6: per = tma_stage_bytes<DIM, MIXED, false, true>(nt, maxb); break;  // CPA
+        default: per = tma_stage_bytes<DIM, MIXED, true, true>(nt, maxb); break;   // 7: CPA with bond vectors
     }
-    return (size_t)c.stages * per;
+    return (size_t)c.stages * per + cpa_bytes(DIM, MIXED, c.unr, c.wpb, c.xi);
 }
 
 size_t epf_tma_smem(int dim, bool mixed, int which, int maxb) {

@@ -483,7 +483,7 @@ cudaError_t launch_gbuild_batch(const BatchArgs &a, bool mixed, int variant, int
     const BatchSchedule sch = batch_gbuild_schedule(variant);
     if (sch.hybrid && dims == 1)  // the 2D launch of the hybrid schedule: lane groups (FP64 sums for MIXED)
         return mixed ? launch_gb<true, 8, 32, 1, true>(a, s) : launch_gb<false, 8, 32, 1, false>(a, s);
-    if (sch.warp) return launch_gbuild_batch_warp(a, mixed, sch.split, dims, sch.acc, s);
+    if (sch.warp) return launch_gbuild_batch_warp(a, mixed, sch.split, dims, sch.tc, s);
     return mixed ? launch_gb_m<true>(a, variant, dims, s) : launch_gb_m<false>(a, variant, dims, s);
 }
 

@@ -29,6 +29,8 @@ namespace {
 
 constexpr int kWarpNodeThreads = 128;  // 4 warps (nodes) per block
 constexpr int kBwCache = 256;          // bond weights per node cached for pass 2 (longer families recompute)
+constexpr int kMonoStride = 36;        // row stride (doubles) of the transposed monomial tile: conflict-minimal reads
+constexpr int kOpStride = 9;           // row stride (doubles) of a chunk's operator rows (odd: conflict-minimal)
 
 // packed upper triangle (p <= q, row-major) of an NOP x NOP symmetric matrix
 template <int NOP>
@@ -95,6 +97,13 @@ __device__ __forceinline__ int rs_entry(int lane, int s) {
     return p;
 }
 
+// D += A B on the FP64 tensor cores (m8n8k4): lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0,1}]
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
 struct BondGeo {
     double dx, dy, dz, bw;
 };
@@ -136,35 +145,46 @@ __device__ __forceinline__ BondGeo bond_geo(const GBuildArgs &a, const PosT *pos
 
 // Shared memory a warp needs for one node of NOP monomials (doubles): weight cache, A, L D L^T, X (rows padded
 // to an even count so that rows load as double2).
-template <int NOP>
+template <int NOP, bool TC = false>
 struct WarpNodeSmem {
     static constexpr int NP = (NOP + 1) & ~1;
+    // bonds whose weight (and bond vector) pass 1 caches for pass 2: 128 with the tensor-core tiles, so that a
+    // 2-warp block fits 8 times on an SM
+    static constexpr int BWC = TC ? 128 : kBwCache;
     // bond vectors cached for pass 2 too (up to nine monomials; larger systems gather them again)
     static constexpr bool CACHE_X = NOP <= 9;
-    static constexpr int XC = CACHE_X ? kBwCache : 2;
+    static constexpr int XC = CACHE_X ? BWC : 2;
     // every section starts on a 16-byte boundary (X is read as double2)
-    alignas(16) double bw[kBwCache];
+    alignas(16) double bw[BWC];
     alignas(16) double xc[3 * XC];
     alignas(16) double A[NOP * NOP];
     alignas(16) double L[NOP * NOP];
     alignas(16) double X[NOP * NP];
     alignas(16) double invD[NP];  // 1 / D of the L D L^T factorisation
+    // TC (up to nine monomials): a chunk's monomials transposed [p][bond] (rows padded to 16, row stride kMonoStride),
+    // its bond weights and its operator rows
+    static constexpr bool TCA = TC && NOP <= 9;
+    alignas(16) double monoT[TCA ? 16 * kMonoStride : 2];
+    alignas(16) double wk[TCA ? 32 : 2];
+    alignas(16) double opb[TCA ? 32 * kOpStride : 2];
 };
 static_assert(offsetof(WarpNodeSmem<14>, X) % 16 == 0 && offsetof(WarpNodeSmem<19>, X) % 16 == 0 &&
                   offsetof(WarpNodeSmem<9>, X) % 16 == 0 && offsetof(WarpNodeSmem<5>, X) % 16 == 0,
               "X rows are read as double2");
 
-// ACC: each lane keeps its own moment sums over all the node's chunks and the warp reduce-scatters them once per
-// node (NE accumulators a lane) instead of once per 32-bond chunk
-template <int DIM, int ORDER, bool MIXED, bool ACC = false>
+// TC (up to nine monomials): the moment sums and the per-bond operator products run on the FP64 tensor cores
+// (mma m8n8k4): per 32-bond chunk the lanes store their bonds' monomials transposed in shared memory, the moment
+// matrix accumulates as A += (W M)^T M over 4-bond k-steps in three 8x8 tiles (no cross-lane reduction), and in
+// pass 2 each 8-bond tile of the chunk multiplies its monomials by X (held as B fragments in registers)
+template <int DIM, int ORDER, bool MIXED, bool TC = false>
 __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int lane,
-                                                 WarpNodeSmem<nop_of(DIM, ORDER)> &sm) {
+                                                 WarpNodeSmem<nop_of(DIM, ORDER), TC> &sm) {
     constexpr QTable<DIM, ORDER> Q{};
     constexpr int NOP = Q.NOP;
     constexpr Tri<NOP> T{};
     constexpr int NE = Tri<NOP>::NE;
     constexpr int L1 = halve(NE), L2 = halve(L1), L3 = halve(L2), L4 = halve(L3), L5 = halve(L4);
-    constexpr int NP = WarpNodeSmem<NOP>::NP;
+    constexpr int NP = WarpNodeSmem<NOP, TC>::NP;
     static_assert(NOP <= 32, "one lane per solve column");
     using PosT = typename Vec<DIM>::T;
     const PosT *pos = static_cast<const PosT *>(a.pos);
@@ -172,7 +192,8 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     const double delta = own_h ? a.node_delta[i - a.node_base] : a.delta;
     const double dxc = own_h ? a.node_dxc[i - a.node_base] : a.dx_char;
     const double inv_delta = 1.0 / delta;
-    constexpr bool XCACHE = WarpNodeSmem<NOP>::CACHE_X;
+    constexpr bool XCACHE = WarpNodeSmem<NOP, TC>::CACHE_X;
+    constexpr int BWC = WarpNodeSmem<NOP, TC>::BWC;
     const int b0 = a.off[i], b1 = a.off[i + 1];
     const PosT xi = pos[i - a.node_base];
 
@@ -180,9 +201,14 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     double acc[L5];
 #pragma unroll
     for (int s = 0; s < L5; ++s) acc[s] = 0.0;
-    double lacc[ACC ? NE : 1];
+    static_assert(!TC || NOP <= 9, "tensor-core path: up to nine monomials");
+    constexpr int MS = kMonoStride;
+    const int grp = lane >> 2, tig = lane & 3;  // mma fragment coordinates
+    double c00[2] = {0.0, 0.0}, c01[2] = {0.0, 0.0}, c11[2] = {0.0, 0.0};  // TC: moment tiles (0,0) (0,8) (8,8)
+    if constexpr (TC) {  // padding rows of the monomial tile stay zero for the node
 #pragma unroll
-    for (int e = 0; e < (ACC ? NE : 1); ++e) lacc[e] = 0.0;
+        for (int p = NOP; p < 16; ++p) sm.monoT[p * MS + lane] = 0.0;
+    }
     int usable = 0;
     {
     const NodeWeight nw(delta, dxc);
@@ -190,7 +216,7 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         const int t = c0 + lane;
         BondGeo g{0.0, 0.0, 0.0, 0.0};
         if (t < b1) g = bond_geo<DIM>(a, pos, xi, t, nw, own_h);
-        if (t < b1 && t - b0 < kBwCache) {
+        if (t < b1 && t - b0 < BWC) {
             sm.bw[t - b0] = g.bw;
             if constexpr (XCACHE) {
                 sm.xc[3 * (t - b0)] = g.dx;
@@ -201,13 +227,27 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         usable += g.bw > 0.0 ? 1 : 0;
         double m[NOP], wm[NOP];
         monomials<DIM, ORDER, double>(g.dx * inv_delta, g.dy * inv_delta, g.dz * inv_delta, m);
+        if constexpr (TC) {
+#pragma unroll
+            for (int p = 0; p < NOP; ++p) sm.monoT[p * MS + lane] = m[p];
+            sm.wk[lane] = g.bw;
+            __syncwarp();
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {  // k-steps of 4 bonds: A frag bw_b m_p(b), B frag m_q(b)
+                const int b = 4 * kk + tig;
+                const double w = sm.wk[b];
+                const double mlo = sm.monoT[grp * MS + b];
+                dmma(c00, w * mlo, mlo);
+                if constexpr (NOP > 8) {
+                    const double mhi = sm.monoT[(8 + grp) * MS + b];
+                    dmma(c01, w * mlo, mhi);
+                    dmma(c11, w * mhi, mhi);
+                }
+            }
+            __syncwarp();
+        } else {
 #pragma unroll
         for (int k = 0; k < NOP; ++k) wm[k] = g.bw * m[k];
-        if constexpr (ACC) {
-#pragma unroll
-            for (int e = 0; e < NE; ++e) lacc[e] = fma(wm[T.p[e]], m[T.q[e]], lacc[e]);
-            continue;
-        }
         // first halving with the products formed as they are exchanged
         double v1[L1];
         {
@@ -230,25 +270,37 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         rs_level<L4, 1>(v4, v5, (lane & 1) != 0);
 #pragma unroll
         for (int s = 0; s < L5; ++s) acc[s] += v5[s];
+        }
     }
-    }
-    if constexpr (ACC) {  // the node's one reduce-scatter
-        double v1[L1], v2[L2], v3[L3], v4[L4];
-        rs_level<NE, 16>(lacc, v1, (lane & 16) != 0);
-        rs_level<L1, 8>(v1, v2, (lane & 8) != 0);
-        rs_level<L2, 4>(v2, v3, (lane & 4) != 0);
-        rs_level<L3, 2>(v3, v4, (lane & 2) != 0);
-        rs_level<L4, 1>(v4, acc, (lane & 1) != 0);
     }
     usable = group_sum_int<kWarp>(usable);
+    if constexpr (TC) {  // the tiles' upper triangle, mirrored (the matrix stays exactly symmetric)
+        auto put = [&](int p, int q, double v) {
+            if (p <= q && q < NOP) {
+                sm.A[p * NOP + q] = v;
+                sm.A[q * NOP + p] = v;
+                sm.L[p * NOP + q] = v;
+                sm.L[q * NOP + p] = v;
+            }
+        };
 #pragma unroll
-    for (int s = 0; s < L5; ++s) {
-        const int e = rs_entry<NE>(lane, s);
-        if (e >= 0) {
-            sm.A[T.p[e] * NOP + T.q[e]] = acc[s];
-            sm.A[T.q[e] * NOP + T.p[e]] = acc[s];
-            sm.L[T.p[e] * NOP + T.q[e]] = acc[s];
-            sm.L[T.q[e] * NOP + T.p[e]] = acc[s];
+        for (int h = 0; h < 2; ++h) {
+            put(grp, 2 * tig + h, c00[h]);
+            if constexpr (NOP > 8) {
+                put(grp, 8 + 2 * tig + h, c01[h]);
+                put(8 + grp, 8 + 2 * tig + h, c11[h]);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int s = 0; s < L5; ++s) {
+            const int e = rs_entry<NE>(lane, s);
+            if (e >= 0) {
+                sm.A[T.p[e] * NOP + T.q[e]] = acc[s];
+                sm.A[T.q[e] * NOP + T.p[e]] = acc[s];
+                sm.L[T.p[e] * NOP + T.q[e]] = acc[s];
+                sm.L[T.q[e] * NOP + T.p[e]] = acc[s];
+            }
         }
     }
     __syncwarp();
@@ -356,11 +408,10 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     double dsum[ND];
 #pragma unroll
     for (int e = 0; e < ND; ++e) dsum[e] = 0.0;
-    for (int c0 = b0; c0 < b1; c0 += kWarp) {
-        const int t = c0 + lane;
-        if (t >= b1) continue;
+    // the bond's geometry in pass 2: cached in pass 1, or formed again past the cache
+    auto geo2 = [&](int t) -> BondGeo {
         BondGeo g;
-        if (t - b0 < kBwCache) {
+        if (t - b0 < BWC) {
             if constexpr (XCACHE) {
                 g.dx = sm.xc[3 * (t - b0)];
                 g.dy = sm.xc[3 * (t - b0) + 1];
@@ -374,25 +425,13 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
                 if constexpr (DIM == 3) g.dz = xj.z - xi.z;
             }
             g.bw = sm.bw[t - b0];
-        } else {  // past the weight cache (families longer than kBwCache): formed again
+        } else {  // past the weight cache (families longer than BWC): formed again
             g = bond_geo<DIM>(a, pos, xi, t, NodeWeight(delta, dxc), own_h);
         }
-        double m[NOP];
-        monomials<DIM, ORDER, double>(g.dx * inv_delta, g.dy * inv_delta, g.dz * inv_delta, m);
-        double op[NOP];
-#pragma unroll
-        for (int k = 0; k < NOP; k += 2) {
-            double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-            for (int p = 0; p < NOP; ++p) {
-                const double2 xr = lds2(&sm.X[p * NP + k]);
-                s0 += xr.x * m[p];
-                s1 += xr.y * m[p];
-            }
-            // op_k = (sum_p X[p][k] m_p) bw / delta^|q_k| (the scale is in the column of X)
-            op[k] = g.bw > 0.0 ? s0 * g.bw : 0.0;
-            if (k + 1 < NOP) op[k + 1 < NOP ? k + 1 : 0] = g.bw > 0.0 ? s1 * g.bw : 0.0;
-        }
+        return g;
+    };
+    // one bond's operator vector out: AoS operators (MIXED: FP32 and the defect's first moments), Navier subset
+    auto emit = [&](int t, const BondGeo &g, const double *op) {
         if (a.ops) {
             if constexpr (MIXED) {
                 float *o = static_cast<float *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
@@ -432,6 +471,80 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
                 }
             }
         }
+    };
+    // TC: X as B fragments (rows = monomials in k-steps of 4, columns = operators in tiles of 8), zero past NOP
+    constexpr int KS = (NOP + 3) / 4, NT2 = NOP > 8 ? 2 : 1;
+    double bx[TC ? KS : 1][TC ? NT2 : 1];
+    if constexpr (TC) {
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks)
+#pragma unroll
+            for (int nt = 0; nt < NT2; ++nt) {
+                const int pr = 4 * ks + tig, kc2 = 8 * nt + grp;
+                bx[ks][nt] = (pr < NOP && kc2 < NOP) ? sm.X[pr * NP + kc2] : 0.0;
+            }
+    }
+    for (int c0 = b0; c0 < b1; c0 += kWarp) {
+        const int t = c0 + lane;
+        if constexpr (TC) {
+            BondGeo g{0.0, 0.0, 0.0, 0.0};
+            if (t < b1) g = geo2(t);
+            double m[NOP];
+            monomials<DIM, ORDER, double>(g.dx * inv_delta, g.dy * inv_delta, g.dz * inv_delta, m);
+#pragma unroll
+            for (int p = 0; p < NOP; ++p) sm.monoT[p * MS + lane] = m[p];
+            sm.wk[lane] = g.bw;
+            __syncwarp();
+#pragma unroll
+            for (int bt = 0; bt < 4; ++bt) {  // 8-bond tiles: D[bond][k] = sum_p m_p(bond) X[p][k]
+                double d0[2] = {0.0, 0.0}, d1[2] = {0.0, 0.0};
+#pragma unroll
+                for (int ks = 0; ks < KS; ++ks) {
+                    const double am = sm.monoT[(4 * ks + tig) * MS + 8 * bt + grp];
+                    dmma(d0, am, bx[ks][0]);
+                    if constexpr (NT2 > 1) dmma(d1, am, bx[ks][NT2 - 1]);
+                }
+                const double w = sm.wk[8 * bt + grp];
+                const int row = (8 * bt + grp) * kOpStride;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k0 = 2 * tig + h;
+                    if (k0 < NOP) sm.opb[row + k0] = w * d0[h];
+                    if constexpr (NT2 > 1) {
+                        const int k1 = 8 + 2 * tig + h;
+                        if (k1 < NOP) sm.opb[row + k1] = w * d1[h];
+                    }
+                }
+            }
+            __syncwarp();
+            if (t < b1) {
+                double op[NOP];
+#pragma unroll
+                for (int k = 0; k < NOP; ++k) op[k] = sm.opb[lane * kOpStride + k];
+                emit(t, g, op);
+            }
+            __syncwarp();
+        } else {
+            if (t >= b1) continue;
+            const BondGeo g = geo2(t);
+            double m[NOP];
+            monomials<DIM, ORDER, double>(g.dx * inv_delta, g.dy * inv_delta, g.dz * inv_delta, m);
+            double op[NOP];
+#pragma unroll
+            for (int k = 0; k < NOP; k += 2) {
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                for (int p = 0; p < NOP; ++p) {
+                    const double2 xr = lds2(&sm.X[p * NP + k]);
+                    s0 += xr.x * m[p];
+                    s1 += xr.y * m[p];
+                }
+                // op_k = (sum_p X[p][k] m_p) bw / delta^|q_k| (the scale is in the column of X)
+                op[k] = g.bw > 0.0 ? s0 * g.bw : 0.0;
+                if (k + 1 < NOP) op[k + 1 < NOP ? k + 1 : 0] = g.bw > 0.0 ? s1 * g.bw : 0.0;
+            }
+            emit(t, g, op);
+        }
     }
     if constexpr (DEF) {
         if (a.defect) {
@@ -448,70 +561,74 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
 
 // single geometry: one warp per node, grid-stride over the nodes; MINB resident blocks bound the registers
 // (128 a thread at 4, where the 3D order-2 node spills a few dozen bytes)
-template <int DIM, int ORDER, bool MIXED, int MINB, bool ACC>
-__global__ void __launch_bounds__(kWarpNodeThreads, MINB) gbuild_warp_kernel(GBuildArgs a) {
+// threads a block: 4 warps, 2 with the tensor-core tiles (whose per-warp shared memory is larger)
+__host__ __device__ constexpr int warp_node_threads(bool tc) { return tc ? 64 : kWarpNodeThreads; }
+
+template <int DIM, int ORDER, bool MIXED, int MINB, bool TC>
+__global__ void __launch_bounds__(warp_node_threads(TC), MINB) gbuild_warp_kernel(GBuildArgs a) {
     constexpr int NOP = nop_of(DIM, ORDER);
-    constexpr int WPB = kWarpNodeThreads / kWarp;
-    __shared__ WarpNodeSmem<NOP> sm[WPB];
+    constexpr int WPB = warp_node_threads(TC) / kWarp;
+    __shared__ WarpNodeSmem<NOP, TC> sm[WPB];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     for (long long i = (long long)blockIdx.x * WPB + w; i < a.n; i += (long long)gridDim.x * WPB)
-        gbuild_warp_node<DIM, ORDER, MIXED, ACC>(a, (int)i, lane, sm[w]);
+        gbuild_warp_node<DIM, ORDER, MIXED, TC>(a, (int)i, lane, sm[w]);
 }
 
-// lane-local moment sums (ACC) up to nine monomials (45 accumulators a lane); larger systems reduce per chunk
-template <int DIM, int ORDER, bool ACC0>
+// tensor-core products (TC) up to nine monomials; larger systems keep the scalar path
+template <int DIM, int ORDER, bool TC0>
 static cudaError_t launch_warp_order(const GBuildArgs &a, bool mixed, cudaStream_t s) {
-    constexpr int WPB = kWarpNodeThreads / kWarp;
     constexpr int NOP = nop_of(DIM, ORDER);
-    constexpr bool ACC = ACC0 && NOP <= 9;
-    constexpr int MINB = NOP <= 5 ? 5 : (NOP <= 9 ? (ACC ? 3 : 4) : 2);
-    auto k = mixed ? gbuild_warp_kernel<DIM, ORDER, true, MINB, ACC> : gbuild_warp_kernel<DIM, ORDER, false, MINB, ACC>;
+    constexpr bool TC = TC0 && NOP <= 9;
+    constexpr int MINB = TC ? 8 : (NOP <= 5 ? 5 : (NOP <= 9 ? 4 : 2));  // TC: 8 blocks of 2 warps
+    constexpr int THREADS = warp_node_threads(TC);
+    auto k = mixed ? gbuild_warp_kernel<DIM, ORDER, true, MINB, TC> : gbuild_warp_kernel<DIM, ORDER, false, MINB, TC>;
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kWarpNodeThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, THREADS, 0);
+    constexpr int WPB = THREADS / kWarp;
     const long long need = ((long long)a.n + WPB - 1) / WPB;
     const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
     const int grid = (int)(need < cap ? (need > 0 ? need : 1) : cap);
-    k<<<grid, kWarpNodeThreads, 0, s>>>(a);
+    k<<<grid, THREADS, 0, s>>>(a);
     return cudaGetLastError();
 }
 
-template <bool ACC>
-static cudaError_t launch_warp_acc(const GBuildArgs &a, int dim, int order, bool mixed, cudaStream_t s) {
+template <bool TC>
+static cudaError_t launch_warp_tc(const GBuildArgs &a, int dim, int order, bool mixed, cudaStream_t s) {
     if (dim == 2) {
         switch (order) {
-            case 1: return launch_warp_order<2, 1, ACC>(a, mixed, s);
-            case 2: return launch_warp_order<2, 2, ACC>(a, mixed, s);
-            case 3: return launch_warp_order<2, 3, ACC>(a, mixed, s);
+            case 1: return launch_warp_order<2, 1, TC>(a, mixed, s);
+            case 2: return launch_warp_order<2, 2, TC>(a, mixed, s);
+            case 3: return launch_warp_order<2, 3, TC>(a, mixed, s);
             case 4: return launch_warp_order<2, 4, false>(a, mixed, s);
             default: return cudaErrorInvalidValue;
         }
     }
     switch (order) {
-        case 1: return launch_warp_order<3, 1, ACC>(a, mixed, s);
-        case 2: return launch_warp_order<3, 2, ACC>(a, mixed, s);
+        case 1: return launch_warp_order<3, 1, TC>(a, mixed, s);
+        case 2: return launch_warp_order<3, 2, TC>(a, mixed, s);
         case 3: return launch_warp_order<3, 3, false>(a, mixed, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_gbuild_warp(const GBuildArgs &a, int dim, int order, bool mixed, bool acc, cudaStream_t s) {
-    return acc ? launch_warp_acc<true>(a, dim, order, mixed, s) : launch_warp_acc<false>(a, dim, order, mixed, s);
+cudaError_t launch_gbuild_warp(const GBuildArgs &a, int dim, int order, bool mixed, bool tc, cudaStream_t s) {
+    return tc ? launch_warp_tc<true>(a, dim, order, mixed, s) : launch_warp_tc<false>(a, dim, order, mixed, s);
 }
 
 // ---- batched clouds: persistent warps over the task table, one node at a time per warp (order 2) ----------------
-template <int A, int B>
+template <int A, int B, bool TC>
 union BatchWarpSmem {
-    WarpNodeSmem<A> s2;
-    WarpNodeSmem<B> s3;
+    WarpNodeSmem<A, TC> s2;
+    WarpNodeSmem<B, TC> s3;
 };
 
-template <bool MIXED, int DIMS, int MINB, bool ACC>
-__global__ void __launch_bounds__(kWarpNodeThreads, MINB) gbuild_batch_warp_kernel(BatchArgs b) {
-    constexpr int WPB = kWarpNodeThreads / kWarp;
-    __shared__ BatchWarpSmem<5, 9> sm[WPB];
+template <bool MIXED, int DIMS, int MINB, bool TC>
+__global__ void __launch_bounds__(warp_node_threads(TC), MINB) gbuild_batch_warp_kernel(BatchArgs b) {
+    constexpr int WPB = warp_node_threads(TC) / kWarp;
+    __shared__ BatchWarpSmem<5, 9, TC> sm[WPB];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     for (;;) {
@@ -539,42 +656,43 @@ __global__ void __launch_bounds__(kWarpNodeThreads, MINB) gbuild_batch_warp_kern
         a.defect = (MIXED && b.defect) ? b.defect + cd.def_off : nullptr;
         for (int k = 0; k < tk.count; ++k) {
             if constexpr ((DIMS & 1) != 0) {
-                if (tk.dim == 2) gbuild_warp_node<2, 2, MIXED, ACC>(a, tk.first + k, lane, sm[w].s2);
+                if (tk.dim == 2) gbuild_warp_node<2, 2, MIXED, TC>(a, tk.first + k, lane, sm[w].s2);
             }
             if constexpr ((DIMS & 2) != 0) {
-                if (tk.dim == 3) gbuild_warp_node<3, 2, MIXED, ACC>(a, tk.first + k, lane, sm[w].s3);
+                if (tk.dim == 3) gbuild_warp_node<3, 2, MIXED, TC>(a, tk.first + k, lane, sm[w].s3);
             }
         }
         __syncwarp();
     }
 }
 
-template <bool MIXED, int DIMS, int MINB, bool ACC>
+template <bool MIXED, int DIMS, int MINB, bool TC>
 static cudaError_t launch_gbw(const BatchArgs &a, cudaStream_t s) {
-    auto k = gbuild_batch_warp_kernel<MIXED, DIMS, MINB, ACC>;
+    auto k = gbuild_batch_warp_kernel<MIXED, DIMS, MINB, TC>;
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kWarpNodeThreads, 0);
-    const long long want = ((long long)a.ntasks + (kWarpNodeThreads / kWarp) - 1) / (kWarpNodeThreads / kWarp);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, warp_node_threads(TC), 0);
+    const long long want = ((long long)a.ntasks + (warp_node_threads(TC) / kWarp) - 1) / (warp_node_threads(TC) / kWarp);
     const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
     const int grid = (int)(want < cap ? (want > 0 ? want : 1) : cap);
-    k<<<grid, kWarpNodeThreads, 0, s>>>(a);
+    k<<<grid, warp_node_threads(TC), 0, s>>>(a);
     return cudaGetLastError();
 }
 
 // split: one launch per dimension (dims 1: 2D tasks, 2: 3D tasks) with its own register bound
-template <bool ACC>
-static cudaError_t launch_gbw_acc(const BatchArgs &a, bool mixed, bool split, int dims, cudaStream_t s) {
-    constexpr int MB3 = ACC ? 3 : 4;  // 3D (and joint) register bound: 45 lane-local sums need ~170 registers
-    if (!split) return mixed ? launch_gbw<true, 3, MB3, ACC>(a, s) : launch_gbw<false, 3, MB3, ACC>(a, s);
-    if (dims == 1) return mixed ? launch_gbw<true, 1, 5, ACC>(a, s) : launch_gbw<false, 1, 5, ACC>(a, s);
-    return mixed ? launch_gbw<true, 2, MB3, ACC>(a, s) : launch_gbw<false, 2, MB3, ACC>(a, s);
+template <bool TC>
+static cudaError_t launch_gbw_tc(const BatchArgs &a, bool mixed, bool split, int dims, cudaStream_t s) {
+    constexpr int MB3 = TC ? 8 : 4;  // 3D (and joint): TC blocks are 2 warps
+    if (!split) return mixed ? launch_gbw<true, 3, MB3, TC>(a, s) : launch_gbw<false, 3, MB3, TC>(a, s);
+    constexpr int MB2 = TC ? 8 : 5;
+    if (dims == 1) return mixed ? launch_gbw<true, 1, MB2, TC>(a, s) : launch_gbw<false, 1, MB2, TC>(a, s);
+    return mixed ? launch_gbw<true, 2, MB3, TC>(a, s) : launch_gbw<false, 2, MB3, TC>(a, s);
 }
 
 // split: one launch per dimension (dims 1: 2D tasks, 2: 3D tasks) with its own register bound
-cudaError_t launch_gbuild_batch_warp(const BatchArgs &a, bool mixed, bool split, int dims, bool acc, cudaStream_t s) {
-    return acc ? launch_gbw_acc<true>(a, mixed, split, dims, s) : launch_gbw_acc<false>(a, mixed, split, dims, s);
+cudaError_t launch_gbuild_batch_warp(const BatchArgs &a, bool mixed, bool split, int dims, bool tc, cudaStream_t s) {
+    return tc ? launch_gbw_tc<true>(a, mixed, split, dims, s) : launch_gbw_tc<false>(a, mixed, split, dims, s);
 }
 
 bool gbuild_warp_supported(int dim, int order) {

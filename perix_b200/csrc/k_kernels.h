@@ -40,8 +40,8 @@ struct GBuildArgs {
 cudaError_t launch_gbuild(const GBuildArgs &a, int dim, int order, bool mixed, int grid, cudaStream_t s);
 bool gbuild_supported(int dim, int order);
 // one warp per node (k_gbuild_warp.cu): FP64 moment sums; MIXED stores FP32 operators (and the order-2 defects)
-// acc: lane-local moment sums reduced once per node (up to nine monomials)
-cudaError_t launch_gbuild_warp(const GBuildArgs &a, int dim, int order, bool mixed, bool acc, cudaStream_t s);
+// tc: moment sums and operator products on the FP64 tensor cores (up to nine monomials)
+cudaError_t launch_gbuild_warp(const GBuildArgs &a, int dim, int order, bool mixed, bool tc, cudaStream_t s);
 bool gbuild_warp_supported(int dim, int order);
 
 // ------------------------------------------------------------------------------ families on the device (A1)
@@ -109,11 +109,11 @@ struct BatchSchedule {
     int lpn2, lpn3;
     bool split;
     bool warp = false;  // g-build: one warp per node (k_gbuild_warp.cu) instead of lane groups
-    bool acc = false;   // g-build, warp per node: lane-local moment sums, one reduce-scatter per node
+    bool tc = false;    // g-build, warp per node: moment sums and operator products on the FP64 tensor cores
     bool hybrid = false;  // g-build, split: lane groups of lpn2 lanes for the 2D clouds, a warp per node for 3D
 };
 constexpr int kBatchVariants = 10;
-cudaError_t launch_gbuild_batch_warp(const BatchArgs &a, bool mixed, bool split, int dims, bool acc, cudaStream_t s);
+cudaError_t launch_gbuild_batch_warp(const BatchArgs &a, bool mixed, bool split, int dims, bool tc, cudaStream_t s);
 BatchSchedule batch_gbuild_schedule(int variant);
 BatchSchedule batch_apply_schedule(int variant);
 // dims: 1 = 2D tasks only, 2 = 3D tasks only, 3 = both

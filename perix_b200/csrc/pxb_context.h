@@ -213,7 +213,7 @@ struct pxb_ctx {
     int device = 0;
     size_t mem_limit = 0;  // device bytes the context may hold (0: no limit beyond the GPU's)
     int gbuild_schedule = -1;  // g-build: -1 by problem, 0 lane groups, 1 one warp per node, 2 the same with
-                               // lane-local moment sums
+                               // its products on the FP64 tensor cores
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
     long long launches = 0;
