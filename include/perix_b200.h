@@ -133,8 +133,8 @@ int pxb_gbuild(pxb_ctx *ctx, int order, int precision, int *n_degenerate, int *f
 /* Schedule of the g-build kernels: 0 lane groups (a group of 8-32 lanes per node; at MIXED the moment sums run in
  * FP32 with two-sum compensation), 1 one warp per node (moment sums in FP64 at both precisions; MIXED stores FP32),
  * 2 the same with its moment sums and per-bond operator products on the FP64 tensor cores (mma m8n8k4; up to nine
- * monomials, larger systems as 1), -1 (default) the one this backend picks: warp per node in 3D and above order 2,
- * lane groups for 2D orders 1-2.
+ * monomials, larger systems as 1), -1 (default) the one this backend picks: warp per node in 3D and above order 2
+ * (with the tensor-core products up to nine monomials), lane groups for 2D orders 1-2.
  * Orders 2D 4 and 3D 3 exist only as the warp-per-node schedule. */
 int pxb_gbuild_set_schedule(pxb_ctx *ctx, int schedule);
 /* nop of the current operator cache and its multi-index table (pqr: 3*nop ints, may be NULL). */

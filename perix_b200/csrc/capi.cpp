@@ -446,8 +446,12 @@ static bool gbuild_use_warp(const pxb_ctx *c, int order) {
 }
 
 static cudaError_t gbuild_launch(pxb_ctx *c, const GBuildArgs &a, int order, bool mixed) {
-    if (gbuild_use_warp(c, order))
-        return launch_gbuild_warp(a, c->g.dim, order, mixed, c->gbuild_schedule == 2, c->stream);
+    if (gbuild_use_warp(c, order)) {
+        // the tensor-core products up to nine monomials unless schedule 1 (scalar warp per node) was chosen
+        const bool small = c->g.dim == 3 ? order <= 2 : order <= 3;
+        const bool tc = c->gbuild_schedule == 2 || (c->gbuild_schedule < 0 && small);
+        return launch_gbuild_warp(a, c->g.dim, order, mixed, tc, c->stream);
+    }
     return launch_gbuild(a, c->g.dim, order, mixed, grid_nodes(c->g.n, kGbuildThreads), c->stream);
 }
 

@@ -204,7 +204,9 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     static_assert(!TC || NOP <= 9, "tensor-core path: up to nine monomials");
     constexpr int MS = kMonoStride;
     const int grp = lane >> 2, tig = lane & 3;  // mma fragment coordinates
-    double c00[2] = {0.0, 0.0}, c01[2] = {0.0, 0.0}, c11[2] = {0.0, 0.0};  // TC: moment tiles (0,0) (0,8) (8,8)
+    // TC: moment tiles (0,0) (0,8) (8,8), two accumulators each (even and odd k-steps: shorter dependency chains)
+    double c00[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, c01[2][2] = {{0.0, 0.0}, {0.0, 0.0}},
+           c11[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     if constexpr (TC) {  // padding rows of the monomial tile stay zero for the node
 #pragma unroll
         for (int p = NOP; p < 16; ++p) sm.monoT[p * MS + lane] = 0.0;
@@ -237,11 +239,11 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
                 const int b = 4 * kk + tig;
                 const double w = sm.wk[b];
                 const double mlo = sm.monoT[grp * MS + b];
-                dmma(c00, w * mlo, mlo);
+                dmma(c00[kk & 1], w * mlo, mlo);
                 if constexpr (NOP > 8) {
                     const double mhi = sm.monoT[(8 + grp) * MS + b];
-                    dmma(c01, w * mlo, mhi);
-                    dmma(c11, w * mhi, mhi);
+                    dmma(c01[kk & 1], w * mlo, mhi);
+                    dmma(c11[kk & 1], w * mhi, mhi);
                 }
             }
             __syncwarp();
@@ -285,10 +287,10 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         };
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            put(grp, 2 * tig + h, c00[h]);
+            put(grp, 2 * tig + h, c00[0][h] + c00[1][h]);
             if constexpr (NOP > 8) {
-                put(grp, 8 + 2 * tig + h, c01[h]);
-                put(8 + grp, 8 + 2 * tig + h, c11[h]);
+                put(grp, 8 + 2 * tig + h, c01[0][h] + c01[1][h]);
+                put(8 + grp, 8 + 2 * tig + h, c11[0][h] + c11[1][h]);
             }
         }
     } else {
@@ -353,6 +355,54 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     solve(x);
     double r[NOP];
     double res = 0.0, maxA = 0.0, maxX = 0.0;
+    if constexpr (TC) {
+        // the residual D - A X on the tensor cores: X (column k in lane k) through shared memory, 8x8 tiles
+#pragma unroll
+        for (int p = 0; p < NOP; ++p) {
+            if (lane < NP) sm.X[p * NP + lane] = lane < NOP ? x[p] : 0.0;
+            maxX = fmax(maxX, fabs(x[p]));
+        }
+        __syncwarp();
+        constexpr int RT = NOP > 8 ? 2 : 1, KS = (NOP + 3) / 4;
+        double rt[RT][RT][2];
+#pragma unroll
+        for (int u = 0; u < RT; ++u)
+#pragma unroll
+            for (int v = 0; v < RT; ++v) rt[u][v][0] = rt[u][v][1] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+            const int kk = 4 * ks + tig;
+            double af[RT], bf[RT];
+#pragma unroll
+            for (int u = 0; u < RT; ++u) {
+                const int row = 8 * u + grp;
+                af[u] = (row < NOP && kk < NOP) ? sm.A[row * NOP + kk] : 0.0;
+                bf[u] = (kk < NOP && row < NOP) ? sm.X[kk * NP + row] : 0.0;  // B[kk][col = 8u + grp]
+                maxA = fmax(maxA, fabs(af[u]));
+            }
+#pragma unroll
+            for (int u = 0; u < RT; ++u)
+#pragma unroll
+                for (int v = 0; v < RT; ++v) dmma(rt[u][v], af[u], bf[v]);
+        }
+#pragma unroll
+        for (int u = 0; u < RT; ++u)
+#pragma unroll
+            for (int v = 0; v < RT; ++v)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int row = 8 * u + grp, col = 8 * v + 2 * tig + h;
+                    if (row < NOP && col < NOP) {
+                        double dv = 0.0;
+#pragma unroll
+                        for (int q = 0; q < NOP; ++q)
+                            if (q == row && q == col) dv = Q.fact[q];
+                        res = fmax(res, fabs(dv - rt[u][v][h]));
+                    }
+                }
+        maxA = group_max<kWarp>(maxA);
+        __syncwarp();  // X is written again below, scaled
+    } else {
 #pragma unroll
     for (int p = 0; p < NOP; ++p) {
         double sres = (p == kc) ? fk : 0.0;
@@ -366,6 +416,7 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         res = fmax(res, fabs(sres));
         maxX = fmax(maxX, fabs(x[p]));
     }
+    }
     // one step of iterative refinement for the larger systems (14, 19 monomials); up to nine monomials the plain
     // solve is already ~1e-14 (family-scaled) from the reference's FullPivLU result, and a refinement step changes
     // nothing measurable there
@@ -374,7 +425,10 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
 #pragma unroll
         for (int q = 0; q < NOP; ++q) x[q] += r[q];
     }
-    if (lane >= NOP) { res = 0.0; maxX = 0.0; }
+    if (lane >= NOP) {
+        maxX = 0.0;
+        if constexpr (!TC) res = 0.0;  // (TC: every lane's residual entries are real ones)
+    }
     res = group_max<kWarp>(res);
     maxX = group_max<kWarp>(maxX);
     double maxB = 0.0;
