@@ -30,7 +30,7 @@ namespace {
 constexpr int kWarpNodeThreads = 128;  // 4 warps (nodes) per block
 constexpr int kBwCache = 256;          // bond weights per node cached for pass 2 (longer families recompute)
 constexpr int kMonoStride = 36;        // row stride (doubles) of the transposed monomial tile: conflict-minimal reads
-constexpr int kOpStride = 9;           // row stride (doubles) of a chunk's operator rows (odd: conflict-minimal)
+constexpr int kOpStride = 9;           // room (doubles) for one bond's staged operator row, up to nine monomials
 
 // packed upper triangle (p <= q, row-major) of an NOP x NOP symmetric matrix
 template <int NOP>
@@ -204,8 +204,10 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     static_assert(!TC || NOP <= 9, "tensor-core path: up to nine monomials");
     constexpr int MS = kMonoStride;
     const int grp = lane >> 2, tig = lane & 3;  // mma fragment coordinates
-    // TC: moment tiles (0,0) (0,8) (8,8), two accumulators each (even and odd k-steps: shorter dependency chains)
-    double c00[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, c01[2][2] = {{0.0, 0.0}, {0.0, 0.0}},
+    // TC: moment tiles (0,0) (0,8) (8,8), two accumulators each (even and odd k-steps: shorter dependency chains);
+    // four for the (0,0) tile when it is the only one (up to eight monomials)
+    constexpr int NA0 = NOP > 8 ? 2 : 4;
+    double c00[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}}, c01[2][2] = {{0.0, 0.0}, {0.0, 0.0}},
            c11[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     if constexpr (TC) {  // padding rows of the monomial tile stay zero for the node
 #pragma unroll
@@ -239,7 +241,7 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
                 const int b = 4 * kk + tig;
                 const double w = sm.wk[b];
                 const double mlo = sm.monoT[grp * MS + b];
-                dmma(c00[kk & 1], w * mlo, mlo);
+                dmma(c00[kk % NA0], w * mlo, mlo);
                 if constexpr (NOP > 8) {
                     const double mhi = sm.monoT[(8 + grp) * MS + b];
                     dmma(c01[kk & 1], w * mlo, mhi);
@@ -281,13 +283,11 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
             if (p <= q && q < NOP) {
                 sm.A[p * NOP + q] = v;
                 sm.A[q * NOP + p] = v;
-                sm.L[p * NOP + q] = v;
-                sm.L[q * NOP + p] = v;
             }
         };
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            put(grp, 2 * tig + h, c00[0][h] + c00[1][h]);
+            put(grp, 2 * tig + h, (c00[0][h] + c00[2][h]) + (c00[1][h] + c00[3][h]));
             if constexpr (NOP > 8) {
                 put(grp, 8 + 2 * tig + h, c01[0][h] + c01[1][h]);
                 put(8 + grp, 8 + 2 * tig + h, c11[0][h] + c11[1][h]);
@@ -307,60 +307,40 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     }
     __syncwarp();
 
-    // ---- solve: A = L D L^T right-looking in sm.L (row r in lane r; D on the diagonal, L below) ----
-    for (int j = 0; j < NOP; ++j) {
-        const double d = sm.L[j * NOP + j];
-        const double cr = (lane > j && lane < NOP) ? sm.L[lane * NOP + j] : 0.0;  // column j before scaling
-        __syncwarp();
-        if (lane > j && lane < NOP) {
-            const double l = cr / d;
-            for (int k = j + 1; k <= lane; ++k) sm.L[lane * NOP + k] -= l * sm.L[k * NOP + j];
-        }
-        __syncwarp();
-        if (lane > j && lane < NOP) sm.L[lane * NOP + j] = cr / d;
-        __syncwarp();
-    }
-    if constexpr (NOP <= 9) {
-        if (lane < NOP) sm.invD[lane] = 1.0 / sm.L[lane * NOP + lane];
-        __syncwarp();
-    }
-    // lane k < NOP: column k of X = A^-1 diag(q!), one refinement step, the consistency test's residual
-    const int kc = lane < NOP ? lane : 0;
-    double fk = 0.0;
-#pragma unroll
-    for (int q = 0; q < NOP; ++q)
-        if (q == kc) fk = Q.fact[q];
-    auto solve = [&](double *x) {
-#pragma unroll
-        for (int r = 0; r < NOP; ++r) {
-#pragma unroll
-            for (int l = 0; l < r; ++l) x[r] -= lds(&sm.L[r * NOP + l]) * x[l];
-        }
-#pragma unroll
-        for (int r = 0; r < NOP; ++r) {
-            // up to nine monomials by the reciprocals (formed once per node); the larger systems divide (fewer
-            // live registers there)
-            if constexpr (NOP <= 9) x[r] *= lds(&sm.invD[r]);
-            else x[r] /= lds(&sm.L[r * NOP + r]);
-        }
-#pragma unroll
-        for (int r = NOP - 1; r >= 0; --r) {
-#pragma unroll
-            for (int l = r + 1; l < NOP; ++l) x[r] -= lds(&sm.L[l * NOP + r]) * x[l];
-        }
-    };
-    double x[NOP];
-#pragma unroll
-    for (int q = 0; q < NOP; ++q) x[q] = (q == kc) ? fk : 0.0;
-    solve(x);
-    double r[NOP];
     double res = 0.0, maxA = 0.0, maxX = 0.0;
+    bool degenerate;
     if constexpr (TC) {
-        // the residual D - A X on the tensor cores: X (column k in lane k) through shared memory, 8x8 tiles
+        // ---- solve (up to nine monomials): Gauss-Jordan on [A | diag(q!)] with row r in lane r's registers; the
+        // pivot row is broadcast by shuffles, so no shared-memory round trip or warp barrier per column.  A is
+        // symmetric positive definite for a usable family (no pivoting, as in the L D L^T path); before step j the
+        // right-hand side of row j is zero past column j.  Lane p < NOP ends with row p of X = A^-1 diag(q!).
+        double ra[NOP], rb[NOP];
 #pragma unroll
-        for (int p = 0; p < NOP; ++p) {
-            if (lane < NP) sm.X[p * NP + lane] = lane < NOP ? x[p] : 0.0;
-            maxX = fmax(maxX, fabs(x[p]));
+        for (int k = 0; k < NOP; ++k) {
+            ra[k] = lane < NOP ? lds(&sm.A[(lane < NOP ? lane : 0) * NOP + k]) : 0.0;
+            rb[k] = (k == lane) ? Q.fact[k] : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < NOP; ++j) {
+            double pa[NOP], pb[NOP];
+#pragma unroll
+            for (int k = j; k < NOP; ++k) pa[k] = __shfl_sync(kFull, ra[k], j);
+#pragma unroll
+            for (int k = 0; k <= j; ++k) pb[k] = __shfl_sync(kFull, rb[k], j);
+            const double inv = 1.0 / pa[j];
+            const bool piv = lane == j;
+            const double f = ra[j] * inv;
+#pragma unroll
+            for (int k = j + 1; k < NOP; ++k) ra[k] = piv ? pa[k] * inv : fma(-f, pa[k], ra[k]);
+#pragma unroll
+            for (int k = 0; k <= j; ++k) rb[k] = piv ? pb[k] * inv : fma(-f, pb[k], rb[k]);
+        }
+        // the consistency test's residual D - A X on the tensor cores (X rows through shared memory, 8x8 tiles)
+        if (lane < NOP) {
+#pragma unroll
+            for (int k = 0; k < NP; ++k) sm.X[lane * NP + k] = k < NOP ? rb[k < NOP ? k : 0] : 0.0;
+#pragma unroll
+            for (int k = 0; k < NOP; ++k) maxX = max_nan(maxX, fabs(rb[k]));
         }
         __syncwarp();
         constexpr int RT = NOP > 8 ? 2 : 1, KS = (NOP + 3) / 4;
@@ -397,46 +377,120 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
 #pragma unroll
                         for (int q = 0; q < NOP; ++q)
                             if (q == row && q == col) dv = Q.fact[q];
-                        res = fmax(res, fabs(dv - rt[u][v][h]));
+                        res = max_nan(res, fabs(dv - rt[u][v][h]));
                     }
                 }
         maxA = group_max<kWarp>(maxA);
+        res = group_max_nan<kWarp>(res);
+        maxX = group_max_nan<kWarp>(maxX);
+        double maxB = 0.0;
+#pragma unroll
+        for (int q = 0; q < NOP; ++q) maxB = fmax(maxB, Q.fact[q]);
+        const double scale = fmax(fmax(maxB, maxA * maxX), DBL_MIN);
+        const bool consistent = (res <= 1.0e-8 * scale);  // NaN-safe: NaN fails
+        degenerate = (usable < NOP) || !consistent;
         __syncwarp();  // X is written again below, scaled
-    } else {
+        // column k carries the operator's scale 1/delta^|q_k|, so that pass 2 only multiplies by the bond weight
+        if (lane < NOP) {
 #pragma unroll
-    for (int p = 0; p < NOP; ++p) {
-        double sres = (p == kc) ? fk : 0.0;
+            for (int k = 0; k < NOP; ++k) {
+                double cs = inv_delta;
 #pragma unroll
-        for (int q = 0; q < NOP; ++q) {
-            const double apq = lds(&sm.A[p * NOP + q]);
-            sres -= apq * x[q];
-            maxA = fmax(maxA, fabs(apq));
+                for (int t2 = 1; t2 < Q.p[k] + Q.q[k] + Q.r[k]; ++t2) cs *= inv_delta;
+                sm.X[lane * NP + k] = degenerate ? 0.0 : rb[k] * cs;
+            }
         }
-        r[p] = sres;
-        res = fmax(res, fabs(sres));
-        maxX = fmax(maxX, fabs(x[p]));
-    }
-    }
-    // one step of iterative refinement for the larger systems (14, 19 monomials); up to nine monomials the plain
-    // solve is already ~1e-14 (family-scaled) from the reference's FullPivLU result, and a refinement step changes
-    // nothing measurable there
-    if constexpr (NOP > 9) {
-        solve(r);
+    } else {
+        // ---- solve: A = L D L^T right-looking in sm.L (row r in lane r; D on the diagonal, L below) ----
+        for (int j = 0; j < NOP; ++j) {
+            const double d = sm.L[j * NOP + j];
+            const double cr = (lane > j && lane < NOP) ? sm.L[lane * NOP + j] : 0.0;  // column j before scaling
+            __syncwarp();
+            if (lane > j && lane < NOP) {
+                const double l = cr / d;
+                for (int k = j + 1; k <= lane; ++k) sm.L[lane * NOP + k] -= l * sm.L[k * NOP + j];
+            }
+            __syncwarp();
+            if (lane > j && lane < NOP) sm.L[lane * NOP + j] = cr / d;
+            __syncwarp();
+        }
+        if constexpr (NOP <= 9) {
+            if (lane < NOP) sm.invD[lane] = 1.0 / sm.L[lane * NOP + lane];
+            __syncwarp();
+        }
+        // lane k < NOP: column k of X = A^-1 diag(q!), one refinement step, the consistency test's residual
+        const int kc = lane < NOP ? lane : 0;
+        double fk = 0.0;
 #pragma unroll
-        for (int q = 0; q < NOP; ++q) x[q] += r[q];
-    }
-    if (lane >= NOP) {
-        maxX = 0.0;
-        if constexpr (!TC) res = 0.0;  // (TC: every lane's residual entries are real ones)
-    }
-    res = group_max<kWarp>(res);
-    maxX = group_max<kWarp>(maxX);
-    double maxB = 0.0;
+        for (int q = 0; q < NOP; ++q)
+            if (q == kc) fk = Q.fact[q];
+        auto solve = [&](double *x) {
 #pragma unroll
-    for (int q = 0; q < NOP; ++q) maxB = fmax(maxB, Q.fact[q]);
-    const double scale = fmax(fmax(maxB, maxA * maxX), DBL_MIN);
-    const bool consistent = (res <= 1.0e-8 * scale);  // NaN-safe: NaN fails
-    const bool degenerate = (usable < NOP) || !consistent;
+            for (int r = 0; r < NOP; ++r) {
+#pragma unroll
+                for (int l = 0; l < r; ++l) x[r] -= lds(&sm.L[r * NOP + l]) * x[l];
+            }
+#pragma unroll
+            for (int r = 0; r < NOP; ++r) {
+                // up to nine monomials by the reciprocals (formed once per node); the larger systems divide (fewer
+                // live registers there)
+                if constexpr (NOP <= 9) x[r] *= lds(&sm.invD[r]);
+                else x[r] /= lds(&sm.L[r * NOP + r]);
+            }
+#pragma unroll
+            for (int r = NOP - 1; r >= 0; --r) {
+#pragma unroll
+                for (int l = r + 1; l < NOP; ++l) x[r] -= lds(&sm.L[l * NOP + r]) * x[l];
+            }
+        };
+        double x[NOP];
+#pragma unroll
+        for (int q = 0; q < NOP; ++q) x[q] = (q == kc) ? fk : 0.0;
+        solve(x);
+        double r[NOP];
+#pragma unroll
+        for (int p = 0; p < NOP; ++p) {
+            double sres = (p == kc) ? fk : 0.0;
+#pragma unroll
+            for (int q = 0; q < NOP; ++q) {
+                const double apq = lds(&sm.A[p * NOP + q]);
+                sres -= apq * x[q];
+                maxA = fmax(maxA, fabs(apq));
+            }
+            r[p] = sres;
+            res = fmax(res, fabs(sres));
+            maxX = fmax(maxX, fabs(x[p]));
+        }
+        // one step of iterative refinement for the larger systems (14, 19 monomials); up to nine monomials the plain
+        // solve is already ~1e-14 (family-scaled) from the reference's FullPivLU result, and a refinement step changes
+        // nothing measurable there
+        if constexpr (NOP > 9) {
+            solve(r);
+#pragma unroll
+            for (int q = 0; q < NOP; ++q) x[q] += r[q];
+        }
+        if (lane >= NOP) {
+            maxX = 0.0;
+            res = 0.0;
+        }
+        res = group_max<kWarp>(res);
+        maxX = group_max<kWarp>(maxX);
+        double maxB = 0.0;
+#pragma unroll
+        for (int q = 0; q < NOP; ++q) maxB = fmax(maxB, Q.fact[q]);
+        const double scale = fmax(fmax(maxB, maxA * maxX), DBL_MIN);
+        const bool consistent = (res <= 1.0e-8 * scale);  // NaN-safe: NaN fails
+        degenerate = (usable < NOP) || !consistent;
+        // column k carries the operator's scale 1/delta^|q_k|, so that pass 2 only multiplies by the bond weight
+        int ord = 1;  // |q_k| of this lane's column: the monomials are ordered by total degree
+        while (ord < ORDER && kc >= nop_of(DIM, ord)) ++ord;
+        double colscale = inv_delta;
+        for (int t2 = 1; t2 < ord; ++t2) colscale *= inv_delta;
+        if (lane < NP) {
+#pragma unroll
+            for (int p = 0; p < NOP; ++p) sm.X[p * NP + lane] = (degenerate || lane >= NOP) ? 0.0 : x[p] * colscale;
+        }
+    }
     const bool deep_ghost = (a.layer != nullptr) && (a.layer[i] > 1);
     if (lane == 0) {
         if (a.degenerate) a.degenerate[i] = degenerate ? 1 : 0;
@@ -444,15 +498,6 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
             atomicAdd(a.n_degenerate, 1u);
             atomicMin(a.first_degenerate, i);
         }
-    }
-    // column k carries the operator's scale 1/delta^|q_k|, so that pass 2 only multiplies by the bond weight
-    int ord = 1;  // |q_k| of this lane's column: the monomials are ordered by total degree
-    while (ord < ORDER && kc >= nop_of(DIM, ord)) ++ord;
-    double colscale = inv_delta;
-    for (int t2 = 1; t2 < ord; ++t2) colscale *= inv_delta;
-    if (lane < NP) {
-#pragma unroll
-        for (int p = 0; p < NOP; ++p) sm.X[p * NP + lane] = (degenerate || lane >= NOP) ? 0.0 : x[p] * colscale;
     }
     __syncwarp();
 
@@ -484,27 +529,17 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         }
         return g;
     };
-    // one bond's operator vector out: AoS operators (MIXED: FP32 and the defect's first moments), Navier subset
-    auto emit = [&](int t, const BondGeo &g, const double *op) {
-        if (a.ops) {
-            if constexpr (MIXED) {
-                float *o = static_cast<float *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
+    // the defect's first moments of one bond's stored (FP32) second-derivative operators and its Navier subset
+    auto emit_rest = [&](int t, const BondGeo &g, const double *op) {
+        if constexpr (DEF) {
+            if (a.ops) {
 #pragma unroll
-                for (int k = 0; k < NOP; ++k) {
+                for (int k = DIM; k < NOP; ++k) {
                     const float gk = (float)op[k];
-                    o[k] = gk;
-                    if constexpr (DEF) {
-                        if (k >= DIM) {
-                            dsum[(k - DIM) * DIM + 0] += (double)gk * g.dx;
-                            dsum[(k - DIM) * DIM + 1] += (double)gk * g.dy;
-                            if constexpr (DIM == 3) dsum[(k - DIM) * DIM + 2] += (double)gk * g.dz;
-                        }
-                    }
+                    dsum[(k - DIM) * DIM + 0] += (double)gk * g.dx;
+                    dsum[(k - DIM) * DIM + 1] += (double)gk * g.dy;
+                    if constexpr (DIM == 3) dsum[(k - DIM) * DIM + 2] += (double)gk * g.dz;
                 }
-            } else {
-                double *o = static_cast<double *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
-#pragma unroll
-                for (int k = 0; k < NOP; ++k) o[k] = op[k];
             }
         }
         if constexpr (ORDER >= 2) {
@@ -526,8 +561,25 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
             }
         }
     };
+    // one bond's operator vector out: AoS operators (MIXED: FP32), then the defect moments and the Navier subset
+    auto emit = [&](int t, const BondGeo &g, const double *op) {
+        if (a.ops) {
+            if constexpr (MIXED) {
+                float *o = static_cast<float *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
+#pragma unroll
+                for (int k = 0; k < NOP; ++k) o[k] = (float)op[k];
+            } else {
+                double *o = static_cast<double *>(a.ops) + (size_t)(t - a.bond_base) * NOP;
+#pragma unroll
+                for (int k = 0; k < NOP; ++k) o[k] = op[k];
+            }
+        }
+        emit_rest(t, g, op);
+    };
     // TC: X as B fragments (rows = monomials in k-steps of 4, columns = operators in tiles of 8), zero past NOP
     constexpr int KS = (NOP + 3) / 4, NT2 = NOP > 8 ? 2 : 1;
+    constexpr int BTG = NT2 > 1 ? 2 : 4;  // 8-bond tiles whose DMMA chains run interleaved
+    constexpr int OS = NOP | 1;           // row stride (doubles) of the staged operator rows: odd, conflict-free
     double bx[TC ? KS : 1][TC ? NT2 : 1];
     if constexpr (TC) {
 #pragma unroll
@@ -549,33 +601,58 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
             for (int p = 0; p < NOP; ++p) sm.monoT[p * MS + lane] = m[p];
             sm.wk[lane] = g.bw;
             __syncwarp();
+            // 8-bond tiles D[bond][k] = sum_p m_p(bond) X[p][k], BTG tiles at a time so that their DMMA chains
+            // interleave
 #pragma unroll
-            for (int bt = 0; bt < 4; ++bt) {  // 8-bond tiles: D[bond][k] = sum_p m_p(bond) X[p][k]
-                double d0[2] = {0.0, 0.0}, d1[2] = {0.0, 0.0};
+            for (int bg = 0; bg < 4; bg += BTG) {
+                double dd[BTG][NT2][2];
+#pragma unroll
+                for (int u = 0; u < BTG; ++u)
+#pragma unroll
+                    for (int nt = 0; nt < NT2; ++nt) dd[u][nt][0] = dd[u][nt][1] = 0.0;
 #pragma unroll
                 for (int ks = 0; ks < KS; ++ks) {
-                    const double am = sm.monoT[(4 * ks + tig) * MS + 8 * bt + grp];
-                    dmma(d0, am, bx[ks][0]);
-                    if constexpr (NT2 > 1) dmma(d1, am, bx[ks][NT2 - 1]);
-                }
-                const double w = sm.wk[8 * bt + grp];
-                const int row = (8 * bt + grp) * kOpStride;
+                    double am[BTG];
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int k0 = 2 * tig + h;
-                    if (k0 < NOP) sm.opb[row + k0] = w * d0[h];
-                    if constexpr (NT2 > 1) {
-                        const int k1 = 8 + 2 * tig + h;
-                        if (k1 < NOP) sm.opb[row + k1] = w * d1[h];
-                    }
+                    for (int u = 0; u < BTG; ++u) am[u] = sm.monoT[(4 * ks + tig) * MS + 8 * (bg + u) + grp];
+#pragma unroll
+                    for (int u = 0; u < BTG; ++u)
+#pragma unroll
+                        for (int nt = 0; nt < NT2; ++nt) dmma(dd[u][nt], am[u], bx[ks][nt]);
+                }
+#pragma unroll
+                for (int u = 0; u < BTG; ++u) {
+                    const double w = sm.wk[8 * (bg + u) + grp];
+                    const int row = (8 * (bg + u) + grp) * OS;
+#pragma unroll
+                    for (int nt = 0; nt < NT2; ++nt)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int k = 8 * nt + 2 * tig + h;
+                            if (k < NOP) sm.opb[row + k] = w * dd[u][nt][h];
+                        }
                 }
             }
             __syncwarp();
-            if (t < b1) {
+            // the chunk's operator vectors are one contiguous AoS block: coalesced stores from the staged rows
+            const int nval = b1 - c0 < kWarp ? b1 - c0 : kWarp;
+            if (a.ops) {
+#pragma unroll
+                for (int e0 = 0; e0 < NOP; ++e0) {
+                    const int e = e0 * kWarp + lane;
+                    if (e < nval * NOP) {
+                        const double v = sm.opb[(e / NOP) * OS + e % NOP];
+                        const size_t o = (size_t)(c0 - a.bond_base) * NOP + e;
+                        if constexpr (MIXED) static_cast<float *>(a.ops)[o] = (float)v;
+                        else static_cast<double *>(a.ops)[o] = v;
+                    }
+                }
+            }
+            if (t < b1 && (a.G || (DEF && a.ops && a.defect))) {
                 double op[NOP];
 #pragma unroll
-                for (int k = 0; k < NOP; ++k) op[k] = sm.opb[lane * kOpStride + k];
-                emit(t, g, op);
+                for (int k = 0; k < NOP; ++k) op[k] = sm.opb[lane * OS + k];
+                emit_rest(t, g, op);
             }
             __syncwarp();
         } else {
