@@ -123,11 +123,9 @@ struct NodeWeight {
 // |xi|^2 (a few ulps from the reference's rounding of 2|xi|/delta); |xi| itself is formed only for rim bonds and
 // for the own-horizon test
 template <int DIM, typename PosT>
-__device__ __forceinline__ BondGeo bond_geo(const GBuildArgs &a, const PosT *pos, const PosT &xi, int t,
-                                            const NodeWeight &nw, bool own_horizon) {
+__device__ __forceinline__ BondGeo bond_geo_at(const PosT &xj, double vj, const PosT &xi, const NodeWeight &nw,
+                                               bool own_horizon) {
     BondGeo g{0.0, 0.0, 0.0, 0.0};
-    const int j = a.nbr[t];
-    const PosT xj = pos[j - a.node_base];
     g.dx = xj.x - xi.x;
     g.dy = xj.y - xi.y;
     if constexpr (DIM == 3) g.dz = xj.z - xi.z;
@@ -135,10 +133,17 @@ __device__ __forceinline__ BondGeo bond_geo(const GBuildArgs &a, const PosT *pos
     if (r2 > 0.0 && !(own_horizon && sqrt(r2) > nw.delta)) {
         double bw = exp(-(r2 * nw.four_inv_d2));
         if (nw.dxc > 0.0 && r2 > nw.rim2) bw *= rim_correction(sqrt(r2), nw.delta, nw.dxc);
-        bw *= a.vol[j];
+        bw *= vj;
         if (bw > 0.0) g.bw = bw;
     }
     return g;
+}
+
+template <int DIM, typename PosT>
+__device__ __forceinline__ BondGeo bond_geo(const GBuildArgs &a, const PosT *pos, const PosT &xi, int t,
+                                            const NodeWeight &nw, bool own_horizon) {
+    const int j = a.nbr[t];
+    return bond_geo_at<DIM>(pos[j - a.node_base], a.vol[j], xi, nw, own_horizon);
 }
 
 }  // namespace
@@ -216,10 +221,34 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     int usable = 0;
     {
     const NodeWeight nw(delta, dxc);
+    // TC: the gathers run ahead of the chunk being summed (neighbour ids two chunks, their positions and volumes
+    // one chunk), so that their latency overlaps the moment products of the chunk before
+    int jn = -1;
+    PosT xq{};
+    double vq = 0.0;
+    if constexpr (TC) {
+        const int j0 = b0 + lane < b1 ? a.nbr[b0 + lane] : -1;
+        if (j0 >= 0) {
+            xq = pos[j0 - a.node_base];
+            vq = a.vol[j0];
+        }
+        jn = b0 + kWarp + lane < b1 ? a.nbr[b0 + kWarp + lane] : -1;
+    }
     for (int c0 = b0; c0 < b1; c0 += kWarp) {
         const int t = c0 + lane;
         BondGeo g{0.0, 0.0, 0.0, 0.0};
-        if (t < b1) g = bond_geo<DIM>(a, pos, xi, t, nw, own_h);
+        if constexpr (TC) {
+            const PosT xj = xq;
+            const double vj = vq;
+            if (jn >= 0) {
+                xq = pos[jn - a.node_base];
+                vq = a.vol[jn];
+            }
+            jn = t + 2 * kWarp < b1 ? a.nbr[t + 2 * kWarp] : -1;
+            if (t < b1) g = bond_geo_at<DIM>(xj, vj, xi, nw, own_h);
+        } else {
+            if (t < b1) g = bond_geo<DIM>(a, pos, xi, t, nw, own_h);
+        }
         if (t < b1 && t - b0 < BWC) {
             sm.bw[t - b0] = g.bw;
             if constexpr (XCACHE) {
@@ -504,9 +533,11 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     // ---- pass 2: per-bond operators ----
     constexpr bool DEF = MIXED && ORDER == 2;
     constexpr int ND = DEF ? (NOP - DIM) * DIM : 1;
-    double dsum[ND];
+    // scalar path: per-lane defect sums; TC: a tensor-core tile D[k - DIM][d] (two accumulators)
+    double dsum[TC ? 1 : ND];
 #pragma unroll
-    for (int e = 0; e < ND; ++e) dsum[e] = 0.0;
+    for (int e = 0; e < (TC ? 1 : ND); ++e) dsum[e] = 0.0;
+    double dfc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     // the bond's geometry in pass 2: cached in pass 1, or formed again past the cache
     auto geo2 = [&](int t) -> BondGeo {
         BondGeo g;
@@ -531,7 +562,7 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     };
     // the defect's first moments of one bond's stored (FP32) second-derivative operators and its Navier subset
     auto emit_rest = [&](int t, const BondGeo &g, const double *op) {
-        if constexpr (DEF) {
+        if constexpr (DEF && !TC) {
             if (a.ops) {
 #pragma unroll
                 for (int k = DIM; k < NOP; ++k) {
@@ -648,7 +679,23 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
                     }
                 }
             }
-            if (t < b1 && (a.G || (DEF && a.ops && a.defect))) {
+            if constexpr (DEF) {
+                // the defect's first moments sum_b g_k(b) xi_d(b) as (G^T M) over the chunk's 4-bond k-steps:
+                // A[k - DIM][b] the stored (FP32) second-derivative operators, B[b][d] the first-order monomials
+                // xi_d / delta of the tile (the factor delta is applied once at the end)
+                if (a.ops && a.defect) {
+#pragma unroll
+                    for (int kk = 0; kk < 8; ++kk) {
+                        const int b = 4 * kk + tig;
+                        const double ga = grp < NOP - DIM
+                                              ? (double)(float)sm.opb[b * OS + (grp < NOP - DIM ? DIM + grp : 0)]
+                                              : 0.0;
+                        const double xb = grp < DIM ? sm.monoT[(grp < DIM ? grp : 0) * MS + b] : 0.0;
+                        dmma(dfc[kk & 1], ga, xb);
+                    }
+                }
+            }
+            if (t < b1 && a.G) {
                 double op[NOP];
 #pragma unroll
                 for (int k = 0; k < NOP; ++k) op[k] = sm.opb[lane * OS + k];
@@ -680,10 +727,22 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     if constexpr (DEF) {
         if (a.defect) {
             float *dst = a.defect + (size_t)(i - a.node_base) * ND;
+            if constexpr (TC) {
+                if (a.ops) {  // lane (grp, tig) holds D[grp][2 tig + h]
 #pragma unroll
-            for (int e = 0; e < ND; ++e) {
-                const double v = group_sum<kWarp>(dsum[e]);
-                if (lane == (e & 31)) dst[e] = (float)v;
+                    for (int h = 0; h < 2; ++h) {
+                        const int d = 2 * tig + h;
+                        if (grp < NOP - DIM && d < DIM) dst[grp * DIM + d] = (float)((dfc[0][h] + dfc[1][h]) * delta);
+                    }
+                } else {
+                    if (lane < ND) dst[lane] = 0.0f;
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < ND; ++e) {
+                    const double v = group_sum<kWarp>(dsum[e]);
+                    if (lane == (e & 31)) dst[e] = (float)v;
+                }
             }
         }
     }
