@@ -162,16 +162,18 @@ struct WarpNodeSmem {
     // every section starts on a 16-byte boundary (X is read as double2)
     alignas(16) double bw[BWC];
     alignas(16) double xc[3 * XC];
-    alignas(16) double A[NOP * NOP];
-    alignas(16) double L[NOP * NOP];
-    alignas(16) double X[NOP * NP];
-    alignas(16) double invD[NP];  // 1 / D of the L D L^T factorisation
     // TC (up to nine monomials): a chunk's monomials transposed [p][bond] (rows padded to 16, row stride kMonoStride),
-    // its bond weights and its operator rows
+    // its bond weights and its operator rows, and column 8 of X (the ninth operator is formed on the CUDA cores);
+    // the L D L^T factors of the scalar path are not kept
     static constexpr bool TCA = TC && NOP <= 9;
+    alignas(16) double A[NOP * NOP];
+    alignas(16) double L[TCA ? 2 : NOP * NOP];
+    alignas(16) double X[NOP * NP];
+    alignas(16) double invD[TCA ? 2 : NP];  // 1 / D of the L D L^T factorisation
     alignas(16) double monoT[TCA ? 16 * kMonoStride : 2];
     alignas(16) double wk[TCA ? 32 : 2];
     alignas(16) double opb[TCA ? 32 * kOpStride : 2];
+    alignas(16) double c8[TCA ? NP : 2];
 };
 static_assert(offsetof(WarpNodeSmem<14>, X) % 16 == 0 && offsetof(WarpNodeSmem<19>, X) % 16 == 0 &&
                   offsetof(WarpNodeSmem<9>, X) % 16 == 0 && offsetof(WarpNodeSmem<5>, X) % 16 == 0,
@@ -209,11 +211,14 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     static_assert(!TC || NOP <= 9, "tensor-core path: up to nine monomials");
     constexpr int MS = kMonoStride;
     const int grp = lane >> 2, tig = lane & 3;  // mma fragment coordinates
-    // TC: moment tiles (0,0) (0,8) (8,8), two accumulators each (even and odd k-steps: shorter dependency chains);
-    // four for the (0,0) tile when it is the only one (up to eight monomials)
-    constexpr int NA0 = NOP > 8 ? 2 : 4;
-    double c00[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}}, c01[2][2] = {{0.0, 0.0}, {0.0, 0.0}},
-           c11[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    // TC: the moment tile (0,0) on the tensor cores, four accumulators (k-steps modulo 4: shorter dependency
+    // chains); with nine monomials the ninth row A[p][8] = sum bw m_p m_8 is summed per lane on the CUDA cores and
+    // reduce-scattered once per node (an (0,8) and an (8,8) tile would use one column of eight)
+    double c00[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    constexpr int N8 = NOP > 8 ? NOP : 1;
+    double a8[N8];
+#pragma unroll
+    for (int p = 0; p < N8; ++p) a8[p] = 0.0;
     if constexpr (TC) {  // padding rows of the monomial tile stay zero for the node
 #pragma unroll
         for (int p = NOP; p < 16; ++p) sm.monoT[p * MS + lane] = 0.0;
@@ -262,20 +267,20 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         monomials<DIM, ORDER, double>(g.dx * inv_delta, g.dy * inv_delta, g.dz * inv_delta, m);
         if constexpr (TC) {
 #pragma unroll
-            for (int p = 0; p < NOP; ++p) sm.monoT[p * MS + lane] = m[p];
+            for (int p = 0; p < (NOP < 8 ? NOP : 8); ++p) sm.monoT[p * MS + lane] = m[p];
             sm.wk[lane] = g.bw;
+            if constexpr (NOP > 8) {
+                const double wm8 = g.bw * m[8];
+#pragma unroll
+                for (int p = 0; p < NOP; ++p) a8[p] = fma(wm8, m[p], a8[p]);
+            }
             __syncwarp();
 #pragma unroll
             for (int kk = 0; kk < 8; ++kk) {  // k-steps of 4 bonds: A frag bw_b m_p(b), B frag m_q(b)
                 const int b = 4 * kk + tig;
                 const double w = sm.wk[b];
                 const double mlo = sm.monoT[grp * MS + b];
-                dmma(c00[kk % NA0], w * mlo, mlo);
-                if constexpr (NOP > 8) {
-                    const double mhi = sm.monoT[(8 + grp) * MS + b];
-                    dmma(c01[kk & 1], w * mlo, mhi);
-                    dmma(c11[kk & 1], w * mhi, mhi);
-                }
+                dmma(c00[kk & 3], w * mlo, mlo);
             }
             __syncwarp();
         } else {
@@ -315,12 +320,17 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
             }
         };
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            put(grp, 2 * tig + h, (c00[0][h] + c00[2][h]) + (c00[1][h] + c00[3][h]));
-            if constexpr (NOP > 8) {
-                put(grp, 8 + 2 * tig + h, c01[0][h] + c01[1][h]);
-                put(8 + grp, 8 + 2 * tig + h, c11[0][h] + c11[1][h]);
-            }
+        for (int h = 0; h < 2; ++h) put(grp, 2 * tig + h, (c00[0][h] + c00[2][h]) + (c00[1][h] + c00[3][h]));
+        if constexpr (NOP > 8) {  // the ninth row: five halvings leave entry rs_entry(lane) of a8 in lane
+            static_assert(NOP == 9, "tensor-core path: up to nine monomials");
+            double v1[5], v2[3], v3[2], v4[1], v5[1];
+            rs_level<9, 16>(a8, v1, (lane & 16) != 0);
+            rs_level<5, 8>(v1, v2, (lane & 8) != 0);
+            rs_level<3, 4>(v2, v3, (lane & 4) != 0);
+            rs_level<2, 2>(v3, v4, (lane & 2) != 0);
+            rs_level<1, 1>(v4, v5, (lane & 1) != 0);
+            const int e = rs_entry<9>(lane, 0);
+            if (e >= 0) put(e, 8, v5[0]);
         }
     } else {
 #pragma unroll
@@ -427,6 +437,7 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
 #pragma unroll
                 for (int t2 = 1; t2 < Q.p[k] + Q.q[k] + Q.r[k]; ++t2) cs *= inv_delta;
                 sm.X[lane * NP + k] = degenerate ? 0.0 : rb[k] * cs;
+                if (k == 8) sm.c8[lane < NOP ? lane : 0] = degenerate ? 0.0 : rb[k] * cs;
             }
         }
     } else {
@@ -608,8 +619,9 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
         emit_rest(t, g, op);
     };
     // TC: X as B fragments (rows = monomials in k-steps of 4, columns = operators in tiles of 8), zero past NOP
-    constexpr int KS = (NOP + 3) / 4, NT2 = NOP > 8 ? 2 : 1;
-    constexpr int BTG = NT2 > 1 ? 2 : 4;  // 8-bond tiles whose DMMA chains run interleaved
+    // (operators 0..7 on the tensor cores; the ninth, when there is one, per lane on the CUDA cores)
+    constexpr int KS = (NOP + 3) / 4, NT2 = 1;
+    constexpr int BTG = 4;  // 8-bond tiles whose DMMA chains run interleaved
     constexpr int OS = NOP | 1;           // row stride (doubles) of the staged operator rows: odd, conflict-free
     double bx[TC ? KS : 1][TC ? NT2 : 1];
     if constexpr (TC) {
@@ -631,6 +643,12 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
 #pragma unroll
             for (int p = 0; p < NOP; ++p) sm.monoT[p * MS + lane] = m[p];
             sm.wk[lane] = g.bw;
+            if constexpr (NOP > 8) {  // op_8 = bw sum_p m_p X[p][8]
+                double s8 = 0.0;
+#pragma unroll
+                for (int p = 0; p < NOP; ++p) s8 = fma(m[p], lds(&sm.c8[p]), s8);
+                sm.opb[lane * OS + 8] = g.bw * s8;
+            }
             __syncwarp();
             // 8-bond tiles D[bond][k] = sum_p m_p(bond) X[p][k], BTG tiles at a time so that their DMMA chains
             // interleave
