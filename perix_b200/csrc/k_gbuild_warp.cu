@@ -622,6 +622,16 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
     // (operators 0..7 on the tensor cores; the ninth, when there is one, per lane on the CUDA cores)
     constexpr int KS = (NOP + 3) / 4, NT2 = 1;
     constexpr int BTG = 4;  // 8-bond tiles whose DMMA chains run interleaved
+    // the chunk's operator rows: FP64, or MIXED the stored FP32 values (rounded once, where they are staged)
+    float *const opf = reinterpret_cast<float *>(sm.opb);
+    auto stage = [&](int idx, double v) {
+        if constexpr (MIXED) opf[idx] = (float)v;
+        else sm.opb[idx] = v;
+    };
+    auto staged = [&](int idx) -> double {
+        if constexpr (MIXED) return (double)opf[idx];
+        else return sm.opb[idx];
+    };
     constexpr int OS = NOP | 1;           // row stride (doubles) of the staged operator rows: odd, conflict-free
     double bx[TC ? KS : 1][TC ? NT2 : 1];
     if constexpr (TC) {
@@ -646,8 +656,12 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
             if constexpr (NOP > 8) {  // op_8 = bw sum_p m_p X[p][8]
                 double s8 = 0.0;
 #pragma unroll
-                for (int p = 0; p < NOP; ++p) s8 = fma(m[p], lds(&sm.c8[p]), s8);
-                sm.opb[lane * OS + 8] = g.bw * s8;
+                for (int p = 0; p < NOP; p += 2) {
+                    const double2 cp = lds2(&sm.c8[p]);  // c8 is padded to an even count
+                    s8 = fma(m[p], cp.x, s8);
+                    if (p + 1 < NOP) s8 = fma(m[p + 1 < NOP ? p + 1 : 0], cp.y, s8);
+                }
+                stage(lane * OS + 8, g.bw * s8);
             }
             __syncwarp();
             // 8-bond tiles D[bond][k] = sum_p m_p(bond) X[p][k], BTG tiles at a time so that their DMMA chains
@@ -678,7 +692,7 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
                             const int k = 8 * nt + 2 * tig + h;
-                            if (k < NOP) sm.opb[row + k] = w * dd[u][nt][h];
+                            if (k < NOP) stage(row + k, w * dd[u][nt][h]);
                         }
                 }
             }
@@ -686,14 +700,16 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
             // the chunk's operator vectors are one contiguous AoS block: coalesced stores from the staged rows
             const int nval = b1 - c0 < kWarp ? b1 - c0 : kWarp;
             if (a.ops) {
+                const size_t o0 = (size_t)(c0 - a.bond_base) * NOP + lane;
+                float *const of = static_cast<float *>(a.ops) + o0;
+                double *const od = static_cast<double *>(a.ops) + o0;
 #pragma unroll
                 for (int e0 = 0; e0 < NOP; ++e0) {
                     const int e = e0 * kWarp + lane;
                     if (e < nval * NOP) {
-                        const double v = sm.opb[(e / NOP) * OS + e % NOP];
-                        const size_t o = (size_t)(c0 - a.bond_base) * NOP + e;
-                        if constexpr (MIXED) static_cast<float *>(a.ops)[o] = (float)v;
-                        else static_cast<double *>(a.ops)[o] = v;
+                        const int si = OS == NOP ? e : (e / NOP) * OS + e % NOP;
+                        if constexpr (MIXED) of[e0 * kWarp] = opf[si];
+                        else od[e0 * kWarp] = sm.opb[si];
                     }
                 }
             }
@@ -706,7 +722,7 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
                     for (int kk = 0; kk < 8; ++kk) {
                         const int b = 4 * kk + tig;
                         const double ga = grp < NOP - DIM
-                                              ? (double)(float)sm.opb[b * OS + (grp < NOP - DIM ? DIM + grp : 0)]
+                                              ? (double)opf[b * OS + (grp < NOP - DIM ? DIM + grp : 0)]
                                               : 0.0;
                         const double xb = grp < DIM ? sm.monoT[(grp < DIM ? grp : 0) * MS + b] : 0.0;
                         dmma(dfc[kk & 1], ga, xb);
@@ -716,7 +732,7 @@ __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int
             if (t < b1 && a.G) {
                 double op[NOP];
 #pragma unroll
-                for (int k = 0; k < NOP; ++k) op[k] = sm.opb[lane * OS + k];
+                for (int k = 0; k < NOP; ++k) op[k] = staged(lane * OS + k);
                 emit_rest(t, g, op);
             }
             __syncwarp();
