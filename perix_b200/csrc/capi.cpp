@@ -703,6 +703,10 @@ static EpfArgs epf_args(pxb_ctx *c) {
         a.sc_bond = e.sc_bond.as<double>();
         a.damage = 1;
     }
+    {  // displacement-first clear-hold bound (uniform critical stretch only)
+        const double s = e.sc * (1.0 - 1.0e-6) - 1.0e-12;
+        a.e2_hold = (e.sc > 0.0 && s > 0.0 && e.r2min > 0.0 && std::isfinite(e.r2min)) ? s * s * e.r2min : 0.0;
+    }
     return a;
 }
 
@@ -746,12 +750,21 @@ extern "C" int pxb_epf_setup(pxb_ctx *c, int precision, double C11, double C12, 
     PXB_CUDA_TRY(launch_navier_pack(e.G.p, e.P.p, (long long)ldb, g.dim, precision == PXB_MIXED, C11, C12, C66,
                                     c->stream));
     PXB_TRY(check_launch(c, "navier pack"));
-    {  // the staged kernels' FP32 bond vectors (the stretch pre-test of the configurations that stage them)
+    {  // the staged kernels' FP32 bond vectors (the stretch pre-test of the configurations that stage them) and the
+       // smallest bond length (the displacement-first test), its key computed in the spare counter slot 5
         PXB_TRY(dev_alloc(c, e.xib, sizeof(float) * (size_t)g.dim * ldb));
         PXB_CUDA_TRY(cudaMemsetAsync(e.xib.p, 0, e.xib.bytes, c->stream));
+        unsigned long long *key = e.counters.as<unsigned long long>() + 5;
+        const unsigned long long inf_key = 0x7ff0000000000000ULL;
+        PXB_TRY(h2d(c, key, &inf_key, sizeof(inf_key)));
         PXB_CUDA_TRY(launch_bond_vectors(g.n, g.dim, g.off.as<int>(), g.nbr.as<int>(), g.pos.p, (long long)ldb,
-                                         e.xib.as<float>(), c->stream));
+                                         e.xib.as<float>(), key, c->stream));
         PXB_TRY(check_launch(c, "bond vectors"));
+        unsigned long long k2 = inf_key;
+        PXB_TRY(d2h(c, &k2, key, sizeof(k2)));
+        PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        std::memcpy(&e.r2min, &k2, sizeof(double));
+        PXB_CUDA_TRY(cudaMemsetAsync(key, 0, sizeof(unsigned long long), c->stream));
     }
     // Bond streams larger than the L2 are staged as evict-first, so that the node rows the neighbour gathers reuse
     // stay resident; streams that fit are left to stay in L2 from one step to the next.

@@ -671,25 +671,39 @@ __global__ void navier_pack_kernel(const T *G, T *P, long long ldb, double C11, 
 }
 
 template <int DIM>
-__global__ void bond_vector_kernel(int n, const int *off, const int *nbr, const void *pos, long long ldb, float *xib) {
+__global__ void bond_vector_kernel(int n, const int *off, const int *nbr, const void *pos, long long ldb, float *xib,
+                                   unsigned long long *r2min_key) {
     using PosT = typename Vec<DIM>::T;
     const PosT *p = static_cast<const PosT *>(pos);
+    double r2min = __longlong_as_double(0x7ff0000000000000LL);  // +inf
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const PosT xi = p[i];
         for (int t = off[i]; t < off[i + 1]; ++t) {
             const PosT xj = p[nbr[t]];
-            xib[t] = (float)(xj.x - xi.x);
-            xib[ldb + t] = (float)(xj.y - xi.y);
-            if constexpr (DIM == 3) xib[2 * ldb + t] = (float)(xj.z - xi.z);
+            const double dx = __dsub_rn(xj.x, xi.x), dy = __dsub_rn(xj.y, xi.y);
+            xib[t] = (float)dx;
+            xib[ldb + t] = (float)dy;
+            double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+            if constexpr (DIM == 3) {
+                const double dz = __dsub_rn(xj.z, xi.z);
+                xib[2 * ldb + t] = (float)dz;
+                r2 = __dadd_rn(r2, __dmul_rn(dz, dz));
+            }
+            if (r2 > 0.0 && r2 < r2min) r2min = r2;
         }
+    }
+    if (r2min_key) {  // positive doubles order as their bit patterns
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r2min = fmin(r2min, __shfl_xor_sync(kFull, r2min, o));
+        if ((threadIdx.x & 31) == 0) atomicMin(r2min_key, dbl_key(r2min));
     }
 }
 
 cudaError_t launch_bond_vectors(int n, int dim, const int *off, const int *nbr, const void *pos, long long ldb,
-                                float *xib, cudaStream_t s) {
+                                float *xib, unsigned long long *r2min_key, cudaStream_t s) {
     const int grid = (int)std::min<long long>(((long long)n + 255) / 256, 148LL * 16);
-    if (dim == 3) bond_vector_kernel<3><<<grid > 0 ? grid : 1, 256, 0, s>>>(n, off, nbr, pos, ldb, xib);
-    else bond_vector_kernel<2><<<grid > 0 ? grid : 1, 256, 0, s>>>(n, off, nbr, pos, ldb, xib);
+    if (dim == 3) bond_vector_kernel<3><<<grid > 0 ? grid : 1, 256, 0, s>>>(n, off, nbr, pos, ldb, xib, r2min_key);
+    else bond_vector_kernel<2><<<grid > 0 ? grid : 1, 256, 0, s>>>(n, off, nbr, pos, ldb, xib, r2min_key);
     return cudaGetLastError();
 }
 

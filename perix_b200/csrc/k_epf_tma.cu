@@ -213,6 +213,9 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     // CPA (bit 2, with PL2): each lane copies its next pass's coefficients from L2 into a private double buffer in
     // shared memory (cp.async) while it computes the current pass, instead of holding them in registers
     constexpr bool CPA = PL2 && (FLAGS & 4) != 0;
+    // EF (bit 3): the displacement-first clear-hold test |e|^2 < e2_hold, which needs no positions; only the bonds
+    // that fail it gather x_j for the reference test
+    constexpr bool EF = (FLAGS & 8) != 0 && !XI;
     constexpr bool XS = XI;
     using PosT = typename Vec<DIM>::T;
     using GT = typename std::conditional<MIXED, float, double>::type;
@@ -438,7 +441,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
             double uj[UNR][DIM];
 #pragma unroll
             for (int q = 0; q < UNR; ++q) {
-                if constexpr (!XS) xj[q] = ldg_vec(pos + j[q]);
+                if constexpr (!XS && !EF) xj[q] = ldg_vec(pos + j[q]);
                 if constexpr (DIM == 2) {
                     const double2 v = __ldg(reinterpret_cast<const double2 *>(a.u) + j[q]);
                     uj[q][0] = v.x;
@@ -461,7 +464,13 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
                 for (int d = 0; d < DIM; ++d) e[q][d] = __dsub_rn(uj[q][d], ui[d]);
                 bool fast = true;  // clearly holds
                 if (a.damage) {
-                    if constexpr (XS) {
+                    if constexpr (EF) {
+                        // |s| = ||xi + e| - |xi|| / |xi| <= |e| / r_min: below the bound the bond holds under either
+                        // criterion, whatever its direction (the bound keeps a 1e-6 relative margin for rounding)
+                        double e2 = e[q][0] * e[q][0] + e[q][1] * e[q][1];
+                        if constexpr (DIM == 3) e2 = fma(e[q][2], e[q][2], e2);
+                        fast = e2 < a.e2_hold;
+                    } else if constexpr (XS) {
                         // FP32 squared test on the staged FP32 bond vector.  Its error (ξ rounded to FP32, e
                         // rounded, FP32 sums: < 1e-6 r^2 wherever |y|^2 is near (1 +- s_c)^2 r^2) stays well inside
                         // the 4e-6 r^2 band; outside the clear-hold region the reference arithmetic decides on the
@@ -509,7 +518,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
                 for (int q = 0; q < UNR; ++q) {
                     if (!slow[q]) continue;
                     int brk;
-                    if constexpr (XS) brk = break_fp64<DIM>(ldg_vec(pos + j[q]), xi, e[q], a);
+                    if constexpr (XS || EF) brk = break_fp64<DIM>(ldg_vec(pos + j[q]), xi, e[q], a);
                     else brk = break_fp64<DIM>(xj[q], xi, e[q], a);
                     if (brk) {
                         a.health[t0a + t0 + q * LPN] = 0;
@@ -669,20 +678,21 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
 // Staged configurations: lanes per node, bonds per lane per pass, stages, minimum resident blocks (launch
 // bounds), warps per block, flags (1: staged FP32 bond vectors for the stretch pre-test, 8 (2D) / 12 (3D) more
 // staged bytes per bond; 2: coefficients prefetched into L2 and loaded per lane instead of staged; 4 (with 2): those
-// loads go through a per-lane double buffer in shared memory filled by cp.async one pass ahead).  A tile is
+// loads go through a per-lane double buffer in shared memory filled by cp.async one pass ahead; 8 (without 1): the
+// displacement-first clear-hold test, positions gathered only for the bonds it does not clear).  A tile is
 // WPB * 32/LPN nodes.
 struct TmaCfg {
     int lpn, unr, stages, minb, wpb, xi;
 };
 #define PXB_TMA2(X)                                                                                               \
-    X(0, 16, 2, 4, 1, 8, 0) X(1, 8, 1, 3, 1, 8, 0) X(2, 8, 4, 3, 1, 8, 0) X(3, 8, 2, 2, 3, 8, 0)                 \
+    X(0, 4, 2, 2, 6, 4, 8) X(1, 4, 4, 2, 4, 4, 8) X(2, 8, 4, 3, 1, 8, 0) X(3, 8, 2, 2, 3, 8, 0)                  \
     X(4, 8, 1, 2, 4, 8, 0) X(5, 8, 2, 2, 4, 8, 0) X(6, 4, 2, 2, 6, 4, 0) X(7, 4, 4, 2, 4, 4, 0)                  \
     X(8, 8, 2, 2, 8, 4, 0) X(9, 4, 2, 2, 3, 8, 0) X(10, 4, 2, 2, 6, 4, 1) X(11, 4, 4, 2, 4, 4, 1)                \
     X(12, 8, 2, 2, 6, 4, 1) X(13, 8, 2, 3, 3, 8, 2) X(14, 4, 2, 3, 3, 8, 2) X(15, 4, 4, 3, 2, 8, 3)
 #define PXB_TMA3(X)                                                                                               \
-    X(0, 32, 2, 2, 1, 8, 0) X(1, 16, 2, 3, 2, 8, 2) X(2, 32, 1, 3, 1, 8, 0) X(3, 16, 2, 2, 1, 8, 0)              \
-    X(4, 16, 1, 2, 2, 8, 0) X(5, 32, 2, 2, 2, 8, 0) X(6, 32, 2, 2, 2, 4, 1) X(7, 32, 1, 2, 4, 4, 1)              \
-    X(8, 16, 2, 2, 2, 4, 1) X(9, 16, 1, 3, 3, 8, 2) X(10, 32, 1, 3, 3, 8, 3) X(11, 32, 2, 3, 2, 4, 1)            \
+    X(0, 32, 2, 2, 1, 8, 0) X(1, 16, 2, 3, 2, 8, 2) X(2, 16, 2, 3, 2, 8, 10) X(3, 16, 2, 2, 1, 8, 0)             \
+    X(4, 16, 2, 3, 3, 8, 10) X(5, 32, 2, 2, 2, 8, 0) X(6, 32, 2, 2, 2, 4, 1) X(7, 32, 1, 2, 4, 4, 1)             \
+    X(8, 16, 2, 2, 2, 8, 10) X(9, 16, 1, 3, 3, 8, 2) X(10, 32, 1, 3, 3, 8, 3) X(11, 32, 2, 3, 2, 8, 10)          \
     X(12, 16, 2, 2, 2, 8, 2) X(13, 16, 2, 3, 3, 8, 6) X(14, 32, 1, 3, 3, 8, 2) X(15, 32, 1, 3, 6, 4, 2)
 #define PXB_CFG(i, l, u, st, mb, w, x) {l, u, st, mb, w, x},
 static constexpr TmaCfg kTma2[kEpfTmaConfigs] = {PXB_TMA2(PXB_CFG)};
@@ -712,13 +722,11 @@ static size_t tma_smem_dm(int which, int maxb) {
     const TmaCfg c = DIM == 3 ? kTma3[which] : kTma2[which];
     const int nt = c.wpb * (kWarp / c.lpn);
     size_t per = 0;
-    switch (c.xi) {
+    switch (c.xi & 3) {  // the stage layout follows the bond-vector (1) and L2-prefetch (2) bits alone
         case 0: per = tma_stage_bytes<DIM, MIXED, false, false>(nt, maxb); break;
         case 1: per = tma_stage_bytes<DIM, MIXED, true, false>(nt, maxb); break;
         case 2: per = tma_stage_bytes<DIM, MIXED, false, true>(nt, maxb); break;
-        case 3: per = tma_stage_bytes<DIM, MIXED, true, true>(nt, maxb); break;
-        case 6: per = tma_stage_bytes<DIM, MIXED, false, true>(nt, maxb); break;  // CPA
-        default: per = tma_stage_bytes<DIM, MIXED, true, true>(nt, maxb); break;   // 7: CPA with bond vectors
+        default: per = tma_stage_bytes<DIM, MIXED, true, true>(nt, maxb); break;
     }
     return (size_t)c.stages * per + cpa_bytes(DIM, MIXED, c.unr, c.wpb, c.xi);
 }

@@ -170,6 +170,10 @@ struct EpfArgs {
     // variable horizon: per-bond critical stretch [nb] (null: sc for every bond); the staged kernels do not read
     // it, launch_epf runs the lane-group kernel instead
     const double *sc_bond = nullptr;
+    // staged kernels with the displacement-first test: a bond whose relative displacement satisfies |e|^2 < e2_hold
+    // clearly holds (its stretch is at most |e| / |xi| < sc for every bond length |xi| >= r_min), so its positions
+    // are not gathered; e2_hold = (sc (1 - 1e-6) - 1e-12)^2 r_min^2 (0: every bond takes the position test)
+    double e2_hold = 0;
 };
 // schedule variants of the explicit kernel (lanes per node x bonds per lane per pass); see k_epf.cu
 constexpr int kEpfTmaConfigs = 16;                // staged (TMA) configurations per dimension
@@ -177,9 +181,11 @@ constexpr int kEpfVariants = 5 + kEpfTmaConfigs;  // 0-2 lane groups, 3-4 CSR ti
 cudaError_t launch_epf(const EpfArgs &a, int dim, bool mixed, int mode, int variant, cudaStream_t s);
 // P[c][t] from G[c][t] (t < ldb, SoA stride ldb): 2D p11 = C11 Gxx + C66 Gyy, p22 = C66 Gxx + C11 Gyy,
 // pxy = (C12 + C66) Gxy; 3D p11/p22/p33 and (C12 + C66) times Gxy, Gxz, Gyz
-// xib[d][t] = (float)(x_j - x_i)[d] for every bond t = (i -> j) (t < off[n]; the tail is left as it is)
+// xib[d][t] = (float)(x_j - x_i)[d] for every bond t = (i -> j) (t < off[n]; the tail is left as it is); and, when
+// r2min_key is given, the smallest positive squared bond length in the reference's rounding (x_j - x_i and the dot
+// product rounded op by op) as an atomicMin over the bit pattern (the caller initialises it to +inf)
 cudaError_t launch_bond_vectors(int n, int dim, const int *off, const int *nbr, const void *pos, long long ldb,
-                                float *xib, cudaStream_t s);
+                                float *xib, unsigned long long *r2min_key, cudaStream_t s);
 cudaError_t launch_navier_pack(const void *G, void *P, long long ldb, int dim, bool mixed, double C11, double C12,
                                double C66, cudaStream_t s);
 int epf_grid(int n, int dim, int variant);

@@ -115,6 +115,7 @@ struct EpfState {
     bool ready = false, started = false;
     int precision = PXB_FP64;
     double C11 = 0, C12 = 0, C66 = 0, rho = 1, b[3] = {0, 0, 0}, sc = 0;
+    double r2min = 0;  // smallest positive squared bond length (reference rounding)
     int tension_only = 1;
     DevBuf G;          // SoA Navier operators [c][ldb], double or float (c = 3 in 2D, 6 in 3D)
     DevBuf P;          // SoA packed Navier coefficients [c][ldb] (same type): the staged step kernels' stream
