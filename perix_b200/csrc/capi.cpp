@@ -130,7 +130,7 @@ size_t ctx_bytes(const pxb_ctx *c) {
     s += bufsz(e.G) + bufsz(e.P) + bufsz(e.xib) + bufsz(e.health) + bufsz(e.u[0]) + bufsz(e.u[1]) + bufsz(e.accel) + bufsz(e.counters) +
          bufsz(e.umax) + bufsz(e.tsched) + bufsz(e.sc_bond);
     s += bufsz(e.adj_ckpt) + bufsz(e.adj_seg) + bufsz(e.adj_p[0]) + bufsz(e.adj_p[1]) + bufsz(e.adj_A) + bufsz(e.adj_R) +
-         bufsz(e.adj_W) + bufsz(e.adj_t) + bufsz(e.adj_dC) + bufsz(e.adj_umax) + bufsz(e.adj_GR) + bufsz(e.adj_HR) + bufsz(e.adj_u0);
+         bufsz(e.adj_W) + bufsz(e.adj_t) + bufsz(e.adj_dC) + bufsz(e.adj_umax) + bufsz(e.adj_GR) + bufsz(e.adj_HR) + bufsz(e.adj_u0) + bufsz(e.adj_SG);
     s += bufsz(e.bc.own) + bufsz(e.bc.src_off) + bufsz(e.bc.tgt) + bufsz(e.bc.comp) + bufsz(e.bc.form) +
          bufsz(e.bc.vals);
     const BatchState &bt = c->batch;
@@ -1514,6 +1514,7 @@ int adj_kernel(pxb_ctx *c, const double *u, const double *w, double scale, doubl
     a.c_w = c_w;
     a.c_o = c_o;
     a.rout = rout;
+    if (e.adj_sg_on) a.SG = e.adj_SG.as<double>();
     launch_epf_adjoint(a, c->g.dim, e.precision == PXB_MIXED, epf_grid(c->g.n, c->g.dim, 0), c->stream);
     return check_launch(c, "epf adjoint step");
 }
@@ -1587,15 +1588,20 @@ extern "C" int pxb_epf_record_d(pxb_ctx *c, const double *u0_d, const double *v0
         c->launches++;
         PXB_TRY(d2d(P[0], u0_d, bytes));
     }
-    // the forward loop, keeping every state u^q (all) or the pair (u^{sK}, u^{sK-1}) at every segment start
+    // the forward loop, keeping every state u^q (all) or the pair (u^{sK}, u^{sK-1}) at every segment start; the
+    // last segment's states are kept as they pass (the reverse sweep starts there, so it is not recomputed)
     int cur = 0;
+    const int qlast = (nseg - 1) * K;
     for (int q = 0; q < nsteps; ++q) {
         if (all) {
             PXB_TRY(d2d(seg + (size_t)q * nd, P[cur], bytes));
-        } else if (q % K == 0) {
-            const size_t s = (size_t)(q / K);
-            PXB_TRY(d2d(ck + (2 * s) * nd, P[cur], bytes));
-            PXB_TRY(d2d(ck + (2 * s + 1) * nd, P[cur ^ 1], bytes));
+        } else {
+            if (q % K == 0) {
+                const size_t s = (size_t)(q / K);
+                PXB_TRY(d2d(ck + (2 * s) * nd, P[cur], bytes));
+                PXB_TRY(d2d(ck + (2 * s + 1) * nd, P[cur ^ 1], bytes));
+            }
+            if (q >= qlast) PXB_TRY(d2d(seg + (size_t)(q - qlast) * nd, P[cur], bytes));
         }
         PXB_TRY(adj_step(c, P[cur], P[cur ^ 1], tdev, q, dt));
         cur ^= 1;
@@ -1606,6 +1612,7 @@ extern "C" int pxb_epf_record_d(pxb_ctx *c, const double *u0_d, const double *v0
     e.rec_steps = nsteps;
     e.rec_K = K;
     e.rec_all = all;
+    e.rec_seg = all ? -1 : nseg - 1;
     return PXB_OK;
 }
 
@@ -1617,11 +1624,31 @@ extern "C" int pxb_epf_adjoint_recorded_d(pxb_ctx *c, const double *ubar_N_d, co
         return fail(PXB_ERR_STATE, "pxb_epf_adjoint_recorded_d: no recorded forward loop (pxb_epf_record_d)");
     if (!ubar_N_d || !u0bar_d) return fail(PXB_ERR_INVALID, "pxb_epf_adjoint_recorded_d: need dJ/du^N and dJ/du0");
     PXB_TRY(ensure_grev(c));
+    struct SgOff {  // the reverse-only kernel is used inside this sweep only
+        EpfState &e;
+        ~SgOff() { e.adj_sg_on = false; }
+    } sg_off{e};
+    e.adj_sg_on = false;
     if (e.adj_GR.p) {  // the frozen mask in reverse-bond order, for this sweep
         PXB_TRY(dev_alloc(c, e.adj_HR, (size_t)std::max(1LL, c->g.nb)));
         PXB_CUDA_TRY(launch_reverse_health(e.health.as<uint8_t>(), c->g.rev.as<int>(), e.adj_HR.as<uint8_t>(), c->g.nb,
                                            c->stream));
         PXB_TRY(check_launch(c, "reverse health"));
+        // the own bonds' operator sums under the frozen mask: with every bond's reverse present, the reverse-only
+        // kernel then reads one operator stream per step instead of two (the missing count uses counter slot 5)
+        const int nc = c->g.dim == 3 ? 6 : 3;
+        if (dev_alloc(c, e.adj_SG, sizeof(double) * nc * (size_t)std::max(1, c->g.n)) == PXB_OK) {
+            unsigned int *miss = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 5);
+            PXB_CUDA_TRY(cudaMemsetAsync(miss, 0, sizeof(unsigned int), c->stream));
+            PXB_CUDA_TRY(launch_own_sums(c->g.n, c->g.dim, e.precision == PXB_MIXED, c->g.off.as<int>(),
+                                         c->g.rev.as<int>(), e.health.as<uint8_t>(), e.G.p, (long long)c->g.ldb,
+                                         e.adj_SG.as<double>(), miss, c->stream));
+            PXB_TRY(check_launch(c, "own sums"));
+            unsigned int nmiss = 1;
+            PXB_TRY(d2h(c, &nmiss, miss, sizeof(nmiss)));
+            PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+            e.adj_sg_on = nmiss == 0;
+        }
     }
     const size_t nd = (size_t)c->g.n * c->g.dim, bytes = sizeof(double) * nd;
     const int nsteps = e.rec_steps, K = e.rec_K;
@@ -1647,7 +1674,10 @@ extern "C" int pxb_epf_adjoint_recorded_d(pxb_ctx *c, const double *ubar_N_d, co
     fill_bc(c, bc);
     for (int s = nseg - 1; s >= 0; --s) {
         const int q0 = s * K, q1 = std::min(nsteps, (s + 1) * K);
-        if (!e.rec_all) {  // recompute the segment's states u^{q0} .. u^{q1-1} from its checkpoint
+        // recompute the segment's states u^{q0} .. u^{q1-1} from its checkpoint, unless seg still holds them (the
+        // last segment, kept by the forward loop, on the first sweep over a recording)
+        if (!e.rec_all && e.rec_seg != s) {
+            e.rec_seg = -1;
             PXB_TRY(d2d(P[0], ck + (size_t)(2 * s) * nd, bytes));
             PXB_TRY(d2d(P[1], ck + (size_t)(2 * s + 1) * nd, bytes));
             int cur = 0;
@@ -1658,6 +1688,7 @@ extern "C" int pxb_epf_adjoint_recorded_d(pxb_ctx *c, const double *ubar_N_d, co
                     cur ^= 1;
                 }
             }
+            e.rec_seg = s;
         }
         for (int q = q1 - 1; q >= q0; --q) {
             const cudaError_t err = launch_bc_transpose(bc, c->g.n, c->g.dim, A, W, c->stream);

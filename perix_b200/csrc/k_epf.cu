@@ -486,8 +486,9 @@ __global__ void __launch_bounds__(kEpfThreads) epf_stream_kernel(EpfArgs a) {
 // Lbar = abar/rho and
 //   ubar_m = sum_{t in fam(m)} ( h_rev(t) P_rev(t) Lbar_{j_t} - h_t P_t Lbar_m )      (gather via rev)
 //   dJ/dC_k = sum_i sum_t h_t Lbar_i . (dP_t/dC_k) eta_t
-template <int DIM, bool MIXED>
-__global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) {
+// REV: the reverse-only mode (EpfAdjArgs::SG with GR and hrev), its own instantiation (fewer registers)
+template <int DIM, bool MIXED, bool REV>
+__global__ void __launch_bounds__(kEpfThreads, REV ? 4 : 1) epf_adjoint_kernel(EpfAdjArgs a) {
     constexpr int WPB = kEpfThreads / kWarp;
     constexpr int NC = (DIM == 3) ? 6 : 3;
     __shared__ double s_dC[WPB][3];
@@ -503,7 +504,46 @@ __global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) 
             um[d] = a.u[(size_t)m * DIM + d];
             U[d] = 0.0;
         }
-        for (int t = a.off[m] + lane; t < a.off[m + 1]; t += kWarp) {
+        // dJ/dC of one bond: L (the source node's scaled adjoint) . dP/dC (G) e, e = u_target - u_source
+        auto acc_dC = [&](const double *L, const double *g, const double *e) {
+            if constexpr (DIM == 3) {
+                const double Gxx = g[0], Gyy = g[1], Gzz = g[2], Gxy = g[3], Gxz = g[4], Gyz = g[5];
+                dC[0] += L[0] * Gxx * e[0] + L[1] * Gyy * e[1] + L[2] * Gzz * e[2];
+                dC[1] += L[0] * (Gxy * e[1] + Gxz * e[2]) + L[1] * (Gxy * e[0] + Gyz * e[2]) +
+                         L[2] * (Gxz * e[0] + Gyz * e[1]);
+                dC[2] += L[0] * ((Gyy + Gzz) * e[0] + Gxy * e[1] + Gxz * e[2]) +
+                         L[1] * (Gxy * e[0] + (Gxx + Gzz) * e[1] + Gyz * e[2]) +
+                         L[2] * (Gxz * e[0] + Gyz * e[1] + (Gxx + Gyy) * e[2]);
+            } else {
+                const double Gxx = g[0], Gyy = g[1], Gxy = g[2];
+                dC[0] += L[0] * Gxx * e[0] + L[1] * Gyy * e[1];
+                dC[1] += L[0] * Gxy * e[1] + L[1] * Gxy * e[0];
+                dC[2] += L[0] * (Gyy * e[0] + Gxy * e[1]) + L[1] * (Gxy * e[0] + Gxx * e[1]);
+            }
+        };
+        constexpr bool rev_only = REV;
+        if constexpr (REV) {
+            // the reverse bond (j -> m): its operators and health from the bond-ordered copies, the source's
+            // adjoint and displacement gathered; its term of (da/du)^T and of dJ/dC
+            for (int t = a.off[m] + lane; t < a.off[m + 1]; t += kWarp) {
+                const int j = __ldg(a.nbr + t);
+                double gr[NC], Lj[DIM], e[DIM], f[DIM];
+                load_G<DIM, MIXED>(a.GR, a.nb, t, gr);
+                const bool hr = a.hrev[t] != 0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    Lj[d] = a.abar[(size_t)j * DIM + d] * lscale;
+                    e[d] = um[d] - a.u[(size_t)j * DIM + d];
+                }
+                if (hr) {
+                    navier_apply<DIM>(gr, a.C11, a.C12, a.C66, Lj, f);
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) U[d] += f[d];
+                    acc_dC(Lj, gr, e);
+                }
+            }
+        }
+        for (int t = a.off[m] + lane; !REV && t < a.off[m + 1]; t += kWarp) {
             const int j = __ldg(a.nbr + t);
             const int r = a.hrev ? 0 : __ldg(a.rev + t);
             double g[NC], f[DIM];
@@ -535,24 +575,19 @@ __global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) 
                 double e[DIM];
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) e[d] = a.u[(size_t)j * DIM + d] - um[d];
-                if constexpr (DIM == 3) {
-                    const double Gxx = g[0], Gyy = g[1], Gzz = g[2], Gxy = g[3], Gxz = g[4], Gyz = g[5];
-                    dC[0] += Lm[0] * Gxx * e[0] + Lm[1] * Gyy * e[1] + Lm[2] * Gzz * e[2];
-                    dC[1] += Lm[0] * (Gxy * e[1] + Gxz * e[2]) + Lm[1] * (Gxy * e[0] + Gyz * e[2]) +
-                             Lm[2] * (Gxz * e[0] + Gyz * e[1]);
-                    dC[2] += Lm[0] * ((Gyy + Gzz) * e[0] + Gxy * e[1] + Gxz * e[2]) +
-                             Lm[1] * (Gxy * e[0] + (Gxx + Gzz) * e[1] + Gyz * e[2]) +
-                             Lm[2] * (Gxz * e[0] + Gyz * e[1] + (Gxx + Gyy) * e[2]);
-                } else {
-                    const double Gxx = g[0], Gyy = g[1], Gxy = g[2];
-                    dC[0] += Lm[0] * Gxx * e[0] + Lm[1] * Gyy * e[1];
-                    dC[1] += Lm[0] * Gxy * e[1] + Lm[1] * Gxy * e[0];
-                    dC[2] += Lm[0] * (Gyy * e[0] + Gxy * e[1]) + Lm[1] * (Gxy * e[0] + Gxx * e[1]);
-                }
+                acc_dC(Lm, g, e);
             }
         }
 #pragma unroll
         for (int d = 0; d < DIM; ++d) U[d] = group_sum<kWarp>(U[d]);
+        if constexpr (rev_only) {  // the own bonds' term, - (sum_t h_t P_t) Lm, from the node's operator sums
+            double sg[NC], f[DIM];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) sg[c] = a.SG[(size_t)m * NC + c];
+            navier_apply<DIM>(sg, a.C11, a.C12, a.C66, Lm, f);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) U[d] -= f[d];
+        }
         if (lane < DIM) {
             const size_t k = (size_t)m * DIM + lane;
             if (a.step) {
@@ -574,6 +609,51 @@ __global__ void __launch_bounds__(kEpfThreads) epf_adjoint_kernel(EpfAdjArgs a) 
         for (int w = 0; w < WPB; ++w) v += s_dC[w][threadIdx.x];
         atomicAdd(a.dC + threadIdx.x, v);
     }
+}
+
+// ---- per-node sums of the healthy own bonds' operators (the adjoint's own-bond term under a frozen mask) --------
+template <int NC, bool MIXED>
+__global__ void own_sum_kernel(int n, const int *off, const int *rev, const uint8_t *health, const void *G,
+                               long long ldb, double *SG, unsigned int *missing) {
+    const int lane = threadIdx.x & 31;
+    unsigned miss = 0;
+    for (int m = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5); m < n;
+         m += (int)((gridDim.x * (long long)blockDim.x) >> 5)) {
+        double s[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) s[c] = 0.0;
+        for (int t = off[m] + lane; t < off[m + 1]; t += kWarp) {
+            if (rev[t] < 0) ++miss;
+            if (!health[t]) continue;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if constexpr (MIXED) s[c] += (double)static_cast<const float *>(G)[(size_t)c * ldb + t];
+                else s[c] += static_cast<const double *>(G)[(size_t)c * ldb + t];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const double v = group_sum<kWarp>(s[c]);
+            if (lane == c) SG[(size_t)m * NC + c] = v;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) miss += __shfl_xor_sync(kFull, miss, o);
+    if (lane == 0 && miss) atomicAdd(missing, miss);
+}
+
+cudaError_t launch_own_sums(int n, int dim, bool mixed, const int *off, const int *rev, const uint8_t *health,
+                            const void *G, long long ldb, double *SG, unsigned int *missing, cudaStream_t s) {
+    const int grid = (int)std::min<long long>(((long long)n * kWarp + 255) / 256, 148LL * 16);
+    const int g = grid > 0 ? grid : 1;
+    if (dim == 3) {
+        if (mixed) own_sum_kernel<6, true><<<g, 256, 0, s>>>(n, off, rev, health, G, ldb, SG, missing);
+        else own_sum_kernel<6, false><<<g, 256, 0, s>>>(n, off, rev, health, G, ldb, SG, missing);
+    } else {
+        if (mixed) own_sum_kernel<3, true><<<g, 256, 0, s>>>(n, off, rev, health, G, ldb, SG, missing);
+        else own_sum_kernel<3, false><<<g, 256, 0, s>>>(n, off, rev, health, G, ldb, SG, missing);
+    }
+    return cudaGetLastError();
 }
 
 // ---- the Navier operators in reverse-bond order: GR[c][t] = G[c][rev t] (0 without a reverse bond) -------------
@@ -739,10 +819,17 @@ static int resident_grid(K kernel, int n, int nodes_per_block, int &cap) {
 // the adjoint kernel's own resident grid (one warp per node, grid-stride), capped by the node count
 template <int DIM, bool MIXED>
 static cudaError_t launch_adj(const EpfAdjArgs &a, cudaStream_t s) {
-    auto k = epf_adjoint_kernel<DIM, MIXED>;
-    static int cap = 0;
-    const int grid = resident_grid(k, a.n, kEpfThreads / kWarp, cap);
-    k<<<grid, kEpfThreads, 0, s>>>(a);
+    if (a.SG && a.GR && a.hrev) {
+        auto k = epf_adjoint_kernel<DIM, MIXED, true>;
+        static int cap = 0;
+        const int grid = resident_grid(k, a.n, kEpfThreads / kWarp, cap);
+        k<<<grid, kEpfThreads, 0, s>>>(a);
+    } else {
+        auto k = epf_adjoint_kernel<DIM, MIXED, false>;
+        static int cap = 0;
+        const int grid = resident_grid(k, a.n, kEpfThreads / kWarp, cap);
+        k<<<grid, kEpfThreads, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 

@@ -230,8 +230,16 @@ struct EpfAdjArgs {
     double scale = 1.0, c_r = 0.0, c_w = 0.0, c_o = 0.0;
     const double *rin = nullptr;
     double *rout = nullptr;
+    // reverse-only mode (with GR and hrev, the damage mask frozen for the sweep): SG[m][c] = sum over the node's
+    // healthy bonds of G[c][t] (launch_own_sums), so the own-bond term is one 3x3 product per node and dJ/dC is
+    // summed over the reverse bonds; the forward operator stream is not read
+    const double *SG = nullptr;
 };
 cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int grid, cudaStream_t s);
+// SG[m][c] = sum_{t in fam(m), health[t]} G[c][t] (nc = 3 in 2D, 6 in 3D, FP64 sums); missing[0] += the bonds
+// without a reverse bond (rev t < 0)
+cudaError_t launch_own_sums(int n, int dim, bool mixed, const int *off, const int *rev, const uint8_t *health,
+                            const void *G, long long ldb, double *SG, unsigned int *missing, cudaStream_t s);
 // hr[t] = health[rev t] for t < nb (0 where rev t < 0)
 cudaError_t launch_reverse_health(const uint8_t *health, const int *rev, uint8_t *hr, long long nb, cudaStream_t s);
 // GR[c][t] = G[c][rev t] for t < nb (0 where rev t < 0), SoA stride ldb

@@ -128,15 +128,18 @@ struct EpfState {
     DevBuf adj_GR;       // the Navier operators in reverse-bond order (the adjoint kernel's second stream)
     DevBuf adj_HR;       // the health mask in reverse-bond order (rebuilt by every reverse sweep)
     bool adj_GR_none = false;  // no room for adj_GR: the adjoint kernel gathers the reverse bonds' operators
+    DevBuf adj_SG;             // per-node sums of the healthy own bonds' operators (rebuilt by every reverse sweep)
+    bool adj_sg_on = false;    // inside a reverse sweep whose families all have reverse bonds: reverse-only kernel
     // the recorded forward loop (pxb_epf_record_d): rec_steps < 0 when there is none; rec_all: every state kept
     double rec_dt = 0.0;
     int rec_steps = -1, rec_K = 1;
     bool rec_all = false;
+    int rec_seg = -1;  // checkpointed recording: the segment whose states adj_seg holds (-1: none)
     DevBuf health;     // uint8 [ldb] (zero tail)
     DevBuf u[2];       // double [n*dim + 8] ping-pong: u[cur] = u^n, u[cur^1] = u^{n-1}
     DevBuf accel;      // double [n*dim]
     DevBuf counters;   // unsigned long long [6]: [0] broken bonds, [2] staged-kernel wait failures (u32),
-                       // [4] broken bonds before the last rate call
+                       // [4] broken bonds before the last rate call, [5] scratch of the set-up and sweep reductions
     PinnedBuf rate_h;  // host copy of counters[0..4] for the per-step rate call
     cudaEvent_t rate_done = nullptr;  // end of a rate call's work (polled by the host)
     // the per-step rate call captured as one graph for one pair of pinned host buffers (u in, acceleration out),
