@@ -502,16 +502,20 @@ def barrier(ws):
 PROFILE_FILES = {"plate": "epf_step_plate.md", "slab": "epf_step_slab.md"}
 
 
-def read_traffic(kind, prec):
-    """DRAM bytes per step-kernel launch from the committed ncu summary of this workload (None until captured)."""
+def read_traffic(kind, prec, variant=None):
+    """DRAM bytes per step-kernel launch from the committed ncu summary of this workload: the line of this precision
+    whose "(variant N)" names the schedule the autotuner picked (None until that one is captured)."""
     path = os.path.join(ROOT, "profiles", PROFILE_FILES[kind])
     if not os.path.exists(path):
         return None
     key = "traffic_bytes_per_launch_%s:" % prec
     for line in open(path):
         if line.strip().startswith(key):
+            rest = line.split(":", 1)[1].strip()
+            if variant is not None and "(variant %d)" % variant not in rest:
+                continue
             try:
-                return float(line.split(":", 1)[1].strip().split()[0])
+                return float(rest.split()[0])
             except ValueError:
                 return None
     return None
@@ -1022,7 +1026,7 @@ def explicit_workload(px, w, steps, warmup, ws, local, e2e_calls):
                        "drop_in_call_us: perix_cuda::assembleExplicitPDDOFracAccel via pxb_cuda_explicit_accel with "
                        "pageable arrays and double health in/out (FP64, the shim's default)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": read_traffic(w["kind"], head), "peak_kind": peak_kind,
+                     "traffic": read_traffic(w["kind"], head, r["tuned"]["variant"]), "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": B, "kernel": kernel_name(w["dim"], head, r["tuned"]),
                      "launch_floor_ms": (r["tuned"]["launch_floor"] or {}).get("ms"),
                      "note": "achieved = algorithmic bytes / CUDA-event step time; launch_floor_ms is an empty "
