@@ -270,6 +270,12 @@ int pxb_epf_adjoint_d(pxb_ctx *ctx, const double *u0_d, const double *v0_d, doub
  * pxb_epf_adjoint_recorded_d as its backward pass, so the loop is not run a second time. */
 int pxb_epf_record_d(pxb_ctx *ctx, const double *u0_d, const double *v0_d, double dt, int nsteps, int checkpoint_every,
                      double *uN_d, double *uNm1_d);
+/* The reverse sweep's bond-force adjoint kernel: 0 a kernel that streams both the forward and the reverse bonds'
+ * operators; 1 (and -1, the default) the reverse-only kernel: the frozen mask's own-bond operator sums are formed
+ * once per sweep, dJ/dC is summed over the reverse bonds, and one operator stream is read per step.  The reverse-only
+ * kernel applies when every bond has its reverse (symmetric families); other meshes fall back to 0.  Results agree
+ * to rounding.  No counterpart in the reference. */
+int pxb_epf_set_adjoint_schedule(pxb_ctx *ctx, int schedule);
 /* The reverse sweep of the last pxb_epf_record_d (PXB_ERR_STATE when there is none); arguments as pxb_epf_adjoint_d. */
 int pxb_epf_adjoint_recorded_d(pxb_ctx *ctx, const double *ubar_N_d, const double *ubar_Nm1_d, double *u0bar_d,
                                double *v0bar_d, double *dC_d);

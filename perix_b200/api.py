@@ -400,8 +400,14 @@ class Context:
         return off, ids[:self.nb]
 
     def gbuild_set_schedule(self, schedule):
-        """-1 default, 0 lane groups, 1 one warp per node (pxb_gbuild_set_schedule)."""
+        """-1 default, 0 lane groups, 1 one warp per node, 2 one warp per node with the FP64 tensor-core tiles
+        (pxb_gbuild_set_schedule)."""
         _check(self.L.pxb_gbuild_set_schedule(self.h, int(schedule)))
+
+    def epf_set_adjoint_schedule(self, schedule):
+        """The recorded reverse sweep's kernel: -1 default (1), 0 both operator streams, 1 reverse-only
+        (pxb_epf_set_adjoint_schedule)."""
+        _check(self.L.pxb_epf_set_adjoint_schedule(self.h, int(schedule)))
 
     def gbuild(self, order=2, precision=FP64, allow_degenerate=False):
         nd = C.c_int(0)

@@ -544,6 +544,13 @@ extern "C" int pxb_gbuild_set_schedule(pxb_ctx *c, int schedule) {
     return PXB_OK;
 }
 
+extern "C" int pxb_epf_set_adjoint_schedule(pxb_ctx *c, int schedule) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_epf_set_adjoint_schedule: NULL context");
+    if (schedule < -1 || schedule > 1) return fail(PXB_ERR_INVALID, "pxb_epf_set_adjoint_schedule: -1, 0 or 1");
+    c->adj_schedule = schedule;
+    return PXB_OK;
+}
+
 extern "C" int pxb_gbuild_info(pxb_ctx *c, int *nop, int *pqr) {
     if (!c) return fail(PXB_ERR_INVALID, "pxb_gbuild_info: NULL context");
     if (!c->ops.ready) return fail(PXB_ERR_STATE, "pxb_gbuild_info: no operator cache (call pxb_gbuild)");
@@ -1637,7 +1644,8 @@ extern "C" int pxb_epf_adjoint_recorded_d(pxb_ctx *c, const double *ubar_N_d, co
         // the own bonds' operator sums under the frozen mask: with every bond's reverse present, the reverse-only
         // kernel then reads one operator stream per step instead of two (the missing count uses counter slot 5)
         const int nc = c->g.dim == 3 ? 6 : 3;
-        if (dev_alloc(c, e.adj_SG, sizeof(double) * nc * (size_t)std::max(1, c->g.n)) == PXB_OK) {
+        if (c->adj_schedule != 0 &&
+            dev_alloc(c, e.adj_SG, sizeof(double) * nc * (size_t)std::max(1, c->g.n)) == PXB_OK) {
             unsigned int *miss = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 5);
             PXB_CUDA_TRY(cudaMemsetAsync(miss, 0, sizeof(unsigned int), c->stream));
             PXB_CUDA_TRY(launch_own_sums(c->g.n, c->g.dim, e.precision == PXB_MIXED, c->g.off.as<int>(),

@@ -583,7 +583,7 @@ __global__ void __launch_bounds__(kEpfThreads, REV ? 4 : 1) epf_adjoint_kernel(E
         if constexpr (rev_only) {  // the own bonds' term, - (sum_t h_t P_t) Lm, from the node's operator sums
             double sg[NC], f[DIM];
 #pragma unroll
-            for (int c = 0; c < NC; ++c) sg[c] = a.SG[(size_t)m * NC + c];
+            for (int c = 0; c < NC; ++c) sg[c] = __ldg(a.SG + (size_t)m * NC + c);
             navier_apply<DIM>(sg, a.C11, a.C12, a.C66, Lm, f);
 #pragma unroll
             for (int d = 0; d < DIM; ++d) U[d] -= f[d];

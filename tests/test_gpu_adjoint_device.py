@@ -27,10 +27,11 @@ def _bcs(w, kind):
     return bcs
 
 
-def _grads(ctx, w, bcs, u0, v0, u_obs, device_run, checkpoint_every):
+def _grads(ctx, w, bcs, u0, v0, u_obs, device_run, checkpoint_every, schedule=-1):
     torch, dev = _torch()
     from perix_b200.autograd import BcPlan, elastic_constants_t, explicit_loop, explicit_run, set_constants
     _ctx(ctx, w, E0)
+    ctx.epf_set_adjoint_schedule(schedule)
     ctx.epf_set_bcs(bcs)
     E = torch.tensor(E0, dtype=torch.float64, device=dev, requires_grad=True)
     u0t = torch.tensor(u0, device=dev, requires_grad=True)
@@ -48,9 +49,10 @@ def _grads(ctx, w, bcs, u0, v0, u_obs, device_run, checkpoint_every):
     return float(J), float(E.grad), u0t.grad.cpu().numpy(), v0t.grad.cpu().numpy(), uN.detach().cpu().numpy()
 
 
+@pytest.mark.parametrize("schedule", [0, 1])
 @pytest.mark.parametrize("checkpoint_every", [0, 7])
 @pytest.mark.parametrize("kind", ["pins", "reflect"])
-def test_device_adjoint_matches_taped_loop(ctx, plate, kind, checkpoint_every):  # noqa: F811
+def test_device_adjoint_matches_taped_loop(ctx, plate, kind, checkpoint_every, schedule):  # noqa: F811
     w = plate
     n = w["L"].n
     rng = np.random.default_rng(8)
@@ -58,7 +60,7 @@ def test_device_adjoint_matches_taped_loop(ctx, plate, kind, checkpoint_every): 
     v0 = rng.standard_normal(2 * n) * 1e-2
     bcs = _bcs(w, kind)
     u_obs = rng.standard_normal(2 * n) * 1e-7
-    J1, dE1, du1, dv1, uN1 = _grads(ctx, w, bcs, u0, v0, u_obs, True, checkpoint_every)
+    J1, dE1, du1, dv1, uN1 = _grads(ctx, w, bcs, u0, v0, u_obs, True, checkpoint_every, schedule)
     J2, dE2, du2, dv2, uN2 = _grads(ctx, w, bcs, u0, v0, u_obs, False, 0)
     assert np.abs(uN1 - uN2).max() <= 1e-10 * np.abs(uN2).max()
     assert abs(J1 - J2) <= 1e-10 * abs(J2)
