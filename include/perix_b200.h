@@ -270,6 +270,11 @@ int pxb_epf_adjoint_d(pxb_ctx *ctx, const double *u0_d, const double *v0_d, doub
  * pxb_epf_adjoint_recorded_d as its backward pass, so the loop is not run a second time. */
 int pxb_epf_record_d(pxb_ctx *ctx, const double *u0_d, const double *v0_d, double dt, int nsteps, int checkpoint_every,
                      double *uN_d, double *uNm1_d);
+/* The per-step rate call (pxb_epf_rate) with pinned host buffers and a staged schedule variant runs pipelined: u
+ * goes up in node chunks, each chunk's kernel starts once the chunk's neighbours have arrived, and its acceleration
+ * goes down while the next chunk computes.  chunks: -1 (default) one chunk per 96 Ki nodes, at most 4 (meshes under
+ * 192 Ki nodes: one); 1 no pipelining; 2..8 that many chunks.  No counterpart in the reference. */
+int pxb_epf_set_rate_chunks(pxb_ctx *ctx, int chunks);
 /* The reverse sweep's bond-force adjoint kernel: 0 a kernel that streams both the forward and the reverse bonds'
  * operators; 1 (and -1, the default) the reverse-only kernel: the frozen mask's own-bond operator sums are formed
  * once per sweep, dJ/dC is summed over the reverse bonds, and one operator stream is read per step.  The reverse-only

@@ -404,6 +404,11 @@ class Context:
         (pxb_gbuild_set_schedule)."""
         _check(self.L.pxb_gbuild_set_schedule(self.h, int(schedule)))
 
+    def epf_set_rate_chunks(self, chunks):
+        """Node chunks of the pipelined per-step rate call (pinned buffers): -1 by mesh size, 1 off, 2..8
+        (pxb_epf_set_rate_chunks)."""
+        _check(self.L.pxb_epf_set_rate_chunks(self.h, int(chunks)))
+
     def epf_set_adjoint_schedule(self, schedule):
         """The recorded reverse sweep's kernel: -1 default (1), 0 both operator streams, 1 reverse-only
         (pxb_epf_set_adjoint_schedule)."""

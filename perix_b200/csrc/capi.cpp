@@ -171,6 +171,11 @@ static void destroy_graphs(EpfState &e) {
     e.rate_last_variant = -1;
     if (e.rate_done) cudaEventDestroy(e.rate_done);
     e.rate_done = nullptr;
+    for (cudaEvent_t ev : e.rate_ev) cudaEventDestroy(ev);
+    e.rate_ev.clear();
+    if (e.rate_up) cudaStreamDestroy(e.rate_up);
+    if (e.rate_down) cudaStreamDestroy(e.rate_down);
+    e.rate_up = e.rate_down = nullptr;
 }
 
 // Waits for the work queued so far by polling an event from the calling thread: the per-step call's wait is short
@@ -544,6 +549,15 @@ extern "C" int pxb_gbuild_set_schedule(pxb_ctx *c, int schedule) {
     return PXB_OK;
 }
 
+extern "C" int pxb_epf_set_rate_chunks(pxb_ctx *c, int chunks) {
+    if (!c) return fail(PXB_ERR_INVALID, "pxb_epf_set_rate_chunks: NULL context");
+    if (chunks < -1 || chunks == 0 || chunks > 8) return fail(PXB_ERR_INVALID, "pxb_epf_set_rate_chunks: -1 or 1..8");
+    c->rate_chunks = chunks;
+    c->epf.rate_plan_done = false;
+    destroy_graphs(c->epf);
+    return PXB_OK;
+}
+
 extern "C" int pxb_epf_set_adjoint_schedule(pxb_ctx *c, int schedule) {
     if (!c) return fail(PXB_ERR_INVALID, "pxb_epf_set_adjoint_schedule: NULL context");
     if (schedule < -1 || schedule > 1) return fail(PXB_ERR_INVALID, "pxb_epf_set_adjoint_schedule: -1, 0 or 1");
@@ -785,10 +799,95 @@ extern "C" int pxb_epf_setup(pxb_ctx *c, int precision, double C11, double C12, 
 
 // The work of one per-step rate call, queued on stream s: upload u into the state slot u[cur], snapshot the
 // broken-bond count on the device, the kernel's RATE epilogue, download the acceleration and the counters.
-static cudaError_t rate_ops(pxb_ctx *c, const double *u, double *accel, cudaStream_t s) {
+// The pipelined rate call's chunk plan, made once per set-up: chunks of about 96 Ki nodes (at most 4; starts on
+// 64-node boundaries, as the staged kernels' node ranges need), each with the chunk whose upload holds its highest
+// neighbour (the upload its kernel waits for).
+static int rate_plan(pxb_ctx *c) {
+    EpfState &e = c->epf;
+    if (e.rate_plan_done) return PXB_OK;
+    e.rate_plan_done = true;
+    e.rate_K = 1;
+    const int n = c->g.n;
+    int K = c->rate_chunks > 0 ? c->rate_chunks : std::min(4, n / 98304);
+    K = std::min(K, n / 64);  // chunks of at least 64 nodes
+    if (K < 2) return PXB_OK;
+    std::vector<int> b((size_t)K + 1);
+    for (int k = 0; k <= K; ++k) b[(size_t)k] = k == K ? n : (int)(((long long)n * k / K) & ~63LL);
+    void *tmp = nullptr;
+    PXB_TRY(scratch(c, sizeof(int) * (2 * (size_t)K + 1), &tmp));
+    int *bd = static_cast<int *>(tmp), *reach = bd + K + 1;
+    PXB_TRY(h2d(c, bd, b.data(), sizeof(int) * b.size()));
+    PXB_CUDA_TRY(cudaMemsetAsync(reach, 0, sizeof(int) * K, c->stream));
+    PXB_CUDA_TRY(launch_chunk_reach(c->g.off.as<int>(), c->g.nbr.as<int>(), bd, K, reach, c->stream));
+    PXB_TRY(check_launch(c, "chunk reach"));
+    std::vector<int> r((size_t)K);
+    PXB_TRY(d2h(c, r.data(), reach, sizeof(int) * K));
+    PXB_TRY(sync(c));
+    e.rate_need.assign((size_t)K, K - 1);
+    for (int k = 0; k < K; ++k) {
+        int p = k;  // the chunk holding the chunk's highest neighbour (never below the chunk itself)
+        while (p + 1 < K && b[(size_t)p + 1] <= r[(size_t)k]) ++p;
+        e.rate_need[(size_t)k] = p;
+    }
+    e.rate_bounds = b;
+    e.rate_K = K;
+    return PXB_OK;
+}
+
+// pinned: both host buffers page-locked (copies from pageable memory are staged synchronously, so chunking them
+// only adds per-chunk overhead)
+static cudaError_t rate_ops(pxb_ctx *c, const double *u, double *accel, cudaStream_t s, bool pinned) {
     EpfState &e = c->epf;
     const size_t nd = (size_t)c->g.n * c->g.dim;
     unsigned long long *cnt = e.counters.as<unsigned long long>();
+    if (pinned && e.rate_K > 1 && epf_is_tma(e.variant)) {
+        // pieces of u go up on one stream, each chunk's kernel starts once its neighbours' piece is there, and each
+        // chunk's acceleration goes down on another stream while the next chunk computes
+        const int K = e.rate_K, dim = c->g.dim;
+        cudaError_t err = cudaSuccess;
+        if (!e.rate_up) err = cudaStreamCreateWithFlags(&e.rate_up, cudaStreamNonBlocking);
+        if (err == cudaSuccess && !e.rate_down) err = cudaStreamCreateWithFlags(&e.rate_down, cudaStreamNonBlocking);
+        while (err == cudaSuccess && e.rate_ev.size() < 2 + 2 * (size_t)K) {
+            cudaEvent_t ev = nullptr;
+            err = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (err == cudaSuccess) e.rate_ev.push_back(ev);
+        }
+        if (err != cudaSuccess) return err;
+        cudaEvent_t *ev = e.rate_ev.data();
+        const int *b = e.rate_bounds.data();
+        double *ud = e.u[e.cur].as<double>();
+        auto span = [&](int k) { return (size_t)(b[k + 1] - b[k]) * dim * sizeof(double); };
+        err = cudaEventRecord(ev[0], s);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(e.rate_up, ev[0], 0);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(e.rate_down, ev[0], 0);
+        for (int p = 0; p < K && err == cudaSuccess; ++p) {
+            err = cudaMemcpyAsync(ud + (size_t)b[p] * dim, u + (size_t)b[p] * dim, span(p), cudaMemcpyHostToDevice,
+                                  e.rate_up);
+            if (err == cudaSuccess) err = cudaEventRecord(ev[2 + p], e.rate_up);
+        }
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(cnt + 4, cnt, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s);
+        EpfArgs a = epf_args(c);
+        a.u = ud;
+        a.accel = e.accel.as<double>();
+        for (int k = 0; k < K && err == cudaSuccess; ++k) {
+            err = cudaStreamWaitEvent(s, ev[2 + e.rate_need[(size_t)k]], 0);
+            a.node0 = b[k];
+            a.n = b[k + 1];
+            if (err == cudaSuccess) err = launch_epf(a, dim, e.precision == PXB_MIXED, EPF_RATE, e.variant, s);
+            if (err == cudaSuccess) err = cudaEventRecord(ev[2 + K + k], s);
+            if (err == cudaSuccess) err = cudaStreamWaitEvent(e.rate_down, ev[2 + K + k], 0);
+            if (err == cudaSuccess)
+                err = cudaMemcpyAsync(accel + (size_t)b[k] * dim, e.accel.as<double>() + (size_t)b[k] * dim, span(k),
+                                      cudaMemcpyDeviceToHost, e.rate_down);
+        }
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(e.rate_h.p, cnt, sizeof(unsigned long long) * 5, cudaMemcpyDeviceToHost,
+                                  e.rate_down);
+        if (err == cudaSuccess) err = cudaEventRecord(ev[1], e.rate_down);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(s, ev[1], 0);
+        return err;
+    }
     cudaError_t err = cudaMemcpyAsync(e.u[e.cur].p, u, sizeof(double) * nd, cudaMemcpyHostToDevice, s);
     // the broken-bond count before the kernel, snapshot on the device: one host synchronisation per call
     if (err == cudaSuccess)
@@ -822,7 +921,7 @@ static int capture_rate(pxb_ctx *c, const double *u, double *accel) {
     e.rate_graph = nullptr;
     cudaGraph_t graph = nullptr;
     PXB_CUDA_TRY(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
-    const cudaError_t oe = rate_ops(c, u, accel, c->own);
+    const cudaError_t oe = rate_ops(c, u, accel, c->own, true);
     const cudaError_t ce = cudaStreamEndCapture(c->own, &graph);
     if (oe != cudaSuccess || ce != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -846,6 +945,7 @@ extern "C" int pxb_epf_rate(pxb_ctx *c, const double *u, double *accel, long lon
     if (!u || !accel) return fail(PXB_ERR_INVALID, "pxb_epf_rate: NULL buffer");
     EpfState &e = c->epf;
     PXB_TRY(ensure_pinned(e.rate_h, sizeof(unsigned long long) * 5));
+    PXB_TRY(rate_plan(c));
     // pinned buffers that the previous call used too, with the same schedule: replay (or capture) the call as one
     // graph; otherwise (first call with these buffers or this schedule, or pageable memory) queue the operations
     // one by one, which also gives a kernel its first, uncaptured launch
@@ -859,7 +959,7 @@ extern "C" int pxb_epf_rate(pxb_ctx *c, const double *u, double *accel, long lon
         PXB_CUDA_TRY(cudaGraphLaunch(e.rate_graph, c->stream));
         c->launches++;
     } else {
-        const cudaError_t err = rate_ops(c, u, accel, c->stream);
+        const cudaError_t err = rate_ops(c, u, accel, c->stream, pinned_host(u) && pinned_host(accel));
         if (err != cudaSuccess) return cuda_fail(err, "epf rate");
         PXB_TRY(check_launch(c, "epf rate"));
     }

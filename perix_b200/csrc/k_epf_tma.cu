@@ -249,14 +249,14 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     // y2 > ((1-sc)^2 + 1e-6) r2 (the rounding of these two constants is far inside the band)
     const double hi_band = a.sc_hi2 - 1.0e-6, lo_band = a.sc_lo2 + 1.0e-6;
 
-    const int ntiles = (a.n + NT - 1) / NT;
+    const int ntiles = (a.n - a.node0 + NT - 1) / NT;
     const int mycount = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
     // one thread: fetch the block's k-th tile into stage k % S
     auto issue = [&](int k) {
         const int st = k % S;
         const int tile = (int)blockIdx.x + k * (int)gridDim.x;
-        const int n0 = tile * NT;
+        const int n0 = a.node0 + tile * NT;
         const int cnt = min(NT, a.n - n0);
         const int t0 = k < kTileDesc ? s_d0[k] : __ldg(a.off + n0);
         const int t1 = k < kTileDesc ? s_d1[k] : __ldg(a.off + n0 + cnt);
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     // the bond ranges of the block's first tiles, all loaded at once: a refill then issues its copies without
     // first waiting on a global load (family offsets never change during a run)
     for (int k = tid; k < mycount && k < kTileDesc; k += WPB * kWarp) {
-        const int n0 = ((int)blockIdx.x + k * (int)gridDim.x) * NT;
+        const int n0 = a.node0 + ((int)blockIdx.x + k * (int)gridDim.x) * NT;
         s_d0[k] = __ldg(a.off + n0);
         s_d1[k] = __ldg(a.off + min(n0 + NT, a.n));
     }
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
         const double *sUp = reinterpret_cast<const double *>(base + SL::up_off(maxb));
         const float *sXi = reinterpret_cast<const float *>(base + SL::xi_off(maxb));
         const int t0a = s_t0a[st];
-        const int n0 = ((int)blockIdx.x + k * (int)gridDim.x) * NT;
+        const int n0 = a.node0 + ((int)blockIdx.x + k * (int)gridDim.x) * NT;
         const int cnt = min(NT, a.n - n0);
         const int li = wib * GPW + grp;  // tile-local node of this group
         const bool act = li < cnt;
@@ -652,7 +652,7 @@ static cudaError_t launch_tma(const EpfArgs &a, cudaStream_t s) {
         cap_blocks = (long long)sms * (per_sm > 0 ? per_sm : 1);
         cap_smem = smem;
     }
-    const long long ntiles = ((long long)a.n + NT - 1) / NT;
+    const long long ntiles = ((long long)a.n - a.node0 + NT - 1) / NT;
     const long long cap = cap_blocks;
     const int grid = (int)(ntiles < cap ? ntiles : cap);
     g_last_shape = LaunchShape{grid > 0 ? grid : 1, WPB * kWarp, smem};

@@ -159,6 +159,7 @@ struct EpfArgs {
     int maxb = 0;                           // TMA variants: staged bonds per tile (multiple of 32)
     unsigned int *err = nullptr;            // TMA variants: pipeline waits that ran out
     int rate = 0;                           // TMA variants: RATE mode (accel out; u_other and BCs unused)
+    int node0 = 0;  // TMA variants: the launch computes nodes [node0, n) (node0 a multiple of 64; RATE mode only)
     // TMA variants, STEP mode: launch with programmatic stream serialisation, so that inside a captured loop of
     // steps the next step's blocks start their set-up while this step's last blocks finish (host-side only)
     int pdl = 0;
@@ -240,6 +241,9 @@ cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int gri
 // without a reverse bond (rev t < 0)
 cudaError_t launch_own_sums(int n, int dim, bool mixed, const int *off, const int *rev, const uint8_t *health,
                             const void *G, long long ldb, double *SG, unsigned int *missing, cudaStream_t s);
+// reach[k] = max(k's bonds' neighbour ids) for the node chunks [bounds[k], bounds[k+1]) (reach zeroed by the caller)
+cudaError_t launch_chunk_reach(const int *off, const int *nbr, const int *bounds, int nchunks, int *reach,
+                               cudaStream_t s);
 // hr[t] = health[rev t] for t < nb (0 where rev t < 0)
 cudaError_t launch_reverse_health(const uint8_t *health, const int *rev, uint8_t *hr, long long nb, cudaStream_t s);
 // GR[c][t] = G[c][rev t] for t < nb (0 where rev t < 0), SoA stride ldb

@@ -145,6 +145,15 @@ struct EpfState {
     // the per-step rate call captured as one graph for one pair of pinned host buffers (u in, acceleration out),
     // the state slot u[cur] and the schedule variant; rate_last_* are the buffers of the previous call
     cudaGraphExec_t rate_graph = nullptr;
+    // pipelined rate call (staged variants, large meshes, pinned buffers): node chunks [rate_bounds[k],
+    // rate_bounds[k+1]), uploaded and computed in order; chunk k's kernel waits for the upload of chunk
+    // rate_need[k] (where its highest neighbour lies), and its acceleration goes down while the next chunk
+    // computes; rate_K <= 1: one upload, one kernel, one download
+    bool rate_plan_done = false;
+    int rate_K = 1;
+    std::vector<int> rate_bounds, rate_need;
+    cudaStream_t rate_up = nullptr, rate_down = nullptr;
+    std::vector<cudaEvent_t> rate_ev;  // [0] start, [1] downloads done, [2..2+K) uploads, [2+K..2+2K) kernels
     const void *rate_u = nullptr, *rate_last_u = nullptr;
     void *rate_a = nullptr, *rate_last_a = nullptr;
     int rate_cur = -1, rate_variant = -1, rate_last_variant = -1;
@@ -219,6 +228,7 @@ struct pxb_ctx {
     int gbuild_schedule = -1;  // g-build: -1 by problem, 0 lane groups, 1 one warp per node, 2 the same with
                                // its products on the FP64 tensor cores
     int adj_schedule = -1;     // recorded reverse sweep: -1 default (1), 0 both operator streams, 1 reverse-only
+    int rate_chunks = -1;      // pipelined rate call: -1 by mesh size, 1 off, 2..8 node chunks
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
     long long launches = 0;

@@ -44,7 +44,8 @@ def slab():
     rng = np.random.default_rng(2024)
     u0 = rng.standard_normal(3 * m.n) * 1e-6
     u, uo, hh, _ = el.run(u0, None, dt, NSTEPS, [b.as_dict() for b in bcs])
-    return dict(m=m, k=k, rho=rho, dt=dt, bcs=bcs, health0=health0, u0=u0, u=u, uo=uo, h=(hh > 0).astype(np.uint8))
+    return dict(m=m, k=k, rho=rho, dt=dt, bcs=bcs, health0=health0, u0=u0, u=u, uo=uo, h=(hh > 0).astype(np.uint8),
+                E=E, nu=nu, G0=G0)
 
 
 def test_slab_families_built_on_device_equal_reference(ctx, slab):
@@ -88,3 +89,46 @@ def test_slab_mixed_steps_within_1e6(ctx, slab, variant):
     u, _, h, _ = _run(ctx, slab, variant, 1)
     assert np.abs(u - slab["u"]).max() <= 1e-6 * np.abs(slab["u"]).max()
     assert (h != slab["h"]).sum() <= 1e-5 * h.size
+
+
+@pytest.mark.parametrize("variant,chunks", [(1, -1), (13, -1), (13, 8)])
+def test_slab_rate_call_matches_reference(ctx, slab, variant, chunks):
+    """The per-step rate call at full size: variant 1 runs one kernel; the staged variant 13 runs the pipelined call
+    with pinned buffers (node chunks, 3 by default or 8, whose kernels start as their neighbours' u arrives and whose
+    accelerations go down while the next chunk computes), through pageable arrays and through pinned ones (repeated calls with the same pinned buffers
+    capture, then replay, the call as a graph; the bonds broken by the first call stay broken, so the later calls
+    break none and return the same accelerations)."""
+    import ctypes as C
+
+    import torch
+    from oracle import RefEpf
+    m, k = slab["m"], slab["k"]
+    el = RefEpf(m, slab["E"], slab["nu"], slab["rho"], slab["G0"])
+    el.rate(np.zeros(3 * m.n))  # seeds the notch
+    acc_ref, h_ref, _ = el.rate(slab["u0"])
+    h_ref = (h_ref > 0).astype(np.uint8)
+    broken_ref = int((slab["health0"] > 0).sum() - h_ref.sum())
+    assert broken_ref > 100
+    scale = np.abs(acc_ref).max()
+    ctx.set_geometry(m.coords, m.vols, m.off, m.ids, m.delta, m.dx_char, 3, mirror=m.mirror)
+
+    def setup():
+        ctx.epf_setup(k["C11"], k["C12"], k["C66"], slab["rho"], (0.0, 0.0, 0.0), k["sc"], True,
+                      health0=slab["health0"])
+        ctx.epf_set_variant(variant)
+        ctx.epf_set_rate_chunks(chunks)
+
+    setup()
+    acc, nbroken = ctx.epf_rate(slab["u0"])
+    assert np.abs(acc - acc_ref).max() <= 1e-10 * scale
+    assert np.array_equal(ctx.epf_state()[2], h_ref) and nbroken == broken_ref
+    setup()
+    uh = torch.from_numpy(slab["u0"].copy()).pin_memory()
+    ah = torch.zeros(3 * m.n, dtype=torch.float64).pin_memory()
+    for call in range(3):
+        ah.zero_()
+        nb = C.c_longlong(-1)
+        assert ctx.L.pxb_epf_rate(ctx.h, C.c_void_p(uh.data_ptr()), C.c_void_p(ah.data_ptr()), C.byref(nb)) == 0
+        assert np.abs(ah.numpy() - acc_ref).max() <= 1e-10 * scale
+        assert nb.value == (broken_ref if call == 0 else 0)
+        assert np.array_equal(ctx.epf_state()[2], h_ref)
