@@ -410,8 +410,8 @@ class Context:
         _check(self.L.pxb_epf_set_rate_chunks(self.h, int(chunks)))
 
     def epf_set_adjoint_schedule(self, schedule):
-        """The recorded reverse sweep's kernel: -1 default (1), 0 both operator streams, 1 reverse-only
-        (pxb_epf_set_adjoint_schedule)."""
+        """The recorded reverse sweep's kernel: -1 default, 0 both operator streams, 1 reverse-only, 2-4 reverse-only
+        staged through shared memory in three launch configurations (pxb_epf_set_adjoint_schedule)."""
         _check(self.L.pxb_epf_set_adjoint_schedule(self.h, int(schedule)))
 
     def gbuild(self, order=2, precision=FP64, allow_degenerate=False):

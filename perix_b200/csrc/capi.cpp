@@ -549,6 +549,9 @@ extern "C" int pxb_gbuild_set_schedule(pxb_ctx *c, int schedule) {
     return PXB_OK;
 }
 
+// the recorded sweep's adjoint schedule in effect (-1: the staged reverse-only kernel, schedule 2)
+static int adj_sched(const pxb_ctx *c) { return c->adj_schedule < 0 ? 2 : c->adj_schedule; }
+
 extern "C" int pxb_epf_set_rate_chunks(pxb_ctx *c, int chunks) {
     if (!c) return fail(PXB_ERR_INVALID, "pxb_epf_set_rate_chunks: NULL context");
     if (chunks < -1 || chunks == 0 || chunks > 8) return fail(PXB_ERR_INVALID, "pxb_epf_set_rate_chunks: -1 or 1..8");
@@ -560,7 +563,7 @@ extern "C" int pxb_epf_set_rate_chunks(pxb_ctx *c, int chunks) {
 
 extern "C" int pxb_epf_set_adjoint_schedule(pxb_ctx *c, int schedule) {
     if (!c) return fail(PXB_ERR_INVALID, "pxb_epf_set_adjoint_schedule: NULL context");
-    if (schedule < -1 || schedule > 1) return fail(PXB_ERR_INVALID, "pxb_epf_set_adjoint_schedule: -1, 0 or 1");
+    if (schedule < -1 || schedule > 4) return fail(PXB_ERR_INVALID, "pxb_epf_set_adjoint_schedule: -1 .. 4");
     c->adj_schedule = schedule;
     return PXB_OK;
 }
@@ -1593,8 +1596,10 @@ int adj_step(pxb_ctx *c, double *cur, double *other, const double *tsched, int q
     return PXB_OK;
 }
 
+// staged: the recorded sweep's per-step call, whose u, w and rin rows the staged reverse-only kernel (adjoint
+// schedule 2) may copy in bulk (16-byte aligned, padded buffers)
 int adj_kernel(pxb_ctx *c, const double *u, const double *w, double scale, double c_r, const double *rin, double c_w,
-               double *ubar, double c_o, double *rout) {
+               double *ubar, double c_o, double *rout, bool staged = false) {
     const EpfState &e = c->epf;
     EpfAdjArgs a;
     a.n = c->g.n;
@@ -1622,6 +1627,18 @@ int adj_kernel(pxb_ctx *c, const double *u, const double *w, double scale, doubl
     a.c_o = c_o;
     a.rout = rout;
     if (e.adj_sg_on) a.SG = e.adj_SG.as<double>();
+    const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(w) |
+                           reinterpret_cast<uintptr_t>(rin)) & 15u) == 0;
+    if (staged && e.adj_sg_on && adj_sched(c) >= 2 && rin && aligned) {
+        a.maxb = epf_adj_tma_maxb(c->g.dim, c->g.max_family);
+        a.err = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 2);
+        if (e.wait_tries >= 0) a.wait_tries = e.wait_tries;
+        a.evict_first = e.evict_first ? 1 : 0;
+        const cudaError_t err = launch_epf_adjoint_tma(a, c->g.dim, e.precision == PXB_MIXED, adj_sched(c) - 2,
+                                                       c->stream);
+        if (err != cudaSuccess) return cuda_fail(err, "staged adjoint step");
+        return check_launch(c, "staged adjoint step");
+    }
     launch_epf_adjoint(a, c->g.dim, e.precision == PXB_MIXED, epf_grid(c->g.n, c->g.dim, 0), c->stream);
     return check_launch(c, "epf adjoint step");
 }
@@ -1662,7 +1679,7 @@ extern "C" int pxb_epf_record_d(pxb_ctx *c, const double *u0_d, const double *v0
     const int K = all ? std::max(nsteps, 1) : checkpoint_every;
     const int nseg = nsteps > 0 ? (nsteps + K - 1) / K : 0;
     PXB_TRY(dev_alloc(c, e.adj_ckpt, all ? 0 : 2 * bytes * (size_t)std::max(nseg, 1)));
-    PXB_TRY(dev_alloc(c, e.adj_seg, bytes * (size_t)K));
+    PXB_TRY(dev_alloc(c, e.adj_seg, bytes * (size_t)K + 64));  // + the staged adjoint's bulk-copy slack
     for (int k = 0; k < 2; ++k) PXB_TRY(dev_alloc(c, e.adj_p[k], bytes + 64));
     PXB_TRY(dev_alloc(c, e.adj_u0, bytes));
     PXB_TRY(dev_alloc(c, e.adj_t, sizeof(double) * (size_t)std::max(nsteps, 1)));
@@ -1737,14 +1754,15 @@ extern "C" int pxb_epf_adjoint_recorded_d(pxb_ctx *c, const double *ubar_N_d, co
     } sg_off{e};
     e.adj_sg_on = false;
     if (e.adj_GR.p) {  // the frozen mask in reverse-bond order, for this sweep
-        PXB_TRY(dev_alloc(c, e.adj_HR, (size_t)std::max(1LL, c->g.nb)));
+        PXB_TRY(dev_alloc(c, e.adj_HR, (size_t)std::max(1LL, c->g.ldb)));  // to ldb: the staged kernel's copies
+        PXB_CUDA_TRY(cudaMemsetAsync(e.adj_HR.p, 0, e.adj_HR.bytes, c->stream));
         PXB_CUDA_TRY(launch_reverse_health(e.health.as<uint8_t>(), c->g.rev.as<int>(), e.adj_HR.as<uint8_t>(), c->g.nb,
                                            c->stream));
         PXB_TRY(check_launch(c, "reverse health"));
         // the own bonds' operator sums under the frozen mask: with every bond's reverse present, the reverse-only
         // kernel then reads one operator stream per step instead of two (the missing count uses counter slot 5)
         const int nc = c->g.dim == 3 ? 6 : 3;
-        if (c->adj_schedule != 0 &&
+        if (adj_sched(c) != 0 &&
             dev_alloc(c, e.adj_SG, sizeof(double) * nc * (size_t)std::max(1, c->g.n)) == PXB_OK) {
             unsigned int *miss = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 5);
             PXB_CUDA_TRY(cudaMemsetAsync(miss, 0, sizeof(unsigned int), c->stream));
@@ -1763,8 +1781,10 @@ extern "C" int pxb_epf_adjoint_recorded_d(pxb_ctx *c, const double *ubar_N_d, co
     const double dt = e.rec_dt, dt2 = dt * dt;
     const int nseg = nsteps > 0 ? (nsteps + K - 1) / K : 0;
     PXB_TRY(dev_alloc(c, e.adj_A, bytes));
-    PXB_TRY(dev_alloc(c, e.adj_R, bytes));
-    PXB_TRY(dev_alloc(c, e.adj_W, bytes));
+    PXB_TRY(dev_alloc(c, e.adj_R, bytes + 64));  // + the staged adjoint's bulk-copy slack
+    PXB_TRY(dev_alloc(c, e.adj_W, bytes + 64));
+    if (adj_sched(c) >= 2)  // the staged adjoint's wait-failure word
+        PXB_CUDA_TRY(cudaMemsetAsync(e.counters.as<unsigned long long>() + 2, 0, sizeof(unsigned int), c->stream));
     PXB_TRY(dev_alloc(c, e.adj_dC, 4 * sizeof(double)));
     PXB_CUDA_TRY(cudaMemsetAsync(e.adj_dC.p, 0, 4 * sizeof(double), c->stream));
     auto d2d = [&](void *dst, const void *src, size_t b) -> int {
@@ -1802,8 +1822,14 @@ extern "C" int pxb_epf_adjoint_recorded_d(pxb_ctx *c, const double *ubar_N_d, co
             const cudaError_t err = launch_bc_transpose(bc, c->g.n, c->g.dim, A, W, c->stream);
             if (err != cudaSuccess) return cuda_fail(err, "bc transpose");
             c->launches++;
-            PXB_TRY(adj_kernel(c, seg + (size_t)(q - q0) * nd, W, dt2, 1.0, Rv, 2.0, A, -1.0, Rv));
+            PXB_TRY(adj_kernel(c, seg + (size_t)(q - q0) * nd, W, dt2, 1.0, Rv, 2.0, A, -1.0, Rv, true));
         }
+    }
+    if (adj_sched(c) >= 2) {  // a staged wait that ran out fails the sweep
+        unsigned int werr = 0;
+        PXB_TRY(d2h(c, &werr, e.counters.as<unsigned long long>() + 2, sizeof(unsigned int)));
+        PXB_TRY(sync(c));
+        if (werr) return wait_failure(c, werr, "staged adjoint sweep");
     }
     // the start: dJ/du0 = A + R + (da/du)^T (dt^2/2 R), dJ/dv0 = -dt R
     PXB_TRY(adj_kernel(c, e.adj_u0.as<double>(), Rv, 0.5 * dt2, 1.0, A, 1.0, u0bar_d, -dt, v0bar_d));

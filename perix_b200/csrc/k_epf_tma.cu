@@ -618,6 +618,258 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_tma_kernel(EpfArgs a) {
     }
 }
 
+// ---- the reverse-only adjoint step, staged -------------------------------------------------------------------
+// The same per-node sums as epf_adjoint_kernel<..., REV> (k_epf.cu) with the step kernel's pipeline: tiles of NT
+// consecutive nodes, one thread copies a tile's neighbour ids, reverse health bytes, family offsets and node rows
+// (u, the scaled adjoint's source abar and rin) into an S-stage ring by cp.async.bulk, the reverse operators GR of the
+// tile are prefetched into L2 and loaded per lane; LPN lanes per node, UNR reverse bonds a lane per pass.  Per node
+//   U = sum_t hrev_t P(GR_t) Lbar_j - P(SG_m) Lbar_m,   Lbar = scale abar / rho,
+//   ubar_m = c_r rin_m + c_w abar_m + U,   rout_m = c_o abar_m,   dJ/dC += Lbar_j . dP/dC(GR_t) (u_m - u_j).
+// Every wait is bounded; a warp that gives up raises the block's flag, the copies in flight are drained (bounded) and
+// err[0] counts the failure.
+template <int DIM, int NT>
+struct AdjStage {
+    static constexpr unsigned ROW = ((unsigned)(NT * DIM + 2) * 8u + 15u) & ~15u;
+    __host__ __device__ static unsigned h_off(int maxb) { return (unsigned)maxb * 4u; }
+    __host__ __device__ static unsigned off_off(int maxb) { return h_off(maxb) + (unsigned)maxb; }
+    __host__ __device__ static unsigned u_off(int maxb) { return off_off(maxb) + (unsigned)(NT + 16) * 4u; }
+    __host__ __device__ static unsigned w_off(int maxb) { return u_off(maxb) + ROW; }
+    __host__ __device__ static unsigned r_off(int maxb) { return w_off(maxb) + ROW; }
+    __host__ __device__ static unsigned bytes(int maxb) { return r_off(maxb) + ROW; }
+};
+
+// f = P(g) e, P the Navier coefficients of the operator sums g (2D Gxx, Gyy, Gxy; 3D Gxx, Gyy, Gzz, Gxy, Gxz, Gyz)
+template <int DIM>
+__device__ __forceinline__ void adj_apply(const double *g, double C11, double C12, double C66, const double *e,
+                                          double *f) {
+    const double ac = C12 + C66;
+    if constexpr (DIM == 3) {
+        const double p11 = C11 * g[0] + C66 * (g[1] + g[2]), p22 = C11 * g[1] + C66 * (g[0] + g[2]),
+                     p33 = C11 * g[2] + C66 * (g[0] + g[1]);
+        const double p12 = ac * g[3], p13 = ac * g[4], p23 = ac * g[5];
+        f[0] = p11 * e[0] + p12 * e[1] + p13 * e[2];
+        f[1] = p12 * e[0] + p22 * e[1] + p23 * e[2];
+        f[2] = p13 * e[0] + p23 * e[1] + p33 * e[2];
+    } else {
+        const double p11 = C11 * g[0] + C66 * g[1], p22 = C66 * g[0] + C11 * g[1], p12 = ac * g[2];
+        f[0] = p11 * e[0] + p12 * e[1];
+        f[1] = p12 * e[0] + p22 * e[1];
+    }
+}
+
+template <int DIM, bool MIXED, int LPN, int UNR, int S, int MINB, int WPB>
+__global__ void __launch_bounds__(WPB * 32, MINB) epf_adjoint_tma_kernel(EpfAdjArgs a) {
+    using GT = typename std::conditional<MIXED, float, double>::type;
+    constexpr int NC = (DIM == 3) ? 6 : 3;
+    constexpr int GPW = kWarp / LPN;
+    constexpr int NT = WPB * GPW;
+    using SL = AdjStage<DIM, NT>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ unsigned long long bar[S];
+    __shared__ int s_t0a[S];
+    __shared__ unsigned s_done[S];
+    __shared__ int s_last[S];
+    __shared__ int s_fail;
+    __shared__ int s_d0[kTileDesc], s_d1[kTileDesc];
+    __shared__ double s_dC[WPB][3];
+
+    const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+    const int gl = lane & (LPN - 1), grp = lane / LPN;
+    const int maxb = a.maxb;
+    const unsigned stage_bytes = SL::bytes(maxb);
+    const GT *GR = static_cast<const GT *>(a.GR);
+    const double lscale = a.scale * a.inv_rho;
+    const int ntiles = (a.n + NT - 1) / NT;
+    const int mycount = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    auto issue = [&](int k) {
+        const int st = k % S;
+        const int n0 = ((int)blockIdx.x + k * (int)gridDim.x) * NT;
+        const int cnt = min(NT, a.n - n0);
+        const int t0 = k < kTileDesc ? s_d0[k] : __ldg(a.off + n0);
+        const int t1 = k < kTileDesc ? s_d1[k] : __ldg(a.off + n0 + cnt);
+        const int t0a = t0 & ~15;
+        const unsigned nbond = up16((unsigned)(t1 - t0a));
+        unsigned char *base = smem + (size_t)st * stage_bytes;
+        const unsigned bytes_off = up16((unsigned)(cnt + 1) * 4u);
+        const unsigned bytes_row = up16((unsigned)cnt * DIM * 8u);
+        const unsigned total = nbond * 5u + bytes_off + 2u * bytes_row + (a.rin ? bytes_row : 0u);
+        s_t0a[st] = t0a;
+        s_last[st] = k;
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&bar[st], total);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) bulk_prefetch_l2(GR + (size_t)c * a.nb + t0a, nbond * (unsigned)sizeof(GT));
+        if (a.evict_first) {
+            const unsigned long long ef = policy_evict_first();
+            bulk_g2s_hint(base, a.nbr + t0a, nbond * 4u, &bar[st], ef);
+            bulk_g2s_hint(base + SL::h_off(maxb), a.hrev + t0a, nbond, &bar[st], ef);
+        } else {
+            bulk_g2s(base, a.nbr + t0a, nbond * 4u, &bar[st]);
+            bulk_g2s(base + SL::h_off(maxb), a.hrev + t0a, nbond, &bar[st]);
+        }
+        bulk_g2s(base + SL::off_off(maxb), a.off + n0, bytes_off, &bar[st]);
+        bulk_g2s(base + SL::u_off(maxb), a.u + (size_t)n0 * DIM, bytes_row, &bar[st]);
+        bulk_g2s(base + SL::w_off(maxb), a.abar + (size_t)n0 * DIM, bytes_row, &bar[st]);
+        if (a.rin) bulk_g2s(base + SL::r_off(maxb), a.rin + (size_t)n0 * DIM, bytes_row, &bar[st]);
+    };
+
+    if (tid == 0) {
+        for (int st = 0; st < S; ++st) {
+            mbar_init(&bar[st], 1);
+            s_done[st] = 0;
+            s_last[st] = -1;
+        }
+        s_fail = 0;
+        fence_mbar_init();
+    }
+    for (int k = tid; k < mycount && k < kTileDesc; k += WPB * kWarp) {
+        const int n0 = ((int)blockIdx.x + k * (int)gridDim.x) * NT;
+        s_d0[k] = __ldg(a.off + n0);
+        s_d1[k] = __ldg(a.off + min(n0 + NT, a.n));
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int k = 0; k < S && k < mycount; ++k) issue(k);
+
+    double dC[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < mycount; ++k) {
+        const int st = k % S;
+        if (*(volatile int *)&s_fail) break;
+        const bool ok_wait = __all_sync(kFull, mbar_wait(&bar[st], (unsigned)((k / S) & 1), a.wait_tries));
+        if (!ok_wait) {
+            if (lane == 0) atomicExch(&s_fail, 1);
+            break;
+        }
+        unsigned char *base = smem + (size_t)st * stage_bytes;
+        const int *sN = reinterpret_cast<const int *>(base);
+        const unsigned char *sH = base + SL::h_off(maxb);
+        const int *sOff = reinterpret_cast<const int *>(base + SL::off_off(maxb));
+        const double *sU = reinterpret_cast<const double *>(base + SL::u_off(maxb));
+        const double *sW = reinterpret_cast<const double *>(base + SL::w_off(maxb));
+        const double *sR = reinterpret_cast<const double *>(base + SL::r_off(maxb));
+        const int t0a = s_t0a[st];
+        const int n0 = ((int)blockIdx.x + k * (int)gridDim.x) * NT;
+        const int cnt = min(NT, a.n - n0);
+        const int li = wib * GPW + grp;
+        const bool act = li < cnt;
+        const int m = n0 + li;
+        int b0 = 0, b1 = 0;
+        double um[DIM], U[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            um[d] = act ? sU[li * DIM + d] : 0.0;
+            U[d] = 0.0;
+        }
+        if (act) {
+            b0 = sOff[li] - t0a;
+            b1 = sOff[li + 1] - t0a;
+        }
+        const GT *Gt = GR + t0a;
+        for (int t0 = b0 + gl; t0 < b1; t0 += LPN * UNR) {
+            int j[UNR];
+            bool h[UNR];
+            GT gv[UNR][NC];
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                const int t = t0 + q * LPN;
+                const bool ok = t < b1;
+                j[q] = ok ? sN[t] : m;  // past the family: the node itself (a valid gather, masked by h = 0)
+                h[q] = ok && sH[t] != 0;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) gv[q][c] = ok ? __ldcs(Gt + (size_t)c * a.nb + t) : GT(0);
+            }
+            double Lj[UNR][DIM], uj[UNR][DIM];
+#pragma unroll
+            for (int q = 0; q < UNR; ++q)
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    Lj[q][d] = __ldg(a.abar + (size_t)j[q] * DIM + d) * lscale;
+                    uj[q][d] = __ldg(a.u + (size_t)j[q] * DIM + d);
+                }
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                if (!h[q]) continue;
+                double g[NC], f[DIM], e[DIM];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) g[c] = (double)gv[q][c];
+                adj_apply<DIM>(g, a.C11, a.C12, a.C66, Lj[q], f);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    U[d] += f[d];
+                    e[d] = um[d] - uj[q][d];
+                }
+                const double *L = Lj[q];
+                if constexpr (DIM == 3) {
+                    dC[0] += L[0] * g[0] * e[0] + L[1] * g[1] * e[1] + L[2] * g[2] * e[2];
+                    dC[1] += L[0] * (g[3] * e[1] + g[4] * e[2]) + L[1] * (g[3] * e[0] + g[5] * e[2]) +
+                             L[2] * (g[4] * e[0] + g[5] * e[1]);
+                    dC[2] += L[0] * ((g[1] + g[2]) * e[0] + g[3] * e[1] + g[4] * e[2]) +
+                             L[1] * (g[3] * e[0] + (g[0] + g[2]) * e[1] + g[5] * e[2]) +
+                             L[2] * (g[4] * e[0] + g[5] * e[1] + (g[0] + g[1]) * e[2]);
+                } else {
+                    dC[0] += L[0] * g[0] * e[0] + L[1] * g[1] * e[1];
+                    dC[1] += L[0] * g[2] * e[1] + L[1] * g[2] * e[0];
+                    dC[2] += L[0] * (g[1] * e[0] + g[2] * e[1]) + L[1] * (g[2] * e[0] + g[0] * e[1]);
+                }
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) U[d] = group_sum<LPN>(U[d]);
+        if (act && gl < DIM) {
+            // the own bonds' term - P(SG_m) Lbar_m, then the central difference's transpose
+            double sg[NC], Lm[DIM], f[DIM];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) sg[c] = __ldg(a.SG + (size_t)m * NC + c);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) Lm[d] = sW[li * DIM + d] * lscale;
+            adj_apply<DIM>(sg, a.C11, a.C12, a.C66, Lm, f);
+            const int d = gl;
+            const double w = sW[li * DIM + d];
+            const double r = a.rin ? sR[li * DIM + d] : 0.0;
+            const size_t kk = (size_t)m * DIM + d;
+            double ud = 0.0, fd = 0.0;
+#pragma unroll
+            for (int e2 = 0; e2 < DIM; ++e2) {
+                if (e2 == d) {
+                    ud = U[e2];
+                    fd = f[e2];
+                }
+            }
+            a.ubar[kk] = a.c_r * r + a.c_w * w + (ud - fd);
+            if (a.rout) a.rout[kk] = a.c_o * w;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            if (atomicAdd(&s_done[st], 1u) == (unsigned)(WPB - 1)) {
+                atomicExch(&s_done[st], 0u);
+                __threadfence_block();
+                if (k + S < mycount) issue(k + S);
+            }
+        }
+    }
+    __syncthreads();
+    if (s_fail && tid == 0) {
+        for (int st = 0; st < S; ++st)
+            if (s_last[st] >= 0) mbar_wait(&bar[st], (unsigned)((s_last[st] / S) & 1));
+        if (a.err) atomicAdd(a.err, 1u);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dC[c] = group_sum<kWarp>(dC[c]);
+    if (lane == 0) {
+        s_dC[wib][0] = dC[0];
+        s_dC[wib][1] = dC[1];
+        s_dC[wib][2] = dC[2];
+    }
+    __syncthreads();
+    if (tid < 3 && a.dC) {
+        double v = 0.0;
+        for (int w = 0; w < WPB; ++w) v += s_dC[w][tid];
+        atomicAdd(a.dC + tid, v);
+    }
+}
+
 static LaunchShape g_last_shape{0, 0, 0};
 
 LaunchShape epf_tma_last_shape() { return g_last_shape; }
@@ -750,6 +1002,86 @@ static cudaError_t launch_tma_dm(const EpfArgs &a, int which, cudaStream_t s) {
 }
 #undef PXB_CASE2
 #undef PXB_CASE3
+
+// the staged adjoint's configurations per dimension (which = 0, 1, 2): lanes per node, reverse bonds a lane per pass,
+// stages, minimum resident blocks, warps per block
+template <int DIM, int W>
+struct AdjCfg;
+template <>
+struct AdjCfg<3, 0> {
+    static constexpr int LPN = 16, UNR = 2, S = 3, MINB = 2, WPB = 8;
+};
+template <>
+struct AdjCfg<3, 1> {
+    static constexpr int LPN = 16, UNR = 1, S = 3, MINB = 3, WPB = 8;
+};
+template <>
+struct AdjCfg<3, 2> {
+    static constexpr int LPN = 16, UNR = 3, S = 3, MINB = 2, WPB = 8;
+};
+template <>
+struct AdjCfg<2, 0> {
+    static constexpr int LPN = 4, UNR = 2, S = 2, MINB = 4, WPB = 4;
+};
+template <>
+struct AdjCfg<2, 1> {
+    static constexpr int LPN = 4, UNR = 1, S = 2, MINB = 6, WPB = 4;
+};
+template <>
+struct AdjCfg<2, 2> {
+    static constexpr int LPN = 8, UNR = 2, S = 2, MINB = 4, WPB = 4;
+};
+
+int epf_adj_tma_maxb(int dim, int max_family) {
+    // the largest tile of the configurations: 16 nodes in 3D, 32 in 2D
+    const int nt = dim == 3 ? 16 : 32;
+    const long long b = (long long)nt * max_family + 32;
+    return (int)((b + 31) / 32 * 32);
+}
+
+template <int DIM, bool MIXED, int W>
+static cudaError_t launch_adj_tma(const EpfAdjArgs &a, cudaStream_t s) {
+    using Cf = AdjCfg<DIM, W>;
+    constexpr int NT = Cf::WPB * (kWarp / Cf::LPN);
+    static_assert(NT <= (DIM == 3 ? 16 : 32), "epf_adj_tma_maxb sizes the largest tile");
+    auto k = epf_adjoint_tma_kernel<DIM, MIXED, Cf::LPN, Cf::UNR, Cf::S, Cf::MINB, Cf::WPB>;
+    const size_t smem = (size_t)Cf::S * AdjStage<DIM, NT>::bytes(a.maxb);
+    static size_t configured = 0;
+    if (smem > configured) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = smem;
+    }
+    static size_t cap_smem = 0;
+    static long long cap_blocks = 0;
+    if (cap_blocks == 0 || cap_smem != smem) {
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, Cf::WPB * kWarp, smem);
+        cap_blocks = (long long)sms * (per_sm > 0 ? per_sm : 1);
+        cap_smem = smem;
+    }
+    const long long ntiles = ((long long)a.n + NT - 1) / NT;
+    const int grid = (int)(ntiles < cap_blocks ? ntiles : cap_blocks);
+    k<<<grid > 0 ? grid : 1, Cf::WPB * kWarp, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int DIM, bool MIXED>
+static cudaError_t launch_adj_tma_w(const EpfAdjArgs &a, int which, cudaStream_t s) {
+    switch (which) {
+        case 1: return launch_adj_tma<DIM, MIXED, 1>(a, s);
+        case 2: return launch_adj_tma<DIM, MIXED, 2>(a, s);
+        default: return launch_adj_tma<DIM, MIXED, 0>(a, s);
+    }
+}
+
+cudaError_t launch_epf_adjoint_tma(const EpfAdjArgs &a, int dim, bool mixed, int which, cudaStream_t s) {
+    if (!a.SG || !a.GR || !a.hrev || a.maxb <= 0) return cudaErrorInvalidValue;
+    if (dim == 3) return mixed ? launch_adj_tma_w<3, true>(a, which, s) : launch_adj_tma_w<3, false>(a, which, s);
+    return mixed ? launch_adj_tma_w<2, true>(a, which, s) : launch_adj_tma_w<2, false>(a, which, s);
+}
 
 cudaError_t launch_epf_tma(const EpfArgs &a, int dim, bool mixed, int which, cudaStream_t s) {
     if (dim == 3) return mixed ? launch_tma_dm<3, true>(a, which, s) : launch_tma_dm<3, false>(a, which, s);

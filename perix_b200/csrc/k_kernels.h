@@ -235,8 +235,20 @@ struct EpfAdjArgs {
     // healthy bonds of G[c][t] (launch_own_sums), so the own-bond term is one 3x3 product per node and dJ/dC is
     // summed over the reverse bonds; the forward operator stream is not read
     const double *SG = nullptr;
+    // staged reverse-only kernel (launch_epf_adjoint_tma): bonds staged per tile (epf_adj_tma_maxb), the wait-failure
+    // counter and budget, the L2 policy of the bond streams
+    int maxb = 0;
+    unsigned int *err = nullptr;
+    int wait_tries = 1 << 19;
+    int evict_first = 0;
 };
 cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int grid, cudaStream_t s);
+// The reverse-only adjoint step with the tile's ids, reverse health and node rows (u, abar, rin) staged through a
+// shared-memory ring by bulk copies, and the reverse operators prefetched into L2 (SG, GR and hrev required; u, abar
+// and rin 16-byte aligned, readable 64 bytes past n*dim; hrev readable to ldb); which = 0, 1, 2 picks the lanes per
+// node / bonds per pass / occupancy configuration.
+cudaError_t launch_epf_adjoint_tma(const EpfAdjArgs &a, int dim, bool mixed, int which, cudaStream_t s);
+int epf_adj_tma_maxb(int dim, int max_family);
 // SG[m][c] = sum_{t in fam(m), health[t]} G[c][t] (nc = 3 in 2D, 6 in 3D, FP64 sums); missing[0] += the bonds
 // without a reverse bond (rev t < 0)
 cudaError_t launch_own_sums(int n, int dim, bool mixed, const int *off, const int *rev, const uint8_t *health,

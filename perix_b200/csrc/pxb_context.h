@@ -227,7 +227,8 @@ struct pxb_ctx {
     size_t mem_limit = 0;  // device bytes the context may hold (0: no limit beyond the GPU's)
     int gbuild_schedule = -1;  // g-build: -1 by problem, 0 lane groups, 1 one warp per node, 2 the same with
                                // its products on the FP64 tensor cores
-    int adj_schedule = -1;     // recorded reverse sweep: -1 default (1), 0 both operator streams, 1 reverse-only
+    int adj_schedule = -1;     // recorded reverse sweep: -1 default (2), 0 both operator streams, 1 reverse-only,
+                               // 2-4 reverse-only staged (bulk-copy ring) in three launch configurations
     int rate_chunks = -1;      // pipelined rate call: -1 by mesh size, 1 off, 2..8 node chunks
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;

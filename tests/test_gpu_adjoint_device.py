@@ -49,7 +49,7 @@ def _grads(ctx, w, bcs, u0, v0, u_obs, device_run, checkpoint_every, schedule=-1
     return float(J), float(E.grad), u0t.grad.cpu().numpy(), v0t.grad.cpu().numpy(), uN.detach().cpu().numpy()
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("checkpoint_every", [0, 7])
 @pytest.mark.parametrize("kind", ["pins", "reflect"])
 def test_device_adjoint_matches_taped_loop(ctx, plate, kind, checkpoint_every, schedule):  # noqa: F811

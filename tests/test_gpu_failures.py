@@ -4,7 +4,9 @@
   before it reaches the driver; raising the cap lets the same call succeed;
 * a staged step kernel whose consumer mbarrier waits are given no tries (pxb_epf_set_wait_budget(ctx, 0)) gives up
   on every tile, drains its bulk copies with the normal budget and reports the failure (PXB_ERR_CUDA, "wait ran
-  out"); with the default budget restored the same context reproduces the reference trajectory."""
+  out"); with the default budget restored the same context reproduces the reference trajectory;
+* the staged reverse sweep of the device adjoint (adjoint schedule 2) with no tries fails the same way, and with the
+  default budget restored gives the gradient of the unstaged reverse-only sweep."""
 import numpy as np
 import pytest
 
@@ -60,3 +62,42 @@ def test_wait_budget_exhausted_reports_error_and_context_recovers(ctx, variant):
     u, _, h, _ = ctx.epf_state()
     assert np.array_equal(h, d["health"])
     assert np.abs(u - d["u"]).max() <= 1e-10 * np.abs(d["u"]).max()
+
+
+def test_staged_adjoint_wait_budget_exhausted_reports_error_and_recovers(ctx):
+    import ctypes as C
+
+    import perix_b200 as px
+    import torch
+    from test_gpu_parity import epf_context, plate_bcs
+    d = load_golden("epf2d")
+    n = d["coords"].size // 3
+    epf_context(ctx, d, 2)
+    ctx.epf_set_variant(11)
+    ctx.epf_set_bcs(plate_bcs(d, px))
+    dev = torch.device("cuda", 0)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    rng = np.random.default_rng(5)
+    u0 = torch.tensor(rng.standard_normal(2 * n) * 1e-7, device=dev)
+    gN = torch.tensor(rng.standard_normal(2 * n), device=dev)
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    assert ctx.L.pxb_epf_record_d(ctx.h, p(u0), None, C.c_double(float(d["dt"])), 20, 0, None, None) == 0
+
+    def sweep(schedule):
+        ctx.epf_set_adjoint_schedule(schedule)
+        u0b, v0b = torch.empty_like(u0), torch.empty_like(u0)
+        dC = torch.zeros(3, dtype=torch.float64, device=dev)
+        st = ctx.L.pxb_epf_adjoint_recorded_d(ctx.h, p(gN), None, p(u0b), p(v0b), p(dC))
+        torch.cuda.synchronize(dev)
+        return st, u0b.cpu().numpy(), dC.cpu().numpy()
+
+    ctx.epf_set_wait_budget(0)
+    st, _, _ = sweep(2)
+    assert st == 2 and "wait ran out" in ctx.L.pxb_last_error().decode()
+    ctx.epf_set_wait_budget(-1)
+    st, g2, c2 = sweep(2)
+    assert st == 0
+    st, g1, c1 = sweep(1)
+    assert st == 0
+    assert np.abs(g2 - g1).max() <= 1e-12 * np.abs(g1).max()
+    assert np.abs(c2 - c1).max() <= 1e-12 * np.abs(c1).max()
