@@ -277,10 +277,11 @@ int pxb_epf_record_d(pxb_ctx *ctx, const double *u0_d, const double *v0_d, doubl
 int pxb_epf_set_rate_chunks(pxb_ctx *ctx, int chunks);
 /* The reverse sweep's bond-force adjoint kernel: 0 a kernel that streams both the forward and the reverse bonds'
  * operators; 1 the reverse-only kernel: the frozen mask's own-bond operator sums are formed once per sweep, dJ/dC
- * is summed over the reverse bonds, and one operator stream is read per step; 2 (and -1, the default), 3, 4 the
+ * is summed over the reverse bonds, and one operator stream is read per step; 2, 3, 4 (and -1, the default: 4) the
  * reverse-only kernel with the tiles' ids, reverse health and node rows staged by bulk copies through a
- * shared-memory ring (bounded waits: a wait that runs out fails the sweep with PXB_ERR_CUDA), in three launch
- * configurations (3D: 2, 1 or 3 reverse bonds a lane per pass at 16 lanes a node; 2D: 4, 4 or 8 lanes a node).  The reverse-only
+ * shared-memory ring (bounded waits: a wait that runs out fails the sweep with PXB_ERR_CUDA) and each reverse
+ * bond's source node gathered as one interleaved (u, adjoint) row, in three launch configurations (3D: 2, 1 or 3
+ * reverse bonds a lane per pass at 16 lanes a node; 2D: 4, 4 or 8 lanes a node).  The reverse-only
  * kernels apply when every bond has its reverse (symmetric families); other meshes fall back to 0.  Results agree
  * to rounding.  No counterpart in the reference. */
 int pxb_epf_set_adjoint_schedule(pxb_ctx *ctx, int schedule);

@@ -130,7 +130,7 @@ size_t ctx_bytes(const pxb_ctx *c) {
     s += bufsz(e.G) + bufsz(e.P) + bufsz(e.xib) + bufsz(e.health) + bufsz(e.u[0]) + bufsz(e.u[1]) + bufsz(e.accel) + bufsz(e.counters) +
          bufsz(e.umax) + bufsz(e.tsched) + bufsz(e.sc_bond);
     s += bufsz(e.adj_ckpt) + bufsz(e.adj_seg) + bufsz(e.adj_p[0]) + bufsz(e.adj_p[1]) + bufsz(e.adj_A) + bufsz(e.adj_R) +
-         bufsz(e.adj_W) + bufsz(e.adj_t) + bufsz(e.adj_dC) + bufsz(e.adj_umax) + bufsz(e.adj_GR) + bufsz(e.adj_HR) + bufsz(e.adj_u0) + bufsz(e.adj_SG);
+         bufsz(e.adj_W) + bufsz(e.adj_t) + bufsz(e.adj_dC) + bufsz(e.adj_umax) + bufsz(e.adj_GR) + bufsz(e.adj_HR) + bufsz(e.adj_u0) + bufsz(e.adj_SG) + bufsz(e.adj_UW);
     s += bufsz(e.bc.own) + bufsz(e.bc.src_off) + bufsz(e.bc.tgt) + bufsz(e.bc.comp) + bufsz(e.bc.form) +
          bufsz(e.bc.vals);
     const BatchState &bt = c->batch;
@@ -549,8 +549,8 @@ extern "C" int pxb_gbuild_set_schedule(pxb_ctx *c, int schedule) {
     return PXB_OK;
 }
 
-// the recorded sweep's adjoint schedule in effect (-1: the staged reverse-only kernel, schedule 2)
-static int adj_sched(const pxb_ctx *c) { return c->adj_schedule < 0 ? 2 : c->adj_schedule; }
+// the recorded sweep's adjoint schedule in effect (-1: the staged reverse-only kernel, schedule 4)
+static int adj_sched(const pxb_ctx *c) { return c->adj_schedule < 0 ? 4 : c->adj_schedule; }
 
 extern "C" int pxb_epf_set_rate_chunks(pxb_ctx *c, int chunks) {
     if (!c) return fail(PXB_ERR_INVALID, "pxb_epf_set_rate_chunks: NULL context");
@@ -1599,7 +1599,7 @@ int adj_step(pxb_ctx *c, double *cur, double *other, const double *tsched, int q
 // staged: the recorded sweep's per-step call, whose u, w and rin rows the staged reverse-only kernel (adjoint
 // schedule 2) may copy in bulk (16-byte aligned, padded buffers)
 int adj_kernel(pxb_ctx *c, const double *u, const double *w, double scale, double c_r, const double *rin, double c_w,
-               double *ubar, double c_o, double *rout, bool staged = false) {
+               double *ubar, double c_o, double *rout, bool staged = false, const double *uw = nullptr) {
     const EpfState &e = c->epf;
     EpfAdjArgs a;
     a.n = c->g.n;
@@ -1634,6 +1634,7 @@ int adj_kernel(pxb_ctx *c, const double *u, const double *w, double scale, doubl
         a.err = reinterpret_cast<unsigned int *>(e.counters.as<unsigned long long>() + 2);
         if (e.wait_tries >= 0) a.wait_tries = e.wait_tries;
         a.evict_first = e.evict_first ? 1 : 0;
+        a.UW = uw;
         const cudaError_t err = launch_epf_adjoint_tma(a, c->g.dim, e.precision == PXB_MIXED, adj_sched(c) - 2,
                                                        c->stream);
         if (err != cudaSuccess) return cuda_fail(err, "staged adjoint step");
@@ -1774,6 +1775,10 @@ extern "C" int pxb_epf_adjoint_recorded_d(pxb_ctx *c, const double *ubar_N_d, co
             PXB_TRY(d2h(c, &nmiss, miss, sizeof(nmiss)));
             PXB_CUDA_TRY(cudaStreamSynchronize(c->stream));
             e.adj_sg_on = nmiss == 0;
+            // the staged kernel's interleaved (u, w) gather rows (without room for them it gathers u and w apart)
+            if (!e.adj_sg_on || adj_sched(c) < 2 ||
+                dev_alloc(c, e.adj_UW, sizeof(double) * 2 * c->g.dim * (size_t)std::max(1, c->g.n)) != PXB_OK)
+                e.adj_UW.release();
         }
     }
     const size_t nd = (size_t)c->g.n * c->g.dim, bytes = sizeof(double) * nd;
@@ -1819,10 +1824,12 @@ extern "C" int pxb_epf_adjoint_recorded_d(pxb_ctx *c, const double *ubar_N_d, co
             e.rec_seg = s;
         }
         for (int q = q1 - 1; q >= q0; --q) {
-            const cudaError_t err = launch_bc_transpose(bc, c->g.n, c->g.dim, A, W, c->stream);
+            const double *uq = seg + (size_t)(q - q0) * nd;
+            double *uw = e.adj_UW.p ? e.adj_UW.as<double>() : nullptr;
+            const cudaError_t err = launch_bc_transpose(bc, c->g.n, c->g.dim, A, W, c->stream, uq, uw);
             if (err != cudaSuccess) return cuda_fail(err, "bc transpose");
             c->launches++;
-            PXB_TRY(adj_kernel(c, seg + (size_t)(q - q0) * nd, W, dt2, 1.0, Rv, 2.0, A, -1.0, Rv, true));
+            PXB_TRY(adj_kernel(c, uq, W, dt2, 1.0, Rv, 2.0, A, -1.0, Rv, true, uw));
         }
     }
     if (adj_sched(c) >= 2) {  // a staged wait that ran out fails the sweep

@@ -713,7 +713,7 @@ cudaError_t launch_reverse_gather(const void *G, void *GR, const int *rev, long 
 // constants) and keeps w elsewhere; entries are grouped by the node that executes them, which for forms 0 and 2 is
 // the source, so the transpose is a gather without atomics: thread per node.
 template <int DIM>
-__global__ void bc_transpose_kernel(EpfArgs b, int n, const double *a, double *w) {
+__global__ void bc_transpose_kernel(EpfArgs b, int n, const double *a, double *w, const double *u, double *uw) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const unsigned own = b.bc_own ? b.bc_own[i] : 0u;
         double v[DIM];
@@ -732,13 +732,21 @@ __global__ void bc_transpose_kernel(EpfArgs b, int n, const double *a, double *w
         }
 #pragma unroll
         for (int d = 0; d < DIM; ++d) w[(size_t)i * DIM + d] = v[d];
+        if (uw) {  // the staged adjoint's gather rows: (u_i, w_i) interleaved
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                uw[(size_t)i * 2 * DIM + d] = u[(size_t)i * DIM + d];
+                uw[(size_t)i * 2 * DIM + DIM + d] = v[d];
+            }
+        }
     }
 }
 
-cudaError_t launch_bc_transpose(const EpfArgs &bc, int n, int dim, const double *a, double *w, cudaStream_t s) {
+cudaError_t launch_bc_transpose(const EpfArgs &bc, int n, int dim, const double *a, double *w, cudaStream_t s,
+                                const double *u, double *uw) {
     const int grid = (int)std::min<long long>(((long long)n + 255) / 256, 148LL * 16);
-    if (dim == 3) bc_transpose_kernel<3><<<grid > 0 ? grid : 1, 256, 0, s>>>(bc, n, a, w);
-    else bc_transpose_kernel<2><<<grid > 0 ? grid : 1, 256, 0, s>>>(bc, n, a, w);
+    if (dim == 3) bc_transpose_kernel<3><<<grid > 0 ? grid : 1, 256, 0, s>>>(bc, n, a, w, u, uw);
+    else bc_transpose_kernel<2><<<grid > 0 ? grid : 1, 256, 0, s>>>(bc, n, a, w, u, uw);
     return cudaGetLastError();
 }
 

@@ -780,13 +780,32 @@ __global__ void __launch_bounds__(WPB * 32, MINB) epf_adjoint_tma_kernel(EpfAdjA
                 for (int c = 0; c < NC; ++c) gv[q][c] = ok ? __ldcs(Gt + (size_t)c * a.nb + t) : GT(0);
             }
             double Lj[UNR][DIM], uj[UNR][DIM];
+            if (a.UW) {  // one interleaved row (u_j, abar_j) a bond: DIM 16-byte loads
 #pragma unroll
-            for (int q = 0; q < UNR; ++q)
+                for (int q = 0; q < UNR; ++q) {
+                    const double2 *row = reinterpret_cast<const double2 *>(a.UW + (size_t)j[q] * 2 * DIM);
+                    double r[2 * DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    Lj[q][d] = __ldg(a.abar + (size_t)j[q] * DIM + d) * lscale;
-                    uj[q][d] = __ldg(a.u + (size_t)j[q] * DIM + d);
+                    for (int h2 = 0; h2 < DIM; ++h2) {
+                        const double2 v = __ldg(row + h2);
+                        r[2 * h2] = v.x;
+                        r[2 * h2 + 1] = v.y;
+                    }
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        uj[q][d] = r[d];
+                        Lj[q][d] = r[DIM + d] * lscale;
+                    }
                 }
+            } else {
+#pragma unroll
+                for (int q = 0; q < UNR; ++q)
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        Lj[q][d] = __ldg(a.abar + (size_t)j[q] * DIM + d) * lscale;
+                        uj[q][d] = __ldg(a.u + (size_t)j[q] * DIM + d);
+                    }
+            }
 #pragma unroll
             for (int q = 0; q < UNR; ++q) {
                 if (!h[q]) continue;

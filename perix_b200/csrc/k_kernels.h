@@ -241,6 +241,9 @@ struct EpfAdjArgs {
     unsigned int *err = nullptr;
     int wait_tries = 1 << 19;
     int evict_first = 0;
+    // staged kernel, optional: the rows (u_j, abar_j) interleaved, [n][2 dim] (launch_bc_transpose's uw), so that a
+    // reverse bond gathers its source node with dim 16-byte loads
+    const double *UW = nullptr;
 };
 cudaError_t launch_epf_adjoint(const EpfAdjArgs &a, int dim, bool mixed, int grid, cudaStream_t s);
 // The reverse-only adjoint step with the tile's ids, reverse health and node rows (u, abar, rin) staged through a
@@ -263,7 +266,9 @@ cudaError_t launch_reverse_gather(const void *G, void *GR, const int *rev, long 
                                   bool mixed, cudaStream_t s);
 // transpose of the BC program's linear part: w[i] = (component owned by the BC pass ? 0 : a[i]) + sum over the
 // entries executed by node i of +-a[target] (form 0: +, form 2: -, constants: none)
-cudaError_t launch_bc_transpose(const EpfArgs &bc, int n, int dim, const double *a, double *w, cudaStream_t s);
+// with uw: also uw[i] = (u[i], w[i]) interleaved ([n][2 dim]: the staged adjoint's gather rows)
+cudaError_t launch_bc_transpose(const EpfArgs &bc, int n, int dim, const double *a, double *w, cudaStream_t s,
+                                const double *u = nullptr, double *uw = nullptr);
 
 // ---------------------------------------------------------------------------------------------------- apply
 struct ApplyArgs {

@@ -129,6 +129,7 @@ struct EpfState {
     DevBuf adj_HR;       // the health mask in reverse-bond order (rebuilt by every reverse sweep)
     bool adj_GR_none = false;  // no room for adj_GR: the adjoint kernel gathers the reverse bonds' operators
     DevBuf adj_SG;             // per-node sums of the healthy own bonds' operators (rebuilt by every reverse sweep)
+    DevBuf adj_UW;             // the staged adjoint's gather rows (u, w) interleaved, [n][2 dim] (empty: apart)
     bool adj_sg_on = false;    // inside a reverse sweep whose families all have reverse bonds: reverse-only kernel
     // the recorded forward loop (pxb_epf_record_d): rec_steps < 0 when there is none; rec_all: every state kept
     double rec_dt = 0.0;
@@ -227,7 +228,7 @@ struct pxb_ctx {
     size_t mem_limit = 0;  // device bytes the context may hold (0: no limit beyond the GPU's)
     int gbuild_schedule = -1;  // g-build: -1 by problem, 0 lane groups, 1 one warp per node, 2 the same with
                                // its products on the FP64 tensor cores
-    int adj_schedule = -1;     // recorded reverse sweep: -1 default (2), 0 both operator streams, 1 reverse-only,
+    int adj_schedule = -1;     // recorded reverse sweep: -1 default (4), 0 both operator streams, 1 reverse-only,
                                // 2-4 reverse-only staged (bulk-copy ring) in three launch configurations
     int rate_chunks = -1;      // pipelined rate call: -1 by mesh size, 1 off, 2..8 node chunks
     cudaStream_t own = nullptr;
