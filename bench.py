@@ -1264,6 +1264,38 @@ def run_profile(args):
         res["assembly"] = asm
         print(json.dumps(res))
         return
+    if args.profile == "slabadjoint":
+        # the slab at --size x --size x 24: a recorded frozen-mask forward of --steps steps with every state kept,
+        # then its reverse sweep (the adjoint kernels a capture looks at), with adjoint schedule --variant (-1: default)
+        import ctypes as C
+        import torch
+        ctx.close()
+        ws = slab_setup(px, nx=args.size, ny=args.size)
+        Ls = ws["L"]
+        dev = torch.device("cuda", 0)
+        c = px.Context(0)
+        c.set_geometry(Ls.coords, Ls.vols, ws["off"], ws["ids"], ws["delta"], Ls.dxyz[0], 3, mirror=Ls.mirror)
+        k3 = px.elastic_constants(3, False, ws["E"], ws["nu"])
+        c.epf_setup(k3[0], k3[1], k3[2], ws["rho"], (0.0, 0.0, 0.0), 0.0, True, health0=ws["health0"])
+        c.epf_set_bcs(ws["bcs"])
+        c.epf_set_adjoint_schedule(args.variant if 0 <= args.variant <= 4 else -1)  # (the default 8: -1)
+        c.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        rng = np.random.default_rng(3)
+        u0 = torch.tensor(rng.standard_normal(3 * Ls.n) * 1e-6, device=dev)
+        gN = torch.tensor(rng.standard_normal(3 * Ls.n), device=dev)
+        u0b, v0b = torch.empty_like(u0), torch.empty_like(u0)
+        dC = torch.zeros(3, dtype=torch.float64, device=dev)
+        p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+        if c.L.pxb_epf_record_d(c.h, p(u0), None, C.c_double(ws["dt"]), args.steps, 0, None, None):
+            raise RuntimeError(c.L.pxb_last_error().decode())
+        t0 = time.perf_counter()
+        if c.L.pxb_epf_adjoint_recorded_d(c.h, p(gN), None, p(u0b), p(v0b), p(dC)):
+            raise RuntimeError(c.L.pxb_last_error().decode())
+        torch.cuda.synchronize(dev)
+        print(json.dumps({"profile": "slabadjoint", "size": args.size, "nodes": Ls.n, "bonds": ws["nb"],
+                          "steps": args.steps, "sweep_s": time.perf_counter() - t0, "dC": dC.tolist()}))
+        c.close()
+        return
     if args.profile == "slabstep":
         # the 3D slab at --size x --size x 24: 100 steps of variant 1, then --steps timed steps of --variant
         ctx.close()
@@ -1360,7 +1392,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="perix", choices=["perix", "reference"])
-    ap.add_argument("--profile", choices=["step", "gbuild", "clouds", "slab", "slabstep", "cloudsapply", "cloudsgbuild", "refgpu", "ch"], default=None,
+    ap.add_argument("--profile", choices=["step", "gbuild", "clouds", "slab", "slabstep", "slabadjoint", "cloudsapply", "cloudsgbuild", "refgpu", "ch"], default=None,
                     help="run one kernel family only (for profiler captures); prints its own JSON line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--variant", type=int, default=8)
