@@ -139,7 +139,8 @@ size_t ctx_bytes(const pxb_ctx *c) {
     const CsrState &k = c->csr;
     s += bufsz(k.rowptr) + bufsz(k.cols) + bufsz(k.slot) + bufsz(k.diag) + bufsz(k.kvals) + bufsz(k.rhs) +
          bufsz(k.u) + bufsz(k.uold) + bufsz(k.fnode) + bufsz(k.mnode);
-    s += bufsz(c->ch.rev) + bufsz(c->ch.lap) + bufsz(c->ch.ghost) + bufsz(c->scratch);
+    s += bufsz(c->ch.rev) + bufsz(c->ch.lap) + bufsz(c->ch.ghost) + bufsz(c->ch.lrv) + bufsz(c->ch.bfl) +
+         bufsz(c->scratch);
     return s;
 }
 
@@ -2062,6 +2063,19 @@ extern "C" int pxb_assemble_scalar(pxb_ctx *c, int type, double coef, double f, 
     return sync(c);
 }
 
+// the CH assembly's bond-order streams of the fixed geometry (vol_j lap[rev t] and the ghost / reverse flags)
+static int ch_bond_streams(pxb_ctx *c) {
+    ChState &h = c->ch;
+    const size_t nb = (size_t)std::max(1LL, c->g.nb);
+    PXB_TRY(dev_alloc(c, h.lrv, sizeof(double) * nb));
+    PXB_TRY(dev_alloc(c, h.bfl, nb));
+    PXB_CUDA_TRY(launch_ch_bond_streams(c->g.n, c->g.off.as<int>(), c->g.nbr.as<int>(), h.rev.as<int>(),
+                                        h.lap.as<double>(), c->g.vol.as<double>(),
+                                        h.ghost.p ? h.ghost.as<char>() : nullptr, h.lrv.as<double>(),
+                                        h.bfl.as<uint8_t>(), c->stream));
+    return check_launch(c, "ch bond streams");
+}
+
 extern "C" int pxb_ch_set_geometry(pxb_ctx *c, const int *rev, const double *lapbond, const char *isghost) {
     PXB_TRY(need_geometry(c, "pxb_ch_set_geometry"));
     if (!rev || !lapbond) return fail(PXB_ERR_INVALID, "pxb_ch_set_geometry: NULL array");
@@ -2071,6 +2085,7 @@ extern "C" int pxb_ch_set_geometry(pxb_ctx *c, const int *rev, const double *lap
     if (c->g.nb == 0) PXB_TRY(dev_alloc(c, h.rev, sizeof(int) * nb));
     PXB_TRY(dev_upload(c, h.lap, lapbond, sizeof(double) * (size_t)c->g.nb));
     if (isghost) PXB_TRY(dev_upload(c, h.ghost, isghost, (size_t)c->g.n));
+    PXB_TRY(ch_bond_streams(c));
     PXB_TRY(sync(c));
     h.ready = true;
     return PXB_OK;
@@ -2098,6 +2113,7 @@ extern "C" int pxb_ch_build_geometry(pxb_ctx *c) {
                                     c->g.mirror.p ? c->g.mirror.as<int>() : nullptr, o.ops.p, o.precision == PXB_MIXED,
                                     o.nop, sxx, syy, szz, h.lap.as<double>(), h.ghost.as<char>(), c->stream));
     PXB_TRY(check_launch(c, "ch geometry"));
+    PXB_TRY(ch_bond_streams(c));
     PXB_TRY(sync(c));
     h.ready = true;
     return PXB_OK;
@@ -2146,6 +2162,10 @@ static int ch_args(pxb_ctx *c, double kappa, double chi, double dt, const double
     a.uold = uold_d;
     a.kvals = kvals_d;
     a.rhs = rhs_d;
+    if (c->ch.lrv.p && c->ch.bfl.p) {
+        a.lrv = c->ch.lrv.as<double>();
+        a.bfl = c->ch.bfl.as<uint8_t>();
+    }
     return PXB_OK;
 }
 
@@ -2355,6 +2375,10 @@ extern "C" int pxb_assemble_ch(pxb_ctx *c, double kappa, double chi, double dt, 
     a.uold = k.uold.as<double>();
     a.kvals = k.kvals.as<double>();
     a.rhs = k.rhs.as<double>();
+    if (c->ch.lrv.p && c->ch.bfl.p) {
+        a.lrv = c->ch.lrv.as<double>();
+        a.bfl = c->ch.bfl.as<uint8_t>();
+    }
     launch_assemble_ch(a, c->stream);
     PXB_TRY(check_launch(c, "assemble_ch"));
     PXB_TRY(d2h(c, kvals, k.kvals.p, sizeof(double) * (size_t)k.nnz));

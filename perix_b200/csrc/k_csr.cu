@@ -486,17 +486,28 @@ __global__ void __launch_bounds__(256) assemble_ch_kernel(ChAsmArgs a) {
         double rcs = 0.0, rms = 0.0, k12 = 0.0, k21 = 0.0;
         for (int t = b0 + gl; t < b1; t += LPN) {
             const int j = __ldg(a.nbr + t);
-            const bool ghostJ = a.ghost && a.ghost[j];
             const double g2 = a.lap[t];
-            double coeff_c = 0.0;
-            if (!ghostJ) {
-                const int r = a.rev[t];
-                double w;
-                if (r >= 0 && Vi > 0.0) w = 0.5 * (Mi * g2 + (a.vol[j] / Vi) * a.mnode[j] * a.lap[r]);
-                else w = Mi * g2;
-                coeff_c = -w;
+            double coeff_c = 0.0, coeff_mu = 0.0;
+            if (a.lrv) {  // the geometry's bond-order streams: only the mobility and u of j are gathered
+                const uint8_t f = a.bfl[t];
+                if (!(f & 1)) {
+                    double w;
+                    if ((f & 2) && Vi > 0.0) w = 0.5 * (Mi * g2 + (a.lrv[t] / Vi) * a.mnode[j]);
+                    else w = Mi * g2;
+                    coeff_c = -w;
+                    coeff_mu = a.kappa * g2;
+                }
+            } else {
+                const bool ghostJ = a.ghost && a.ghost[j];
+                if (!ghostJ) {
+                    const int r = a.rev[t];
+                    double w;
+                    if (r >= 0 && Vi > 0.0) w = 0.5 * (Mi * g2 + (a.vol[j] / Vi) * a.mnode[j] * a.lap[r]);
+                    else w = Mi * g2;
+                    coeff_c = -w;
+                    coeff_mu = a.kappa * g2;
+                }
             }
-            const double coeff_mu = ghostJ ? 0.0 : a.kappa * g2;
             rcs += coeff_c * (a.u[2 * (size_t)j + 1] - mu);  // u may be only 8-byte aligned (a caller's pointer)
             rms += coeff_mu * (a.u[2 * (size_t)j] - c);
             k12 += coeff_c;
@@ -525,6 +536,24 @@ __global__ void __launch_bounds__(256) assemble_ch_kernel(ChAsmArgs a) {
             a.rhs[rm] = mu - fp + rms;
         }
     }
+}
+
+__global__ void ch_bond_streams_kernel(int n, const int *off, const int *nbr, const int *rev, const double *lap,
+                                       const double *vol, const char *ghost, double *lrv, uint8_t *bfl) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        for (int t = off[i]; t < off[i + 1]; ++t) {
+            const int j = nbr[t], r = rev[t];
+            lrv[t] = r >= 0 ? vol[j] * lap[r] : 0.0;
+            bfl[t] = (uint8_t)(((ghost && ghost[j]) ? 1 : 0) | (r >= 0 ? 2 : 0));
+        }
+    }
+}
+
+cudaError_t launch_ch_bond_streams(int n, const int *off, const int *nbr, const int *rev, const double *lap,
+                                   const double *vol, const char *ghost, double *lrv, uint8_t *bfl, cudaStream_t s) {
+    const int grid = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
+    ch_bond_streams_kernel<<<grid > 0 ? grid : 1, 256, 0, s>>>(n, off, nbr, rev, lap, vol, ghost, lrv, bfl);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_assemble_ch(const ChAsmArgs &a, cudaStream_t s) {

@@ -350,8 +350,15 @@ struct ChAsmArgs {
     const int *rowptr = nullptr, *slot = nullptr, *diag = nullptr;
     const double *u = nullptr, *uold = nullptr;
     double *kvals = nullptr, *rhs = nullptr;
+    // optional bond-order streams of the fixed geometry (launch_ch_bond_streams): lrv[t] = vol[j] lap[rev t] (0
+    // without a reverse bond) and bfl[t] = (ghost j) | 2 (reverse bond exists); with them the kernel gathers only
+    // the neighbour's mobility and u
+    const double *lrv = nullptr;
+    const uint8_t *bfl = nullptr;
 };
 cudaError_t launch_assemble_ch(const ChAsmArgs &a, cudaStream_t s);
+cudaError_t launch_ch_bond_streams(int n, const int *off, const int *nbr, const int *rev, const double *lap,
+                                   const double *vol, const char *ghost, double *lrv, uint8_t *bfl, cudaStream_t s);
 // Stress-coupled Cahn-Hilliard (rows c, mu, u_x, u_y[, u_z] per node; ndof = dim + 2): the device twin of
 // the reference's stressCahnHilliardKernel (src/PDSystem/CudaAssembleKernels.cu:685-874) on the FP64 order-2
 // operator cache.  sl = operator slots of d/dx d/dy d/dz d2/dx2 d2/dxdy d2/dy2 d2/dxdz d2/dydz d2/dz2 (-1 absent).

@@ -197,6 +197,7 @@ struct CsrState {
 struct ChState {
     bool ready = false;
     DevBuf rev, lap, ghost;
+    DevBuf lrv, bfl;  // the assembly's bond-order streams: vol_j lap[rev t]; ghost j | 2 (reverse exists)
     // implicit run (ch_solver.cpp): state, Newton / BiCGStab work vectors, block-Jacobi inverse, history
     DevBuf U, Uold, dU, rhs, kv, mnode, binv, red, ones, hist;
     DevBuf w[11];
