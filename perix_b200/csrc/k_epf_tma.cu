@@ -962,7 +962,7 @@ struct TmaCfg {
     X(12, 8, 2, 2, 6, 4, 1) X(13, 8, 2, 3, 3, 8, 2) X(14, 4, 2, 3, 3, 8, 2) X(15, 4, 4, 3, 2, 8, 3)
 #define PXB_TMA3(X)                                                                                               \
     X(0, 32, 2, 2, 1, 8, 0) X(1, 16, 2, 3, 2, 8, 2) X(2, 16, 2, 3, 2, 8, 10) X(3, 16, 3, 2, 2, 8, 10)            \
-    X(4, 16, 2, 3, 3, 8, 10) X(5, 8, 2, 2, 2, 8, 10) X(6, 32, 2, 2, 2, 4, 1) X(7, 16, 1, 2, 3, 8, 10)            \
+    X(4, 16, 3, 3, 2, 8, 10) X(5, 8, 2, 2, 2, 8, 10) X(6, 32, 2, 2, 2, 4, 1) X(7, 16, 1, 2, 3, 8, 10)            \
     X(8, 16, 2, 2, 2, 8, 10) X(9, 16, 1, 3, 3, 8, 2) X(10, 32, 1, 3, 3, 8, 3) X(11, 32, 2, 3, 2, 8, 10)          \
     X(12, 16, 2, 2, 2, 8, 2) X(13, 16, 2, 3, 3, 8, 6) X(14, 32, 1, 3, 3, 8, 2) X(15, 32, 1, 3, 6, 4, 2)
 #define PXB_CFG(i, l, u, st, mb, w, x) {l, u, st, mb, w, x},
