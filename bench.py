@@ -1398,7 +1398,7 @@ def main():
     ap.add_argument("--variant", type=int, default=8)
     ap.add_argument("--size", type=int, default=120, help="--profile c5step: slab of size x size x 24 nodes")
     ap.add_argument("--headline-only", action="store_true",
-                    help="the plate step line alone (no batched-cloud, slab, reference-GPU and Poisson keys)")
+                    help="the slab step line alone (no plate, batched-cloud, adjoint, reference-GPU, Poisson and CH keys)")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)

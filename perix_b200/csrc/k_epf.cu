@@ -612,11 +612,12 @@ __global__ void __launch_bounds__(kEpfThreads, REV ? 4 : 1) epf_adjoint_kernel(E
 }
 
 // ---- the highest neighbour id of each node chunk (the pipelined rate call's upload dependencies) ---------------
+constexpr int kReachBlocks = 256;  // blocks per chunk
 __global__ void chunk_reach_kernel(const int *off, const int *nbr, const int *bounds, int *reach) {
-    const int k = blockIdx.x;
+    const int k = blockIdx.x / kReachBlocks, part = blockIdx.x % kReachBlocks;
     const int t0 = off[bounds[k]], t1 = off[bounds[k + 1]];
     int r = 0;
-    for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) r = max(r, nbr[t]);
+    for (int t = t0 + part * blockDim.x + threadIdx.x; t < t1; t += kReachBlocks * blockDim.x) r = max(r, nbr[t]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) r = max(r, __shfl_xor_sync(kFull, r, o));
     if ((threadIdx.x & 31) == 0) atomicMax(reach + k, r);
@@ -624,7 +625,7 @@ __global__ void chunk_reach_kernel(const int *off, const int *nbr, const int *bo
 
 cudaError_t launch_chunk_reach(const int *off, const int *nbr, const int *bounds, int nchunks, int *reach,
                                cudaStream_t s) {
-    chunk_reach_kernel<<<nchunks > 0 ? nchunks : 1, 256, 0, s>>>(off, nbr, bounds, reach);
+    chunk_reach_kernel<<<(nchunks > 0 ? nchunks : 1) * kReachBlocks, 256, 0, s>>>(off, nbr, bounds, reach);
     return cudaGetLastError();
 }
 
