@@ -844,7 +844,8 @@ static cudaError_t rate_ops(pxb_ctx *c, const double *u, double *accel, cudaStre
     EpfState &e = c->epf;
     const size_t nd = (size_t)c->g.n * c->g.dim;
     unsigned long long *cnt = e.counters.as<unsigned long long>();
-    if (pinned && e.rate_K > 1 && epf_is_tma(e.variant)) {
+    // (a per-bond critical stretch runs the lane-group kernel, which computes every node: no chunking then)
+    if (pinned && e.rate_K > 1 && epf_is_tma(e.variant) && !e.sc_bond.p) {
         // pieces of u go up on one stream, each chunk's kernel starts once its neighbours' piece is there, and each
         // chunk's acceleration goes down on another stream while the next chunk computes
         const int K = e.rate_K, dim = c->g.dim;
