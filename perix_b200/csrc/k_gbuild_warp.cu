@@ -14,6 +14,11 @@
 //   pass 2  one bond per lane again: op_k = (sum_p X[p][k] m_p) bw / delta^|q_k| for every slot k, written as the
 //           AoS operator vector and/or the SoA Navier subset; MIXED stores FP32 (sums stay FP64) and, at order 2,
 //           the per-node first moments of the stored second-derivative operators (GBuildArgs::defect).
+// With TC (up to nine monomials, the default there) the same three phases use the FP64 tensor cores
+// (mma.sync.m8n8k4.f64): pass 1 accumulates the (0,0) tile of A = (W M)^T M from each chunk's transposed monomials
+// (the ninth row per lane on the CUDA cores), the solve is Gauss-Jordan on [A | diag(q!)] with a row per lane in
+// registers and its residual D - A X a tensor-core product, and pass 2 forms operators 0-7 as 8-bond tiles (the
+// ninth per lane) staged in shared memory and stored as one coalesced block per chunk.
 // Per-node horizons (GBuildArgs::node_delta / node_dxc) follow the reference's variable-horizon path: node i
 // uses its own delta_i and spacing, and bonds longer than delta_i stay out of its moment system and get zero
 // operators (CalcPDOperators.cpp:113-147, 307-354).
@@ -181,8 +186,9 @@ static_assert(offsetof(WarpNodeSmem<14>, X) % 16 == 0 && offsetof(WarpNodeSmem<1
 
 // TC (up to nine monomials): the moment sums and the per-bond operator products run on the FP64 tensor cores
 // (mma m8n8k4): per 32-bond chunk the lanes store their bonds' monomials transposed in shared memory, the moment
-// matrix accumulates as A += (W M)^T M over 4-bond k-steps in three 8x8 tiles (no cross-lane reduction), and in
-// pass 2 each 8-bond tile of the chunk multiplies its monomials by X (held as B fragments in registers)
+// matrix accumulates as A += (W M)^T M over 4-bond k-steps in the (0,0) 8x8 tile (no cross-lane reduction; a
+// ninth monomial's row is summed per lane), and in pass 2 each 8-bond tile of the chunk multiplies its monomials
+// by X (held as B fragments in registers)
 template <int DIM, int ORDER, bool MIXED, bool TC = false>
 __device__ __forceinline__ void gbuild_warp_node(const GBuildArgs &a, int i, int lane,
                                                  WarpNodeSmem<nop_of(DIM, ORDER), TC> &sm) {
