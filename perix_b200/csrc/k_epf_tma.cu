@@ -16,6 +16,8 @@
 // Every wait is bounded: a warp that gives up raises a shared flag and leaves the tile loop, the others leave
 // at their next tile, the block's copies still in flight are waited for (bounded), and the kernel records
 // the failure in err[0].  No TMA multicast is used.
+// The same pipeline serves the device adjoint's reverse sweep (epf_adjoint_tma_kernel, below): the tile's ids,
+// reverse health bytes and node rows staged, the reverse operators prefetched into L2.
 #include <type_traits>
 
 #include "k_kernels.h"
