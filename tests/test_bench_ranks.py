@@ -51,3 +51,14 @@ def test_algorithmic_bytes_formula():
     # 2D FP64: nb*(4 + 3*8 + 1) + N*64
     assert bench.algorithmic_bytes(81200, 2251924, 2, "fp64") == 2251924 * 29 + 81200 * 64
     assert bench.algorithmic_bytes(10, 100, 3, "mixed") == 100 * (4 + 24 + 1) + 10 * 96
+
+
+def test_roofline_traffic_is_the_tuned_variants_capture():
+    """roofline.traffic comes from the committed ncu summary line of the very variant the autotuner picked; a variant
+    without a captured line reports none rather than another variant's bytes."""
+    import bench
+    assert bench.read_traffic("slab", "mixed", 8) == 1.477e9
+    assert bench.read_traffic("slab", "fp64", 13) == 2.594e9
+    assert bench.read_traffic("plate", "mixed", 5) == 43007000.0
+    assert bench.read_traffic("slab", "mixed", 3) is None
+    assert bench.read_traffic("slab", "fp64", 99) is None
